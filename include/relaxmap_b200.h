@@ -1,0 +1,187 @@
+/*
+ * relaxmap_b200: C ABI of the B200 map-equation optimiser (RelaxMap drop-in).
+ *
+ * The reference (uwescience/RelaxMap) is a monolithic OpenMP executable with no
+ * plugin or FFI layer. Its internal driver API is class Network (Module.h:99-200)
+ * called from OmpRelaxmap.cpp; each entry point below replaces one of those
+ * calls, cited per function. Conventions:
+ *   - Ownership: the caller owns every host array; inputs are copied in,
+ *     outputs are written to caller-sized host buffers. The library owns all
+ *     device memory through the opaque handle, freed by rmx_graph_destroy.
+ *   - Errors: every call returns rmx_status; no C++ exception crosses the ABI.
+ *     rmx_last_error() gives a thread-local message for the last failure.
+ *   - Threading: a handle is bound to one CUDA stream and is not thread-safe;
+ *     distinct handles may be used concurrently from different threads.
+ *   - Node ids are int32 (0..N-1), link offsets int64, flows/weights FP64.
+ *   - Code lengths are returned in nats unless the name says bits.
+ * There is no CPU fallback: without a usable CUDA device, calls that compute
+ * return RMX_ERR_CUDA.
+ */
+#ifndef RELAXMAP_B200_H
+#define RELAXMAP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    RMX_OK = 0,
+    RMX_ERR_INVALID = 1,        /* bad argument (null pointer, id out of range, ...) */
+    RMX_ERR_IO = 2,             /* file could not be opened / written */
+    RMX_ERR_FORMAT = 3,         /* malformed Pajek header (the reference exits -1) */
+    RMX_ERR_CUDA = 4,           /* CUDA runtime error or no device */
+    RMX_ERR_OOM = 5,            /* device allocation failed */
+    RMX_ERR_NO_CONVERGENCE = 6, /* iteration cap reached where convergence is required */
+    RMX_ERR_TIMEOUT = 7,        /* a device-side watchdog budget ran out */
+    RMX_ERR_STATE = 8           /* call out of order (e.g. no result yet) */
+} rmx_status;
+
+typedef struct rmx_graph rmx_graph;
+
+/* Solver options: the reference CLI arguments (OmpRelaxmap.cpp:43-79) plus
+ * engine knobs. */
+typedef struct {
+    uint32_t seed;        /* argv[1]: random seed (OmpRelaxmap.cpp:55) */
+    int32_t threads;      /* argv[3]: host threads for parsing (device work ignores it) */
+    int32_t attempts;     /* argv[4]: independent attempts, best code length kept */
+    double threshold;     /* argv[5]: stop threshold in bits (OmpRelaxmap.cpp:62) */
+    double vthresh;       /* argv[6]: per-move threshold, negated internally (:63-66) */
+    int32_t max_iter;     /* argv[7]: sweeps per stage (OmpRelaxmap.cpp:49) */
+    int32_t prior;        /* argv[9] == "prior": active-set sweeps (OmpRelaxmap.cpp:70-72) */
+    int32_t sub_batches;  /* engine: relaxation sub-batches per sweep (0 = automatic) */
+    int32_t verbose;      /* 1: print the reference's progress lines to stdout */
+} rmx_opts;
+
+/* Per-kernel-class device time recorded with CUDA events while profiling is on. */
+typedef struct {
+    int64_t launches;
+    double ms;          /* summed event time */
+    double bytes;       /* algorithmic bytes moved (compulsory traffic model) */
+} rmx_kernel_stat;
+
+enum {
+    RMX_K_SPMV = 0,     /* power-iteration launch (one cooperative launch per solve) */
+    RMX_K_EVAL,         /* move evaluation, all degree bins */
+    RMX_K_COMMIT,       /* move commit + module statistic updates */
+    RMX_K_COARSEN,      /* modules -> super-nodes (sort + segmented reduce) */
+    RMX_K_CODELEN,      /* code length reductions */
+    RMX_K_OTHER,
+    RMX_K_COUNT
+};
+
+typedef struct {
+    rmx_kernel_stat k[RMX_K_COUNT];
+    int64_t sweeps;          /* move sweeps run (node + super-node + coarse-tune) */
+    int64_t supersteps;
+    int64_t power_iters;
+    double total_ms;         /* last rmx_optimize, device time on the handle's stream */
+} rmx_profile;
+
+const char *rmx_last_error(void);
+const char *rmx_version(void);
+void rmx_opts_default(rmx_opts *o);
+
+/* Graph from an edge list held in host memory. Replaces the loaders' edge map
+ * plus the edge preparation of main: duplicate (src,dst) pairs are summed in
+ * input order (FileIO.cpp:157, :220), then self-loops and pairs whose summed
+ * weight is <= 0 are dropped (OmpRelaxmap.cpp:117-135). w may be NULL (weight
+ * 1); node_w may be NULL (uniform teleportation, FileIO.cpp:229), otherwise
+ * the Pajek node weights (FileIO.cpp:114-120: values <= 0 already mapped to 1
+ * by the caller). Builds CSR (out-links) and CSC (in-links) on the device. */
+rmx_status rmx_graph_create(const int32_t *src, const int32_t *dst, const double *w, int64_t n_edges,
+                            int32_t n_nodes, const double *node_w, rmx_graph **out);
+
+/* Load a .net (Pajek) or any other extension (edge list) file with the
+ * reference's parsing rules (FileIO.cpp:32-171, :177-265; format chosen by
+ * extension as at OmpRelaxmap.cpp:60, :93-98) and build the device graph.
+ * Node names are kept for rmx_write_outputs. */
+rmx_status rmx_graph_load_file(const char *path, int32_t threads, rmx_graph **out);
+
+/* Parse a file with the loader rules of rmx_graph_load_file on the host only
+ * (no device work). Raw links in file order with duplicates kept (their sum is
+ * formed by rmx_graph_create) and self-links removed (their count in
+ * *n_self). Call with NULL buffers to get *n_nodes / *n_edges, then again with
+ * src/dst/w of *n_edges entries and node_w of *n_nodes entries (node_w gets
+ * the Pajek node weights, 1 for edge lists). */
+rmx_status rmx_parse_file(const char *path, int32_t threads, int32_t *n_nodes, int64_t *n_edges, int64_t *n_self,
+                          int32_t *src, int32_t *dst, double *w, double *node_w);
+
+rmx_status rmx_graph_destroy(rmx_graph *g);
+
+/* N, kept links, and self-links that were dropped (OmpRelaxmap.cpp:117-142). */
+rmx_status rmx_graph_info(const rmx_graph *g, int32_t *n_nodes, int64_t *n_links, int64_t *n_self_links);
+
+/* Kept links as CSR (off[N+1], dst[E], w[E]: the summed input weights) and
+ * the teleport weight per node (OmpRelaxmap.cpp:113-115). Any pointer may be NULL. */
+rmx_status rmx_graph_links(const rmx_graph *g, int64_t *off, int32_t *dst, double *w, double *teleport);
+
+/* Network::initiate (Module.cpp:210-333): dangling detection, row
+ * normalisation, stationary flow by power iteration (calculateSteadyState,
+ * Module.cpp:340-469: tau = 0.15, at most 200 iterations, stop when the L1
+ * change is <= 1e-15 after at least 50), edge flows. Idempotent. Outputs may
+ * be NULL: p[N] node flow, f[E] edge flow in CSR order, exit[N] singleton exit
+ * (Module.cpp:67-99), dangling[N]; *iters = power iterations; *L0 = initial
+ * code length in nats (calibrate, Module.cpp:474-501). */
+rmx_status rmx_initiate(rmx_graph *g, double *p, double *f, double *exitpr, uint8_t *dangling, int32_t *iters,
+                        double *L0);
+
+/* From-scratch code length of a partition (module id per node, any int32
+ * labels in [0,N)), in nats: Network::calculateCodeLength (Module.cpp:2966-3002),
+ * FP64 throughout. Runs rmx_initiate first if needed. */
+rmx_status rmx_codelength(rmx_graph *g, const int32_t *part, double *L);
+
+/* convertModulesToSuperNodes (Module.cpp:3008-3077) for partition part:
+ * modules renumbered in ascending id order (sn_of_mod[N], -1 for unused ids),
+ * inter-super-node links summed in member-node then link order (bit-identical
+ * FP64 sums), CSR sorted by destination and CSC by source. Buffers are sized N
+ * (+1 for offsets) and E by the caller. Outputs may be NULL individually. */
+rmx_status rmx_coarsen(rmx_graph *g, const int32_t *part, int32_t *n_sn, int64_t *n_sn_links, int32_t *sn_of_mod,
+                       int64_t *out_off, int32_t *out_dst, double *out_f, int64_t *in_off, int32_t *in_src,
+                       double *in_f);
+
+/* The move decision of every node against a fixed snapshot (the evaluation
+ * phase of Network::parallelMove, Module.cpp:1004-1123): candidates are the
+ * modules of out/in neighbours plus, where allow_new[u] != 0 (may be NULL),
+ * an empty module; best_mod[u] is the module with the most negative change
+ * (ties to the lowest id), -2 for a new module, -1 when none is negative;
+ * best_delta[u] is that change in nats. Module statistics are formed from
+ * part. No module or partition state of the handle is modified. */
+rmx_status rmx_evaluate_moves(rmx_graph *g, const int32_t *part, const uint8_t *allow_new, int32_t *best_mod,
+                              double *best_delta);
+
+/* The whole optimiser (OmpRelaxmap.cpp:155-233): initiate, superstep 1
+ * (fine-tune), then alternating fine/coarse supersteps until a superstep gains
+ * less than opts->threshold bits; attempts > 1 repeats with seeds seed+k and
+ * keeps the lowest code length. part_out[N] (may be NULL) receives the module
+ * index per node (the .clu labels minus one); *L_out the code length in nats;
+ * *n_modules the number of non-empty modules. */
+rmx_status rmx_optimize(rmx_graph *g, const rmx_opts *opts, int32_t *part_out, double *L_out, int32_t *n_modules);
+
+/* Per-superstep code lengths (bits) of the last rmx_optimize; returns the count. */
+int32_t rmx_superstep_codelengths(const rmx_graph *g, double *bits, int32_t cap);
+
+/* Write <outdir>/<name>.tree and <outdir>/<name>.clu exactly as the reference
+ * (print_twoLevel_Cluster OmpRelaxmap.cpp:790-812, .clu writer :240-249) for
+ * the partition part and code length L (nats). name keeps its leading '/'. */
+rmx_status rmx_write_outputs(rmx_graph *g, const int32_t *part, double L, const char *outdir, const char *name);
+
+/* Device-time profiling of the handle's kernels (CUDA events on its stream). */
+rmx_status rmx_set_profiling(rmx_graph *g, int32_t on);
+rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out);
+
+/* The CUDA stream (cudaStream_t) all work of this handle is issued on. */
+void *rmx_graph_stream(const rmx_graph *g);
+
+/* Block until the handle's stream is idle. */
+rmx_status rmx_sync(rmx_graph *g);
+
+/* The reference command line (OmpRelaxmap.cpp:41-252), same positional
+ * arguments and output files; returns the process exit code. */
+int rmx_cli_main(int argc, char **argv);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

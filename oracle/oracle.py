@@ -490,3 +490,46 @@ class Ref:
                                     _ptr(steps), 64, C.byref(ns))
         return dict(seconds=t, L_bits=Lb.value, L_computed_bits=Lc.value, n_modules=nm.value, part=part,
                     steps=steps[:min(ns.value, 64)].copy())
+
+
+def _plogp(x: float) -> float:
+    import math
+    return x * math.log(x) if x > 0.0 else 0.0
+
+
+def delta_to(units: dict, mod, ms: dict, sum_exit: float, u: int, m: int) -> float:
+    """Code-length change of moving unit u to module m (-2: an empty module)
+    against a snapshot, by the formula of Module.cpp:1047-1115 (pure Python,
+    for single decisions in tests)."""
+    A = int(mod[u])
+    oA = iA = om = im = 0.0
+    for j in range(units["out_off"][u], units["out_off"][u + 1]):
+        t = mod[units["out_dst"][j]]
+        if t == A:
+            oA += BETA * units["out_f"][j]
+        elif t == m:
+            om += BETA * units["out_f"][j]
+    for j in range(units["in_off"][u], units["in_off"][u + 1]):
+        t = mod[units["in_src"][j]]
+        if t == A:
+            iA += BETA * units["in_f"][j]
+        elif t == m:
+            im += BETA * units["in_f"][j]
+    pu, tu, du, eu = units["p"][u], units["tw"][u], units["dsize"][u], units["exit"][u]
+    eA, PA, DA, TWA = ms["exit"][A], ms["P"][A], ms["D"][A], ms["TW"][A]
+    oA += (ALPHA * pu + BETA * du) * (TWA - tu)
+    iA += (ALPHA * (PA - pu) + BETA * (DA - du)) * tu
+    nexA = eA - eu + oA + iA
+    if m == -2:
+        em = Pm = 0.0
+        nexm = eu
+    else:
+        em, Pm = ms["exit"][m], ms["P"][m]
+        om += (ALPHA * pu + BETA * du) * ms["TW"][m]
+        im += (ALPHA * Pm + BETA * ms["D"][m]) * tu
+        nexm = em + eu - om - im
+    nse = sum_exit + nexA + nexm - eA - em
+    d_all = _plogp(nse) - _plogp(sum_exit)
+    d_exit = _plogp(nexA) + _plogp(nexm) - _plogp(eA) - _plogp(em)
+    d_stay = _plogp(nexA + PA - pu) + _plogp(nexm + Pm + pu) - _plogp(eA + PA) - _plogp(em + Pm)
+    return d_all - 2.0 * d_exit + d_stay

@@ -1,0 +1,237 @@
+"""ctypes binding of librelaxmap_b200.so (include/relaxmap_b200.h).
+
+There is no CPU fallback: importing works without a GPU, but every call that
+computes raises RmxError when the CUDA library or device is unavailable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "librelaxmap_b200.so"
+
+RMX_OK = 0
+STATUS = {0: "RMX_OK", 1: "RMX_ERR_INVALID", 2: "RMX_ERR_IO", 3: "RMX_ERR_FORMAT", 4: "RMX_ERR_CUDA",
+          5: "RMX_ERR_OOM", 6: "RMX_ERR_NO_CONVERGENCE", 7: "RMX_ERR_TIMEOUT", 8: "RMX_ERR_STATE"}
+KERNELS = ["spmv", "eval", "commit", "coarsen", "codelen", "other"]
+
+# every symbol include/relaxmap_b200.h declares
+EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_create", "rmx_graph_load_file",
+           "rmx_parse_file",
+           "rmx_graph_destroy", "rmx_graph_info", "rmx_graph_links", "rmx_initiate", "rmx_codelength",
+           "rmx_coarsen", "rmx_evaluate_moves", "rmx_optimize", "rmx_superstep_codelengths", "rmx_write_outputs",
+           "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main"]
+
+
+class RmxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Opts(C.Structure):
+    _fields_ = [("seed", C.c_uint32), ("threads", C.c_int32), ("attempts", C.c_int32), ("threshold", C.c_double),
+                ("vthresh", C.c_double), ("max_iter", C.c_int32), ("prior", C.c_int32),
+                ("sub_batches", C.c_int32), ("verbose", C.c_int32)]
+
+
+class KernelStat(C.Structure):
+    _fields_ = [("launches", C.c_int64), ("ms", C.c_double), ("bytes", C.c_double)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("k", KernelStat * 6), ("sweeps", C.c_int64), ("supersteps", C.c_int64),
+                ("power_iters", C.c_int64), ("total_ms", C.c_double)]
+
+
+_L = None
+_P = C.c_void_p
+
+
+def lib():
+    """Load the library (raises if it was not built)."""
+    global _L
+    if _L is None:
+        if not LIB_PATH.exists():
+            raise RmxError(4, f"{LIB_PATH} missing: build it with `python -m relaxmap_b200.build`")
+        L = C.CDLL(str(LIB_PATH))
+        L.rmx_last_error.restype = C.c_char_p
+        L.rmx_version.restype = C.c_char_p
+        L.rmx_graph_stream.restype = C.c_void_p
+        L.rmx_superstep_codelengths.restype = C.c_int32
+        for fn in EXPORTS:
+            if fn not in ("rmx_last_error", "rmx_version", "rmx_graph_stream", "rmx_superstep_codelengths",
+                          "rmx_opts_default"):
+                getattr(L, fn).restype = C.c_int
+        _L = L
+    return _L
+
+
+def _check(st: int):
+    if st != RMX_OK:
+        raise RmxError(st, lib().rmx_last_error().decode(errors="replace"))
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def default_opts(**kw) -> Opts:
+    o = Opts()
+    lib().rmx_opts_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Graph:
+    """A graph resident on the GPU (one rmx_graph handle)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        n, e, s = C.c_int32(), C.c_int64(), C.c_int64()
+        _check(lib().rmx_graph_info(self._h, C.byref(n), C.byref(e), C.byref(s)))
+        self.n, self.n_links, self.n_self = n.value, e.value, s.value
+
+    @classmethod
+    def from_edges(cls, src, dst, w=None, n: int | None = None, node_w=None) -> "Graph":
+        src = np.ascontiguousarray(src, dtype=np.int32)
+        dst = np.ascontiguousarray(dst, dtype=np.int32)
+        if n is None:
+            n = int(max(src.max(initial=-1), dst.max(initial=-1))) + 1
+        wa = None if w is None else np.ascontiguousarray(w, dtype=np.float64)
+        nw = None if node_w is None else np.ascontiguousarray(node_w, dtype=np.float64)
+        h = C.c_void_p()
+        _check(lib().rmx_graph_create(_p(src), _p(dst), _p(wa), C.c_int64(len(src)), C.c_int32(n), _p(nw),
+                                      C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_host_ptrs(cls, src_ptr: int, dst_ptr: int, w_ptr: int | None, n_edges: int, n: int) -> "Graph":
+        """Graph from raw host pointers (e.g. pinned buffers)."""
+        h = C.c_void_p()
+        _check(lib().rmx_graph_create(C.c_void_p(src_ptr), C.c_void_p(dst_ptr),
+                                      C.c_void_p(w_ptr) if w_ptr else None, C.c_int64(n_edges), C.c_int32(n), None,
+                                      C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_file(cls, path, threads: int = 1) -> "Graph":
+        h = C.c_void_p()
+        _check(lib().rmx_graph_load_file(str(path).encode(), C.c_int32(threads), C.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if self._h:
+            lib().rmx_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- queries
+    def links(self):
+        off = np.zeros(self.n + 1, dtype=np.int64)
+        dst = np.zeros(max(self.n_links, 1), dtype=np.int32)
+        w = np.zeros(max(self.n_links, 1))
+        tw = np.zeros(self.n)
+        _check(lib().rmx_graph_links(self._h, _p(off), _p(dst), _p(w), _p(tw)))
+        return off, dst[:self.n_links], w[:self.n_links], tw
+
+    def initiate(self) -> dict:
+        n, m = self.n, self.n_links
+        p, f, ex = np.zeros(n), np.zeros(max(m, 1)), np.zeros(n)
+        dg = np.zeros(n, dtype=np.uint8)
+        it, L0 = C.c_int32(), C.c_double()
+        _check(lib().rmx_initiate(self._h, _p(p), _p(f), _p(ex), _p(dg), C.byref(it), C.byref(L0)))
+        return dict(p=p, f=f[:m], exit=ex, dangling=dg, iters=it.value, L0=L0.value)
+
+    def codelength(self, part) -> float:
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        L = C.c_double()
+        _check(lib().rmx_codelength(self._h, _p(part), C.byref(L)))
+        return L.value
+
+    def coarsen(self, part) -> dict:
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        n, m = self.n, max(self.n_links, 1)
+        nsn, nl = C.c_int32(), C.c_int64()
+        snm = np.zeros(n, dtype=np.int32)
+        oo, od, of = np.zeros(n + 1, dtype=np.int64), np.zeros(m, dtype=np.int32), np.zeros(m)
+        io, is_, if_ = np.zeros(n + 1, dtype=np.int64), np.zeros(m, dtype=np.int32), np.zeros(m)
+        _check(lib().rmx_coarsen(self._h, _p(part), C.byref(nsn), C.byref(nl), _p(snm), _p(oo), _p(od), _p(of),
+                                 _p(io), _p(is_), _p(if_)))
+        k, s = nl.value, nsn.value
+        return dict(n_sn=s, sn_of_mod=snm, out_off=oo[:s + 1], out_dst=od[:k], out_f=of[:k], in_off=io[:s + 1],
+                    in_src=is_[:k], in_f=if_[:k])
+
+    def evaluate_moves(self, part, allow_new=None):
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        an = None if allow_new is None else np.ascontiguousarray(allow_new, dtype=np.uint8)
+        bm = np.zeros(self.n, dtype=np.int32)
+        bd = np.zeros(self.n)
+        _check(lib().rmx_evaluate_moves(self._h, _p(part), _p(an), _p(bm), _p(bd)))
+        return bm, bd
+
+    def optimize(self, **kw) -> dict:
+        o = default_opts(**kw)
+        part = np.zeros(self.n, dtype=np.int32)
+        L, nm = C.c_double(), C.c_int32()
+        _check(lib().rmx_optimize(self._h, C.byref(o), _p(part), C.byref(L), C.byref(nm)))
+        steps = np.zeros(256)
+        ns = lib().rmx_superstep_codelengths(self._h, _p(steps), 256)
+        return dict(part=part, L=L.value, L_bits=L.value / math.log(2.0), n_modules=nm.value,
+                    steps_bits=steps[:min(ns, 256)].copy())
+
+    def write_outputs(self, part, L: float, outdir: str, name: str):
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        _check(lib().rmx_write_outputs(self._h, _p(part), C.c_double(L), str(outdir).encode(), name.encode()))
+
+    def set_profiling(self, on: bool):
+        _check(lib().rmx_set_profiling(self._h, int(on)))
+
+    def profile(self) -> dict:
+        pr = Profile()
+        _check(lib().rmx_get_profile(self._h, C.byref(pr)))
+        out = {name: dict(launches=pr.k[i].launches, ms=pr.k[i].ms, bytes=pr.k[i].bytes)
+               for i, name in enumerate(KERNELS)}
+        out.update(sweeps=pr.sweeps, supersteps=pr.supersteps, power_iters=pr.power_iters, total_ms=pr.total_ms)
+        return out
+
+    def stream_ptr(self) -> int:
+        return lib().rmx_graph_stream(self._h) or 0
+
+    def sync(self):
+        _check(lib().rmx_sync(self._h))
+
+
+def parse_file(path, threads: int = 1) -> dict:
+    """Host-only parse with the loader rules (no GPU needed)."""
+    n, m, ns = C.c_int32(), C.c_int64(), C.c_int64()
+    _check(lib().rmx_parse_file(str(path).encode(), C.c_int32(threads), C.byref(n), C.byref(m), C.byref(ns), None,
+                                None, None, None))
+    src = np.zeros(max(m.value, 1), dtype=np.int32)
+    dst = np.zeros(max(m.value, 1), dtype=np.int32)
+    w = np.zeros(max(m.value, 1))
+    nw = np.zeros(max(n.value, 1))
+    _check(lib().rmx_parse_file(str(path).encode(), C.c_int32(threads), C.byref(n), C.byref(m), C.byref(ns), _p(src),
+                                _p(dst), _p(w), _p(nw)))
+    k = m.value
+    return dict(n=n.value, src=src[:k], dst=dst[:k], w=w[:k], node_w=nw[:n.value], n_self=ns.value)
+
+
+def cli(argv: list[str]) -> int:
+    arr = (C.c_char_p * len(argv))(*[a.encode() for a in argv])
+    return lib().rmx_cli_main(len(argv), arr)

@@ -1,0 +1,287 @@
+// extern "C" boundary: every entry point converts exceptions into rmx_status
+// and records a thread-local message (no C++ exception crosses the ABI).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "rmx_graph.hpp"
+#include "rmx_io.hpp"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+rmx_status fail(rmx_status s, const std::string &msg) {
+    g_last_error = msg;
+    return s;
+}
+
+template <typename F>
+rmx_status guard(F &&f) {
+    try {
+        f();
+        return RMX_OK;
+    } catch (const rmx::CudaError &e) {
+        return fail(e.code == cudaErrorMemoryAllocation ? RMX_ERR_OOM : RMX_ERR_CUDA, e.what());
+    } catch (const rmx::FormatError &e) {
+        return fail(RMX_ERR_FORMAT, e.what());
+    } catch (const rmx::IoError &e) {
+        return fail(RMX_ERR_IO, e.what());
+    } catch (const std::invalid_argument &e) {
+        return fail(RMX_ERR_INVALID, e.what());
+    } catch (const std::bad_alloc &) {
+        return fail(RMX_ERR_OOM, "host allocation failed");
+    } catch (const std::exception &e) {
+        return fail(RMX_ERR_CUDA, e.what());
+    }
+}
+
+void need(const void *p, const char *what) {
+    if (!p) throw std::invalid_argument(std::string(what) + " is NULL");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *rmx_last_error(void) { return g_last_error.c_str(); }
+
+const char *rmx_version(void) { return "relaxmap_b200 0.1 (sm_100a)"; }
+
+void rmx_opts_default(rmx_opts *o) {
+    if (!o) return;
+    o->seed = 1;
+    o->threads = 1;
+    o->attempts = 1;
+    o->threshold = 1e-3;
+    o->vthresh = 0.0;
+    o->max_iter = 10;
+    o->prior = 1;
+    o->sub_batches = 0;
+    o->verbose = 0;
+}
+
+rmx_status rmx_graph_create(const int32_t *src, const int32_t *dst, const double *w, int64_t n_edges, int32_t n_nodes,
+                            const double *node_w, rmx_graph **out) {
+    if (!out) return fail(RMX_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    rmx_graph *g = nullptr;
+    rmx_status st = guard([&] {
+        g = new rmx_graph();
+        g->create(src, dst, w, n_edges, n_nodes, node_w);
+    });
+    if (st != RMX_OK) {
+        delete g;
+        return st;
+    }
+    *out = g;
+    return RMX_OK;
+}
+
+rmx_status rmx_graph_load_file(const char *path, int32_t threads, rmx_graph **out) {
+    if (!out) return fail(RMX_ERR_INVALID, "out is NULL");
+    if (!path) return fail(RMX_ERR_INVALID, "path is NULL");
+    *out = nullptr;
+    rmx_graph *g = nullptr;
+    rmx_status st = guard([&] {
+        rmx::ParsedGraph pg = rmx::parse_file(path, threads);
+        if (pg.n <= 0) throw rmx::FormatError(std::string("no nodes in ") + path);
+        g = new rmx_graph();
+        g->create(pg.src.data(), pg.dst.data(), pg.w.data(), (int64_t)pg.src.size(), pg.n,
+                  pg.node_w.empty() ? nullptr : pg.node_w.data());
+        g->n_self += pg.n_self;
+        g->names.swap(pg.names);
+    });
+    if (st != RMX_OK) {
+        delete g;
+        return st;
+    }
+    *out = g;
+    return RMX_OK;
+}
+
+rmx_status rmx_parse_file(const char *path, int32_t threads, int32_t *n_nodes, int64_t *n_edges, int64_t *n_self,
+                          int32_t *src, int32_t *dst, double *w, double *node_w) {
+    return guard([&] {
+        need(path, "path");
+        rmx::ParsedGraph pg = rmx::parse_file(path, threads);
+        if (n_nodes) *n_nodes = pg.n;
+        if (n_edges) *n_edges = (int64_t)pg.src.size();
+        if (n_self) *n_self = pg.n_self;
+        const size_t m = pg.src.size();
+        if (src) std::memcpy(src, pg.src.data(), sizeof(int32_t) * m);
+        if (dst) std::memcpy(dst, pg.dst.data(), sizeof(int32_t) * m);
+        if (w) std::memcpy(w, pg.w.data(), sizeof(double) * m);
+        if (node_w)
+            for (int32_t i = 0; i < pg.n; i++) node_w[i] = pg.node_w.empty() ? 1.0 : pg.node_w[i];
+    });
+}
+
+rmx_status rmx_graph_destroy(rmx_graph *g) {
+    return guard([&] { delete g; });
+}
+
+rmx_status rmx_graph_info(const rmx_graph *g, int32_t *n_nodes, int64_t *n_links, int64_t *n_self_links) {
+    return guard([&] {
+        need(g, "graph");
+        if (n_nodes) *n_nodes = g->N;
+        if (n_links) *n_links = g->E;
+        if (n_self_links) *n_self_links = g->n_self;
+    });
+}
+
+rmx_status rmx_graph_links(const rmx_graph *g, int64_t *off, int32_t *dst, double *w, double *teleport) {
+    return guard([&] {
+        need(g, "graph");
+        cudaStream_t s = g->stream;
+        if (off) RMX_CUDA(cudaMemcpyAsync(off, g->out_off, sizeof(int64_t) * (g->N + 1), cudaMemcpyDeviceToHost, s));
+        if (dst && g->E) RMX_CUDA(cudaMemcpyAsync(dst, g->out_dst, sizeof(int32_t) * g->E, cudaMemcpyDeviceToHost, s));
+        if (w && g->E) RMX_CUDA(cudaMemcpyAsync(w, g->out_w0, sizeof(double) * g->E, cudaMemcpyDeviceToHost, s));
+        if (teleport) RMX_CUDA(cudaMemcpyAsync(teleport, g->tw, sizeof(double) * g->N, cudaMemcpyDeviceToHost, s));
+        RMX_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+rmx_status rmx_initiate(rmx_graph *g, double *p, double *f, double *exitpr, uint8_t *dangling, int32_t *iters,
+                        double *L0) {
+    return guard([&] {
+        need(g, "graph");
+        g->initiate();
+        cudaStream_t s = g->stream;
+        if (p) RMX_CUDA(cudaMemcpyAsync(p, g->p, sizeof(double) * g->N, cudaMemcpyDeviceToHost, s));
+        if (f && g->E) RMX_CUDA(cudaMemcpyAsync(f, g->out_f, sizeof(double) * g->E, cudaMemcpyDeviceToHost, s));
+        if (dangling) RMX_CUDA(cudaMemcpyAsync(dangling, g->dangling, g->N, cudaMemcpyDeviceToHost, s));
+        if (exitpr) {
+            size_t mk = g->scratch.mark();
+            double *ex = g->scratch.alloc<double>(g->N);
+            rmx::singleton_exits(g->N, g->out_off, g->out_f, g->p, g->tw, g->dangling, ex, s);
+            RMX_CUDA(cudaMemcpyAsync(exitpr, ex, sizeof(double) * g->N, cudaMemcpyDeviceToHost, s));
+            RMX_CUDA(cudaStreamSynchronize(s));
+            g->scratch.release(mk);
+        }
+        RMX_CUDA(cudaStreamSynchronize(s));
+        if (iters) *iters = g->power_iters;
+        if (L0) *L0 = g->L0;
+    });
+}
+
+rmx_status rmx_codelength(rmx_graph *g, const int32_t *part, double *L) {
+    return guard([&] {
+        need(g, "graph");
+        need(part, "part");
+        need(L, "L");
+        *L = g->codelength_fp64(part);
+    });
+}
+
+rmx_status rmx_coarsen(rmx_graph *g, const int32_t *part, int32_t *n_sn, int64_t *n_sn_links, int32_t *sn_of_mod,
+                       int64_t *out_off, int32_t *out_dst, double *out_f, int64_t *in_off, int32_t *in_src,
+                       double *in_f) {
+    return guard([&] {
+        need(g, "graph");
+        need(part, "part");
+        g->coarsen_hook(part, n_sn, n_sn_links, sn_of_mod, out_off, out_dst, out_f, in_off, in_src, in_f);
+    });
+}
+
+rmx_status rmx_evaluate_moves(rmx_graph *g, const int32_t *part, const uint8_t *allow_new, int32_t *best_mod,
+                              double *best_delta) {
+    return guard([&] {
+        need(g, "graph");
+        need(part, "part");
+        need(best_mod, "best_mod");
+        need(best_delta, "best_delta");
+        g->evaluate_hook(part, allow_new, best_mod, best_delta);
+    });
+}
+
+rmx_status rmx_optimize(rmx_graph *g, const rmx_opts *opts, int32_t *part_out, double *L_out, int32_t *n_modules) {
+    return guard([&] {
+        need(g, "graph");
+        rmx_opts o;
+        if (opts)
+            o = *opts;
+        else
+            rmx_opts_default(&o);
+        const double L = g->optimize(o, part_out, n_modules);
+        if (L_out) *L_out = L;
+    });
+}
+
+int32_t rmx_superstep_codelengths(const rmx_graph *g, double *bits, int32_t cap) {
+    if (!g) return 0;
+    const int32_t n = (int32_t)g->step_bits.size();
+    for (int32_t i = 0; i < n && i < cap && bits; i++) bits[i] = g->step_bits[i];
+    return n;
+}
+
+rmx_status rmx_write_outputs(rmx_graph *g, const int32_t *part, double L, const char *outdir, const char *name) {
+    return guard([&] {
+        need(g, "graph");
+        need(part, "part");
+        need(outdir, "outdir");
+        need(name, "name");
+        g->initiate();
+        std::vector<int32_t> pv(part, part + g->N);
+        for (int32_t m : pv)
+            if ((uint32_t)m >= (uint32_t)g->N) throw std::invalid_argument("module id outside 0..N-1");
+        std::vector<double> size(g->N);
+        RMX_CUDA(cudaMemcpyAsync(size.data(), g->p, sizeof(double) * g->N, cudaMemcpyDeviceToHost, g->stream));
+        RMX_CUDA(cudaStreamSynchronize(g->stream));
+        std::vector<uint8_t> seen(g->N, 0);
+        int32_t nm = 0;
+        for (int32_t m : pv)
+            if (!seen[m]) {
+                seen[m] = 1;
+                nm++;
+            }
+        const std::string base = std::string(outdir) + "/" + name;
+        rmx::write_tree(base + ".tree", L / std::log(2.0), nm, pv, size, g->names);
+        rmx::write_clu(base + ".clu", pv);
+    });
+}
+
+rmx_status rmx_set_profiling(rmx_graph *g, int32_t on) {
+    return guard([&] {
+        need(g, "graph");
+        g->timers.on = on != 0;
+        g->timers.reset();
+        g->prof = rmx_profile{};
+        g->edges_evaluated = 0;
+        g->units_evaluated = 0;
+    });
+}
+
+rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out) {
+    return guard([&] {
+        need(g, "graph");
+        need(out, "out");
+        rmx_graph *h = const_cast<rmx_graph *>(g);
+        if (h->timers.on) h->timers.resolve();
+        *out = g->prof;
+        for (int k = 0; k < RMX_K_COUNT; k++) {
+            out->k[k].launches = g->timers.launches[k];
+            out->k[k].ms = g->timers.ms[k];
+            out->k[k].bytes = 0.0;
+        }
+        // compulsory traffic of the move evaluation: per link visit the
+        // neighbour id (4 B), its fixed-point flow (8 B) and the neighbour's
+        // module (4 B); per evaluated unit its list entry, offsets, attributes,
+        // module, own module statistics and the proposal written.
+        out->k[RMX_K_EVAL].bytes = 16.0 * (double)g->edges_evaluated + 108.0 * (double)g->units_evaluated;
+        out->power_iters = g->power_iters;
+    });
+}
+
+void *rmx_graph_stream(const rmx_graph *g) { return g ? (void *)g->stream : nullptr; }
+
+rmx_status rmx_sync(rmx_graph *g) {
+    return guard([&] {
+        need(g, "graph");
+        RMX_CUDA(cudaStreamSynchronize(g->stream));
+    });
+}
+
+}  // extern "C"

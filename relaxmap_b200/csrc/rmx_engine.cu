@@ -1,0 +1,911 @@
+// The optimiser driver: graph construction, initiate, and the superstep loop of
+// the reference (OmpRelaxmap.cpp:155-233, stochastic_greedy_partition :263-429,
+// generate_sub_modules :502-638) orchestrating the device kernels.
+//
+// Control flow and stop rules are the reference's; the moves themselves are
+// the bulk-synchronous sub-batch sweeps of rmx_moves.cu. Every sweep ends with
+// one small device->host read (code length, moved nodes, next active count),
+// the only synchronisation inside the loop.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "rmx_graph.hpp"
+
+using namespace rmx;
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+const double kLn2 = std::log(2.0);
+
+__global__ void k_fill(double *a, int64_t n, double v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        a[i] = v;
+}
+
+__global__ void k_flags_nonempty(int32_t cap, const int32_t *count, int64_t *flag) {
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < cap; m += (int64_t)gridDim.x * blockDim.x)
+        flag[m] = count[m] > 0 ? 1 : 0;
+}
+
+// modules -> super-nodes (convertModulesToSuperNodes, Module.cpp:3015-3022 and
+// SuperNode(Module, int) Node.cpp:76-106): the super-node carries the module's
+// statistics exactly and keeps the module id.
+__global__ void k_sn_from_modules(int32_t cap, const int32_t *count, const int64_t *snid, const Stat4 *mstat,
+                                  int32_t *sn_mod, Stat4 *sn_attr, int32_t *sn_nnodes, int32_t *sn_inst) {
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < cap; m += (int64_t)gridDim.x * blockDim.x) {
+        if (count[m] <= 0) continue;
+        const int64_t s = snid[m];
+        sn_mod[s] = (int32_t)m;
+        sn_attr[s] = mstat[m];
+        sn_nnodes[s] = count[m];
+        sn_inst[s] = 0;
+    }
+}
+
+__global__ void k_group_of_nodes(int32_t n, const int32_t *mod, const int64_t *snid, int32_t *node_sn) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        node_sn[v] = (int32_t)snid[mod[v]];
+}
+
+__global__ void k_project(int32_t n, const int32_t *node_sn, const int32_t *sn_mod, int32_t *nmod) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        nmod[v] = sn_mod[node_sn[v]];
+}
+
+// Intra-module links for the coarse-tune sub-networks (generate_network_from_module,
+// OmpRelaxmap.cpp:664-684): per row, the links whose other end shares the module.
+__global__ void k_intra_count(int32_t n, const int64_t *off, const int32_t *nbr, const int32_t *mod, int64_t *cnt) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = gw; u < n; u += nw) {
+        const int32_t m = mod[u];
+        int c = 0;
+        for (int64_t e = off[u] + lane; e < off[u + 1]; e += 32) c += mod[nbr[e]] == m;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+        if (lane == 0) cnt[u] = c;
+    }
+}
+
+__global__ void k_intra_fill(int32_t n, const int64_t *off, const int32_t *nbr, const fx_t *fx, const int32_t *mod,
+                             const int64_t *noff, int32_t *nnbr, fx_t *nfx, fx_t *row_sum) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = gw; u < n; u += nw) {
+        const int32_t m = mod[u];
+        int64_t pos = noff[u];
+        fx_t sum = 0;
+        for (int64_t base = off[u]; base < off[u + 1]; base += 32) {
+            const int64_t e = base + lane;
+            const bool keep = e < off[u + 1] && mod[nbr[e]] == m;
+            const unsigned bal = __ballot_sync(kFull, keep);
+            if (keep) {
+                const int64_t q = pos + __popc(bal & lt);
+                nnbr[q] = nbr[e];
+                nfx[q] = fx[e];
+                sum += fx[e];
+            }
+            pos += __popc(bal);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFull, sum, o);
+        if (row_sum && lane == 0) row_sum[u] = sum;
+    }
+}
+
+__global__ void k_sub_attr(int32_t n, const Stat4 *nattr, const fx_t *intra_out, Stat4 *sattr) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        Stat4 a = nattr[v];
+        a.OUT = intra_out[v];
+        sattr[v] = a;
+    }
+}
+
+__global__ void k_sub_s0(int32_t n, const double *p, const int32_t *inst, fx_t *s0) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x)
+        atomic_add_fx(s0 + inst[v], to_fxl(plogp(p[v])));
+}
+
+__global__ void k_inst_active(int32_t n, const int32_t *count, uint8_t *active) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        active[k] = count[k] > 1 ? 1 : 0;
+}
+
+// partition_module_network's stop rule per sub-network (OmpRelaxmap.cpp:458-459).
+__global__ void k_inst_stop(int32_t n, const double *L, double *L_prev, uint8_t *active, double threshold,
+                            double ln2, unsigned long long *n_active) {
+    unsigned long long c = 0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+        if (!active[k]) continue;
+        if ((L_prev[k] - L[k]) / ln2 < threshold)
+            active[k] = 0;
+        else
+            c++;
+        L_prev[k] = L[k];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(n_active, c);
+}
+
+__global__ void k_copy_L(int32_t n, const double *L, double *L_prev) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        L_prev[k] = L[k];
+}
+
+// super-nodes of sub-modules (SuperNode(SubModule*,...) Node.cpp:108-137): sums
+// of the member nodes; the module is the parent module of the members.
+__global__ void k_sn_from_nodes(int32_t n, const int32_t *node_sn, const int32_t *nmod, const Stat4 *nattr,
+                                int32_t *sn_mod, Stat4 *sn_attr, int32_t *sn_nnodes) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t s = node_sn[v];
+        sn_mod[s] = nmod[v];
+        const Stat4 a = nattr[v];
+        atomic_add_fx(&sn_attr[s].P, a.P);
+        atomic_add_fx(&sn_attr[s].TW, a.TW);
+        atomic_add_fx(&sn_attr[s].D, a.D);
+        atomicAdd(sn_nnodes + s, 1);
+    }
+}
+
+__global__ void k_sn_out(int32_t n, const int64_t *off, const fx_t *fx, Stat4 *attr) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
+        fx_t o = 0;
+        for (int64_t e = off[s]; e < off[s + 1]; e++) o += fx[e];
+        attr[s].OUT = o;
+    }
+}
+
+__global__ void k_count_nonzero(int32_t cap, const int32_t *count, unsigned long long *out) {
+    unsigned long long c = 0;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < cap; m += (int64_t)gridDim.x * blockDim.x)
+        c += count[m] > 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+__global__ void k_max_degree(int32_t n, const int64_t *out_off, const int64_t *in_off, unsigned long long *mx) {
+    unsigned long long d = 0;
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+        unsigned long long x = (out_off[u + 1] - out_off[u]) + (in_off[u + 1] - in_off[u]);
+        d = x > d ? x : d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long y = __shfl_xor_sync(kFull, d, o);
+        d = y > d ? y : d;
+    }
+    if ((threadIdx.x & 31) == 0 && d) atomicMax(mx, d);
+}
+
+// From-scratch FP64 code length (calculateCodeLength, Module.cpp:2966-3002).
+__global__ void k_fp64_nodes(int32_t n, const int32_t *part, const double *p, const double *tw, const uint8_t *dang,
+                             double *P, double *TW, double *D, int32_t *cnt) {
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t m = part[v];
+        atomicAdd(P + m, p[v]);
+        atomicAdd(TW + m, tw[v]);
+        if (dang[v]) atomicAdd(D + m, p[v]);
+        atomicAdd(cnt + m, 1);
+    }
+}
+
+__global__ void k_fp64_out(int32_t n, const int64_t *off, const int32_t *dst, const double *f, const int32_t *part,
+                           double *OUT) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t u = gw; u < n; u += nw) {
+        const int32_t m = part[u];
+        double o = 0.0;
+        for (int64_t e = off[u] + lane; e < off[u + 1]; e += 32)
+            if (part[dst[e]] != m) o += f[e];
+#pragma unroll
+        for (int q = 16; q > 0; q >>= 1) o += __shfl_xor_sync(kFull, o, q);
+        if (lane == 0 && o != 0.0) atomicAdd(OUT + m, o);
+    }
+}
+
+__global__ void k_fp64_terms(int32_t n, const double *P, const double *TW, const double *D, const double *OUT,
+                             const int32_t *cnt, const double *p, double *parts) {
+    __shared__ double sh[4][8];
+    double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < n; m += (int64_t)gridDim.x * blockDim.x) {
+        a3 += plogp(p[m]);
+        if (cnt[m] <= 0) continue;
+        double e = kAlpha * (1.0 - TW[m]) * P[m];
+        e += kBeta * (OUT[m] + (1.0 - TW[m]) * D[m]);
+        a0 += e;
+        a1 += plogp(e);
+        a2 += plogp(e + P[m]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(kFull, a0, o);
+        a1 += __shfl_xor_sync(kFull, a1, o);
+        a2 += __shfl_xor_sync(kFull, a2, o);
+        a3 += __shfl_xor_sync(kFull, a3, o);
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        sh[0][w] = a0;
+        sh[1][w] = a1;
+        sh[2][w] = a2;
+        sh[3][w] = a3;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double v = 0;
+        for (int q = 0; q < 8; q++) v += sh[threadIdx.x][q];
+        parts[4 * blockIdx.x + threadIdx.x] = v;
+    }
+}
+
+uint32_t mix_seed(uint32_t a, uint64_t b) {
+    uint64_t x = a * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull);
+    x ^= x >> 31;
+    x *= 0xBF58476D1CE4E5B9ull;
+    x ^= x >> 29;
+    return (uint32_t)(x ^ (x >> 32));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ Timers
+namespace rmx {
+
+void Timers::begin(int k, cudaStream_t s) {
+    if (!on) return;
+    if (used == pool.size()) {
+        cudaEvent_t e;
+        RMX_CUDA(cudaEventCreate(&e));
+        pool.push_back(e);
+    }
+    open[k] = pool[used++];
+    RMX_CUDA(cudaEventRecord(open[k], s));
+}
+
+void Timers::end(int k, cudaStream_t s) {
+    if (!on) return;
+    if (used == pool.size()) {
+        cudaEvent_t e;
+        RMX_CUDA(cudaEventCreate(&e));
+        pool.push_back(e);
+    }
+    cudaEvent_t e = pool[used++];
+    RMX_CUDA(cudaEventRecord(e, s));
+    pending.push_back({k, open[k], e});
+    launches[k]++;
+    if (used > 16384) resolve();
+}
+
+void Timers::resolve() {
+    for (auto &p : pending) {
+        RMX_CUDA(cudaEventSynchronize(p.b));
+        float t = 0;
+        RMX_CUDA(cudaEventElapsedTime(&t, p.a, p.b));
+        ms[p.k] += t;
+    }
+    pending.clear();
+    used = 0;
+}
+
+void Timers::reset() {
+    pending.clear();
+    used = 0;
+    for (int k = 0; k < kTimerCount; k++) {
+        ms[k] = 0;
+        launches[k] = 0;
+    }
+}
+
+void Timers::destroy() {
+    for (auto e : pool) cudaEventDestroy(e);
+    pool.clear();
+    pending.clear();
+    used = 0;
+}
+
+}  // namespace rmx
+
+// ------------------------------------------------------------------ rmx_graph
+
+rmx_graph::~rmx_graph() {
+    timers.destroy();
+    if (work.gtable) cudaFree(work.gtable);
+    if (work.gkeys) cudaFree(work.gkeys);
+    perm.destroy();
+    scratch.destroy();
+    if (stream) cudaStreamDestroy(stream);
+}
+
+void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, int64_t n_edges, int32_t n,
+                       const double *node_weights) {
+    if (n <= 0) throw std::invalid_argument("graph needs at least one node");
+    if (n_edges < 0 || (n_edges > 0 && (!src || !dst))) throw std::invalid_argument("edge arrays missing");
+    if (n_edges >= (int64_t(1) << 31)) throw std::invalid_argument("more than 2^31-1 input edges");
+    for (int64_t e = 0; e < n_edges; e++)
+        if ((uint32_t)src[e] >= (uint32_t)n || (uint32_t)dst[e] >= (uint32_t)n)
+            throw std::invalid_argument("edge endpoint outside 0..N-1");
+    N = n;
+    node_w.assign(n, 1.0);
+    tot_w = (double)n;  // FileIO.cpp:229
+    if (node_weights) {
+        tot_w = 0.0;
+        for (int32_t i = 0; i < n; i++) {
+            node_w[i] = node_weights[i];
+            tot_w += node_weights[i];
+        }
+    }
+    RMX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    configure_eval_kernels();
+    const int64_t Eb = std::max<int64_t>(n_edges, 1);
+    scratch.init((size_t)(88 * Eb + 24 * (int64_t)n) + (64u << 20));
+    // long-lived arrays: node CSR/CSC, three levels, module and instance state
+    perm.init((size_t)(112 * Eb + 440 * (int64_t)n) + (64u << 20));
+    out_off = perm.alloc<int64_t>(n + 1);
+    in_off = perm.alloc<int64_t>(n + 1);
+    int32_t *d_src = scratch.alloc<int32_t>(Eb), *d_dst = scratch.alloc<int32_t>(Eb);
+    double *d_w = scratch.alloc<double>(Eb);
+    if (n_edges > 0) {
+        RMX_CUDA(cudaMemcpyAsync(d_src, src, sizeof(int32_t) * n_edges, cudaMemcpyHostToDevice, stream));
+        RMX_CUDA(cudaMemcpyAsync(d_dst, dst, sizeof(int32_t) * n_edges, cudaMemcpyHostToDevice, stream));
+        if (w)
+            RMX_CUDA(cudaMemcpyAsync(d_w, w, sizeof(double) * n_edges, cudaMemcpyHostToDevice, stream));
+        else {
+            k_fill<<<blocks_for(n_edges, 256, 4096), 256, 0, stream>>>(d_w, n_edges, 1.0);
+            RMX_LAUNCHED();
+        }
+    }
+    // kept links <= input edges: size link arrays by the input count
+    out_dst = perm.alloc<int32_t>(Eb);
+    out_w0 = perm.alloc<double>(Eb);
+    in_src = perm.alloc<int32_t>(Eb);
+    in_w = perm.alloc<double>(Eb);
+    dtmp = perm.alloc<int64_t>(16);
+    size_t mk = scratch.mark();
+    CsrBuild cb = build_csr(n, n_edges, d_src, d_dst, d_w, out_off, out_dst, out_w0, in_off, in_src, in_w, scratch,
+                            stream, dtmp);
+    scratch.release(0);
+    (void)mk;
+    E = cb.n_links;
+    n_self = cb.n_self;
+    const int64_t Em = std::max<int64_t>(E, 1);
+    out_f = perm.alloc<double>(Em);
+    out_fx = perm.alloc<fx_t>(Em);
+    in_fx = perm.alloc<fx_t>(Em);
+    tw = perm.alloc<double>(n);
+    p = perm.alloc<double>(n);
+    dangling = perm.alloc<uint8_t>(n);
+    std::vector<double> twh(n);
+    for (int32_t i = 0; i < n; i++) twh[i] = node_w[i] / tot_w;  // OmpRelaxmap.cpp:113-115
+    RMX_CUDA(cudaMemcpyAsync(tw, twh.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+    nattr = perm.alloc<Stat4>(n);
+    nmod = perm.alloc<int32_t>(n);
+    zeros = perm.alloc<int32_t>(n);
+    node_sn = perm.alloc<int32_t>(n);
+    submod = perm.alloc<int32_t>(n);
+    s0 = perm.alloc<fx_t>(1);
+    RMX_CUDA(cudaMemsetAsync(zeros, 0, sizeof(int32_t) * n, stream));
+    alloc_engine();
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    // SpMV sub-warp width from the mean in-degree
+    const double avg = (double)E / n;
+    spmv_vec = avg <= 6 ? 4 : (avg <= 12 ? 8 : (avg <= 24 ? 16 : 32));
+}
+
+void rmx_graph::alloc_engine() {
+    const int32_t n = N;
+    const int64_t Em = std::max<int64_t>(E, 1);
+    node_lv.n = n;
+    node_lv.m = E;
+    node_lv.out_off = out_off;
+    node_lv.in_off = in_off;
+    node_lv.out_dst = out_dst;
+    node_lv.in_src = in_src;
+    node_lv.out_fx = out_fx;
+    node_lv.in_fx = in_fx;
+    node_lv.attr = nattr;
+    node_lv.mod = nmod;
+    node_lv.inst = zeros;
+    node_lv.nnodes = nullptr;
+    for (Level *lv : {&sn_lv, &sub_lv}) {
+        lv->out_off = perm.alloc<int64_t>(n + 1);
+        lv->in_off = perm.alloc<int64_t>(n + 1);
+        lv->out_dst = perm.alloc<int32_t>(Em);
+        lv->in_src = perm.alloc<int32_t>(Em);
+        lv->out_fx = perm.alloc<fx_t>(Em);
+        lv->in_fx = perm.alloc<fx_t>(Em);
+        lv->attr = perm.alloc<Stat4>(n);
+        lv->nnodes = perm.alloc<int32_t>(n);
+    }
+    sn_lv.mod = perm.alloc<int32_t>(n);
+    sn_lv.inst = zeros;
+    sub_lv.mod = submod;
+    sub_lv.inst = nmod;  // instance of a node in coarse-tune = its parent module
+    sub_lv.nnodes = nullptr;
+    for (ModState *M : {&mods, &submods}) {
+        M->cap = n;
+        M->stat = perm.alloc<Stat4>(n);
+        M->count = perm.alloc<int32_t>(n);
+        M->inst = perm.alloc<int32_t>(n);
+    }
+    inst1.n = 1;
+    instsub.n = n;
+    for (InstState *I : {&inst1, &instsub}) {
+        const int32_t k = I->n;
+        I->sum_exit = perm.alloc<double>(k);
+        I->L = perm.alloc<double>(k);
+        I->L_prev = perm.alloc<double>(k);
+        I->s0 = perm.alloc<fx_t>(k);
+        I->acc = perm.alloc<fx_t>(3 * (int64_t)k);
+        I->active = perm.alloc<uint8_t>(k);
+    }
+    inst1.s0 = s0;
+    work.list = perm.alloc<int32_t>(n);
+    work.list2 = perm.alloc<int32_t>(n);
+    work.bucket = perm.alloc<uint16_t>(n);
+    work.bucket_off = perm.alloc<int64_t>(260);
+    work.ranges = perm.alloc<int64_t>(2 * 86);
+    work.prop = perm.alloc<int32_t>(n);
+    work.pdelta = perm.alloc<double>(n);
+    work.ptarget = perm.alloc<int32_t>(n);
+    work.prevmod = perm.alloc<int32_t>(n);
+    work.stamp = perm.alloc<uint32_t>(n);
+    work.next_active = perm.alloc<uint8_t>(n);
+    work.free_list = perm.alloc<int32_t>(n);
+    work.claim = perm.alloc<unsigned long long>(n);
+    work.counters = perm.alloc<int64_t>(kCntSlots);
+    RMX_CUDA(cudaMemsetAsync(work.stamp, 0, sizeof(uint32_t) * n, stream));
+    RMX_CUDA(cudaMemsetAsync(work.claim, 0, sizeof(unsigned long long) * n, stream));
+    RMX_CUDA(cudaMemsetAsync(work.next_active, 0, n, stream));
+    RMX_CUDA(cudaMemsetAsync(work.counters, 0, sizeof(int64_t) * kCntSlots, stream));
+}
+
+int64_t rmx_graph::max_degree(const Level &lv) {
+    unsigned long long *mx = reinterpret_cast<unsigned long long *>(dtmp + 8);
+    RMX_CUDA(cudaMemsetAsync(mx, 0, 8, stream));
+    k_max_degree<<<blocks_for(lv.n, 256, num_sms() * 8), 256, 0, stream>>>(lv.n, lv.out_off, lv.in_off, mx);
+    RMX_LAUNCHED();
+    unsigned long long h = 0;
+    RMX_CUDA(cudaMemcpyAsync(&h, mx, 8, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    return (int64_t)h;
+}
+
+void rmx_graph::ensure_hub_table(int64_t maxdeg) {
+    if (maxdeg <= block_bin_max_degree()) return;
+    int64_t cap = 64;
+    while (cap < 2 * maxdeg) cap <<= 1;
+    if (cap <= work.gcap) return;
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    if (work.gtable) cudaFree(work.gtable);
+    if (work.gkeys) cudaFree(work.gkeys);
+    work.gtable = nullptr;
+    work.gkeys = nullptr;
+    work.gcap = 0;
+    const int hb = hub_blocks();
+    RMX_CUDA(cudaMalloc(&work.gtable, sizeof(fx_t) * 2 * cap * hb));
+    RMX_CUDA(cudaMalloc(&work.gkeys, sizeof(int32_t) * cap * hb));
+    work.gcap = cap;
+}
+
+void rmx_graph::initiate() {
+    if (initiated) return;
+    timers.begin(kTimerOther, stream);
+    normalise(N, out_off, out_w0, out_f, in_off, in_src, in_w, in_w, dangling, scratch, stream);
+    timers.end(kTimerOther, stream);
+    timers.begin(kTimerSpmv, stream);
+    power_iters = power_iteration(N, in_off, in_src, in_w, tw, dangling, p, scratch, stream, spmv_vec);
+    timers.end(kTimerSpmv, stream);
+    timers.begin(kTimerOther, stream);
+    edge_flows(N, E, out_off, out_f, out_fx, in_src, in_w, in_fx, p, tw, dangling, nattr, s0, stream);
+    timers.end(kTimerOther, stream);
+    init_singletons(node_lv, mods, stream);
+    RMX_CUDA(cudaMemsetAsync(inst1.active, 1, 1, stream));
+    instance_codelength(mods, inst1, stream);
+    RMX_CUDA(cudaMemcpyAsync(&L0, inst1.L, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    ensure_hub_table(max_degree(node_lv));
+    initiated = true;
+}
+
+// ---------------------------------------------------------------- sweeps
+
+double rmx_graph::sweep_single(Level &lv, bool prior, bool allow_new, double vthresh, int64_t &n_active) {
+    RMX_CUDA(cudaMemsetAsync(work.counters + kCntMoved, 0, sizeof(int64_t), stream));
+    if (prior) RMX_CUDA(cudaMemsetAsync(work.next_active, 0, lv.n, stream));
+    if (allow_new) free_modules(mods, work, scratch, stream);
+    const uint32_t seed = mix_seed(run_seed, ++sweep_no);
+    bucket_units(lv, work, n_active, seed, nsub, scratch, stream);
+    SweepArgs sa{vthresh, allow_new ? 1 : 0};
+    Timers *tm = timers.on ? &timers : nullptr;
+    for (int sb = 0; sb < nsub; sb++) sweep_subbatch(lv, mods, inst1, work, sa, sb, ++stamp, prior, stream, tm);
+    timers.begin(kTimerCodelen, stream);
+    instance_codelength(mods, inst1, stream);
+    timers.end(kTimerCodelen, stream);
+    if (prior) compact_flags(work.next_active, lv.n, work.list, work.counters + kCntActive, scratch, stream);
+    struct {
+        double L;
+    } hL;
+    int64_t cnt[kCntSlots];
+    RMX_CUDA(cudaMemcpyAsync(&hL.L, inst1.L, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaMemcpyAsync(cnt, work.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    units_evaluated += n_active;
+    edges_evaluated = cnt[kCntEdges];
+    prof.sweeps++;
+    if (prior) n_active = cnt[kCntActive];
+    if (opt.verbose >= 2) printf("  sweep: code length = %g, moved %lld\n", hL.L / kLn2, (long long)cnt[kCntMoved]);
+    return hL.L;
+}
+
+// The first loop of stochastic_greedy_partition (OmpRelaxmap.cpp:291-339), or
+// the inner super-node loop (:379-411): at most max_iter sweeps, stop when a
+// sweep gains less than threshold bits (and did not lose).
+double rmx_graph::stage_sweeps(Level &lv, bool allow_new, double L) {
+    const bool prior = opt.prior != 0;
+    const double vthresh = prior ? -opt.vthresh : 0.0;  // OmpRelaxmap.cpp:66, Module.cpp:1490 vs :1127
+    int64_t n_active = lv.n;
+    all_units(lv.n, work, stream);
+    if (lv.n > 0) ensure_hub_table(max_degree(lv));
+    int iter = 0;
+    bool stop = false;
+    while (!stop && iter < opt.max_iter) {
+        const double oldL = L;
+        if (!prior && iter > 0) {
+            all_units(lv.n, work, stream);
+            n_active = lv.n;
+        }
+        L = sweep_single(lv, prior, allow_new, vthresh, n_active);
+        iter++;
+        if (oldL - L >= 0 && (oldL - L) / kLn2 < opt.threshold) stop = true;
+    }
+    return L;
+}
+
+void rmx_graph::project_sn_to_nodes() {
+    k_project<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, node_sn, sn_lv.mod, nmod);
+    RMX_LAUNCHED();
+}
+
+// convertModulesToSuperNodes (Module.cpp:3008-3077) on the engine's partition.
+void rmx_graph::convert_to_supernodes() {
+    timers.begin(kTimerCoarsen, stream);
+    count_units(node_lv, mods, stream);
+    size_t mk = scratch.mark();
+    int64_t *snid = scratch.alloc<int64_t>(N + 1);
+    k_flags_nonempty<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, mods.count, snid);
+    RMX_LAUNCHED();
+    scan_exclusive(snid, snid, N, dtmp + 0, scratch, stream);
+    int64_t nsn = 0;
+    RMX_CUDA(cudaMemcpyAsync(&nsn, dtmp + 0, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+    k_sn_from_modules<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, mods.count, snid, mods.stat,
+                                                                              sn_lv.mod, sn_lv.attr, sn_lv.nnodes,
+                                                                              zeros);
+    RMX_LAUNCHED();
+    k_group_of_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, nmod, snid, node_sn);
+    RMX_LAUNCHED();
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    sn_lv.n = (int32_t)nsn;
+    sn_lv.m = coarsen_links(N, out_off, out_dst, nullptr, out_fx, node_sn, sn_lv.n, sn_lv.out_off, sn_lv.out_dst,
+                            nullptr, sn_lv.out_fx, sn_lv.in_off, sn_lv.in_src, nullptr, sn_lv.in_fx, scratch, stream);
+    scratch.release(mk);
+    count_units(sn_lv, mods, stream);
+    timers.end(kTimerCoarsen, stream);
+}
+
+// generate_sub_modules (OmpRelaxmap.cpp:502-638): every module becomes an
+// independent sub-network of its members and internal links (flows kept),
+// optimised by node moves only (partition_module_network with fast=true:
+// Network::move semantics, no empty-module option, stop per sub-network);
+// the resulting sub-modules become the super-nodes of the next superstep,
+// starting in their parent module.
+void rmx_graph::generate_sub_modules() {
+    timers.begin(kTimerCoarsen, stream);
+    count_units(node_lv, mods, stream);  // nodes per parent module
+    size_t mk = scratch.mark();
+    int64_t *cnt_out = scratch.alloc<int64_t>(N + 1), *cnt_in = scratch.alloc<int64_t>(N + 1);
+    const unsigned GW = blocks_for((int64_t)N * 32, 256, num_sms() * 32);
+    RMX_CUDA(cudaMemsetAsync(cnt_out + N, 0, sizeof(int64_t), stream));
+    RMX_CUDA(cudaMemsetAsync(cnt_in + N, 0, sizeof(int64_t), stream));
+    k_intra_count<<<GW, 256, 0, stream>>>(N, out_off, out_dst, nmod, cnt_out);
+    RMX_LAUNCHED();
+    k_intra_count<<<GW, 256, 0, stream>>>(N, in_off, in_src, nmod, cnt_in);
+    RMX_LAUNCHED();
+    scan_exclusive(cnt_out, sub_lv.out_off, N + 1, nullptr, scratch, stream);
+    scan_exclusive(cnt_in, sub_lv.in_off, N + 1, nullptr, scratch, stream);
+    fx_t *intra_out = reinterpret_cast<fx_t *>(cnt_out);  // counts are consumed by the scans above
+    k_intra_fill<<<GW, 256, 0, stream>>>(N, out_off, out_dst, out_fx, nmod, sub_lv.out_off, sub_lv.out_dst,
+                                         sub_lv.out_fx, intra_out);
+    RMX_LAUNCHED();
+    k_intra_fill<<<GW, 256, 0, stream>>>(N, in_off, in_src, in_fx, nmod, sub_lv.in_off, sub_lv.in_src, sub_lv.in_fx,
+                                         nullptr);
+    RMX_LAUNCHED();
+    k_sub_attr<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, nattr, intra_out, sub_lv.attr);
+    RMX_LAUNCHED();
+    scratch.release(mk);
+    sub_lv.n = N;
+    RMX_CUDA(cudaMemcpyAsync(&sub_lv.m, sub_lv.out_off + N, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+    // sub-problem state: singleton sub-modules, per-parent code lengths
+    init_singletons(sub_lv, submods, stream);
+    RMX_CUDA(cudaMemsetAsync(instsub.s0, 0, sizeof(fx_t) * N, stream));
+    k_sub_s0<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, p, nmod, instsub.s0);
+    RMX_LAUNCHED();
+    k_inst_active<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, mods.count, instsub.active);
+    RMX_LAUNCHED();
+    instance_codelength(submods, instsub, stream);
+    k_copy_L<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, instsub.L, instsub.L_prev);
+    RMX_LAUNCHED();
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    timers.end(kTimerCoarsen, stream);
+    if (sub_lv.m > 0) {
+        ensure_hub_table(max_degree(sub_lv));
+        Timers *tm = timers.on ? &timers : nullptr;
+        SweepArgs sa{0.0, 0};  // Network::move: best < 0, no empty module (Module.cpp:606, :667)
+        for (int iter = 0; iter < opt.max_iter; iter++) {
+            all_units(N, work, stream);
+            const uint32_t seed = mix_seed(run_seed, ++sweep_no);
+            bucket_units(sub_lv, work, N, seed, nsub, scratch, stream);
+            for (int sb = 0; sb < nsub; sb++)
+                sweep_subbatch(sub_lv, submods, instsub, work, sa, sb, ++stamp, false, stream, tm);
+            timers.begin(kTimerCodelen, stream);
+            instance_codelength(submods, instsub, stream);
+            unsigned long long *na = reinterpret_cast<unsigned long long *>(dtmp + 9);
+            RMX_CUDA(cudaMemsetAsync(na, 0, 8, stream));
+            k_inst_stop<<<blocks_for(N, 256, num_sms() * 8), 256, 0, stream>>>(
+                N, instsub.L, instsub.L_prev, instsub.active, opt.threshold, kLn2, na);
+            RMX_LAUNCHED();
+            timers.end(kTimerCodelen, stream);
+            unsigned long long h = 0;
+            RMX_CUDA(cudaMemcpyAsync(&h, na, 8, cudaMemcpyDeviceToHost, stream));
+            RMX_CUDA(cudaStreamSynchronize(stream));
+            prof.sweeps++;
+            if (h == 0) break;
+        }
+    }
+    // sub-modules -> super-nodes (generateSuperNodesFromSubModules, Module.cpp:3083-3158)
+    timers.begin(kTimerCoarsen, stream);
+    count_units(sub_lv, submods, stream);
+    mk = scratch.mark();
+    int64_t *snid = scratch.alloc<int64_t>(N + 1);
+    k_flags_nonempty<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, submods.count, snid);
+    RMX_LAUNCHED();
+    scan_exclusive(snid, snid, N, dtmp + 0, scratch, stream);
+    k_group_of_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, submod, snid, node_sn);
+    RMX_LAUNCHED();
+    int64_t nsn = 0;
+    RMX_CUDA(cudaMemcpyAsync(&nsn, dtmp + 0, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    sn_lv.n = (int32_t)nsn;
+    RMX_CUDA(cudaMemsetAsync(sn_lv.attr, 0, sizeof(Stat4) * nsn, stream));
+    RMX_CUDA(cudaMemsetAsync(sn_lv.nnodes, 0, sizeof(int32_t) * nsn, stream));
+    k_sn_from_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, node_sn, nmod, nattr, sn_lv.mod,
+                                                                            sn_lv.attr, sn_lv.nnodes);
+    RMX_LAUNCHED();
+    sn_lv.m = coarsen_links(N, out_off, out_dst, nullptr, out_fx, node_sn, sn_lv.n, sn_lv.out_off, sn_lv.out_dst,
+                            nullptr, sn_lv.out_fx, sn_lv.in_off, sn_lv.in_src, nullptr, sn_lv.in_fx, scratch, stream);
+    k_sn_out<<<blocks_for(nsn, 256, num_sms() * 32), 256, 0, stream>>>(sn_lv.n, sn_lv.out_off, sn_lv.out_fx,
+                                                                       sn_lv.attr);
+    RMX_LAUNCHED();
+    scratch.release(mk);
+    timers.end(kTimerCoarsen, stream);
+}
+
+// One superstep (stochastic_greedy_partition, OmpRelaxmap.cpp:263-429).
+double rmx_graph::stage(bool fine, double L) {
+    Level &lv = fine ? node_lv : sn_lv;
+    count_units(lv, mods, stream);
+    // Node sweeps may open a new module only once member lists exist, i.e.
+    // after the first superstep (members.size() > 1 test, Module.cpp:1435);
+    // super-node sweeps test the live module flow (Module.cpp:2620).
+    const bool allow_first = fine ? superstep > 1 : true;
+    L = stage_sweeps(lv, allow_first, L);
+    if (!fine) project_sn_to_nodes();
+    double oldL;
+    do {
+        oldL = L;
+        convert_to_supernodes();
+        L = stage_sweeps(sn_lv, true, L);
+        project_sn_to_nodes();
+    } while ((oldL - L) / kLn2 > opt.threshold);
+    return L;
+}
+
+int32_t rmx_graph::count_modules() {
+    count_units(node_lv, mods, stream);
+    unsigned long long *c = reinterpret_cast<unsigned long long *>(dtmp + 10);
+    RMX_CUDA(cudaMemsetAsync(c, 0, 8, stream));
+    k_count_nonzero<<<blocks_for(N, 256, num_sms() * 8), 256, 0, stream>>>(N, mods.count, c);
+    RMX_LAUNCHED();
+    unsigned long long h = 0;
+    RMX_CUDA(cudaMemcpyAsync(&h, c, 8, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    return (int32_t)h;
+}
+
+// main's superstep loop (OmpRelaxmap.cpp:181-219).
+double rmx_graph::run_attempt(uint32_t seed) {
+    run_seed = seed;
+    init_singletons(node_lv, mods, stream);
+    RMX_CUDA(cudaMemsetAsync(inst1.active, 1, 1, stream));
+    double L = L0;
+    step_bits.clear();
+    superstep = 1;
+    bool fine = true;
+    double oldL = L;
+    L = stage(fine, L);
+    step_bits.push_back(L / kLn2);
+    if (opt.verbose)
+        printf("SuperStep [%d] - codeLength = %g in %d modules.\n", superstep, L / kLn2, count_modules());
+    bool next = !((oldL - L) / kLn2 < opt.threshold);
+    while (next) {
+        oldL = L;
+        superstep++;
+        L = stage(fine, L);
+        step_bits.push_back(L / kLn2);
+        if (opt.verbose)
+            printf("SuperStep [%d] - codeLength = %g in %d modules.\n", superstep, L / kLn2, count_modules());
+        if ((oldL - L) / kLn2 < opt.threshold) next = false;
+        fine = !fine;
+        if (next && !fine) generate_sub_modules();
+    }
+    prof.supersteps += superstep;
+    return L;
+}
+
+double rmx_graph::optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modules) {
+    opt = o;
+    if (opt.max_iter < 0) opt.max_iter = 0;
+    if (opt.attempts < 1) opt.attempts = 1;
+    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 85) : (N >= 4096 ? 8 : 4);
+    cudaEvent_t t0, t1;
+    RMX_CUDA(cudaEventCreate(&t0));
+    RMX_CUDA(cudaEventCreate(&t1));
+    RMX_CUDA(cudaEventRecord(t0, stream));
+    initiate();
+    double best = INFINITY;
+    std::vector<int32_t> part(N);
+    std::vector<double> best_steps;
+    for (int a = 0; a < opt.attempts; a++) {
+        const double L = run_attempt(opt.seed + (uint32_t)a);
+        if (L < best) {
+            best = L;
+            best_steps = step_bits;
+            RMX_CUDA(cudaMemcpyAsync(part.data(), nmod, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, stream));
+            RMX_CUDA(cudaStreamSynchronize(stream));
+        }
+    }
+    step_bits = best_steps;
+    RMX_CUDA(cudaEventRecord(t1, stream));
+    RMX_CUDA(cudaEventSynchronize(t1));
+    float ms = 0;
+    RMX_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    prof.total_ms = ms;
+    if (part_out) std::memcpy(part_out, part.data(), sizeof(int32_t) * N);
+    if (n_modules) {
+        int32_t nm = 0;
+        std::vector<uint8_t> seen(N, 0);
+        for (int32_t v = 0; v < N; v++)
+            if (!seen[part[v]]) {
+                seen[part[v]] = 1;
+                nm++;
+            }
+        *n_modules = nm;
+    }
+    if (timers.on) timers.resolve();
+    return best;
+}
+
+// ---------------------------------------------------------------- parity hooks
+
+double rmx_graph::codelength_fp64(const int32_t *part_host) {
+    initiate();
+    for (int32_t v = 0; v < N; v++)
+        if ((uint32_t)part_host[v] >= (uint32_t)N) throw std::invalid_argument("module id outside 0..N-1");
+    size_t mk = scratch.mark();
+    int32_t *part = scratch.alloc<int32_t>(N);
+    double *P = scratch.alloc<double>(N), *TW = scratch.alloc<double>(N), *D = scratch.alloc<double>(N),
+           *OUT = scratch.alloc<double>(N);
+    int32_t *cnt = scratch.alloc<int32_t>(N);
+    const unsigned G = num_sms() * 4;
+    double *parts = scratch.alloc<double>(4 * G);
+    RMX_CUDA(cudaMemcpyAsync(part, part_host, sizeof(int32_t) * N, cudaMemcpyHostToDevice, stream));
+    for (double *a : {P, TW, D, OUT}) RMX_CUDA(cudaMemsetAsync(a, 0, sizeof(double) * N, stream));
+    RMX_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * N, stream));
+    k_fp64_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, part, p, tw, dangling, P, TW, D, cnt);
+    RMX_LAUNCHED();
+    k_fp64_out<<<blocks_for((int64_t)N * 32, 256, num_sms() * 32), 256, 0, stream>>>(N, out_off, out_dst, out_f, part,
+                                                                                     OUT);
+    RMX_LAUNCHED();
+    k_fp64_terms<<<G, 256, 0, stream>>>(N, P, TW, D, OUT, cnt, p, parts);
+    RMX_LAUNCHED();
+    std::vector<double> h(4 * G);
+    RMX_CUDA(cudaMemcpyAsync(h.data(), parts, sizeof(double) * 4 * G, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    scratch.release(mk);
+    double a[4] = {0, 0, 0, 0};
+    for (unsigned b = 0; b < G; b++)
+        for (int q = 0; q < 4; q++) a[q] += h[4 * b + q];
+    auto pl = [](double x) { return x > 0.0 ? x * std::log(x) : 0.0; };
+    return pl(a[0]) - 2.0 * a[1] + a[2] - a[3];
+}
+
+void rmx_graph::coarsen_hook(const int32_t *part_host, int32_t *n_sn, int64_t *n_links, int32_t *sn_of_mod,
+                             int64_t *o_off, int32_t *o_dst, double *o_f, int64_t *i_off, int32_t *i_src,
+                             double *i_f) {
+    initiate();
+    for (int32_t v = 0; v < N; v++)
+        if ((uint32_t)part_host[v] >= (uint32_t)N) throw std::invalid_argument("module id outside 0..N-1");
+    size_t mk = scratch.mark();
+    const int64_t Em = std::max<int64_t>(E, 1);
+    int32_t *part = scratch.alloc<int32_t>(N);
+    int64_t *snid = scratch.alloc<int64_t>(N + 1);
+    int32_t *grp = scratch.alloc<int32_t>(N), *cnt = scratch.alloc<int32_t>(N);
+    int64_t *g_out_off = scratch.alloc<int64_t>(N + 1), *g_in_off = scratch.alloc<int64_t>(N + 1);
+    int32_t *g_dst = scratch.alloc<int32_t>(Em), *g_src = scratch.alloc<int32_t>(Em);
+    double *g_f = scratch.alloc<double>(Em), *g_if = scratch.alloc<double>(Em);
+    fx_t *g_fx = scratch.alloc<fx_t>(Em), *g_ifx = scratch.alloc<fx_t>(Em);
+    RMX_CUDA(cudaMemcpyAsync(part, part_host, sizeof(int32_t) * N, cudaMemcpyHostToDevice, stream));
+    RMX_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int32_t) * N, stream));
+    Level tmp = node_lv;
+    tmp.mod = part;
+    ModState M = mods;
+    M.count = cnt;
+    count_units(tmp, M, stream);
+    k_flags_nonempty<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, cnt, snid);
+    RMX_LAUNCHED();
+    scan_exclusive(snid, snid, N, dtmp + 0, scratch, stream);
+    k_group_of_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, part, snid, grp);
+    RMX_LAUNCHED();
+    int64_t nsn = 0;
+    RMX_CUDA(cudaMemcpyAsync(&nsn, dtmp + 0, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    const int64_t m = coarsen_links(N, out_off, out_dst, out_f, out_fx, grp, (int32_t)nsn, g_out_off, g_dst, g_f,
+                                    g_fx, g_in_off, g_src, g_if, g_ifx, scratch, stream);
+    std::vector<int64_t> sid(N);
+    RMX_CUDA(cudaMemcpyAsync(sid.data(), snid, sizeof(int64_t) * N, cudaMemcpyDeviceToHost, stream));
+    std::vector<int32_t> hc(N);
+    RMX_CUDA(cudaMemcpyAsync(hc.data(), cnt, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, stream));
+    if (o_off) RMX_CUDA(cudaMemcpyAsync(o_off, g_out_off, sizeof(int64_t) * (nsn + 1), cudaMemcpyDeviceToHost, stream));
+    if (i_off) RMX_CUDA(cudaMemcpyAsync(i_off, g_in_off, sizeof(int64_t) * (nsn + 1), cudaMemcpyDeviceToHost, stream));
+    if (m > 0) {
+        if (o_dst) RMX_CUDA(cudaMemcpyAsync(o_dst, g_dst, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, stream));
+        if (o_f) RMX_CUDA(cudaMemcpyAsync(o_f, g_f, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
+        if (i_src) RMX_CUDA(cudaMemcpyAsync(i_src, g_src, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, stream));
+        if (i_f) RMX_CUDA(cudaMemcpyAsync(i_f, g_if, sizeof(double) * m, cudaMemcpyDeviceToHost, stream));
+    }
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    scratch.release(mk);
+    if (sn_of_mod)
+        for (int32_t i = 0; i < N; i++) sn_of_mod[i] = hc[i] > 0 ? (int32_t)sid[i] : -1;
+    if (n_sn) *n_sn = (int32_t)nsn;
+    if (n_links) *n_links = m;
+}
+
+void rmx_graph::evaluate_hook(const int32_t *part_host, const uint8_t *allow_new_host, int32_t *best_mod,
+                              double *best_delta) {
+    initiate();
+    for (int32_t v = 0; v < N; v++)
+        if ((uint32_t)part_host[v] >= (uint32_t)N) throw std::invalid_argument("module id outside 0..N-1");
+    size_t mk = scratch.mark();
+    uint8_t *an = nullptr;
+    if (allow_new_host) {
+        an = scratch.alloc<uint8_t>(N);
+        RMX_CUDA(cudaMemcpyAsync(an, allow_new_host, N, cudaMemcpyHostToDevice, stream));
+    }
+    RMX_CUDA(cudaMemcpyAsync(nmod, part_host, sizeof(int32_t) * N, cudaMemcpyHostToDevice, stream));
+    module_stats_from_units(node_lv, mods, stream);
+    RMX_CUDA(cudaMemsetAsync(inst1.active, 1, 1, stream));
+    instance_codelength(mods, inst1, stream);
+    evaluate_all(node_lv, mods, inst1, work, an, 0.0, scratch, stream);
+    RMX_CUDA(cudaMemcpyAsync(best_mod, work.prop, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaMemcpyAsync(best_delta, work.pdelta, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    scratch.release(mk);
+}

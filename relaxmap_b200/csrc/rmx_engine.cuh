@@ -1,0 +1,158 @@
+// Internal engine interfaces: device layout of the graph, the move levels and
+// the module state, and the launchers of every hot-path kernel.
+//
+// HBM layout (structure of arrays; N nodes, E kept links):
+//   node CSR  out_off[N+1] i64 | out_dst[E] i32 | out_w0[E] f64 (summed input
+//             weight) | out_f[E] f64 (normalised weight, then flow) | out_fx[E]
+//   node CSC  in_off[N+1] i64 | in_src[E] i32 | in_w[E] f64 (normalised) | in_fx[E]
+//   nodes     tw[N] f64 teleport weight | dangling[N] u8 | p[N] f64 flow
+//   units     attr[n] Stat4 (fixed-point P, TW, D, OUT) | mod[n] | inst[n] | nnodes[n]
+//   modules   stat[M] Stat4 | count[M] i32 | inst[M] i32        (M = N ids)
+// A "level" is the set of moving units: nodes, super-nodes (modules of the
+// previous stage) or sub-module super-nodes (coarse-tune), each with its own
+// CSR/CSC of aggregated fixed-point flows.
+#pragma once
+#include <vector>
+
+#include "rmx_common.cuh"
+#include "rmx_prims.cuh"
+
+namespace rmx {
+
+struct Level {
+    int32_t n = 0;      // units
+    int64_t m = 0;      // links
+    int64_t *out_off = nullptr, *in_off = nullptr;
+    int32_t *out_dst = nullptr, *in_src = nullptr;
+    fx_t *out_fx = nullptr, *in_fx = nullptr;
+    Stat4 *attr = nullptr;
+    int32_t *mod = nullptr;     // module id of each unit
+    int32_t *inst = nullptr;    // instance (independent sub-problem) of each unit
+    int32_t *nnodes = nullptr;  // original nodes inside each unit
+};
+
+struct ModState {
+    int32_t cap = 0;
+    Stat4 *stat = nullptr;
+    int32_t *count = nullptr;   // units of the current level in the module
+    int32_t *inst = nullptr;
+};
+
+// Per-instance code-length bookkeeping (one instance = the whole graph, or
+// one sub-problem of the coarse-tune / batched engine).
+struct InstState {
+    int32_t n = 0;
+    double *sum_exit = nullptr;   // sum of module exits
+    double *L = nullptr;          // code length (nats)
+    double *L_prev = nullptr;     // at the start of the current stage step
+    fx_t *s0 = nullptr;           // sum p log p of member nodes (fixed 2^-58)
+    fx_t *acc = nullptr;          // 3 per instance: sum exit, sum plogp(q), sum plogp(q+P)
+    uint8_t *active = nullptr;    // still iterating
+};
+
+// Sweep parameters passed to the move kernels.
+struct SweepArgs {
+    double vthresh;          // accept when best change < vthresh (<= 0)
+    int allow_new;           // empty-module candidate enabled for this stage
+};
+
+// ---------------------------------------------------------------- graph build
+struct CsrBuild {
+    int64_t n_links = 0, n_self = 0;
+};
+// Sort + sum duplicate pairs, drop self-loops and non-positive sums, build CSR
+// and CSC. src/dst/w are device arrays of n_edges entries (consumed).
+CsrBuild build_csr(int32_t n, int64_t n_edges, int32_t *d_src, int32_t *d_dst, double *d_w, int64_t *out_off,
+                   int32_t *out_dst, double *out_w0, int64_t *in_off, int32_t *in_src, double *in_w, Arena &ar,
+                   cudaStream_t s, int64_t *self_count_dev);
+
+// ---------------------------------------------------------------- flows
+// Row-normalise (CSR and CSC), power iteration, edge flows, unit attributes.
+struct FlowOut {
+    int iters = 0;
+};
+int power_iteration(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
+                    const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, int vec);
+void normalise(int32_t n, const int64_t *out_off, const double *out_w0, double *out_f, const int64_t *in_off,
+               const int32_t *in_src, const double *in_w_raw, double *in_w, uint8_t *dangling, Arena &ar,
+               cudaStream_t s);
+void edge_flows(int32_t n, int64_t m, const int64_t *out_off, double *out_f, fx_t *out_fx, const int32_t *in_src,
+                const double *in_w, fx_t *in_fx, const double *p, const double *tw, const uint8_t *dangling,
+                Stat4 *attr, fx_t *s0_acc, cudaStream_t s);
+void singleton_exits(int32_t n, const int64_t *out_off, const double *out_f, const double *p, const double *tw,
+                     const uint8_t *dangling, double *exitpr, cudaStream_t s);
+
+// ---------------------------------------------------------------- moves
+void init_singletons(const Level &L, ModState &M, cudaStream_t s);
+void module_stats_from_units(const Level &L, ModState &M, cudaStream_t s);
+void count_units(const Level &L, ModState &M, cudaStream_t s);
+// Code length per instance from the module statistics.
+void instance_codelength(const ModState &M, InstState &I, cudaStream_t s);
+// Device time per kernel class, recorded with CUDA events on the stream.
+enum { kTimerSpmv = 0, kTimerEval, kTimerCommit, kTimerCoarsen, kTimerCodelen, kTimerOther, kTimerCount };
+struct Timers {
+    bool on = false;
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    struct Pending {
+        int k;
+        cudaEvent_t a, b;
+    };
+    std::vector<Pending> pending;
+    cudaEvent_t open[kTimerCount] = {};
+    double ms[kTimerCount] = {};
+    int64_t launches[kTimerCount] = {};
+    void begin(int k, cudaStream_t s);
+    void end(int k, cudaStream_t s);
+    void resolve();  // synchronises on the recorded events
+    void reset();
+    void destroy();
+};
+
+// Counter slots in SweepWork::counters (device int64).
+enum { kCntActive = 0, kCntFree = 1, kCntMoved = 3, kCntEdges = 4, kCntUnits = 5, kCntSlots = 8 };
+
+// Per-level sweep workspace (sized for the largest level: N units, N modules).
+struct SweepWork {
+    int32_t *list = nullptr, *list2 = nullptr;  // active units; active units grouped by bucket
+    uint16_t *bucket = nullptr;
+    int64_t *bucket_off = nullptr;              // nsub * 3 + 1 bucket boundaries (device)
+    int64_t *ranges = nullptr;                  // [beg,end) of each sub-batch (device)
+    int32_t *prop = nullptr;                    // proposed module (-1 none, -2 empty module)
+    double *pdelta = nullptr;
+    int32_t *ptarget = nullptr;                 // claimed empty module
+    int32_t *prevmod = nullptr;
+    uint32_t *stamp = nullptr;                  // sub-batch stamp of the last move of a unit
+    uint8_t *next_active = nullptr;
+    int32_t *free_list = nullptr;
+    unsigned long long *claim = nullptr;        // per module id
+    int64_t *counters = nullptr;
+    fx_t *gtable = nullptr;                     // hub hash tables: hub_blocks() slices
+    int32_t *gkeys = nullptr;
+    int64_t gcap = 0;
+};
+
+void configure_eval_kernels();
+int hub_blocks();
+int64_t warp_bin_max_degree();
+int64_t block_bin_max_degree();
+void all_units(int32_t n, SweepWork &W, cudaStream_t s);
+void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed, int nsub, Arena &ar, cudaStream_t s);
+void free_modules(const ModState &M, SweepWork &W, Arena &ar, cudaStream_t s);
+// Evaluate, claim, commit and apply link deltas for sub-batch sb.
+void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &W, const SweepArgs &a, int sb,
+                    uint32_t stamp, bool mark_active, cudaStream_t s, Timers *tm);
+// Move evaluation only, for the parity hook (no commit).
+void evaluate_all(const Level &L, const ModState &M, const InstState &I, SweepWork &W, const uint8_t *allow_new,
+                  double vthresh, Arena &ar, cudaStream_t s);
+
+// ---------------------------------------------------------------- coarsening
+// Group nodes by group[v] (0..ng-1) and aggregate the node CSR into a group
+// CSR/CSC: FP64 sums in node/link order (bit-exact to the reference) and
+// fixed-point sums for the engine. Returns the number of group links.
+int64_t coarsen_links(int32_t n, const int64_t *out_off, const int32_t *out_dst, const double *out_f,
+                      const fx_t *out_fx, const int32_t *group, int32_t ng, int64_t *g_out_off, int32_t *g_out_dst,
+                      double *g_out_f, fx_t *g_out_fx, int64_t *g_in_off, int32_t *g_in_src, double *g_in_f,
+                      fx_t *g_in_fx, Arena &ar, cudaStream_t s);
+
+}  // namespace rmx

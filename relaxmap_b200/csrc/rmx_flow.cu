@@ -1,0 +1,397 @@
+// Graph construction and stationary flow.
+//
+// build_csr     loader edge map + edge preparation (FileIO.cpp:157, :220;
+//               OmpRelaxmap.cpp:117-135, 158-162) as a stable radix sort of
+//               (src,dst), sequential in-order duplicate sums, compaction, and
+//               a stable transpose for the in-links.
+// normalise     Network::initiate's dangling detection and row normalisation
+//               (Module.cpp:228-247), sequential row sums as in the reference.
+// power_iteration  calculateSteadyState (Module.cpp:340-469) as ONE cooperative
+//               persistent launch: pull SpMV over the CSC with the teleport and
+//               dangling terms folded in, deterministic grid reductions for the
+//               normaliser, L1 change and dangling mass, the reference's stop
+//               rule evaluated identically by every block.
+// edge_flows    Module.cpp:275-286 plus the fixed-point unit attributes.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+
+#include "rmx_engine.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace rmx {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+static int bits_for(int64_t n) {
+    int b = 1;
+    while ((int64_t(1) << b) < n) b++;
+    return b;
+}
+
+// ------------------------------------------------------------ CSR build
+
+__global__ void k_make_keys(const int32_t *src, const int32_t *dst, int64_t n, int b, uint64_t *keys, uint32_t *vals) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        keys[e] = ((uint64_t)(uint32_t)src[e] << b) | (uint32_t)dst[e];
+        vals[e] = (uint32_t)e;
+    }
+}
+
+__global__ void k_heads(const uint64_t *keys, int64_t n, uint8_t *flag) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        flag[e] = (e == 0 || keys[e] != keys[e - 1]) ? 1 : 0;
+}
+
+// One thread per distinct (src,dst): weights summed sequentially in input order.
+__global__ void k_sum_dups(const uint64_t *keys, const uint32_t *vals, const double *w, const int32_t *head,
+                           const int64_t *n_heads, int64_t n, int b, int32_t *usrc, int32_t *udst, double *uw,
+                           uint8_t *keep, unsigned long long *n_self) {
+    int64_t U = *n_heads;
+    uint64_t mask = (uint64_t(1) << b) - 1;
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < U; u += (int64_t)gridDim.x * blockDim.x) {
+        int64_t beg = head[u], end = (u + 1 < U) ? head[u + 1] : n;
+        double s = w[vals[beg]];
+        for (int64_t j = beg + 1; j < end; j++) s += w[vals[j]];
+        uint64_t k = keys[beg];
+        int32_t a = (int32_t)(k >> b), d = (int32_t)(k & mask);
+        usrc[u] = a;
+        udst[u] = d;
+        uw[u] = s;
+        bool pos = s > 0.0;
+        keep[u] = (pos && a != d) ? 1 : 0;
+        if (pos && a == d) atomicAdd(n_self, 1ull);
+    }
+}
+
+__global__ void k_gather_kept(const int32_t *kept, const int64_t *n_kept, const int32_t *usrc, const int32_t *udst,
+                              const double *uw, int32_t *lsrc, int32_t *out_dst, double *out_w0,
+                              unsigned long long *row_count) {
+    int64_t K = *n_kept;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < K; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t u = kept[i];
+        lsrc[i] = usrc[u];
+        out_dst[i] = udst[u];
+        out_w0[i] = uw[u];
+        atomicAdd(&row_count[usrc[u]], 1ull);
+    }
+}
+
+__global__ void k_dst_keys(const int32_t *dst, int64_t m, uint64_t *keys, uint32_t *vals, unsigned long long *col_count) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        keys[i] = (uint64_t)(uint32_t)dst[i];
+        vals[i] = (uint32_t)i;
+        atomicAdd(&col_count[dst[i]], 1ull);
+    }
+}
+
+__global__ void k_gather_csc(const uint32_t *perm, int64_t m, const int32_t *lsrc, const double *w0, int32_t *in_src,
+                             double *in_w) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m; i += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t j = perm[i];
+        in_src[i] = lsrc[j];
+        in_w[i] = w0[j];
+    }
+}
+
+CsrBuild build_csr(int32_t n, int64_t n_edges, int32_t *d_src, int32_t *d_dst, double *d_w, int64_t *out_off,
+                   int32_t *out_dst, double *out_w0, int64_t *in_off, int32_t *in_src, double *in_w, Arena &ar,
+                   cudaStream_t s, int64_t *scratch_dev) {
+    CsrBuild r;
+    const int T = 256;
+    const unsigned G = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n_edges + T - 1) / T, num_sms() * 32));
+    RMX_CUDA(cudaMemsetAsync(out_off, 0, sizeof(int64_t) * (n + 1), s));
+    RMX_CUDA(cudaMemsetAsync(in_off, 0, sizeof(int64_t) * (n + 1), s));
+    if (n_edges == 0) return r;
+    size_t mk = ar.mark();
+    const int b = bits_for(std::max<int64_t>(n, 2));
+    uint64_t *keys = ar.alloc<uint64_t>(n_edges), *keys2 = ar.alloc<uint64_t>(n_edges);
+    uint32_t *vals = ar.alloc<uint32_t>(n_edges), *vals2 = ar.alloc<uint32_t>(n_edges);
+    k_make_keys<<<G, T, 0, s>>>(d_src, d_dst, n_edges, b, keys, vals);
+    RMX_LAUNCHED();
+    radix_sort_pairs(keys, vals, keys2, vals2, n_edges, 2 * b, ar, s);
+    uint8_t *flag = ar.alloc<uint8_t>(n_edges);
+    k_heads<<<G, T, 0, s>>>(keys, n_edges, flag);
+    RMX_LAUNCHED();
+    int32_t *head = ar.alloc<int32_t>(n_edges);
+    int64_t *cnt = scratch_dev;  // [0] heads [1] kept [2] self-loops
+    RMX_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int64_t) * 3, s));
+    compact_flags(flag, n_edges, head, cnt + 0, ar, s);
+    int32_t *usrc = ar.alloc<int32_t>(n_edges), *udst = ar.alloc<int32_t>(n_edges);
+    double *uw = ar.alloc<double>(n_edges);
+    uint8_t *keep = flag;  // reuse
+    k_sum_dups<<<G, T, 0, s>>>(keys, vals, d_w, head, cnt + 0, n_edges, b, usrc, udst, uw, keep,
+                               reinterpret_cast<unsigned long long *>(cnt + 2));
+    RMX_LAUNCHED();
+    int64_t U = 0;
+    RMX_CUDA(cudaMemcpyAsync(&U, cnt + 0, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    int32_t *kept = head;  // heads no longer needed after k_sum_dups... (it is: read above, stream-ordered)
+    kept = ar.alloc<int32_t>(std::max<int64_t>(U, 1));
+    compact_flags(keep, U, kept, cnt + 1, ar, s);
+    int32_t *lsrc = ar.alloc<int32_t>(std::max<int64_t>(U, 1));
+    k_gather_kept<<<G, T, 0, s>>>(kept, cnt + 1, usrc, udst, uw, lsrc, out_dst, out_w0,
+                                  reinterpret_cast<unsigned long long *>(out_off));
+    RMX_LAUNCHED();
+    int64_t host_cnt[3];
+    RMX_CUDA(cudaMemcpyAsync(host_cnt, cnt, sizeof(host_cnt), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    const int64_t m = host_cnt[1];
+    r.n_links = m;
+    r.n_self = host_cnt[2];
+    scan_exclusive(out_off, out_off, n + 1, nullptr, ar, s);
+    if (m > 0) {
+        k_dst_keys<<<G, T, 0, s>>>(out_dst, m, keys, vals, reinterpret_cast<unsigned long long *>(in_off));
+        RMX_LAUNCHED();
+        radix_sort_pairs(keys, vals, keys2, vals2, m, b, ar, s);
+        k_gather_csc<<<G, T, 0, s>>>(vals, m, lsrc, out_w0, in_src, in_w);
+        RMX_LAUNCHED();
+    }
+    scan_exclusive(in_off, in_off, n + 1, nullptr, ar, s);
+    ar.release(mk);
+    return r;
+}
+
+// ------------------------------------------------------------ normalise
+
+__global__ void k_normalise_rows(int32_t n, const int64_t *off, const double *w0, double *wn, double *rowsum,
+                                 uint8_t *dangling) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int64_t b = off[i], e = off[i + 1];
+        double s = 0.0;
+        for (int64_t j = b; j < e; j++) s += w0[j];
+        for (int64_t j = b; j < e; j++) wn[j] = w0[j] / s;
+        rowsum[i] = s;
+        dangling[i] = (b == e) ? 1 : 0;
+    }
+}
+
+__global__ void k_normalise_cols(int64_t m, const int32_t *in_src, const double *raw, double *wn,
+                                 const double *rowsum) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+        wn[k] = raw[k] / rowsum[in_src[k]];
+}
+
+void normalise(int32_t n, const int64_t *out_off, const double *out_w0, double *out_f, const int64_t *in_off,
+               const int32_t *in_src, const double *in_w_raw, double *in_w, uint8_t *dangling, Arena &ar,
+               cudaStream_t s) {
+    size_t mk = ar.mark();
+    double *rowsum = ar.alloc<double>(std::max(n, 1));
+    k_normalise_rows<<<blocks_for(n, 128, num_sms() * 16), 128, 0, s>>>(n, out_off, out_w0, out_f, rowsum, dangling);
+    RMX_LAUNCHED();
+    int64_t m = 0;
+    RMX_CUDA(cudaMemcpyAsync(&m, in_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    if (m > 0) {
+        k_normalise_cols<<<blocks_for(m, 256, num_sms() * 32), 256, 0, s>>>(m, in_src, in_w_raw, in_w, rowsum);
+        RMX_LAUNCHED();
+    }
+    ar.release(mk);
+}
+
+// ------------------------------------------------------------ power iteration
+
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (w == 0) {
+        t = lane < NT / 32 ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(kFull, t, o);
+    }
+    __syncthreads();
+    return t;  // valid in thread 0
+}
+
+// Sum of nb per-block partials in one fixed order; every block and thread gets
+// the identical value.
+__device__ __forceinline__ double sum_parts(const double *parts, int nb, double *sh) {
+    if (threadIdx.x < 32) {
+        double v = 0.0;
+        for (int i = threadIdx.x; i < nb; i += 32) v += __ldcg(parts + i);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+        if (threadIdx.x == 0) sh[0] = v;
+    }
+    __syncthreads();
+    double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+constexpr int kPowT = 256;
+
+template <int VEC>
+__global__ void __launch_bounds__(kPowT) k_power(const int64_t *__restrict__ in_off, const int32_t *__restrict__ in_src,
+                                                 const double *__restrict__ in_w, const double *__restrict__ tw,
+                                                 const uint8_t *__restrict__ dang, int32_t n, double *x, double *y,
+                                                 double *parts, int *iters_out) {
+    cg::grid_group grid = cg::this_grid();
+    __shared__ double sh[32];
+    const int nb = gridDim.x;
+    double *Sp = parts, *Dp = parts + nb, *Ep = parts + 2 * nb;
+    const int64_t gtid = (int64_t)blockIdx.x * kPowT + threadIdx.x, gthreads = (int64_t)nb * kPowT;
+
+    double dl = 0.0;
+    const double x0 = 1.0 / n;
+    for (int64_t i = gtid; i < n; i += gthreads) {
+        x[i] = x0;
+        if (dang[i]) dl += x0;
+    }
+    dl = block_sum<kPowT>(dl, sh);
+    if (threadIdx.x == 0) Dp[blockIdx.x] = dl;
+    grid.sync();
+
+    constexpr int RPW = 32 / VEC;  // rows per warp per step
+    const int lane = threadIdx.x & 31, sub = lane / VEC, lv = lane % VEC;
+    const int64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+    int iter = 0;
+    for (;;) {
+        const double D = sum_parts(Dp, nb, sh);
+        const double coef = kAlpha + kBeta * D;
+        double ls = 0.0;
+        for (int64_t base = gwarp * RPW; base < n; base += nwarps * RPW) {
+            const int64_t r = base + sub;
+            double acc = 0.0;
+            if (r < n) {
+                const int64_t e = in_off[r + 1];
+                for (int64_t k = in_off[r] + lv; k < e; k += VEC) acc += kBeta * in_w[k] * __ldcg(x + in_src[k]);
+            }
+#pragma unroll
+            for (int o = VEC / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+            if (r < n && lv == 0) {
+                const double v = coef * tw[r] + acc;
+                y[r] = v;
+                ls += v;
+            }
+        }
+        ls = block_sum<kPowT>(ls, sh);
+        if (threadIdx.x == 0) Sp[blockIdx.x] = ls;
+        grid.sync();
+        const double S = sum_parts(Sp, nb, sh);
+        double el = 0.0;
+        dl = 0.0;
+        for (int64_t i = gtid; i < n; i += gthreads) {
+            const double xn = __ldcg(y + i) / S;
+            el += fabs(xn - x[i]);
+            x[i] = xn;
+            if (dang[i]) dl += xn;
+        }
+        el = block_sum<kPowT>(el, sh);
+        dl = block_sum<kPowT>(dl, sh);
+        if (threadIdx.x == 0) {
+            Ep[blockIdx.x] = el;
+            Dp[blockIdx.x] = dl;
+        }
+        grid.sync();
+        const double diff = sum_parts(Ep, nb, sh);
+        iter++;
+        if (iter >= 200 || (diff <= 1.0e-15 && iter >= 50)) break;  // Module.cpp:460
+    }
+    if (gtid == 0) *iters_out = iter;
+}
+
+template <int VEC>
+static int launch_power(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
+                        const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s) {
+    int dev = 0, per_sm = 0, coop = 0;
+    RMX_CUDA(cudaGetDevice(&dev));
+    RMX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) throw CudaError(cudaErrorNotSupported, "cooperative launch not supported");
+    RMX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_power<VEC>, kPowT, 0));
+    int nb = std::max(1, std::min(per_sm, 4)) * num_sms();
+    nb = (int)std::min<int64_t>(nb, std::max<int64_t>(1, ((int64_t)n * VEC + kPowT - 1) / kPowT));
+    size_t mk = ar.mark();
+    double *y = ar.alloc<double>(std::max(n, 1));
+    double *parts = ar.alloc<double>(3 * nb);
+    int *iters = ar.alloc<int>(1);
+    void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w, (void *)&tw, (void *)&dangling, (void *)&n,
+                    (void *)&p, (void *)&y, (void *)&parts, (void *)&iters};
+    RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));
+    int h = 0;
+    RMX_CUDA(cudaMemcpyAsync(&h, iters, sizeof(int), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    ar.release(mk);
+    return h;
+}
+
+int power_iteration(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
+                    const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, int vec) {
+    if (n <= 0) return 0;
+    switch (vec) {
+        case 4: return launch_power<4>(n, in_off, in_src, in_w, tw, dangling, p, ar, s);
+        case 8: return launch_power<8>(n, in_off, in_src, in_w, tw, dangling, p, ar, s);
+        case 16: return launch_power<16>(n, in_off, in_src, in_w, tw, dangling, p, ar, s);
+        default: return launch_power<32>(n, in_off, in_src, in_w, tw, dangling, p, ar, s);
+    }
+}
+
+// ------------------------------------------------------------ flows
+
+__global__ void k_flow_rows(int32_t n, const int64_t *off, double *f, fx_t *fx, const double *p, const double *tw,
+                            const uint8_t *dangling, Stat4 *attr, fx_t *s0) {
+    fx_t s0l = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double pi = p[i];
+        fx_t out = 0;
+        for (int64_t j = off[i]; j < off[i + 1]; j++) {
+            const double v = pi * f[j];  // Module.cpp:280
+            f[j] = v;
+            const fx_t q = to_fx(v);
+            fx[j] = q;
+            out += q;
+        }
+        Stat4 a;
+        a.P = to_fx(pi);
+        a.TW = to_fx(tw[i]);
+        a.D = dangling[i] ? a.P : 0;
+        a.OUT = out;
+        attr[i] = a;
+        s0l += to_fxl(plogp(pi));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s0l += __shfl_xor_sync(kFull, s0l, o);
+    if ((threadIdx.x & 31) == 0 && s0l != 0) atomic_add_fx(s0, s0l);
+}
+
+__global__ void k_flow_cols(int64_t m, const int32_t *in_src, const double *in_w, const double *p, fx_t *in_fx) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+        in_fx[k] = to_fx(p[in_src[k]] * in_w[k]);
+}
+
+void edge_flows(int32_t n, int64_t m, const int64_t *out_off, double *out_f, fx_t *out_fx, const int32_t *in_src,
+                const double *in_w, fx_t *in_fx, const double *p, const double *tw, const uint8_t *dangling,
+                Stat4 *attr, fx_t *s0_acc, cudaStream_t s) {
+    RMX_CUDA(cudaMemsetAsync(s0_acc, 0, sizeof(fx_t), s));
+    k_flow_rows<<<blocks_for(n, 128, num_sms() * 16), 128, 0, s>>>(n, out_off, out_f, out_fx, p, tw, dangling, attr,
+                                                                   s0_acc);
+    RMX_LAUNCHED();
+    if (m > 0) {
+        k_flow_cols<<<blocks_for(m, 256, num_sms() * 32), 256, 0, s>>>(m, in_src, in_w, p, in_fx);
+        RMX_LAUNCHED();
+    }
+}
+
+// Singleton exit exactly as Module::Module(int, Node*) (Module.cpp:76-95).
+__global__ void k_singleton_exit(int32_t n, const int64_t *off, const double *f, const double *p, const double *tw,
+                                 const uint8_t *dangling, double *ex) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int64_t j = off[i]; j < off[i + 1]; j++) s += f[j];
+        ex[i] = dangling[i] ? (1.0 - tw[i]) * p[i] : kAlpha * (1.0 - tw[i]) * p[i] + kBeta * s;
+    }
+}
+
+void singleton_exits(int32_t n, const int64_t *out_off, const double *out_f, const double *p, const double *tw,
+                     const uint8_t *dangling, double *exitpr, cudaStream_t s) {
+    k_singleton_exit<<<blocks_for(n, 128, num_sms() * 16), 128, 0, s>>>(n, out_off, out_f, p, tw, dangling, exitpr);
+    RMX_LAUNCHED();
+}
+
+}  // namespace rmx

@@ -1,0 +1,78 @@
+// The opaque handle behind the C ABI: one graph resident on one device, its
+// CUDA stream, the device arenas, and the engine state of the optimiser.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/relaxmap_b200.h"
+#include "rmx_engine.cuh"
+
+struct rmx_graph {
+    // ---- host-side description
+    int32_t N = 0;
+    int64_t E = 0;       // kept links
+    int64_t n_self = 0;  // dropped self-links with positive weight
+    std::vector<std::string> names;
+    std::vector<double> node_w;
+    double tot_w = 0.0;
+
+    // ---- device
+    cudaStream_t stream = nullptr;
+    rmx::Arena perm, scratch;
+    int64_t *out_off = nullptr, *in_off = nullptr;
+    int32_t *out_dst = nullptr, *in_src = nullptr;
+    double *out_w0 = nullptr, *out_f = nullptr, *in_w = nullptr;
+    rmx::fx_t *out_fx = nullptr, *in_fx = nullptr;
+    double *tw = nullptr, *p = nullptr;
+    uint8_t *dangling = nullptr;
+    rmx::Stat4 *nattr = nullptr;
+    int32_t *nmod = nullptr, *zeros = nullptr, *node_sn = nullptr, *submod = nullptr;
+    rmx::fx_t *s0 = nullptr;
+    int64_t *dtmp = nullptr;  // small device scratch (counters)
+
+    rmx::Level node_lv, sn_lv, sub_lv;
+    rmx::ModState mods, submods;
+    rmx::InstState inst1, instsub;
+    rmx::SweepWork work;
+    rmx::Timers timers;
+
+    // ---- state
+    bool initiated = false;
+    int power_iters = 0;
+    int spmv_vec = 32;
+    double L0 = 0.0;
+    uint32_t stamp = 0;
+    uint64_t sweep_no = 0;
+    std::vector<double> step_bits;
+    rmx_profile prof{};
+    int64_t edges_evaluated = 0, units_evaluated = 0;
+
+    // current run settings
+    rmx_opts opt{};
+    uint32_t run_seed = 0;
+    int nsub = 4;
+    int superstep = 0;
+
+    ~rmx_graph();
+    void create(const int32_t *src, const int32_t *dst, const double *w, int64_t n_edges, int32_t n,
+                const double *node_weights);
+    void initiate();
+    double codelength_fp64(const int32_t *part_host);
+    void coarsen_hook(const int32_t *part, int32_t *n_sn, int64_t *n_links, int32_t *sn_of_mod, int64_t *o_off,
+                      int32_t *o_dst, double *o_f, int64_t *i_off, int32_t *i_src, double *i_f);
+    void evaluate_hook(const int32_t *part, const uint8_t *allow_new, int32_t *best_mod, double *best_delta);
+    double optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modules);
+
+  private:
+    void alloc_engine();
+    void ensure_hub_table(int64_t max_degree);
+    double run_attempt(uint32_t seed);
+    double stage(bool fine, double L);
+    double stage_sweeps(rmx::Level &lv, bool allow_new, double L);
+    double sweep_single(rmx::Level &lv, bool prior, bool allow_new, double vthresh, int64_t &n_active);
+    void convert_to_supernodes();
+    void generate_sub_modules();
+    void project_sn_to_nodes();
+    int32_t count_modules();
+    int64_t max_degree(const rmx::Level &lv);
+};

@@ -1,0 +1,362 @@
+// Input parsing and output writing with the reference's exact rules.
+//
+// Both reference loaders read lines with getline and split them with
+// `istringstream >> string` into one string variable `buf` that lives across
+// lines. A read that finds no token leaves `buf` unchanged, so a blank line in
+// an edge list re-reads the previous line's last token. After any processed
+// line `buf` holds that line's third token or "" (it is cleared before the
+// weight is read), so the state entering a line depends only on the previous
+// processed line: the parser below reproduces it, also across the chunk
+// boundaries of the multi-threaded edge-list parse.
+#include "rmx_io.hpp"
+
+#include <algorithm>
+#include <cerrno>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <thread>
+
+namespace rmx {
+
+namespace {
+
+inline bool is_ws(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; }
+
+struct Tok {
+    const char *b = nullptr, *e = nullptr;
+    bool empty() const { return b == e; }
+    std::string str() const { return std::string(b, e); }
+};
+
+// One line as an istringstream: successive >> reads until the first failure.
+struct LineStream {
+    const char *p, *end;
+    bool failed = false;
+    LineStream(const char *b, const char *e) : p(b), end(e) {}
+    // istringstream >> buf: on failure buf is left as it was
+    void read(Tok &buf) {
+        if (failed) return;
+        while (p < end && is_ws(*p)) p++;
+        if (p == end) {
+            failed = true;
+            return;
+        }
+        const char *s = p;
+        while (p < end && !is_ws(*p)) p++;
+        buf.b = s;
+        buf.e = p;
+    }
+};
+
+// C atol / atoi on a token (the token has no leading whitespace).
+long long c_atol(const Tok &t) {
+    const char *p = t.b;
+    bool neg = false;
+    if (p < t.e && (*p == '+' || *p == '-')) neg = *p++ == '-';
+    unsigned long long v = 0;
+    while (p < t.e && *p >= '0' && *p <= '9') v = v * 10 + (unsigned)(*p++ - '0');
+    return neg ? -(long long)v : (long long)v;
+}
+
+// C atof (strtod) on a token.
+double c_atof(const Tok &t) {
+    char buf[96];
+    size_t n = (size_t)(t.e - t.b);
+    if (n < sizeof buf) {
+        memcpy(buf, t.b, n);
+        buf[n] = 0;
+        return strtod(buf, nullptr);
+    }
+    std::string s(t.b, t.e);
+    return strtod(s.c_str(), nullptr);
+}
+
+std::vector<char> read_all(const std::string &path) {
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) throw IoError("cannot open " + path + ": " + strerror(errno));
+    std::vector<char> data;
+    char chunk[1 << 16];
+    size_t r;
+    while ((r = fread(chunk, 1, sizeof chunk, f)) > 0) data.insert(data.end(), chunk, chunk + r);
+    fclose(f);
+    return data;
+}
+
+// [begin, end) of every getline() line (no trailing empty line after a final '\n').
+void split_lines(const std::vector<char> &d, size_t from, size_t to, std::vector<std::pair<size_t, size_t>> &out) {
+    size_t s = from;
+    for (size_t i = from; i < to; i++)
+        if (d[i] == '\n') {
+            out.push_back({s, i});
+            s = i + 1;
+        }
+    if (s < to) out.push_back({s, to});
+}
+
+struct EdgeChunk {
+    std::vector<long long> a, b;
+    std::vector<double> w;
+};
+
+// Parse edge-list lines [l0, l1); `buf` is the stream state entering l0.
+void parse_edge_lines(const std::vector<char> &d, const std::vector<std::pair<size_t, size_t>> &lines, size_t l0,
+                      size_t l1, Tok buf, EdgeChunk &out) {
+    const char *base = d.data();
+    for (size_t l = l0; l < l1; l++) {
+        const char *b = base + lines[l].first, *e = base + lines[l].second;
+        if (b < e && *b == '#') continue;  // FileIO.cpp:198 (line[0] of "" is '\0')
+        LineStream ss(b, e);
+        ss.read(buf);
+        const long long x = c_atol(buf);
+        ss.read(buf);
+        const long long y = c_atol(buf);
+        buf = Tok();
+        ss.read(buf);
+        const double w = buf.empty() ? 1.0 : c_atof(buf);
+        out.a.push_back(x);
+        out.b.push_back(y);
+        out.w.push_back(w);
+    }
+}
+
+// State of `buf` after the last processed line before line l.
+Tok state_before(const std::vector<char> &d, const std::vector<std::pair<size_t, size_t>> &lines, size_t l) {
+    const char *base = d.data();
+    while (l > 0) {
+        l--;
+        const char *b = base + lines[l].first, *e = base + lines[l].second;
+        if (b < e && *b == '#') continue;
+        LineStream ss(b, e);
+        Tok t;
+        ss.read(t);
+        ss.read(t);
+        Tok third;
+        ss.read(third);
+        return third;  // "" unless the line had a third token
+    }
+    return Tok();
+}
+
+}  // namespace
+
+ParsedGraph parse_edge_list(const std::string &path, int threads) {
+    std::vector<char> d = read_all(path);
+    std::vector<std::pair<size_t, size_t>> lines;
+    lines.reserve(d.size() / 8 + 1);
+    split_lines(d, 0, d.size(), lines);
+    const size_t nl = lines.size();
+    int T = std::max(1, std::min(threads, 64));
+    if (nl < 100000) T = 1;
+    std::vector<EdgeChunk> chunks(T);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < T; t++) {
+        const size_t l0 = nl * t / T, l1 = nl * (t + 1) / T;
+        auto job = [&, t, l0, l1] { parse_edge_lines(d, lines, l0, l1, state_before(d, lines, l0), chunks[t]); };
+        if (T == 1)
+            job();
+        else
+            pool.emplace_back(job);
+    }
+    for (auto &th : pool) th.join();
+    // every id seen, renumbered in ascending order (FileIO.cpp:242-255)
+    std::vector<long long> ids;
+    size_t total = 0;
+    for (auto &c : chunks) total += c.a.size();
+    ids.reserve(2 * total);
+    for (auto &c : chunks) {
+        ids.insert(ids.end(), c.a.begin(), c.a.end());
+        ids.insert(ids.end(), c.b.begin(), c.b.end());
+    }
+    std::sort(ids.begin(), ids.end());
+    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+    if (ids.size() >= (size_t)INT32_MAX) throw FormatError("more than 2^31-1 nodes");
+    ParsedGraph g;
+    g.n = (int32_t)ids.size();
+    g.n_lines = (int64_t)total;
+    g.names.resize(ids.size());
+    for (size_t i = 0; i < ids.size(); i++) g.names[i] = std::to_string(ids[i]);
+    const bool dense = !ids.empty() && (ids.back() - ids.front()) < (long long)(4 * ids.size() + 1024);
+    std::vector<int32_t> table;
+    if (dense) {
+        table.assign((size_t)(ids.back() - ids.front() + 1), -1);
+        for (size_t i = 0; i < ids.size(); i++) table[(size_t)(ids[i] - ids.front())] = (int32_t)i;
+    }
+    auto ren = [&](long long x) -> int32_t {
+        if (dense) return table[(size_t)(x - ids.front())];
+        return (int32_t)(std::lower_bound(ids.begin(), ids.end(), x) - ids.begin());
+    };
+    g.src.reserve(total);
+    g.dst.reserve(total);
+    g.w.reserve(total);
+    std::map<int32_t, double> self;
+    for (auto &c : chunks) {
+        for (size_t i = 0; i < c.a.size(); i++) {
+            const int32_t x = ren(c.a[i]), y = ren(c.b[i]);
+            if (x == y) {
+                self[x] += c.w[i];
+                continue;
+            }
+            g.src.push_back(x);
+            g.dst.push_back(y);
+            g.w.push_back(c.w[i]);
+        }
+        EdgeChunk().a.swap(c.a);
+    }
+    for (auto &kv : self)
+        if (kv.second > 0.0) g.n_self++;
+    return g;
+}
+
+ParsedGraph parse_pajek(const std::string &path) {
+    std::vector<char> d;
+    try {
+        d = read_all(path);
+    } catch (const IoError &) {
+        // the reference reads from a failed stream: "not in Pajek format"
+        throw FormatError("the network file is not in Pajek format...exiting");
+    }
+    std::vector<std::pair<size_t, size_t>> lines;
+    split_lines(d, 0, d.size(), lines);
+    const char *base = d.data();
+    size_t li = 0;
+    Tok buf;
+    long long n = 0;
+    auto line_at = [&](size_t i, const char *&b, const char *&e) {
+        if (i < lines.size()) {
+            b = base + lines[i].first;
+            e = base + lines[i].second;
+        } else {
+            b = e = base;
+        }
+    };
+    while (n == 0) {  // FileIO.cpp:59-77
+        if (li >= lines.size()) throw FormatError("the network file is not in Pajek format...exiting");
+        const char *b, *e;
+        line_at(li++, b, e);
+        LineStream ss(b, e);
+        ss.read(buf);
+        const std::string t = buf.str();
+        if (t == "*Vertices" || t == "*vertices" || t == "*VERTICES") {
+            ss.read(buf);
+            n = c_atol(buf);
+        } else {
+            throw FormatError("the network file is not in Pajek format...exiting");
+        }
+    }
+    if (n < 0 || n >= INT32_MAX) throw FormatError("invalid vertex count");
+    if (li + (size_t)n > lines.size()) throw FormatError("Number of nodes not matching, exiting");
+    ParsedGraph g;
+    g.n = (int32_t)n;
+    g.names.resize((size_t)n);
+    g.node_w.assign((size_t)n, 1.0);
+    for (long long i = 0; i < n; i++) {  // FileIO.cpp:86-121
+        const char *b, *e;
+        line_at(li++, b, e);
+        LineStream ss(b, e);
+        ss.read(buf);
+        const char *q0 = nullptr, *q1 = nullptr;
+        for (const char *c = b; c < e; c++)
+            if (*c == '"') {
+                if (!q0) q0 = c;
+                q1 = c;
+            }
+        LineStream rest(b, e);
+        if (q0 && q0 < q1) {
+            g.names[i].assign(q0 + 1, q1);
+            rest = LineStream(q1 + 1, e);
+        } else {
+            rest.read(buf);
+            rest.read(buf);
+            g.names[i] = buf.str();
+        }
+        static const char one[] = "1";
+        buf.b = one;
+        buf.e = one + 1;
+        rest.read(buf);
+        double x = c_atof(buf);
+        if (x <= 0.0) x = 1.0;
+        g.node_w[i] = x;
+    }
+    {  // FileIO.cpp:126-134
+        const char *b, *e;
+        line_at(li++, b, e);
+        LineStream ss(b, e);
+        ss.read(buf);
+        const std::string t = buf.str();
+        if (t != "*Edges" && t != "*edges" && t != "*Arcs" && t != "*arcs")
+            throw FormatError("Number of nodes not matching, exiting");
+    }
+    std::map<long long, double> self;
+    for (; li < lines.size(); li++) {  // FileIO.cpp:140-160
+        const char *b = base + lines[li].first, *e = base + lines[li].second;
+        LineStream ss(b, e);
+        ss.read(buf);
+        const long long x = c_atol(buf) - 1;
+        ss.read(buf);
+        const long long y = c_atol(buf) - 1;
+        buf = Tok();
+        ss.read(buf);
+        const double w = buf.empty() ? 1.0 : c_atof(buf);
+        g.n_lines++;
+        if (x == y) {  // self-links are counted then dropped (OmpRelaxmap.cpp:123-128)
+            self[x] += w;
+            continue;
+        }
+        if (x < 0 || y < 0 || x >= n || y >= n)
+            throw FormatError("link " + std::to_string(x + 1) + " " + std::to_string(y + 1) + " outside 1.." +
+                              std::to_string(n));
+        g.src.push_back((int32_t)x);
+        g.dst.push_back((int32_t)y);
+        g.w.push_back(w);
+    }
+    for (auto &kv : self)
+        if (kv.second > 0.0) g.n_self++;
+    return g;
+}
+
+ParsedGraph parse_file(const std::string &path, int threads) {
+    const size_t dot = path.find_last_of('.');
+    const std::string ext = dot == std::string::npos ? std::string() : path.substr(dot);
+    if (ext == ".net") return parse_pajek(path);
+    return parse_edge_list(path, threads);
+}
+
+void write_tree(const std::string &file, double L_bits, int32_t n_modules, const std::vector<int32_t> &part,
+                const std::vector<double> &size, const std::vector<std::string> &names) {
+    FILE *f = fopen(file.c_str(), "wb");
+    if (!f) throw IoError("cannot write " + file);
+    fprintf(f, "# Code length %g in %d modules.\n", L_bits, n_modules);
+    const size_t n = part.size();
+    // members of each module in node order (updateMembersInModule, Module.cpp:2900-2901),
+    // modules in index order, renumbered 1.. over the non-empty ones
+    std::vector<int64_t> head(n + 1, 0);
+    for (size_t v = 0; v < n; v++) head[(size_t)part[v] + 1]++;
+    for (size_t m = 0; m < n; m++) head[m + 1] += head[m];
+    std::vector<int32_t> mem(n);
+    std::vector<int64_t> fill(head.begin(), head.end() - 1);
+    for (size_t v = 0; v < n; v++) mem[fill[(size_t)part[v]]++] = (int32_t)v;
+    int mod = 0;
+    for (size_t m = 0; m < n; m++) {
+        if (head[m + 1] == head[m]) continue;
+        mod++;
+        for (int64_t j = head[m]; j < head[m + 1]; j++) {
+            const int32_t v = mem[j];
+            fprintf(f, "%d:%lld %g \"%s\"\n", mod, (long long)(j - head[m] + 1), size[v],
+                    v < (int32_t)names.size() ? names[v].c_str() : "");
+        }
+    }
+    fclose(f);
+}
+
+void write_clu(const std::string &file, const std::vector<int32_t> &part) {
+    FILE *f = fopen(file.c_str(), "wb");
+    if (!f) throw IoError("cannot write " + file);
+    fprintf(f, "*Vertices %zu\r\n", part.size());
+    for (int32_t m : part) fprintf(f, "%d\r\n", m + 1);
+    fclose(f);
+}
+
+}  // namespace rmx

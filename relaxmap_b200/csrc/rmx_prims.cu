@@ -1,0 +1,315 @@
+// Device-wide primitives (see rmx_prims.cuh).
+#include <algorithm>
+
+#include "rmx_prims.cuh"
+
+namespace rmx {
+
+int num_sms() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0)
+            n = 148;
+    }
+    return n;
+}
+
+void Arena::init(size_t bytes) {
+    RMX_CUDA(cudaMalloc(&base, bytes));
+    cap = bytes;
+    top = peak = 0;
+}
+
+void Arena::destroy() {
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = top = peak = 0;
+}
+
+void *Arena::alloc_bytes(size_t bytes) {
+    size_t a = (top + 255) & ~size_t(255);
+    if (a + bytes > cap) throw CudaError(cudaErrorMemoryAllocation, "device scratch arena exhausted");
+    top = a + bytes;
+    peak = std::max(peak, top);
+    return base + a;
+}
+
+// ------------------------------------------------------------------- scan
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kScanT = 512, kScanI = 8, kScanTile = kScanT * kScanI;
+
+// Exclusive scan of one value per thread across the block; *total = block sum.
+template <typename T>
+__device__ __forceinline__ T block_exclusive(T v, T *warp_sums, T *total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    T x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        T s = lane < nw ? warp_sums[lane] : T(0);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T y = __shfl_up_sync(kFull, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < nw) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    T pre = (w > 0 ? warp_sums[w - 1] : T(0)) + x - v;
+    *total = warp_sums[nw - 1];
+    __syncthreads();
+    return pre;
+}
+
+template <typename T>
+__global__ void k_scan_block_sums(const T *in, int64_t n, T *bsum) {
+    __shared__ T ws[32];
+    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanI;
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanI; i++)
+        if (base + i < n) s += in[base + i];
+    T tot;
+    block_exclusive(s, ws, &tot);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+template <typename T>
+__global__ void k_scan_apply(const T *in, T *out, int64_t n, const T *boff, T *total) {
+    __shared__ T ws[32];
+    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanI;
+    T v[kScanI];
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < kScanI; i++) {
+        v[i] = base + i < n ? in[base + i] : T(0);
+        s += v[i];
+    }
+    T tot;
+    T pre = block_exclusive(s, ws, &tot) + (boff ? boff[blockIdx.x] : T(0));
+#pragma unroll
+    for (int i = 0; i < kScanI; i++) {
+        if (base + i < n) out[base + i] = pre;
+        pre += v[i];
+    }
+    if (total && !boff && threadIdx.x == 0) *total = tot;
+}
+
+template <typename T>
+static void scan_impl(const T *in, T *out, int64_t n, T *total, Arena &ar, cudaStream_t s) {
+    if (n <= 0) {
+        if (total) RMX_CUDA(cudaMemsetAsync(total, 0, sizeof(T), s));
+        return;
+    }
+    int64_t nb = (n + kScanTile - 1) / kScanTile;
+    if (nb == 1) {
+        k_scan_apply<T><<<1, kScanT, 0, s>>>(in, out, n, nullptr, total);
+        RMX_LAUNCHED();
+        return;
+    }
+    size_t m = ar.mark();
+    T *bsum = ar.alloc<T>(nb);
+    k_scan_block_sums<T><<<(unsigned)nb, kScanT, 0, s>>>(in, n, bsum);
+    RMX_LAUNCHED();
+    scan_impl<T>(bsum, bsum, nb, total, ar, s);
+    k_scan_apply<T><<<(unsigned)nb, kScanT, 0, s>>>(in, out, n, bsum, nullptr);
+    RMX_LAUNCHED();
+    ar.release(m);
+}
+
+void scan_exclusive(const int64_t *in, int64_t *out, int64_t n, int64_t *total, Arena &ar, cudaStream_t s) {
+    scan_impl<long long>(reinterpret_cast<const long long *>(in), reinterpret_cast<long long *>(out), n,
+                         reinterpret_cast<long long *>(total), ar, s);
+}
+void scan_exclusive(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *total, Arena &ar, cudaStream_t s) {
+    scan_impl<unsigned>(in, out, n, total, ar, s);
+}
+
+// ------------------------------------------------------------- compaction
+
+__global__ void k_flag_count(const uint8_t *flags, int64_t n, long long *bsum) {
+    __shared__ long long ws[32];
+    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanI;
+    long long c = 0;
+#pragma unroll
+    for (int i = 0; i < kScanI; i++)
+        if (base + i < n && flags[base + i]) c++;
+    long long tot;
+    block_exclusive(c, ws, &tot);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+}
+
+__global__ void k_flag_scatter(const uint8_t *flags, int64_t n, const long long *boff, int32_t *out) {
+    __shared__ long long ws[32];
+    int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanI;
+    uint8_t f[kScanI];
+    long long c = 0;
+#pragma unroll
+    for (int i = 0; i < kScanI; i++) {
+        f[i] = (base + i < n) ? flags[base + i] : 0;
+        c += f[i] != 0;
+    }
+    long long tot;
+    long long pre = block_exclusive(c, ws, &tot) + boff[blockIdx.x];
+#pragma unroll
+    for (int i = 0; i < kScanI; i++)
+        if (f[i]) out[pre++] = (int32_t)(base + i);
+}
+
+void compact_flags(const uint8_t *flags, int64_t n, int32_t *out, int64_t *count, Arena &ar, cudaStream_t s) {
+    if (n <= 0) {
+        RMX_CUDA(cudaMemsetAsync(count, 0, sizeof(int64_t), s));
+        return;
+    }
+    size_t m = ar.mark();
+    int64_t nb = (n + kScanTile - 1) / kScanTile;
+    long long *bsum = ar.alloc<long long>(nb);
+    k_flag_count<<<(unsigned)nb, kScanT, 0, s>>>(flags, n, bsum);
+    RMX_LAUNCHED();
+    scan_impl<long long>(bsum, bsum, nb, reinterpret_cast<long long *>(count), ar, s);
+    k_flag_scatter<<<(unsigned)nb, kScanT, 0, s>>>(flags, n, bsum, out);
+    RMX_LAUNCHED();
+    ar.release(m);
+}
+
+// ------------------------------------------------------------- radix sort
+// One stable counting pass: per-tile digit histograms laid out digit-major,
+// an exclusive scan over them gives each (digit, tile) its output offset, and
+// the scatter ranks equal digits within a tile in input order (warp match +
+// per-warp counters). Tiles hold kRsT * kRsI elements in round-major order.
+
+constexpr int kRsT = 256, kRsI = 16, kRsTile = kRsT * kRsI, kRsW = kRsT / 32;
+
+struct KeyDigit {
+    const uint64_t *k;
+    int shift;
+    unsigned mask;
+    __device__ unsigned operator()(int64_t e) const { return (unsigned)(k[e] >> shift) & mask; }
+};
+struct ArrDigit {
+    const uint16_t *d;
+    __device__ unsigned operator()(int64_t e) const { return d[e]; }
+};
+
+template <typename Dig>
+__global__ void __launch_bounds__(kRsT) k_rs_hist(Dig dig, int64_t n, int nb, unsigned *hist, int64_t ntiles) {
+    __shared__ unsigned cnt[256];
+    for (int i = threadIdx.x; i < nb; i += kRsT) cnt[i] = 0;
+    __syncthreads();
+    int64_t base = (int64_t)blockIdx.x * kRsTile;
+#pragma unroll 4
+    for (int r = 0; r < kRsI; r++) {
+        int64_t e = base + (int64_t)r * kRsT + threadIdx.x;
+        if (e < n) atomicAdd(&cnt[dig(e)], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nb; i += kRsT) hist[(int64_t)i * ntiles + blockIdx.x] = cnt[i];
+}
+
+template <typename Dig, typename K, typename V>
+__global__ void __launch_bounds__(kRsT) k_rs_scatter(Dig dig, const K *kin, K *kout, const V *vin, V *vout, int64_t n,
+                                                     int nb, const unsigned *offs, int64_t ntiles) {
+    __shared__ unsigned run[256];
+    __shared__ unsigned wc[kRsW][256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < 256; i += kRsT) {
+        run[i] = i < nb ? offs[(int64_t)i * ntiles + blockIdx.x] : 0u;
+#pragma unroll
+        for (int q = 0; q < kRsW; q++) wc[q][i] = 0;
+    }
+    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+    int64_t base = (int64_t)blockIdx.x * kRsTile;
+    for (int r = 0; r < kRsI; r++) {
+        int64_t e = base + (int64_t)r * kRsT + threadIdx.x;
+        bool valid = e < n;
+        unsigned d = valid ? dig(e) : 0x10000u;
+        unsigned peers = __match_any_sync(kFull, d);
+        unsigned rank = __popc(peers & lt);
+        if (valid && rank == 0) wc[w][d] = __popc(peers);
+        __syncthreads();
+        if (valid) {
+            unsigned pos = run[d] + rank;
+            for (int q = 0; q < w; q++) pos += wc[q][d];
+            if (kout) kout[pos] = kin[e];
+            vout[pos] = vin[e];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nb; i += kRsT) {
+            unsigned t = 0;
+#pragma unroll
+            for (int q = 0; q < kRsW; q++) {
+                t += wc[q][i];
+                wc[q][i] = 0;
+            }
+            run[i] += t;
+        }
+        __syncthreads();
+    }
+}
+
+void radix_sort_pairs(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32_t *vals_alt, int64_t n,
+                      int key_bits, Arena &ar, cudaStream_t s) {
+    if (n <= 1 || key_bits <= 0) return;
+    if (n >= (int64_t(1) << 32)) throw std::invalid_argument("radix_sort_pairs: more than 2^32 items");
+    int64_t ntiles = (n + kRsTile - 1) / kRsTile;
+    size_t m = ar.mark();
+    unsigned *hist = ar.alloc<unsigned>(256 * ntiles);
+    uint64_t *ks = keys, *kd = keys_alt;
+    uint32_t *vs = vals, *vd = vals_alt;
+    for (int shift = 0; shift < key_bits; shift += 8) {
+        int bits = std::min(8, key_bits - shift);
+        int nb = 1 << bits;
+        KeyDigit dig{ks, shift, (unsigned)nb - 1u};
+        k_rs_hist<<<(unsigned)ntiles, kRsT, 0, s>>>(dig, n, nb, hist, ntiles);
+        RMX_LAUNCHED();
+        scan_impl<unsigned>(hist, hist, (int64_t)nb * ntiles, nullptr, ar, s);
+        k_rs_scatter<<<(unsigned)ntiles, kRsT, 0, s>>>(dig, ks, kd, vs, vd, n, nb, hist, ntiles);
+        RMX_LAUNCHED();
+        std::swap(ks, kd);
+        std::swap(vs, vd);
+    }
+    if (ks != keys) {
+        RMX_CUDA(cudaMemcpyAsync(keys, ks, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s));
+        RMX_CUDA(cudaMemcpyAsync(vals, vs, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+    }
+    ar.release(m);
+}
+
+__global__ void k_bucket_bounds(const unsigned *offs, int64_t ntiles, int nb, int64_t n, int64_t *bucket_off) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nb) bucket_off[i] = offs[(int64_t)i * ntiles];
+    if (i == nb) bucket_off[nb] = n;
+}
+
+void bucket_partition(const uint16_t *bucket, const int32_t *vals_in, int32_t *vals_out, int64_t n, int nb,
+                      int64_t *bucket_off, Arena &ar, cudaStream_t s) {
+    if (nb < 1 || nb > 256) throw std::invalid_argument("bucket_partition: 1..256 buckets");
+    if (n <= 0) {
+        RMX_CUDA(cudaMemsetAsync(bucket_off, 0, sizeof(int64_t) * (nb + 1), s));
+        return;
+    }
+    int64_t ntiles = (n + kRsTile - 1) / kRsTile;
+    size_t m = ar.mark();
+    unsigned *hist = ar.alloc<unsigned>((size_t)nb * ntiles);
+    ArrDigit dig{bucket};
+    k_rs_hist<<<(unsigned)ntiles, kRsT, 0, s>>>(dig, n, nb, hist, ntiles);
+    RMX_LAUNCHED();
+    scan_impl<unsigned>(hist, hist, (int64_t)nb * ntiles, nullptr, ar, s);
+    k_rs_scatter<ArrDigit, int32_t, int32_t>
+        <<<(unsigned)ntiles, kRsT, 0, s>>>(dig, nullptr, nullptr, vals_in, vals_out, n, nb, hist, ntiles);
+    RMX_LAUNCHED();
+    k_bucket_bounds<<<1, 288, 0, s>>>(hist, ntiles, nb, n, bucket_off);
+    RMX_LAUNCHED();
+    ar.release(m);
+}
+
+}  // namespace rmx

@@ -1,0 +1,45 @@
+// Device-wide primitives: exclusive scan, stable compaction, stable LSD radix
+// sort and stable bucket partition. All are deterministic (results do not
+// depend on scheduling) and run on the caller's stream with scratch from an
+// Arena (no allocation inside).
+#pragma once
+#include "rmx_common.cuh"
+
+namespace rmx {
+
+// Bump allocator over one device allocation. mark()/release() give scoped
+// scratch; alloc() throws CudaError(cudaErrorMemoryAllocation) when full.
+struct Arena {
+    char *base = nullptr;
+    size_t cap = 0, top = 0, peak = 0;
+    void init(size_t bytes);
+    void destroy();
+    void *alloc_bytes(size_t bytes);
+    template <typename T>
+    T *alloc(size_t n) {
+        return static_cast<T *>(alloc_bytes(n * sizeof(T)));
+    }
+    size_t mark() const { return top; }
+    void release(size_t m) { top = m; }
+};
+
+// out[i] = sum_{j<i} in[i] for i < n; if total != nullptr, *total (device) =
+// sum of all n. in and out may alias.
+void scan_exclusive(const int64_t *in, int64_t *out, int64_t n, int64_t *total, Arena &ar, cudaStream_t s);
+void scan_exclusive(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *total, Arena &ar, cudaStream_t s);
+
+// Indices i (ascending) with flags[i] != 0 written to out; *count (device).
+void compact_flags(const uint8_t *flags, int64_t n, int32_t *out, int64_t *count, Arena &ar, cudaStream_t s);
+
+// Stable sort of (key, value) pairs by key bits [0, key_bits). Sorted data ends
+// in keys/vals (the alt buffers are scratch of the same size).
+void radix_sort_pairs(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32_t *vals_alt, int64_t n,
+                      int key_bits, Arena &ar, cudaStream_t s);
+
+// Stable partition of items by a small bucket id (< nb <= 256): vals_out holds
+// the values grouped by bucket, input order kept within a bucket; bucket_off
+// (device, nb+1 entries) receives the bucket boundaries.
+void bucket_partition(const uint16_t *bucket, const int32_t *vals_in, int32_t *vals_out, int64_t n, int nb,
+                      int64_t *bucket_off, Arena &ar, cudaStream_t s);
+
+}  // namespace rmx

@@ -1,0 +1,120 @@
+"""Host-side logic without a GPU: the C ABI library loads and exports every
+declared symbol, the loaders follow the reference's parsing rules, and input
+errors map to status codes."""
+import re
+
+import numpy as np
+import pytest
+
+from conftest import FIXTURES, GOLDEN, ROOT, golden
+
+
+def test_exports_match_header(built_lib):
+    import ctypes
+    from relaxmap_b200 import EXPORTS
+    hdr = (ROOT / "include" / "relaxmap_b200.h").read_text()
+    declared = set(re.findall(r"\b(rmx_\w+)\s*\(", hdr))
+    assert declared == set(EXPORTS)
+    L = ctypes.CDLL(str(built_lib))
+    for name in declared:
+        assert hasattr(L, name), name
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("threads", [1, 4])
+def test_parse_matches_reference_loader(built_lib, name, threads):
+    from relaxmap_b200 import parse_file
+    g = golden(name)
+    d = parse_file(GOLDEN / name, threads=threads)
+    assert d["n"] == int(g["n"])
+    acc = {}
+    for a, b, x in zip(d["src"].tolist(), d["dst"].tolist(), d["w"].tolist()):
+        acc[(a, b)] = acc.get((a, b), 0.0) + x
+    ref = {(a, b): x for a, b, x in zip(g["map_src"].tolist(), g["map_dst"].tolist(), g["map_w"].tolist()) if a != b}
+    assert acc == ref
+    np.testing.assert_array_equal(d["node_w"], g["node_w"])
+
+
+def _cmp_oracle(path, oracle_mod):
+    from relaxmap_b200 import parse_file
+    O = oracle_mod
+    ld = O.parse_pajek(path) if str(path).endswith(".net") else O.parse_txt(path)
+    for t in (1, 3):
+        d = parse_file(path, threads=t)
+        assert d["n"] == ld.n
+        acc = {}
+        for a, b, x in zip(d["src"].tolist(), d["dst"].tolist(), d["w"].tolist()):
+            acc[(a, b)] = acc.get((a, b), 0.0) + x
+        ref = {(a, b): x for a, b, x in zip(ld.src.tolist(), ld.dst.tolist(), ld.w.tolist()) if a != b}
+        assert acc == ref
+        n_self = sum(1 for a, b, x in zip(ld.src.tolist(), ld.dst.tolist(), ld.w.tolist()) if a == b and x > 0)
+        assert d["n_self"] == n_self
+    return ld
+
+
+def test_edge_list_quirks(built_lib, oracle_mod, tmp_path):
+    """Comments, CRLF, weights, duplicates, self-links, sparse / negative ids,
+    and a blank line re-reading the previous token (a phantom self-link)."""
+    p = tmp_path / "q.txt"
+    p.write_bytes(b"# comment\n5 9 2.5\r\n9 5\n\n5 9 0.5\n-3 5 1e-1\n7 7 4\n  100\t5 3\n\n")
+    ld = _cmp_oracle(p, oracle_mod)
+    # a blank line after "9 5" re-reads "" (node 0); after "100 5 3" it re-reads "3"
+    assert ld.names == ["-3", "0", "3", "5", "7", "9", "100"]
+
+
+def test_edge_list_large_threads(built_lib, oracle_mod, tmp_path):
+    rng = np.random.default_rng(2)
+    lines = []
+    for i in range(120000):
+        r = rng.random()
+        if r < 0.01:
+            lines.append("")
+        elif r < 0.02:
+            lines.append("# c")
+        elif r < 0.5:
+            lines.append(f"{rng.integers(0, 5000)} {rng.integers(0, 5000)}")
+        else:
+            lines.append(f"{rng.integers(0, 5000)}\t{rng.integers(0, 5000)}\t{rng.uniform(-1, 5)!r}")
+    p = tmp_path / "big.txt"
+    p.write_text("\n".join(lines) + "\n")
+    _cmp_oracle(p, oracle_mod)
+
+
+def test_pajek_quirks(built_lib, oracle_mod, tmp_path):
+    p = tmp_path / "q.net"
+    p.write_text('*Vertices 5\n1 "a b" 2.0\n2 "c"\n3 d 0.5\n4\n5 "e" -1\n*Arcs\n1 2\n2 3 0.5\n1 2 1.5\n3 3 2\n\n5 1\n')
+    ld = _cmp_oracle(p, oracle_mod)
+    assert ld.names == ["a b", "c", "d", "4", "e"]
+    np.testing.assert_array_equal(ld.node_w, [2.0, 1.0, 0.5, 1.0, 1.0])
+
+
+def test_errors_without_device(built_lib, tmp_path):
+    from relaxmap_b200 import Graph, RmxError, parse_file
+    with pytest.raises(RmxError) as e:
+        parse_file(tmp_path / "missing.txt")
+    assert e.value.status == 2  # RMX_ERR_IO
+    bad = tmp_path / "bad.net"
+    bad.write_text("*Network x\n")
+    with pytest.raises(RmxError) as e:
+        Graph.from_file(bad)
+    assert e.value.status == 3  # RMX_ERR_FORMAT (the reference exits -1)
+    bad.write_text("*Vertices 2\n1\n2\n*Edges\n1 3\n")
+    with pytest.raises(RmxError) as e:
+        parse_file(bad)
+    assert e.value.status == 3
+    bad.write_text("*Vertices 3\n1\n2\n3\n*ARCS\n")
+    with pytest.raises(RmxError) as e:
+        parse_file(bad)
+    assert e.value.status == 3
+
+
+def test_synth_deterministic():
+    from relaxmap_b200 import synth
+    a = synth.config_small(seed=42)
+    b = synth.config_small(seed=42)
+    np.testing.assert_array_equal(a.src, b.src)
+    np.testing.assert_array_equal(a.dst, b.dst)
+    assert a.n == 1000 and 15 < a.m / a.n < 21
+    r = synth.rmat(10, 16, seed=1)
+    assert r.n == 1024 and np.all(r.src != r.dst)
+    assert len(np.unique(r.src.astype(np.int64) * r.n + r.dst)) == r.m

@@ -1,0 +1,79 @@
+"""Stationary flow, edge flows and the initial code length on the GPU against
+the reference (golden vectors) and the oracle (larger seeded graphs)."""
+import numpy as np
+import pytest
+
+from conftest import FIXTURES, GOLDEN, golden
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l1(a, b):
+    return np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300)
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_flows_match_reference(built_lib, name):
+    from relaxmap_b200 import Graph
+    g = golden(name)
+    with Graph.from_file(GOLDEN / name) as G:
+        off, dst, w, tw = G.links()
+        np.testing.assert_array_equal(off, g["off"])
+        np.testing.assert_array_equal(dst, g["dst"])
+        keep = (g["map_w"] > 0) & (g["map_src"] != g["map_dst"])
+        np.testing.assert_array_equal(w, g["map_w"][keep])
+        np.testing.assert_array_equal(tw, g["tw"])
+        r = G.initiate()
+    assert rel_l1(r["p"], g["p"]) <= 1e-12          # flow within 1e-12 relative L1
+    assert rel_l1(r["f"], g["f"]) <= 1e-12
+    assert rel_l1(r["exit"], g["exit"]) <= 1e-12
+    np.testing.assert_array_equal(r["dangling"], g["dangling"])
+    assert abs(r["L0"] - float(g["L0"])) <= 1e-10
+    assert 50 <= r["iters"] <= 200
+
+
+@pytest.mark.parametrize("weights", [None, "uniform", "lognormal"])
+def test_flows_synthetic_vs_oracle(built_lib, oracle_mod, weights):
+    from relaxmap_b200 import Graph, synth
+    O = oracle_mod
+    sg = synth.planted_partition(5000, 12, 300, 10, 200, 0.35, seed=3, weights=weights)
+    # some dangling nodes: drop every out-link of 3% of the nodes
+    rng = np.random.default_rng(0)
+    dead = rng.random(sg.n) < 0.03
+    keep = ~dead[sg.src]
+    src, dst = sg.src[keep], sg.dst[keep]
+    w = None if sg.w is None else sg.w[keep]
+    prep = O.prepare(O.from_edges(sg.n, src, dst, w))
+    st = O.initiate(prep)
+    with Graph.from_edges(src, dst, w, n=sg.n) as G:
+        r = G.initiate()
+    assert rel_l1(r["p"], st["p"]) <= 1e-12
+    assert rel_l1(r["f"], st["f"]) <= 1e-12
+    assert abs(r["L0"] - st["L0"]) <= 1e-10
+
+
+def test_node_weights_teleport(built_lib, oracle_mod, tmp_path):
+    """Pajek node weights set non-uniform teleportation (FileIO.cpp:114-120)."""
+    from relaxmap_b200 import Graph
+    O = oracle_mod
+    rng = np.random.default_rng(5)
+    n = 300
+    src = rng.integers(0, n, 3000)
+    dst = rng.integers(0, n, 3000)
+    nw = rng.uniform(0.1, 5.0, n)
+    path = tmp_path / "g.net"
+    with open(path, "w") as f:
+        f.write(f"*Vertices {n}\n")
+        for i in range(n):
+            f.write(f'{i + 1} "v{i}" {nw[i]!r}\n')
+        f.write("*Arcs\n")
+        for a, b in zip(src, dst):
+            f.write(f"{a + 1} {b + 1} 1.5\n")
+    prep = O.load(path)
+    st = O.initiate(prep)
+    with Graph.from_file(path) as G:
+        _, _, _, tw = G.links()
+        np.testing.assert_array_equal(tw, prep.tw)
+        r = G.initiate()
+    assert rel_l1(r["p"], st["p"]) <= 1e-12
+    assert abs(r["L0"] - st["L0"]) <= 1e-10

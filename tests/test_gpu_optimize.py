@@ -1,0 +1,68 @@
+"""The whole optimiser on the GPU: known answers, quality against the
+reference's median over 8 seeds, exact code-length bookkeeping, determinism."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden
+
+pytestmark = pytest.mark.gpu
+
+
+def test_flow_known_answer(built_lib):
+    from relaxmap_b200 import Graph
+    with Graph.from_file(GOLDEN / "flow.net") as G:
+        r = G.optimize(seed=1)
+    assert round(r["L_bits"], 5) == 3.32773
+    assert r["n_modules"] == 4
+    groups = {}
+    for v, m in enumerate(r["part"]):
+        groups.setdefault(m, []).append(v)
+    assert sorted(groups.values()) == [[0, 1, 2, 3], [4, 5, 6, 7], [8, 9, 10, 11], [12, 13, 14, 15]]
+
+
+@pytest.mark.parametrize("name", ["directNet_1k_sm_mu_03.txt", "small_planted.txt", "flow.txt"])
+@pytest.mark.parametrize("prior", [1, 0])
+def test_quality_vs_reference_median(built_lib, name, prior):
+    """Final code length within 0.5% of the reference's median over 8 seeds."""
+    from relaxmap_b200 import Graph
+    g = golden(name)
+    ref_median = float(np.median(g["final_L_computed_bits"]))
+    Ls = []
+    with Graph.from_file(GOLDEN / name) as G:
+        for seed in range(1, 9):
+            r = G.optimize(seed=seed, prior=prior)
+            # the running code length equals a from-scratch FP64 recompute
+            assert abs(r["L"] - G.codelength(r["part"])) <= 1e-10
+            Ls.append(r["L_bits"])
+    assert np.median(Ls) <= ref_median * 1.005, (np.median(Ls), ref_median)
+
+
+def test_deterministic_per_seed(built_lib):
+    from relaxmap_b200 import Graph
+    with Graph.from_file(GOLDEN / "small_planted.txt") as G:
+        a = G.optimize(seed=5)
+        b = G.optimize(seed=5)
+    np.testing.assert_array_equal(a["part"], b["part"])
+    assert a["L"] == b["L"]
+
+
+def test_attempts_keep_best(built_lib):
+    from relaxmap_b200 import Graph
+    with Graph.from_file(GOLDEN / "directNet_1k_sm_mu_03.txt") as G:
+        singles = [G.optimize(seed=s)["L"] for s in (3, 4, 5)]
+        best = G.optimize(seed=3, attempts=3)["L"]
+    assert best == min(singles)
+
+
+def test_synthetic_vs_oracle_codelength(built_lib, oracle_mod):
+    from relaxmap_b200 import Graph, synth
+    O = oracle_mod
+    sg = synth.planted_partition(20000, 15, 500, 20, 400, 0.3, seed=7, weights="uniform")
+    prep = O.prepare(O.from_edges(sg.n, sg.src, sg.dst, sg.w))
+    st = O.initiate(prep)
+    with Graph.from_edges(sg.src, sg.dst, sg.w, n=sg.n) as G:
+        r = G.optimize(seed=1)
+    assert abs(r["L"] - O.codelength(prep, st, r["part"])) <= 1e-10
+    # the planted partition is a good solution; the optimiser must match or beat it
+    L_planted = O.codelength(prep, st, sg.community)
+    assert r["L"] <= L_planted * 1.005
