@@ -1,0 +1,328 @@
+"""Benchmark: edges/s per full optimiser run on one B200 (or N replicas).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload mid|small|rmat20|rmat24]
+
+One step = one full run of the map-equation optimiser (flow power iteration,
+all supersteps, final partition) on the workload graph:
+  value  graph resident in HBM (built once), device time of K runs (CUDA
+         events on the engine's stream); edges/s = input links / time per run
+  e2e    the same through the C ABI from pinned HOST buffers every step:
+         rmx_graph_create (host->device copy, device CSR/CSC build),
+         rmx_optimize (partition copied back), rmx_graph_destroy
+The single-graph optimiser does not shard: with N GPUs every rank runs its own
+replica (no collective); value = all ranks' links / the slowest rank's time.
+--impl reference times the reference (compiled from its own sources, all host
+threads) on a bounded sample of the same workload family.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "edges/s per full run"
+UNIT = "edges/s"
+
+
+def workload(name: str):
+    from relaxmap_b200 import synth
+    if name == "small":
+        g = synth.config_small(seed=42)
+        desc = "planted partition N=1000, out-degree power law 2 (mean 20, max 50), communities [10,50], mu=0.3, unweighted"
+    elif name == "mid":
+        g = synth.config_mid(seed=42)
+        desc = ("planted partition N=1,000,000, out-degree power law 2 (mean 20, max 1000), communities power law "
+                "[20,1000], mu=0.4, weights U[1,10]")
+    elif name.startswith("rmat"):
+        scale = int(name[4:])
+        g = synth.rmat(scale, 16, seed=42)
+        desc = f"R-MAT scale {scale}, edge factor 16, (0.57,0.19,0.19,0.05), self-loops/duplicates removed"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return g, desc
+
+
+def reference_sample(name: str):
+    """The bounded CPU sample: the same generator and distributions at 1/5 of
+    the nodes (the reference's std::map build and OpenMP sweeps on the full
+    1M-node graph take minutes per run)."""
+    from relaxmap_b200 import synth
+    if name == "mid":
+        g = synth.config_mid(seed=42, n=200_000)
+        return g, "planted partition N=200,000 with the mid distributions (1/5 of the nodes), seed 1"
+    if name == "small":
+        return synth.config_small(seed=42), "the full small graph, seed 1"
+    g = synth.rmat(16, 16, seed=42)
+    return g, "R-MAT scale 16 with the same parameters"
+
+
+def run_reference(g, threads: int, seed: int = 1) -> dict:
+    """Reference optimiser on graph g: its loader-equivalent edge map, edge
+    preparation, initiate and partition (the 'w/o file IO' region)."""
+    import numpy as np
+
+    from oracle import oracle as O
+    ld = O.Loaded(g.n, [], np.ones(g.n), float(g.n), g.src.astype(np.int64), g.dst.astype(np.int64),
+                  np.ones(g.m) if g.w is None else g.w)
+    R = O.Ref(loaded=ld)
+    tp = R.prepare(threads)
+    r = R.partition(seed=seed, threads=threads, threshold=1e-3, vthresh=0.0, max_iter=10, prior=True)
+    return dict(seconds=tp + r["seconds"], L_bits=r["L_computed_bits"], n_modules=r["n_modules"])
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except ValueError:
+                continue
+            for k, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(k)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the move-evaluation kernel from the committed
+    ncu summary (profiles/), scaled as that summary states."""
+    p = ROOT / "profiles" / "eval_kernel_ncu.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_eval_link:"):
+            try:
+                return float(line.split(":", 1)[1])
+            except ValueError:
+                return None
+    return None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mid")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        bench_reference(args, world)
+        return
+
+    import numpy as np
+    import torch
+
+    from relaxmap_b200 import Graph
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+
+    g, desc = workload(args.workload)
+    E = g.m
+    # ---- resident graph
+    G = Graph.from_edges(g.src, g.dst, g.w, n=g.n)
+    G.initiate()
+    stream = torch.cuda.ExternalStream(G.stream_ptr())
+    for _ in range(args.warmup):
+        G.optimize(seed=1)
+    G.set_profiling(True)
+    launches0 = G.profile()["kernel_launches"]
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    results = []
+    with Clocks(torch.cuda.current_device()) as clk:
+        e0.record(stream)
+        for k in range(args.steps):
+            results.append(G.optimize(seed=1 + k))
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    prof = G.profile()
+    gpu_launches = prof["kernel_launches"] - launches0
+    G.set_profiling(False)
+    ms_step = ms / args.steps
+    t = torch.tensor([ms_step], device="cuda")
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    ms_step_max = float(t.item())
+    value = world * E / (ms_step_max / 1e3)
+    L_bits = [r["L_bits"] for r in results]
+
+    # ---- end to end through the C ABI with pinned host buffers
+    src = torch.from_numpy(g.src).pin_memory()
+    dst = torch.from_numpy(g.dst).pin_memory()
+    w = torch.from_numpy(g.w).pin_memory() if g.w is not None else None
+    e2e_steps = max(1, min(args.steps, 3))
+    Gw = Graph.from_host_ptrs(src.data_ptr(), dst.data_ptr(), w.data_ptr() if w is not None else 0, E, g.n)
+    Gw.optimize(seed=1)
+    Gw.close()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        Ge = Graph.from_host_ptrs(src.data_ptr(), dst.data_ptr(), w.data_ptr() if w is not None else 0, E, g.n)
+        Ge.optimize(seed=1 + k)  # the partition is copied back to host memory inside
+        Ge.close()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    t = torch.tensor([e2e_s], device="cuda")
+    if pg:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    e2e_value = world * E / float(t.item())
+
+    # ---- roofline of the dominant kernel class (move evaluation)
+    pk = peaks()
+    ev = prof["eval"]
+    achieved = ev["bytes"] / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
+    per_link = ncu_traffic()
+    traffic = None
+    if per_link is not None and ev["launches"] > 0:
+        traffic = per_link * prof["links_evaluated"] / ev["launches"]
+    shares = {k: prof[k]["ms"] for k in ("spmv", "eval", "commit", "coarsen", "codelen", "other")}
+    tot = sum(shares.values()) or 1.0
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, seed 42)",
+        "config": {"workload": desc, "nodes": g.n, "links": E, "solver": "seed 1..K, threshold 1e-3, vThresh 0.0, "
+                   "maxIter 10, prior", "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (resident graph ~2 GB)"},
+        "quality": {"L_bits_median": statistics.median(L_bits), "n_modules": results[0]["n_modules"]},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(E * (8 + (8 if w is not None else 0))),
+                "d2h_bytes_per_step": int(4 * g.n + 8)},
+        "roofline": {"kernel": "move evaluation (warp/block/hub bins)", "bound": "hbm", "achieved": achieved,
+                     "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+                     "peak_source": pk["source"], "traffic": traffic,
+                     "algorithmic_bytes_per_launch": ev["bytes"] / max(ev["launches"], 1),
+                     "launch_ms_avg": ev["ms"] / max(ev["launches"], 1)},
+        "kernel_time_share": {k: round(v / tot, 4) for k, v in shares.items()},
+        "gpu_launches": int(gpu_launches),
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            sg, sdesc = reference_sample(args.workload)
+            r = run_reference(sg, os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": sg.m / r["seconds"], "unit": UNIT, "cores": os.cpu_count(),
+                                    "kind": "reference", "sample": sdesc + f" ({sg.m} links, {r['seconds']:.2f} s, "
+                                    f"L={r['L_bits']:.5f} bits)"}
+        except Exception as e:  # the reference build is test infrastructure; report, do not fail
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                                    "sample": f"unavailable: {e}"}
+    if rank == 0:
+        print(json.dumps(line))
+    G.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def bench_reference(args, world):
+    sg, sdesc = reference_sample(args.workload)
+    threads = os.cpu_count() or 1
+    try:
+        for _ in range(args.warmup):
+            run_reference(sg, threads)
+        secs = []
+        for k in range(args.steps):
+            secs.append(run_reference(sg, threads, seed=1 + k)["seconds"])
+    except Exception as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference harness failed: {e}"}))
+        return
+    s = sum(secs) / len(secs)
+    v = sg.m / s
+    _, desc = (None, "")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": s * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, seed 42)",
+        "config": {"workload": sdesc, "nodes": sg.n, "links": sg.m, "solver": "threshold 1e-3, vThresh 0.0, "
+                   "maxIter 10, prior", "parallelism": f"{threads} host threads"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sdesc},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+if __name__ == "__main__":
+    main()

@@ -77,6 +77,9 @@ typedef struct {
     int64_t supersteps;
     int64_t power_iters;
     double total_ms;         /* last rmx_optimize, device time on the handle's stream */
+    int64_t kernel_launches; /* kernels this library launched (all handles) since it was loaded */
+    int64_t links_evaluated; /* unit links read by move evaluation since profiling was enabled */
+    int64_t units_evaluated; /* units evaluated since profiling was enabled */
 } rmx_profile;
 
 const char *rmx_last_error(void);

@@ -44,7 +44,8 @@ class KernelStat(C.Structure):
 
 class Profile(C.Structure):
     _fields_ = [("k", KernelStat * 6), ("sweeps", C.c_int64), ("supersteps", C.c_int64),
-                ("power_iters", C.c_int64), ("total_ms", C.c_double)]
+                ("power_iters", C.c_int64), ("total_ms", C.c_double), ("kernel_launches", C.c_int64),
+                ("links_evaluated", C.c_int64), ("units_evaluated", C.c_int64)]
 
 
 _L = None
@@ -207,7 +208,9 @@ class Graph:
         _check(lib().rmx_get_profile(self._h, C.byref(pr)))
         out = {name: dict(launches=pr.k[i].launches, ms=pr.k[i].ms, bytes=pr.k[i].bytes)
                for i, name in enumerate(KERNELS)}
-        out.update(sweeps=pr.sweeps, supersteps=pr.supersteps, power_iters=pr.power_iters, total_ms=pr.total_ms)
+        out.update(sweeps=pr.sweeps, supersteps=pr.supersteps, power_iters=pr.power_iters, total_ms=pr.total_ms,
+                   kernel_launches=pr.kernel_launches, links_evaluated=pr.links_evaluated,
+                   units_evaluated=pr.units_evaluated)
         return out
 
     def stream_ptr(self) -> int:

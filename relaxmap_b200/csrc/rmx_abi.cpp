@@ -249,8 +249,8 @@ rmx_status rmx_set_profiling(rmx_graph *g, int32_t on) {
         g->timers.on = on != 0;
         g->timers.reset();
         g->prof = rmx_profile{};
-        g->edges_evaluated = 0;
-        g->units_evaluated = 0;
+        RMX_CUDA(cudaMemsetAsync(g->work.counters + rmx::kCntEdges, 0, 3 * sizeof(int64_t), g->stream));
+        RMX_CUDA(cudaStreamSynchronize(g->stream));
     });
 }
 
@@ -266,12 +266,20 @@ rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out) {
             out->k[k].ms = g->timers.ms[k];
             out->k[k].bytes = 0.0;
         }
-        // compulsory traffic of the move evaluation: per link visit the
-        // neighbour id (4 B), its fixed-point flow (8 B) and the neighbour's
-        // module (4 B); per evaluated unit its list entry, offsets, attributes,
-        // module, own module statistics and the proposal written.
-        out->k[RMX_K_EVAL].bytes = 16.0 * (double)g->edges_evaluated + 108.0 * (double)g->units_evaluated;
+        int64_t c[3];
+        RMX_CUDA(cudaMemcpyAsync(c, g->work.counters + rmx::kCntEdges, sizeof c, cudaMemcpyDeviceToHost, g->stream));
+        RMX_CUDA(cudaStreamSynchronize(g->stream));
+        out->links_evaluated = c[0];
+        out->units_evaluated = c[1];
+        // Compulsory traffic of the move evaluation, each array touched once:
+        // per link read, the neighbour id (4 B), its fixed-point flow (8 B) and
+        // the neighbour's module (4 B); per unit, its list entry (4), CSR and
+        // CSC offsets (32), attributes (32), module (4), instance (4), its own
+        // module's statistics (32), proposal and change written (12); per
+        // candidate module, its statistics record (32).
+        out->k[RMX_K_EVAL].bytes = 16.0 * (double)c[0] + 120.0 * (double)c[1] + 32.0 * (double)c[2];
         out->power_iters = g->power_iters;
+        out->kernel_launches = (int64_t)__atomic_load_n(&rmx::g_kernel_launches, __ATOMIC_RELAXED);
     });
 }
 

@@ -72,8 +72,15 @@ inline void check(cudaError_t e, const char *what, const char *file, int line) {
         throw CudaError(e, buf);
     }
 }
+// Kernels launched by this library since load (every launch site goes through
+// RMX_LAUNCHED).
+extern unsigned long long g_kernel_launches;
+inline void launched(const char *file, int line) {
+    __atomic_fetch_add(&g_kernel_launches, 1ull, __ATOMIC_RELAXED);
+    check(cudaGetLastError(), "kernel launch", file, line);
+}
 #define RMX_CUDA(x) ::rmx::check((x), #x, __FILE__, __LINE__)
-#define RMX_LAUNCHED() ::rmx::check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+#define RMX_LAUNCHED() ::rmx::launched(__FILE__, __LINE__)
 
 inline unsigned blocks_for(int64_t n, int threads, int64_t cap = 1 << 20) {
     int64_t b = (n + threads - 1) / threads;

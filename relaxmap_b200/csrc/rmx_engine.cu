@@ -315,6 +315,11 @@ void Timers::destroy() {
 
 rmx_graph::~rmx_graph() {
     timers.destroy();
+    for (cudaStream_t a : work.aux)
+        if (a) cudaStreamDestroy(a);
+    if (work.fork) cudaEventDestroy(work.fork);
+    for (cudaEvent_t e : work.join)
+        if (e) cudaEventDestroy(e);
     if (work.gtable) cudaFree(work.gtable);
     if (work.gkeys) cudaFree(work.gkeys);
     perm.destroy();
@@ -463,6 +468,9 @@ void rmx_graph::alloc_engine() {
     RMX_CUDA(cudaMemsetAsync(work.claim, 0, sizeof(unsigned long long) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.next_active, 0, n, stream));
     RMX_CUDA(cudaMemsetAsync(work.counters, 0, sizeof(int64_t) * kCntSlots, stream));
+    for (cudaStream_t &a : work.aux) RMX_CUDA(cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking));
+    RMX_CUDA(cudaEventCreateWithFlags(&work.fork, cudaEventDisableTiming));
+    for (cudaEvent_t &e : work.join) RMX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 }
 
 int64_t rmx_graph::max_degree(const Level &lv) {
@@ -487,9 +495,9 @@ void rmx_graph::ensure_hub_table(int64_t maxdeg) {
     work.gtable = nullptr;
     work.gkeys = nullptr;
     work.gcap = 0;
-    const int hb = hub_blocks();
-    RMX_CUDA(cudaMalloc(&work.gtable, sizeof(fx_t) * 2 * cap * hb));
-    RMX_CUDA(cudaMalloc(&work.gkeys, sizeof(int32_t) * cap * hb));
+    const int64_t hb = hub_blocks(), slots = hub_slots(cap);
+    RMX_CUDA(cudaMalloc(&work.gtable, sizeof(fx_t) * 2 * slots * hb));
+    RMX_CUDA(cudaMalloc(&work.gkeys, sizeof(int32_t) * slots * hb));
     work.gcap = cap;
 }
 
@@ -523,7 +531,8 @@ double rmx_graph::sweep_single(Level &lv, bool prior, bool allow_new, double vth
     bucket_units(lv, work, n_active, seed, nsub, scratch, stream);
     SweepArgs sa{vthresh, allow_new ? 1 : 0};
     Timers *tm = timers.on ? &timers : nullptr;
-    for (int sb = 0; sb < nsub; sb++) sweep_subbatch(lv, mods, inst1, work, sa, sb, ++stamp, prior, stream, tm);
+    for (int sb = 0; sb < nsub; sb++)
+        sweep_subbatch(lv, mods, inst1, work, sa, sb, ++stamp, mix_seed(seed, sb), prior, stream, tm);
     timers.begin(kTimerCodelen, stream);
     instance_codelength(mods, inst1, stream);
     timers.end(kTimerCodelen, stream);
@@ -535,11 +544,11 @@ double rmx_graph::sweep_single(Level &lv, bool prior, bool allow_new, double vth
     RMX_CUDA(cudaMemcpyAsync(&hL.L, inst1.L, sizeof(double), cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaMemcpyAsync(cnt, work.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaStreamSynchronize(stream));
-    units_evaluated += n_active;
-    edges_evaluated = cnt[kCntEdges];
     prof.sweeps++;
     if (prior) n_active = cnt[kCntActive];
-    if (opt.verbose >= 2) printf("  sweep: code length = %g, moved %lld\n", hL.L / kLn2, (long long)cnt[kCntMoved]);
+    if (opt.verbose >= 2)
+        printf("  sweep: n=%d active=%lld code length = %.17g, moved %lld\n", lv.n, (long long)n_active, hL.L / kLn2,
+               (long long)cnt[kCntMoved]);
     return hL.L;
 }
 
@@ -651,7 +660,7 @@ void rmx_graph::generate_sub_modules() {
             const uint32_t seed = mix_seed(run_seed, ++sweep_no);
             bucket_units(sub_lv, work, N, seed, nsub, scratch, stream);
             for (int sb = 0; sb < nsub; sb++)
-                sweep_subbatch(sub_lv, submods, instsub, work, sa, sb, ++stamp, false, stream, tm);
+                sweep_subbatch(sub_lv, submods, instsub, work, sa, sb, ++stamp, mix_seed(seed, sb), false, stream, tm);
             timers.begin(kTimerCodelen, stream);
             instance_codelength(submods, instsub, stream);
             unsigned long long *na = reinterpret_cast<unsigned long long *>(dtmp + 9);
@@ -730,8 +739,10 @@ int32_t rmx_graph::count_modules() {
 // main's superstep loop (OmpRelaxmap.cpp:181-219).
 double rmx_graph::run_attempt(uint32_t seed) {
     run_seed = seed;
+    sweep_no = 0;  // every random choice derives from (seed, sweep, sub-batch)
     init_singletons(node_lv, mods, stream);
     RMX_CUDA(cudaMemsetAsync(inst1.active, 1, 1, stream));
+    instance_codelength(mods, inst1, stream);  // sum of exits of the singleton state
     double L = L0;
     step_bits.clear();
     superstep = 1;

@@ -110,7 +110,7 @@ struct Timers {
 };
 
 // Counter slots in SweepWork::counters (device int64).
-enum { kCntActive = 0, kCntFree = 1, kCntMoved = 3, kCntEdges = 4, kCntUnits = 5, kCntSlots = 8 };
+enum { kCntActive = 0, kCntFree = 1, kCntMoved = 3, kCntEdges = 4, kCntUnits = 5, kCntCands = 6, kCntSlots = 8 };
 
 // Per-level sweep workspace (sized for the largest level: N units, N modules).
 struct SweepWork {
@@ -127,21 +127,27 @@ struct SweepWork {
     int32_t *free_list = nullptr;
     unsigned long long *claim = nullptr;        // per module id
     int64_t *counters = nullptr;
-    fx_t *gtable = nullptr;                     // hub hash tables: hub_blocks() slices
-    int32_t *gkeys = nullptr;
+    fx_t *gtable = nullptr;                     // hub hash tables: hub_blocks() slices of
+    int32_t *gkeys = nullptr;                   //   hub_slots(gcap) entries (table + candidates)
     int64_t gcap = 0;
+    cudaStream_t aux[2] = {nullptr, nullptr};   // concurrent degree bins
+    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
 };
 
 void configure_eval_kernels();
 int hub_blocks();
 int64_t warp_bin_max_degree();
 int64_t block_bin_max_degree();
+int64_t hub_slots(int64_t cap);
 void all_units(int32_t n, SweepWork &W, cudaStream_t s);
 void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed, int nsub, Arena &ar, cudaStream_t s);
 void free_modules(const ModState &M, SweepWork &W, Arena &ar, cudaStream_t s);
 // Evaluate, claim, commit and apply link deltas for sub-batch sb.
+// stamp: unique per sub-batch over the handle's life (marks this sub-batch's
+// movers); hseed: a function of (attempt seed, sweep, sub-batch) only, so runs
+// with the same seed make the same choices.
 void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &W, const SweepArgs &a, int sb,
-                    uint32_t stamp, bool mark_active, cudaStream_t s, Timers *tm);
+                    uint32_t stamp, uint32_t hseed, bool mark_active, cudaStream_t s, Timers *tm);
 // Move evaluation only, for the parity hook (no commit).
 void evaluate_all(const Level &L, const ModState &M, const InstState &I, SweepWork &W, const uint8_t *allow_new,
                   double vthresh, Arena &ar, cudaStream_t s);

@@ -314,6 +314,7 @@ static int launch_power(int32_t n, const int64_t *in_off, const int32_t *in_src,
     void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w, (void *)&tw, (void *)&dangling, (void *)&n,
                     (void *)&p, (void *)&y, (void *)&parts, (void *)&iters};
     RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));
+    RMX_LAUNCHED();
     int h = 0;
     RMX_CUDA(cudaMemcpyAsync(&h, iters, sizeof(int), cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));

@@ -45,7 +45,6 @@ struct rmx_graph {
     uint64_t sweep_no = 0;
     std::vector<double> step_bits;
     rmx_profile prof{};
-    int64_t edges_evaluated = 0, units_evaluated = 0;
 
     // current run settings
     rmx_opts opt{};

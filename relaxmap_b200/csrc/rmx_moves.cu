@@ -58,40 +58,36 @@ __device__ __forceinline__ bool better(double d1, int32_t m1, double d2, int32_t
     return d1 < d2 || (d1 == d2 && m1 < m2);
 }
 
-// Everything about the moving unit that every candidate needs.
+// Everything about the moving unit that every candidate needs. The terms of
+// the code-length change that depend only on the unit and its old module
+// (Module.cpp:1109-1112: sumAllExitPr, exit and stay of the old module before
+// and after) are folded into K once per unit.
 struct UnitCtx {
-    double pu, tu, du, eu, cu;  // flow, teleport weight, dangling flow, exit, tau*p + (1-tau)*d
-    double eA, PA, nexA, nPA;   // old module: exit, flow, exit and flow after leaving
+    double pu, tu, eu, cu;  // flow, teleport weight, exit, tau*p + (1-tau)*d
+    double eA, nexA;        // old module exit before / after the unit leaves
     double sum_exit;
+    double K;               // -plogp(se) - 2 (plogp(nexA) - plogp(eA)) + plogp(nexA + nPA) - plogp(eA + PA)
     int32_t A;
 };
 
-__device__ __forceinline__ double delta_L(double se, double nse, double e1, double P1, double e2, double P2,
-                                          double ne1, double nP1, double ne2, double nP2) {
-    // Module.cpp:1109-1115
-    double d_all = plogp(nse) - plogp(se);
-    double d_exit = plogp(ne1) + plogp(ne2) - plogp(e1) - plogp(e2);
-    double d_stay = plogp(ne1 + nP1) + plogp(ne2 + nP2) - plogp(e1 + P1) - plogp(e2 + P2);
-    return d_all - 2.0 * d_exit + d_stay;
-}
-
 // Change of moving the unit into module with statistics st, given the unit's
-// aggregated out-/in-flow (fixed point, before the 1-tau factor) to it.
+// aggregated out-/in-flow (fixed point, before the 1-tau factor) to it:
+// d_all - 2 d_exit + d_stay of Module.cpp:1109-1115 with the unit terms in K.
 __device__ __forceinline__ double candidate_delta(const UnitCtx &c, const Stat4 &st, fx_t ofx, fx_t ifx) {
     const double P = from_fx(st.P), TW = from_fx(st.TW), D = from_fx(st.D), OUT = from_fx(st.OUT);
     const double em = exit_flow(P, TW, D, OUT);
-    const double om = kBeta * from_fx(ofx) + c.cu * TW;                   // Module.cpp:1058
+    const double om = kBeta * from_fx(ofx) + c.cu * TW;                        // Module.cpp:1058
     const double im = kBeta * from_fx(ifx) + (kAlpha * P + kBeta * D) * c.tu;  // Module.cpp:1059
-    const double nexm = em + c.eu - om - im;                              // Module.cpp:1104
-    const double nse = c.sum_exit + c.nexA + nexm - c.eA - em;           // Module.cpp:1106
-    return delta_L(c.sum_exit, nse, c.eA, c.PA, em, P, c.nexA, c.nPA, nexm, P + c.pu);
+    const double nexm = em + c.eu - om - im;                                   // Module.cpp:1104
+    const double nse = c.sum_exit + c.nexA + nexm - c.eA - em;                 // Module.cpp:1106
+    return plogp(nse) + c.K - 2.0 * (plogp(nexm) - plogp(em)) + (plogp(nexm + P + c.pu) - plogp(em + P));
 }
 
 // The empty-module option: exit e_u, no shared flow (Module.cpp:1072-1077).
 __device__ __forceinline__ double newmod_delta(const UnitCtx &c) {
     const double nexm = c.eu;
     const double nse = c.sum_exit + c.nexA + nexm - c.eA;
-    return delta_L(c.sum_exit, nse, c.eA, c.PA, 0.0, 0.0, c.nexA, c.nPA, nexm, c.pu);
+    return plogp(nse) + c.K - 2.0 * plogp(nexm) + plogp(nexm + c.pu);
 }
 
 __device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, double sum_exit, int32_t A, fx_t oA,
@@ -99,17 +95,16 @@ __device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, do
     UnitCtx c;
     c.pu = from_fx(ua.P);
     c.tu = from_fx(ua.TW);
-    c.du = from_fx(ua.D);
-    c.eu = exit_flow(c.pu, c.tu, c.du, from_fx(ua.OUT));
-    c.cu = kAlpha * c.pu + kBeta * c.du;
-    c.PA = from_fx(ma.P);
-    const double TWA = from_fx(ma.TW), DA = from_fx(ma.D);
-    c.eA = exit_flow(c.PA, TWA, DA, from_fx(ma.OUT));
-    const double outA = kBeta * from_fx(oA) + c.cu * (TWA - c.tu);                            // :1047
-    const double inA = kBeta * from_fx(iA) + (kAlpha * (c.PA - c.pu) + kBeta * (DA - c.du)) * c.tu;  // :1048
-    c.nexA = c.eA - c.eu + outA + inA;                                                         // :1084
-    c.nPA = c.PA - c.pu;
+    const double du = from_fx(ua.D);
+    c.eu = exit_flow(c.pu, c.tu, du, from_fx(ua.OUT));
+    c.cu = kAlpha * c.pu + kBeta * du;
+    const double PA = from_fx(ma.P), TWA = from_fx(ma.TW), DA = from_fx(ma.D);
+    c.eA = exit_flow(PA, TWA, DA, from_fx(ma.OUT));
+    const double outA = kBeta * from_fx(oA) + c.cu * (TWA - c.tu);                             // :1047
+    const double inA = kBeta * from_fx(iA) + (kAlpha * (PA - c.pu) + kBeta * (DA - du)) * c.tu;  // :1048
+    c.nexA = c.eA - c.eu + outA + inA;                                                          // :1084
     c.sum_exit = sum_exit;
+    c.K = -plogp(sum_exit) - 2.0 * (plogp(c.nexA) - plogp(c.eA)) + (plogp(c.nexA + (PA - c.pu)) - plogp(c.eA + PA));
     c.A = A;
     return c;
 }
@@ -131,7 +126,7 @@ struct EvalArgs {
     const int64_t *range;  // [beg, end) at range[0], range[1]
     int32_t *prop;
     double *pdelta;
-    unsigned long long *edges_seen;
+    unsigned long long *stats;  // [0] links read [1] units evaluated [2] candidates evaluated
     double vthresh;
     int allow_new;             // stage-level switch
     const uint8_t *allow_new_unit;  // optional per-unit override (parity hook)
@@ -163,219 +158,231 @@ __device__ __forceinline__ void finish_unit(const EvalArgs &a, int32_t u, const 
     a.pdelta[u] = best;
 }
 
-// ---------------------------------------------------------------- warp kernel
-// One warp per unit with out+in degree <= 64: table of up to 128 slots in
-// shared memory per warp.
+// ---------------------------------------------------------------- evaluation
+// Degree bins (out+in degree d of the unit at this level):
+//   warp   d <= 128   one warp per unit, table of <= 256 slots per warp in
+//                     shared memory, candidates compacted in place
+//   block  d <= 1024  128 threads per unit, table of <= 2048 slots plus the
+//                     candidate list in shared memory
+//   hub    d > 1024   512 threads per unit, table + candidate list in a
+//                     per-block slice of a global table
+// Each unit: clear the table, insert every link's neighbour module with its
+// fixed-point flow (integer atomics, so the sums do not depend on the order),
+// look up the own module, compact the other occupied slots into a dense
+// candidate list, and evaluate the candidates with all lanes.
 
-constexpr int kWarpCap = 128, kWarpMaxDeg = 64, kEvalWarps = 8;
+constexpr int kWarpMaxDeg = 128, kWarpCap = 256, kEvalWarps = 8;
 constexpr int kBins = 3;  // degree bins: warp, block (shared table), hub (global table)
+constexpr int kBlkT = 128, kBlkMaxDeg = 1024, kBlkCap = 2048, kBlkSlots = kBlkCap + kBlkCap / 2;
+constexpr int kHubT = 512;
 
-__global__ void __launch_bounds__(kEvalWarps * 32) k_eval_warp(EvalArgs a) {
+__device__ __forceinline__ int tab_find(const int32_t *keys, int mask, int32_t key) {
+    int s = tab_slot(key, mask);
+    for (int probe = 0; probe <= mask; probe++) {
+        const int32_t k = keys[s];
+        if (k == key) return s;
+        if (k == kEmpty) return -1;
+        s = (s + 1) & mask;
+    }
+    return -1;
+}
+
+template <int NT>
+__device__ __forceinline__ void gsync() {
+    if (NT == 32)
+        __syncwarp();
+    else
+        __syncthreads();
+}
+
+template <int NT>
+struct GroupShared {  // reductions across the warps of a block group
+    double best[NT / 32];
+    int32_t mod[NT / 32];
+    int ncand;
+};
+
+// One unit evaluated by a group of NT threads (a warp or a block); r = rank.
+// For the warp group the candidate list overwrites the table (ck == keys).
+template <int NT>
+__device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, const int r, int32_t *keys, fx_t *vo,
+                                          fx_t *vi, int32_t *ck, fx_t *co, fx_t *ci, GroupShared<NT> *sh,
+                                          unsigned long long &seen, unsigned long long &cands) {
+    const int lane = r & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t ob = a.out_off[u], ib = a.in_off[u];
+    const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
+    int64_t cap = 32;
+    while (cap < 2 * d) cap <<= 1;
+    const int mask = (int)(cap - 1);
+    for (int64_t s = r; s < cap; s += NT) {
+        keys[s] = kEmpty;
+        vo[s] = 0;
+        vi[s] = 0;
+    }
+    gsync<NT>();
+    for (int64_t j = r; j < d; j += NT) {
+        const bool isout = j < dout;
+        const int64_t e = isout ? ob + j : ib + (j - dout);
+        const int32_t nb = isout ? a.out_dst[e] : a.in_src[e];
+        const fx_t q = isout ? a.out_fx[e] : a.in_fx[e];
+        const int s = tab_insert(keys, mask, a.mod[nb]);
+        atomic_add_fx(isout ? vo + s : vi + s, q);
+    }
+    gsync<NT>();
+    const int32_t A = a.mod[u];
+    const int sA = tab_find(keys, mask, A);
+    const fx_t oA = sA >= 0 ? vo[sA] : 0, iA = sA >= 0 ? vi[sA] : 0;
+    const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
+    int nc = 0;
+    if (NT == 32) {
+        for (int64_t base = 0; base < cap; base += 32) {
+            const int64_t s = base + lane;
+            const int32_t k = keys[s];
+            const fx_t o = vo[s], i2 = vi[s];
+            const bool occ = k != kEmpty && k != A;
+            const unsigned bal = __ballot_sync(kFull, occ);
+            __syncwarp();
+            if (occ) {
+                const int p = nc + __popc(bal & lt);
+                ck[p] = k;
+                co[p] = o;
+                ci[p] = i2;
+            }
+            nc += __popc(bal);
+        }
+        __syncwarp();
+    } else {
+        if (r == 0) sh->ncand = 0;
+        __syncthreads();
+        for (int64_t base = r & ~31; base < cap; base += NT) {
+            const int64_t s = base + lane;
+            int32_t k = kEmpty;
+            fx_t o = 0, i2 = 0;
+            if (s < cap) {
+                k = keys[s];
+                o = vo[s];
+                i2 = vi[s];
+            }
+            const bool occ = k != kEmpty && k != A;
+            const unsigned bal = __ballot_sync(kFull, occ);
+            int p0 = 0;
+            if (lane == 0 && bal) p0 = atomicAdd(&sh->ncand, __popc(bal));
+            p0 = __shfl_sync(kFull, p0, 0);
+            if (occ) {
+                const int p = p0 + __popc(bal & lt);
+                ck[p] = k;
+                co[p] = o;
+                ci[p] = i2;
+            }
+        }
+        __syncthreads();
+        nc = sh->ncand;
+    }
+    double best = 0.0;
+    int32_t bm = INT_MAX;
+    for (int q = r; q < nc; q += NT) {
+        const int32_t m = ck[q];
+        const double dl = candidate_delta(c, a.mstat[m], co[q], ci[q]);
+        if (better(dl, m, best, bm)) {
+            best = dl;
+            bm = m;
+        }
+    }
+    // lanes without a candidate hold (0, INT_MAX), which no real candidate loses to
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob2 = __shfl_xor_sync(kFull, best, o);
+        const int32_t om = __shfl_xor_sync(kFull, bm, o);
+        if (better(ob2, om, best, bm)) {
+            best = ob2;
+            bm = om;
+        }
+    }
+    if (NT > 32) {
+        if (lane == 0) {
+            sh->best[r >> 5] = best;
+            sh->mod[r >> 5] = bm;
+        }
+        __syncthreads();
+        if (r == 0)
+            for (int q = 1; q < NT / 32; q++)
+                if (better(sh->best[q], sh->mod[q], best, bm)) {
+                    best = sh->best[q];
+                    bm = sh->mod[q];
+                }
+    }
+    if (r == 0) {
+        finish_unit(a, u, c, best, bm);
+        seen += d;
+        cands += nc;
+    }
+    gsync<NT>();
+}
+
+__device__ __forceinline__ void flush_stats(const EvalArgs &a, unsigned long long seen, unsigned long long units,
+                                            unsigned long long cands) {
+    if (units) {
+        atomicAdd(a.stats + 0, seen);
+        atomicAdd(a.stats + 1, units);
+        atomicAdd(a.stats + 2, cands);
+    }
+}
+
+__global__ void __launch_bounds__(kEvalWarps * 32, 3) k_eval_warp(EvalArgs a) {
     __shared__ int32_t skey[kEvalWarps][kWarpCap];
     __shared__ fx_t sout[kEvalWarps][kWarpCap];
     __shared__ fx_t sin_[kEvalWarps][kWarpCap];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    int32_t *keys = skey[w];
-    fx_t *vo = sout[w], *vi = sin_[w];
     const int64_t beg = a.range[0], end = a.range[1];
-    const int64_t gw = ((int64_t)blockIdx.x * kEvalWarps + w), nw = (int64_t)gridDim.x * kEvalWarps;
-    unsigned long long seen = 0;
+    const int64_t gw = (int64_t)blockIdx.x * kEvalWarps + w, nw = (int64_t)gridDim.x * kEvalWarps;
+    unsigned long long seen = 0, units = 0, cands = 0;
     for (int64_t i = beg + gw; i < end; i += nw) {
         const int32_t u = a.list[i];
         if (!a.inst_active[a.uinst[u]]) {
             if (lane == 0) a.prop[u] = -1;
             continue;
         }
-        const int64_t ob = a.out_off[u], ib = a.in_off[u];
-        const int dout = (int)(a.out_off[u + 1] - ob), din = (int)(a.in_off[u + 1] - ib), d = dout + din;
-        int cap = 32;
-        while (cap < 2 * d) cap <<= 1;
-        const int mask = cap - 1;
-        for (int s = lane; s < cap; s += 32) {
-            keys[s] = kEmpty;
-            vo[s] = 0;
-            vi[s] = 0;
-        }
-        __syncwarp();
-        for (int j = lane; j < d; j += 32) {
-            int32_t nb;
-            fx_t q;
-            bool isout = j < dout;
-            if (isout) {
-                nb = a.out_dst[ob + j];
-                q = a.out_fx[ob + j];
-            } else {
-                nb = a.in_src[ib + j - dout];
-                q = a.in_fx[ib + j - dout];
-            }
-            const int s = tab_insert(keys, mask, a.mod[nb]);
-            atomic_add_fx(isout ? vo + s : vi + s, q);
-        }
-        seen += d;
-        __syncwarp();
-        const int32_t A = a.mod[u];
-        // flows to the unit's own module
-        fx_t oA = 0, iA = 0;
-        for (int s = lane; s < cap; s += 32)
-            if (keys[s] == A) {
-                oA = vo[s];
-                iA = vi[s];
-            }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            oA += __shfl_xor_sync(kFull, oA, o);
-            iA += __shfl_xor_sync(kFull, iA, o);
-        }
-        const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
-        double best = 0.0;
-        int32_t bm = INT_MAX;
-        for (int s = lane; s < cap; s += 32) {
-            const int32_t m = keys[s];
-            if (m == kEmpty || m == A) continue;
-            const double dl = candidate_delta(c, a.mstat[m], vo[s], vi[s]);
-            if (better(dl, m, best, bm)) {
-                best = dl;
-                bm = m;
-            }
-        }
-        // lanes that saw no candidate hold (0, INT_MAX): never better than a real one
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob2 = __shfl_xor_sync(kFull, best, o);
-            const int32_t om = __shfl_xor_sync(kFull, bm, o);
-            if (better(ob2, om, best, bm)) {
-                best = ob2;
-                bm = om;
-            }
-        }
-        if (lane == 0) finish_unit(a, u, c, best, bm);
-        __syncwarp();
+        eval_unit<32>(a, u, lane, skey[w], sout[w], sin_[w], skey[w], sout[w], sin_[w], nullptr, seen, cands);
+        units++;
     }
-    if (lane == 0 && seen) atomicAdd(a.edges_seen, seen);
+    if (lane == 0) flush_stats(a, seen, units, cands);
 }
 
-// ---------------------------------------------------------------- block kernel
-// One block per unit; the table lives in shared memory (CAP slots) or, for
-// hubs, in a per-block slice of a global table.
-
 template <int NT, bool GLOBAL>
-__global__ void __launch_bounds__(NT) k_eval_block(EvalArgs a, int cap_smem) {
+__global__ void __launch_bounds__(NT, GLOBAL ? 1 : 3) k_eval_block(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
-    __shared__ double rbest[NT / 32];
-    __shared__ int32_t rmod[NT / 32];
-    __shared__ fx_t rA[2][NT / 32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __shared__ GroupShared<NT> sh;
     int32_t *keys;
     fx_t *vo, *vi;
-    int64_t capmax;
+    int64_t slots;
     if (GLOBAL) {
-        capmax = a.gcap;
-        keys = a.gkeys + (int64_t)blockIdx.x * capmax;
-        vo = a.gtable + (int64_t)blockIdx.x * capmax * 2;
-        vi = vo + capmax;
+        slots = a.gcap + a.gcap / 2;
+        keys = a.gkeys + (int64_t)blockIdx.x * slots;
+        vo = a.gtable + (int64_t)blockIdx.x * slots * 2;
+        vi = vo + slots;
     } else {
-        capmax = cap_smem;
+        slots = kBlkSlots;
         vo = reinterpret_cast<fx_t *>(dsm);
-        vi = vo + cap_smem;
-        keys = reinterpret_cast<int32_t *>(vi + cap_smem);
+        vi = vo + kBlkSlots;
+        keys = reinterpret_cast<int32_t *>(vi + kBlkSlots);
     }
     const int64_t beg = a.range[0], end = a.range[1];
-    unsigned long long seen = 0;
+    unsigned long long seen = 0, units = 0, cands = 0;
     for (int64_t i = beg + blockIdx.x; i < end; i += gridDim.x) {
         const int32_t u = a.list[i];
         if (!a.inst_active[a.uinst[u]]) {
             if (threadIdx.x == 0) a.prop[u] = -1;
             continue;
         }
-        const int64_t ob = a.out_off[u], ib = a.in_off[u];
-        const int64_t dout = a.out_off[u + 1] - ob, din = a.in_off[u + 1] - ib, d = dout + din;
-        int64_t cap = 64;
+        // the candidate list follows the table: cap + cap/2 <= slots
+        const int64_t d = (a.out_off[u + 1] - a.out_off[u]) + (a.in_off[u + 1] - a.in_off[u]);
+        int64_t cap = 32;
         while (cap < 2 * d) cap <<= 1;
-        if (cap > capmax) cap = capmax;  // never for correctly binned units
-        const int mask = (int)(cap - 1);
-        for (int64_t s = threadIdx.x; s < cap; s += NT) {
-            keys[s] = kEmpty;
-            vo[s] = 0;
-            vi[s] = 0;
-        }
-        __syncthreads();
-        for (int64_t j = threadIdx.x; j < d; j += NT) {
-            int32_t nb;
-            fx_t q;
-            bool isout = j < dout;
-            if (isout) {
-                nb = a.out_dst[ob + j];
-                q = a.out_fx[ob + j];
-            } else {
-                nb = a.in_src[ib + j - dout];
-                q = a.in_fx[ib + j - dout];
-            }
-            const int s = tab_insert(keys, mask, a.mod[nb]);
-            if (s >= 0) atomic_add_fx(isout ? vo + s : vi + s, q);
-        }
-        seen += d;
-        __syncthreads();
-        const int32_t A = a.mod[u];
-        fx_t oA = 0, iA = 0;
-        for (int64_t s = threadIdx.x; s < cap; s += NT)
-            if (keys[s] == A) {
-                oA = vo[s];
-                iA = vi[s];
-            }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            oA += __shfl_xor_sync(kFull, oA, o);
-            iA += __shfl_xor_sync(kFull, iA, o);
-        }
-        if (lane == 0) {
-            rA[0][w] = oA;
-            rA[1][w] = iA;
-        }
-        __syncthreads();
-        oA = 0;
-        iA = 0;
-#pragma unroll
-        for (int q = 0; q < NT / 32; q++) {
-            oA += rA[0][q];
-            iA += rA[1][q];
-        }
-        const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
-        double best = 0.0;
-        int32_t bm = INT_MAX;
-        for (int64_t s = threadIdx.x; s < cap; s += NT) {
-            const int32_t m = keys[s];
-            if (m == kEmpty || m == A) continue;
-            const double dl = candidate_delta(c, a.mstat[m], vo[s], vi[s]);
-            if (better(dl, m, best, bm)) {
-                best = dl;
-                bm = m;
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob2 = __shfl_xor_sync(kFull, best, o);
-            const int32_t om = __shfl_xor_sync(kFull, bm, o);
-            if (better(ob2, om, best, bm)) {
-                best = ob2;
-                bm = om;
-            }
-        }
-        if (lane == 0) {
-            rbest[w] = best;
-            rmod[w] = bm;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int q = 1; q < NT / 32; q++)
-                if (better(rbest[q], rmod[q], best, bm)) {
-                    best = rbest[q];
-                    bm = rmod[q];
-                }
-            finish_unit(a, u, c, best, bm);
-        }
-        __syncthreads();
+        eval_unit<NT>(a, u, threadIdx.x, keys, vo, vi, keys + cap, vo + cap, vi + cap, &sh, seen, cands);
+        units++;
     }
-    if (threadIdx.x == 0 && seen) atomicAdd(a.edges_seen, seen);
+    if (threadIdx.x == 0) flush_stats(a, seen, units, cands);
 }
 
 // ---------------------------------------------------------------- commit
@@ -396,6 +403,7 @@ struct CommitArgs {
     const int64_t *n_free;
     unsigned long long *moved_nodes;
     uint32_t stamp;
+    uint32_t hseed;  // per (attempt seed, sweep, sub-batch): picks the free id a unit bids for
 };
 
 __device__ __forceinline__ unsigned long long claim_key(uint32_t stamp, int32_t u) {
@@ -413,7 +421,7 @@ __global__ void k_claim(CommitArgs a) {
         if (a.prop[u] != kNewMod) continue;
         int32_t m = -1;
         if (nf > 0) {
-            int64_t s = mix32((uint32_t)u ^ (a.stamp * 0x9e3779b9U)) % nf;
+            int64_t s = mix32((uint32_t)u ^ a.hseed) % nf;
             for (int probe = 0; probe < 8; probe++, s = (s + 1) % nf) {
                 const int32_t cand = a.free_list[s];
                 if (a.mcount[cand] == 0) {
@@ -476,8 +484,12 @@ struct DeltaArgs {
 };
 
 // Out-flow bookkeeping for the movers of this sub-batch; warp per unit.
-// Link u->w adds its flow to OUT[mod(u)] iff mod(u) != mod(w). Links whose
-// both ends moved are handled once, by the source's out-link loop.
+// Link u->w adds its flow to OUT[mod(u)] iff mod(u) != mod(w). When u moves
+// A -> T only OUT[A] and OUT[T] change: out-links leave A's count if they
+// crossed and join T's if they now cross; in-links from A become crossing
+// (OUT[A] grows) and in-links from T stop crossing (OUT[T] shrinks). Links whose
+// two ends both moved are handled once, by the source's out-link loop. The
+// warp sums its lanes' changes, so each mover costs two atomics.
 __global__ void __launch_bounds__(256) k_delta(DeltaArgs a) {
     const int lane = threadIdx.x & 31;
     const int64_t beg = a.range[0], end = a.range[1];
@@ -488,14 +500,15 @@ __global__ void __launch_bounds__(256) k_delta(DeltaArgs a) {
         const bool moved = a.stamp_of[u] == a.stamp;
         if (!moved && !a.mark) continue;
         const int32_t A = moved ? a.prevmod[u] : a.mod[u], T = a.mod[u];
+        fx_t dA = 0, dT = 0;
         for (int64_t e = a.out_off[u] + lane; e < a.out_off[u + 1]; e += 32) {
             const int32_t w = a.out_dst[e];
             if (moved) {
                 const fx_t q = a.out_fx[e];
                 const bool wm = a.stamp_of[w] == a.stamp;
                 const int32_t bn = a.mod[w], bo = wm ? a.prevmod[w] : bn;
-                if (A != bo) atomic_add_fx(&a.mstat[A].OUT, -q);
-                if (T != bn) atomic_add_fx(&a.mstat[T].OUT, q);
+                if (A != bo) dA -= q;
+                if (T != bn) dT += q;
             }
             if (a.mark) a.next_active[w] = 1;
         }
@@ -504,11 +517,22 @@ __global__ void __launch_bounds__(256) k_delta(DeltaArgs a) {
             if (moved && a.stamp_of[w] != a.stamp) {
                 const int32_t b = a.mod[w];
                 if (b == A)
-                    atomic_add_fx(&a.mstat[A].OUT, a.in_fx[e]);
+                    dA += a.in_fx[e];
                 else if (b == T)
-                    atomic_add_fx(&a.mstat[T].OUT, -a.in_fx[e]);
+                    dT -= a.in_fx[e];
             }
             if (a.mark) a.next_active[w] = 1;
+        }
+        if (moved) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                dA += __shfl_xor_sync(kFull, dA, o);
+                dT += __shfl_xor_sync(kFull, dT, o);
+            }
+            if (lane == 0) {
+                if (dA) atomic_add_fx(&a.mstat[A].OUT, dA);
+                if (dT) atomic_add_fx(&a.mstat[T].OUT, dT);
+            }
         }
     }
 }
@@ -673,7 +697,7 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     a.range = nullptr;
     a.prop = W.prop;
     a.pdelta = W.pdelta;
-    a.edges_seen = reinterpret_cast<unsigned long long *>(W.counters + kCntEdges);
+    a.stats = reinterpret_cast<unsigned long long *>(W.counters + kCntEdges);
     a.vthresh = vthresh;
     a.allow_new = allow_new;
     a.allow_new_unit = allow_unit;
@@ -684,31 +708,39 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     return a;
 }
 
-constexpr int kBlkT = 256, kBlkCap = 4096, kHubT = 512;
-
 int hub_blocks() { return std::min(num_sms(), 64); }
-int64_t block_bin_max_degree() { return kBlkCap / 2; }
+int64_t block_bin_max_degree() { return kBlkMaxDeg; }
 int64_t warp_bin_max_degree() { return kWarpMaxDeg; }
+int64_t hub_slots(int64_t cap) { return cap + cap / 2; }
 
-static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket, cudaStream_t s) {
-    a.range = bucket_off + first_bucket + 0;  // bin 0: warp per unit
-    k_eval_warp<<<num_sms() * 8, kEvalWarps * 32, 0, s>>>(a);
+// The three bins of a sub-batch run concurrently: the block and hub kernels
+// on two auxiliary streams forked from and joined back into s.
+static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket, const SweepWork &W, cudaStream_t s) {
+    RMX_CUDA(cudaEventRecord(W.fork, s));
+    RMX_CUDA(cudaStreamWaitEvent(W.aux[0], W.fork, 0));
+    RMX_CUDA(cudaStreamWaitEvent(W.aux[1], W.fork, 0));
+    a.range = bucket_off + first_bucket + 1;
+    k_eval_block<kBlkT, false><<<num_sms() * 3, kBlkT, (size_t)kBlkSlots * (2 * sizeof(fx_t) + sizeof(int32_t)),
+                                 W.aux[0]>>>(a);
     RMX_LAUNCHED();
-    a.range = bucket_off + first_bucket + 1;  // bin 1: block per unit, shared-memory table
-    const size_t smem = (size_t)kBlkCap * (2 * sizeof(fx_t) + sizeof(int32_t));
-    k_eval_block<kBlkT, false><<<num_sms() * 2, kBlkT, smem, s>>>(a, kBlkCap);
-    RMX_LAUNCHED();
-    if (a.gcap > 0) {  // bin 2: hubs, per-block slice of a global table
+    if (a.gcap > 0) {
         a.range = bucket_off + first_bucket + 2;
-        k_eval_block<kHubT, true><<<hub_blocks(), kHubT, 0, s>>>(a, 0);
+        k_eval_block<kHubT, true><<<hub_blocks(), kHubT, 0, W.aux[1]>>>(a);
         RMX_LAUNCHED();
     }
+    a.range = bucket_off + first_bucket + 0;
+    k_eval_warp<<<num_sms() * 3, kEvalWarps * 32, 0, s>>>(a);
+    RMX_LAUNCHED();
+    RMX_CUDA(cudaEventRecord(W.join[0], W.aux[0]));
+    RMX_CUDA(cudaEventRecord(W.join[1], W.aux[1]));
+    RMX_CUDA(cudaStreamWaitEvent(s, W.join[0], 0));
+    RMX_CUDA(cudaStreamWaitEvent(s, W.join[1], 0));
 }
 
 void configure_eval_kernels() {
     static bool done = false;
     if (done) return;
-    const size_t smem = (size_t)kBlkCap * (2 * sizeof(fx_t) + sizeof(int32_t));
+    const size_t smem = (size_t)kBlkSlots * (2 * sizeof(fx_t) + sizeof(int32_t));
     RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     done = true;
 }
@@ -730,7 +762,7 @@ __global__ void k_bucket(const int32_t *list, const int64_t *n_active, const int
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t u = list[i];
         const int64_t d = (out_off[u + 1] - out_off[u]) + (in_off[u + 1] - in_off[u]);
-        const int bin = d <= kWarpMaxDeg ? 0 : (d <= kBlkCap / 2 ? 1 : 2);
+        const int bin = d <= kWarpMaxDeg ? 0 : (d <= kBlkMaxDeg ? 1 : 2);
         const int sb = nsub > 1 ? (int)(mix32((uint32_t)u ^ seed) % (uint32_t)nsub) : 0;
         bucket[i] = (uint16_t)(sb * kBins + bin);
     }
@@ -770,10 +802,10 @@ void free_modules(const ModState &M, SweepWork &W, Arena &ar, cudaStream_t s) {
 }
 
 void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &W, const SweepArgs &sa, int sb,
-                    uint32_t stamp, bool mark_active, cudaStream_t s, Timers *tm) {
+                    uint32_t stamp, uint32_t hseed, bool mark_active, cudaStream_t s, Timers *tm) {
     EvalArgs ea = eval_args(L, M, I, W, sa.vthresh, sa.allow_new, nullptr, 1);
     if (tm) tm->begin(kTimerEval, s);
-    launch_eval(ea, W.bucket_off, sb * kBins, s);
+    launch_eval(ea, W.bucket_off, sb * kBins, W, s);
     if (tm) tm->end(kTimerEval, s);
     if (tm) tm->begin(kTimerCommit, s);
     CommitArgs ca;
@@ -795,6 +827,7 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     ca.n_free = W.counters + kCntFree;
     ca.moved_nodes = reinterpret_cast<unsigned long long *>(W.counters + kCntMoved);
     ca.stamp = stamp;
+    ca.hseed = hseed;
     const unsigned G = num_sms() * 8;
     if (sa.allow_new) {
         k_claim<<<G, 256, 0, s>>>(ca);
@@ -831,7 +864,7 @@ void evaluate_all(const Level &L, const ModState &M, const InstState &I, SweepWo
     EvalArgs ea = eval_args(L, M, I, W, vthresh, 0, allow_new, 0);
     // allow_new == nullptr means "no empty-module candidate" for the hook
     if (!allow_new) ea.allow_new = 0;
-    launch_eval(ea, W.bucket_off, 0, s);
+    launch_eval(ea, W.bucket_off, 0, W, s);
 }
 
 }  // namespace rmx

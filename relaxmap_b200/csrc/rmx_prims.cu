@@ -5,6 +5,8 @@
 
 namespace rmx {
 
+unsigned long long g_kernel_launches = 0;
+
 int num_sms() {
     static int n = 0;
     if (n == 0) {
