@@ -75,7 +75,7 @@ def reflib():
             getattr(R, fn).restype = C.c_double
         for fn in ("rmxref_num_links", "rmxref_num_map_edges", "rmxref_sn_num_links"):
             getattr(R, fn).restype = C.c_longlong
-        for fn in ("rmxref_nnode", "rmxref_convert", "rmxref_node_name"):
+        for fn in ("rmxref_nnode", "rmxref_convert", "rmxref_node_name", "rmxref_coarse_tune"):
             getattr(R, fn).restype = C.c_int
         _REF = R
     return _REF
@@ -472,6 +472,13 @@ class Ref:
                              _ptr(od), _ptr(of), _ptr(io), _ptr(is_), _ptr(if_))
         return dict(n_sn=nsn, modidx=mi, size=sz, exit=ex, tw=tw, dsize=ds, nmembers=nm, out_off=oo, out_dst=od,
                     out_f=of, in_off=io, in_src=is_, in_f=if_)
+
+    def coarse_tune(self, threads=1, threshold=1e-3, max_iter=10):
+        """generate_sub_modules on the installed partition: (#sub-modules, sub-module per node, parent per SN)."""
+        sub = np.zeros(self.n, dtype=_i32)
+        par = np.zeros(self.n, dtype=_i32)
+        k = self.R.rmxref_coarse_tune(self._h, threads, C.c_double(threshold), max_iter, _ptr(sub), _ptr(par))
+        return k, sub, par[:k]
 
     def node_sweeps(self, seed, prior, vthresh, threshold, max_iter):
         part = np.zeros(self.n, dtype=_i32)

@@ -331,6 +331,19 @@ double rmxref_node_sweeps(void *p, unsigned seed, int prior, double vthresh_arg,
     return net.CodeLength();
 }
 
+// generate_sub_modules (OmpRelaxmap.cpp:502-638) on the installed partition:
+// returns the number of sub-module super-nodes and writes each node's
+// sub-module index (ndToSubMod) and each super-node's parent module.
+int rmxref_coarse_tune(void *p, int numTh, double threshold, int maxIter, int *sub_of_node, int *sn_parent) {
+    RefNet *h = (RefNet *)p;
+    Network &net = h->net;
+    Quiet q;
+    generate_sub_modules(net, numTh, threshold, maxIter);
+    for (int i = 0; i < net.NNode(); i++) sub_of_node[i] = net.ndToSubMod[i];
+    for (size_t s = 0; s < net.superNodes.size(); s++) sn_parent[s] = net.superNodes[s].ModIdx();
+    return (int)net.superNodes.size();
+}
+
 // The reference's superstep loop (OmpRelaxmap.cpp:170-233) on a prepared network.
 // vthresh_arg is the CLI value (negated internally as at OmpRelaxmap.cpp:66).
 // Writes the final module index per node, the incremental code length and the

@@ -435,6 +435,7 @@ void rmx_graph::alloc_engine() {
     for (ModState *M : {&mods, &submods}) {
         M->cap = n;
         M->stat = perm.alloc<Stat4>(n);
+        M->term = perm.alloc<double2>(n);
         M->count = perm.alloc<int32_t>(n);
         M->inst = perm.alloc<int32_t>(n);
     }
@@ -454,7 +455,7 @@ void rmx_graph::alloc_engine() {
     work.list2 = perm.alloc<int32_t>(n);
     work.bucket = perm.alloc<uint16_t>(n);
     work.bucket_off = perm.alloc<int64_t>(260);
-    work.ranges = perm.alloc<int64_t>(2 * 86);
+    work.ranges = perm.alloc<int64_t>(2 * 43);
     work.prop = perm.alloc<int32_t>(n);
     work.pdelta = perm.alloc<double>(n);
     work.ptarget = perm.alloc<int32_t>(n);
@@ -528,10 +529,11 @@ double rmx_graph::sweep_single(Level &lv, bool prior, bool allow_new, double vth
     if (prior) RMX_CUDA(cudaMemsetAsync(work.next_active, 0, lv.n, stream));
     if (allow_new) free_modules(mods, work, scratch, stream);
     const uint32_t seed = mix_seed(run_seed, ++sweep_no);
-    bucket_units(lv, work, n_active, seed, nsub, scratch, stream);
+    const int ns = sub_batches_for(n_active);
+    bucket_units(lv, work, n_active, seed, ns, scratch, stream);
     SweepArgs sa{vthresh, allow_new ? 1 : 0};
     Timers *tm = timers.on ? &timers : nullptr;
-    for (int sb = 0; sb < nsub; sb++)
+    for (int sb = 0; sb < ns; sb++)
         sweep_subbatch(lv, mods, inst1, work, sa, sb, ++stamp, mix_seed(seed, sb), prior, stream, tm);
     timers.begin(kTimerCodelen, stream);
     instance_codelength(mods, inst1, stream);
@@ -658,8 +660,9 @@ void rmx_graph::generate_sub_modules() {
         for (int iter = 0; iter < opt.max_iter; iter++) {
             all_units(N, work, stream);
             const uint32_t seed = mix_seed(run_seed, ++sweep_no);
-            bucket_units(sub_lv, work, N, seed, nsub, scratch, stream);
-            for (int sb = 0; sb < nsub; sb++)
+            const int ns = sub_batches_for(N);
+            bucket_units(sub_lv, work, N, seed, ns, scratch, stream);
+            for (int sb = 0; sb < ns; sb++)
                 sweep_subbatch(sub_lv, submods, instsub, work, sa, sb, ++stamp, mix_seed(seed, sb), false, stream, tm);
             timers.begin(kTimerCodelen, stream);
             instance_codelength(submods, instsub, stream);
@@ -724,6 +727,15 @@ double rmx_graph::stage(bool fine, double L) {
     return L;
 }
 
+// Sub-batches per sweep. A fixed count for every sweep: fewer sub-batches in
+// sweeps with small active sets make those sweeps cheaper but let
+// simultaneous moves oscillate, which costs more sweeps than it saves (and
+// code length); measured on the planted-partition benchmarks.
+int rmx_graph::sub_batches_for(int64_t n_active) const {
+    (void)n_active;
+    return nsub;
+}
+
 int32_t rmx_graph::count_modules() {
     count_units(node_lv, mods, stream);
     unsigned long long *c = reinterpret_cast<unsigned long long *>(dtmp + 10);
@@ -772,7 +784,7 @@ double rmx_graph::optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modu
     opt = o;
     if (opt.max_iter < 0) opt.max_iter = 0;
     if (opt.attempts < 1) opt.attempts = 1;
-    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 85) : (N >= 4096 ? 8 : 4);
+    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 42) : 4;
     cudaEvent_t t0, t1;
     RMX_CUDA(cudaEventCreate(&t0));
     RMX_CUDA(cudaEventCreate(&t1));

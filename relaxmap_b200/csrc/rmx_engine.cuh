@@ -34,6 +34,7 @@ struct Level {
 struct ModState {
     int32_t cap = 0;
     Stat4 *stat = nullptr;
+    double2 *term = nullptr;    // cached {plogp(exit), plogp(exit + P)} of each module
     int32_t *count = nullptr;   // units of the current level in the module
     int32_t *inst = nullptr;
 };
@@ -86,6 +87,8 @@ void singleton_exits(int32_t n, const int64_t *out_off, const double *out_f, con
 void init_singletons(const Level &L, ModState &M, cudaStream_t s);
 void module_stats_from_units(const Level &L, ModState &M, cudaStream_t s);
 void count_units(const Level &L, ModState &M, cudaStream_t s);
+// Refresh the cached log terms of every module from its statistics.
+void refresh_terms(ModState &M, cudaStream_t s);
 // Code length per instance from the module statistics.
 void instance_codelength(const ModState &M, InstState &I, cudaStream_t s);
 // Device time per kernel class, recorded with CUDA events on the stream.

@@ -73,5 +73,6 @@ struct rmx_graph {
     void generate_sub_modules();
     void project_sn_to_nodes();
     int32_t count_modules();
+    int sub_batches_for(int64_t n_active) const;
     int64_t max_degree(const rmx::Level &lv);
 };

@@ -73,14 +73,16 @@ struct UnitCtx {
 // Change of moving the unit into module with statistics st, given the unit's
 // aggregated out-/in-flow (fixed point, before the 1-tau factor) to it:
 // d_all - 2 d_exit + d_stay of Module.cpp:1109-1115 with the unit terms in K.
-__device__ __forceinline__ double candidate_delta(const UnitCtx &c, const Stat4 &st, fx_t ofx, fx_t ifx) {
+// t = the module's cached {plogp(exit), plogp(exit + P)}.
+__device__ __forceinline__ double candidate_delta(const UnitCtx &c, const Stat4 &st, const double2 t, fx_t ofx,
+                                                  fx_t ifx) {
     const double P = from_fx(st.P), TW = from_fx(st.TW), D = from_fx(st.D), OUT = from_fx(st.OUT);
     const double em = exit_flow(P, TW, D, OUT);
     const double om = kBeta * from_fx(ofx) + c.cu * TW;                        // Module.cpp:1058
     const double im = kBeta * from_fx(ifx) + (kAlpha * P + kBeta * D) * c.tu;  // Module.cpp:1059
     const double nexm = em + c.eu - om - im;                                   // Module.cpp:1104
     const double nse = c.sum_exit + c.nexA + nexm - c.eA - em;                 // Module.cpp:1106
-    return plogp(nse) + c.K - 2.0 * (plogp(nexm) - plogp(em)) + (plogp(nexm + P + c.pu) - plogp(em + P));
+    return plogp(nse) + c.K - 2.0 * (plogp(nexm) - t.x) + (plogp(nexm + P + c.pu) - t.y);
 }
 
 // The empty-module option: exit e_u, no shared flow (Module.cpp:1072-1077).
@@ -90,8 +92,8 @@ __device__ __forceinline__ double newmod_delta(const UnitCtx &c) {
     return plogp(nse) + c.K - 2.0 * plogp(nexm) + plogp(nexm + c.pu);
 }
 
-__device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, double sum_exit, int32_t A, fx_t oA,
-                                            fx_t iA) {
+__device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, const double2 tA, double sum_exit,
+                                            int32_t A, fx_t oA, fx_t iA) {
     UnitCtx c;
     c.pu = from_fx(ua.P);
     c.tu = from_fx(ua.TW);
@@ -104,7 +106,7 @@ __device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, do
     const double inA = kBeta * from_fx(iA) + (kAlpha * (PA - c.pu) + kBeta * (DA - du)) * c.tu;  // :1048
     c.nexA = c.eA - c.eu + outA + inA;                                                          // :1084
     c.sum_exit = sum_exit;
-    c.K = -plogp(sum_exit) - 2.0 * (plogp(c.nexA) - plogp(c.eA)) + (plogp(c.nexA + (PA - c.pu)) - plogp(c.eA + PA));
+    c.K = -plogp(sum_exit) - 2.0 * (plogp(c.nexA) - tA.x) + (plogp(c.nexA + (PA - c.pu)) - tA.y);
     c.A = A;
     return c;
 }
@@ -118,6 +120,7 @@ struct EvalArgs {
     const int32_t *mod, *uinst;
     // modules / instances
     const Stat4 *mstat;
+    const double2 *mterm;
     const int32_t *mcount;
     const double *inst_sum_exit;
     const uint8_t *inst_active;
@@ -134,11 +137,13 @@ struct EvalArgs {
     fx_t *gtable;              // hub tables: [block][gcap] out, in
     int32_t *gkeys;
     int64_t gcap;
+    uint8_t *next_active;      // prioritised mode: neighbours of units that propose a move
+    int mark;
 };
 
 // Decide and write the proposal for unit u given the argmin over candidates.
-__device__ __forceinline__ void finish_unit(const EvalArgs &a, int32_t u, const UnitCtx &c, double best,
-                                            int32_t bm) {
+__device__ __forceinline__ int32_t finish_unit(const EvalArgs &a, int32_t u, const UnitCtx &c, double best,
+                                               int32_t bm) {
     bool allow = a.allow_new_unit ? a.allow_new_unit[u] != 0 : (a.allow_new && a.mcount[c.A] > 1);
     if (allow) {
         double dn = newmod_delta(c);
@@ -156,10 +161,26 @@ __device__ __forceinline__ void finish_unit(const EvalArgs &a, int32_t u, const 
     }
     a.prop[u] = out;
     a.pdelta[u] = best;
+    // a unit that found a move below the threshold activates its neighbours
+    // for the next prioritised sweep, whether or not the move is then taken
+    // (Module.cpp:1661-1668)
+    return (bm != INT_MAX && best < a.vthresh) ? 1 : 0;
+}
+
+// Mark every out/in neighbour of u active (a group of NT threads, rank r).
+template <int NT>
+__device__ __forceinline__ void mark_neighbours(const EvalArgs &a, int32_t u, int r) {
+    const int64_t ob = a.out_off[u], oe = a.out_off[u + 1], ib = a.in_off[u], ie = a.in_off[u + 1];
+    for (int64_t e = ob + r; e < oe; e += NT) a.next_active[a.out_dst[e]] = 1;
+    for (int64_t e = ib + r; e < ie; e += NT) a.next_active[a.in_src[e]] = 1;
 }
 
 // ---------------------------------------------------------------- evaluation
 // Degree bins (out+in degree d of the unit at this level):
+//   reg    d <= 32    8, 16 or 32 lanes per unit, one link per lane: the
+//                     group sorts (module, flows) by module with a bitonic
+//                     network and sums equal runs with a segmented scan, all
+//                     in registers; each run's last lane is one candidate
 //   warp   d <= 128   one warp per unit, table of <= 256 slots per warp in
 //                     shared memory, candidates compacted in place
 //   block  d <= 1024  128 threads per unit, table of <= 2048 slots plus the
@@ -172,7 +193,10 @@ __device__ __forceinline__ void finish_unit(const EvalArgs &a, int32_t u, const 
 // candidate list, and evaluate the candidates with all lanes.
 
 constexpr int kWarpMaxDeg = 128, kWarpCap = 256, kEvalWarps = 8;
-constexpr int kBins = 3;  // degree bins: warp, block (shared table), hub (global table)
+// degree bins: 8 / 16 / 32 lanes in registers, warp (shared table), block
+// (shared table), hub (global table)
+constexpr int kBins = 6;
+constexpr int kBinReg8 = 0, kBinReg16 = 1, kBinReg32 = 2, kBinWarp = 3, kBinBlock = 4, kBinHub = 5;
 constexpr int kBlkT = 128, kBlkMaxDeg = 1024, kBlkCap = 2048, kBlkSlots = kBlkCap + kBlkCap / 2;
 constexpr int kHubT = 512;
 
@@ -233,7 +257,7 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
     const int32_t A = a.mod[u];
     const int sA = tab_find(keys, mask, A);
     const fx_t oA = sA >= 0 ? vo[sA] : 0, iA = sA >= 0 ? vi[sA] : 0;
-    const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
+    const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
     int nc = 0;
     if (NT == 32) {
         for (int64_t base = 0; base < cap; base += 32) {
@@ -283,7 +307,7 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
     int32_t bm = INT_MAX;
     for (int q = r; q < nc; q += NT) {
         const int32_t m = ck[q];
-        const double dl = candidate_delta(c, a.mstat[m], co[q], ci[q]);
+        const double dl = candidate_delta(c, a.mstat[m], a.mterm[m], co[q], ci[q]);
         if (better(dl, m, best, bm)) {
             best = dl;
             bm = m;
@@ -312,12 +336,154 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
                     bm = sh->mod[q];
                 }
     }
+    int act = 0;
     if (r == 0) {
-        finish_unit(a, u, c, best, bm);
+        act = finish_unit(a, u, c, best, bm);
         seen += d;
         cands += nc;
     }
+    if (a.mark) {
+        if (NT == 32) {
+            act = __shfl_sync(kFull, act, 0);
+        } else {
+            if (r == 0) sh->ncand = act;
+            __syncthreads();
+            act = sh->ncand;
+        }
+        if (act) mark_neighbours<NT>(a, u, r);
+    }
     gsync<NT>();
+}
+
+// Group of W lanes per unit (d <= W), everything in registers.
+template <int W>
+__device__ __forceinline__ void eval_unit_reg(const EvalArgs &a, const int32_t u, const bool valid, const int gl,
+                                              const unsigned gmask, unsigned long long &seen,
+                                              unsigned long long &cands) {
+    int32_t key = INT_MAX, nbr = -1;
+    fx_t vo = 0, vi = 0;
+    int64_t d = 0;
+    int32_t A = -1;
+    if (valid) {
+        const int64_t ob = a.out_off[u], ib = a.in_off[u];
+        const int64_t dout = a.out_off[u + 1] - ob;
+        d = dout + (a.in_off[u + 1] - ib);
+        A = a.mod[u];
+        if (gl < d) {
+            const bool isout = gl < dout;
+            const int64_t e = isout ? ob + gl : ib + (gl - dout);
+            nbr = isout ? a.out_dst[e] : a.in_src[e];
+            key = a.mod[nbr];
+            if (isout)
+                vo = a.out_fx[e];
+            else
+                vi = a.in_fx[e];
+        }
+    }
+    // bitonic sort of (key, vo, vi) by key within the group
+#pragma unroll
+    for (int k = 2; k <= W; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const int32_t pk = __shfl_xor_sync(kFull, key, j, W);
+            const fx_t po = __shfl_xor_sync(kFull, vo, j, W);
+            const fx_t pi = __shfl_xor_sync(kFull, vi, j, W);
+            const bool up = (gl & k) == 0, lower = (gl & j) == 0;
+            const bool take = lower == up ? pk < key : pk > key;
+            if (take) {
+                key = pk;
+                vo = po;
+                vi = pi;
+            }
+        }
+    }
+    // sums over runs of equal keys (segmented inclusive scan)
+#pragma unroll
+    for (int off = 1; off < W; off <<= 1) {
+        const int32_t k2 = __shfl_up_sync(kFull, key, off, W);
+        const fx_t o2 = __shfl_up_sync(kFull, vo, off, W);
+        const fx_t i2 = __shfl_up_sync(kFull, vi, off, W);
+        if (gl >= off && k2 == key) {
+            vo += o2;
+            vi += i2;
+        }
+    }
+    const int32_t nk = __shfl_down_sync(kFull, key, 1, W);
+    const bool tail = key != INT_MAX && (gl == W - 1 || nk != key);
+    // flows to the unit's own module from the lane ending A's run
+    const unsigned own = __ballot_sync(kFull, tail && key == A) & gmask;
+    const int src = own ? __ffs(own) - 1 : (threadIdx.x & 31);
+    fx_t oA = __shfl_sync(kFull, vo, src), iA = __shfl_sync(kFull, vi, src);
+    if (!own) oA = iA = 0;
+    double best = 0.0;
+    int32_t bm = INT_MAX;
+    UnitCtx c;
+    if (valid) {
+        c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
+        if (tail && key != A) {
+            best = candidate_delta(c, a.mstat[key], a.mterm[key], vo, vi);
+            bm = key;
+        }
+    }
+    const unsigned ncand = __popc(__ballot_sync(kFull, tail && key != A) & gmask);
+#pragma unroll
+    for (int o = W / 2; o > 0; o >>= 1) {
+        const double ob2 = __shfl_xor_sync(kFull, best, o, W);
+        const int32_t om = __shfl_xor_sync(kFull, bm, o, W);
+        if (better(ob2, om, best, bm)) {
+            best = ob2;
+            bm = om;
+        }
+    }
+    int act = 0;
+    if (valid && gl == 0) {
+        act = finish_unit(a, u, c, best, bm);
+        seen += d;
+        cands += ncand;
+    }
+    if (a.mark) {
+        act = __shfl_sync(kFull, act, (threadIdx.x & 31) & ~(W - 1));
+        if (act && nbr >= 0) a.next_active[nbr] = 1;
+    }
+}
+
+// Bins reg8, reg16, reg32: ranges range[0..3) of consecutive buckets.
+__global__ void __launch_bounds__(256) k_eval_reg(EvalArgs a) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long seen = 0, units = 0, cands = 0;
+#define RMX_REG_BIN(W, b)                                                                       \
+    {                                                                                           \
+        const int64_t beg = a.range[b], end = a.range[b + 1];                                   \
+        const int g = lane / W, gl = lane % W;                                                  \
+        const unsigned gmask = (W == 32 ? kFull : ((1u << W) - 1u)) << (g * W);                 \
+        for (int64_t base = beg + gw * (32 / W); base < end; base += nw * (32 / W)) {           \
+            const int64_t i = base + g;                                                         \
+            bool valid = i < end;                                                               \
+            const int32_t u = valid ? a.list[i] : 0;                                            \
+            if (valid && !a.inst_active[a.uinst[u]]) {                                          \
+                if (gl == 0) a.prop[u] = -1;                                                    \
+                valid = false;                                                                  \
+            }                                                                                   \
+            eval_unit_reg<W>(a, u, valid, gl, gmask, seen, cands);                              \
+            if (valid && gl == 0) units++;                                                      \
+        }                                                                                       \
+    }
+    RMX_REG_BIN(8, 0)
+    RMX_REG_BIN(16, 1)
+    RMX_REG_BIN(32, 2)
+#undef RMX_REG_BIN
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        seen += __shfl_xor_sync(kFull, seen, o);
+        units += __shfl_xor_sync(kFull, units, o);
+        cands += __shfl_xor_sync(kFull, cands, o);
+    }
+    if (lane == 0 && units) {
+        atomicAdd(a.stats + 0, seen);
+        atomicAdd(a.stats + 1, units);
+        atomicAdd(a.stats + 2, cands);
+    }
 }
 
 __device__ __forceinline__ void flush_stats(const EvalArgs &a, unsigned long long seen, unsigned long long units,
@@ -471,16 +637,13 @@ __global__ void k_commit(CommitArgs a) {
 struct DeltaArgs {
     const int32_t *list;
     const int64_t *range;
-    const int32_t *prop;
     const int32_t *mod, *prevmod;
     const uint32_t *stamp_of;
     const int64_t *out_off, *in_off;
     const int32_t *out_dst, *in_src;
     const fx_t *out_fx, *in_fx;
     Stat4 *mstat;
-    uint8_t *next_active;
     uint32_t stamp;
-    int mark;
 };
 
 // Out-flow bookkeeping for the movers of this sub-batch; warp per unit.
@@ -496,48 +659,71 @@ __global__ void __launch_bounds__(256) k_delta(DeltaArgs a) {
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t i = beg + gw; i < end; i += nw) {
         const int32_t u = a.list[i];
-        if (a.prop[u] == -1) continue;
-        const bool moved = a.stamp_of[u] == a.stamp;
-        if (!moved && !a.mark) continue;
-        const int32_t A = moved ? a.prevmod[u] : a.mod[u], T = a.mod[u];
+        if (a.stamp_of[u] != a.stamp) continue;  // did not move in this sub-batch
+        const int32_t A = a.prevmod[u], T = a.mod[u];
         fx_t dA = 0, dT = 0;
         for (int64_t e = a.out_off[u] + lane; e < a.out_off[u + 1]; e += 32) {
             const int32_t w = a.out_dst[e];
-            if (moved) {
-                const fx_t q = a.out_fx[e];
-                const bool wm = a.stamp_of[w] == a.stamp;
-                const int32_t bn = a.mod[w], bo = wm ? a.prevmod[w] : bn;
-                if (A != bo) dA -= q;
-                if (T != bn) dT += q;
-            }
-            if (a.mark) a.next_active[w] = 1;
+            const fx_t q = a.out_fx[e];
+            const bool wm = a.stamp_of[w] == a.stamp;
+            const int32_t bn = a.mod[w], bo = wm ? a.prevmod[w] : bn;
+            if (A != bo) dA -= q;
+            if (T != bn) dT += q;
         }
         for (int64_t e = a.in_off[u] + lane; e < a.in_off[u + 1]; e += 32) {
             const int32_t w = a.in_src[e];
-            if (moved && a.stamp_of[w] != a.stamp) {
+            if (a.stamp_of[w] != a.stamp) {
                 const int32_t b = a.mod[w];
                 if (b == A)
                     dA += a.in_fx[e];
                 else if (b == T)
                     dT -= a.in_fx[e];
             }
-            if (a.mark) a.next_active[w] = 1;
         }
-        if (moved) {
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                dA += __shfl_xor_sync(kFull, dA, o);
-                dT += __shfl_xor_sync(kFull, dT, o);
-            }
-            if (lane == 0) {
-                if (dA) atomic_add_fx(&a.mstat[A].OUT, dA);
-                if (dT) atomic_add_fx(&a.mstat[T].OUT, dT);
-            }
+        for (int o = 16; o > 0; o >>= 1) {
+            dA += __shfl_xor_sync(kFull, dA, o);
+            dT += __shfl_xor_sync(kFull, dT, o);
+        }
+        if (lane == 0) {
+            if (dA) atomic_add_fx(&a.mstat[A].OUT, dA);
+            if (dT) atomic_add_fx(&a.mstat[T].OUT, dT);
         }
     }
 }
 
 // ---------------------------------------------------------------- stats
+
+__device__ __forceinline__ double2 module_terms(const Stat4 &st) {
+    const double P = from_fx(st.P);
+    const double e = exit_flow(P, from_fx(st.TW), from_fx(st.D), from_fx(st.OUT));
+    return make_double2(plogp(e), plogp(e + P));
+}
+
+__global__ void k_terms_all(int32_t cap, const Stat4 *mstat, double2 *term) {
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < cap; m += (int64_t)gridDim.x * blockDim.x)
+        term[m] = module_terms(mstat[m]);
+}
+
+void refresh_terms(ModState &M, cudaStream_t s) {
+    k_terms_all<<<blocks_for(M.cap, 256, num_sms() * 32), 256, 0, s>>>(M.cap, M.stat, M.term);
+    RMX_LAUNCHED();
+}
+
+// After a sub-batch: the two modules of every mover get fresh cached terms
+// (a module touched by several movers is written with the same value).
+__global__ void k_terms_movers(const int32_t *list, const int64_t *range, const uint32_t *stamp_of, uint32_t stamp,
+                               const int32_t *mod, const int32_t *prevmod, const Stat4 *mstat, double2 *term) {
+    const int64_t beg = range[0], end = range[1];
+    for (int64_t i = beg + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < end;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t u = list[i];
+        if (stamp_of[u] != stamp) continue;
+        const int32_t A = prevmod[u], T = mod[u];
+        term[A] = module_terms(mstat[A]);
+        term[T] = module_terms(mstat[T]);
+    }
+}
 
 __global__ void k_init_singletons(int32_t n, const Stat4 *attr, const int32_t *uinst, int32_t *mod, Stat4 *mstat,
                                   int32_t *mcount, int32_t *minst) {
@@ -558,6 +744,7 @@ void init_singletons(const Level &L, ModState &M, cudaStream_t s) {
     k_init_singletons<<<blocks_for(L.n, 256, num_sms() * 32), 256, 0, s>>>(L.n, L.attr, L.inst, L.mod, M.stat, M.count,
                                                                            M.inst);
     RMX_LAUNCHED();
+    refresh_terms(M, s);
 }
 
 __global__ void k_stats_nodes(int32_t n, const Stat4 *attr, const int32_t *mod, const int32_t *uinst, Stat4 *mstat,
@@ -597,6 +784,7 @@ void module_stats_from_units(const Level &L, ModState &M, cudaStream_t s) {
     k_stats_links<<<blocks_for((int64_t)L.n * 32, 256, num_sms() * 32), 256, 0, s>>>(L.n, L.out_off, L.out_dst,
                                                                                      L.out_fx, L.mod, M.stat);
     RMX_LAUNCHED();
+    refresh_terms(M, s);
 }
 
 __global__ void k_count_units(int32_t n, const int32_t *mod, int32_t *mcount) {
@@ -612,8 +800,8 @@ void count_units(const Level &L, ModState &M, cudaStream_t s) {
 
 // Sum of module terms per instance in fixed point (deterministic).
 template <bool SINGLE>
-__global__ void __launch_bounds__(256) k_mod_terms(int32_t cap, const Stat4 *mstat, const int32_t *mcount,
-                                                   const int32_t *minst, fx_t *acc) {
+__global__ void __launch_bounds__(256) k_mod_terms(int32_t cap, const Stat4 *mstat, const double2 *mterm,
+                                                   const int32_t *mcount, const int32_t *minst, fx_t *acc) {
     __shared__ fx_t sh[3][8];
     fx_t t0 = 0, t1 = 0, t2 = 0;
     for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < cap; m += (int64_t)gridDim.x * blockDim.x) {
@@ -621,7 +809,8 @@ __global__ void __launch_bounds__(256) k_mod_terms(int32_t cap, const Stat4 *mst
         const Stat4 st = mstat[m];
         const double P = from_fx(st.P);
         const double e = exit_flow(P, from_fx(st.TW), from_fx(st.D), from_fx(st.OUT));
-        const fx_t a0 = to_fxl(e), a1 = to_fxl(plogp(e)), a2 = to_fxl(plogp(e + P));
+        const double2 t = mterm[m];
+        const fx_t a0 = to_fxl(e), a1 = to_fxl(t.x), a2 = to_fxl(t.y);
         if (SINGLE) {
             t0 += a0;
             t1 += a1;
@@ -666,10 +855,11 @@ __global__ void k_inst_L(int32_t ninst, const fx_t *acc, const fx_t *s0, double 
 void instance_codelength(const ModState &M, InstState &I, cudaStream_t s) {
     RMX_CUDA(cudaMemsetAsync(I.acc, 0, sizeof(fx_t) * 3 * I.n, s));
     if (I.n == 1)
-        k_mod_terms<true><<<blocks_for(M.cap, 256, num_sms() * 8), 256, 0, s>>>(M.cap, M.stat, M.count, M.inst, I.acc);
+        k_mod_terms<true><<<blocks_for(M.cap, 256, num_sms() * 8), 256, 0, s>>>(M.cap, M.stat, M.term, M.count, M.inst,
+                                                                                I.acc);
     else
-        k_mod_terms<false><<<blocks_for(M.cap, 256, num_sms() * 8), 256, 0, s>>>(M.cap, M.stat, M.count, M.inst,
-                                                                                 I.acc);
+        k_mod_terms<false><<<blocks_for(M.cap, 256, num_sms() * 8), 256, 0, s>>>(M.cap, M.stat, M.term, M.count,
+                                                                                 M.inst, I.acc);
     RMX_LAUNCHED();
     k_inst_L<<<blocks_for(I.n, 256, 4096), 256, 0, s>>>(I.n, I.acc, I.s0, I.sum_exit, I.L);
     RMX_LAUNCHED();
@@ -690,6 +880,7 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     a.mod = L.mod;
     a.uinst = L.inst;
     a.mstat = M.stat;
+    a.mterm = M.term;
     a.mcount = M.count;
     a.inst_sum_exit = I.sum_exit;
     a.inst_active = I.active;
@@ -705,6 +896,8 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     a.gtable = W.gtable;
     a.gkeys = W.gkeys;
     a.gcap = W.gcap;
+    a.next_active = W.next_active;
+    a.mark = 0;
     return a;
 }
 
@@ -719,17 +912,20 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     RMX_CUDA(cudaEventRecord(W.fork, s));
     RMX_CUDA(cudaStreamWaitEvent(W.aux[0], W.fork, 0));
     RMX_CUDA(cudaStreamWaitEvent(W.aux[1], W.fork, 0));
-    a.range = bucket_off + first_bucket + 1;
+    a.range = bucket_off + first_bucket + kBinBlock;
     k_eval_block<kBlkT, false><<<num_sms() * 3, kBlkT, (size_t)kBlkSlots * (2 * sizeof(fx_t) + sizeof(int32_t)),
                                  W.aux[0]>>>(a);
     RMX_LAUNCHED();
     if (a.gcap > 0) {
-        a.range = bucket_off + first_bucket + 2;
+        a.range = bucket_off + first_bucket + kBinHub;
         k_eval_block<kHubT, true><<<hub_blocks(), kHubT, 0, W.aux[1]>>>(a);
         RMX_LAUNCHED();
     }
-    a.range = bucket_off + first_bucket + 0;
-    k_eval_warp<<<num_sms() * 3, kEvalWarps * 32, 0, s>>>(a);
+    a.range = bucket_off + first_bucket + kBinWarp;
+    k_eval_warp<<<num_sms() * 3, kEvalWarps * 32, 0, W.aux[1]>>>(a);
+    RMX_LAUNCHED();
+    a.range = bucket_off + first_bucket + kBinReg8;
+    k_eval_reg<<<num_sms() * 8, 256, 0, s>>>(a);
     RMX_LAUNCHED();
     RMX_CUDA(cudaEventRecord(W.join[0], W.aux[0]));
     RMX_CUDA(cudaEventRecord(W.join[1], W.aux[1]));
@@ -742,6 +938,8 @@ void configure_eval_kernels() {
     if (done) return;
     const size_t smem = (size_t)kBlkSlots * (2 * sizeof(fx_t) + sizeof(int32_t));
     RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_warp, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     done = true;
 }
 
@@ -762,7 +960,12 @@ __global__ void k_bucket(const int32_t *list, const int64_t *n_active, const int
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t u = list[i];
         const int64_t d = (out_off[u + 1] - out_off[u]) + (in_off[u + 1] - in_off[u]);
-        const int bin = d <= kWarpMaxDeg ? 0 : (d <= kBlkMaxDeg ? 1 : 2);
+        const int bin = d <= 8 ? kBinReg8
+                        : d <= 16 ? kBinReg16
+                        : d <= 32 ? kBinReg32
+                        : d <= kWarpMaxDeg ? kBinWarp
+                        : d <= kBlkMaxDeg ? kBinBlock
+                                          : kBinHub;
         const int sb = nsub > 1 ? (int)(mix32((uint32_t)u ^ seed) % (uint32_t)nsub) : 0;
         bucket[i] = (uint16_t)(sb * kBins + bin);
     }
@@ -778,7 +981,7 @@ __global__ void k_ranges(const int64_t *bucket_off, int nsub, int64_t *ranges) {
 
 void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed, int nsub, Arena &ar,
                   cudaStream_t s) {
-    if (nsub * kBins > 255) throw std::invalid_argument("too many sub-batches");
+    if (nsub * kBins > 256) throw std::invalid_argument("too many sub-batches");
     k_bucket<<<blocks_for(n_active, 256, num_sms() * 32), 256, 0, s>>>(W.list, W.counters + kCntActive, L.out_off,
                                                                        L.in_off, seed, nsub, W.bucket);
     RMX_LAUNCHED();
@@ -804,6 +1007,7 @@ void free_modules(const ModState &M, SweepWork &W, Arena &ar, cudaStream_t s) {
 void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &W, const SweepArgs &sa, int sb,
                     uint32_t stamp, uint32_t hseed, bool mark_active, cudaStream_t s, Timers *tm) {
     EvalArgs ea = eval_args(L, M, I, W, sa.vthresh, sa.allow_new, nullptr, 1);
+    ea.mark = mark_active ? 1 : 0;
     if (tm) tm->begin(kTimerEval, s);
     launch_eval(ea, W.bucket_off, sb * kBins, W, s);
     if (tm) tm->end(kTimerEval, s);
@@ -838,7 +1042,6 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     DeltaArgs da;
     da.list = W.list2;
     da.range = W.ranges + 2 * sb;
-    da.prop = W.prop;
     da.mod = L.mod;
     da.prevmod = W.prevmod;
     da.stamp_of = W.stamp;
@@ -849,10 +1052,10 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     da.out_fx = L.out_fx;
     da.in_fx = L.in_fx;
     da.mstat = M.stat;
-    da.next_active = W.next_active;
     da.stamp = stamp;
-    da.mark = mark_active ? 1 : 0;
     k_delta<<<G, 256, 0, s>>>(da);
+    RMX_LAUNCHED();
+    k_terms_movers<<<G, 256, 0, s>>>(W.list2, W.ranges + 2 * sb, W.stamp, stamp, L.mod, W.prevmod, M.stat, M.term);
     RMX_LAUNCHED();
     if (tm) tm->end(kTimerCommit, s);
 }
