@@ -180,6 +180,36 @@ void *rmx_graph_stream(const rmx_graph *g);
 /* Block until the handle's stream is idle. */
 rmx_status rmx_sync(rmx_graph *g);
 
+/* Largest graph rmx_steady_state_noalloc accepts. */
+#define RMX_NOALLOC_MAX_NODES (1 << 20)
+
+/* The stationary flow of rmx_initiate for callers that cannot allocate device
+ * memory: a memory pool that owns the whole device under a fixed budget, work
+ * being recorded into a CUDA graph, or a latency-bound path that must not pay
+ * for an allocation's device-wide synchronisation. This entry point has no
+ * counterpart in the reference (it computes calculateSteadyState only as part
+ * of Network::initiate).
+ * Every pointer is device memory owned by the caller: the in-links as CSC
+ * (in_off[n_nodes+1], in_src[n_links], in_w[n_links] = row-normalised link
+ * weights w_ab / sum_b w_ab), teleport[n_nodes], dangling[n_nodes] (1 for nodes
+ * without out-links), p_out[n_nodes] (result); iters_out (device int, may be
+ * NULL) receives the number of power iterations. n_nodes must not exceed
+ * RMX_NOALLOC_MAX_NODES (larger graphs: RMX_ERR_INVALID). The work is queued
+ * on `stream` (a cudaStream_t, NULL for the legacy default stream) and the call
+ * returns without waiting for it.
+ * Temporary storage is one array of about 8 MB inside this library, present on
+ * every device that loads it until the process exits; it calls no cudaMalloc
+ * or cudaFree. The first call on each device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current; make that first call
+ * before capturing a stream. All calls on a device share the array: calls whose
+ * work overlaps on the GPU (other streams, other host threads) race and give
+ * wrong results; order them on one stream or with events. Error text:
+ * rmx_noalloc_last_error(). */
+rmx_status rmx_steady_state_noalloc(int32_t n_nodes, int64_t n_links, const int64_t *in_off, const int32_t *in_src,
+                                    const double *in_w, const double *teleport, const uint8_t *dangling,
+                                    double *p_out, int32_t *iters_out, void *stream);
+const char *rmx_noalloc_last_error(void);
+
 /* The reference command line (OmpRelaxmap.cpp:41-252), same positional
  * arguments and output files; returns the process exit code. */
 int rmx_cli_main(int argc, char **argv);

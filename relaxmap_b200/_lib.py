@@ -23,7 +23,8 @@ EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_creat
            "rmx_parse_file",
            "rmx_graph_destroy", "rmx_graph_info", "rmx_graph_links", "rmx_initiate", "rmx_codelength",
            "rmx_coarsen", "rmx_evaluate_moves", "rmx_optimize", "rmx_superstep_codelengths", "rmx_write_outputs",
-           "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main"]
+           "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main",
+           "rmx_steady_state_noalloc", "rmx_noalloc_last_error"]
 
 
 class RmxError(RuntimeError):
@@ -60,12 +61,13 @@ def lib():
             raise RmxError(4, f"{LIB_PATH} missing: build it with `python -m relaxmap_b200.build`")
         L = C.CDLL(str(LIB_PATH))
         L.rmx_last_error.restype = C.c_char_p
+        L.rmx_noalloc_last_error.restype = C.c_char_p
         L.rmx_version.restype = C.c_char_p
         L.rmx_graph_stream.restype = C.c_void_p
         L.rmx_superstep_codelengths.restype = C.c_int32
         for fn in EXPORTS:
             if fn not in ("rmx_last_error", "rmx_version", "rmx_graph_stream", "rmx_superstep_codelengths",
-                          "rmx_opts_default"):
+                          "rmx_opts_default", "rmx_noalloc_last_error"):
                 getattr(L, fn).restype = C.c_int
         _L = L
     return _L
@@ -233,6 +235,18 @@ def parse_file(path, threads: int = 1) -> dict:
                                 _p(dst), _p(w), _p(nw)))
     k = m.value
     return dict(n=n.value, src=src[:k], dst=dst[:k], w=w[:k], node_w=nw[:n.value], n_self=ns.value)
+
+
+def steady_state_noalloc(n_nodes: int, n_links: int, in_off_ptr: int, in_src_ptr: int, in_w_ptr: int,
+                         teleport_ptr: int, dangling_ptr: int, p_out_ptr: int, iters_ptr: int = 0,
+                         stream_ptr: int = 0) -> None:
+    """rmx_steady_state_noalloc on caller-owned device buffers (raw pointers)."""
+    st = lib().rmx_steady_state_noalloc(C.c_int32(n_nodes), C.c_int64(n_links), C.c_void_p(in_off_ptr),
+                                        C.c_void_p(in_src_ptr or None), C.c_void_p(in_w_ptr or None),
+                                        C.c_void_p(teleport_ptr), C.c_void_p(dangling_ptr), C.c_void_p(p_out_ptr),
+                                        C.c_void_p(iters_ptr or None), C.c_void_p(stream_ptr or None))
+    if st != RMX_OK:
+        raise RmxError(st, lib().rmx_noalloc_last_error().decode(errors="replace"))
 
 
 def cli(argv: list[str]) -> int:

@@ -74,6 +74,13 @@ struct FlowOut {
 };
 int power_iteration(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
                     const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, int vec);
+// The same solve writing into caller-provided scratch (y[n], parts[3*max_blocks],
+// iters on the device); asynchronous, allocates nothing.
+void power_iteration_into(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w,
+                          const double *tw, const uint8_t *dangling, double *p, double *y, double *parts,
+                          int max_blocks, int *iters, cudaStream_t s, int vec);
+// Sub-warp width of the pull SpMV for a mean in-degree.
+int spmv_width(double mean_in_degree);
 void normalise(int32_t n, const int64_t *out_off, const double *out_w0, double *out_f, const int64_t *in_off,
                const int32_t *in_src, const double *in_w_raw, double *in_w, uint8_t *dangling, Arena &ar,
                cudaStream_t s);

@@ -322,6 +322,42 @@ static int launch_power(int32_t n, const int64_t *in_off, const int32_t *in_src,
     return h;
 }
 
+// Launch of the same solve into caller-provided scratch: y[n], parts[3 * max_blocks],
+// *iters; nothing is allocated and nothing waits on the stream.
+template <int VEC>
+static void launch_power_into(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w,
+                              const double *tw, const uint8_t *dangling, double *p, double *y, double *parts,
+                              int max_blocks, int *iters, cudaStream_t s) {
+    int dev = 0, per_sm = 0;
+    RMX_CUDA(cudaGetDevice(&dev));
+    RMX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_power<VEC>, kPowT, 0));
+    int nb = std::max(1, std::min(per_sm, 4)) * num_sms();
+    nb = (int)std::min<int64_t>(nb, std::max<int64_t>(1, ((int64_t)n * VEC + kPowT - 1) / kPowT));
+    nb = std::min(nb, max_blocks);
+    void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w, (void *)&tw, (void *)&dangling, (void *)&n,
+                    (void *)&p, (void *)&y, (void *)&parts, (void *)&iters};
+    RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));
+    RMX_LAUNCHED();
+}
+
+void power_iteration_into(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w,
+                          const double *tw, const uint8_t *dangling, double *p, double *y, double *parts,
+                          int max_blocks, int *iters, cudaStream_t s, int vec) {
+    if (n <= 0) return;
+    switch (vec) {
+        case 4: return launch_power_into<4>(n, in_off, in_src, in_w, tw, dangling, p, y, parts, max_blocks, iters, s);
+        case 8: return launch_power_into<8>(n, in_off, in_src, in_w, tw, dangling, p, y, parts, max_blocks, iters, s);
+        case 16:
+            return launch_power_into<16>(n, in_off, in_src, in_w, tw, dangling, p, y, parts, max_blocks, iters, s);
+        default:
+            return launch_power_into<32>(n, in_off, in_src, in_w, tw, dangling, p, y, parts, max_blocks, iters, s);
+    }
+}
+
+int spmv_width(double mean_in_degree) {
+    return mean_in_degree <= 6 ? 4 : (mean_in_degree <= 12 ? 8 : (mean_in_degree <= 24 ? 16 : 32));
+}
+
 int power_iteration(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
                     const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, int vec) {
     if (n <= 0) return 0;
