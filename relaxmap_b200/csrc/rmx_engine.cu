@@ -455,7 +455,7 @@ void rmx_graph::alloc_engine() {
     work.list2 = perm.alloc<int32_t>(n);
     work.bucket = perm.alloc<uint16_t>(n);
     work.bucket_off = perm.alloc<int64_t>(260);
-    work.ranges = perm.alloc<int64_t>(2 * 43);
+    work.ranges = perm.alloc<int64_t>(2 * 37);
     work.prop = perm.alloc<int32_t>(n);
     work.pdelta = perm.alloc<double>(n);
     work.ptarget = perm.alloc<int32_t>(n);
@@ -784,7 +784,7 @@ double rmx_graph::optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modu
     opt = o;
     if (opt.max_iter < 0) opt.max_iter = 0;
     if (opt.attempts < 1) opt.attempts = 1;
-    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 42) : 4;
+    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 36) : 4;
     cudaEvent_t t0, t1;
     RMX_CUDA(cudaEventCreate(&t0));
     RMX_CUDA(cudaEventCreate(&t1));

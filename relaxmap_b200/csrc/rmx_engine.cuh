@@ -138,10 +138,10 @@ struct SweepWork {
     unsigned long long *claim = nullptr;        // per module id
     int64_t *counters = nullptr;
     fx_t *gtable = nullptr;                     // hub hash tables: hub_blocks() slices of
-    int32_t *gkeys = nullptr;                   //   hub_slots(gcap) entries (table + candidates)
+    int32_t *gkeys = nullptr;                   //   hub_slots(gcap) entries
     int64_t gcap = 0;
-    cudaStream_t aux[2] = {nullptr, nullptr};   // concurrent degree bins
-    cudaEvent_t fork = nullptr, join[2] = {nullptr, nullptr};
+    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};  // concurrent degree bins
+    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
 };
 
 void configure_eval_kernels();

@@ -183,21 +183,22 @@ __device__ __forceinline__ void mark_neighbours(const EvalArgs &a, int32_t u, in
 //                     in registers; each run's last lane is one candidate
 //   warp   d <= 128   one warp per unit, table of <= 256 slots per warp in
 //                     shared memory, candidates compacted in place
-//   block  d <= 1024  128 threads per unit, table of <= 2048 slots plus the
-//                     candidate list in shared memory
-//   hub    d > 1024   512 threads per unit, table + candidate list in a
-//                     per-block slice of a global table
+//   block  d <= 1024  256 threads per unit, table of <= 2048 slots in shared memory
+//   large  d <= 4096  512 threads per unit, table of <= 8192 slots in shared memory
+//   hub    d > 4096   512 threads per unit, table in a per-block slice of a
+//                     global table (one block per SM)
 // Each unit: clear the table, insert every link's neighbour module with its
 // fixed-point flow (integer atomics, so the sums do not depend on the order),
-// look up the own module, compact the other occupied slots into a dense
-// candidate list, and evaluate the candidates with all lanes.
+// look up the own module, compact the other occupied slots in place into a
+// dense candidate list, and evaluate the candidates with all lanes.
 
 constexpr int kWarpMaxDeg = 128, kWarpCap = 256, kEvalWarps = 8;
 // degree bins: 8 / 16 / 32 lanes in registers, warp (shared table), block
 // (shared table), hub (global table)
-constexpr int kBins = 6;
-constexpr int kBinReg8 = 0, kBinReg16 = 1, kBinReg32 = 2, kBinWarp = 3, kBinBlock = 4, kBinHub = 5;
-constexpr int kBlkT = 128, kBlkMaxDeg = 1024, kBlkCap = 2048, kBlkSlots = kBlkCap + kBlkCap / 2;
+constexpr int kBins = 7;
+constexpr int kBinReg8 = 0, kBinReg16 = 1, kBinReg32 = 2, kBinWarp = 3, kBinBlock = 4, kBinLarge = 5, kBinHub = 6;
+constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
+constexpr int kLrgT = 512, kLrgMaxDeg = 4096, kLrgCap = 8192;
 constexpr int kHubT = 512;
 
 __device__ __forceinline__ int tab_find(const int32_t *keys, int mask, int32_t key) {
@@ -223,11 +224,12 @@ template <int NT>
 struct GroupShared {  // reductions across the warps of a block group
     double best[NT / 32];
     int32_t mod[NT / 32];
+    int wpos[NT / 32];
     int ncand;
 };
 
 // One unit evaluated by a group of NT threads (a warp or a block); r = rank.
-// For the warp group the candidate list overwrites the table (ck == keys).
+// The candidate list overwrites the table in place (ck == keys).
 template <int NT>
 __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, const int r, int32_t *keys, fx_t *vo,
                                           fx_t *vi, int32_t *ck, fx_t *co, fx_t *ci, GroupShared<NT> *sh,
@@ -277,10 +279,10 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
         }
         __syncwarp();
     } else {
-        if (r == 0) sh->ncand = 0;
-        __syncthreads();
-        for (int64_t base = r & ~31; base < cap; base += NT) {
-            const int64_t s = base + lane;
+        // chunks of NT slots in order; a block-wide scan of the occupancy gives
+        // every candidate its dense position, which never exceeds its slot
+        for (int64_t base = 0; base < cap; base += NT) {
+            const int64_t s = base + r;
             int32_t k = kEmpty;
             fx_t o = 0, i2 = 0;
             if (s < cap) {
@@ -290,18 +292,29 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
             }
             const bool occ = k != kEmpty && k != A;
             const unsigned bal = __ballot_sync(kFull, occ);
-            int p0 = 0;
-            if (lane == 0 && bal) p0 = atomicAdd(&sh->ncand, __popc(bal));
-            p0 = __shfl_sync(kFull, p0, 0);
+            if (lane == 0) sh->wpos[r >> 5] = __popc(bal);
+            __syncthreads();
+            if (r < 32) {
+                int v = r < NT / 32 ? sh->wpos[r] : 0;
+                const int own = v;
+#pragma unroll
+                for (int q = 1; q < 32; q <<= 1) {
+                    const int y = __shfl_up_sync(kFull, v, q);
+                    if (r >= q) v += y;
+                }
+                if (r < NT / 32) sh->wpos[r] = v - own;
+                if (r == 31) sh->ncand = v;
+            }
+            __syncthreads();
             if (occ) {
-                const int p = p0 + __popc(bal & lt);
+                const int p = nc + sh->wpos[r >> 5] + __popc(bal & lt);
                 ck[p] = k;
                 co[p] = o;
                 ci[p] = i2;
             }
+            nc += sh->ncand;
+            __syncthreads();
         }
-        __syncthreads();
-        nc = sh->ncand;
     }
     double best = 0.0;
     int32_t bm = INT_MAX;
@@ -515,23 +528,21 @@ __global__ void __launch_bounds__(kEvalWarps * 32, 3) k_eval_warp(EvalArgs a) {
     if (lane == 0) flush_stats(a, seen, units, cands);
 }
 
-template <int NT, bool GLOBAL>
-__global__ void __launch_bounds__(NT, GLOBAL ? 1 : 3) k_eval_block(EvalArgs a) {
+template <int NT, int CAP, bool GLOBAL>
+__global__ void __launch_bounds__(NT) k_eval_block(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ GroupShared<NT> sh;
     int32_t *keys;
     fx_t *vo, *vi;
-    int64_t slots;
     if (GLOBAL) {
-        slots = a.gcap + a.gcap / 2;
+        const int64_t slots = a.gcap;
         keys = a.gkeys + (int64_t)blockIdx.x * slots;
         vo = a.gtable + (int64_t)blockIdx.x * slots * 2;
         vi = vo + slots;
     } else {
-        slots = kBlkSlots;
         vo = reinterpret_cast<fx_t *>(dsm);
-        vi = vo + kBlkSlots;
-        keys = reinterpret_cast<int32_t *>(vi + kBlkSlots);
+        vi = vo + CAP;
+        keys = reinterpret_cast<int32_t *>(vi + CAP);
     }
     const int64_t beg = a.range[0], end = a.range[1];
     unsigned long long seen = 0, units = 0, cands = 0;
@@ -541,11 +552,7 @@ __global__ void __launch_bounds__(NT, GLOBAL ? 1 : 3) k_eval_block(EvalArgs a) {
             if (threadIdx.x == 0) a.prop[u] = -1;
             continue;
         }
-        // the candidate list follows the table: cap + cap/2 <= slots
-        const int64_t d = (a.out_off[u + 1] - a.out_off[u]) + (a.in_off[u + 1] - a.in_off[u]);
-        int64_t cap = 32;
-        while (cap < 2 * d) cap <<= 1;
-        eval_unit<NT>(a, u, threadIdx.x, keys, vo, vi, keys + cap, vo + cap, vi + cap, &sh, seen, cands);
+        eval_unit<NT>(a, u, threadIdx.x, keys, vo, vi, keys, vo, vi, &sh, seen, cands);
         units++;
     }
     if (threadIdx.x == 0) flush_stats(a, seen, units, cands);
@@ -901,44 +908,54 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     return a;
 }
 
-int hub_blocks() { return std::min(num_sms(), 64); }
-int64_t block_bin_max_degree() { return kBlkMaxDeg; }
+int hub_blocks() { return num_sms(); }
+int64_t block_bin_max_degree() { return kLrgMaxDeg; }
 int64_t warp_bin_max_degree() { return kWarpMaxDeg; }
-int64_t hub_slots(int64_t cap) { return cap + cap / 2; }
+int64_t hub_slots(int64_t cap) { return cap; }
 
-// The three bins of a sub-batch run concurrently: the block and hub kernels
-// on two auxiliary streams forked from and joined back into s.
+constexpr size_t kBlkSmem = (size_t)kBlkCap * (2 * sizeof(fx_t) + sizeof(int32_t));
+constexpr size_t kLrgSmem = (size_t)kLrgCap * (2 * sizeof(fx_t) + sizeof(int32_t));
+
+// The bins of a sub-batch run concurrently: block, large + hub, and the warp
+// bin on three auxiliary streams forked from and joined back into s, the
+// register bins on s itself.
 static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket, const SweepWork &W, cudaStream_t s) {
     RMX_CUDA(cudaEventRecord(W.fork, s));
-    RMX_CUDA(cudaStreamWaitEvent(W.aux[0], W.fork, 0));
-    RMX_CUDA(cudaStreamWaitEvent(W.aux[1], W.fork, 0));
+    for (int k = 0; k < 3; k++) RMX_CUDA(cudaStreamWaitEvent(W.aux[k], W.fork, 0));
     a.range = bucket_off + first_bucket + kBinBlock;
-    k_eval_block<kBlkT, false><<<num_sms() * 3, kBlkT, (size_t)kBlkSlots * (2 * sizeof(fx_t) + sizeof(int32_t)),
-                                 W.aux[0]>>>(a);
+    k_eval_block<kBlkT, kBlkCap, false><<<num_sms() * 2, kBlkT, kBlkSmem, W.aux[0]>>>(a);
+    RMX_LAUNCHED();
+    a.range = bucket_off + first_bucket + kBinLarge;
+    k_eval_block<kLrgT, kLrgCap, false><<<num_sms(), kLrgT, kLrgSmem, W.aux[1]>>>(a);
     RMX_LAUNCHED();
     if (a.gcap > 0) {
         a.range = bucket_off + first_bucket + kBinHub;
-        k_eval_block<kHubT, true><<<hub_blocks(), kHubT, 0, W.aux[1]>>>(a);
+        k_eval_block<kHubT, 0, true><<<hub_blocks(), kHubT, 0, W.aux[1]>>>(a);
         RMX_LAUNCHED();
     }
     a.range = bucket_off + first_bucket + kBinWarp;
-    k_eval_warp<<<num_sms() * 3, kEvalWarps * 32, 0, W.aux[1]>>>(a);
+    k_eval_warp<<<num_sms() * 3, kEvalWarps * 32, 0, W.aux[2]>>>(a);
     RMX_LAUNCHED();
     a.range = bucket_off + first_bucket + kBinReg8;
     k_eval_reg<<<num_sms() * 8, 256, 0, s>>>(a);
     RMX_LAUNCHED();
-    RMX_CUDA(cudaEventRecord(W.join[0], W.aux[0]));
-    RMX_CUDA(cudaEventRecord(W.join[1], W.aux[1]));
-    RMX_CUDA(cudaStreamWaitEvent(s, W.join[0], 0));
-    RMX_CUDA(cudaStreamWaitEvent(s, W.join[1], 0));
+    for (int k = 0; k < 3; k++) {
+        RMX_CUDA(cudaEventRecord(W.join[k], W.aux[k]));
+        RMX_CUDA(cudaStreamWaitEvent(s, W.join[k], 0));
+    }
 }
 
 void configure_eval_kernels() {
     static bool done = false;
     if (done) return;
-    const size_t smem = (size_t)kBlkSlots * (2 * sizeof(fx_t) + sizeof(int32_t));
-    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, kBlkCap, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kBlkSmem));
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kLrgT, kLrgCap, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kLrgSmem));
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, kBlkCap, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  100));
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kLrgT, kLrgCap, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  100));
     RMX_CUDA(cudaFuncSetAttribute(k_eval_warp, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     done = true;
 }
@@ -965,6 +982,7 @@ __global__ void k_bucket(const int32_t *list, const int64_t *n_active, const int
                         : d <= 32 ? kBinReg32
                         : d <= kWarpMaxDeg ? kBinWarp
                         : d <= kBlkMaxDeg ? kBinBlock
+                        : d <= kLrgMaxDeg ? kBinLarge
                                           : kBinHub;
         const int sb = nsub > 1 ? (int)(mix32((uint32_t)u ^ seed) % (uint32_t)nsub) : 0;
         bucket[i] = (uint16_t)(sb * kBins + bin);
