@@ -350,7 +350,7 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     const int64_t Eb = std::max<int64_t>(n_edges, 1);
     scratch.init((size_t)(88 * Eb + 24 * (int64_t)n) + (64u << 20));
     // long-lived arrays: node CSR/CSC, three levels, module and instance state
-    perm.init((size_t)(112 * Eb + 440 * (int64_t)n) + (64u << 20));
+    perm.init((size_t)(144 * Eb + 560 * (int64_t)n) + (64u << 20));
     out_off = perm.alloc<int64_t>(n + 1);
     in_off = perm.alloc<int64_t>(n + 1);
     int32_t *d_src = scratch.alloc<int32_t>(Eb), *d_dst = scratch.alloc<int32_t>(Eb);
@@ -417,7 +417,7 @@ void rmx_graph::alloc_engine() {
     node_lv.mod = nmod;
     node_lv.inst = zeros;
     node_lv.nnodes = nullptr;
-    for (Level *lv : {&sn_lv, &sub_lv}) {
+    for (Level *lv : {&sn_buf[0], &sn_buf[1], &sub_lv}) {
         lv->out_off = perm.alloc<int64_t>(n + 1);
         lv->in_off = perm.alloc<int64_t>(n + 1);
         lv->out_dst = perm.alloc<int32_t>(Em);
@@ -427,8 +427,10 @@ void rmx_graph::alloc_engine() {
         lv->attr = perm.alloc<Stat4>(n);
         lv->nnodes = perm.alloc<int32_t>(n);
     }
-    sn_lv.mod = perm.alloc<int32_t>(n);
-    sn_lv.inst = zeros;
+    for (Level &lv : sn_buf) {
+        lv.mod = perm.alloc<int32_t>(n);
+        lv.inst = zeros;
+    }
     sub_lv.mod = submod;
     sub_lv.inst = nmod;  // instance of a node in coarse-tune = its parent module
     sub_lv.nnodes = nullptr;
@@ -579,14 +581,18 @@ double rmx_graph::stage_sweeps(Level &lv, bool allow_new, double L) {
 }
 
 void rmx_graph::project_sn_to_nodes() {
-    k_project<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, node_sn, sn_lv.mod, nmod);
+    k_project<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, node_sn, sn().mod, nmod);
     RMX_LAUNCHED();
 }
 
 // convertModulesToSuperNodes (Module.cpp:3008-3077) on the engine's partition.
-void rmx_graph::convert_to_supernodes() {
+// The super-node links carry fixed-point flows, whose sums are exact in any
+// order, so after a super-node stage the new level is aggregated from the
+// current super-node links (a few times fewer than node links) with the same
+// result as from the node links.
+void rmx_graph::convert_to_supernodes(bool from_sn) {
     timers.begin(kTimerCoarsen, stream);
-    count_units(node_lv, mods, stream);
+    count_units(node_lv, mods, stream);  // nodes per module
     size_t mk = scratch.mark();
     int64_t *snid = scratch.alloc<int64_t>(N + 1);
     k_flags_nonempty<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, mods.count, snid);
@@ -594,18 +600,30 @@ void rmx_graph::convert_to_supernodes() {
     scan_exclusive(snid, snid, N, dtmp + 0, scratch, stream);
     int64_t nsn = 0;
     RMX_CUDA(cudaMemcpyAsync(&nsn, dtmp + 0, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
-    k_sn_from_modules<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, mods.count, snid, mods.stat,
-                                                                              sn_lv.mod, sn_lv.attr, sn_lv.nnodes,
-                                                                              zeros);
+    Level &src = sn(), &dst = sn_buf[1 - sn_cur];
+    k_sn_from_modules<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, mods.count, snid, mods.stat, dst.mod,
+                                                                              dst.attr, dst.nnodes, zeros);
     RMX_LAUNCHED();
+    int32_t *group = nullptr;
+    if (from_sn) {
+        group = scratch.alloc<int32_t>(std::max(src.n, 1));
+        k_group_of_nodes<<<blocks_for(src.n, 256, num_sms() * 32), 256, 0, stream>>>(src.n, src.mod, snid, group);
+        RMX_LAUNCHED();
+    }
     k_group_of_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, nmod, snid, node_sn);
     RMX_LAUNCHED();
     RMX_CUDA(cudaStreamSynchronize(stream));
-    sn_lv.n = (int32_t)nsn;
-    sn_lv.m = coarsen_links(N, out_off, out_dst, nullptr, out_fx, node_sn, sn_lv.n, sn_lv.out_off, sn_lv.out_dst,
-                            nullptr, sn_lv.out_fx, sn_lv.in_off, sn_lv.in_src, nullptr, sn_lv.in_fx, scratch, stream);
+    dst.n = (int32_t)nsn;
+    if (from_sn)
+        dst.m = coarsen_links(src.n, src.out_off, src.out_dst, nullptr, src.out_fx, group, dst.n, dst.out_off,
+                              dst.out_dst, nullptr, dst.out_fx, dst.in_off, dst.in_src, nullptr, dst.in_fx, scratch,
+                              stream);
+    else
+        dst.m = coarsen_links(N, out_off, out_dst, nullptr, out_fx, node_sn, dst.n, dst.out_off, dst.out_dst, nullptr,
+                              dst.out_fx, dst.in_off, dst.in_src, nullptr, dst.in_fx, scratch, stream);
     scratch.release(mk);
-    count_units(sn_lv, mods, stream);
+    sn_cur = 1 - sn_cur;
+    count_units(sn(), mods, stream);
     timers.end(kTimerCoarsen, stream);
 }
 
@@ -692,16 +710,17 @@ void rmx_graph::generate_sub_modules() {
     int64_t nsn = 0;
     RMX_CUDA(cudaMemcpyAsync(&nsn, dtmp + 0, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaStreamSynchronize(stream));
-    sn_lv.n = (int32_t)nsn;
-    RMX_CUDA(cudaMemsetAsync(sn_lv.attr, 0, sizeof(Stat4) * nsn, stream));
-    RMX_CUDA(cudaMemsetAsync(sn_lv.nnodes, 0, sizeof(int32_t) * nsn, stream));
-    k_sn_from_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, node_sn, nmod, nattr, sn_lv.mod,
-                                                                            sn_lv.attr, sn_lv.nnodes);
+    Level &sl = sn();
+    sl.n = (int32_t)nsn;
+    RMX_CUDA(cudaMemsetAsync(sl.attr, 0, sizeof(Stat4) * nsn, stream));
+    RMX_CUDA(cudaMemsetAsync(sl.nnodes, 0, sizeof(int32_t) * nsn, stream));
+    k_sn_from_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, node_sn, nmod, nattr, sl.mod,
+                                                                            sl.attr, sl.nnodes);
     RMX_LAUNCHED();
-    sn_lv.m = coarsen_links(N, out_off, out_dst, nullptr, out_fx, node_sn, sn_lv.n, sn_lv.out_off, sn_lv.out_dst,
-                            nullptr, sn_lv.out_fx, sn_lv.in_off, sn_lv.in_src, nullptr, sn_lv.in_fx, scratch, stream);
-    k_sn_out<<<blocks_for(nsn, 256, num_sms() * 32), 256, 0, stream>>>(sn_lv.n, sn_lv.out_off, sn_lv.out_fx,
-                                                                       sn_lv.attr);
+    sl.m = coarsen_links(N, out_off, out_dst, nullptr, out_fx, node_sn, sl.n, sl.out_off, sl.out_dst,
+                            nullptr, sl.out_fx, sl.in_off, sl.in_src, nullptr, sl.in_fx, scratch, stream);
+    k_sn_out<<<blocks_for(nsn, 256, num_sms() * 32), 256, 0, stream>>>(sl.n, sl.out_off, sl.out_fx,
+                                                                       sl.attr);
     RMX_LAUNCHED();
     scratch.release(mk);
     timers.end(kTimerCoarsen, stream);
@@ -709,7 +728,7 @@ void rmx_graph::generate_sub_modules() {
 
 // One superstep (stochastic_greedy_partition, OmpRelaxmap.cpp:263-429).
 double rmx_graph::stage(bool fine, double L) {
-    Level &lv = fine ? node_lv : sn_lv;
+    Level &lv = fine ? node_lv : sn();
     count_units(lv, mods, stream);
     // Node sweeps may open a new module only once member lists exist, i.e.
     // after the first superstep (members.size() > 1 test, Module.cpp:1435);
@@ -718,10 +737,12 @@ double rmx_graph::stage(bool fine, double L) {
     L = stage_sweeps(lv, allow_first, L);
     if (!fine) project_sn_to_nodes();
     double oldL;
+    bool from_sn = !fine;  // after node sweeps the first conversion reads the node links
     do {
         oldL = L;
-        convert_to_supernodes();
-        L = stage_sweeps(sn_lv, true, L);
+        convert_to_supernodes(from_sn);
+        from_sn = true;
+        L = stage_sweeps(sn(), true, L);
         project_sn_to_nodes();
     } while ((oldL - L) / kLn2 > opt.threshold);
     return L;

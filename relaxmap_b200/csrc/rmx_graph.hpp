@@ -30,7 +30,10 @@ struct rmx_graph {
     rmx::fx_t *s0 = nullptr;
     int64_t *dtmp = nullptr;  // small device scratch (counters)
 
-    rmx::Level node_lv, sn_lv, sub_lv;
+    rmx::Level node_lv, sub_lv;
+    rmx::Level sn_buf[2];  // super-node levels: the current one and the next conversion's target
+    int sn_cur = 0;
+    rmx::Level &sn() { return sn_buf[sn_cur]; }
     rmx::ModState mods, submods;
     rmx::InstState inst1, instsub;
     rmx::SweepWork work;
@@ -69,7 +72,7 @@ struct rmx_graph {
     double stage(bool fine, double L);
     double stage_sweeps(rmx::Level &lv, bool allow_new, double L);
     double sweep_single(rmx::Level &lv, bool prior, bool allow_new, double vthresh, int64_t &n_active);
-    void convert_to_supernodes();
+    void convert_to_supernodes(bool from_sn);
     void generate_sub_modules();
     void project_sn_to_nodes();
     int32_t count_modules();
