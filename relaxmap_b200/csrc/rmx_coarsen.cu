@@ -14,6 +14,7 @@
 //   4. rows come out sorted by destination; a stable sort of the pair list by
 //      destination gives the in-links in ascending source order.
 #include <algorithm>
+#include <climits>
 
 #include "rmx_engine.cuh"
 
@@ -158,6 +159,354 @@ int64_t coarsen_links(int32_t n, const int64_t *out_off, const int32_t *out_dst,
     scan_exclusive(g_in_off, g_in_off, ng + 1, nullptr, ar, s);
     ar.release(mk);
     return H;
+}
+
+}  // namespace rmx
+
+// ---------------------------------------------------------------------------
+// Engine aggregation by hashing (fixed-point flows only).
+//
+// The move engine needs the group links' fixed-point sums, which are exact in
+// any order, and it never depends on the order of links inside a row. So
+// instead of sorting every crossing link, the members of each group are
+// listed (counting sort by group), and one warp (small groups) or one block
+// (large groups) per group sums its members' links into a hash table keyed
+// by the destination group, in shared memory or, for the largest groups, in a
+// per-block slice of a global table. The rows are then packed and transposed
+// with a counting sort by destination.
+namespace rmx {
+
+constexpr unsigned kFullMask = 0xffffffffu;
+constexpr int32_t kNoKey = -1;
+constexpr int kAggWarpLinks = 128, kAggWarpCap = 256, kAggWarps = 8;
+constexpr int kAggT = 512, kAggCap = 8192;
+
+__device__ __forceinline__ uint32_t agg_hash(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352dU;
+    x ^= x >> 15;
+    x *= 0x846ca68bU;
+    x ^= x >> 16;
+    return x;
+}
+
+// Slot of key (inserted if absent; fresh = it was absent), or -1 if the table is full.
+__device__ __forceinline__ int agg_insert(int32_t *keys, int mask, int32_t key, bool &fresh) {
+    int s = (int)(agg_hash((uint32_t)key) & (uint32_t)mask);
+    for (int probe = 0; probe <= mask; probe++) {
+        const int32_t prev = atomicCAS(keys + s, kNoKey, key);
+        if (prev == kNoKey || prev == key) {
+            fresh = prev == kNoKey;
+            return s;
+        }
+        s = (s + 1) & mask;
+    }
+    return -1;
+}
+
+__global__ void k_agg_count(int32_t n, const int64_t *off, const int32_t *group, unsigned long long *gcnt,
+                            unsigned long long *glinks) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t g = group[r];
+        atomicAdd(gcnt + g, 1ull);
+        atomicAdd(glinks + g, (unsigned long long)(off[r + 1] - off[r]));
+    }
+}
+
+__global__ void k_agg_members(int32_t n, const int32_t *group, const int64_t *gmoff, unsigned long long *gfill,
+                              int32_t *members) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t g = group[r];
+        members[gmoff[g] + (int64_t)atomicAdd(gfill + g, 1ull)] = (int32_t)r;
+    }
+}
+
+__global__ void k_agg_bins(int32_t ng, const int64_t *gloff, uint8_t *small, uint8_t *large,
+                           unsigned long long *maxlinks) {
+    unsigned long long mx = 0;
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t l = gloff[g + 1] - gloff[g];
+        small[g] = l <= kAggWarpLinks ? 1 : 0;
+        large[g] = l > kAggWarpLinks ? 1 : 0;
+        mx = max(mx, (unsigned long long)l);
+    }
+    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFullMask, mx, o));
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(maxlinks, mx);
+}
+
+struct AggArgs {
+    const int64_t *off;
+    const int32_t *dst;
+    const fx_t *fx;
+    const int32_t *group;
+    const int64_t *gmoff, *gloff;
+    const int32_t *members;
+    int32_t *slab_dst;  // packed rows at gloff[g] (capacity = member links)
+    fx_t *slab_fx;
+    int64_t *rowlen;
+    fx_t *rowsum;        // optional: sum of the row's flows (out-flow of the group)
+    const int32_t *list; // groups of this bin
+    const int64_t *count;
+    int32_t *gkeys;      // global tables for groups too large for shared memory
+    fx_t *gvals;
+    int64_t gcap;
+    int32_t ngroups;
+};
+
+// One group by a team of NT threads (r = rank); keys/vals: a table of cap
+// slots. A table sized below twice the group's link count may hold at most
+// `limit` distinct keys: past that the group is abandoned (returns false,
+// uniformly across the team) and nothing of it is written. wsh: NT/32 + 2 ints.
+template <int NT>
+__device__ __forceinline__ bool agg_group(const AggArgs &a, int32_t g, int r, int32_t *keys, fx_t *vals, int64_t cap,
+                                          int limit, int *wsh) {
+    const int lane = r & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int mask = (int)(cap - 1);
+    int *nkeys = wsh + NT / 32 + 1;
+    for (int64_t s = r; s < cap; s += NT) {
+        keys[s] = kNoKey;
+        vals[s] = 0;
+    }
+    if (NT > 32 && r == 0) *nkeys = 0;
+    if (NT == 32) __syncwarp(); else __syncthreads();
+    const int64_t mb = a.gmoff[g], me = a.gmoff[g + 1];
+    for (int64_t m = mb + (r >> 5); m < me; m += NT / 32) {  // a warp per member, lanes over its links
+        if (NT > 32 && *(volatile int *)nkeys > limit) break;
+        const int32_t u = a.members[m];
+        for (int64_t e = a.off[u] + lane; e < a.off[u + 1]; e += 32) {
+            const int32_t b = a.group[a.dst[e]];
+            if (b == g) continue;
+            bool fresh;
+            const int s = agg_insert(keys, mask, b, fresh);
+            if (s < 0) break;  // only a table sized below the bound can fill up; nkeys > limit already
+            if (NT > 32 && fresh) atomicAdd(nkeys, 1);
+            atomicAdd(reinterpret_cast<unsigned long long *>(vals + s), (unsigned long long)a.fx[e]);
+        }
+    }
+    if (NT == 32) __syncwarp(); else __syncthreads();
+    if (NT > 32 && *nkeys > limit) {
+        __syncthreads();  // every thread has read the count before the next group resets it
+        return false;
+    }
+    // pack the occupied slots into the group's slab: every warp counts its own
+    // contiguous slice, a scan over the warps gives the offsets, then writes
+    const int64_t base_out = a.gloff[g];
+    const int64_t seg = cap / (NT / 32), lo = (int64_t)(r >> 5) * seg, hi = lo + seg;
+    int cnt = 0;
+    for (int64_t base = lo; base < hi; base += 32) {
+        const int64_t s = base + lane;
+        cnt += __popc(__ballot_sync(kFullMask, s < hi && keys[s] != kNoKey));
+    }
+    int woff = 0, nout = cnt;
+    if (NT > 32) {
+        if (lane == 0) wsh[r >> 5] = cnt;
+        __syncthreads();
+        if (r < 32) {
+            int x = r < NT / 32 ? wsh[r] : 0;
+            const int own = x;
+#pragma unroll
+            for (int q = 1; q < 32; q <<= 1) {
+                const int y = __shfl_up_sync(kFullMask, x, q);
+                if (r >= q) x += y;
+            }
+            if (r < NT / 32) wsh[r] = x - own;
+            if (r == 31) wsh[NT / 32] = x;
+        }
+        __syncthreads();
+        woff = wsh[r >> 5];
+        nout = wsh[NT / 32];
+    }
+    fx_t sum = 0;
+    int done = 0;
+    for (int64_t base = lo; base < hi; base += 32) {
+        const int64_t s = base + lane;
+        const int32_t k = s < hi ? keys[s] : kNoKey;
+        const bool occ = k != kNoKey;
+        const unsigned bal = __ballot_sync(kFullMask, occ);
+        if (occ) {
+            const int64_t p = base_out + woff + done + __popc(bal & lt);
+            a.slab_dst[p] = k;
+            a.slab_fx[p] = vals[s];
+            sum += vals[s];
+        }
+        done += __popc(bal);
+    }
+    if (a.rowsum) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(kFullMask, sum, o);
+        if (lane == 0 && sum) atomicAdd(reinterpret_cast<unsigned long long *>(a.rowsum + g), (unsigned long long)sum);
+    }
+    if (r == 0) a.rowlen[g] = nout;
+    if (NT == 32) __syncwarp(); else __syncthreads();
+    return true;
+}
+
+__global__ void __launch_bounds__(kAggWarps * 32) k_agg_warp(AggArgs a) {
+    __shared__ int32_t skeys[kAggWarps][kAggWarpCap];
+    __shared__ fx_t svals[kAggWarps][kAggWarpCap];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t n = *a.count;
+    for (int64_t i = (int64_t)blockIdx.x * kAggWarps + w; i < n; i += (int64_t)gridDim.x * kAggWarps) {
+        const int32_t g = a.list[i];
+        const int64_t links = a.gloff[g + 1] - a.gloff[g];
+        int64_t cap = 32;
+        while (cap < 2 * links) cap <<= 1;
+        agg_group<32>(a, g, lane, skeys[w], svals[w], cap, INT_MAX, nullptr);
+    }
+}
+
+// Large groups: distinct destination groups are usually far fewer than links
+// (most links of a module go to a few neighbours), so every group first tries
+// the shared-memory table, kept at most 3/4 full, and only a group with more
+// distinct neighbours than that is redone in a global slice sized by its links.
+__global__ void __launch_bounds__(kAggT, 2) k_agg_block(AggArgs a) {
+    extern __shared__ __align__(16) unsigned char dsm[];
+    __shared__ int wsh[kAggT / 32 + 2];
+    fx_t *svals = reinterpret_cast<fx_t *>(dsm);
+    int32_t *skeys = reinterpret_cast<int32_t *>(svals + kAggCap);
+    const int64_t n = *a.count;
+    for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int32_t g = a.list[i];
+        const int64_t bound = min(a.gloff[g + 1] - a.gloff[g], (int64_t)a.ngroups);
+        int64_t cap = 64;
+        while (cap < 2 * bound) cap <<= 1;
+        if (cap <= kAggCap) {
+            agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh);
+        } else if (!agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, kAggCap, kAggCap / 4 * 3, wsh)) {
+            agg_group<kAggT>(a, g, threadIdx.x, a.gkeys + (int64_t)blockIdx.x * a.gcap,
+                             a.gvals + (int64_t)blockIdx.x * a.gcap, cap, INT_MAX, wsh);
+        }
+    }
+}
+
+__global__ void k_agg_pack(int32_t ng, const int64_t *gloff, const int64_t *g_out_off, const int32_t *slab_dst,
+                           const fx_t *slab_fx, int32_t *out_dst, fx_t *out_fx, unsigned long long *colcnt) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t g = gw; g < ng; g += nw) {
+        const int64_t src = gloff[g], o = g_out_off[g], len = g_out_off[g + 1] - o;
+        for (int64_t j = lane; j < len; j += 32) {
+            const int32_t b = slab_dst[src + j];
+            out_dst[o + j] = b;
+            out_fx[o + j] = slab_fx[src + j];
+            atomicAdd(colcnt + b, 1ull);
+        }
+    }
+}
+
+__global__ void k_agg_transpose(int32_t ng, const int64_t *g_out_off, const int32_t *out_dst, const fx_t *out_fx,
+                                const int64_t *g_in_off, unsigned long long *colfill, int32_t *in_src, fx_t *in_fx) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t g = gw; g < ng; g += nw)
+        for (int64_t e = g_out_off[g] + lane; e < g_out_off[g + 1]; e += 32) {
+            const int32_t b = out_dst[e];
+            const int64_t q = g_in_off[b] + (int64_t)atomicAdd(colfill + b, 1ull);
+            in_src[q] = (int32_t)g;
+            in_fx[q] = out_fx[e];
+        }
+}
+
+int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *group,
+                        int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx, int64_t *g_in_off,
+                        int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, fx_t *&gtab, int64_t &gtab_cap, Arena &ar,
+                        cudaStream_t s) {
+    static bool configured = false;
+    if (!configured) {
+        const int smem = (int)(kAggCap * (sizeof(fx_t) + sizeof(int32_t)));
+        RMX_CUDA(cudaFuncSetAttribute(k_agg_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        configured = true;
+    }
+    int64_t E = 0;
+    RMX_CUDA(cudaMemcpyAsync(&E, off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    if (rowsum) RMX_CUDA(cudaMemsetAsync(rowsum, 0, sizeof(fx_t) * std::max(ng, 1), s));
+    if (ng <= 0) return 0;
+    size_t mk = ar.mark();
+    const unsigned G = num_sms() * 16;
+    int64_t *gmoff = ar.alloc<int64_t>(ng + 1), *gloff = ar.alloc<int64_t>(ng + 1);
+    unsigned long long *fill = ar.alloc<unsigned long long>(ng + 1);
+    int64_t *tot = ar.alloc<int64_t>(4);
+    RMX_CUDA(cudaMemsetAsync(gmoff, 0, sizeof(int64_t) * (ng + 1), s));
+    RMX_CUDA(cudaMemsetAsync(gloff, 0, sizeof(int64_t) * (ng + 1), s));
+    k_agg_count<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, off, group,
+                                                                    reinterpret_cast<unsigned long long *>(gmoff),
+                                                                    reinterpret_cast<unsigned long long *>(gloff));
+    RMX_LAUNCHED();
+    scan_exclusive(gmoff, gmoff, ng + 1, nullptr, ar, s);
+    scan_exclusive(gloff, gloff, ng + 1, nullptr, ar, s);
+    int32_t *members = ar.alloc<int32_t>(std::max(n, 1));
+    RMX_CUDA(cudaMemsetAsync(fill, 0, sizeof(unsigned long long) * (ng + 1), s));
+    k_agg_members<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, group, gmoff, fill, members);
+    RMX_LAUNCHED();
+    // largest group (links) for the global tables
+    std::vector<int64_t> hl(2);
+    uint8_t *fsmall = ar.alloc<uint8_t>(ng), *flarge = ar.alloc<uint8_t>(ng);
+    RMX_CUDA(cudaMemsetAsync(tot, 0, sizeof(int64_t) * 4, s));
+    k_agg_bins<<<blocks_for(ng, 256, num_sms() * 32), 256, 0, s>>>(ng, gloff, fsmall, flarge,
+                                                                   reinterpret_cast<unsigned long long *>(tot + 3));
+    RMX_LAUNCHED();
+    int32_t *lsmall = ar.alloc<int32_t>(ng), *llarge = ar.alloc<int32_t>(ng);
+    compact_flags(fsmall, ng, lsmall, tot + 0, ar, s);
+    compact_flags(flarge, ng, llarge, tot + 1, ar, s);
+    int32_t *slab_dst = ar.alloc<int32_t>(std::max<int64_t>(E, 1));
+    fx_t *slab_fx = ar.alloc<fx_t>(std::max<int64_t>(E, 1));
+    int64_t *rowlen = g_out_off;  // row lengths, scanned in place into offsets below
+    RMX_CUDA(cudaMemsetAsync(rowlen, 0, sizeof(int64_t) * (ng + 1), s));
+    // a group of L links needs a table of next_pow2(2L) slots; beyond shared memory, a global slice per block
+    int64_t maxlinks = 0;
+    RMX_CUDA(cudaMemcpyAsync(&maxlinks, tot + 3, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    int64_t need = 64;
+    while (need < 2 * std::min<int64_t>(maxlinks, ng)) need <<= 1;
+    const int nblk = num_sms() * 2;
+    if (need > kAggCap && need > gtab_cap) {
+        RMX_CUDA(cudaStreamSynchronize(s));
+        if (gtab) cudaFree(gtab);
+        gtab = nullptr;
+        RMX_CUDA(cudaMalloc(&gtab, (sizeof(fx_t) + sizeof(int32_t)) * need * nblk));
+        gtab_cap = need;
+    }
+    AggArgs a;
+    a.off = off;
+    a.dst = dst;
+    a.fx = fx;
+    a.group = group;
+    a.gmoff = gmoff;
+    a.gloff = gloff;
+    a.members = members;
+    a.slab_dst = slab_dst;
+    a.slab_fx = slab_fx;
+    a.rowlen = rowlen;
+    a.rowsum = rowsum;
+    a.gvals = gtab;
+    a.gkeys = gtab ? reinterpret_cast<int32_t *>(gtab + gtab_cap * nblk) : nullptr;
+    a.gcap = gtab_cap;
+    a.ngroups = ng;
+    a.list = lsmall;
+    a.count = tot + 0;
+    k_agg_warp<<<num_sms() * 8, kAggWarps * 32, 0, s>>>(a);
+    RMX_LAUNCHED();
+    a.list = llarge;
+    a.count = tot + 1;
+    k_agg_block<<<nblk, kAggT, kAggCap * (sizeof(fx_t) + sizeof(int32_t)), s>>>(a);
+    RMX_LAUNCHED();
+    scan_exclusive(rowlen, g_out_off, ng + 1, tot + 2, ar, s);
+    RMX_CUDA(cudaMemsetAsync(g_in_off, 0, sizeof(int64_t) * (ng + 1), s));
+    k_agg_pack<<<G, 256, 0, s>>>(ng, gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx,
+                                 reinterpret_cast<unsigned long long *>(g_in_off));
+    RMX_LAUNCHED();
+    scan_exclusive(g_in_off, g_in_off, ng + 1, nullptr, ar, s);
+    RMX_CUDA(cudaMemsetAsync(fill, 0, sizeof(unsigned long long) * (ng + 1), s));
+    k_agg_transpose<<<G, 256, 0, s>>>(ng, g_out_off, g_out_dst, g_out_fx, g_in_off, fill, g_in_src, g_in_fx);
+    RMX_LAUNCHED();
+    int64_t m = 0;
+    RMX_CUDA(cudaMemcpyAsync(&m, tot + 2, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    ar.release(mk);
+    (void)hl;
+    return m;
 }
 
 }  // namespace rmx

@@ -151,12 +151,9 @@ __global__ void k_sn_from_nodes(int32_t n, const int32_t *node_sn, const int32_t
     }
 }
 
-__global__ void k_sn_out(int32_t n, const int64_t *off, const fx_t *fx, Stat4 *attr) {
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x) {
-        fx_t o = 0;
-        for (int64_t e = off[s]; e < off[s + 1]; e++) o += fx[e];
-        attr[s].OUT = o;
-    }
+__global__ void k_sn_set_out(int32_t n, const fx_t *rowsum, Stat4 *attr) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
+        attr[s].OUT = rowsum[s];
 }
 
 __global__ void k_count_nonzero(int32_t cap, const int32_t *count, unsigned long long *out) {
@@ -322,6 +319,7 @@ rmx_graph::~rmx_graph() {
         if (e) cudaEventDestroy(e);
     if (work.gtable) cudaFree(work.gtable);
     if (work.gkeys) cudaFree(work.gkeys);
+    if (agg_tab) cudaFree(agg_tab);
     perm.destroy();
     scratch.destroy();
     if (stream) cudaStreamDestroy(stream);
@@ -615,12 +613,12 @@ void rmx_graph::convert_to_supernodes(bool from_sn) {
     RMX_CUDA(cudaStreamSynchronize(stream));
     dst.n = (int32_t)nsn;
     if (from_sn)
-        dst.m = coarsen_links(src.n, src.out_off, src.out_dst, nullptr, src.out_fx, group, dst.n, dst.out_off,
-                              dst.out_dst, nullptr, dst.out_fx, dst.in_off, dst.in_src, nullptr, dst.in_fx, scratch,
-                              stream);
+        dst.m = aggregate_links(src.n, src.out_off, src.out_dst, src.out_fx, group, dst.n, dst.out_off, dst.out_dst,
+                                dst.out_fx, dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_tab, agg_cap, scratch,
+                                stream);
     else
-        dst.m = coarsen_links(N, out_off, out_dst, nullptr, out_fx, node_sn, dst.n, dst.out_off, dst.out_dst, nullptr,
-                              dst.out_fx, dst.in_off, dst.in_src, nullptr, dst.in_fx, scratch, stream);
+        dst.m = aggregate_links(N, out_off, out_dst, out_fx, node_sn, dst.n, dst.out_off, dst.out_dst, dst.out_fx,
+                                dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_tab, agg_cap, scratch, stream);
     scratch.release(mk);
     sn_cur = 1 - sn_cur;
     count_units(sn(), mods, stream);
@@ -717,11 +715,13 @@ void rmx_graph::generate_sub_modules() {
     k_sn_from_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, node_sn, nmod, nattr, sl.mod,
                                                                             sl.attr, sl.nnodes);
     RMX_LAUNCHED();
-    sl.m = coarsen_links(N, out_off, out_dst, nullptr, out_fx, node_sn, sl.n, sl.out_off, sl.out_dst,
-                            nullptr, sl.out_fx, sl.in_off, sl.in_src, nullptr, sl.in_fx, scratch, stream);
-    k_sn_out<<<blocks_for(nsn, 256, num_sms() * 32), 256, 0, stream>>>(sl.n, sl.out_off, sl.out_fx,
-                                                                       sl.attr);
-    RMX_LAUNCHED();
+    {
+        fx_t *rowsum = scratch.alloc<fx_t>(std::max<int64_t>(nsn, 1));
+        sl.m = aggregate_links(N, out_off, out_dst, out_fx, node_sn, sl.n, sl.out_off, sl.out_dst, sl.out_fx,
+                               sl.in_off, sl.in_src, sl.in_fx, rowsum, agg_tab, agg_cap, scratch, stream);
+        k_sn_set_out<<<blocks_for(nsn, 256, num_sms() * 32), 256, 0, stream>>>(sl.n, rowsum, sl.attr);
+        RMX_LAUNCHED();
+    }
     scratch.release(mk);
     timers.end(kTimerCoarsen, stream);
 }

@@ -171,4 +171,13 @@ int64_t coarsen_links(int32_t n, const int64_t *out_off, const int32_t *out_dst,
                       double *g_out_f, fx_t *g_out_fx, int64_t *g_in_off, int32_t *g_in_src, double *g_in_f,
                       fx_t *g_in_fx, Arena &ar, cudaStream_t s);
 
+// Engine aggregation of rows (nodes or super-nodes) into groups by hashing:
+// fixed-point sums only, rows and columns in no particular order. rowsum (may
+// be NULL) receives each group's total out-flow. gtab / gtab_cap: a global
+// table grown on demand for groups too large for shared memory.
+int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *group,
+                        int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx, int64_t *g_in_off,
+                        int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, fx_t *&gtab, int64_t &gtab_cap, Arena &ar,
+                        cudaStream_t s);
+
 }  // namespace rmx

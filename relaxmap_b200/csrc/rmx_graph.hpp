@@ -38,6 +38,8 @@ struct rmx_graph {
     rmx::InstState inst1, instsub;
     rmx::SweepWork work;
     rmx::Timers timers;
+    rmx::fx_t *agg_tab = nullptr;  // global hash tables of the link aggregation (grown on demand)
+    int64_t agg_cap = 0;
 
     // ---- state
     bool initiated = false;

@@ -224,7 +224,6 @@ template <int NT>
 struct GroupShared {  // reductions across the warps of a block group
     double best[NT / 32];
     int32_t mod[NT / 32];
-    int wpos[NT / 32];
     int ncand;
 };
 
@@ -260,67 +259,37 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
     const int sA = tab_find(keys, mask, A);
     const fx_t oA = sA >= 0 ? vo[sA] : 0, iA = sA >= 0 ? vi[sA] : 0;
     const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
+    if (NT > 32) __syncthreads();  // every lookup is done before slots are overwritten
+    // Each warp compacts its own contiguous slice of the table in place (the
+    // dense position never passes the slot being read) and evaluates it.
+    const int64_t seg = cap / (NT / 32), lo = (int64_t)(r >> 5) * seg, hi = lo + seg;
     int nc = 0;
-    if (NT == 32) {
-        for (int64_t base = 0; base < cap; base += 32) {
-            const int64_t s = base + lane;
-            const int32_t k = keys[s];
-            const fx_t o = vo[s], i2 = vi[s];
-            const bool occ = k != kEmpty && k != A;
-            const unsigned bal = __ballot_sync(kFull, occ);
-            __syncwarp();
-            if (occ) {
-                const int p = nc + __popc(bal & lt);
-                ck[p] = k;
-                co[p] = o;
-                ci[p] = i2;
-            }
-            nc += __popc(bal);
+    for (int64_t base = lo; base < hi; base += 32) {
+        const int64_t s = base + lane;
+        int32_t k = kEmpty;
+        fx_t o = 0, i2 = 0;
+        if (s < hi) {
+            k = keys[s];
+            o = vo[s];
+            i2 = vi[s];
         }
+        const bool occ = k != kEmpty && k != A;
+        const unsigned bal = __ballot_sync(kFull, occ);
         __syncwarp();
-    } else {
-        // chunks of NT slots in order; a block-wide scan of the occupancy gives
-        // every candidate its dense position, which never exceeds its slot
-        for (int64_t base = 0; base < cap; base += NT) {
-            const int64_t s = base + r;
-            int32_t k = kEmpty;
-            fx_t o = 0, i2 = 0;
-            if (s < cap) {
-                k = keys[s];
-                o = vo[s];
-                i2 = vi[s];
-            }
-            const bool occ = k != kEmpty && k != A;
-            const unsigned bal = __ballot_sync(kFull, occ);
-            if (lane == 0) sh->wpos[r >> 5] = __popc(bal);
-            __syncthreads();
-            if (r < 32) {
-                int v = r < NT / 32 ? sh->wpos[r] : 0;
-                const int own = v;
-#pragma unroll
-                for (int q = 1; q < 32; q <<= 1) {
-                    const int y = __shfl_up_sync(kFull, v, q);
-                    if (r >= q) v += y;
-                }
-                if (r < NT / 32) sh->wpos[r] = v - own;
-                if (r == 31) sh->ncand = v;
-            }
-            __syncthreads();
-            if (occ) {
-                const int p = nc + sh->wpos[r >> 5] + __popc(bal & lt);
-                ck[p] = k;
-                co[p] = o;
-                ci[p] = i2;
-            }
-            nc += sh->ncand;
-            __syncthreads();
+        if (occ) {
+            const int64_t p = lo + nc + __popc(bal & lt);
+            ck[p] = k;
+            co[p] = o;
+            ci[p] = i2;
         }
+        nc += __popc(bal);
     }
+    __syncwarp();
     double best = 0.0;
     int32_t bm = INT_MAX;
-    for (int q = r; q < nc; q += NT) {
-        const int32_t m = ck[q];
-        const double dl = candidate_delta(c, a.mstat[m], a.mterm[m], co[q], ci[q]);
+    for (int q = lane; q < nc; q += 32) {
+        const int32_t m = ck[lo + q];
+        const double dl = candidate_delta(c, a.mstat[m], a.mterm[m], co[lo + q], ci[lo + q]);
         if (better(dl, m, best, bm)) {
             best = dl;
             bm = m;
@@ -350,10 +319,10 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
                 }
     }
     int act = 0;
+    if (lane == 0) cands += nc;
     if (r == 0) {
         act = finish_unit(a, u, c, best, bm);
         seen += d;
-        cands += nc;
     }
     if (a.mark) {
         if (NT == 32) {
@@ -508,6 +477,13 @@ __device__ __forceinline__ void flush_stats(const EvalArgs &a, unsigned long lon
     }
 }
 
+__device__ __forceinline__ void flush_stats_split(const EvalArgs &a, unsigned long long seen, unsigned long long units,
+                                                  unsigned long long cands) {
+    if (seen) atomicAdd(a.stats + 0, seen);
+    if (units) atomicAdd(a.stats + 1, units);
+    if (cands) atomicAdd(a.stats + 2, cands);
+}
+
 __global__ void __launch_bounds__(kEvalWarps * 32, 3) k_eval_warp(EvalArgs a) {
     __shared__ int32_t skey[kEvalWarps][kWarpCap];
     __shared__ fx_t sout[kEvalWarps][kWarpCap];
@@ -529,7 +505,7 @@ __global__ void __launch_bounds__(kEvalWarps * 32, 3) k_eval_warp(EvalArgs a) {
 }
 
 template <int NT, int CAP, bool GLOBAL>
-__global__ void __launch_bounds__(NT) k_eval_block(EvalArgs a) {
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 3) k_eval_block(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ GroupShared<NT> sh;
     int32_t *keys;
@@ -555,7 +531,8 @@ __global__ void __launch_bounds__(NT) k_eval_block(EvalArgs a) {
         eval_unit<NT>(a, u, threadIdx.x, keys, vo, vi, keys, vo, vi, &sh, seen, cands);
         units++;
     }
-    if (threadIdx.x == 0) flush_stats(a, seen, units, cands);
+    // every warp found its own share of the candidates; thread 0 alone counted the links
+    if ((threadIdx.x & 31) == 0) flush_stats_split(a, threadIdx.x == 0 ? seen : 0, threadIdx.x == 0 ? units : 0, cands);
 }
 
 // ---------------------------------------------------------------- commit
