@@ -35,14 +35,15 @@ METRIC = "edges/s per full run"
 UNIT = "edges/s"
 
 
-def workload(name: str):
+def workload(name: str, nodes: int | None = None):
     from relaxmap_b200 import synth
     if name == "small":
         g = synth.config_small(seed=42)
         desc = "planted partition N=1000, out-degree power law 2 (mean 20, max 50), communities [10,50], mu=0.3, unweighted"
     elif name == "mid":
-        g = synth.config_mid(seed=42)
-        desc = ("planted partition N=1,000,000, out-degree power law 2 (mean 20, max 1000), communities power law "
+        n = nodes or 1_000_000
+        g = synth.config_mid(seed=42, n=n)
+        desc = (f"planted partition N={n:,}, out-degree power law 2 (mean 20, max 1000), communities power law "
                 "[20,1000], mu=0.4, weights U[1,10]")
     elif name.startswith("rmat"):
         scale = int(name[4:])
@@ -157,6 +158,22 @@ def ncu_traffic():
     return None
 
 
+def profile_run(g, desc: str):
+    """One graph build, flow and optimiser run: the unit that ncu launch lists
+    and kernel captures are taken over."""
+    from relaxmap_b200 import Graph
+    G = Graph.from_edges(g.src, g.dst, g.w, n=g.n)
+    G.initiate()
+    G.set_profiling(True)
+    t0 = time.perf_counter()
+    r = G.optimize(seed=1)
+    dt = time.perf_counter() - t0
+    p = G.profile()
+    G.close()
+    print(json.dumps({"workload": desc, "nodes": g.n, "links": g.m, "seconds": dt, "L_bits": r["L_bits"],
+                      "n_modules": r["n_modules"], "profile": p}))
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -172,6 +189,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mid")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nodes", type=int, default=None, help="mid workload: node count (smaller profiling cases)")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="build the graph, then exactly one optimiser run (seed 1); prints the engine counters "
+                         "(the command profiled by ncu)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
 
@@ -195,8 +216,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
 
-    g, desc = workload(args.workload)
+    g, desc = workload(args.workload, args.nodes)
     E = g.m
+    if args.profile_run:
+        profile_run(g, desc)
+        return
     # ---- resident graph
     G = Graph.from_edges(g.src, g.dst, g.w, n=g.n)
     G.initiate()

@@ -198,6 +198,19 @@ constexpr int kWarpMaxDeg = 128, kWarpCap = 256, kEvalWarps = 8;
 constexpr int kBins = 7;
 constexpr int kBinReg8 = 0, kBinReg16 = 1, kBinReg32 = 2, kBinWarp = 3, kBinBlock = 4, kBinLarge = 5, kBinHub = 6;
 constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
+// resident blocks per SM of the block bin and grid multipliers of the bins
+#ifndef RMX_BLK_MINB
+#define RMX_BLK_MINB 4
+#endif
+#ifndef RMX_BLK_GRID
+#define RMX_BLK_GRID 4
+#endif
+#ifndef RMX_WARP_GRID
+#define RMX_WARP_GRID 3
+#endif
+#ifndef RMX_REG_GRID
+#define RMX_REG_GRID 8
+#endif
 constexpr int kLrgT = 512, kLrgMaxDeg = 4096, kLrgCap = 8192;
 constexpr int kHubT = 512;
 
@@ -505,7 +518,7 @@ __global__ void __launch_bounds__(kEvalWarps * 32, 3) k_eval_warp(EvalArgs a) {
 }
 
 template <int NT, int CAP, bool GLOBAL>
-__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : 3) k_eval_block(EvalArgs a) {
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : RMX_BLK_MINB) k_eval_block(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ GroupShared<NT> sh;
     int32_t *keys;
@@ -900,7 +913,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     RMX_CUDA(cudaEventRecord(W.fork, s));
     for (int k = 0; k < 3; k++) RMX_CUDA(cudaStreamWaitEvent(W.aux[k], W.fork, 0));
     a.range = bucket_off + first_bucket + kBinBlock;
-    k_eval_block<kBlkT, kBlkCap, false><<<num_sms() * 2, kBlkT, kBlkSmem, W.aux[0]>>>(a);
+    k_eval_block<kBlkT, kBlkCap, false><<<num_sms() * RMX_BLK_GRID, kBlkT, kBlkSmem, W.aux[0]>>>(a);
     RMX_LAUNCHED();
     a.range = bucket_off + first_bucket + kBinLarge;
     k_eval_block<kLrgT, kLrgCap, false><<<num_sms(), kLrgT, kLrgSmem, W.aux[1]>>>(a);
@@ -911,10 +924,10 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
         RMX_LAUNCHED();
     }
     a.range = bucket_off + first_bucket + kBinWarp;
-    k_eval_warp<<<num_sms() * 3, kEvalWarps * 32, 0, W.aux[2]>>>(a);
+    k_eval_warp<<<num_sms() * RMX_WARP_GRID, kEvalWarps * 32, 0, W.aux[2]>>>(a);
     RMX_LAUNCHED();
     a.range = bucket_off + first_bucket + kBinReg8;
-    k_eval_reg<<<num_sms() * 8, 256, 0, s>>>(a);
+    k_eval_reg<<<num_sms() * RMX_REG_GRID, 256, 0, s>>>(a);
     RMX_LAUNCHED();
     for (int k = 0; k < 3; k++) {
         RMX_CUDA(cudaEventRecord(W.join[k], W.aux[k]));
