@@ -179,6 +179,7 @@ namespace rmx {
 constexpr unsigned kFullMask = 0xffffffffu;
 constexpr int32_t kNoKey = -1;
 constexpr int kAggWarpLinks = 128, kAggWarpCap = 256, kAggWarps = 8;
+constexpr int kAggMidT = 128, kAggMidLinks = 1024, kAggMidCap = 2048;
 constexpr int kAggT = 512, kAggCap = 8192;
 
 __device__ __forceinline__ uint32_t agg_hash(uint32_t x) {
@@ -221,13 +222,16 @@ __global__ void k_agg_members(int32_t n, const int32_t *group, const int64_t *gm
     }
 }
 
-__global__ void k_agg_bins(int32_t ng, const int64_t *gloff, uint8_t *small, uint8_t *large,
+// Groups by the bound on their distinct neighbours, min(links, groups): a
+// warp (<= 128), a 128-thread block (<= 1024) or a 512-thread block.
+__global__ void k_agg_bins(int32_t ng, const int64_t *gloff, uint8_t *small, uint8_t *mid, uint8_t *large,
                            unsigned long long *maxlinks) {
     unsigned long long mx = 0;
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t l = gloff[g + 1] - gloff[g];
-        small[g] = l <= kAggWarpLinks ? 1 : 0;
-        large[g] = l > kAggWarpLinks ? 1 : 0;
+        const int64_t l = gloff[g + 1] - gloff[g], b = min(l, (int64_t)ng);
+        small[g] = b <= kAggWarpLinks ? 1 : 0;
+        mid[g] = b > kAggWarpLinks && b <= kAggMidLinks ? 1 : 0;
+        large[g] = b > kAggMidLinks ? 1 : 0;
         mx = max(mx, (unsigned long long)l);
     }
     for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFullMask, mx, o));
@@ -349,10 +353,24 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_agg_warp(AggArgs a) {
     const int64_t n = *a.count;
     for (int64_t i = (int64_t)blockIdx.x * kAggWarps + w; i < n; i += (int64_t)gridDim.x * kAggWarps) {
         const int32_t g = a.list[i];
-        const int64_t links = a.gloff[g + 1] - a.gloff[g];
+        const int64_t bound = min(a.gloff[g + 1] - a.gloff[g], (int64_t)a.ngroups);
         int64_t cap = 32;
-        while (cap < 2 * links) cap <<= 1;
+        while (cap < 2 * bound) cap <<= 1;
         agg_group<32>(a, g, lane, skeys[w], svals[w], cap, INT_MAX, nullptr);
+    }
+}
+
+__global__ void __launch_bounds__(kAggMidT) k_agg_mid(AggArgs a) {
+    __shared__ int32_t skeys[kAggMidCap];
+    __shared__ fx_t svals[kAggMidCap];
+    __shared__ int wsh[kAggMidT / 32 + 2];
+    const int64_t n = *a.count;
+    for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
+        const int32_t g = a.list[i];
+        const int64_t bound = min(a.gloff[g + 1] - a.gloff[g], (int64_t)a.ngroups);
+        int64_t cap = 64;
+        while (cap < 2 * bound) cap <<= 1;
+        agg_group<kAggMidT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh);
     }
 }
 
@@ -411,7 +429,7 @@ __global__ void k_agg_transpose(int32_t ng, const int64_t *g_out_off, const int3
 int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *group,
                         int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx, int64_t *g_in_off,
                         int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, fx_t *&gtab, int64_t &gtab_cap, Arena &ar,
-                        cudaStream_t s) {
+                        cudaStream_t s, const SweepWork *W) {
     static bool configured = false;
     if (!configured) {
         const int smem = (int)(kAggCap * (sizeof(fx_t) + sizeof(int32_t)));
@@ -427,7 +445,7 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     const unsigned G = num_sms() * 16;
     int64_t *gmoff = ar.alloc<int64_t>(ng + 1), *gloff = ar.alloc<int64_t>(ng + 1);
     unsigned long long *fill = ar.alloc<unsigned long long>(ng + 1);
-    int64_t *tot = ar.alloc<int64_t>(4);
+    int64_t *tot = ar.alloc<int64_t>(8);
     RMX_CUDA(cudaMemsetAsync(gmoff, 0, sizeof(int64_t) * (ng + 1), s));
     RMX_CUDA(cudaMemsetAsync(gloff, 0, sizeof(int64_t) * (ng + 1), s));
     k_agg_count<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, off, group,
@@ -442,13 +460,14 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     RMX_LAUNCHED();
     // largest group (links) for the global tables
     std::vector<int64_t> hl(2);
-    uint8_t *fsmall = ar.alloc<uint8_t>(ng), *flarge = ar.alloc<uint8_t>(ng);
-    RMX_CUDA(cudaMemsetAsync(tot, 0, sizeof(int64_t) * 4, s));
-    k_agg_bins<<<blocks_for(ng, 256, num_sms() * 32), 256, 0, s>>>(ng, gloff, fsmall, flarge,
+    uint8_t *fsmall = ar.alloc<uint8_t>(ng), *fmid = ar.alloc<uint8_t>(ng), *flarge = ar.alloc<uint8_t>(ng);
+    RMX_CUDA(cudaMemsetAsync(tot, 0, sizeof(int64_t) * 5, s));
+    k_agg_bins<<<blocks_for(ng, 256, num_sms() * 32), 256, 0, s>>>(ng, gloff, fsmall, fmid, flarge,
                                                                    reinterpret_cast<unsigned long long *>(tot + 3));
     RMX_LAUNCHED();
-    int32_t *lsmall = ar.alloc<int32_t>(ng), *llarge = ar.alloc<int32_t>(ng);
+    int32_t *lsmall = ar.alloc<int32_t>(ng), *lmid = ar.alloc<int32_t>(ng), *llarge = ar.alloc<int32_t>(ng);
     compact_flags(fsmall, ng, lsmall, tot + 0, ar, s);
+    compact_flags(fmid, ng, lmid, tot + 4, ar, s);
     compact_flags(flarge, ng, llarge, tot + 1, ar, s);
     int32_t *slab_dst = ar.alloc<int32_t>(std::max<int64_t>(E, 1));
     fx_t *slab_fx = ar.alloc<fx_t>(std::max<int64_t>(E, 1));
@@ -484,14 +503,31 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     a.gkeys = gtab ? reinterpret_cast<int32_t *>(gtab + gtab_cap * nblk) : nullptr;
     a.gcap = gtab_cap;
     a.ngroups = ng;
+    // the three bins run concurrently: warp and mid bins on the two auxiliary streams
+    cudaStream_t s_small = s, s_mid = s;
+    if (W) {
+        RMX_CUDA(cudaEventRecord(W->fork, s));
+        for (int k = 0; k < 2; k++) RMX_CUDA(cudaStreamWaitEvent(W->aux[k], W->fork, 0));
+        s_small = W->aux[0];
+        s_mid = W->aux[1];
+    }
     a.list = lsmall;
     a.count = tot + 0;
-    k_agg_warp<<<num_sms() * 8, kAggWarps * 32, 0, s>>>(a);
+    k_agg_warp<<<num_sms() * 8, kAggWarps * 32, 0, s_small>>>(a);
+    RMX_LAUNCHED();
+    a.list = lmid;
+    a.count = tot + 4;
+    k_agg_mid<<<num_sms() * 8, kAggMidT, 0, s_mid>>>(a);
     RMX_LAUNCHED();
     a.list = llarge;
     a.count = tot + 1;
     k_agg_block<<<nblk, kAggT, kAggCap * (sizeof(fx_t) + sizeof(int32_t)), s>>>(a);
     RMX_LAUNCHED();
+    if (W)
+        for (int k = 0; k < 2; k++) {
+            RMX_CUDA(cudaEventRecord(W->join[k], W->aux[k]));
+            RMX_CUDA(cudaStreamWaitEvent(s, W->join[k], 0));
+        }
     scan_exclusive(rowlen, g_out_off, ng + 1, tot + 2, ar, s);
     RMX_CUDA(cudaMemsetAsync(g_in_off, 0, sizeof(int64_t) * (ng + 1), s));
     k_agg_pack<<<G, 256, 0, s>>>(ng, gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx,

@@ -615,10 +615,10 @@ void rmx_graph::convert_to_supernodes(bool from_sn) {
     if (from_sn)
         dst.m = aggregate_links(src.n, src.out_off, src.out_dst, src.out_fx, group, dst.n, dst.out_off, dst.out_dst,
                                 dst.out_fx, dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_tab, agg_cap, scratch,
-                                stream);
+                                stream, &work);
     else
         dst.m = aggregate_links(N, out_off, out_dst, out_fx, node_sn, dst.n, dst.out_off, dst.out_dst, dst.out_fx,
-                                dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_tab, agg_cap, scratch, stream);
+                                dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_tab, agg_cap, scratch, stream, &work);
     scratch.release(mk);
     sn_cur = 1 - sn_cur;
     count_units(sn(), mods, stream);
@@ -718,7 +718,7 @@ void rmx_graph::generate_sub_modules() {
     {
         fx_t *rowsum = scratch.alloc<fx_t>(std::max<int64_t>(nsn, 1));
         sl.m = aggregate_links(N, out_off, out_dst, out_fx, node_sn, sl.n, sl.out_off, sl.out_dst, sl.out_fx,
-                               sl.in_off, sl.in_src, sl.in_fx, rowsum, agg_tab, agg_cap, scratch, stream);
+                               sl.in_off, sl.in_src, sl.in_fx, rowsum, agg_tab, agg_cap, scratch, stream, &work);
         k_sn_set_out<<<blocks_for(nsn, 256, num_sms() * 32), 256, 0, stream>>>(sl.n, rowsum, sl.attr);
         RMX_LAUNCHED();
     }

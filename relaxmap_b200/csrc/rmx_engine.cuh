@@ -174,10 +174,11 @@ int64_t coarsen_links(int32_t n, const int64_t *out_off, const int32_t *out_dst,
 // Engine aggregation of rows (nodes or super-nodes) into groups by hashing:
 // fixed-point sums only, rows and columns in no particular order. rowsum (may
 // be NULL) receives each group's total out-flow. gtab / gtab_cap: a global
-// table grown on demand for groups too large for shared memory.
+// table grown on demand for groups too large for shared memory. W (may be
+// NULL): auxiliary streams and events on which the size bins run concurrently.
 int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *group,
                         int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx, int64_t *g_in_off,
                         int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, fx_t *&gtab, int64_t &gtab_cap, Arena &ar,
-                        cudaStream_t s);
+                        cudaStream_t s, const SweepWork *W);
 
 }  // namespace rmx
