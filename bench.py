@@ -146,7 +146,7 @@ def peaks() -> dict:
 def ncu_traffic():
     """DRAM bytes per launch of the move-evaluation kernel from the committed
     ncu summary (profiles/), scaled as that summary states."""
-    p = ROOT / "profiles" / "eval_kernel_ncu.md"
+    p = ROOT / "profiles" / "move_eval_mid400k.md"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
