@@ -174,6 +174,21 @@ def profile_run(g, desc: str):
                       "n_modules": r["n_modules"], "profile": p}))
 
 
+def slowest_over_ranks(vals, pg, device):
+    """Element-wise max over ranks: the slowest rank sets the job's time.
+    Every rank makes this call at the same point (one all_reduce)."""
+    import torch
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    if pg is not None:
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def job_throughput(world: int, units_per_rank: float, seconds: float) -> float:
+    """Whole-job throughput: every rank's units over the slowest rank's time."""
+    return world * units_per_rank / seconds
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -245,11 +260,8 @@ def main():
     gpu_launches = prof["kernel_launches"] - launches0
     G.set_profiling(False)
     ms_step = ms / args.steps
-    t = torch.tensor([ms_step], device="cuda")
-    if pg:
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    ms_step_max = float(t.item())
-    value = world * E / (ms_step_max / 1e3)
+    ms_step_max = slowest_over_ranks([ms_step], pg, "cuda")[0]
+    value = job_throughput(world, E, ms_step_max / 1e3)
     L_bits = [r["L_bits"] for r in results]
 
     # ---- end to end through the C ABI with pinned host buffers
@@ -273,10 +285,7 @@ def main():
         Ge.close()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     build_s /= e2e_steps
-    t = torch.tensor([e2e_s], device="cuda")
-    if pg:
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    e2e_value = world * E / float(t.item())
+    e2e_value = job_throughput(world, E, slowest_over_ranks([e2e_s], pg, "cuda")[0])
 
     # ---- roofline of the dominant kernel class (move evaluation)
     pk = peaks()
