@@ -170,6 +170,25 @@ int32_t rmx_superstep_codelengths(const rmx_graph *g, double *bits, int32_t cap)
  * the partition part and code length L (nats). name keeps its leading '/'. */
 rmx_status rmx_write_outputs(rmx_graph *g, const int32_t *part, double L, const char *outdir, const char *name);
 
+/* Code length of a FIXED partition as a function of the link weights and the
+ * teleportation probability tau (fixed at 0.15 in the reference,
+ * Module.cpp:340-469 and :2966-3002). The reference has no gradient: these two
+ * calls are new API built on its forward model (row normalisation
+ * Module.cpp:237-247, stationary flow with dangling mass redistributed by
+ * teleport weight, module exit flows, calculateCodeLength).
+ * rmx_adjoint_forward: *L (nats) at tau; p[N] (may be NULL) the stationary flow
+ * at tau (power iteration with the reference's stop rule).
+ * rmx_adjoint_backward: the same L (may be NULL), dL_dw[E] (may be NULL) the
+ * derivative with respect to every kept link weight in the graph's CSR order
+ * (the order of rmx_graph_links; input duplicates share their summed link's
+ * value, dropped self-loops have none), *dL_dtau (may be NULL). The stationary
+ * flow is recomputed, then one transposed solve (pull over the out-links)
+ * gives the adjoint of the flow. part: module id per node in [0,N); tau in
+ * (0,1). */
+rmx_status rmx_adjoint_forward(rmx_graph *g, const int32_t *part, double tau, double *L, double *p);
+rmx_status rmx_adjoint_backward(rmx_graph *g, const int32_t *part, double tau, double *dL_dw, double *dL_dtau,
+                                double *L);
+
 /* Device-time profiling of the handle's kernels (CUDA events on its stream). */
 rmx_status rmx_set_profiling(rmx_graph *g, int32_t on);
 rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out);

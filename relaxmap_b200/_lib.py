@@ -24,7 +24,7 @@ EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_creat
            "rmx_graph_destroy", "rmx_graph_info", "rmx_graph_links", "rmx_initiate", "rmx_codelength",
            "rmx_coarsen", "rmx_evaluate_moves", "rmx_optimize", "rmx_superstep_codelengths", "rmx_write_outputs",
            "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main",
-           "rmx_steady_state_noalloc", "rmx_noalloc_last_error"]
+           "rmx_steady_state_noalloc", "rmx_noalloc_last_error", "rmx_adjoint_forward", "rmx_adjoint_backward"]
 
 
 class RmxError(RuntimeError):
@@ -166,6 +166,26 @@ class Graph:
         L = C.c_double()
         _check(lib().rmx_codelength(self._h, _p(part), C.byref(L)))
         return L.value
+
+    def adjoint_forward(self, part, tau: float = 0.15, want_p: bool = False) -> dict:
+        """Code length (nats) of a fixed partition at teleportation probability tau."""
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        L = C.c_double()
+        p = np.zeros(self.n) if want_p else None
+        _check(lib().rmx_adjoint_forward(self._h, _p(part), C.c_double(tau), C.byref(L),
+                                         _p(p) if p is not None else None))
+        out = {"L": L.value}
+        if p is not None:
+            out["p"] = p
+        return out
+
+    def adjoint_backward(self, part, tau: float = 0.15) -> dict:
+        """dL/dw per link (CSR order of links()), dL/dtau and L at a fixed partition."""
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        g = np.zeros(max(self.n_links, 1))
+        dt, L = C.c_double(), C.c_double()
+        _check(lib().rmx_adjoint_backward(self._h, _p(part), C.c_double(tau), _p(g), C.byref(dt), C.byref(L)))
+        return {"dL_dw": g[: self.n_links], "dL_dtau": dt.value, "L": L.value}
 
     def coarsen(self, part) -> dict:
         part = np.ascontiguousarray(part, dtype=np.int32)

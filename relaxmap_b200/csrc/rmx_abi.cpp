@@ -176,6 +176,25 @@ rmx_status rmx_codelength(rmx_graph *g, const int32_t *part, double *L) {
     });
 }
 
+rmx_status rmx_adjoint_forward(rmx_graph *g, const int32_t *part, double tau, double *L, double *p) {
+    return guard([&] {
+        need(g, "graph");
+        need(part, "part");
+        need(L, "L");
+        g->adjoint(part, tau, L, p, nullptr, nullptr, nullptr);
+    });
+}
+
+rmx_status rmx_adjoint_backward(rmx_graph *g, const int32_t *part, double tau, double *dL_dw, double *dL_dtau,
+                                double *L) {
+    return guard([&] {
+        need(g, "graph");
+        need(part, "part");
+        if (!dL_dw && !dL_dtau) throw std::invalid_argument("dL_dw and dL_dtau are both NULL");
+        g->adjoint(part, tau, L, nullptr, dL_dw, dL_dtau, nullptr);
+    });
+}
+
 rmx_status rmx_coarsen(rmx_graph *g, const int32_t *part, int32_t *n_sn, int64_t *n_sn_links, int32_t *sn_of_mod,
                        int64_t *out_off, int32_t *out_dst, double *out_f, int64_t *in_off, int32_t *in_src,
                        double *in_f) {

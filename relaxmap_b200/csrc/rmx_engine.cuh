@@ -72,8 +72,9 @@ CsrBuild build_csr(int32_t n, int64_t n_edges, int32_t *d_src, int32_t *d_dst, d
 struct FlowOut {
     int iters = 0;
 };
+// alpha: teleportation probability (the reference's 0.15 unless a caller varies it).
 int power_iteration(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
-                    const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, int vec);
+                    const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, int vec, double alpha = kAlpha);
 // The same solve writing into caller-provided scratch (y[n], parts[3*max_blocks],
 // iters on the device); asynchronous, allocates nothing.
 void power_iteration_into(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w,

@@ -231,7 +231,7 @@ template <int VEC>
 __global__ void __launch_bounds__(kPowT) k_power(const int64_t *__restrict__ in_off, const int32_t *__restrict__ in_src,
                                                  const double *__restrict__ in_w, const double *__restrict__ tw,
                                                  const uint8_t *__restrict__ dang, int32_t n, double *x, double *y,
-                                                 double *parts, int *iters_out) {
+                                                 double *parts, int *iters_out, double alpha) {
     cg::grid_group grid = cg::this_grid();
     __shared__ double sh[32];
     const int nb = gridDim.x;
@@ -254,14 +254,15 @@ __global__ void __launch_bounds__(kPowT) k_power(const int64_t *__restrict__ in_
     int iter = 0;
     for (;;) {
         const double D = sum_parts(Dp, nb, sh);
-        const double coef = kAlpha + kBeta * D;
+        const double beta = 1.0 - alpha;  // 1.0 - 0.15 is kBeta exactly
+        const double coef = alpha + beta * D;
         double ls = 0.0;
         for (int64_t base = gwarp * RPW; base < n; base += nwarps * RPW) {
             const int64_t r = base + sub;
             double acc = 0.0;
             if (r < n) {
                 const int64_t e = in_off[r + 1];
-                for (int64_t k = in_off[r] + lv; k < e; k += VEC) acc += kBeta * in_w[k] * __ldcg(x + in_src[k]);
+                for (int64_t k = in_off[r] + lv; k < e; k += VEC) acc += beta * in_w[k] * __ldcg(x + in_src[k]);
             }
 #pragma unroll
             for (int o = VEC / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(kPowT) k_power(const int64_t *__restrict__ in_
 
 template <int VEC>
 static int launch_power(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
-                        const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s) {
+                        const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, double alpha) {
     int dev = 0, per_sm = 0, coop = 0;
     RMX_CUDA(cudaGetDevice(&dev));
     RMX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
@@ -312,7 +313,7 @@ static int launch_power(int32_t n, const int64_t *in_off, const int32_t *in_src,
     double *parts = ar.alloc<double>(3 * nb);
     int *iters = ar.alloc<int>(1);
     void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w, (void *)&tw, (void *)&dangling, (void *)&n,
-                    (void *)&p, (void *)&y, (void *)&parts, (void *)&iters};
+                    (void *)&p, (void *)&y, (void *)&parts, (void *)&iters, (void *)&alpha};
     RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));
     RMX_LAUNCHED();
     int h = 0;
@@ -334,8 +335,9 @@ static void launch_power_into(int32_t n, const int64_t *in_off, const int32_t *i
     int nb = std::max(1, std::min(per_sm, 4)) * num_sms();
     nb = (int)std::min<int64_t>(nb, std::max<int64_t>(1, ((int64_t)n * VEC + kPowT - 1) / kPowT));
     nb = std::min(nb, max_blocks);
+    double alpha = kAlpha;
     void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w, (void *)&tw, (void *)&dangling, (void *)&n,
-                    (void *)&p, (void *)&y, (void *)&parts, (void *)&iters};
+                    (void *)&p, (void *)&y, (void *)&parts, (void *)&iters, (void *)&alpha};
     RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));
     RMX_LAUNCHED();
 }
@@ -359,13 +361,13 @@ int spmv_width(double mean_in_degree) {
 }
 
 int power_iteration(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
-                    const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, int vec) {
+                    const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, int vec, double alpha) {
     if (n <= 0) return 0;
     switch (vec) {
-        case 4: return launch_power<4>(n, in_off, in_src, in_w, tw, dangling, p, ar, s);
-        case 8: return launch_power<8>(n, in_off, in_src, in_w, tw, dangling, p, ar, s);
-        case 16: return launch_power<16>(n, in_off, in_src, in_w, tw, dangling, p, ar, s);
-        default: return launch_power<32>(n, in_off, in_src, in_w, tw, dangling, p, ar, s);
+        case 4: return launch_power<4>(n, in_off, in_src, in_w, tw, dangling, p, ar, s, alpha);
+        case 8: return launch_power<8>(n, in_off, in_src, in_w, tw, dangling, p, ar, s, alpha);
+        case 16: return launch_power<16>(n, in_off, in_src, in_w, tw, dangling, p, ar, s, alpha);
+        default: return launch_power<32>(n, in_off, in_src, in_w, tw, dangling, p, ar, s, alpha);
     }
 }
 

@@ -66,6 +66,10 @@ struct rmx_graph {
                       int32_t *o_dst, double *o_f, int64_t *i_off, int32_t *i_src, double *i_f);
     void evaluate_hook(const int32_t *part, const uint8_t *allow_new, int32_t *best_mod, double *best_delta);
     double optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modules);
+    // Code length of a fixed partition at teleportation probability tau, and
+    // optionally its gradient (rmx_adjoint.cu).
+    void adjoint(const int32_t *part, double tau, double *L, double *p, double *grad, double *dL_dtau,
+                 int *solve_iters);
 
   private:
     void alloc_engine();

@@ -1,0 +1,77 @@
+"""rmx_adjoint_forward / rmx_adjoint_backward against the CPU FP64 adjoint
+(oracle/adjoint.py, itself pinned against centred differences of the
+reference's code length).
+
+Tolerances: the device solves both systems by iteration to a relative L1
+change of 1e-15, the oracle by sparse LU; L agrees to 1e-12 relative, the flow
+to 1e-12 relative L1, dL/dw to 1e-9 relative L1 (and 1e-9 of the largest
+component elementwise), dL/dtau to 1e-9 relative."""
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+O = pytest.importorskip("oracle.oracle")
+AD = pytest.importorskip("oracle.adjoint")
+
+
+def _rel_l1(a, b):
+    return np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300)
+
+
+def _check(G, part, tau):
+    off, dst, w, tw = G.links()
+    ref = AD.backward(off, dst, w, tw, part, t=tau)
+    fw = G.adjoint_forward(part, tau, want_p=True)
+    assert abs(fw["L"] - ref["L"]) <= 1e-12 * abs(ref["L"])
+    assert _rel_l1(fw["p"], ref["p"]) <= 1e-12
+    bw = G.adjoint_backward(part, tau)
+    assert abs(bw["L"] - ref["L"]) <= 1e-12 * abs(ref["L"])
+    g, rg = bw["dL_dw"], ref["dL_dw"]
+    assert len(g) == len(rg)
+    assert _rel_l1(g, rg) <= 1e-9, _rel_l1(g, rg)
+    assert np.abs(g - rg).max() <= 1e-9 * np.abs(rg).max()
+    assert abs(bw["dL_dtau"] - ref["dL_dt"]) <= 1e-9 * abs(ref["dL_dt"])
+    return bw
+
+
+@pytest.mark.parametrize("name", ["directNet_1k_sm_mu_03.txt", "flow.net", "small_planted.txt"])
+@pytest.mark.parametrize("tau", [0.15, 0.3])
+def test_adjoint_golden(built_lib, name, tau):
+    from relaxmap_b200 import Graph
+    with Graph.from_file(GOLDEN / name) as G:
+        part = G.optimize(seed=1)["part"]
+        if tau == 0.15:  # at the reference's teleportation the forward is calculateCodeLength
+            assert abs(G.adjoint_forward(part, tau)["L"] - G.codelength(part)) <= 1e-12 * G.codelength(part)
+        _check(G, part, tau)
+
+
+def test_adjoint_planted_lognormal(built_lib):
+    """The adjoint workload's shape (lognormal weights, mu = 0.3) at 20K nodes,
+    with dangling nodes and a partition that is not an optimum."""
+    from relaxmap_b200 import Graph, synth
+    g = synth.planted_partition(20_000, 20, 1000, 20, 1000, 0.3, seed=5, weights="lognormal")
+    src, dst, w = g.src, g.dst, g.w
+    keep = src % 97 != 0  # some nodes without out-links
+    with Graph.from_edges(src[keep], dst[keep], w[keep], n=g.n) as G:
+        part = np.asarray(G.optimize(seed=2)["part"], dtype=np.int32)
+        rng = np.random.default_rng(3)
+        moved = rng.random(g.n) < 0.05
+        part[moved] = rng.integers(0, g.n, moved.sum())
+        _check(G, part, 0.15)
+
+
+def test_adjoint_rejects_bad_input(built_lib):
+    from relaxmap_b200 import Graph, RmxError
+    with Graph.from_file(GOLDEN / "flow.net") as G:
+        part = np.zeros(G.n, dtype=np.int32)
+        for tau in (0.0, 1.0, -0.5):
+            with pytest.raises(RmxError) as e:
+                G.adjoint_forward(part, tau)
+            assert e.value.status == 1
+        bad = part.copy()
+        bad[0] = G.n
+        with pytest.raises(RmxError):
+            G.adjoint_backward(bad, 0.15)
