@@ -68,6 +68,7 @@ enum {
     RMX_K_COARSEN,      /* modules -> super-nodes (sort + segmented reduce) */
     RMX_K_CODELEN,      /* code length reductions */
     RMX_K_OTHER,
+    RMX_K_ADJOINT,      /* transposed flow solve of rmx_adjoint_backward (one cooperative launch per call) */
     RMX_K_COUNT
 };
 
@@ -80,6 +81,7 @@ typedef struct {
     int64_t kernel_launches; /* kernels this library launched (all handles) since it was loaded */
     int64_t links_evaluated; /* unit links read by move evaluation since profiling was enabled */
     int64_t units_evaluated; /* units evaluated since profiling was enabled */
+    int64_t adjoint_iters;   /* sweeps of the transposed solve since profiling was enabled */
 } rmx_profile;
 
 const char *rmx_last_error(void);

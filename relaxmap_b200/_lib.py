@@ -16,7 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "librelaxmap_b200.so"
 RMX_OK = 0
 STATUS = {0: "RMX_OK", 1: "RMX_ERR_INVALID", 2: "RMX_ERR_IO", 3: "RMX_ERR_FORMAT", 4: "RMX_ERR_CUDA",
           5: "RMX_ERR_OOM", 6: "RMX_ERR_NO_CONVERGENCE", 7: "RMX_ERR_TIMEOUT", 8: "RMX_ERR_STATE"}
-KERNELS = ["spmv", "eval", "commit", "coarsen", "codelen", "other"]
+KERNELS = ["spmv", "eval", "commit", "coarsen", "codelen", "other", "adjoint"]
 
 # every symbol include/relaxmap_b200.h declares
 EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_create", "rmx_graph_load_file",
@@ -44,9 +44,9 @@ class KernelStat(C.Structure):
 
 
 class Profile(C.Structure):
-    _fields_ = [("k", KernelStat * 6), ("sweeps", C.c_int64), ("supersteps", C.c_int64),
+    _fields_ = [("k", KernelStat * 7), ("sweeps", C.c_int64), ("supersteps", C.c_int64),
                 ("power_iters", C.c_int64), ("total_ms", C.c_double), ("kernel_launches", C.c_int64),
-                ("links_evaluated", C.c_int64), ("units_evaluated", C.c_int64)]
+                ("links_evaluated", C.c_int64), ("units_evaluated", C.c_int64), ("adjoint_iters", C.c_int64)]
 
 
 _L = None
@@ -232,7 +232,7 @@ class Graph:
                for i, name in enumerate(KERNELS)}
         out.update(sweeps=pr.sweeps, supersteps=pr.supersteps, power_iters=pr.power_iters, total_ms=pr.total_ms,
                    kernel_launches=pr.kernel_launches, links_evaluated=pr.links_evaluated,
-                   units_evaluated=pr.units_evaluated)
+                   units_evaluated=pr.units_evaluated, adjoint_iters=pr.adjoint_iters)
         return out
 
     def stream_ptr(self) -> int:

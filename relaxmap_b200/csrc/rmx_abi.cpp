@@ -297,6 +297,12 @@ rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out) {
         // module's statistics (32), proposal and change written (12); per
         // candidate module, its statistics record (32).
         out->k[RMX_K_EVAL].bytes = 16.0 * (double)c[0] + 120.0 * (double)c[1] + 32.0 * (double)c[2];
+        // The transposed solve, per sweep: link index, weight and the gathered
+        // adjoint value (4 + 8 + 8 B per link); per node, the offsets, row sum,
+        // right-hand side, teleport weight, dangling flag, the old value read
+        // and the new one written and copied back (8+8+8+8+1+8+8+8+8 B).
+        out->k[RMX_K_ADJOINT].bytes =
+            (double)g->prof.adjoint_iters * (20.0 * (double)g->E + 65.0 * (double)g->N);
         out->power_iters = g->power_iters;
         out->kernel_launches = (int64_t)__atomic_load_n(&rmx::g_kernel_launches, __ATOMIC_RELAXED);
     });

@@ -75,8 +75,8 @@ __global__ void k_adj_rows(int32_t n, const int64_t *off, const int32_t *dst, co
     if (lane == 0 && sl != 0) atomic_add_fx(s0, sl);
 }
 
-// Per module: q_m and the code-length sums. parts[4*block + k] = block sums of
-// q, plogp(q), plogp(q+P), and (1-TW)P - OUT - (1-TW)D weighted later.
+// Per module: q_m and the code-length sums; parts[3*block + k] = block sums of
+// q, plogp(q) and plogp(q+P).
 __global__ void k_adj_mod1(int32_t n, const Stat4 *mstat, double alpha, double *q, double *parts) {
     __shared__ double sh[3][kAdjT / 32];
     double a0 = 0, a1 = 0, a2 = 0;
@@ -406,6 +406,7 @@ void rmx_graph::adjoint(const int32_t *part_host, double tau, double *L_out, dou
         const int max_iter = 4000;
         const double tol = 1e-15;
         int it = 0;
+        timers.begin(kTimerAdjoint, stream);
         switch (spmv_vec) {
             case 4: it = launch_solve<4>(N, out_off, out_dst, out_w0, rowsum, tw, dangling, c, beta, lam, lam2, sp,
                                          kMaxBlocks, max_iter, tol, iters, stream); break;
@@ -416,6 +417,8 @@ void rmx_graph::adjoint(const int32_t *part_host, double tau, double *L_out, dou
             default: it = launch_solve<32>(N, out_off, out_dst, out_w0, rowsum, tw, dangling, c, beta, lam, lam2, sp,
                                            kMaxBlocks, max_iter, tol, iters, stream); break;
         }
+        timers.end(kTimerAdjoint, stream);
+        if (timers.on) prof.adjoint_iters += it;
         if (solve_iters) *solve_iters = it;
         if (grad_out) {
             double *grad = A.alloc<double>(Em);

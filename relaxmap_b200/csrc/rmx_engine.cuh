@@ -100,7 +100,7 @@ void refresh_terms(ModState &M, cudaStream_t s);
 // Code length per instance from the module statistics.
 void instance_codelength(const ModState &M, InstState &I, cudaStream_t s);
 // Device time per kernel class, recorded with CUDA events on the stream.
-enum { kTimerSpmv = 0, kTimerEval, kTimerCommit, kTimerCoarsen, kTimerCodelen, kTimerOther, kTimerCount };
+enum { kTimerSpmv = 0, kTimerEval, kTimerCommit, kTimerCoarsen, kTimerCodelen, kTimerOther, kTimerAdjoint, kTimerCount };
 struct Timers {
     bool on = false;
     std::vector<cudaEvent_t> pool;
