@@ -172,6 +172,35 @@ int32_t rmx_superstep_codelengths(const rmx_graph *g, double *bits, int32_t cap)
  * the partition part and code length L (nats). name keeps its leading '/'. */
 rmx_status rmx_write_outputs(rmx_graph *g, const int32_t *part, double L, const char *outdir, const char *name);
 
+/* ---- Batched multi-graph x multi-attempt optimisation.
+ * The reference optimises one network per run and its attempts one after
+ * another (OmpRelaxmap.cpp:181-219); a batch optimises many graphs, each
+ * `attempts` times, together. rmx_batch_create copies the graphs to host
+ * memory: graph k has n_nodes[k] nodes and n_edges[k] edges, stored one graph
+ * after another in src/dst (ids local to the graph, 0..n_nodes[k]-1) and w (may
+ * be NULL: weight 1); node_w (may be NULL) the Pajek-style node weights, one
+ * graph after another. Edge preparation per graph is rmx_graph_create's. */
+typedef struct rmx_batch rmx_batch;
+rmx_status rmx_batch_create(int32_t n_graphs, const int32_t *n_nodes, const int64_t *n_edges, const int32_t *src,
+                            const int32_t *dst, const double *w, const double *node_w, rmx_batch **out);
+/* Device budget of one wave: graph-attempt copies are packed into one
+ * disjoint-union graph of at most max_links links and max_nodes nodes (a
+ * single graph's attempts always form one wave). Defaults 2^27 and 2^25. */
+rmx_status rmx_batch_set_wave(rmx_batch *b, int64_t max_links, int64_t max_nodes);
+/* Runs every graph opts->attempts times (stop rules per graph-attempt as in
+ * rmx_optimize, opts->seed for all; copies differ in their random choices) and
+ * keeps each graph's lowest code length. Outputs (each may be NULL):
+ * part_out[sum n_nodes] module per node, graph by graph, renumbered 0.. in
+ * order of first appearance; L_out[n_graphs] nats; n_modules[n_graphs];
+ * best_attempt[n_graphs] the attempt index kept. */
+rmx_status rmx_batch_optimize(rmx_batch *b, const rmx_opts *opts, int32_t *part_out, double *L_out,
+                              int32_t *n_modules, int32_t *best_attempt);
+/* The last rmx_batch_optimize: waves, graph-attempt instances and the device
+ * time of the optimiser runs (ms, CUDA events; host packing excluded). */
+rmx_status rmx_batch_info(const rmx_batch *b, int32_t *n_graphs, int32_t *waves, int64_t *instances,
+                          double *device_ms);
+rmx_status rmx_batch_destroy(rmx_batch *b);
+
 /* Code length of a FIXED partition as a function of the link weights and the
  * teleportation probability tau (fixed at 0.15 in the reference,
  * Module.cpp:340-469 and :2966-3002). The reference has no gradient: these two

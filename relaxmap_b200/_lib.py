@@ -24,7 +24,8 @@ EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_creat
            "rmx_graph_destroy", "rmx_graph_info", "rmx_graph_links", "rmx_initiate", "rmx_codelength",
            "rmx_coarsen", "rmx_evaluate_moves", "rmx_optimize", "rmx_superstep_codelengths", "rmx_write_outputs",
            "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main",
-           "rmx_steady_state_noalloc", "rmx_noalloc_last_error", "rmx_adjoint_forward", "rmx_adjoint_backward"]
+           "rmx_steady_state_noalloc", "rmx_noalloc_last_error", "rmx_adjoint_forward", "rmx_adjoint_backward",
+           "rmx_batch_create", "rmx_batch_set_wave", "rmx_batch_optimize", "rmx_batch_info", "rmx_batch_destroy"]
 
 
 class RmxError(RuntimeError):
@@ -240,6 +241,64 @@ class Graph:
 
     def sync(self):
         _check(lib().rmx_sync(self._h))
+
+
+class Batch:
+    """Many graphs optimised together, each `attempts` times (rmx_batch_*).
+
+    graphs: a list of (n_nodes, src, dst, w) with graph-local node ids; w may
+    be None. node_w: optional list of per-graph node-weight arrays."""
+
+    def __init__(self, graphs, node_w=None):
+        self.sizes = np.array([int(g[0]) for g in graphs], dtype=np.int32)
+        ne = np.array([len(g[1]) for g in graphs], dtype=np.int64)
+        src = np.ascontiguousarray(np.concatenate([np.asarray(g[1], dtype=np.int32) for g in graphs]))
+        dst = np.ascontiguousarray(np.concatenate([np.asarray(g[2], dtype=np.int32) for g in graphs]))
+        has_w = any(g[3] is not None for g in graphs)
+        w = None
+        if has_w:
+            w = np.ascontiguousarray(np.concatenate([np.ones(len(g[1])) if g[3] is None else
+                                                     np.asarray(g[3], dtype=np.float64) for g in graphs]))
+        nw = None if node_w is None else np.ascontiguousarray(np.concatenate(node_w), dtype=np.float64)
+        h = C.c_void_p()
+        _check(lib().rmx_batch_create(C.c_int32(len(graphs)), _p(self.sizes), _p(ne), _p(src), _p(dst), _p(w),
+                                      _p(nw), C.byref(h)))
+        self._h = h
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes, dtype=np.int64)])
+
+    def set_wave(self, max_links: int, max_nodes: int):
+        _check(lib().rmx_batch_set_wave(self._h, C.c_int64(max_links), C.c_int64(max_nodes)))
+
+    def optimize(self, **kw) -> dict:
+        o = default_opts(**kw)
+        G = len(self.sizes)
+        part = np.zeros(int(self.offsets[-1]), dtype=np.int32)
+        L, nm, ba = np.zeros(G), np.zeros(G, dtype=np.int32), np.zeros(G, dtype=np.int32)
+        _check(lib().rmx_batch_optimize(self._h, C.byref(o), _p(part), _p(L), _p(nm), _p(ba)))
+        return {"part": [part[self.offsets[k]:self.offsets[k + 1]] for k in range(G)], "L": L,
+                "L_bits": L / np.log(2.0), "n_modules": nm, "best_attempt": ba}
+
+    def info(self) -> dict:
+        g, wv, ins, ms = C.c_int32(), C.c_int32(), C.c_int64(), C.c_double()
+        _check(lib().rmx_batch_info(self._h, C.byref(g), C.byref(wv), C.byref(ins), C.byref(ms)))
+        return {"graphs": g.value, "waves": wv.value, "instances": ins.value, "device_ms": ms.value}
+
+    def close(self):
+        if self._h:
+            lib().rmx_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def parse_file(path, threads: int = 1) -> dict:

@@ -20,9 +20,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-Wall", "-diag-suppress", "177"]
 CU = ["rmx_prims.cu", "rmx_flow.cu", "rmx_moves.cu", "rmx_coarsen.cu", "rmx_engine.cu", "rmx_adjoint.cu", "rmx_noalloc.cu"]
-CPP = ["rmx_io.cpp", "rmx_abi.cpp", "rmx_cli.cpp"]
-CUDA_CPP = {"rmx_abi.cpp"}
-HEADERS = ["rmx_common.cuh", "rmx_prims.cuh", "rmx_engine.cuh", "rmx_graph.hpp", "rmx_io.hpp"]
+CPP = ["rmx_io.cpp", "rmx_abi.cpp", "rmx_cli.cpp", "rmx_batch.cpp"]
+CUDA_CPP = {"rmx_abi.cpp", "rmx_batch.cpp"}
+HEADERS = ["rmx_common.cuh", "rmx_prims.cuh", "rmx_engine.cuh", "rmx_graph.hpp", "rmx_io.hpp", "rmx_batch.hpp"]
 
 
 def _stale(target: Path, deps) -> bool:

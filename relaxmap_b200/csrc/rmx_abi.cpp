@@ -6,6 +6,7 @@
 #include <new>
 #include <string>
 
+#include "rmx_batch.hpp"
 #include "rmx_graph.hpp"
 #include "rmx_io.hpp"
 
@@ -174,6 +175,58 @@ rmx_status rmx_codelength(rmx_graph *g, const int32_t *part, double *L) {
         need(L, "L");
         *L = g->codelength_fp64(part);
     });
+}
+
+rmx_status rmx_batch_create(int32_t n_graphs, const int32_t *n_nodes, const int64_t *n_edges, const int32_t *src,
+                            const int32_t *dst, const double *w, const double *node_w, rmx_batch **out) {
+    if (!out) return fail(RMX_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    rmx_batch *b = nullptr;
+    rmx_status st = guard([&] {
+        b = new rmx_batch();
+        b->create(n_graphs, n_nodes, n_edges, src, dst, w, node_w);
+    });
+    if (st != RMX_OK) {
+        delete b;
+        return st;
+    }
+    *out = b;
+    return RMX_OK;
+}
+
+rmx_status rmx_batch_set_wave(rmx_batch *b, int64_t max_links, int64_t max_nodes) {
+    return guard([&] {
+        need(b, "batch");
+        if (max_links < 1 || max_nodes < 1) throw std::invalid_argument("wave budget must be positive");
+        b->wave_links = max_links;
+        b->wave_nodes = max_nodes;
+    });
+}
+
+rmx_status rmx_batch_optimize(rmx_batch *b, const rmx_opts *opts, int32_t *part_out, double *L_out,
+                              int32_t *n_modules, int32_t *best_attempt) {
+    return guard([&] {
+        need(b, "batch");
+        rmx_opts o;
+        rmx_opts_default(&o);
+        if (opts) o = *opts;
+        b->optimize(o, part_out, L_out, n_modules, best_attempt);
+    });
+}
+
+rmx_status rmx_batch_info(const rmx_batch *b, int32_t *n_graphs, int32_t *waves, int64_t *instances,
+                          double *device_ms) {
+    return guard([&] {
+        need(b, "batch");
+        if (n_graphs) *n_graphs = b->G;
+        if (waves) *waves = b->last_waves;
+        if (instances) *instances = b->last_instances;
+        if (device_ms) *device_ms = b->last_ms;
+    });
+}
+
+rmx_status rmx_batch_destroy(rmx_batch *b) {
+    return guard([&] { delete b; });
 }
 
 rmx_status rmx_adjoint_forward(rmx_graph *g, const int32_t *part, double tau, double *L, double *p) {

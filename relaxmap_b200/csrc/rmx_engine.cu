@@ -33,14 +33,15 @@ __global__ void k_flags_nonempty(int32_t cap, const int32_t *count, int64_t *fla
 // SuperNode(Module, int) Node.cpp:76-106): the super-node carries the module's
 // statistics exactly and keeps the module id.
 __global__ void k_sn_from_modules(int32_t cap, const int32_t *count, const int64_t *snid, const Stat4 *mstat,
-                                  int32_t *sn_mod, Stat4 *sn_attr, int32_t *sn_nnodes, int32_t *sn_inst) {
+                                  const int32_t *minst, int32_t *sn_mod, Stat4 *sn_attr, int32_t *sn_nnodes,
+                                  int32_t *sn_inst) {
     for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < cap; m += (int64_t)gridDim.x * blockDim.x) {
         if (count[m] <= 0) continue;
         const int64_t s = snid[m];
         sn_mod[s] = (int32_t)m;
         sn_attr[s] = mstat[m];
         sn_nnodes[s] = count[m];
-        sn_inst[s] = 0;
+        if (minst) sn_inst[s] = minst[m];
     }
 }
 
@@ -109,9 +110,12 @@ __global__ void k_sub_s0(int32_t n, const double *p, const int32_t *inst, fx_t *
         atomic_add_fx(s0 + inst[v], to_fxl(plogp(p[v])));
 }
 
-__global__ void k_inst_active(int32_t n, const int32_t *count, uint8_t *active) {
+// A parent module is coarse-tuned if it has two or more members and its
+// instance is still running.
+__global__ void k_inst_active(int32_t n, const int32_t *count, const int32_t *minst, const uint8_t *top_active,
+                              uint8_t *active) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-        active[k] = count[k] > 1 ? 1 : 0;
+        active[k] = count[k] > 1 && top_active[minst[k]] ? 1 : 0;
 }
 
 // partition_module_network's stop rule per sub-network (OmpRelaxmap.cpp:458-459).
@@ -139,10 +143,12 @@ __global__ void k_copy_L(int32_t n, const double *L, double *L_prev) {
 // super-nodes of sub-modules (SuperNode(SubModule*,...) Node.cpp:108-137): sums
 // of the member nodes; the module is the parent module of the members.
 __global__ void k_sn_from_nodes(int32_t n, const int32_t *node_sn, const int32_t *nmod, const Stat4 *nattr,
-                                int32_t *sn_mod, Stat4 *sn_attr, int32_t *sn_nnodes) {
+                                const int32_t *node_inst, int32_t *sn_mod, Stat4 *sn_attr, int32_t *sn_nnodes,
+                                int32_t *sn_inst) {
     for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
         const int32_t s = node_sn[v];
         sn_mod[s] = nmod[v];
+        if (node_inst) sn_inst[s] = node_inst[v];
         const Stat4 a = nattr[v];
         atomic_add_fx(&sn_attr[s].P, a.P);
         atomic_add_fx(&sn_attr[s].TW, a.TW);
@@ -325,13 +331,42 @@ rmx_graph::~rmx_graph() {
     if (stream) cudaStreamDestroy(stream);
 }
 
+// Copy k of a graph: its node range starts at noff[k], its links at lbase[k];
+// both ends of every link are shifted from the canonical copy's numbering
+// (nodes from cbase[k]). Offsets: one entry per node plus the final one.
+__global__ void k_replicate_csr(int32_t K, const int64_t *noff, const int64_t *cbase, const int64_t *lbase,
+                                const int64_t *c_off, const int32_t *c_adj, const double *c_w, int64_t *off,
+                                int32_t *adj, double *w) {
+    for (int32_t k = blockIdx.x; k < K; k += gridDim.x) {
+        const int64_t nb = noff[k], nn = noff[k + 1] - nb, cb = cbase[k], lb = lbase[k];
+        const int64_t c0 = c_off[cb], cl = c_off[cb + nn] - c0;
+        const int64_t shift = nb - cb;
+        for (int64_t i = threadIdx.x; i < nn; i += blockDim.x) off[nb + i] = lb + (c_off[cb + i] - c0);
+        for (int64_t j = threadIdx.x; j < cl; j += blockDim.x) {
+            adj[lb + j] = (int32_t)(c_adj[c0 + j] + shift);
+            w[lb + j] = c_w[c0 + j];
+        }
+        if (k == K - 1 && threadIdx.x == 0) off[nb + nn] = lb + cl;
+    }
+}
+
+static void replicate_csr(int32_t K, const int64_t *noff, const int64_t *cbase, const int64_t *lbase,
+                          const int64_t *c_off, const int32_t *c_adj, const double *c_w, int64_t *off, int32_t *adj,
+                          double *w, cudaStream_t s) {
+    k_replicate_csr<<<std::min(K, num_sms() * 16), 256, 0, s>>>(K, noff, cbase, lbase, c_off, c_adj, c_w, off, adj,
+                                                                 w);
+    RMX_LAUNCHED();
+}
+
 void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, int64_t n_edges, int32_t n,
-                       const double *node_weights) {
+                       const double *node_weights, const UnionSpec *u) {
     if (n <= 0) throw std::invalid_argument("graph needs at least one node");
     if (n_edges < 0 || (n_edges > 0 && (!src || !dst))) throw std::invalid_argument("edge arrays missing");
     if (n_edges >= (int64_t(1) << 31)) throw std::invalid_argument("more than 2^31-1 input edges");
+    const bool repl = u && u->n_canon > 0;  // edges describe the canonical copies only
+    const int32_t n_in = repl ? u->n_canon : n;
     for (int64_t e = 0; e < n_edges; e++)
-        if ((uint32_t)src[e] >= (uint32_t)n || (uint32_t)dst[e] >= (uint32_t)n)
+        if ((uint32_t)src[e] >= (uint32_t)n_in || (uint32_t)dst[e] >= (uint32_t)n_in)
             throw std::invalid_argument("edge endpoint outside 0..N-1");
     N = n;
     node_w.assign(n, 1.0);
@@ -343,16 +378,24 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
             tot_w += node_weights[i];
         }
     }
+    if (u) {  // a disjoint union of instances: node ranges, canonical copies
+        if (u->K < 1 || (int64_t)u->inst_noff[u->K] != n || u->inst_noff[0] != 0)
+            throw std::invalid_argument("instance node ranges do not cover the graph");
+        K = u->K;
+        inst_noff.assign(u->inst_noff, u->inst_noff + K + 1);
+        inst_canon.assign(u->inst_canon, u->inst_canon + K);
+    }
     RMX_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     configure_eval_kernels();
-    const int64_t Eb = std::max<int64_t>(n_edges, 1);
-    scratch.init((size_t)(88 * Eb + 24 * (int64_t)n) + (64u << 20));
+    // input edges, and an upper bound on the kept links of the whole union
+    const int64_t Ein = std::max<int64_t>(n_edges, 1), Eb = std::max<int64_t>(repl ? u->full_edges : n_edges, 1);
+    scratch.init((size_t)(88 * Eb + 24 * (int64_t)n + 40 * (int64_t)K) + (64u << 20));
     // long-lived arrays: node CSR/CSC, three levels, module and instance state
-    perm.init((size_t)(144 * Eb + 560 * (int64_t)n) + (64u << 20));
+    perm.init((size_t)(144 * Eb + 560 * (int64_t)n + (K > 1 ? 16 * (int64_t)n + 64 * (int64_t)K : 0)) + (64u << 20));
     out_off = perm.alloc<int64_t>(n + 1);
     in_off = perm.alloc<int64_t>(n + 1);
-    int32_t *d_src = scratch.alloc<int32_t>(Eb), *d_dst = scratch.alloc<int32_t>(Eb);
-    double *d_w = scratch.alloc<double>(Eb);
+    int32_t *d_src = scratch.alloc<int32_t>(Ein), *d_dst = scratch.alloc<int32_t>(Ein);
+    double *d_w = scratch.alloc<double>(Ein);
     if (n_edges > 0) {
         RMX_CUDA(cudaMemcpyAsync(d_src, src, sizeof(int32_t) * n_edges, cudaMemcpyHostToDevice, stream));
         RMX_CUDA(cudaMemcpyAsync(d_dst, dst, sizeof(int32_t) * n_edges, cudaMemcpyHostToDevice, stream));
@@ -369,13 +412,49 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     in_src = perm.alloc<int32_t>(Eb);
     in_w = perm.alloc<double>(Eb);
     dtmp = perm.alloc<int64_t>(16);
-    size_t mk = scratch.mark();
-    CsrBuild cb = build_csr(n, n_edges, d_src, d_dst, d_w, out_off, out_dst, out_w0, in_off, in_src, in_w, scratch,
-                            stream, dtmp);
+    if (!repl) {
+        CsrBuild cb = build_csr(n, n_edges, d_src, d_dst, d_w, out_off, out_dst, out_w0, in_off, in_src, in_w,
+                                scratch, stream, dtmp);
+        E = cb.n_links;
+        n_self = cb.n_self;
+    } else {
+        // CSR/CSC of the canonical copies, then every copy written from its canonical one
+        const int32_t nc = u->n_canon;
+        int64_t *c_out_off = scratch.alloc<int64_t>(nc + 1), *c_in_off = scratch.alloc<int64_t>(nc + 1);
+        int32_t *c_out_dst = scratch.alloc<int32_t>(Ein), *c_in_src = scratch.alloc<int32_t>(Ein);
+        double *c_out_w = scratch.alloc<double>(Ein), *c_in_w = scratch.alloc<double>(Ein);
+        CsrBuild cb = build_csr(nc, n_edges, d_src, d_dst, d_w, c_out_off, c_out_dst, c_out_w, c_in_off, c_in_src,
+                                c_in_w, scratch, stream, dtmp);
+        std::vector<int64_t> hoff(nc + 1);
+        RMX_CUDA(cudaMemcpyAsync(hoff.data(), c_out_off, sizeof(int64_t) * (nc + 1), cudaMemcpyDeviceToHost, stream));
+        RMX_CUDA(cudaStreamSynchronize(stream));
+        // per instance: canonical node base and union link base (links of a copy = its canonical copy's)
+        std::vector<int64_t> cbase(K), lbase(K + 1, 0);
+        std::vector<int64_t> canon_node(K, -1);
+        int64_t nb = 0;
+        for (int32_t k = 0; k < K; k++)
+            if (inst_canon[k] == k) {
+                canon_node[k] = nb;
+                nb += inst_noff[k + 1] - inst_noff[k];
+            }
+        if (nb != nc) throw std::invalid_argument("canonical copies do not match the canonical node count");
+        for (int32_t k = 0; k < K; k++) {
+            cbase[k] = canon_node[inst_canon[k]];
+            const int64_t sz = inst_noff[k + 1] - inst_noff[k];
+            lbase[k + 1] = lbase[k] + hoff[cbase[k] + sz] - hoff[cbase[k]];
+        }
+        if (lbase[K] > Eb) throw std::invalid_argument("union link bound too small");
+        int64_t *d_cbase = scratch.alloc<int64_t>(K), *d_lbase = scratch.alloc<int64_t>(K + 1),
+                *d_noff = scratch.alloc<int64_t>(K + 1);
+        RMX_CUDA(cudaMemcpyAsync(d_cbase, cbase.data(), sizeof(int64_t) * K, cudaMemcpyHostToDevice, stream));
+        RMX_CUDA(cudaMemcpyAsync(d_lbase, lbase.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice, stream));
+        RMX_CUDA(cudaMemcpyAsync(d_noff, inst_noff.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice, stream));
+        replicate_csr(K, d_noff, d_cbase, d_lbase, c_out_off, c_out_dst, c_out_w, out_off, out_dst, out_w0, stream);
+        replicate_csr(K, d_noff, d_cbase, d_lbase, c_in_off, c_in_src, c_in_w, in_off, in_src, in_w, stream);
+        E = lbase[K];
+        n_self = cb.n_self;
+    }
     scratch.release(0);
-    (void)mk;
-    E = cb.n_links;
-    n_self = cb.n_self;
     const int64_t Em = std::max<int64_t>(E, 1);
     out_f = perm.alloc<double>(Em);
     out_fx = perm.alloc<fx_t>(Em);
@@ -384,7 +463,16 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     p = perm.alloc<double>(n);
     dangling = perm.alloc<uint8_t>(n);
     std::vector<double> twh(n);
-    for (int32_t i = 0; i < n; i++) twh[i] = node_w[i] / tot_w;  // OmpRelaxmap.cpp:113-115
+    if (K == 1) {
+        for (int32_t i = 0; i < n; i++) twh[i] = node_w[i] / tot_w;  // OmpRelaxmap.cpp:113-115
+    } else {  // teleportation normalised within every instance
+        for (int32_t k = 0; k < K; k++) {
+            double t = node_weights ? 0.0 : (double)(inst_noff[k + 1] - inst_noff[k]);
+            if (node_weights)
+                for (int64_t i = inst_noff[k]; i < inst_noff[k + 1]; i++) t += node_w[i];
+            for (int64_t i = inst_noff[k]; i < inst_noff[k + 1]; i++) twh[i] = node_w[i] / t;
+        }
+    }
     RMX_CUDA(cudaMemcpyAsync(tw, twh.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream));
     nattr = perm.alloc<Stat4>(n);
     nmod = perm.alloc<int32_t>(n);
@@ -393,6 +481,10 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     submod = perm.alloc<int32_t>(n);
     s0 = perm.alloc<fx_t>(1);
     RMX_CUDA(cudaMemsetAsync(zeros, 0, sizeof(int32_t) * n, stream));
+    if (K > 1) {
+        node_inst = perm.alloc<int32_t>(n);
+        RMX_CUDA(cudaMemcpyAsync(node_inst, u->node_inst, sizeof(int32_t) * n, cudaMemcpyHostToDevice, stream));
+    }
     alloc_engine();
     RMX_CUDA(cudaStreamSynchronize(stream));
     // SpMV sub-warp width from the mean in-degree
@@ -413,7 +505,7 @@ void rmx_graph::alloc_engine() {
     node_lv.in_fx = in_fx;
     node_lv.attr = nattr;
     node_lv.mod = nmod;
-    node_lv.inst = zeros;
+    node_lv.inst = K > 1 ? node_inst : zeros;
     node_lv.nnodes = nullptr;
     for (Level *lv : {&sn_buf[0], &sn_buf[1], &sub_lv}) {
         lv->out_off = perm.alloc<int64_t>(n + 1);
@@ -427,7 +519,7 @@ void rmx_graph::alloc_engine() {
     }
     for (Level &lv : sn_buf) {
         lv.mod = perm.alloc<int32_t>(n);
-        lv.inst = zeros;
+        lv.inst = K > 1 ? perm.alloc<int32_t>(n) : zeros;
     }
     sub_lv.mod = submod;
     sub_lv.inst = nmod;  // instance of a node in coarse-tune = its parent module
@@ -439,7 +531,7 @@ void rmx_graph::alloc_engine() {
         M->count = perm.alloc<int32_t>(n);
         M->inst = perm.alloc<int32_t>(n);
     }
-    inst1.n = 1;
+    inst1.n = K;
     instsub.n = n;
     for (InstState *I : {&inst1, &instsub}) {
         const int32_t k = I->n;
@@ -450,7 +542,7 @@ void rmx_graph::alloc_engine() {
         I->acc = perm.alloc<fx_t>(3 * (int64_t)k);
         I->active = perm.alloc<uint8_t>(k);
     }
-    inst1.s0 = s0;
+    if (K == 1) inst1.s0 = s0;
     work.list = perm.alloc<int32_t>(n);
     work.list2 = perm.alloc<int32_t>(n);
     work.bucket = perm.alloc<uint16_t>(n);
@@ -508,23 +600,65 @@ void rmx_graph::initiate() {
     normalise(N, out_off, out_w0, out_f, in_off, in_src, in_w, in_w, dangling, scratch, stream);
     timers.end(kTimerOther, stream);
     timers.begin(kTimerSpmv, stream);
-    power_iters = power_iteration(N, in_off, in_src, in_w, tw, dangling, p, scratch, stream, spmv_vec);
+    if (K == 1)
+        power_iters = power_iteration(N, in_off, in_src, in_w, tw, dangling, p, scratch, stream, spmv_vec);
+    else
+        power_iters = union_flows();
     timers.end(kTimerSpmv, stream);
     timers.begin(kTimerOther, stream);
     edge_flows(N, E, out_off, out_f, out_fx, in_src, in_w, in_fx, p, tw, dangling, nattr, s0, stream);
+    if (K > 1) {  // sum p log p of every instance's nodes
+        RMX_CUDA(cudaMemsetAsync(inst1.s0, 0, sizeof(fx_t) * K, stream));
+        k_sub_s0<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, p, node_inst, inst1.s0);
+        RMX_LAUNCHED();
+    }
     timers.end(kTimerOther, stream);
     init_singletons(node_lv, mods, stream);
-    RMX_CUDA(cudaMemsetAsync(inst1.active, 1, 1, stream));
+    RMX_CUDA(cudaMemsetAsync(inst1.active, 1, (size_t)K, stream));
     instance_codelength(mods, inst1, stream);
-    RMX_CUDA(cudaMemcpyAsync(&L0, inst1.L, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    L0v.assign(K, 0.0);
+    RMX_CUDA(cudaMemcpyAsync(L0v.data(), inst1.L, sizeof(double) * K, cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaStreamSynchronize(stream));
+    L0 = L0v[0];
     ensure_hub_table(max_degree(node_lv));
     initiated = true;
 }
 
+// Flows of a disjoint union: each canonical instance (the first copy of a
+// graph) iterated on its own, the other copies sharing its flow.
+int rmx_graph::union_flows() {
+    std::vector<int64_t> comp;
+    for (int32_t k = 0; k < K; k++)
+        if (inst_canon[k] == k) {
+            comp.push_back(inst_noff[k]);
+            comp.push_back(inst_noff[k + 1]);
+        }
+    const int32_t nc = (int32_t)(comp.size() / 2);
+    size_t mk = scratch.mark();
+    int64_t *d_comp = scratch.alloc<int64_t>(comp.size()), *d_noff = scratch.alloc<int64_t>(K + 1);
+    int32_t *d_canon = scratch.alloc<int32_t>(K);
+    RMX_CUDA(cudaMemcpyAsync(d_comp, comp.data(), sizeof(int64_t) * comp.size(), cudaMemcpyHostToDevice, stream));
+    RMX_CUDA(cudaMemcpyAsync(d_noff, inst_noff.data(), sizeof(int64_t) * (K + 1), cudaMemcpyHostToDevice, stream));
+    RMX_CUDA(cudaMemcpyAsync(d_canon, inst_canon.data(), sizeof(int32_t) * K, cudaMemcpyHostToDevice, stream));
+    const int it = power_iteration_components(N, nc, d_comp, node_inst, d_noff, d_canon, in_off, in_src, in_w, tw,
+                                              dangling, p, scratch, stream, spmv_vec);
+    scratch.release(mk);
+    return it;
+}
+
 // ---------------------------------------------------------------- sweeps
 
-double rmx_graph::sweep_single(Level &lv, bool prior, bool allow_new, double vthresh, int64_t &n_active) {
+// Uploads which instances take part in the next sweeps (their units are
+// evaluated; the others keep their modules).
+void rmx_graph::set_active(const std::vector<uint8_t> &m) {
+    if (K == 1)
+        RMX_CUDA(cudaMemsetAsync(inst1.active, m[0], 1, stream));
+    else  // staged from pageable memory before the call returns
+        RMX_CUDA(cudaMemcpyAsync(inst1.active, m.data(), (size_t)K, cudaMemcpyHostToDevice, stream));
+}
+
+void rmx_graph::sweep_single(Level &lv, bool prior, bool allow_new, double vthresh, int64_t &n_active,
+                             std::vector<double> &L) {
     RMX_CUDA(cudaMemsetAsync(work.counters + kCntMoved, 0, sizeof(int64_t), stream));
     if (prior) RMX_CUDA(cudaMemsetAsync(work.next_active, 0, lv.n, stream));
     if (allow_new) free_modules(mods, work, scratch, stream);
@@ -539,43 +673,51 @@ double rmx_graph::sweep_single(Level &lv, bool prior, bool allow_new, double vth
     instance_codelength(mods, inst1, stream);
     timers.end(kTimerCodelen, stream);
     if (prior) compact_flags(work.next_active, lv.n, work.list, work.counters + kCntActive, scratch, stream);
-    struct {
-        double L;
-    } hL;
     int64_t cnt[kCntSlots];
-    RMX_CUDA(cudaMemcpyAsync(&hL.L, inst1.L, sizeof(double), cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaMemcpyAsync(L.data(), inst1.L, sizeof(double) * K, cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaMemcpyAsync(cnt, work.counters, sizeof(cnt), cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaStreamSynchronize(stream));
     prof.sweeps++;
     if (prior) n_active = cnt[kCntActive];
     if (opt.verbose >= 2)
-        printf("  sweep: n=%d active=%lld code length = %.17g, moved %lld\n", lv.n, (long long)n_active, hL.L / kLn2,
+        printf("  sweep: n=%d active=%lld code length = %.17g, moved %lld\n", lv.n, (long long)n_active, L[0] / kLn2,
                (long long)cnt[kCntMoved]);
-    return hL.L;
+}
+
+static bool any_set(const std::vector<uint8_t> &m) {
+    for (uint8_t v : m)
+        if (v) return true;
+    return false;
 }
 
 // The first loop of stochastic_greedy_partition (OmpRelaxmap.cpp:291-339), or
 // the inner super-node loop (:379-411): at most max_iter sweeps, stop when a
 // sweep gains less than threshold bits (and did not lose).
-double rmx_graph::stage_sweeps(Level &lv, bool allow_new, double L) {
+//
+// Every instance (one graph, or one graph-attempt copy of a batch) follows
+// these rules on its own code length; an instance that stops keeps its
+// modules while the others continue.
+void rmx_graph::stage_sweeps(Level &lv, bool allow_new, std::vector<double> &L, const std::vector<uint8_t> &act) {
     const bool prior = opt.prior != 0;
     const double vthresh = prior ? -opt.vthresh : 0.0;  // OmpRelaxmap.cpp:66, Module.cpp:1490 vs :1127
     int64_t n_active = lv.n;
     all_units(lv.n, work, stream);
     if (lv.n > 0) ensure_hub_table(max_degree(lv));
+    std::vector<uint8_t> sweeping = act;
+    std::vector<double> oldL;
     int iter = 0;
-    bool stop = false;
-    while (!stop && iter < opt.max_iter) {
-        const double oldL = L;
+    while (any_set(sweeping) && iter < opt.max_iter) {
+        oldL = L;
         if (!prior && iter > 0) {
             all_units(lv.n, work, stream);
             n_active = lv.n;
         }
-        L = sweep_single(lv, prior, allow_new, vthresh, n_active);
+        set_active(sweeping);
+        sweep_single(lv, prior, allow_new, vthresh, n_active, L);
         iter++;
-        if (oldL - L >= 0 && (oldL - L) / kLn2 < opt.threshold) stop = true;
+        for (int32_t k = 0; k < K; k++)
+            if (sweeping[k] && oldL[k] - L[k] >= 0 && (oldL[k] - L[k]) / kLn2 < opt.threshold) sweeping[k] = 0;
     }
-    return L;
 }
 
 void rmx_graph::project_sn_to_nodes() {
@@ -599,8 +741,8 @@ void rmx_graph::convert_to_supernodes(bool from_sn) {
     int64_t nsn = 0;
     RMX_CUDA(cudaMemcpyAsync(&nsn, dtmp + 0, sizeof(int64_t), cudaMemcpyDeviceToHost, stream));
     Level &src = sn(), &dst = sn_buf[1 - sn_cur];
-    k_sn_from_modules<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, mods.count, snid, mods.stat, dst.mod,
-                                                                              dst.attr, dst.nnodes, zeros);
+    k_sn_from_modules<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(
+        N, mods.count, snid, mods.stat, K > 1 ? mods.inst : nullptr, dst.mod, dst.attr, dst.nnodes, dst.inst);
     RMX_LAUNCHED();
     int32_t *group = nullptr;
     if (from_sn) {
@@ -662,7 +804,8 @@ void rmx_graph::generate_sub_modules() {
     RMX_CUDA(cudaMemsetAsync(instsub.s0, 0, sizeof(fx_t) * N, stream));
     k_sub_s0<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, p, nmod, instsub.s0);
     RMX_LAUNCHED();
-    k_inst_active<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, mods.count, instsub.active);
+    k_inst_active<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, mods.count, mods.inst, inst1.active,
+                                                                          instsub.active);
     RMX_LAUNCHED();
     instance_codelength(submods, instsub, stream);
     k_copy_L<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, instsub.L, instsub.L_prev);
@@ -712,8 +855,8 @@ void rmx_graph::generate_sub_modules() {
     sl.n = (int32_t)nsn;
     RMX_CUDA(cudaMemsetAsync(sl.attr, 0, sizeof(Stat4) * nsn, stream));
     RMX_CUDA(cudaMemsetAsync(sl.nnodes, 0, sizeof(int32_t) * nsn, stream));
-    k_sn_from_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(N, node_sn, nmod, nattr, sl.mod,
-                                                                            sl.attr, sl.nnodes);
+    k_sn_from_nodes<<<blocks_for(N, 256, num_sms() * 32), 256, 0, stream>>>(
+        N, node_sn, nmod, nattr, K > 1 ? node_inst : nullptr, sl.mod, sl.attr, sl.nnodes, sl.inst);
     RMX_LAUNCHED();
     {
         fx_t *rowsum = scratch.alloc<fx_t>(std::max<int64_t>(nsn, 1));
@@ -727,25 +870,27 @@ void rmx_graph::generate_sub_modules() {
 }
 
 // One superstep (stochastic_greedy_partition, OmpRelaxmap.cpp:263-429).
-double rmx_graph::stage(bool fine, double L) {
+void rmx_graph::stage(bool fine, std::vector<double> &L, const std::vector<uint8_t> &run) {
     Level &lv = fine ? node_lv : sn();
     count_units(lv, mods, stream);
     // Node sweeps may open a new module only once member lists exist, i.e.
     // after the first superstep (members.size() > 1 test, Module.cpp:1435);
     // super-node sweeps test the live module flow (Module.cpp:2620).
     const bool allow_first = fine ? superstep > 1 : true;
-    L = stage_sweeps(lv, allow_first, L);
+    stage_sweeps(lv, allow_first, L, run);
     if (!fine) project_sn_to_nodes();
-    double oldL;
+    std::vector<uint8_t> act = run;
+    std::vector<double> oldL;
     bool from_sn = !fine;  // after node sweeps the first conversion reads the node links
     do {
         oldL = L;
         convert_to_supernodes(from_sn);
         from_sn = true;
-        L = stage_sweeps(sn(), true, L);
+        stage_sweeps(sn(), true, L, act);
         project_sn_to_nodes();
-    } while ((oldL - L) / kLn2 > opt.threshold);
-    return L;
+        for (int32_t k = 0; k < K; k++)
+            if (act[k] && !((oldL[k] - L[k]) / kLn2 > opt.threshold)) act[k] = 0;
+    } while (any_set(act));
 }
 
 // Sub-batches per sweep. A fixed count for every sweep: fewer sub-batches in
@@ -769,35 +914,60 @@ int32_t rmx_graph::count_modules() {
     return (int32_t)h;
 }
 
-// main's superstep loop (OmpRelaxmap.cpp:181-219).
-double rmx_graph::run_attempt(uint32_t seed) {
+// main's superstep loop (OmpRelaxmap.cpp:181-219), per instance.
+std::vector<double> rmx_graph::run_attempt(uint32_t seed) {
     run_seed = seed;
     sweep_no = 0;  // every random choice derives from (seed, sweep, sub-batch)
     init_singletons(node_lv, mods, stream);
-    RMX_CUDA(cudaMemsetAsync(inst1.active, 1, 1, stream));
+    std::vector<uint8_t> run(K, 1), next(K, 0);
+    set_active(run);
     instance_codelength(mods, inst1, stream);  // sum of exits of the singleton state
-    double L = L0;
+    std::vector<double> L = L0v, oldL = L;
     step_bits.clear();
     superstep = 1;
     bool fine = true;
-    double oldL = L;
-    L = stage(fine, L);
-    step_bits.push_back(L / kLn2);
+    stage(fine, L, run);
+    step_bits.push_back(L[0] / kLn2);
     if (opt.verbose)
-        printf("SuperStep [%d] - codeLength = %g in %d modules.\n", superstep, L / kLn2, count_modules());
-    bool next = !((oldL - L) / kLn2 < opt.threshold);
-    while (next) {
+        printf("SuperStep [%d] - codeLength = %g in %d modules.\n", superstep, L[0] / kLn2, count_modules());
+    for (int32_t k = 0; k < K; k++) next[k] = !((oldL[k] - L[k]) / kLn2 < opt.threshold);
+    while (any_set(next)) {
+        run = next;
         oldL = L;
         superstep++;
-        L = stage(fine, L);
-        step_bits.push_back(L / kLn2);
+        stage(fine, L, run);
+        step_bits.push_back(L[0] / kLn2);
         if (opt.verbose)
-            printf("SuperStep [%d] - codeLength = %g in %d modules.\n", superstep, L / kLn2, count_modules());
-        if ((oldL - L) / kLn2 < opt.threshold) next = false;
+            printf("SuperStep [%d] - codeLength = %g in %d modules.\n", superstep, L[0] / kLn2, count_modules());
+        for (int32_t k = 0; k < K; k++) next[k] = run[k] && !((oldL[k] - L[k]) / kLn2 < opt.threshold);
         fine = !fine;
-        if (next && !fine) generate_sub_modules();
+        if (any_set(next) && !fine) {
+            set_active(next);  // coarse-tune only the modules of instances still running
+            generate_sub_modules();
+        }
     }
     prof.supersteps += superstep;
+    return L;
+}
+
+std::vector<double> rmx_graph::run_union(const rmx_opts &o) {
+    opt = o;
+    if (opt.max_iter < 0) opt.max_iter = 0;
+    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 36) : 4;
+    cudaEvent_t t0, t1;
+    RMX_CUDA(cudaEventCreate(&t0));
+    RMX_CUDA(cudaEventCreate(&t1));
+    RMX_CUDA(cudaEventRecord(t0, stream));
+    initiate();
+    std::vector<double> L = run_attempt(opt.seed);
+    RMX_CUDA(cudaEventRecord(t1, stream));
+    RMX_CUDA(cudaEventSynchronize(t1));
+    float ms = 0;
+    RMX_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    prof.total_ms = ms;
+    if (timers.on) timers.resolve();
     return L;
 }
 
@@ -815,7 +985,7 @@ double rmx_graph::optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modu
     std::vector<int32_t> part(N);
     std::vector<double> best_steps;
     for (int a = 0; a < opt.attempts; a++) {
-        const double L = run_attempt(opt.seed + (uint32_t)a);
+        const double L = run_attempt(opt.seed + (uint32_t)a)[0];
         if (L < best) {
             best = L;
             best_steps = step_bits;

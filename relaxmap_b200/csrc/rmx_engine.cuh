@@ -80,6 +80,14 @@ int power_iteration(int32_t n, const int64_t *in_off, const int32_t *in_src, con
 void power_iteration_into(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w,
                           const double *tw, const uint8_t *dangling, double *p, double *y, double *parts,
                           int max_blocks, int *iters, cudaStream_t s, int vec);
+// The stationary flow of every component of a disjoint union: one block per
+// canonical component (comp: [lo, hi) node ranges, device), then every other
+// instance copies its canonical instance's flow. Returns the largest
+// iteration count.
+int power_iteration_components(int32_t n, int32_t n_comp, const int64_t *comp, const int32_t *node_inst,
+                               const int64_t *inst_noff, const int32_t *inst_canon, const int64_t *in_off,
+                               const int32_t *in_src, const double *in_w, const double *tw, const uint8_t *dangling,
+                               double *p, Arena &ar, cudaStream_t s, int vec);
 // Sub-warp width of the pull SpMV for a mean in-degree.
 int spmv_width(double mean_in_degree);
 void normalise(int32_t n, const int64_t *out_off, const double *out_w0, double *out_f, const int64_t *in_off,

@@ -15,6 +15,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "rmx_engine.cuh"
 
@@ -354,6 +355,121 @@ void power_iteration_into(int32_t n, const int64_t *in_off, const int32_t *in_sr
         default:
             return launch_power_into<32>(n, in_off, in_src, in_w, tw, dangling, p, y, parts, max_blocks, iters, s);
     }
+}
+
+// ------------------------------------------------ per-component power iteration
+
+constexpr int kCompT = 256;
+
+// Sum over the block, returned to every thread.
+__device__ __forceinline__ double comp_block_sum(double v, double *sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();  // sh free from the previous use
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+#pragma unroll
+    for (int k = 0; k < kCompT / 32; k++) t += sh[k];
+    return t;
+}
+
+// calculateSteadyState for many independent graphs held as one disjoint union:
+// one block per component (node range [lo, hi)), with the component's own
+// dangling mass, normaliser, L1 change and the reference's stop rule
+// (Module.cpp:340-469). tw is normalised within every component.
+template <int VEC>
+__global__ void __launch_bounds__(kCompT) k_power_comp(int32_t n_comp, const int64_t *__restrict__ comp,
+                                                       const int64_t *__restrict__ in_off,
+                                                       const int32_t *__restrict__ in_src,
+                                                       const double *__restrict__ in_w, const double *__restrict__ tw,
+                                                       const uint8_t *__restrict__ dang, double *x, double *y,
+                                                       int *iters) {
+    __shared__ double sh[kCompT / 32];
+    constexpr int RPW = 32 / VEC;
+    const int lane = threadIdx.x & 31, sub = lane / VEC, lv = lane % VEC, warp = threadIdx.x >> 5;
+    constexpr int NW = kCompT / 32;
+    for (int32_t c = blockIdx.x; c < n_comp; c += gridDim.x) {
+        const int64_t lo = comp[2 * c], hi = comp[2 * c + 1];
+        const double x0 = 1.0 / (double)(hi - lo);
+        double dl = 0.0;
+        for (int64_t i = lo + threadIdx.x; i < hi; i += kCompT) {
+            x[i] = x0;
+            if (dang[i]) dl += x0;
+        }
+        double D = comp_block_sum(dl, sh);
+        int iter = 0;
+        for (;;) {
+            const double coef = kAlpha + kBeta * D;
+            double ls = 0.0;
+            for (int64_t base = lo + (int64_t)warp * RPW; base < hi; base += (int64_t)NW * RPW) {
+                const int64_t r = base + sub;
+                double acc = 0.0;
+                if (r < hi) {
+                    const int64_t e = in_off[r + 1];
+                    for (int64_t k = in_off[r] + lv; k < e; k += VEC) acc += kBeta * in_w[k] * x[in_src[k]];
+                }
+#pragma unroll
+                for (int o = VEC / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+                if (r < hi && lv == 0) {
+                    const double v = coef * tw[r] + acc;
+                    y[r] = v;
+                    ls += v;
+                }
+            }
+            const double S = comp_block_sum(ls, sh);  // also orders the y writes before the reads below
+            double el = 0.0;
+            dl = 0.0;
+            for (int64_t i = lo + threadIdx.x; i < hi; i += kCompT) {
+                const double xn = y[i] / S;
+                el += fabs(xn - x[i]);
+                x[i] = xn;
+                if (dang[i]) dl += xn;
+            }
+            const double diff = comp_block_sum(el, sh);
+            D = comp_block_sum(dl, sh);
+            iter++;
+            if (iter >= 200 || (diff <= 1.0e-15 && iter >= 50)) break;  // Module.cpp:460
+        }
+        if (threadIdx.x == 0) iters[c] = iter;
+        __syncthreads();
+    }
+}
+
+// Copies of a graph share its flow: p of every non-canonical instance is read
+// from its canonical copy.
+__global__ void k_replicate_flows(int32_t n, const int32_t *node_inst, const int64_t *inst_noff,
+                                  const int32_t *inst_canon, double *p) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t k = node_inst[i], c = inst_canon[k];
+        if (c != k) p[i] = p[i - inst_noff[k] + inst_noff[c]];
+    }
+}
+
+int power_iteration_components(int32_t n, int32_t n_comp, const int64_t *comp, const int32_t *node_inst,
+                               const int64_t *inst_noff, const int32_t *inst_canon, const int64_t *in_off,
+                               const int32_t *in_src, const double *in_w, const double *tw, const uint8_t *dangling,
+                               double *p, Arena &ar, cudaStream_t s, int vec) {
+    if (n <= 0 || n_comp <= 0) return 0;
+    size_t mk = ar.mark();
+    double *y = ar.alloc<double>(n);
+    int *iters = ar.alloc<int>(n_comp);
+    const unsigned G = (unsigned)std::min<int64_t>(n_comp, (int64_t)num_sms() * 8);
+    switch (vec) {
+        case 4: k_power_comp<4><<<G, kCompT, 0, s>>>(n_comp, comp, in_off, in_src, in_w, tw, dangling, p, y, iters); break;
+        case 8: k_power_comp<8><<<G, kCompT, 0, s>>>(n_comp, comp, in_off, in_src, in_w, tw, dangling, p, y, iters); break;
+        case 16: k_power_comp<16><<<G, kCompT, 0, s>>>(n_comp, comp, in_off, in_src, in_w, tw, dangling, p, y, iters); break;
+        default: k_power_comp<32><<<G, kCompT, 0, s>>>(n_comp, comp, in_off, in_src, in_w, tw, dangling, p, y, iters); break;
+    }
+    RMX_LAUNCHED();
+    k_replicate_flows<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, node_inst, inst_noff, inst_canon, p);
+    RMX_LAUNCHED();
+    std::vector<int> h(n_comp);
+    RMX_CUDA(cudaMemcpyAsync(h.data(), iters, sizeof(int) * n_comp, cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    ar.release(mk);
+    return *std::max_element(h.begin(), h.end());
 }
 
 int spmv_width(double mean_in_degree) {

@@ -7,6 +7,22 @@
 #include "../../include/relaxmap_b200.h"
 #include "rmx_engine.cuh"
 
+// A disjoint union of K instances (host arrays): node_inst[N] the instance of
+// every node, inst_noff[K+1] their node ranges, inst_canon[K] the first copy
+// of the same graph (whose flow the instance shares; k itself if first).
+// With n_canon > 0 the edge arrays describe only the canonical copies, their
+// nodes numbered 0..n_canon-1 in instance order, and every other copy is
+// written on the device from its canonical copy's CSR/CSC; full_edges bounds
+// the input edges of the whole union (sizes the link arrays).
+struct UnionSpec {
+    int32_t K;
+    const int32_t *node_inst;
+    const int64_t *inst_noff;
+    const int32_t *inst_canon;
+    int32_t n_canon = 0;
+    int64_t full_edges = 0;
+};
+
 struct rmx_graph {
     // ---- host-side description
     int32_t N = 0;
@@ -41,6 +57,14 @@ struct rmx_graph {
     rmx::fx_t *agg_tab = nullptr;  // global hash tables of the link aggregation (grown on demand)
     int64_t agg_cap = 0;
 
+    // ---- instances: 1 for a single graph; a batch is a disjoint union of
+    // graph-attempt copies, node ranges inst_noff[k]..inst_noff[k+1]
+    int32_t K = 1;
+    int32_t *node_inst = nullptr;       // device: instance of every node (zeros when K == 1)
+    std::vector<int64_t> inst_noff;     // host, K + 1
+    std::vector<int32_t> inst_canon;    // host: the copy whose flow instance k shares (itself if first)
+    std::vector<double> L0v;            // initial code length per instance
+
     // ---- state
     bool initiated = false;
     int power_iters = 0;
@@ -59,7 +83,9 @@ struct rmx_graph {
 
     ~rmx_graph();
     void create(const int32_t *src, const int32_t *dst, const double *w, int64_t n_edges, int32_t n,
-                const double *node_weights);
+                const double *node_weights, const UnionSpec *u = nullptr);
+    // One run over every instance of a union (seed for all); per-instance code lengths (nats).
+    std::vector<double> run_union(const rmx_opts &o);
     void initiate();
     double codelength_fp64(const int32_t *part_host);
     void coarsen_hook(const int32_t *part, int32_t *n_sn, int64_t *n_links, int32_t *sn_of_mod, int64_t *o_off,
@@ -74,10 +100,13 @@ struct rmx_graph {
   private:
     void alloc_engine();
     void ensure_hub_table(int64_t max_degree);
-    double run_attempt(uint32_t seed);
-    double stage(bool fine, double L);
-    double stage_sweeps(rmx::Level &lv, bool allow_new, double L);
-    double sweep_single(rmx::Level &lv, bool prior, bool allow_new, double vthresh, int64_t &n_active);
+    std::vector<double> run_attempt(uint32_t seed);
+    void stage(bool fine, std::vector<double> &L, const std::vector<uint8_t> &run);
+    void stage_sweeps(rmx::Level &lv, bool allow_new, std::vector<double> &L, const std::vector<uint8_t> &act);
+    void sweep_single(rmx::Level &lv, bool prior, bool allow_new, double vthresh, int64_t &n_active,
+                      std::vector<double> &L);
+    void set_active(const std::vector<uint8_t> &m);
+    int union_flows();
     void convert_to_supernodes(bool from_sn);
     void generate_sub_modules();
     void project_sn_to_nodes();

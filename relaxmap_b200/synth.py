@@ -180,3 +180,22 @@ def config_mid(seed: int = 42, n: int = 1_000_000) -> SynthGraph:
 
 def config_adjoint(seed: int = 42, n: int = 1_000_000) -> SynthGraph:
     return planted_partition(n, 20, 1000, 20, 1000, 0.3, seed, weights="lognormal")
+
+
+def batched_graphs(n_graphs: int = 4096, seed: int = 42, n_range=(200, 20000), mu_range=(0.1, 0.6),
+                   deg_range=(5, 30)) -> list:
+    """The batched workload: graphs with N ~ U[200,20000], mu ~ U[0.1,0.6],
+    mean out-degree ~ U[5,30] (power law 2, max 10x the mean), communities
+    power law in [10,200]; graph k is generated from seed (seed, k)."""
+    rng = np.random.default_rng(seed)
+    ns = rng.integers(n_range[0], n_range[1] + 1, n_graphs)
+    mus = rng.uniform(*mu_range, n_graphs)
+    degs = rng.uniform(*deg_range, n_graphs)
+    return [(int(ns[k]), float(degs[k]), float(mus[k]), int(np.random.SeedSequence([seed, k]).generate_state(1)[0]))
+            for k in range(n_graphs)]
+
+
+def batched_graph(spec) -> SynthGraph:
+    """One graph of batched_graphs' list."""
+    n, deg, mu, s = spec
+    return planted_partition(n, deg, max(2, min(n // 2, int(10 * deg))), 10, 200, mu, s)
