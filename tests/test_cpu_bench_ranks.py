@@ -66,3 +66,49 @@ def test_reference_arm_other_ranks_exit_without_work():
                        env=env, capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_lpt_assign_balances_and_covers():
+    import numpy as np
+
+    from relaxmap_b200.sharding import lpt_assign
+    rng = np.random.default_rng(1)
+    w = rng.integers(1000, 600000, 4096).astype(np.float64)
+    for world in (1, 2, 4, 8):
+        parts = lpt_assign(w, world)
+        allg = np.sort(np.concatenate(parts))
+        assert np.array_equal(allg, np.arange(len(w)))
+        loads = [w[p].sum() for p in parts]
+        assert max(loads) <= w.sum() / world + w.max()  # LPT bound: within one item of the mean
+
+
+def _combine_rank(rank, world, port, q):
+    import datetime
+
+    import numpy as np
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    from relaxmap_b200.sharding import combine, lpt_assign
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        w = np.arange(1, 11, dtype=np.float64)
+        mine = lpt_assign(w, world)[rank]
+        q.put((rank, combine(10, mine, mine * 1.5, dist, "cpu").tolist()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_batched_results_combine_over_two_ranks():
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_combine_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+    assert all(p.exitcode == 0 for p in procs)
+    for _ in range(world):
+        rank, v = q.get(timeout=10)
+        assert v == [1.5 * g for g in range(10)]  # every graph once, from whichever rank ran it
