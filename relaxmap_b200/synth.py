@@ -165,6 +165,38 @@ def rmat(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 
     return SynthGraph(n, src, dst, None, None, f"rmat_s{scale}_ef{edge_factor}")
 
 
+def rmat_device(scale: int, edge_factor: int = 16, a=0.57, b=0.19, c=0.19, seed: int = 42,
+                chunk: int = 1 << 26) -> SynthGraph:
+    """R-MAT as rmat(), drawn on the GPU with torch's generator (for scale >= 22,
+    where the host generator takes minutes): the same distribution, a different
+    stream of random numbers for the same seed."""
+    import torch
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed)
+    n = 1 << scale
+    m = edge_factor * n
+    keys = []
+    for s0 in range(0, m, chunk):
+        k = min(chunk, m - s0)
+        u = torch.zeros(k, dtype=torch.int64, device="cuda")
+        v = torch.zeros(k, dtype=torch.int64, device="cuda")
+        for lvl in range(scale):
+            r = torch.rand(k, generator=gen, device="cuda", dtype=torch.float64)
+            bu = r >= a + b
+            bv = ((r >= a) & (r < a + b)) | (r >= a + b + c)
+            u |= bu.to(torch.int64) << lvl
+            v |= bv.to(torch.int64) << lvl
+        keep = u != v
+        keys.append(torch.unique(u[keep] * n + v[keep]))
+        del u, v, keep
+    key = torch.unique(torch.cat(keys))
+    del keys
+    perm = torch.randperm(n, generator=gen, device="cuda")
+    src = perm[key // n].to(torch.int32).cpu().numpy()
+    dst = perm[key % n].to(torch.int32).cpu().numpy()
+    return SynthGraph(n, src, dst, None, None, f"rmat_s{scale}_ef{edge_factor}_device")
+
+
 # The benchmark configurations (sizes, distributions, seeds).
 def config_small(seed: int = 42) -> SynthGraph:
     """N=1000, out-degree power law (2, mean 20, max 50), communities power law
