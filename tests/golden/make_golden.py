@@ -19,6 +19,11 @@ Writes, per fixture graph <g>:
                              (convertModulesToSuperNodes) on the reference flows
   flow.ref.tree / flow.ref.clu   the reference CLI's output files for flow.net
                                  (seed 1, 1 thread, 1e-3, 0.0, 10, prior)
+  quality.ref.npz          larger seeded graphs regenerated by the tests
+                           (QUALITY_CASES): the reference's final code length
+                           (bits, recomputed) for seeds 1..8 at 8 threads, prior
+
+    python tests/golden/make_golden.py quality   # only quality.ref.npz
 """
 from __future__ import annotations
 
@@ -90,6 +95,30 @@ def golden(name: str):
           "(8 thr)", np.median(out["final_L_bits"][1]))
 
 
+# name -> generator call; the tests rebuild the same graphs from these seeds
+QUALITY_CASES = {
+    "rmat14": lambda: synth.rmat(14, 16, seed=42),
+    "planted20k_mid": lambda: synth.config_mid(seed=42, n=20_000),
+    "planted20k_adjoint": lambda: synth.config_adjoint(seed=42, n=20_000),
+}
+
+
+def quality():
+    out = {}
+    for name, make in QUALITY_CASES.items():
+        g = make()
+        ld = O.from_edges(g.n, g.src, g.dst, g.w)
+        Lc = []
+        for seed in SEEDS:
+            R = O.Ref(loaded=ld)
+            R.prepare(8)
+            Lc.append(R.partition(seed=seed, threads=8, threshold=1e-3, vthresh=0.0, max_iter=10,
+                                  prior=True)["L_computed_bits"])
+        out[name] = np.array(Lc)
+        print(name, "N", g.n, "E", g.m, "median L bits", np.median(Lc))
+    np.savez_compressed(HERE / "quality.ref.npz", **out)
+
+
 def cli_outputs():
     with tempfile.TemporaryDirectory() as td:
         src = Path(td) / "in"
@@ -103,7 +132,11 @@ def cli_outputs():
 
 if __name__ == "__main__":
     O.build(reference=True)
+    if sys.argv[1:] == ["quality"]:
+        quality()
+        sys.exit(0)
     copy_inputs()
     for name in ("flow.net", "flow.txt", "directNet_1k_sm_mu_03.txt", "small_planted.txt"):
         golden(name)
     cli_outputs()
+    quality()

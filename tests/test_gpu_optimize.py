@@ -37,6 +37,30 @@ def test_quality_vs_reference_median(built_lib, name, prior):
     assert np.median(Ls) <= ref_median * 1.005, (np.median(Ls), ref_median)
 
 
+QUALITY = {
+    "rmat14": lambda synth: synth.rmat(14, 16, seed=42),
+    "planted20k_mid": lambda synth: synth.config_mid(seed=42, n=20_000),
+    "planted20k_adjoint": lambda synth: synth.config_adjoint(seed=42, n=20_000),
+}
+
+
+@pytest.mark.parametrize("name", sorted(QUALITY))
+def test_quality_larger_graphs(built_lib, name):
+    """The R-MAT, mid and adjoint shapes at ~20K nodes (the same seeded
+    generators): median over 8 seeds within 0.5% of the reference's median over
+    8 seeds (tests/golden/quality.ref.npz, made by make_golden.py)."""
+    from relaxmap_b200 import Graph, synth
+    ref_median = float(np.median(np.load(GOLDEN / "quality.ref.npz")[name]))
+    g = QUALITY[name](synth)
+    Ls = []
+    with Graph.from_edges(g.src, g.dst, g.w, n=g.n) as G:
+        for seed in range(1, 9):
+            r = G.optimize(seed=seed)
+            assert abs(r["L"] - G.codelength(r["part"])) <= 1e-10
+            Ls.append(r["L_bits"])
+    assert np.median(Ls) <= ref_median * 1.005, (np.median(Ls), ref_median)
+
+
 def test_deterministic_per_seed(built_lib):
     from relaxmap_b200 import Graph
     with Graph.from_file(GOLDEN / "small_planted.txt") as G:
