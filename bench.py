@@ -418,6 +418,20 @@ def bench_batched(args, world: int, rank: int, pg):
                 "d2h_bytes_per_step": int(nodes * 4 + len(mine) * 16)},
         "clocks": clk.summary(),
     }
+    if rank == 0 and world == 1:
+        # the same graphs one by one through rmx_optimize (16 attempts each): a
+        # sample of every 64th graph of this rank, device time per graph
+        from relaxmap_b200 import Graph
+        sample = gs[::64]
+        seq_s = 0.0
+        for g in sample:
+            with Graph.from_edges(g[1], g[2], g[3], n=g[0]) as Gs:
+                Gs.optimize(seed=1, attempts=BATCH_ATTEMPTS)
+                seq_s += Gs.profile()["total_ms"] / 1e3
+        seq_rate = len(sample) / seq_s
+        line["sequential_plain_gpu"] = {"value": seq_rate, "unit": "graphs/s", "sample": f"every 64th graph "
+                                        f"({len(sample)} graphs), rmx_optimize with 16 attempts each, device time",
+                                        "batched_over_sequential": line["value"] / seq_rate}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         secs = []
         for g in gs[:4]:
@@ -454,8 +468,10 @@ def bench_adjoint(args, world: int, rank: int, pg):
     G = Graph.from_edges(g.src, g.dst, g.w, n=g.n)
     G.initiate()
     stream = torch.cuda.ExternalStream(G.stream_ptr())
+    # the gradient lands in pinned host memory (the caller's choice of buffer)
+    grad_host = torch.empty(max(G.n_links, 1), dtype=torch.float64).pin_memory().numpy()
     for _ in range(args.warmup):
-        G.adjoint_backward(part)
+        G.adjoint_backward(part, out=grad_host)
     G.set_profiling(True)
     launches0 = G.profile()["kernel_launches"]
     if pg:
@@ -465,12 +481,20 @@ def bench_adjoint(args, world: int, rank: int, pg):
     with Clocks(torch.cuda.current_device()) as clk:
         e0.record(stream)
         for _ in range(args.steps):
-            r = G.adjoint_backward(part)
+            r = G.adjoint_backward(part, out=grad_host)
         e1.record(stream)
         torch.cuda.synchronize()
     ms_step = e0.elapsed_time(e1) / args.steps
     prof = G.profile()
     G.set_profiling(False)
+    # the forward pass alone (flow + code length of the partition), same timing
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        G.adjoint_forward(part)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = f0.elapsed_time(f1) / args.steps
     ms_max = slowest_over_ranks([ms_step], pg, "cuda")[0]
     value = job_throughput(world, E, ms_max / 1e3)
     # end to end: graph built from pinned host buffers, gradient back in host memory
@@ -484,7 +508,7 @@ def bench_adjoint(args, world: int, rank: int, pg):
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         Ge = Graph.from_host_ptrs(src.data_ptr(), dst.data_ptr(), w.data_ptr(), E, g.n)
-        Ge.adjoint_backward(part)
+        Ge.adjoint_backward(part, out=grad_host)
         Ge.close()
     e2e_s = slowest_over_ranks([(time.perf_counter() - t0) / e2e_steps], pg, "cuda")[0]
     pk = peaks()
@@ -498,6 +522,7 @@ def bench_adjoint(args, world: int, rank: int, pg):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (resident graph ~1.5 GB)"},
         "quality": {"L_nats": r["L"], "dL_dtau": r["dL_dtau"]},
+        "forward_ms": fwd_ms, "backward_over_forward": ms_step / fwd_ms,
         "e2e": {"value": job_throughput(world, E, e2e_s), "unit": UNIT, "h2d_bytes_per_step": int(E * 16),
                 "d2h_bytes_per_step": int(G.n_links * 8 + 16)},
         "roofline": {"kernel": "transposed flow solve (k_adj_solve)", "bound": "hbm", "achieved": achieved,

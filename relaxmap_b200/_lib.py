@@ -180,10 +180,17 @@ class Graph:
             out["p"] = p
         return out
 
-    def adjoint_backward(self, part, tau: float = 0.15) -> dict:
-        """dL/dw per link (CSR order of links()), dL/dtau and L at a fixed partition."""
+    def adjoint_backward(self, part, tau: float = 0.15, out=None) -> dict:
+        """dL/dw per link (CSR order of links()), dL/dtau and L at a fixed partition.
+        out: optional float64 array of n_links entries to receive dL/dw (e.g. a
+        view of pinned host memory, which the device copies into fastest)."""
         part = np.ascontiguousarray(part, dtype=np.int32)
-        g = np.zeros(max(self.n_links, 1))
+        if out is not None:
+            if out.dtype != np.float64 or not out.flags["C_CONTIGUOUS"] or len(out) < max(self.n_links, 1):
+                raise ValueError("out must be a contiguous float64 array of n_links entries")
+            g = out
+        else:
+            g = np.zeros(max(self.n_links, 1))
         dt, L = C.c_double(), C.c_double()
         _check(lib().rmx_adjoint_backward(self._h, _p(part), C.c_double(tau), _p(g), C.byref(dt), C.byref(L)))
         return {"dL_dw": g[: self.n_links], "dL_dtau": dt.value, "L": L.value}

@@ -186,68 +186,115 @@ __device__ __forceinline__ double adj_sum_parts(const double *parts, int nb, dou
     return r;
 }
 
+// Rows of one degree class, W lanes per row (W <= 32), every warp of the grid
+// taking 32/W rows at a time; rows of more than W links loop. Returns the
+// thread's share of sum tw_r y_r over the rows it wrote.
+template <int W>
+__device__ __forceinline__ double adj_pull_rows(const int32_t *__restrict__ rows, int64_t lo, int64_t hi,
+                                                const int64_t *__restrict__ off, const int32_t *__restrict__ dst,
+                                                const double *__restrict__ w0, const double *__restrict__ rowsum,
+                                                const uint8_t *__restrict__ dang, const double *__restrict__ c,
+                                                const double *__restrict__ tw, double beta, double T, const double *x,
+                                                double *y, int64_t gwarp, int64_t nwarps) {
+    constexpr int RPW = 32 / W;
+    const int lane = threadIdx.x & 31, sub = lane / W, lv = lane % W;
+    double ts = 0.0;
+    for (int64_t base = lo + gwarp * RPW; base < hi; base += nwarps * RPW) {
+        const int64_t i = base + sub;
+        double acc = 0.0;
+        int32_t r = -1;
+        if (i < hi) {
+            r = rows[i];
+            const int64_t e = off[r + 1];
+            for (int64_t k = off[r] + lv; k < e; k += W) acc += w0[k] * __ldcg(x + dst[k]);
+        }
+#pragma unroll
+        for (int o = W / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (r >= 0 && lv == 0) {
+            const double s = rowsum[r];
+            const double v = c[r] + beta * ((s > 0.0 ? acc / s : 0.0) + (dang[r] ? T : 0.0));
+            y[r] = v;
+            ts += tw[r] * v;
+        }
+    }
+    return ts;
+}
+
 // The transposed solve lambda = c + beta (W~ lambda + d (tw . lambda)) as one
-// cooperative launch: x <- c, then iterate the pull over the out-links until
-// the L1 change is below tol * L1 norm or max_iter sweeps. The contraction
-// factor is beta, so the error falls by beta per sweep.
-template <int VEC>
-__global__ void __launch_bounds__(kAdjT) k_adj_solve(const int64_t *__restrict__ off, const int32_t *__restrict__ dst,
-                                                     const double *__restrict__ w0, const double *__restrict__ rowsum,
-                                                     const double *__restrict__ tw, const uint8_t *__restrict__ dang,
-                                                     const double *__restrict__ c, int32_t n, double beta, double *x,
-                                                     double *y, double *parts, int max_iter, double tol,
-                                                     int *iters_out) {
+// cooperative launch, W~ the row-normalised out-links. Plain iteration
+// converges only as beta^k: M = W~^T + tw d^T is column-stochastic, so the
+// all-ones direction is an eigenvector of M^T with eigenvalue 1. The solution
+// obeys one exact linear condition, tw . lambda = p . c / t (multiply the
+// system by p^T and use p = beta M p + t tw), so after every sweep the iterate
+// is shifted along the ones vector to meet it: a Wielandt deflation of that
+// eigenvalue, leaving the contraction factor beta |lambda_2(M)| of the power
+// iteration. The dangling term then always uses tw . lambda = p . c / t.
+// Stops when the L1 change is below tol * L1 norm, or after max_iter sweeps.
+// Out-degrees are heavy-tailed, so rows come grouped by degree class (rows[],
+// class boundaries cls[0..7]: <= 1, 2, 4, 8, 16, 32 links, more), each class
+// with its own lane width.
+__global__ void __launch_bounds__(kAdjT, 4) k_adj_solve(const int64_t *__restrict__ off, const int32_t *__restrict__ dst,
+                                                        const double *__restrict__ w0,
+                                                        const double *__restrict__ rowsum,
+                                                        const double *__restrict__ tw, const uint8_t *__restrict__ dang,
+                                                        const double *__restrict__ c, const double *__restrict__ p,
+                                                        int32_t n, double alpha, double *x, double *y, double *parts,
+                                                        int max_iter, double tol, int *iters_out,
+                                                        const int32_t *__restrict__ rows,
+                                                        const int64_t *__restrict__ cls) {
     cg::grid_group grid = cg::this_grid();
     __shared__ double sh[32];
     const int nb = gridDim.x;
-    double *Tp = parts, *Ep = parts + nb, *Np = parts + 2 * nb;
+    const double beta = 1.0 - alpha;
+    double *Sp = parts, *Ep = parts + nb, *Np = parts + 2 * nb;
     const int64_t gtid = (int64_t)blockIdx.x * kAdjT + threadIdx.x, gthreads = (int64_t)nb * kAdjT;
-    double tl = 0.0;
+    double pc = 0.0, tc = 0.0;
     for (int64_t i = gtid; i < n; i += gthreads) {
-        x[i] = c[i];
-        tl += tw[i] * c[i];
+        pc += p[i] * c[i];
+        tc += tw[i] * c[i];
     }
-    tl = adj_block_sum<kAdjT>(tl, sh);
-    if (threadIdx.x == 0) Tp[blockIdx.x] = tl;
+    pc = adj_block_sum<kAdjT>(pc, sh);
+    tc = adj_block_sum<kAdjT>(tc, sh);
+    if (threadIdx.x == 0) {
+        Sp[blockIdx.x] = pc;
+        Ep[blockIdx.x] = tc;
+    }
     grid.sync();
-    constexpr int RPW = 32 / VEC;
-    const int lane = threadIdx.x & 31, sub = lane / VEC, lv = lane % VEC;
+    const double target = adj_sum_parts(Sp, nb, sh) / alpha;  // tw . lambda at the solution
+    const double d0 = target - adj_sum_parts(Ep, nb, sh);
+    for (int64_t i = gtid; i < n; i += gthreads) x[i] = c[i] + d0;
+    grid.sync();
     const int64_t gwarp = gtid >> 5, nwarps = gthreads >> 5;
+    int64_t cb[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) cb[k] = cls[k];
     int iter = 0;
     for (;;) {
-        const double T = adj_sum_parts(Tp, nb, sh);
-        for (int64_t base = gwarp * RPW; base < n; base += nwarps * RPW) {
-            const int64_t r = base + sub;
-            double acc = 0.0;
-            if (r < n) {
-                const int64_t e = off[r + 1];
-                for (int64_t k = off[r] + lv; k < e; k += VEC) acc += w0[k] * __ldcg(x + dst[k]);
-            }
-#pragma unroll
-            for (int o = VEC / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFullA, acc, o);
-            if (r < n && lv == 0) {
-                const double s = rowsum[r];
-                const double pull = s > 0.0 ? acc / s : 0.0;
-                y[r] = c[r] + beta * (pull + (dang[r] ? T : 0.0));
-            }
-        }
+        double ts = 0.0;
+        ts += adj_pull_rows<1>(rows, cb[0], cb[1], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp, nwarps);
+        ts += adj_pull_rows<2>(rows, cb[1], cb[2], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp, nwarps);
+        ts += adj_pull_rows<4>(rows, cb[2], cb[3], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp, nwarps);
+        ts += adj_pull_rows<8>(rows, cb[3], cb[4], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp, nwarps);
+        ts += adj_pull_rows<16>(rows, cb[4], cb[5], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp,
+                                nwarps);
+        ts += adj_pull_rows<32>(rows, cb[5], cb[7], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp,
+                                nwarps);
+        ts = adj_block_sum<kAdjT>(ts, sh);
+        if (threadIdx.x == 0) Sp[blockIdx.x] = ts;
         grid.sync();
+        const double shift = target - adj_sum_parts(Sp, nb, sh);
         double el = 0.0, nl = 0.0;
-        tl = 0.0;
         for (int64_t i = gtid; i < n; i += gthreads) {
-            const double v = __ldcg(y + i);
+            const double v = __ldcg(y + i) + shift;
             el += fabs(v - x[i]);
             nl += fabs(v);
-            tl += tw[i] * v;
             x[i] = v;
         }
         el = adj_block_sum<kAdjT>(el, sh);
         nl = adj_block_sum<kAdjT>(nl, sh);
-        tl = adj_block_sum<kAdjT>(tl, sh);
         if (threadIdx.x == 0) {
             Ep[blockIdx.x] = el;
             Np[blockIdx.x] = nl;
-            Tp[blockIdx.x] = tl;
         }
         grid.sync();
         const double diff = adj_sum_parts(Ep, nb, sh), norm = adj_sum_parts(Np, nb, sh);
@@ -311,24 +358,44 @@ __global__ void k_adj_dots(int32_t n, const double *lam, const double *tw, const
     }
 }
 
-template <int VEC>
+// Degree class of every row: 0..5 for <= 1, 2, 4, 8, 16, 32 links, 6 beyond.
+__global__ void k_adj_classes(int32_t n, const int64_t *off, uint16_t *cls, int32_t *ids) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = off[r + 1] - off[r];
+        int k = 0;
+        while (k < 6 && d > (int64_t(1) << k)) k++;
+        cls[r] = (uint16_t)k;
+        ids[r] = (int32_t)r;
+    }
+}
+
 int launch_solve(int32_t n, const int64_t *off, const int32_t *dst, const double *w0, const double *rowsum,
-                 const double *tw, const uint8_t *dang, const double *c, double beta, double *x, double *y,
-                 double *parts, int max_blocks, int max_iter, double tol, int *iters, cudaStream_t s) {
+                 const double *tw, const uint8_t *dang, const double *c, const double *p, double alpha, double *x,
+                 double *y, double *parts, int max_blocks, int max_iter, double tol, int *iters, Arena &ar,
+                 cudaStream_t s) {
     int dev = 0, per_sm = 0;
     RMX_CUDA(cudaGetDevice(&dev));
-    RMX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_solve<VEC>, kAdjT, 0));
+    RMX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_solve, kAdjT, 0));
     int nb = std::max(1, std::min(per_sm, 4)) * num_sms();
-    nb = (int)std::min<int64_t>(nb, std::max<int64_t>(1, ((int64_t)n * VEC + kAdjT - 1) / kAdjT));
+    nb = (int)std::min<int64_t>(nb, std::max<int64_t>(1, ((int64_t)n * 8 + kAdjT - 1) / kAdjT));
     nb = std::min(nb, max_blocks);
-    void *args[] = {(void *)&off, (void *)&dst,   (void *)&w0,       (void *)&rowsum, (void *)&tw,
-                    (void *)&dang, (void *)&c,    (void *)&n,        (void *)&beta,   (void *)&x,
-                    (void *)&y,   (void *)&parts, (void *)&max_iter, (void *)&tol,    (void *)&iters};
-    RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_adj_solve<VEC>, dim3(nb), dim3(kAdjT), args, 0, s));
+    size_t mk = ar.mark();
+    uint16_t *cls = ar.alloc<uint16_t>(std::max(n, 1));
+    int32_t *ids = ar.alloc<int32_t>(std::max(n, 1)), *rows = ar.alloc<int32_t>(std::max(n, 1));
+    int64_t *bounds = ar.alloc<int64_t>(8);
+    k_adj_classes<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, off, cls, ids);
+    RMX_LAUNCHED();
+    bucket_partition(cls, ids, rows, n, 7, bounds, ar, s);
+    void *args[] = {(void *)&off,   (void *)&dst,  (void *)&w0,       (void *)&rowsum, (void *)&tw,
+                    (void *)&dang,  (void *)&c,    (void *)&p,        (void *)&n,      (void *)&alpha,
+                    (void *)&x,     (void *)&y,    (void *)&parts,    (void *)&max_iter, (void *)&tol,
+                    (void *)&iters, (void *)&rows, (void *)&bounds};
+    RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_adj_solve, dim3(nb), dim3(kAdjT), args, 0, s));
     RMX_LAUNCHED();
     int h = 0;
     RMX_CUDA(cudaMemcpyAsync(&h, iters, sizeof(int), cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));
+    ar.release(mk);
     return h;
 }
 
@@ -344,7 +411,7 @@ struct Workspace {
 using namespace rmx;
 
 // Forward (and, with grad != nullptr, backward) pass. The partition is
-// validated on the host; the workspace is one device allocation of ~120 B per
+// validated on the host; the workspace is one device allocation of ~160 B per
 // node + 8 B per link, released before returning.
 void rmx_graph::adjoint(const int32_t *part_host, double tau, double *L_out, double *p_out, double *grad_out,
                         double *dL_dtau, int *solve_iters) {
@@ -355,7 +422,7 @@ void rmx_graph::adjoint(const int32_t *part_host, double tau, double *L_out, dou
     const int64_t Em = std::max<int64_t>(E, 1);
     const unsigned G = num_sms() * 4;
     const int kMaxBlocks = num_sms() * 4;
-    Workspace ws((size_t)N * 128 + (size_t)Em * 8 + (size_t)G * 64 + (size_t)kMaxBlocks * 32 + (16u << 20));
+    Workspace ws((size_t)N * 160 + (size_t)Em * 8 + (size_t)G * 64 + (size_t)kMaxBlocks * 32 + (32u << 20));
     Arena &A = ws.ar;
     int32_t *part = A.alloc<int32_t>(N);
     double *pa = A.alloc<double>(N), *rowsum = A.alloc<double>(N), *cross = A.alloc<double>(N);
@@ -402,21 +469,13 @@ void rmx_graph::adjoint(const int32_t *part_host, double tau, double *L_out, dou
         double explicit_t = 0;
         for (unsigned b = 0; b < G; b++) explicit_t += ht[b];
         double *sp = parts + 3 * G;
-        // the error of lambda falls by beta per sweep: 1e-15 relative within a few hundred sweeps
+        // deflated, the error falls as fast as in the power iteration
         const int max_iter = 4000;
         const double tol = 1e-15;
         int it = 0;
         timers.begin(kTimerAdjoint, stream);
-        switch (spmv_vec) {
-            case 4: it = launch_solve<4>(N, out_off, out_dst, out_w0, rowsum, tw, dangling, c, beta, lam, lam2, sp,
-                                         kMaxBlocks, max_iter, tol, iters, stream); break;
-            case 8: it = launch_solve<8>(N, out_off, out_dst, out_w0, rowsum, tw, dangling, c, beta, lam, lam2, sp,
-                                         kMaxBlocks, max_iter, tol, iters, stream); break;
-            case 16: it = launch_solve<16>(N, out_off, out_dst, out_w0, rowsum, tw, dangling, c, beta, lam, lam2, sp,
-                                           kMaxBlocks, max_iter, tol, iters, stream); break;
-            default: it = launch_solve<32>(N, out_off, out_dst, out_w0, rowsum, tw, dangling, c, beta, lam, lam2, sp,
-                                           kMaxBlocks, max_iter, tol, iters, stream); break;
-        }
+        it = launch_solve(N, out_off, out_dst, out_w0, rowsum, tw, dangling, c, pa, tau, lam, lam2, sp, kMaxBlocks,
+                          max_iter, tol, iters, A, stream);
         timers.end(kTimerAdjoint, stream);
         if (timers.on) prof.adjoint_iters += it;
         if (solve_iters) *solve_iters = it;
