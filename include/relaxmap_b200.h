@@ -82,6 +82,7 @@ typedef struct {
     int64_t links_evaluated; /* unit links read by move evaluation since profiling was enabled */
     int64_t units_evaluated; /* units evaluated since profiling was enabled */
     int64_t adjoint_iters;   /* sweeps of the transposed solve since profiling was enabled */
+    double level_ms[3];      /* device time of the sweep loops on nodes, super-nodes, coarse-tune sub-problems */
 } rmx_profile;
 
 const char *rmx_last_error(void);

@@ -47,7 +47,8 @@ class KernelStat(C.Structure):
 class Profile(C.Structure):
     _fields_ = [("k", KernelStat * 7), ("sweeps", C.c_int64), ("supersteps", C.c_int64),
                 ("power_iters", C.c_int64), ("total_ms", C.c_double), ("kernel_launches", C.c_int64),
-                ("links_evaluated", C.c_int64), ("units_evaluated", C.c_int64), ("adjoint_iters", C.c_int64)]
+                ("links_evaluated", C.c_int64), ("units_evaluated", C.c_int64), ("adjoint_iters", C.c_int64),
+                ("level_ms", C.c_double * 3)]
 
 
 _L = None
@@ -240,7 +241,8 @@ class Graph:
                for i, name in enumerate(KERNELS)}
         out.update(sweeps=pr.sweeps, supersteps=pr.supersteps, power_iters=pr.power_iters, total_ms=pr.total_ms,
                    kernel_launches=pr.kernel_launches, links_evaluated=pr.links_evaluated,
-                   units_evaluated=pr.units_evaluated, adjoint_iters=pr.adjoint_iters)
+                   units_evaluated=pr.units_evaluated, adjoint_iters=pr.adjoint_iters,
+                   level_ms={"nodes": pr.level_ms[0], "super_nodes": pr.level_ms[1], "coarse_tune": pr.level_ms[2]})
         return out
 
     def stream_ptr(self) -> int:

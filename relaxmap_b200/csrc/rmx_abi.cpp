@@ -356,6 +356,7 @@ rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out) {
         // and the new one written and copied back (8+8+8+8+1+8+8+8+8 B).
         out->k[RMX_K_ADJOINT].bytes =
             (double)g->prof.adjoint_iters * (20.0 * (double)g->E + 65.0 * (double)g->N);
+        for (int k = 0; k < 3; k++) out->level_ms[k] = g->timers.ms[rmx::kTimerLvNode + k];
         out->power_iters = g->power_iters;
         out->kernel_launches = (int64_t)__atomic_load_n(&rmx::g_kernel_launches, __ATOMIC_RELAXED);
     });

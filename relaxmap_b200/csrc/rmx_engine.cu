@@ -705,6 +705,8 @@ void rmx_graph::stage_sweeps(Level &lv, bool allow_new, std::vector<double> &L, 
     if (lv.n > 0) ensure_hub_table(max_degree(lv));
     std::vector<uint8_t> sweeping = act;
     std::vector<double> oldL;
+    const int lvt = &lv == &node_lv ? kTimerLvNode : kTimerLvSN;
+    timers.begin(lvt, stream);
     int iter = 0;
     while (any_set(sweeping) && iter < opt.max_iter) {
         oldL = L;
@@ -718,6 +720,7 @@ void rmx_graph::stage_sweeps(Level &lv, bool allow_new, std::vector<double> &L, 
         for (int32_t k = 0; k < K; k++)
             if (sweeping[k] && oldL[k] - L[k] >= 0 && (oldL[k] - L[k]) / kLn2 < opt.threshold) sweeping[k] = 0;
     }
+    timers.end(lvt, stream);
 }
 
 void rmx_graph::project_sn_to_nodes() {
@@ -816,6 +819,7 @@ void rmx_graph::generate_sub_modules() {
         ensure_hub_table(max_degree(sub_lv));
         Timers *tm = timers.on ? &timers : nullptr;
         SweepArgs sa{0.0, 0};  // Network::move: best < 0, no empty module (Module.cpp:606, :667)
+        timers.begin(kTimerLvSub, stream);
         for (int iter = 0; iter < opt.max_iter; iter++) {
             all_units(N, work, stream);
             const uint32_t seed = mix_seed(run_seed, ++sweep_no);
@@ -837,6 +841,7 @@ void rmx_graph::generate_sub_modules() {
             prof.sweeps++;
             if (h == 0) break;
         }
+        timers.end(kTimerLvSub, stream);
     }
     // sub-modules -> super-nodes (generateSuperNodesFromSubModules, Module.cpp:3083-3158)
     timers.begin(kTimerCoarsen, stream);
@@ -953,7 +958,7 @@ std::vector<double> rmx_graph::run_attempt(uint32_t seed) {
 std::vector<double> rmx_graph::run_union(const rmx_opts &o) {
     opt = o;
     if (opt.max_iter < 0) opt.max_iter = 0;
-    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 36) : 4;
+    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 32) : 4;
     cudaEvent_t t0, t1;
     RMX_CUDA(cudaEventCreate(&t0));
     RMX_CUDA(cudaEventCreate(&t1));
@@ -975,7 +980,7 @@ double rmx_graph::optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modu
     opt = o;
     if (opt.max_iter < 0) opt.max_iter = 0;
     if (opt.attempts < 1) opt.attempts = 1;
-    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 36) : 4;
+    nsub = opt.sub_batches > 0 ? std::min(opt.sub_batches, 32) : 4;
     cudaEvent_t t0, t1;
     RMX_CUDA(cudaEventCreate(&t0));
     RMX_CUDA(cudaEventCreate(&t1));

@@ -108,7 +108,11 @@ void refresh_terms(ModState &M, cudaStream_t s);
 // Code length per instance from the module statistics.
 void instance_codelength(const ModState &M, InstState &I, cudaStream_t s);
 // Device time per kernel class, recorded with CUDA events on the stream.
-enum { kTimerSpmv = 0, kTimerEval, kTimerCommit, kTimerCoarsen, kTimerCodelen, kTimerOther, kTimerAdjoint, kTimerCount };
+enum {
+    kTimerSpmv = 0, kTimerEval, kTimerCommit, kTimerCoarsen, kTimerCodelen, kTimerOther, kTimerAdjoint,
+    // whole sweep loops by level (they contain the kernel classes above)
+    kTimerLvNode, kTimerLvSN, kTimerLvSub, kTimerCount
+};
 struct Timers {
     bool on = false;
     std::vector<cudaEvent_t> pool;
@@ -149,8 +153,8 @@ struct SweepWork {
     fx_t *gtable = nullptr;                     // hub hash tables: hub_blocks() slices of
     int32_t *gkeys = nullptr;                   //   hub_slots(gcap) entries
     int64_t gcap = 0;
-    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};  // concurrent degree bins
-    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};  // concurrent degree bins
+    cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
 void configure_eval_kernels();

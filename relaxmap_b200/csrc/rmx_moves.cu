@@ -195,8 +195,11 @@ __device__ __forceinline__ void mark_neighbours(const EvalArgs &a, int32_t u, in
 constexpr int kWarpMaxDeg = 128, kWarpCap = 256, kEvalWarps = 8;
 // degree bins: 8 / 16 / 32 lanes in registers, warp (shared table), block
 // (shared table), hub (global table)
-constexpr int kBins = 7;
-constexpr int kBinReg8 = 0, kBinReg16 = 1, kBinReg32 = 2, kBinWarp = 3, kBinBlock = 4, kBinLarge = 5, kBinHub = 6;
+constexpr int kBins = 8;
+constexpr int kBinReg8 = 0, kBinReg16 = 1, kBinReg32 = 2, kBinWarp = 3, kBinMid = 4, kBinBlock = 5, kBinLarge = 6,
+              kBinHub = 7;
+// units of 129..512 links: four warps each (eight teams per SM), a 1024-slot table
+constexpr int kMidT = 128, kMidMaxDeg = 512, kMidCap = 1024;
 constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
 // resident blocks per SM of the block bin and grid multipliers of the bins
 #ifndef RMX_BLK_MINB
@@ -210,6 +213,16 @@ constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
 #endif
 #ifndef RMX_REG_GRID
 #define RMX_REG_GRID 8
+#endif
+// resident blocks per SM the register bin, warp bin and out-flow update are compiled for
+#ifndef RMX_REG_MINB
+#define RMX_REG_MINB 4
+#endif
+#ifndef RMX_WARP_MINB
+#define RMX_WARP_MINB 3
+#endif
+#ifndef RMX_DELTA_MINB
+#define RMX_DELTA_MINB 6
 #endif
 constexpr int kLrgT = 512, kLrgMaxDeg = 4096, kLrgCap = 8192;
 constexpr int kHubT = 512;
@@ -443,7 +456,7 @@ __device__ __forceinline__ void eval_unit_reg(const EvalArgs &a, const int32_t u
 }
 
 // Bins reg8, reg16, reg32: ranges range[0..3) of consecutive buckets.
-__global__ void __launch_bounds__(256) k_eval_reg(EvalArgs a) {
+__global__ void __launch_bounds__(256, RMX_REG_MINB) k_eval_reg(EvalArgs a) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long seen = 0, units = 0, cands = 0;
@@ -497,7 +510,7 @@ __device__ __forceinline__ void flush_stats_split(const EvalArgs &a, unsigned lo
     if (cands) atomicAdd(a.stats + 2, cands);
 }
 
-__global__ void __launch_bounds__(kEvalWarps * 32, 3) k_eval_warp(EvalArgs a) {
+__global__ void __launch_bounds__(kEvalWarps * 32, RMX_WARP_MINB) k_eval_warp(EvalArgs a) {
     __shared__ int32_t skey[kEvalWarps][kWarpCap];
     __shared__ fx_t sout[kEvalWarps][kWarpCap];
     __shared__ fx_t sin_[kEvalWarps][kWarpCap];
@@ -518,7 +531,7 @@ __global__ void __launch_bounds__(kEvalWarps * 32, 3) k_eval_warp(EvalArgs a) {
 }
 
 template <int NT, int CAP, bool GLOBAL>
-__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : RMX_BLK_MINB) k_eval_block(EvalArgs a) {
+__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : (NT == 128 ? 8 : RMX_BLK_MINB)) k_eval_block(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ GroupShared<NT> sh;
     int32_t *keys;
@@ -633,7 +646,7 @@ __global__ void k_commit(CommitArgs a) {
 
 struct DeltaArgs {
     const int32_t *list;
-    const int64_t *range;
+    const int64_t *beg, *end;  // the units at list[*beg .. *end)
     const int32_t *mod, *prevmod;
     const uint32_t *stamp_of;
     const int64_t *out_off, *in_off;
@@ -650,33 +663,40 @@ struct DeltaArgs {
 // (OUT[A] grows) and in-links from T stop crossing (OUT[T] shrinks). Links whose
 // two ends both moved are handled once, by the source's out-link loop. The
 // warp sums its lanes' changes, so each mover costs two atomics.
-__global__ void __launch_bounds__(256) k_delta(DeltaArgs a) {
+// Changes of OUT[A] and OUT[T] from the links of mover u, summed by the
+// calling thread over links j = first, first + stride, ...
+__device__ __forceinline__ void delta_links(const DeltaArgs &a, int32_t u, int32_t A, int32_t T, int first, int stride,
+                                            fx_t &dA, fx_t &dT) {
+    for (int64_t e = a.out_off[u] + first; e < a.out_off[u + 1]; e += stride) {
+        const int32_t w = a.out_dst[e];
+        const fx_t q = a.out_fx[e];
+        const bool wm = a.stamp_of[w] == a.stamp;
+        const int32_t bn = a.mod[w], bo = wm ? a.prevmod[w] : bn;
+        if (A != bo) dA -= q;
+        if (T != bn) dT += q;
+    }
+    for (int64_t e = a.in_off[u] + first; e < a.in_off[u + 1]; e += stride) {
+        const int32_t w = a.in_src[e];
+        if (a.stamp_of[w] != a.stamp) {
+            const int32_t b = a.mod[w];
+            if (b == A)
+                dA += a.in_fx[e];
+            else if (b == T)
+                dT -= a.in_fx[e];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256, RMX_DELTA_MINB) k_delta(DeltaArgs a) {
     const int lane = threadIdx.x & 31;
-    const int64_t beg = a.range[0], end = a.range[1];
+    const int64_t beg = *a.beg, end = *a.end;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t i = beg + gw; i < end; i += nw) {
         const int32_t u = a.list[i];
         if (a.stamp_of[u] != a.stamp) continue;  // did not move in this sub-batch
         const int32_t A = a.prevmod[u], T = a.mod[u];
         fx_t dA = 0, dT = 0;
-        for (int64_t e = a.out_off[u] + lane; e < a.out_off[u + 1]; e += 32) {
-            const int32_t w = a.out_dst[e];
-            const fx_t q = a.out_fx[e];
-            const bool wm = a.stamp_of[w] == a.stamp;
-            const int32_t bn = a.mod[w], bo = wm ? a.prevmod[w] : bn;
-            if (A != bo) dA -= q;
-            if (T != bn) dT += q;
-        }
-        for (int64_t e = a.in_off[u] + lane; e < a.in_off[u + 1]; e += 32) {
-            const int32_t w = a.in_src[e];
-            if (a.stamp_of[w] != a.stamp) {
-                const int32_t b = a.mod[w];
-                if (b == A)
-                    dA += a.in_fx[e];
-                else if (b == T)
-                    dT -= a.in_fx[e];
-            }
-        }
+        delta_links(a, u, A, T, lane, 32, dA, dT);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             dA += __shfl_xor_sync(kFull, dA, o);
@@ -686,6 +706,41 @@ __global__ void __launch_bounds__(256) k_delta(DeltaArgs a) {
             if (dA) atomic_add_fx(&a.mstat[A].OUT, dA);
             if (dT) atomic_add_fx(&a.mstat[T].OUT, dT);
         }
+    }
+}
+
+// Movers of more than 128 links: a block each, so that one heavy super-node
+// does not leave a single warp walking thousands of links.
+__global__ void __launch_bounds__(256) k_delta_block(DeltaArgs a) {
+    __shared__ fx_t sh[2][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t beg = *a.beg, end = *a.end;
+    for (int64_t i = beg + blockIdx.x; i < end; i += gridDim.x) {
+        const int32_t u = a.list[i];
+        if (a.stamp_of[u] != a.stamp) continue;  // uniform across the block
+        const int32_t A = a.prevmod[u], T = a.mod[u];
+        fx_t dA = 0, dT = 0;
+        delta_links(a, u, A, T, threadIdx.x, 256, dA, dT);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dA += __shfl_xor_sync(kFull, dA, o);
+            dT += __shfl_xor_sync(kFull, dT, o);
+        }
+        if (lane == 0) {
+            sh[0][w] = dA;
+            sh[1][w] = dT;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            fx_t tA = 0, tT = 0;
+            for (int k = 0; k < 8; k++) {
+                tA += sh[0][k];
+                tT += sh[1][k];
+            }
+            if (tA) atomic_add_fx(&a.mstat[A].OUT, tA);
+            if (tT) atomic_add_fx(&a.mstat[T].OUT, tT);
+        }
+        __syncthreads();
     }
 }
 
@@ -904,6 +959,7 @@ int64_t warp_bin_max_degree() { return kWarpMaxDeg; }
 int64_t hub_slots(int64_t cap) { return cap; }
 
 constexpr size_t kBlkSmem = (size_t)kBlkCap * (2 * sizeof(fx_t) + sizeof(int32_t));
+constexpr size_t kMidSmem = (size_t)kMidCap * (2 * sizeof(fx_t) + sizeof(int32_t));
 constexpr size_t kLrgSmem = (size_t)kLrgCap * (2 * sizeof(fx_t) + sizeof(int32_t));
 
 // The bins of a sub-batch run concurrently: block, large + hub, and the warp
@@ -911,7 +967,10 @@ constexpr size_t kLrgSmem = (size_t)kLrgCap * (2 * sizeof(fx_t) + sizeof(int32_t
 // register bins on s itself.
 static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket, const SweepWork &W, cudaStream_t s) {
     RMX_CUDA(cudaEventRecord(W.fork, s));
-    for (int k = 0; k < 3; k++) RMX_CUDA(cudaStreamWaitEvent(W.aux[k], W.fork, 0));
+    for (int k = 0; k < 4; k++) RMX_CUDA(cudaStreamWaitEvent(W.aux[k], W.fork, 0));
+    a.range = bucket_off + first_bucket + kBinMid;
+    k_eval_block<kMidT, kMidCap, false><<<num_sms() * 8, kMidT, kMidSmem, W.aux[3]>>>(a);
+    RMX_LAUNCHED();
     a.range = bucket_off + first_bucket + kBinBlock;
     k_eval_block<kBlkT, kBlkCap, false><<<num_sms() * RMX_BLK_GRID, kBlkT, kBlkSmem, W.aux[0]>>>(a);
     RMX_LAUNCHED();
@@ -929,7 +988,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     a.range = bucket_off + first_bucket + kBinReg8;
     k_eval_reg<<<num_sms() * RMX_REG_GRID, 256, 0, s>>>(a);
     RMX_LAUNCHED();
-    for (int k = 0; k < 3; k++) {
+    for (int k = 0; k < 4; k++) {
         RMX_CUDA(cudaEventRecord(W.join[k], W.aux[k]));
         RMX_CUDA(cudaStreamWaitEvent(s, W.join[k], 0));
     }
@@ -971,6 +1030,7 @@ __global__ void k_bucket(const int32_t *list, const int64_t *n_active, const int
                         : d <= 16 ? kBinReg16
                         : d <= 32 ? kBinReg32
                         : d <= kWarpMaxDeg ? kBinWarp
+                        : d <= kMidMaxDeg ? kBinMid
                         : d <= kBlkMaxDeg ? kBinBlock
                         : d <= kLrgMaxDeg ? kBinLarge
                                           : kBinHub;
@@ -1049,7 +1109,6 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     RMX_LAUNCHED();
     DeltaArgs da;
     da.list = W.list2;
-    da.range = W.ranges + 2 * sb;
     da.mod = L.mod;
     da.prevmod = W.prevmod;
     da.stamp_of = W.stamp;
@@ -1061,7 +1120,15 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     da.in_fx = L.in_fx;
     da.mstat = M.stat;
     da.stamp = stamp;
+    // light movers (<= 128 links) a warp each, heavy ones a block each
+    const int64_t *bo = W.bucket_off + sb * kBins;
+    da.beg = bo + kBinReg8;
+    da.end = bo + kBinMid;
     k_delta<<<G, 256, 0, s>>>(da);
+    RMX_LAUNCHED();
+    da.beg = bo + kBinMid;
+    da.end = bo + kBins;
+    k_delta_block<<<num_sms() * 4, 256, 0, s>>>(da);
     RMX_LAUNCHED();
     k_terms_movers<<<G, 256, 0, s>>>(W.list2, W.ranges + 2 * sb, W.stamp, stamp, L.mod, W.prevmod, M.stat, M.term);
     RMX_LAUNCHED();
