@@ -153,6 +153,7 @@ struct SweepWork {
     fx_t *gtable = nullptr;                     // hub hash tables: hub_blocks() slices of
     int32_t *gkeys = nullptr;                   //   hub_slots(gcap) entries
     int64_t gcap = 0;
+    std::vector<int64_t> bucket_host;  // host copy of bucket_off after bucket_units
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};  // concurrent degree bins
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
 };

@@ -965,33 +965,66 @@ constexpr size_t kLrgSmem = (size_t)kLrgCap * (2 * sizeof(fx_t) + sizeof(int32_t
 // The bins of a sub-batch run concurrently: block, large + hub, and the warp
 // bin on three auxiliary streams forked from and joined back into s, the
 // register bins on s itself.
+static unsigned fit_grid(int64_t items, int64_t per_block, int64_t max_grid) {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(max_grid, (items + per_block - 1) / per_block));
+}
+
+// The bins of a sub-batch run concurrently: mid, block, large + hub, and warp
+// bins on four auxiliary streams forked from and joined back into s, the
+// register bins on s itself. Only non-empty bins are launched (sizes from the
+// host copy of the bucket offsets); a lone bin runs on s without the fork.
 static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket, const SweepWork &W, cudaStream_t s) {
-    RMX_CUDA(cudaEventRecord(W.fork, s));
-    for (int k = 0; k < 4; k++) RMX_CUDA(cudaStreamWaitEvent(W.aux[k], W.fork, 0));
-    a.range = bucket_off + first_bucket + kBinMid;
-    k_eval_block<kMidT, kMidCap, false><<<num_sms() * 8, kMidT, kMidSmem, W.aux[3]>>>(a);
-    RMX_LAUNCHED();
-    a.range = bucket_off + first_bucket + kBinBlock;
-    k_eval_block<kBlkT, kBlkCap, false><<<num_sms() * RMX_BLK_GRID, kBlkT, kBlkSmem, W.aux[0]>>>(a);
-    RMX_LAUNCHED();
-    a.range = bucket_off + first_bucket + kBinLarge;
-    k_eval_block<kLrgT, kLrgCap, false><<<num_sms(), kLrgT, kLrgSmem, W.aux[1]>>>(a);
-    RMX_LAUNCHED();
-    if (a.gcap > 0) {
-        a.range = bucket_off + first_bucket + kBinHub;
-        k_eval_block<kHubT, 0, true><<<hub_blocks(), kHubT, 0, W.aux[1]>>>(a);
+    const int64_t *h = W.bucket_host.data() + first_bucket;
+    auto cnt = [&](int b0, int b1) { return h[b1] - h[b0]; };
+    const int64_t n_mid = cnt(kBinMid, kBinMid + 1), n_blk = cnt(kBinBlock, kBinBlock + 1),
+                  n_lrg = cnt(kBinLarge, kBinLarge + 1), n_hub = a.gcap > 0 ? cnt(kBinHub, kBinHub + 1) : 0,
+                  n_warp = cnt(kBinWarp, kBinWarp + 1), n_reg = cnt(kBinReg8, kBinReg32 + 1);
+    const bool use[4] = {n_blk > 0, n_lrg + n_hub > 0, n_warp > 0, n_mid > 0};
+    const int streams = (int)use[0] + (int)use[1] + (int)use[2] + (int)use[3] + (n_reg > 0 ? 1 : 0);
+    const bool fork = streams > 1;
+    auto on = [&](int k) { return fork ? W.aux[k] : s; };
+    if (fork) {
+        RMX_CUDA(cudaEventRecord(W.fork, s));
+        for (int k = 0; k < 4; k++)
+            if (use[k]) RMX_CUDA(cudaStreamWaitEvent(W.aux[k], W.fork, 0));
+    }
+    if (n_mid > 0) {
+        a.range = bucket_off + first_bucket + kBinMid;
+        k_eval_block<kMidT, kMidCap, false><<<fit_grid(n_mid, 1, num_sms() * 8), kMidT, kMidSmem, on(3)>>>(a);
         RMX_LAUNCHED();
     }
-    a.range = bucket_off + first_bucket + kBinWarp;
-    k_eval_warp<<<num_sms() * RMX_WARP_GRID, kEvalWarps * 32, 0, W.aux[2]>>>(a);
-    RMX_LAUNCHED();
-    a.range = bucket_off + first_bucket + kBinReg8;
-    k_eval_reg<<<num_sms() * RMX_REG_GRID, 256, 0, s>>>(a);
-    RMX_LAUNCHED();
-    for (int k = 0; k < 4; k++) {
-        RMX_CUDA(cudaEventRecord(W.join[k], W.aux[k]));
-        RMX_CUDA(cudaStreamWaitEvent(s, W.join[k], 0));
+    if (n_blk > 0) {
+        a.range = bucket_off + first_bucket + kBinBlock;
+        k_eval_block<kBlkT, kBlkCap, false><<<fit_grid(n_blk, 1, num_sms() * RMX_BLK_GRID), kBlkT, kBlkSmem, on(0)>>>(
+            a);
+        RMX_LAUNCHED();
     }
+    if (n_lrg > 0) {
+        a.range = bucket_off + first_bucket + kBinLarge;
+        k_eval_block<kLrgT, kLrgCap, false><<<fit_grid(n_lrg, 1, num_sms()), kLrgT, kLrgSmem, on(1)>>>(a);
+        RMX_LAUNCHED();
+    }
+    if (n_hub > 0) {  // global table slices are indexed by block: at most hub_blocks() blocks
+        a.range = bucket_off + first_bucket + kBinHub;
+        k_eval_block<kHubT, 0, true><<<fit_grid(n_hub, 1, hub_blocks()), kHubT, 0, on(1)>>>(a);
+        RMX_LAUNCHED();
+    }
+    if (n_warp > 0) {
+        a.range = bucket_off + first_bucket + kBinWarp;
+        k_eval_warp<<<fit_grid(n_warp, kEvalWarps, num_sms() * RMX_WARP_GRID), kEvalWarps * 32, 0, on(2)>>>(a);
+        RMX_LAUNCHED();
+    }
+    if (n_reg > 0) {
+        a.range = bucket_off + first_bucket + kBinReg8;
+        k_eval_reg<<<fit_grid(n_reg, 8, num_sms() * RMX_REG_GRID), 256, 0, s>>>(a);
+        RMX_LAUNCHED();
+    }
+    if (fork)
+        for (int k = 0; k < 4; k++)
+            if (use[k]) {
+                RMX_CUDA(cudaEventRecord(W.join[k], W.aux[k]));
+                RMX_CUDA(cudaStreamWaitEvent(s, W.join[k], 0));
+            }
 }
 
 void configure_eval_kernels() {
@@ -1056,6 +1089,11 @@ void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed,
     bucket_partition(W.bucket, W.list, W.list2, n_active, nsub * kBins, W.bucket_off, ar, s);
     k_ranges<<<1, 128, 0, s>>>(W.bucket_off, nsub, W.ranges);
     RMX_LAUNCHED();
+    // the bins' sizes on the host: empty bins are not launched, grids fit the work
+    W.bucket_host.resize((size_t)nsub * kBins + 1);
+    RMX_CUDA(cudaMemcpyAsync(W.bucket_host.data(), W.bucket_off, sizeof(int64_t) * W.bucket_host.size(),
+                             cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
 }
 
 __global__ void k_empty_flags(int32_t cap, const int32_t *mcount, uint8_t *flag) {
@@ -1074,6 +1112,9 @@ void free_modules(const ModState &M, SweepWork &W, Arena &ar, cudaStream_t s) {
 
 void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &W, const SweepArgs &sa, int sb,
                     uint32_t stamp, uint32_t hseed, bool mark_active, cudaStream_t s, Timers *tm) {
+    const int64_t *hb = W.bucket_host.data() + sb * kBins;
+    const int64_t total = hb[kBins] - hb[0], n_light = hb[kBinMid] - hb[kBinReg8], n_heavy = hb[kBins] - hb[kBinMid];
+    if (total == 0) return;
     EvalArgs ea = eval_args(L, M, I, W, sa.vthresh, sa.allow_new, nullptr, 1);
     ea.mark = mark_active ? 1 : 0;
     if (tm) tm->begin(kTimerEval, s);
@@ -1100,7 +1141,7 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     ca.moved_nodes = reinterpret_cast<unsigned long long *>(W.counters + kCntMoved);
     ca.stamp = stamp;
     ca.hseed = hseed;
-    const unsigned G = num_sms() * 8;
+    const unsigned G = fit_grid(total, 256, num_sms() * 8);
     if (sa.allow_new) {
         k_claim<<<G, 256, 0, s>>>(ca);
         RMX_LAUNCHED();
@@ -1122,14 +1163,18 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     da.stamp = stamp;
     // light movers (<= 128 links) a warp each, heavy ones a block each
     const int64_t *bo = W.bucket_off + sb * kBins;
-    da.beg = bo + kBinReg8;
-    da.end = bo + kBinMid;
-    k_delta<<<G, 256, 0, s>>>(da);
-    RMX_LAUNCHED();
-    da.beg = bo + kBinMid;
-    da.end = bo + kBins;
-    k_delta_block<<<num_sms() * 4, 256, 0, s>>>(da);
-    RMX_LAUNCHED();
+    if (n_light > 0) {
+        da.beg = bo + kBinReg8;
+        da.end = bo + kBinMid;
+        k_delta<<<fit_grid(n_light, 8, num_sms() * 8), 256, 0, s>>>(da);
+        RMX_LAUNCHED();
+    }
+    if (n_heavy > 0) {
+        da.beg = bo + kBinMid;
+        da.end = bo + kBins;
+        k_delta_block<<<fit_grid(n_heavy, 1, num_sms() * 4), 256, 0, s>>>(da);
+        RMX_LAUNCHED();
+    }
     k_terms_movers<<<G, 256, 0, s>>>(W.list2, W.ranges + 2 * sb, W.stamp, stamp, L.mod, W.prevmod, M.stat, M.term);
     RMX_LAUNCHED();
     if (tm) tm->end(kTimerCommit, s);
