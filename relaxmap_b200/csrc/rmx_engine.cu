@@ -326,6 +326,9 @@ rmx_graph::~rmx_graph() {
     if (work.gtable) cudaFree(work.gtable);
     if (work.gkeys) cudaFree(work.gkeys);
     if (agg_tab) cudaFree(agg_tab);
+    for (SweepGraph &g : sweep_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (work.hparams) cudaFreeHost(work.hparams);
     perm.destroy();
     scratch.destroy();
     if (stream) cudaStreamDestroy(stream);
@@ -557,6 +560,8 @@ void rmx_graph::alloc_engine() {
     work.free_list = perm.alloc<int32_t>(n);
     work.claim = perm.alloc<unsigned long long>(n);
     work.counters = perm.alloc<int64_t>(kCntSlots);
+    work.dparams = perm.alloc<uint32_t>(64);
+    RMX_CUDA(cudaMallocHost(&work.hparams, sizeof(uint32_t) * 64));
     RMX_CUDA(cudaMemsetAsync(work.stamp, 0, sizeof(uint32_t) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.claim, 0, sizeof(unsigned long long) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.next_active, 0, n, stream));
@@ -648,6 +653,58 @@ int rmx_graph::union_flows() {
 
 // ---------------------------------------------------------------- sweeps
 
+// Buckets the active units of lv into ns sub-batches and runs them. Without
+// profiling the sub-batch pipeline (about ten launches per sub-batch over
+// five streams) is one CUDA graph, captured once per (level, module state,
+// instances, sweep options) and replayed: the sub-batches' stamps and hash
+// seeds live in device memory, and every kernel reads its unit range there.
+// With profiling on, the kernels are launched one by one between the timing
+// events, grids fitted to the bin sizes.
+void rmx_graph::run_subbatches(Level &lv, int64_t n_active, ModState &M, InstState &I, const SweepArgs &sa, int ns,
+                               bool mark, uint32_t seed) {
+    const bool graphs = !timers.on && use_graphs;
+    bucket_units(lv, work, n_active, seed, ns, scratch, stream, !graphs);
+    for (int sb = 0; sb < ns; sb++) {
+        work.hparams[2 * sb] = ++stamp;
+        work.hparams[2 * sb + 1] = mix_seed(seed, sb);
+    }
+    RMX_CUDA(cudaMemcpyAsync(work.dparams, work.hparams, sizeof(uint32_t) * 2 * ns, cudaMemcpyHostToDevice, stream));
+    if (!graphs) {
+        Timers *tm = timers.on ? &timers : nullptr;
+        for (int sb = 0; sb < ns; sb++)
+            sweep_subbatch(lv, M, I, work, sa, sb, work.dparams + 2 * sb, mark, true, stream, tm);
+        return;
+    }
+    const SweepGraphKey key{&lv, &M, &I, sa.allow_new, mark ? 1 : 0, sa.vthresh, ns, work.gtable, work.gcap};
+    SweepGraph *gr = nullptr;
+    for (SweepGraph &g : sweep_graphs)
+        if (g.key == key) gr = &g;
+    if (!gr) {
+        const unsigned long long c0 = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
+        cudaGraph_t graph = nullptr;
+        RMX_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            for (int sb = 0; sb < ns; sb++)
+                sweep_subbatch(lv, M, I, work, sa, sb, work.dparams + 2 * sb, mark, false, stream, nullptr);
+        } catch (...) {
+            cudaStreamEndCapture(stream, &graph);
+            if (graph) cudaGraphDestroy(graph);
+            throw;
+        }
+        RMX_CUDA(cudaStreamEndCapture(stream, &graph));
+        const unsigned long long c1 = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
+        __atomic_fetch_sub(&g_kernel_launches, c1 - c0, __ATOMIC_RELAXED);  // counted when replayed
+        cudaGraphExec_t exec = nullptr;
+        const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        RMX_CUDA(e);
+        sweep_graphs.push_back({key, exec, c1 - c0});
+        gr = &sweep_graphs.back();
+    }
+    RMX_CUDA(cudaGraphLaunch(gr->exec, stream));
+    __atomic_fetch_add(&g_kernel_launches, gr->kernels, __ATOMIC_RELAXED);
+}
+
 // Uploads which instances take part in the next sweeps (their units are
 // evaluated; the others keep their modules).
 void rmx_graph::set_active(const std::vector<uint8_t> &m) {
@@ -664,11 +721,8 @@ void rmx_graph::sweep_single(Level &lv, bool prior, bool allow_new, double vthre
     if (allow_new) free_modules(mods, work, scratch, stream);
     const uint32_t seed = mix_seed(run_seed, ++sweep_no);
     const int ns = sub_batches_for(n_active);
-    bucket_units(lv, work, n_active, seed, ns, scratch, stream);
     SweepArgs sa{vthresh, allow_new ? 1 : 0};
-    Timers *tm = timers.on ? &timers : nullptr;
-    for (int sb = 0; sb < ns; sb++)
-        sweep_subbatch(lv, mods, inst1, work, sa, sb, ++stamp, mix_seed(seed, sb), prior, stream, tm);
+    run_subbatches(lv, n_active, mods, inst1, sa, ns, prior, seed);
     timers.begin(kTimerCodelen, stream);
     instance_codelength(mods, inst1, stream);
     timers.end(kTimerCodelen, stream);
@@ -824,9 +878,7 @@ void rmx_graph::generate_sub_modules() {
             all_units(N, work, stream);
             const uint32_t seed = mix_seed(run_seed, ++sweep_no);
             const int ns = sub_batches_for(N);
-            bucket_units(sub_lv, work, N, seed, ns, scratch, stream);
-            for (int sb = 0; sb < ns; sb++)
-                sweep_subbatch(sub_lv, submods, instsub, work, sa, sb, ++stamp, mix_seed(seed, sb), false, stream, tm);
+            run_subbatches(sub_lv, N, submods, instsub, sa, ns, false, seed);
             timers.begin(kTimerCodelen, stream);
             instance_codelength(submods, instsub, stream);
             unsigned long long *na = reinterpret_cast<unsigned long long *>(dtmp + 9);

@@ -154,6 +154,8 @@ struct SweepWork {
     int32_t *gkeys = nullptr;                   //   hub_slots(gcap) entries
     int64_t gcap = 0;
     std::vector<int64_t> bucket_host;  // host copy of bucket_off after bucket_units
+    uint32_t *dparams = nullptr;       // device {stamp, hseed} per sub-batch of the current sweep
+    uint32_t *hparams = nullptr;       // pinned host staging of dparams
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};  // concurrent degree bins
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
 };
@@ -164,14 +166,17 @@ int64_t warp_bin_max_degree();
 int64_t block_bin_max_degree();
 int64_t hub_slots(int64_t cap);
 void all_units(int32_t n, SweepWork &W, cudaStream_t s);
-void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed, int nsub, Arena &ar, cudaStream_t s);
+// host_counts: also copy the bin offsets to W.bucket_host (one stream sync).
+void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed, int nsub, Arena &ar, cudaStream_t s,
+                  bool host_counts = true);
 void free_modules(const ModState &M, SweepWork &W, Arena &ar, cudaStream_t s);
 // Evaluate, claim, commit and apply link deltas for sub-batch sb.
-// stamp: unique per sub-batch over the handle's life (marks this sub-batch's
-// movers); hseed: a function of (attempt seed, sweep, sub-batch) only, so runs
-// with the same seed make the same choices.
+// sp: device {stamp, hseed} of the sub-batch. stamp: unique per sub-batch over
+// the handle's life (marks this sub-batch's movers); hseed: a function of
+// (attempt seed, sweep, sub-batch) only, so runs with the same seed make the
+// same choices. fitted: use the host bin sizes (see bucket_units).
 void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &W, const SweepArgs &a, int sb,
-                    uint32_t stamp, uint32_t hseed, bool mark_active, cudaStream_t s, Timers *tm);
+                    const uint32_t *sp, bool mark_active, bool fitted, cudaStream_t s, Timers *tm);
 // Move evaluation only, for the parity hook (no commit).
 void evaluate_all(const Level &L, const ModState &M, const InstState &I, SweepWork &W, const uint8_t *allow_new,
                   double vthresh, Arena &ar, cudaStream_t s);

@@ -23,6 +23,27 @@ struct UnionSpec {
     int64_t full_edges = 0;
 };
 
+// The captured sub-batch pipeline of one sweep configuration.
+struct SweepGraphKey {
+    const rmx::Level *lv;
+    const rmx::ModState *M;
+    const rmx::InstState *I;
+    int allow_new, mark;
+    double vthresh;
+    int nsub;
+    const void *gtable;
+    int64_t gcap;
+    bool operator==(const SweepGraphKey &o) const {
+        return lv == o.lv && M == o.M && I == o.I && allow_new == o.allow_new && mark == o.mark &&
+               vthresh == o.vthresh && nsub == o.nsub && gtable == o.gtable && gcap == o.gcap;
+    }
+};
+struct SweepGraph {
+    SweepGraphKey key;
+    cudaGraphExec_t exec;
+    unsigned long long kernels;  // kernel nodes, counted as launches per replay
+};
+
 struct rmx_graph {
     // ---- host-side description
     int32_t N = 0;
@@ -65,6 +86,10 @@ struct rmx_graph {
     std::vector<int32_t> inst_canon;    // host: the copy whose flow instance k shares (itself if first)
     std::vector<double> L0v;            // initial code length per instance
 
+    // ---- CUDA graphs of the sweep pipeline (off: every kernel launched directly)
+    bool use_graphs = true;
+    std::vector<SweepGraph> sweep_graphs;
+
     // ---- state
     bool initiated = false;
     int power_iters = 0;
@@ -106,6 +131,8 @@ struct rmx_graph {
     void sweep_single(rmx::Level &lv, bool prior, bool allow_new, double vthresh, int64_t &n_active,
                       std::vector<double> &L);
     void set_active(const std::vector<uint8_t> &m);
+    void run_subbatches(rmx::Level &lv, int64_t n_active, rmx::ModState &M, rmx::InstState &I,
+                        const rmx::SweepArgs &sa, int ns, bool mark, uint32_t seed);
     int union_flows();
     void convert_to_supernodes(bool from_sn);
     void generate_sub_modules();

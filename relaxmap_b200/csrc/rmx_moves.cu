@@ -578,8 +578,9 @@ struct CommitArgs {
     const int32_t *free_list;
     const int64_t *n_free;
     unsigned long long *moved_nodes;
-    uint32_t stamp;
-    uint32_t hseed;  // per (attempt seed, sweep, sub-batch): picks the free id a unit bids for
+    // device {stamp, hseed} of the sub-batch: stamp marks its movers, hseed (a
+    // function of attempt seed, sweep and sub-batch) picks the free id a unit bids for
+    const uint32_t *sp;
 };
 
 __device__ __forceinline__ unsigned long long claim_key(uint32_t stamp, int32_t u) {
@@ -589,6 +590,7 @@ __device__ __forceinline__ unsigned long long claim_key(uint32_t stamp, int32_t 
 // Units proposing an empty module bid for a free id chosen by hash; the
 // smallest unit id wins each id (atomicMax on an inverted key), losers stay.
 __global__ void k_claim(CommitArgs a) {
+    const uint32_t stamp = a.sp[0], hseed = a.sp[1];
     const int64_t beg = a.range[0], end = a.range[1];
     const int64_t nf = *a.n_free;
     for (int64_t i = beg + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < end;
@@ -597,7 +599,7 @@ __global__ void k_claim(CommitArgs a) {
         if (a.prop[u] != kNewMod) continue;
         int32_t m = -1;
         if (nf > 0) {
-            int64_t s = mix32((uint32_t)u ^ a.hseed) % nf;
+            int64_t s = mix32((uint32_t)u ^ hseed) % nf;
             for (int probe = 0; probe < 8; probe++, s = (s + 1) % nf) {
                 const int32_t cand = a.free_list[s];
                 if (a.mcount[cand] == 0) {
@@ -607,11 +609,12 @@ __global__ void k_claim(CommitArgs a) {
             }
         }
         a.ptarget[u] = m;
-        if (m >= 0) atomicMax(a.claim + m, claim_key(a.stamp, u));
+        if (m >= 0) atomicMax(a.claim + m, claim_key(stamp, u));
     }
 }
 
 __global__ void k_commit(CommitArgs a) {
+    const uint32_t stamp = a.sp[0];
     const int64_t beg = a.range[0], end = a.range[1];
     unsigned long long moved = 0;
     for (int64_t i = beg + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < end;
@@ -621,13 +624,13 @@ __global__ void k_commit(CommitArgs a) {
         if (t == -1) continue;
         if (t == kNewMod) {
             t = a.ptarget[u];
-            if (t < 0 || a.claim[t] != claim_key(a.stamp, u)) continue;
+            if (t < 0 || a.claim[t] != claim_key(stamp, u)) continue;
             a.minst[t] = a.uinst[u];
         }
         const int32_t A = a.mod[u];
         a.prevmod[u] = A;
         a.mod[u] = t;
-        a.stamp_of[u] = a.stamp;
+        a.stamp_of[u] = stamp;
         const Stat4 s = a.attr[u];
         atomic_add_fx(&a.mstat[t].P, s.P);
         atomic_add_fx(&a.mstat[t].TW, s.TW);
@@ -653,7 +656,7 @@ struct DeltaArgs {
     const int32_t *out_dst, *in_src;
     const fx_t *out_fx, *in_fx;
     Stat4 *mstat;
-    uint32_t stamp;
+    const uint32_t *sp;  // device {stamp, hseed} of the sub-batch
 };
 
 // Out-flow bookkeeping for the movers of this sub-batch; warp per unit.
@@ -665,19 +668,19 @@ struct DeltaArgs {
 // warp sums its lanes' changes, so each mover costs two atomics.
 // Changes of OUT[A] and OUT[T] from the links of mover u, summed by the
 // calling thread over links j = first, first + stride, ...
-__device__ __forceinline__ void delta_links(const DeltaArgs &a, int32_t u, int32_t A, int32_t T, int first, int stride,
-                                            fx_t &dA, fx_t &dT) {
+__device__ __forceinline__ void delta_links(const DeltaArgs &a, uint32_t stamp, int32_t u, int32_t A, int32_t T,
+                                            int first, int stride, fx_t &dA, fx_t &dT) {
     for (int64_t e = a.out_off[u] + first; e < a.out_off[u + 1]; e += stride) {
         const int32_t w = a.out_dst[e];
         const fx_t q = a.out_fx[e];
-        const bool wm = a.stamp_of[w] == a.stamp;
+        const bool wm = a.stamp_of[w] == stamp;
         const int32_t bn = a.mod[w], bo = wm ? a.prevmod[w] : bn;
         if (A != bo) dA -= q;
         if (T != bn) dT += q;
     }
     for (int64_t e = a.in_off[u] + first; e < a.in_off[u + 1]; e += stride) {
         const int32_t w = a.in_src[e];
-        if (a.stamp_of[w] != a.stamp) {
+        if (a.stamp_of[w] != stamp) {
             const int32_t b = a.mod[w];
             if (b == A)
                 dA += a.in_fx[e];
@@ -689,14 +692,15 @@ __device__ __forceinline__ void delta_links(const DeltaArgs &a, int32_t u, int32
 
 __global__ void __launch_bounds__(256, RMX_DELTA_MINB) k_delta(DeltaArgs a) {
     const int lane = threadIdx.x & 31;
+    const uint32_t stamp = a.sp[0];
     const int64_t beg = *a.beg, end = *a.end;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t i = beg + gw; i < end; i += nw) {
         const int32_t u = a.list[i];
-        if (a.stamp_of[u] != a.stamp) continue;  // did not move in this sub-batch
+        if (a.stamp_of[u] != stamp) continue;  // did not move in this sub-batch
         const int32_t A = a.prevmod[u], T = a.mod[u];
         fx_t dA = 0, dT = 0;
-        delta_links(a, u, A, T, lane, 32, dA, dT);
+        delta_links(a, stamp, u, A, T, lane, 32, dA, dT);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             dA += __shfl_xor_sync(kFull, dA, o);
@@ -714,13 +718,14 @@ __global__ void __launch_bounds__(256, RMX_DELTA_MINB) k_delta(DeltaArgs a) {
 __global__ void __launch_bounds__(256) k_delta_block(DeltaArgs a) {
     __shared__ fx_t sh[2][8];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t stamp = a.sp[0];
     const int64_t beg = *a.beg, end = *a.end;
     for (int64_t i = beg + blockIdx.x; i < end; i += gridDim.x) {
         const int32_t u = a.list[i];
-        if (a.stamp_of[u] != a.stamp) continue;  // uniform across the block
+        if (a.stamp_of[u] != stamp) continue;  // uniform across the block
         const int32_t A = a.prevmod[u], T = a.mod[u];
         fx_t dA = 0, dT = 0;
-        delta_links(a, u, A, T, threadIdx.x, 256, dA, dT);
+        delta_links(a, stamp, u, A, T, threadIdx.x, 256, dA, dT);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             dA += __shfl_xor_sync(kFull, dA, o);
@@ -764,8 +769,9 @@ void refresh_terms(ModState &M, cudaStream_t s) {
 
 // After a sub-batch: the two modules of every mover get fresh cached terms
 // (a module touched by several movers is written with the same value).
-__global__ void k_terms_movers(const int32_t *list, const int64_t *range, const uint32_t *stamp_of, uint32_t stamp,
+__global__ void k_terms_movers(const int32_t *list, const int64_t *range, const uint32_t *stamp_of, const uint32_t *sp,
                                const int32_t *mod, const int32_t *prevmod, const Stat4 *mstat, double2 *term) {
+    const uint32_t stamp = sp[0];
     const int64_t beg = range[0], end = range[1];
     for (int64_t i = beg + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < end;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -973,9 +979,11 @@ static unsigned fit_grid(int64_t items, int64_t per_block, int64_t max_grid) {
 // bins on four auxiliary streams forked from and joined back into s, the
 // register bins on s itself. Only non-empty bins are launched (sizes from the
 // host copy of the bucket offsets); a lone bin runs on s without the fork.
-static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket, const SweepWork &W, cudaStream_t s) {
-    const int64_t *h = W.bucket_host.data() + first_bucket;
-    auto cnt = [&](int b0, int b1) { return h[b1] - h[b0]; };
+static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket, const SweepWork &W, bool fitted,
+                        cudaStream_t s) {
+    const int64_t *h = fitted ? W.bucket_host.data() + first_bucket : nullptr;
+    // without host sizes every bin counts as non-empty and takes its full grid
+    auto cnt = [&](int b0, int b1) { return fitted ? h[b1] - h[b0] : (int64_t)1 << 40; };
     const int64_t n_mid = cnt(kBinMid, kBinMid + 1), n_blk = cnt(kBinBlock, kBinBlock + 1),
                   n_lrg = cnt(kBinLarge, kBinLarge + 1), n_hub = a.gcap > 0 ? cnt(kBinHub, kBinHub + 1) : 0,
                   n_warp = cnt(kBinWarp, kBinWarp + 1), n_reg = cnt(kBinReg8, kBinReg32 + 1);
@@ -1081,7 +1089,7 @@ __global__ void k_ranges(const int64_t *bucket_off, int nsub, int64_t *ranges) {
 }
 
 void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed, int nsub, Arena &ar,
-                  cudaStream_t s) {
+                  cudaStream_t s, bool host_counts) {
     if (nsub * kBins > 256) throw std::invalid_argument("too many sub-batches");
     k_bucket<<<blocks_for(n_active, 256, num_sms() * 32), 256, 0, s>>>(W.list, W.counters + kCntActive, L.out_off,
                                                                        L.in_off, seed, nsub, W.bucket);
@@ -1089,6 +1097,7 @@ void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed,
     bucket_partition(W.bucket, W.list, W.list2, n_active, nsub * kBins, W.bucket_off, ar, s);
     k_ranges<<<1, 128, 0, s>>>(W.bucket_off, nsub, W.ranges);
     RMX_LAUNCHED();
+    if (!host_counts) return;
     // the bins' sizes on the host: empty bins are not launched, grids fit the work
     W.bucket_host.resize((size_t)nsub * kBins + 1);
     RMX_CUDA(cudaMemcpyAsync(W.bucket_host.data(), W.bucket_off, sizeof(int64_t) * W.bucket_host.size(),
@@ -1111,14 +1120,18 @@ void free_modules(const ModState &M, SweepWork &W, Arena &ar, cudaStream_t s) {
 }
 
 void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &W, const SweepArgs &sa, int sb,
-                    uint32_t stamp, uint32_t hseed, bool mark_active, cudaStream_t s, Timers *tm) {
-    const int64_t *hb = W.bucket_host.data() + sb * kBins;
-    const int64_t total = hb[kBins] - hb[0], n_light = hb[kBinMid] - hb[kBinReg8], n_heavy = hb[kBins] - hb[kBinMid];
+                    const uint32_t *sp, bool mark_active, bool fitted, cudaStream_t s, Timers *tm) {
+    // fitted: bin sizes known on the host (skip empty work, size grids); else
+    // every kernel is launched with its full grid and reads its range on the
+    // device (the form captured into a CUDA graph)
+    const int64_t *hb = fitted ? W.bucket_host.data() + sb * kBins : nullptr;
+    const int64_t total = fitted ? hb[kBins] - hb[0] : 1, n_light = fitted ? hb[kBinMid] - hb[kBinReg8] : 1,
+                  n_heavy = fitted ? hb[kBins] - hb[kBinMid] : 1;
     if (total == 0) return;
     EvalArgs ea = eval_args(L, M, I, W, sa.vthresh, sa.allow_new, nullptr, 1);
     ea.mark = mark_active ? 1 : 0;
     if (tm) tm->begin(kTimerEval, s);
-    launch_eval(ea, W.bucket_off, sb * kBins, W, s);
+    launch_eval(ea, W.bucket_off, sb * kBins, W, fitted, s);
     if (tm) tm->end(kTimerEval, s);
     if (tm) tm->begin(kTimerCommit, s);
     CommitArgs ca;
@@ -1139,9 +1152,8 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     ca.free_list = W.free_list;
     ca.n_free = W.counters + kCntFree;
     ca.moved_nodes = reinterpret_cast<unsigned long long *>(W.counters + kCntMoved);
-    ca.stamp = stamp;
-    ca.hseed = hseed;
-    const unsigned G = fit_grid(total, 256, num_sms() * 8);
+    ca.sp = sp;
+    const unsigned G = fitted ? fit_grid(total, 256, num_sms() * 8) : num_sms() * 8;
     if (sa.allow_new) {
         k_claim<<<G, 256, 0, s>>>(ca);
         RMX_LAUNCHED();
@@ -1160,22 +1172,22 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     da.out_fx = L.out_fx;
     da.in_fx = L.in_fx;
     da.mstat = M.stat;
-    da.stamp = stamp;
+    da.sp = sp;
     // light movers (<= 128 links) a warp each, heavy ones a block each
     const int64_t *bo = W.bucket_off + sb * kBins;
     if (n_light > 0) {
         da.beg = bo + kBinReg8;
         da.end = bo + kBinMid;
-        k_delta<<<fit_grid(n_light, 8, num_sms() * 8), 256, 0, s>>>(da);
+        k_delta<<<fitted ? fit_grid(n_light, 8, num_sms() * 8) : num_sms() * 8, 256, 0, s>>>(da);
         RMX_LAUNCHED();
     }
     if (n_heavy > 0) {
         da.beg = bo + kBinMid;
         da.end = bo + kBins;
-        k_delta_block<<<fit_grid(n_heavy, 1, num_sms() * 4), 256, 0, s>>>(da);
+        k_delta_block<<<fitted ? fit_grid(n_heavy, 1, num_sms() * 4) : num_sms() * 4, 256, 0, s>>>(da);
         RMX_LAUNCHED();
     }
-    k_terms_movers<<<G, 256, 0, s>>>(W.list2, W.ranges + 2 * sb, W.stamp, stamp, L.mod, W.prevmod, M.stat, M.term);
+    k_terms_movers<<<G, 256, 0, s>>>(W.list2, W.ranges + 2 * sb, W.stamp, sp, L.mod, W.prevmod, M.stat, M.term);
     RMX_LAUNCHED();
     if (tm) tm->end(kTimerCommit, s);
 }
@@ -1187,7 +1199,7 @@ void evaluate_all(const Level &L, const ModState &M, const InstState &I, SweepWo
     EvalArgs ea = eval_args(L, M, I, W, vthresh, 0, allow_new, 0);
     // allow_new == nullptr means "no empty-module candidate" for the hook
     if (!allow_new) ea.allow_new = 0;
-    launch_eval(ea, W.bucket_off, 0, W, s);
+    launch_eval(ea, W.bucket_off, 0, W, true, s);
 }
 
 }  // namespace rmx
