@@ -272,6 +272,7 @@ def main():
     with Clocks(torch.cuda.current_device()) as clk:
         e0.record(stream)
         for k in range(args.steps):
+            G.reset_flow()  # every step recomputes the flow, as the reference's timed region does
             results.append(G.optimize(seed=1 + k))
         e1.record(stream)
         torch.cuda.synchronize()

@@ -133,6 +133,11 @@ rmx_status rmx_graph_links(const rmx_graph *g, int64_t *off, int32_t *dst, doubl
 rmx_status rmx_initiate(rmx_graph *g, double *p, double *f, double *exitpr, uint8_t *dangling, int32_t *iters,
                         double *L0);
 
+/* Drop the handle's stationary flow and edge flows: the next rmx_initiate,
+ * rmx_optimize or rmx_codelength recomputes them (OmpRelaxmap.cpp:113-155,
+ * the part of the reference's timed region before the partitioning). */
+rmx_status rmx_reset_flow(rmx_graph *g);
+
 /* From-scratch code length of a partition (module id per node, any int32
  * labels in [0,N)), in nats: Network::calculateCodeLength (Module.cpp:2966-3002),
  * FP64 throughout. Runs rmx_initiate first if needed. */

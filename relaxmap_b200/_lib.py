@@ -25,7 +25,8 @@ EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_creat
            "rmx_coarsen", "rmx_evaluate_moves", "rmx_optimize", "rmx_superstep_codelengths", "rmx_write_outputs",
            "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main",
            "rmx_steady_state_noalloc", "rmx_noalloc_last_error", "rmx_adjoint_forward", "rmx_adjoint_backward",
-           "rmx_batch_create", "rmx_batch_set_wave", "rmx_batch_optimize", "rmx_batch_info", "rmx_batch_destroy"]
+           "rmx_batch_create", "rmx_batch_set_wave", "rmx_batch_optimize", "rmx_batch_info", "rmx_batch_destroy",
+           "rmx_reset_flow"]
 
 
 class RmxError(RuntimeError):
@@ -244,6 +245,10 @@ class Graph:
                    units_evaluated=pr.units_evaluated, adjoint_iters=pr.adjoint_iters,
                    level_ms={"nodes": pr.level_ms[0], "super_nodes": pr.level_ms[1], "coarse_tune": pr.level_ms[2]})
         return out
+
+    def reset_flow(self):
+        """The next initiate/optimize recomputes the stationary flow."""
+        _check(lib().rmx_reset_flow(self._h))
 
     def stream_ptr(self) -> int:
         return lib().rmx_graph_stream(self._h) or 0

@@ -168,6 +168,14 @@ rmx_status rmx_initiate(rmx_graph *g, double *p, double *f, double *exitpr, uint
     });
 }
 
+rmx_status rmx_reset_flow(rmx_graph *g) {
+    return guard([&] {
+        need(g, "graph");
+        RMX_CUDA(cudaStreamSynchronize(g->stream));
+        g->initiated = false;
+    });
+}
+
 rmx_status rmx_codelength(rmx_graph *g, const int32_t *part, double *L) {
     return guard([&] {
         need(g, "graph");

@@ -602,7 +602,9 @@ void rmx_graph::ensure_hub_table(int64_t maxdeg) {
 void rmx_graph::initiate() {
     if (initiated) return;
     timers.begin(kTimerOther, stream);
-    normalise(N, out_off, out_w0, out_f, in_off, in_src, in_w, in_w, dangling, scratch, stream);
+    // the CSC weights are normalised in place, once; the CSR flows are rebuilt from the raw weights
+    normalise(N, out_off, out_w0, out_f, in_off, in_src, in_w, in_w, dangling, scratch, stream, !cols_normalised);
+    cols_normalised = true;
     timers.end(kTimerOther, stream);
     timers.begin(kTimerSpmv, stream);
     if (K == 1)
@@ -653,16 +655,19 @@ int rmx_graph::union_flows() {
 
 // ---------------------------------------------------------------- sweeps
 
-// Buckets the active units of lv into ns sub-batches and runs them. Without
-// profiling the sub-batch pipeline (about ten launches per sub-batch over
-// five streams) is one CUDA graph, captured once per (level, module state,
-// instances, sweep options) and replayed: the sub-batches' stamps and hash
-// seeds live in device memory, and every kernel reads its unit range there.
-// With profiling on, the kernels are launched one by one between the timing
-// events, grids fitted to the bin sizes.
+// Buckets the active units of lv into ns sub-batches and runs them. From the
+// handle's second run on (capture and instantiation cost more than one run's
+// launches save), and without profiling, the sub-batch pipeline (about ten
+// launches per sub-batch over five streams) is one CUDA graph, captured once
+// per (level, module state, instances, sweep options) and replayed: the
+// sub-batches' stamps and hash seeds live in device memory, and every kernel
+// reads its unit range there. Otherwise the kernels are launched one by one,
+// empty bins skipped and grids fitted to the bin sizes.
 void rmx_graph::run_subbatches(Level &lv, int64_t n_active, ModState &M, InstState &I, const SweepArgs &sa, int ns,
                                bool mark, uint32_t seed) {
-    const bool graphs = !timers.on && use_graphs;
+    // a single run on a handle is cheaper launched directly than captured: graphs
+    // start with the handle's second attempt / optimiser run
+    const bool graphs = !timers.on && use_graphs && runs_done > 0;
     bucket_units(lv, work, n_active, seed, ns, scratch, stream, !graphs);
     for (int sb = 0; sb < ns; sb++) {
         work.hparams[2 * sb] = ++stamp;
@@ -1004,6 +1009,7 @@ std::vector<double> rmx_graph::run_attempt(uint32_t seed) {
         }
     }
     prof.supersteps += superstep;
+    runs_done++;
     return L;
 }
 

@@ -90,9 +90,10 @@ int power_iteration_components(int32_t n, int32_t n_comp, const int64_t *comp, c
                                double *p, Arena &ar, cudaStream_t s, int vec);
 // Sub-warp width of the pull SpMV for a mean in-degree.
 int spmv_width(double mean_in_degree);
+// cols: also normalise the CSC weights (in place when in_w_raw == in_w: once).
 void normalise(int32_t n, const int64_t *out_off, const double *out_w0, double *out_f, const int64_t *in_off,
                const int32_t *in_src, const double *in_w_raw, double *in_w, uint8_t *dangling, Arena &ar,
-               cudaStream_t s);
+               cudaStream_t s, bool cols = true);
 void edge_flows(int32_t n, int64_t m, const int64_t *out_off, double *out_f, fx_t *out_fx, const int32_t *in_src,
                 const double *in_w, fx_t *in_fx, const double *p, const double *tw, const uint8_t *dangling,
                 Stat4 *attr, fx_t *s0_acc, cudaStream_t s);

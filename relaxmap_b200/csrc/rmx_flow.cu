@@ -176,14 +176,16 @@ __global__ void k_normalise_cols(int64_t m, const int32_t *in_src, const double 
 
 void normalise(int32_t n, const int64_t *out_off, const double *out_w0, double *out_f, const int64_t *in_off,
                const int32_t *in_src, const double *in_w_raw, double *in_w, uint8_t *dangling, Arena &ar,
-               cudaStream_t s) {
+               cudaStream_t s, bool cols) {
     size_t mk = ar.mark();
     double *rowsum = ar.alloc<double>(std::max(n, 1));
     k_normalise_rows<<<blocks_for(n, 128, num_sms() * 16), 128, 0, s>>>(n, out_off, out_w0, out_f, rowsum, dangling);
     RMX_LAUNCHED();
     int64_t m = 0;
-    RMX_CUDA(cudaMemcpyAsync(&m, in_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
-    RMX_CUDA(cudaStreamSynchronize(s));
+    if (cols) {
+        RMX_CUDA(cudaMemcpyAsync(&m, in_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+        RMX_CUDA(cudaStreamSynchronize(s));
+    }
     if (m > 0) {
         k_normalise_cols<<<blocks_for(m, 256, num_sms() * 32), 256, 0, s>>>(m, in_src, in_w_raw, in_w, rowsum);
         RMX_LAUNCHED();

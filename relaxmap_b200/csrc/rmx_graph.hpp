@@ -87,11 +87,16 @@ struct rmx_graph {
     std::vector<double> L0v;            // initial code length per instance
 
     // ---- CUDA graphs of the sweep pipeline (off: every kernel launched directly)
-    bool use_graphs = true;
+#ifndef RMX_USE_GRAPHS
+#define RMX_USE_GRAPHS 1
+#endif
+    bool use_graphs = RMX_USE_GRAPHS != 0;
+    int64_t runs_done = 0;  // completed optimiser runs (attempts) on this handle
     std::vector<SweepGraph> sweep_graphs;
 
     // ---- state
     bool initiated = false;
+    bool cols_normalised = false;  // in_w holds the normalised weights
     int power_iters = 0;
     int spmv_vec = 32;
     double L0 = 0.0;

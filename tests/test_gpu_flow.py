@@ -77,3 +77,23 @@ def test_node_weights_teleport(built_lib, oracle_mod, tmp_path):
         r = G.initiate()
     assert rel_l1(r["p"], st["p"]) <= 1e-12
     assert abs(r["L0"] - st["L0"]) <= 1e-10
+
+
+def test_reset_flow_recomputes_the_same_flow(built_lib):
+    """rmx_reset_flow: the next initiate recomputes p and the edge flows from
+    the raw weights; they equal the first computation bit for bit, and so do
+    the partitions that follow."""
+    from relaxmap_b200 import Graph
+    with Graph.from_file(GOLDEN / "directNet_1k_sm_mu_03.txt") as G:
+        a = G.initiate()
+        ra = G.optimize(seed=3)
+        for _ in range(2):
+            G.reset_flow()
+            b = G.initiate()
+            np.testing.assert_array_equal(a["p"], b["p"])
+            np.testing.assert_array_equal(a["f"], b["f"])
+            assert a["L0"] == b["L0"]
+        G.reset_flow()
+        rb = G.optimize(seed=3)
+        assert ra["L"] == rb["L"]
+        np.testing.assert_array_equal(ra["part"], rb["part"])
