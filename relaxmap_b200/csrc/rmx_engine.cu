@@ -328,7 +328,6 @@ rmx_graph::~rmx_graph() {
     if (agg_tab) cudaFree(agg_tab);
     for (SweepGraph &g : sweep_graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
-    if (work.hparams) cudaFreeHost(work.hparams);
     perm.destroy();
     scratch.destroy();
     if (stream) cudaStreamDestroy(stream);
@@ -561,7 +560,6 @@ void rmx_graph::alloc_engine() {
     work.claim = perm.alloc<unsigned long long>(n);
     work.counters = perm.alloc<int64_t>(kCntSlots);
     work.dparams = perm.alloc<uint32_t>(64);
-    RMX_CUDA(cudaMallocHost(&work.hparams, sizeof(uint32_t) * 64));
     RMX_CUDA(cudaMemsetAsync(work.stamp, 0, sizeof(uint32_t) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.claim, 0, sizeof(unsigned long long) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.next_active, 0, n, stream));
@@ -673,6 +671,7 @@ void rmx_graph::run_subbatches(Level &lv, int64_t n_active, ModState &M, InstSta
         work.hparams[2 * sb] = ++stamp;
         work.hparams[2 * sb + 1] = mix_seed(seed, sb);
     }
+    // from pageable memory: staged before the call returns, so hparams is free again at once
     RMX_CUDA(cudaMemcpyAsync(work.dparams, work.hparams, sizeof(uint32_t) * 2 * ns, cudaMemcpyHostToDevice, stream));
     if (!graphs) {
         Timers *tm = timers.on ? &timers : nullptr;

@@ -156,7 +156,7 @@ struct SweepWork {
     int64_t gcap = 0;
     std::vector<int64_t> bucket_host;  // host copy of bucket_off after bucket_units
     uint32_t *dparams = nullptr;       // device {stamp, hseed} per sub-batch of the current sweep
-    uint32_t *hparams = nullptr;       // pinned host staging of dparams
+    uint32_t hparams[64] = {};         // host staging of dparams
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};  // concurrent degree bins
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
 };
