@@ -39,6 +39,10 @@ namespace {
 
 constexpr unsigned kFullA = 0xffffffffu;
 constexpr int kAdjT = 256;
+// resident blocks per SM the transposed solve is compiled for (and launched with)
+#ifndef RMX_ADJ_MINB
+#define RMX_ADJ_MINB 4
+#endif
 
 __device__ __forceinline__ double dlog(double x) { return x > 0.0 ? log(x) : 0.0; }
 
@@ -233,7 +237,7 @@ __device__ __forceinline__ double adj_pull_rows(const int32_t *__restrict__ rows
 // Out-degrees are heavy-tailed, so rows come grouped by degree class (rows[],
 // class boundaries cls[0..7]: <= 1, 2, 4, 8, 16, 32 links, more), each class
 // with its own lane width.
-__global__ void __launch_bounds__(kAdjT, 4) k_adj_solve(const int64_t *__restrict__ off, const int32_t *__restrict__ dst,
+__global__ void __launch_bounds__(kAdjT, RMX_ADJ_MINB) k_adj_solve(const int64_t *__restrict__ off, const int32_t *__restrict__ dst,
                                                         const double *__restrict__ w0,
                                                         const double *__restrict__ rowsum,
                                                         const double *__restrict__ tw, const uint8_t *__restrict__ dang,
@@ -376,7 +380,7 @@ int launch_solve(int32_t n, const int64_t *off, const int32_t *dst, const double
     int dev = 0, per_sm = 0;
     RMX_CUDA(cudaGetDevice(&dev));
     RMX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adj_solve, kAdjT, 0));
-    int nb = std::max(1, std::min(per_sm, 4)) * num_sms();
+    int nb = std::max(1, std::min(per_sm, RMX_ADJ_MINB)) * num_sms();
     nb = (int)std::min<int64_t>(nb, std::max<int64_t>(1, ((int64_t)n * 8 + kAdjT - 1) / kAdjT));
     nb = std::min(nb, max_blocks);
     size_t mk = ar.mark();

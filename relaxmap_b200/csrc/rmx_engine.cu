@@ -491,7 +491,7 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     RMX_CUDA(cudaStreamSynchronize(stream));
     // SpMV sub-warp width from the mean in-degree
     const double avg = (double)E / n;
-    spmv_vec = avg <= 6 ? 4 : (avg <= 12 ? 8 : (avg <= 24 ? 16 : 32));
+    spmv_vec = spmv_width(avg);
 }
 
 void rmx_graph::alloc_engine() {
