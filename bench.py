@@ -280,6 +280,7 @@ def main():
     gpu_launches = G.profile()["kernel_launches"] - launches0
     # one more run with the timing events: kernel-class times and bytes for the roofline
     G.set_profiling(True)
+    G.reset_flow()
     G.optimize(seed=1)
     prof = G.profile()
     G.set_profiling(False)
