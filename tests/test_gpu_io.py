@@ -65,3 +65,26 @@ def test_invalid_arguments(built_lib):
     with pytest.raises(RmxError) as e:
         Graph.from_edges(np.array([0, 1]), np.array([1, 5]), n=3)
     assert e.value.status == 1
+
+
+def test_cli_normal_mode_selflinks_and_attempts(built_lib, tmp_path):
+    """The other argument forms of OmpRelaxmap.cpp:43-79: `normal` instead of
+    `prior`, the optional `selflinks` (self links are still excluded, with the
+    reference's message) and several attempts (the best is written)."""
+    exe = ROOT / "relaxmap_b200" / "ompRelaxmap"
+    net = tmp_path / "loops.txt"
+    lines = (GOLDEN / "directNet_1k_sm_mu_03.txt").read_text().splitlines()
+    lines += ["5 5", "7 7 2.0"]
+    net.write_text("\n".join(lines) + "\n")
+    out = tmp_path / "out"
+    out.mkdir()
+    r = subprocess.run([str(exe), "3", str(net), "4", "3", "1e-3", "0.0", "10", str(out), "normal", "selflinks"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "current version always excludes self links." in r.stdout
+    assert "ignoring 2 self link(s)." in r.stdout
+    done = [l for l in r.stdout.splitlines() if l.startswith("DONE: Code Length = ")]
+    assert done, r.stdout
+    L = float(done[-1].split("=")[1].split()[0])
+    assert L <= 7.98793 * 1.005  # within the quality bar of the reference median on this graph
+    assert (out / "loops.tree").exists() and (out / "loops.clu").exists()
