@@ -493,14 +493,17 @@ def bench_adjoint(args, world: int, rank: int, pg):
     ms_step = e0.elapsed_time(e1) / args.steps
     prof = G.profile()
     G.set_profiling(False)
-    # the forward pass alone (flow + code length of the partition), same timing
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(args.steps):
+    # the forward pass alone (flow + code length of the partition): median over
+    # calls, each between its own events on the engine's stream
+    fwd = []
+    for _ in range(max(args.steps, 3)):
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
         G.adjoint_forward(part)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    fwd_ms = f0.elapsed_time(f1) / args.steps
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fwd.append(f0.elapsed_time(f1))
+    fwd_ms = statistics.median(fwd)
     ms_max = slowest_over_ranks([ms_step], pg, "cuda")[0]
     value = job_throughput(world, E, ms_max / 1e3)
     # end to end: graph built from pinned host buffers, gradient back in host memory

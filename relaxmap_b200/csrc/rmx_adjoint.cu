@@ -43,6 +43,10 @@ constexpr int kAdjT = 256;
 #ifndef RMX_ADJ_MINB
 #define RMX_ADJ_MINB 4
 #endif
+// links per lane in the degree classes up to 16 links (1 or 2)
+#ifndef RMX_ADJ_LPL
+#define RMX_ADJ_LPL 2
+#endif
 
 __device__ __forceinline__ double dlog(double x) { return x > 0.0 ? log(x) : 0.0; }
 
@@ -276,10 +280,14 @@ __global__ void __launch_bounds__(kAdjT, RMX_ADJ_MINB) k_adj_solve(const int64_t
     for (;;) {
         double ts = 0.0;
         ts += adj_pull_rows<1>(rows, cb[0], cb[1], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp, nwarps);
-        ts += adj_pull_rows<2>(rows, cb[1], cb[2], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp, nwarps);
-        ts += adj_pull_rows<4>(rows, cb[2], cb[3], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp, nwarps);
-        ts += adj_pull_rows<8>(rows, cb[3], cb[4], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp, nwarps);
-        ts += adj_pull_rows<16>(rows, cb[4], cb[5], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp,
+        ts += adj_pull_rows<2 / RMX_ADJ_LPL>(rows, cb[1], cb[2], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y,
+                                             gwarp, nwarps);
+        ts += adj_pull_rows<4 / RMX_ADJ_LPL>(rows, cb[2], cb[3], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y,
+                                             gwarp, nwarps);
+        ts += adj_pull_rows<8 / RMX_ADJ_LPL>(rows, cb[3], cb[4], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y,
+                                             gwarp, nwarps);
+        ts += adj_pull_rows<16 / RMX_ADJ_LPL>(rows, cb[4], cb[5], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y,
+                                              gwarp,
                                 nwarps);
         ts += adj_pull_rows<32>(rows, cb[5], cb[7], off, dst, w0, rowsum, dang, c, tw, beta, target, x, y, gwarp,
                                 nwarps);
