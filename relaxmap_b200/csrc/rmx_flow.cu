@@ -15,6 +15,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <climits>
 #include <vector>
 
 #include "rmx_engine.cuh"
@@ -234,11 +235,25 @@ constexpr int kPowT = 256;
 #define RMX_POW_MINB 6
 #endif
 
+// Rows of more than heavy_deg in-links (in-degree hubs) are not left to one
+// lane group: their links come in chunks of kPowChunk, a warp per chunk, and
+// after a grid barrier every such row sums its chunks' partials in chunk order.
+constexpr int64_t kPowChunk = 256;
+struct PowSplit {
+    const int32_t *rows = nullptr;       // heavy rows
+    int32_t n_rows = 0;
+    const int64_t *row_chunk = nullptr;  // chunks of heavy row h: row_chunk[h] .. row_chunk[h+1]
+    const int64_t *chunk_beg = nullptr, *chunk_end = nullptr;  // link range of every chunk
+    int64_t n_chunks = 0;
+    double *cpart = nullptr;             // partial pull of every chunk
+    int64_t heavy_deg = INT64_MAX;
+};
+
 template <int VEC>
 __global__ void __launch_bounds__(kPowT, RMX_POW_MINB) k_power(const int64_t *__restrict__ in_off, const int32_t *__restrict__ in_src,
                                                  const double *__restrict__ in_w, const double *__restrict__ tw,
                                                  const uint8_t *__restrict__ dang, int32_t n, double *x, double *y,
-                                                 double *parts, int *iters_out, double alpha) {
+                                                 double *parts, int *iters_out, double alpha, PowSplit sp) {
     cg::grid_group grid = cg::this_grid();
     __shared__ double sh[32];
     const int nb = gridDim.x;
@@ -267,16 +282,42 @@ __global__ void __launch_bounds__(kPowT, RMX_POW_MINB) k_power(const int64_t *__
         for (int64_t base = gwarp * RPW; base < n; base += nwarps * RPW) {
             const int64_t r = base + sub;
             double acc = 0.0;
-            if (r < n) {
-                const int64_t e = in_off[r + 1];
-for (int64_t k = in_off[r] + lv; k < e; k += VEC) acc += beta * in_w[k] * __ldcg(x + in_src[k]);
+            bool mine = r < n;
+            if (mine) {
+                const int64_t b = in_off[r], e = in_off[r + 1];
+                mine = e - b <= sp.heavy_deg;
+                if (mine)
+                    for (int64_t k = b + lv; k < e; k += VEC) acc += beta * in_w[k] * __ldcg(x + in_src[k]);
             }
 #pragma unroll
             for (int o = VEC / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
-            if (r < n && lv == 0) {
+            if (mine && lv == 0) {
                 const double v = coef * tw[r] + acc;
                 y[r] = v;
                 ls += v;
+            }
+        }
+        if (sp.n_rows > 0) {  // the same branch in every block
+            for (int64_t c = gwarp; c < sp.n_chunks; c += nwarps) {
+                double acc = 0.0;
+                for (int64_t k = sp.chunk_beg[c] + lane; k < sp.chunk_end[c]; k += 32)
+                    acc += beta * in_w[k] * __ldcg(x + in_src[k]);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+                if (lane == 0) sp.cpart[c] = acc;
+            }
+            grid.sync();
+            for (int64_t h = gwarp; h < sp.n_rows; h += nwarps) {
+                const int32_t r = sp.rows[h];
+                double acc = 0.0;
+                for (int64_t c = sp.row_chunk[h] + lane; c < sp.row_chunk[h + 1]; c += 32) acc += __ldcg(sp.cpart + c);
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+                if (lane == 0) {
+                    const double v = coef * tw[r] + acc;
+                    y[r] = v;
+                    ls += v;
+                }
             }
         }
         ls = block_sum<kPowT>(ls, sh);
@@ -305,6 +346,65 @@ for (int64_t k = in_off[r] + lv; k < e; k += VEC) acc += beta * in_w[k] * __ldcg
     if (gtid == 0) *iters_out = iter;
 }
 
+__global__ void k_pow_heavy_flags(int32_t n, const int64_t *in_off, int64_t heavy_deg, uint8_t *flag) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+        flag[r] = in_off[r + 1] - in_off[r] > heavy_deg ? 1 : 0;
+}
+
+__global__ void k_pow_heavy_ranges(const int32_t *rows, int64_t nh, const int64_t *in_off, int64_t *be) {
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nh; h += (int64_t)gridDim.x * blockDim.x) {
+        be[2 * h] = in_off[rows[h]];
+        be[2 * h + 1] = in_off[rows[h] + 1];
+    }
+}
+
+// The heavy rows of a CSC and their chunk tables, in arena memory (released
+// with the caller's mark).
+static PowSplit heavy_split(int32_t n, const int64_t *in_off, int64_t heavy_deg, Arena &ar, cudaStream_t s) {
+    PowSplit sp;
+    if (n <= 0) return sp;
+    uint8_t *flag = ar.alloc<uint8_t>(n);
+    int32_t *rows = ar.alloc<int32_t>(n);
+    int64_t *cnt = ar.alloc<int64_t>(1);
+    k_pow_heavy_flags<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, in_off, heavy_deg, flag);
+    RMX_LAUNCHED();
+    compact_flags(flag, n, rows, cnt, ar, s);
+    int64_t nh = 0;
+    RMX_CUDA(cudaMemcpyAsync(&nh, cnt, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    if (nh == 0) return sp;
+    int64_t *be = ar.alloc<int64_t>(2 * nh);
+    k_pow_heavy_ranges<<<blocks_for(nh, 256, num_sms() * 8), 256, 0, s>>>(rows, nh, in_off, be);
+    RMX_LAUNCHED();
+    std::vector<int64_t> hbe(2 * nh);
+    RMX_CUDA(cudaMemcpyAsync(hbe.data(), be, sizeof(int64_t) * 2 * nh, cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    std::vector<int64_t> rc(nh + 1, 0), cb, ce;
+    for (int64_t h = 0; h < nh; h++) {
+        for (int64_t k = hbe[2 * h]; k < hbe[2 * h + 1]; k += kPowChunk) {
+            cb.push_back(k);
+            ce.push_back(std::min(k + kPowChunk, hbe[2 * h + 1]));
+        }
+        rc[h + 1] = (int64_t)cb.size();
+    }
+    const int64_t nc = (int64_t)cb.size();
+    int64_t *d_rc = ar.alloc<int64_t>(nh + 1), *d_cb = ar.alloc<int64_t>(nc), *d_ce = ar.alloc<int64_t>(nc);
+    double *cpart = ar.alloc<double>(nc);
+    RMX_CUDA(cudaMemcpyAsync(d_rc, rc.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice, s));
+    RMX_CUDA(cudaMemcpyAsync(d_cb, cb.data(), sizeof(int64_t) * nc, cudaMemcpyHostToDevice, s));
+    RMX_CUDA(cudaMemcpyAsync(d_ce, ce.data(), sizeof(int64_t) * nc, cudaMemcpyHostToDevice, s));
+    RMX_CUDA(cudaStreamSynchronize(s));  // the host tables are freed on return
+    sp.rows = rows;
+    sp.n_rows = (int32_t)nh;
+    sp.row_chunk = d_rc;
+    sp.chunk_beg = d_cb;
+    sp.chunk_end = d_ce;
+    sp.n_chunks = nc;
+    sp.cpart = cpart;
+    sp.heavy_deg = heavy_deg;
+    return sp;
+}
+
 template <int VEC>
 static int launch_power(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
                         const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, double alpha) {
@@ -319,8 +419,9 @@ static int launch_power(int32_t n, const int64_t *in_off, const int32_t *in_src,
     double *y = ar.alloc<double>(std::max(n, 1));
     double *parts = ar.alloc<double>(3 * nb);
     int *iters = ar.alloc<int>(1);
-    void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w, (void *)&tw, (void *)&dangling, (void *)&n,
-                    (void *)&p, (void *)&y, (void *)&parts, (void *)&iters, (void *)&alpha};
+    PowSplit sp = heavy_split(n, in_off, 64 * VEC, ar, s);
+    void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w,  (void *)&tw,    (void *)&dangling, (void *)&n,
+                    (void *)&p,      (void *)&y,      (void *)&parts, (void *)&iters, (void *)&alpha,    (void *)&sp};
     RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));
     RMX_LAUNCHED();
     int h = 0;
@@ -343,8 +444,9 @@ static void launch_power_into(int32_t n, const int64_t *in_off, const int32_t *i
     nb = (int)std::min<int64_t>(nb, std::max<int64_t>(1, ((int64_t)n * VEC + kPowT - 1) / kPowT));
     nb = std::min(nb, max_blocks);
     double alpha = kAlpha;
-    void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w, (void *)&tw, (void *)&dangling, (void *)&n,
-                    (void *)&p, (void *)&y, (void *)&parts, (void *)&iters, (void *)&alpha};
+    PowSplit sp;  // no chunked rows: nothing beyond the caller's scratch
+    void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w,  (void *)&tw,    (void *)&dangling, (void *)&n,
+                    (void *)&p,      (void *)&y,      (void *)&parts, (void *)&iters, (void *)&alpha,    (void *)&sp};
     RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));
     RMX_LAUNCHED();
 }
