@@ -118,3 +118,34 @@ def test_synth_deterministic():
     r = synth.rmat(10, 16, seed=1)
     assert r.n == 1024 and np.all(r.src != r.dst)
     assert len(np.unique(r.src.astype(np.int64) * r.n + r.dst)) == r.m
+
+
+def test_batch_host_validation(built_lib):
+    """rmx_batch_create only copies and checks the graphs in host memory: ids
+    local to each graph, at least one node per graph; wave budgets positive.
+    Nothing here touches a device."""
+    from relaxmap_b200 import Batch, RmxError
+    ok = [(3, np.array([0, 1], np.int32), np.array([1, 2], np.int32), None),
+          (2, np.array([1], np.int32), np.array([0], np.int32), np.array([2.5]))]
+    with Batch(ok) as B:
+        info = B.info()
+        assert info == {"graphs": 2, "waves": 0, "instances": 0, "device_ms": 0.0}
+        with pytest.raises(RmxError) as e:
+            B.set_wave(0, 10)
+        assert e.value.status == 1
+        B.set_wave(1 << 20, 1 << 20)
+        assert list(B.offsets) == [0, 3, 5]
+    for bad in ([(3, np.array([0, 3], np.int32), np.array([1, 2], np.int32), None)],  # id beyond its graph
+                [(0, np.zeros(0, np.int32), np.zeros(0, np.int32), None)],           # empty graph
+                [(2, np.array([-1], np.int32), np.array([0], np.int32), None)]):     # negative id
+        with pytest.raises(RmxError) as e:
+            Batch(bad)
+        assert e.value.status == 1
+
+
+def test_lpt_weights_edge_cases():
+    from relaxmap_b200.sharding import lpt_assign
+    parts = lpt_assign([5.0], 4)  # more ranks than graphs: some ranks get none
+    assert [len(p) for p in parts] == [1, 0, 0, 0]
+    parts = lpt_assign([1.0, 1.0, 1.0, 1.0], 2)
+    assert sorted(len(p) for p in parts) == [2, 2]
