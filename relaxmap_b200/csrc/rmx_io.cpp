@@ -11,6 +11,7 @@
 #include "rmx_io.hpp"
 
 #include <algorithm>
+#include <climits>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -78,6 +79,18 @@ std::vector<char> read_all(const std::string &path) {
     FILE *f = fopen(path.c_str(), "rb");
     if (!f) throw IoError("cannot open " + path + ": " + strerror(errno));
     std::vector<char> data;
+    if (fseek(f, 0, SEEK_END) == 0) {  // regular file: one read of its size
+        const long sz = ftell(f);
+        if (sz > 0) {
+            rewind(f);
+            data.resize((size_t)sz);
+            size_t got = 0, r;
+            while (got < data.size() && (r = fread(data.data() + got, 1, data.size() - got, f)) > 0) got += r;
+            data.resize(got);
+        } else {
+            rewind(f);
+        }
+    }
     char chunk[1 << 16];
     size_t r;
     while ((r = fread(chunk, 1, sizeof chunk, f)) > 0) data.insert(data.end(), chunk, chunk + r);
@@ -101,13 +114,18 @@ struct EdgeChunk {
     std::vector<double> w;
 };
 
-// Parse edge-list lines [l0, l1); `buf` is the stream state entering l0.
-void parse_edge_lines(const std::vector<char> &d, const std::vector<std::pair<size_t, size_t>> &lines, size_t l0,
-                      size_t l1, Tok buf, EdgeChunk &out) {
+}  // namespace
+
+// Lines of byte range [from, to) (from at a line start), the lines getline
+// would give, each read as load_linkList_format_network reads a line
+// (FileIO.cpp:196-222): two integers and an optional weight; `buf` is the
+// stream state entering the range.
+void parse_edge_bytes(const std::vector<char> &d, size_t from, size_t to, Tok buf, EdgeChunk &out) {
     const char *base = d.data();
-    for (size_t l = l0; l < l1; l++) {
-        const char *b = base + lines[l].first, *e = base + lines[l].second;
-        if (b < e && *b == '#') continue;  // FileIO.cpp:198 (line[0] of "" is '\0')
+    size_t s = from;
+    auto line = [&](size_t b0, size_t e0) {
+        const char *b = base + b0, *e = base + e0;
+        if (b < e && *b == '#') return;  // FileIO.cpp:198 (line[0] of "" is '\0')
         LineStream ss(b, e);
         ss.read(buf);
         const long long x = c_atol(buf);
@@ -119,92 +137,154 @@ void parse_edge_lines(const std::vector<char> &d, const std::vector<std::pair<si
         out.a.push_back(x);
         out.b.push_back(y);
         out.w.push_back(w);
+    };
+    for (const char *p = base + from, *end = base + to; p < end;) {
+        const char *nl = static_cast<const char *>(memchr(p, '\n', (size_t)(end - p)));
+        if (!nl) break;
+        const size_t i = (size_t)(nl - base);
+        line(s, i);
+        s = i + 1;
+        p = nl + 1;
     }
+    if (s < to) line(s, to);
 }
 
-// State of `buf` after the last processed line before line l.
-Tok state_before(const std::vector<char> &d, const std::vector<std::pair<size_t, size_t>> &lines, size_t l) {
+// State of `buf` entering the line that starts at byte pos: the third token
+// (or "") of the last non-comment line before it.
+Tok state_before_pos(const std::vector<char> &d, size_t pos) {
     const char *base = d.data();
-    while (l > 0) {
-        l--;
-        const char *b = base + lines[l].first, *e = base + lines[l].second;
-        if (b < e && *b == '#') continue;
-        LineStream ss(b, e);
-        Tok t;
-        ss.read(t);
-        ss.read(t);
-        Tok third;
-        ss.read(third);
-        return third;  // "" unless the line had a third token
+    size_t e = pos;  // the previous line ends at e - 1 ('\n')
+    while (e > 0) {
+        const size_t le = e - 1;  // index of the '\n' ending the previous line
+        size_t b = le;
+        while (b > 0 && base[b - 1] != '\n') b--;
+        if (!(b < le && base[b] == '#')) {
+            LineStream ss(base + b, base + le);
+            Tok t;
+            ss.read(t);
+            ss.read(t);
+            Tok third;
+            ss.read(third);
+            return third;
+        }
+        e = b;
     }
     return Tok();
 }
 
-}  // namespace
-
 ParsedGraph parse_edge_list(const std::string &path, int threads) {
     std::vector<char> d = read_all(path);
-    std::vector<std::pair<size_t, size_t>> lines;
-    lines.reserve(d.size() / 8 + 1);
-    split_lines(d, 0, d.size(), lines);
-    const size_t nl = lines.size();
     int T = std::max(1, std::min(threads, 64));
-    if (nl < 100000) T = 1;
+    if (d.size() < (size_t(1) << 20)) T = 1;
+    // byte chunks that start at line starts
+    std::vector<size_t> cut(T + 1, d.size());
+    cut[0] = 0;
+    for (int t = 1; t < T; t++) {
+        size_t c = std::max(cut[t - 1], d.size() * t / T);
+        while (c < d.size() && c > 0 && d[c - 1] != '\n') c++;
+        cut[t] = c;
+    }
     std::vector<EdgeChunk> chunks(T);
-    std::vector<std::thread> pool;
-    for (int t = 0; t < T; t++) {
-        const size_t l0 = nl * t / T, l1 = nl * (t + 1) / T;
-        auto job = [&, t, l0, l1] { parse_edge_lines(d, lines, l0, l1, state_before(d, lines, l0), chunks[t]); };
-        if (T == 1)
-            job();
-        else
-            pool.emplace_back(job);
-    }
-    for (auto &th : pool) th.join();
-    // every id seen, renumbered in ascending order (FileIO.cpp:242-255)
-    std::vector<long long> ids;
+    std::vector<long long> lo(T, LLONG_MAX), hi(T, LLONG_MIN);
+    auto parallel = [&](auto &&job) {
+        if (T == 1) {
+            job(0);
+            return;
+        }
+        std::vector<std::thread> pool;
+        for (int t = 0; t < T; t++) pool.emplace_back(job, t);
+        for (auto &th : pool) th.join();
+    };
+    parallel([&](int t) {
+        const size_t reserve = (cut[t + 1] - cut[t]) / 16 + 16;
+        chunks[t].a.reserve(reserve);
+        chunks[t].b.reserve(reserve);
+        chunks[t].w.reserve(reserve);
+        parse_edge_bytes(d, cut[t], cut[t + 1], state_before_pos(d, cut[t]), chunks[t]);
+        for (size_t i = 0; i < chunks[t].a.size(); i++) {
+            lo[t] = std::min({lo[t], chunks[t].a[i], chunks[t].b[i]});
+            hi[t] = std::max({hi[t], chunks[t].a[i], chunks[t].b[i]});
+        }
+    });
+    std::vector<char>().swap(d);
     size_t total = 0;
-    for (auto &c : chunks) total += c.a.size();
-    ids.reserve(2 * total);
-    for (auto &c : chunks) {
-        ids.insert(ids.end(), c.a.begin(), c.a.end());
-        ids.insert(ids.end(), c.b.begin(), c.b.end());
+    long long mn = LLONG_MAX, mx = LLONG_MIN;
+    for (int t = 0; t < T; t++) {
+        total += chunks[t].a.size();
+        mn = std::min(mn, lo[t]);
+        mx = std::max(mx, hi[t]);
     }
-    std::sort(ids.begin(), ids.end());
-    ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
-    if (ids.size() >= (size_t)INT32_MAX) throw FormatError("more than 2^31-1 nodes");
+    // every id seen, renumbered in ascending order (FileIO.cpp:242-255): by a
+    // presence table when the ids are dense, else by sorting them
     ParsedGraph g;
+    std::vector<long long> ids;
+    std::vector<int32_t> table;
+    const bool dense = total > 0 && (unsigned long long)(mx - mn) < 4ull * (2 * total) + 1024;
+    if (dense) {
+        const size_t range = (size_t)(mx - mn) + 1;
+        std::vector<uint8_t> seen(range, 0);
+        parallel([&](int t) {
+            for (size_t i = 0; i < chunks[t].a.size(); i++) {
+                __atomic_store_n(&seen[(size_t)(chunks[t].a[i] - mn)], (uint8_t)1, __ATOMIC_RELAXED);
+                __atomic_store_n(&seen[(size_t)(chunks[t].b[i] - mn)], (uint8_t)1, __ATOMIC_RELAXED);
+            }
+        });
+        table.assign(range, -1);
+        int64_t k = 0;
+        for (size_t v = 0; v < range; v++)
+            if (seen[v]) {
+                table[v] = (int32_t)k++;
+                ids.push_back(mn + (long long)v);
+            }
+        if (k >= (int64_t)INT32_MAX) throw FormatError("more than 2^31-1 nodes");
+    } else {
+        ids.reserve(2 * total);
+        for (auto &c : chunks) {
+            ids.insert(ids.end(), c.a.begin(), c.a.end());
+            ids.insert(ids.end(), c.b.begin(), c.b.end());
+        }
+        std::sort(ids.begin(), ids.end());
+        ids.erase(std::unique(ids.begin(), ids.end()), ids.end());
+        if (ids.size() >= (size_t)INT32_MAX) throw FormatError("more than 2^31-1 nodes");
+    }
     g.n = (int32_t)ids.size();
     g.n_lines = (int64_t)total;
     g.names.resize(ids.size());
     for (size_t i = 0; i < ids.size(); i++) g.names[i] = std::to_string(ids[i]);
-    const bool dense = !ids.empty() && (ids.back() - ids.front()) < (long long)(4 * ids.size() + 1024);
-    std::vector<int32_t> table;
-    if (dense) {
-        table.assign((size_t)(ids.back() - ids.front() + 1), -1);
-        for (size_t i = 0; i < ids.size(); i++) table[(size_t)(ids[i] - ids.front())] = (int32_t)i;
-    }
     auto ren = [&](long long x) -> int32_t {
-        if (dense) return table[(size_t)(x - ids.front())];
+        if (dense) return table[(size_t)(x - mn)];
         return (int32_t)(std::lower_bound(ids.begin(), ids.end(), x) - ids.begin());
     };
-    g.src.reserve(total);
-    g.dst.reserve(total);
-    g.w.reserve(total);
-    std::map<int32_t, double> self;
-    for (auto &c : chunks) {
+    // non-self links per chunk, then every chunk renumbered into its slice in order
+    std::vector<size_t> keep(T + 1, 0);
+    parallel([&](int t) {
+        size_t k = 0;
+        for (size_t i = 0; i < chunks[t].a.size(); i++) k += chunks[t].a[i] != chunks[t].b[i];
+        keep[t + 1] = k;
+    });
+    for (int t = 0; t < T; t++) keep[t + 1] += keep[t];
+    g.src.resize(keep[T]);
+    g.dst.resize(keep[T]);
+    g.w.resize(keep[T]);
+    std::vector<std::vector<std::pair<int32_t, double>>> selfs(T);
+    parallel([&](int t) {
+        size_t o = keep[t];
+        const EdgeChunk &c = chunks[t];
         for (size_t i = 0; i < c.a.size(); i++) {
-            const int32_t x = ren(c.a[i]), y = ren(c.b[i]);
-            if (x == y) {
-                self[x] += c.w[i];
+            const int32_t x = ren(c.a[i]);
+            if (c.a[i] == c.b[i]) {
+                selfs[t].push_back({x, c.w[i]});
                 continue;
             }
-            g.src.push_back(x);
-            g.dst.push_back(y);
-            g.w.push_back(c.w[i]);
+            g.src[o] = x;
+            g.dst[o] = ren(c.b[i]);
+            g.w[o] = c.w[i];
+            o++;
         }
-        EdgeChunk().a.swap(c.a);
-    }
+    });
+    std::map<int32_t, double> self;  // summed in input order, as the edge map does
+    for (auto &v : selfs)
+        for (auto &kv : v) self[kv.first] += kv.second;
     for (auto &kv : self)
         if (kv.second > 0.0) g.n_self++;
     return g;
