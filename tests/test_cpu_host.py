@@ -35,11 +35,11 @@ def test_parse_matches_reference_loader(built_lib, name, threads):
     np.testing.assert_array_equal(d["node_w"], g["node_w"])
 
 
-def _cmp_oracle(path, oracle_mod):
+def _cmp_oracle(path, oracle_mod, threads=(1, 3)):
     from relaxmap_b200 import parse_file
     O = oracle_mod
     ld = O.parse_pajek(path) if str(path).endswith(".net") else O.parse_txt(path)
-    for t in (1, 3):
+    for t in threads:
         d = parse_file(path, threads=t)
         assert d["n"] == ld.n
         acc = {}
@@ -78,6 +78,27 @@ def test_edge_list_large_threads(built_lib, oracle_mod, tmp_path):
     p = tmp_path / "big.txt"
     p.write_text("\n".join(lines) + "\n")
     _cmp_oracle(p, oracle_mod)
+
+
+def test_edge_list_quirks_at_range_boundaries(built_lib, oracle_mod, tmp_path):
+    """Byte ranges of the parallel parse start at line starts; with four lines
+    in ten a blank, whitespace-only, bare-CR, one-token or comment line, many
+    ranges open on a blank-like line that re-reads the stream state carried in
+    (the last non-comment line's third token): 1, 5 and 13 of the range starts
+    at 7, 16 and 64 threads follow a line with a weight, so a lost state
+    changes the edge map."""
+    rng = np.random.default_rng(11)
+    kinds = rng.choice(8, size=110000, p=[0.15, 0.05, 0.05, 0.05, 0.10, 0.25, 0.30, 0.05])
+    ids = rng.integers(0, 3000, size=(110000, 2))
+    wts = rng.uniform(0.0, 4.0, size=110000)
+    lines = []
+    for k, (a, b), x in zip(kinds.tolist(), ids.tolist(), wts.tolist()):
+        lines.append(["", " \t ", "\r", f"{a}", f"# {a} {b} 7", f"{a} {b}",
+                      f"{a}\t{b}\t{x!r}", f"{a} {b} {x:.3f}\r"][k])
+    p = tmp_path / "dense_quirks.txt"
+    p.write_text("\n".join(lines) + "\n")
+    assert p.stat().st_size > (1 << 20)  # large enough for the multi-range parse
+    _cmp_oracle(p, oracle_mod, threads=(1, 2, 7, 16, 64))
 
 
 def test_pajek_quirks(built_lib, oracle_mod, tmp_path):
