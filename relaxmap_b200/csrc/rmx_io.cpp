@@ -17,7 +17,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <map>
+#include <mutex>
 #include <thread>
 
 namespace rmx {
@@ -59,7 +61,7 @@ long long c_atol(const Tok &t) {
     if (p < t.e && (*p == '+' || *p == '-')) neg = *p++ == '-';
     unsigned long long v = 0;
     while (p < t.e && *p >= '0' && *p <= '9') v = v * 10 + (unsigned)(*p++ - '0');
-    return neg ? -(long long)v : (long long)v;
+    return (long long)(neg ? 0ull - v : v);  // negated unsigned: -2^63 has no signed negation
 }
 
 // C atof (strtod) on a token.
@@ -186,14 +188,32 @@ ParsedGraph parse_edge_list(const std::string &path, int threads) {
     }
     std::vector<EdgeChunk> chunks(T);
     std::vector<long long> lo(T, LLONG_MAX), hi(T, LLONG_MIN);
+    // job(t) on T threads; the first exception a job throws (or a failed
+    // thread start) is rethrown here after every started thread has joined
     auto parallel = [&](auto &&job) {
         if (T == 1) {
             job(0);
             return;
         }
+        std::exception_ptr err;
+        std::mutex err_mu;
+        auto guarded = [&](int t) {
+            try {
+                job(t);
+            } catch (...) {
+                std::lock_guard<std::mutex> lk(err_mu);
+                if (!err) err = std::current_exception();
+            }
+        };
         std::vector<std::thread> pool;
-        for (int t = 0; t < T; t++) pool.emplace_back(job, t);
+        try {
+            for (int t = 0; t < T; t++) pool.emplace_back(guarded, t);
+        } catch (...) {
+            std::lock_guard<std::mutex> lk(err_mu);
+            if (!err) err = std::current_exception();
+        }
         for (auto &th : pool) th.join();
+        if (err) std::rethrow_exception(err);
     };
     parallel([&](int t) {
         const size_t reserve = (cut[t + 1] - cut[t]) / 16 + 16;
@@ -219,14 +239,16 @@ ParsedGraph parse_edge_list(const std::string &path, int threads) {
     ParsedGraph g;
     std::vector<long long> ids;
     std::vector<int32_t> table;
-    const bool dense = total > 0 && (unsigned long long)(mx - mn) < 4ull * (2 * total) + 1024;
+    // (the span in unsigned arithmetic: ids may cover the whole 64-bit range)
+    const unsigned long long span = (unsigned long long)mx - (unsigned long long)mn;
+    const bool dense = total > 0 && span < 4ull * (2 * total) + 1024;
     if (dense) {
-        const size_t range = (size_t)(mx - mn) + 1;
+        const size_t range = (size_t)span + 1;
         std::vector<uint8_t> seen(range, 0);
         parallel([&](int t) {
             for (size_t i = 0; i < chunks[t].a.size(); i++) {
-                __atomic_store_n(&seen[(size_t)(chunks[t].a[i] - mn)], (uint8_t)1, __ATOMIC_RELAXED);
-                __atomic_store_n(&seen[(size_t)(chunks[t].b[i] - mn)], (uint8_t)1, __ATOMIC_RELAXED);
+                __atomic_store_n(&seen[(size_t)chunks[t].a[i] - (size_t)mn], (uint8_t)1, __ATOMIC_RELAXED);
+                __atomic_store_n(&seen[(size_t)chunks[t].b[i] - (size_t)mn], (uint8_t)1, __ATOMIC_RELAXED);
             }
         });
         table.assign(range, -1);
@@ -234,7 +256,7 @@ ParsedGraph parse_edge_list(const std::string &path, int threads) {
         for (size_t v = 0; v < range; v++)
             if (seen[v]) {
                 table[v] = (int32_t)k++;
-                ids.push_back(mn + (long long)v);
+                ids.push_back((long long)((unsigned long long)mn + v));
             }
         if (k >= (int64_t)INT32_MAX) throw FormatError("more than 2^31-1 nodes");
     } else {
@@ -252,7 +274,7 @@ ParsedGraph parse_edge_list(const std::string &path, int threads) {
     g.names.resize(ids.size());
     for (size_t i = 0; i < ids.size(); i++) g.names[i] = std::to_string(ids[i]);
     auto ren = [&](long long x) -> int32_t {
-        if (dense) return table[(size_t)(x - mn)];
+        if (dense) return table[(size_t)x - (size_t)mn];
         return (int32_t)(std::lower_bound(ids.begin(), ids.end(), x) - ids.begin());
     };
     // non-self links per chunk, then every chunk renumbered into its slice in order

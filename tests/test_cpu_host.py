@@ -101,6 +101,16 @@ def test_edge_list_quirks_at_range_boundaries(built_lib, oracle_mod, tmp_path):
     _cmp_oracle(p, oracle_mod, threads=(1, 2, 7, 16, 64))
 
 
+def test_edge_list_ids_across_the_64_bit_range(built_lib, oracle_mod, tmp_path):
+    """Ids at both ends of the 64-bit range: sparse, so renumbered by sorting,
+    and their span does not fit a signed difference."""
+    p = tmp_path / "wide.txt"
+    p.write_text("-9223372036854775808 9223372036854775807 2\n9223372036854775807 0\n"
+                 "0 -9223372036854775808 0.5\n5 5 1\n-1 0\n")
+    ld = _cmp_oracle(p, oracle_mod)
+    assert ld.names == ["-9223372036854775808", "-1", "0", "5", "9223372036854775807"]
+
+
 def test_pajek_quirks(built_lib, oracle_mod, tmp_path):
     p = tmp_path / "q.net"
     p.write_text('*Vertices 5\n1 "a b" 2.0\n2 "c"\n3 d 0.5\n4\n5 "e" -1\n*Arcs\n1 2\n2 3 0.5\n1 2 1.5\n3 3 2\n\n5 1\n')
