@@ -236,6 +236,14 @@ void *rmx_graph_stream(const rmx_graph *g);
 /* Block until the handle's stream is idle. */
 rmx_status rmx_sync(rmx_graph *g);
 
+/* The device memory of a graph handle (and the scratch of an adjoint call)
+ * comes from a per-device pool that keeps what is freed: closing a handle and
+ * creating another of similar size reuses that memory without a cudaMalloc /
+ * cudaFree pair (whose release of a few GB can take from milliseconds to over
+ * a second). This returns every pool block that no open handle holds to the
+ * driver. No reference counterpart (the reference holds no device memory). */
+rmx_status rmx_release_device_cache(void);
+
 /* Largest graph rmx_steady_state_noalloc accepts. */
 #define RMX_NOALLOC_MAX_NODES (1 << 20)
 

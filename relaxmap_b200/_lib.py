@@ -26,7 +26,7 @@ EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_creat
            "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main",
            "rmx_steady_state_noalloc", "rmx_noalloc_last_error", "rmx_adjoint_forward", "rmx_adjoint_backward",
            "rmx_batch_create", "rmx_batch_set_wave", "rmx_batch_optimize", "rmx_batch_info", "rmx_batch_destroy",
-           "rmx_reset_flow"]
+           "rmx_reset_flow", "rmx_release_device_cache"]
 
 
 class RmxError(RuntimeError):
@@ -340,6 +340,12 @@ def steady_state_noalloc(n_nodes: int, n_links: int, in_off_ptr: int, in_src_ptr
                                         C.c_void_p(iters_ptr or None), C.c_void_p(stream_ptr or None))
     if st != RMX_OK:
         raise RmxError(st, lib().rmx_noalloc_last_error().decode(errors="replace"))
+
+
+def release_device_cache():
+    """Return the device memory that closed handles left in the library's
+    per-device pool to the driver (rmx_release_device_cache)."""
+    _check(lib().rmx_release_device_cache())
 
 
 def cli(argv: list[str]) -> int:

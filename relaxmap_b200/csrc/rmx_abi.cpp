@@ -379,4 +379,8 @@ rmx_status rmx_sync(rmx_graph *g) {
     });
 }
 
+rmx_status rmx_release_device_cache(void) {
+    return guard([&] { rmx::release_device_cache(); });
+}
+
 }  // extern "C"

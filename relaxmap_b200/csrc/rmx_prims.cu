@@ -1,5 +1,7 @@
 // Device-wide primitives (see rmx_prims.cuh).
 #include <algorithm>
+#include <cstdint>
+#include <mutex>
 
 #include "rmx_prims.cuh"
 
@@ -18,16 +20,105 @@ int num_sms() {
     return n;
 }
 
+namespace {
+
+constexpr int kMaxDevices = 64;
+
+struct DevicePool {
+    bool tried = false;
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t stream = nullptr;  // allocations and frees are ordered on it
+};
+
+std::mutex g_pool_mu;
+DevicePool g_pools[kMaxDevices];
+
+// The arena pool of device dev, created on first use: its release threshold is
+// the maximum, so freed blocks stay reserved by the process for the next
+// arena. Null when the device has no memory pools (or creating one failed).
+DevicePool *device_pool(int dev) {
+    if (dev < 0 || dev >= kMaxDevices) return nullptr;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    DevicePool &d = g_pools[dev];
+    if (!d.tried) {
+        d.tried = true;
+        int supported = 0;
+        bool ok = cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev) == cudaSuccess &&
+                  supported != 0;
+        cudaMemPool_t p = nullptr;
+        cudaStream_t s = nullptr;
+        if (ok) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            ok = cudaMemPoolCreate(&p, &props) == cudaSuccess;
+        }
+        if (ok) {
+            uint64_t keep = UINT64_MAX;
+            ok = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess &&
+                 cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
+        }
+        if (ok) {
+            d.pool = p;
+            d.stream = s;
+        } else {
+            if (p) cudaMemPoolDestroy(p);
+            (void)cudaGetLastError();  // the failed query or creation is not a launch error
+        }
+    }
+    return d.pool ? &d : nullptr;
+}
+
+}  // namespace
+
 void Arena::init(size_t bytes) {
-    RMX_CUDA(cudaMalloc(&base, bytes));
+    RMX_CUDA(cudaGetDevice(&dev));
+    DevicePool *d = device_pool(dev);
+    if (d) {
+        RMX_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&base), bytes, d->pool, d->stream));
+        RMX_CUDA(cudaStreamSynchronize(d->stream));  // usable on every stream from here on
+        pool_stream = d->stream;
+    } else {
+        RMX_CUDA(cudaMalloc(&base, bytes));
+        pool_stream = nullptr;
+    }
     cap = bytes;
     top = peak = 0;
 }
 
 void Arena::destroy() {
-    if (base) cudaFree(base);
+    if (base) {
+        if (pool_stream) {
+            // cudaFree would synchronise the device; so does this, before the
+            // block goes back to the pool, so no queued work still uses it
+            int cur = -1;
+            cudaGetDevice(&cur);
+            if (cur != dev) cudaSetDevice(dev);
+            cudaDeviceSynchronize();
+            cudaFreeAsync(base, pool_stream);
+            if (cur != dev && cur >= 0) cudaSetDevice(cur);
+        } else {
+            cudaFree(base);
+        }
+    }
     base = nullptr;
+    pool_stream = nullptr;
     cap = top = peak = 0;
+}
+
+void release_device_cache() {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    int cur = -1;
+    RMX_CUDA(cudaGetDevice(&cur));
+    for (int dev = 0; dev < kMaxDevices; dev++) {
+        DevicePool &d = g_pools[dev];
+        if (!d.pool) continue;
+        RMX_CUDA(cudaSetDevice(dev));
+        RMX_CUDA(cudaStreamSynchronize(d.stream));  // frees queued on the pool's stream have happened
+        RMX_CUDA(cudaMemPoolTrimTo(d.pool, 0));
+    }
+    RMX_CUDA(cudaSetDevice(cur));
 }
 
 void *Arena::alloc_bytes(size_t bytes) {

@@ -9,9 +9,15 @@ namespace rmx {
 
 // Bump allocator over one device allocation. mark()/release() give scoped
 // scratch; alloc() throws CudaError(cudaErrorMemoryAllocation) when full.
+// The allocation comes from a per-device memory pool that keeps freed blocks
+// (see release_device_cache), so closing one graph handle and opening another
+// of similar size reuses the same device memory without a cudaMalloc /
+// cudaFree pair; on a device without memory pools it is a plain cudaMalloc.
 struct Arena {
     char *base = nullptr;
     size_t cap = 0, top = 0, peak = 0;
+    int dev = -1;                          // device of the allocation
+    cudaStream_t pool_stream = nullptr;    // set when the block came from the pool
     void init(size_t bytes);
     void destroy();
     void *alloc_bytes(size_t bytes);
@@ -22,6 +28,10 @@ struct Arena {
     size_t mark() const { return top; }
     void release(size_t m) { top = m; }
 };
+
+// Returns every unused block of the arena pools to the driver (all devices
+// that have one). Arenas still held are untouched.
+void release_device_cache();
 
 // out[i] = sum_{j<i} in[i] for i < n; if total != nullptr, *total (device) =
 // sum of all n. in and out may alias.
