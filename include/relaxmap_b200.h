@@ -221,7 +221,10 @@ rmx_status rmx_batch_destroy(rmx_batch *b);
  * value, dropped self-loops have none), *dL_dtau (may be NULL). The stationary
  * flow is recomputed, then one transposed solve (pull over the out-links)
  * gives the adjoint of the flow. part: module id per node in [0,N); tau in
- * (0,1). */
+ * (0,1). The solve stops when its L1 change is at most 1e-15 of the norm; if
+ * 4000 sweeps do not get there (a small tau on a slowly mixing graph: the
+ * error falls by about (1-tau)|lambda_2| per sweep) the call returns
+ * RMX_ERR_NO_CONVERGENCE and writes neither dL_dw nor dL_dtau. */
 rmx_status rmx_adjoint_forward(rmx_graph *g, const int32_t *part, double tau, double *L, double *p);
 rmx_status rmx_adjoint_backward(rmx_graph *g, const int32_t *part, double tau, double *dL_dw, double *dL_dtau,
                                 double *L);

@@ -26,6 +26,8 @@ rmx_status guard(F &&f) {
         return RMX_OK;
     } catch (const rmx::CudaError &e) {
         return fail(e.code == cudaErrorMemoryAllocation ? RMX_ERR_OOM : RMX_ERR_CUDA, e.what());
+    } catch (const rmx::NoConvergence &e) {
+        return fail(RMX_ERR_NO_CONVERGENCE, e.what());
     } catch (const rmx::FormatError &e) {
         return fail(RMX_ERR_FORMAT, e.what());
     } catch (const rmx::IoError &e) {

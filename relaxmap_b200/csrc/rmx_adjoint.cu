@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <string>
 #include <vector>
 
 #include "rmx_graph.hpp"
@@ -491,6 +492,15 @@ void rmx_graph::adjoint(const int32_t *part_host, double tau, double *L_out, dou
         timers.end(kTimerAdjoint, stream);
         if (timers.on) prof.adjoint_iters += it;
         if (solve_iters) *solve_iters = it;
+        // Stopped on the sweep cap: the adjoint, and every derivative taken
+        // from it, is not within tolerance, so none is returned. (A solve that
+        // met the tolerance on exactly the last sweep is reported the same way.)
+        // The error falls by about (1 - tau) |lambda_2| per sweep, so this
+        // happens for a small tau on a graph whose walk mixes slowly.
+        if (it >= max_iter)
+            throw NoConvergence("adjoint solve: the L1 change stayed above 1e-15 of the norm for " +
+                                std::to_string(max_iter) + " sweeps (tau " + std::to_string(tau) +
+                                " is too small for this graph's mixing)");
         if (grad_out) {
             double *grad = A.alloc<double>(Em);
             if (E > 0) {

@@ -65,6 +65,11 @@ struct CudaError : std::runtime_error {
     CudaError(cudaError_t c, const std::string &m) : std::runtime_error(m), code(c) {}
 };
 
+// An iteration that must converge stopped on its cap (RMX_ERR_NO_CONVERGENCE).
+struct NoConvergence : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
 inline void check(cudaError_t e, const char *what, const char *file, int line) {
     if (e != cudaSuccess) {
         char buf[512];

@@ -75,3 +75,25 @@ def test_adjoint_rejects_bad_input(built_lib):
         bad[0] = G.n
         with pytest.raises(RmxError):
             G.adjoint_backward(bad, 0.15)
+
+
+def test_adjoint_solve_cap_reports_no_convergence(built_lib):
+    """A ring where every node links to the next (weight 1) and the one after
+    (weight 0.5) mixes slowly: |lambda_2| of its walk is 1 - O((2 pi / n)^2),
+    so the solve's error falls by barely (1 - tau) per sweep. At tau = 1e-4 the
+    1e-15 tolerance is out of reach of the 4000-sweep cap and the call reports
+    RMX_ERR_NO_CONVERGENCE instead of an inaccurate gradient. The handle stays
+    usable: at tau = 0.15 the same graph converges (~180 sweeps) and matches
+    the oracle (two out-links per node, so dL/dw is not identically zero)."""
+    from relaxmap_b200 import Graph, RmxError
+    n = 1000
+    a = np.arange(n, dtype=np.int32)
+    src = np.concatenate([a, a])
+    dst = np.concatenate([(a + 1) % n, (a + 2) % n]).astype(np.int32)
+    w = np.concatenate([np.ones(n), np.full(n, 0.5)])
+    part = np.repeat(np.arange(3, dtype=np.int32), [100, 200, 700])
+    with Graph.from_edges(src, dst, w, n=n) as G:
+        with pytest.raises(RmxError) as e:
+            G.adjoint_backward(part, 1e-4)
+        assert e.value.status == 6  # RMX_ERR_NO_CONVERGENCE
+        _check(G, part, 0.15)
