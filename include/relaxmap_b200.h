@@ -240,11 +240,13 @@ void *rmx_graph_stream(const rmx_graph *g);
 rmx_status rmx_sync(rmx_graph *g);
 
 /* The device memory of a graph handle (and the scratch of an adjoint call)
- * comes from a per-device pool that keeps what is freed: closing a handle and
- * creating another of similar size reuses that memory without a cudaMalloc /
- * cudaFree pair (whose release of a few GB can take from milliseconds to over
- * a second). This returns every pool block that no open handle holds to the
- * driver. No reference counterpart (the reference holds no device memory). */
+ * is kept in a process-wide cache when the handle closes, up to a quarter of
+ * each device's memory: the next handle or call of similar size (a cached
+ * block is reused for requests of at least half its size) takes it without a
+ * cudaMalloc / cudaFree pair, and an allocation that fails empties the cache
+ * and retries. This frees every cached block (all devices); handles still open
+ * are untouched. No reference counterpart (the reference holds no device
+ * memory). */
 rmx_status rmx_release_device_cache(void);
 
 /* Largest graph rmx_steady_state_noalloc accepts. */

@@ -343,8 +343,8 @@ def steady_state_noalloc(n_nodes: int, n_links: int, in_off_ptr: int, in_src_ptr
 
 
 def release_device_cache():
-    """Return the device memory that closed handles left in the library's
-    per-device pool to the driver (rmx_release_device_cache)."""
+    """Free the device memory that closed handles left in the library's block
+    cache (rmx_release_device_cache)."""
     _check(lib().rmx_release_device_cache())
 
 

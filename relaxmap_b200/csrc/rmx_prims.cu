@@ -1,7 +1,8 @@
 // Device-wide primitives (see rmx_prims.cuh).
 #include <algorithm>
-#include <cstdint>
+#include <cstddef>
 #include <mutex>
+#include <vector>
 
 #include "rmx_prims.cuh"
 
@@ -22,66 +23,80 @@ int num_sms() {
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-
-struct DevicePool {
-    bool tried = false;
-    cudaMemPool_t pool = nullptr;
-    cudaStream_t stream = nullptr;  // allocations and frees are ordered on it
+// Blocks of destroyed arenas, oldest first, kept for the next arena that fits.
+struct CachedBlock {
+    char *ptr;
+    size_t bytes;
+    int dev;
 };
 
-std::mutex g_pool_mu;
-DevicePool g_pools[kMaxDevices];
+std::mutex g_cache_mu;
+std::vector<CachedBlock> g_cache;
 
-// The arena pool of device dev, created on first use: its release threshold is
-// the maximum, so freed blocks stay reserved by the process for the next
-// arena. Null when the device has no memory pools (or creating one failed).
-DevicePool *device_pool(int dev) {
-    if (dev < 0 || dev >= kMaxDevices) return nullptr;
-    std::lock_guard<std::mutex> lk(g_pool_mu);
-    DevicePool &d = g_pools[dev];
-    if (!d.tried) {
-        d.tried = true;
-        int supported = 0;
-        bool ok = cudaDeviceGetAttribute(&supported, cudaDevAttrMemoryPoolsSupported, dev) == cudaSuccess &&
-                  supported != 0;
-        cudaMemPool_t p = nullptr;
-        cudaStream_t s = nullptr;
-        if (ok) {
-            cudaMemPoolProps props = {};
-            props.allocType = cudaMemAllocationTypePinned;
-            props.location.type = cudaMemLocationTypeDevice;
-            props.location.id = dev;
-            ok = cudaMemPoolCreate(&p, &props) == cudaSuccess;
-        }
-        if (ok) {
-            uint64_t keep = UINT64_MAX;
-            ok = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess &&
-                 cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess;
-        }
-        if (ok) {
-            d.pool = p;
-            d.stream = s;
-        } else {
-            if (p) cudaMemPoolDestroy(p);
-            (void)cudaGetLastError();  // the failed query or creation is not a launch error
-        }
+// Bytes of cached blocks the current device may keep: a quarter of its memory.
+size_t cache_budget() {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
     }
-    return d.pool ? &d : nullptr;
+    return total_b / 4;
+}
+
+// cudaFree the cached blocks of device dev (current), oldest first, until at
+// most keep bytes of them remain. The caller holds g_cache_mu.
+void trim_locked(int dev, size_t keep) {
+    size_t held = 0;
+    for (const CachedBlock &b : g_cache)
+        if (b.dev == dev) held += b.bytes;
+    for (size_t i = 0; i < g_cache.size() && held > keep;) {
+        if (g_cache[i].dev != dev) {
+            i++;
+            continue;
+        }
+        cudaFree(g_cache[i].ptr);
+        held -= g_cache[i].bytes;
+        g_cache.erase(g_cache.begin() + (std::ptrdiff_t)i);
+    }
+}
+
+// The smallest cached block of device dev that holds `bytes` and is at most
+// twice that size, taken out of the cache; null if there is none.
+char *take_cached(int dev, size_t bytes, size_t *block_bytes) {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    size_t best = g_cache.size();
+    for (size_t i = 0; i < g_cache.size(); i++) {
+        const CachedBlock &b = g_cache[i];
+        if (b.dev != dev || b.bytes < bytes || b.bytes / 2 > bytes) continue;
+        if (best == g_cache.size() || b.bytes < g_cache[best].bytes) best = i;
+    }
+    if (best == g_cache.size()) return nullptr;
+    char *p = g_cache[best].ptr;
+    *block_bytes = g_cache[best].bytes;
+    g_cache.erase(g_cache.begin() + (std::ptrdiff_t)best);
+    return p;
 }
 
 }  // namespace
 
 void Arena::init(size_t bytes) {
     RMX_CUDA(cudaGetDevice(&dev));
-    DevicePool *d = device_pool(dev);
-    if (d) {
-        RMX_CUDA(cudaMallocFromPoolAsync(reinterpret_cast<void **>(&base), bytes, d->pool, d->stream));
-        RMX_CUDA(cudaStreamSynchronize(d->stream));  // usable on every stream from here on
-        pool_stream = d->stream;
-    } else {
-        RMX_CUDA(cudaMalloc(&base, bytes));
-        pool_stream = nullptr;
+    base = take_cached(dev, bytes, &block);
+    if (!base) {
+        cudaError_t e = cudaMalloc(&base, bytes);
+        if (e == cudaErrorMemoryAllocation) {  // the cache may hold what is missing
+            (void)cudaGetLastError();
+            {
+                std::lock_guard<std::mutex> lk(g_cache_mu);
+                trim_locked(dev, 0);
+            }
+            e = cudaMalloc(&base, bytes);
+        }
+        if (e != cudaSuccess) {
+            base = nullptr;
+            check(e, "cudaMalloc (device arena)", __FILE__, __LINE__);
+        }
+        block = bytes;
     }
     cap = bytes;
     top = peak = 0;
@@ -89,36 +104,44 @@ void Arena::init(size_t bytes) {
 
 void Arena::destroy() {
     if (base) {
-        if (pool_stream) {
-            // cudaFree would synchronise the device; so does this, before the
-            // block goes back to the pool, so no queued work still uses it
-            int cur = -1;
-            cudaGetDevice(&cur);
-            if (cur != dev) cudaSetDevice(dev);
-            cudaDeviceSynchronize();
-            cudaFreeAsync(base, pool_stream);
-            if (cur != dev && cur >= 0) cudaSetDevice(cur);
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != dev) cudaSetDevice(dev);
+        // wait for the device first, as cudaFree would: no queued work still
+        // uses the block when another arena takes it
+        if (cudaDeviceSynchronize() == cudaSuccess) {
+            std::lock_guard<std::mutex> lk(g_cache_mu);
+            const size_t budget = cache_budget();
+            if (block <= budget) {
+                g_cache.push_back({base, block, dev});
+                trim_locked(dev, budget);
+            } else {
+                cudaFree(base);
+            }
         } else {
             cudaFree(base);
         }
+        if (cur >= 0 && cur != dev) cudaSetDevice(cur);
     }
     base = nullptr;
-    pool_stream = nullptr;
-    cap = top = peak = 0;
+    cap = top = peak = block = 0;
 }
 
 void release_device_cache() {
-    std::lock_guard<std::mutex> lk(g_pool_mu);
+    std::lock_guard<std::mutex> lk(g_cache_mu);
     int cur = -1;
     RMX_CUDA(cudaGetDevice(&cur));
-    for (int dev = 0; dev < kMaxDevices; dev++) {
-        DevicePool &d = g_pools[dev];
-        if (!d.pool) continue;
-        RMX_CUDA(cudaSetDevice(dev));
-        RMX_CUDA(cudaStreamSynchronize(d.stream));  // frees queued on the pool's stream have happened
-        RMX_CUDA(cudaMemPoolTrimTo(d.pool, 0));
+    cudaError_t first = cudaSuccess;
+    while (!g_cache.empty()) {
+        const CachedBlock b = g_cache.back();
+        g_cache.pop_back();
+        cudaError_t e = cudaSetDevice(b.dev);
+        if (e == cudaSuccess) e = cudaFree(b.ptr);
+        if (first == cudaSuccess) first = e;
     }
-    RMX_CUDA(cudaSetDevice(cur));
+    cudaError_t e = cudaSetDevice(cur);
+    if (first == cudaSuccess) first = e;
+    check(first, "release_device_cache", __FILE__, __LINE__);
 }
 
 void *Arena::alloc_bytes(size_t bytes) {

@@ -9,15 +9,16 @@ namespace rmx {
 
 // Bump allocator over one device allocation. mark()/release() give scoped
 // scratch; alloc() throws CudaError(cudaErrorMemoryAllocation) when full.
-// The allocation comes from a per-device memory pool that keeps freed blocks
-// (see release_device_cache), so closing one graph handle and opening another
-// of similar size reuses the same device memory without a cudaMalloc /
-// cudaFree pair; on a device without memory pools it is a plain cudaMalloc.
+// The block is a cudaMalloc allocation that destroy() keeps in a process-wide
+// cache (up to a quarter of the device's memory) instead of freeing: the next
+// arena that fits (at most twice its size) takes it, so closing a graph handle
+// and opening another of similar size costs no cudaMalloc / cudaFree pair.
+// release_device_cache() frees the cached blocks.
 struct Arena {
     char *base = nullptr;
     size_t cap = 0, top = 0, peak = 0;
-    int dev = -1;                          // device of the allocation
-    cudaStream_t pool_stream = nullptr;    // set when the block came from the pool
+    size_t block = 0;  // size of the underlying allocation (>= cap)
+    int dev = -1;      // device of the allocation
     void init(size_t bytes);
     void destroy();
     void *alloc_bytes(size_t bytes);
@@ -29,8 +30,7 @@ struct Arena {
     void release(size_t m) { top = m; }
 };
 
-// Returns every unused block of the arena pools to the driver (all devices
-// that have one). Arenas still held are untouched.
+// cudaFree every cached arena block (all devices). Arenas in use are untouched.
 void release_device_cache();
 
 // out[i] = sum_{j<i} in[i] for i < n; if total != nullptr, *total (device) =

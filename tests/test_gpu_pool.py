@@ -1,8 +1,8 @@
-"""Device memory of graph handles comes from the library's per-device pool
-(rmx_release_device_cache): after a handle closes its arenas stay reserved by
-the process, the next handle of the same size reuses them instead of growing
-the reservation, its optimiser run is identical to the first handle's, and
-the release hands the unused blocks back to the driver."""
+"""Device memory of closed graph handles stays in the library's block cache
+(rmx_release_device_cache): after a handle closes its arenas stay allocated,
+the next handle of the same size reuses them instead of allocating more, its
+optimiser run is identical to the first handle's, and the release frees the
+cached blocks."""
 import numpy as np
 import pytest
 
