@@ -229,6 +229,26 @@ rmx_status rmx_adjoint_forward(rmx_graph *g, const int32_t *part, double tau, do
 rmx_status rmx_adjoint_backward(rmx_graph *g, const int32_t *part, double tau, double *dL_dw, double *dL_dtau,
                                 double *L);
 
+/* Launch shape of move evaluation, process-wide: the grid cap of each degree
+ * bin in blocks per SM. Results do not depend on these values (every bin's
+ * kernel loops over its units by grid stride and module statistics are exact
+ * integer sums), only the time does. rmx_set_tuning takes effect at the next
+ * launch; sweep pipelines captured as CUDA graphs under other values are
+ * captured again. Each value must lie in [1, 64] (else RMX_ERR_INVALID);
+ * `reserved` is ignored. The Python module relaxmap_b200.autotune picks the
+ * values by timing. No reference counterpart. */
+typedef struct rmx_tuning {
+    int32_t eval_mid_grid;   /* units of 129-512 links (default 8) */
+    int32_t eval_block_grid; /* 513-1024 links (default 4) */
+    int32_t eval_large_grid; /* 1025-4096 links (default 1) */
+    int32_t eval_warp_grid;  /* 33-128 links (default 3) */
+    int32_t eval_reg_grid;   /* up to 32 links (default 8) */
+    int32_t reserved[3];
+} rmx_tuning;
+
+rmx_status rmx_get_tuning(rmx_tuning *out);
+rmx_status rmx_set_tuning(const rmx_tuning *t);
+
 /* Device-time profiling of the handle's kernels (CUDA events on its stream). */
 rmx_status rmx_set_profiling(rmx_graph *g, int32_t on);
 rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out);

@@ -26,7 +26,7 @@ EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_creat
            "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main",
            "rmx_steady_state_noalloc", "rmx_noalloc_last_error", "rmx_adjoint_forward", "rmx_adjoint_backward",
            "rmx_batch_create", "rmx_batch_set_wave", "rmx_batch_optimize", "rmx_batch_info", "rmx_batch_destroy",
-           "rmx_reset_flow", "rmx_release_device_cache"]
+           "rmx_reset_flow", "rmx_release_device_cache", "rmx_get_tuning", "rmx_set_tuning"]
 
 
 class RmxError(RuntimeError):
@@ -340,6 +340,34 @@ def steady_state_noalloc(n_nodes: int, n_links: int, in_off_ptr: int, in_src_ptr
                                         C.c_void_p(iters_ptr or None), C.c_void_p(stream_ptr or None))
     if st != RMX_OK:
         raise RmxError(st, lib().rmx_noalloc_last_error().decode(errors="replace"))
+
+
+TUNING_FIELDS = ("eval_mid_grid", "eval_block_grid", "eval_large_grid", "eval_warp_grid", "eval_reg_grid")
+
+
+class Tuning(C.Structure):
+    _fields_ = [(f, C.c_int32) for f in TUNING_FIELDS] + [("reserved", C.c_int32 * 3)]
+
+
+def get_tuning() -> dict:
+    """The process-wide launch shape of move evaluation (rmx_get_tuning): grid
+    cap of each degree bin in blocks per SM."""
+    t = Tuning()
+    _check(lib().rmx_get_tuning(C.byref(t)))
+    return {f: getattr(t, f) for f in TUNING_FIELDS}
+
+
+def set_tuning(**values) -> dict:
+    """Change some of the grid caps (rmx_set_tuning); the others keep their
+    current values. Returns the new setting."""
+    unknown = set(values) - set(TUNING_FIELDS)
+    if unknown:
+        raise ValueError(f"unknown tuning fields {sorted(unknown)}")
+    cur = get_tuning()
+    cur.update({k: int(v) for k, v in values.items()})
+    t = Tuning(*[cur[f] for f in TUNING_FIELDS])
+    _check(lib().rmx_set_tuning(C.byref(t)))
+    return cur
 
 
 def release_device_cache():

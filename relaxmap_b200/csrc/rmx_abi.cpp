@@ -381,6 +381,32 @@ rmx_status rmx_sync(rmx_graph *g) {
     });
 }
 
+rmx_status rmx_get_tuning(rmx_tuning *out) {
+    return guard([&] {
+        need(out, "out");
+        const rmx::EvalTuning t = rmx::eval_tuning();
+        *out = rmx_tuning{};
+        out->eval_mid_grid = t.mid;
+        out->eval_block_grid = t.block;
+        out->eval_large_grid = t.large;
+        out->eval_warp_grid = t.warp;
+        out->eval_reg_grid = t.reg;
+    });
+}
+
+rmx_status rmx_set_tuning(const rmx_tuning *t) {
+    return guard([&] {
+        need(t, "tuning");
+        rmx::EvalTuning v;
+        v.mid = t->eval_mid_grid;
+        v.block = t->eval_block_grid;
+        v.large = t->eval_large_grid;
+        v.warp = t->eval_warp_grid;
+        v.reg = t->eval_reg_grid;
+        rmx::set_eval_tuning(v);
+    });
+}
+
 rmx_status rmx_release_device_cache(void) {
     return guard([&] { rmx::release_device_cache(); });
 }

@@ -679,11 +679,26 @@ void rmx_graph::run_subbatches(Level &lv, int64_t n_active, ModState &M, InstSta
             sweep_subbatch(lv, M, I, work, sa, sb, work.dparams + 2 * sb, mark, true, stream, tm);
         return;
     }
-    const SweepGraphKey key{&lv, &M, &I, sa.allow_new, mark ? 1 : 0, sa.vthresh, ns, work.gtable, work.gcap};
+    const SweepGraphKey key{&lv, &M, &I, sa.allow_new, mark ? 1 : 0, sa.vthresh, ns, work.gtable, work.gcap,
+                            eval_tuning_generation()};
     SweepGraph *gr = nullptr;
     for (SweepGraph &g : sweep_graphs)
         if (g.key == key) gr = &g;
     if (!gr) {
+        // graphs captured under another launch tuning are never launched again
+        bool stale = false;
+        for (const SweepGraph &g : sweep_graphs) stale |= g.key.tuning_gen != key.tuning_gen;
+        if (stale) {
+            RMX_CUDA(cudaStreamSynchronize(stream));  // none of them is still running
+            std::vector<SweepGraph> keep;
+            for (SweepGraph &g : sweep_graphs) {
+                if (g.key.tuning_gen == key.tuning_gen)
+                    keep.push_back(g);
+                else if (g.exec)
+                    cudaGraphExecDestroy(g.exec);
+            }
+            sweep_graphs.swap(keep);
+        }
         const unsigned long long c0 = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
         cudaGraph_t graph = nullptr;
         RMX_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));

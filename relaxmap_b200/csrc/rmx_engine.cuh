@@ -163,6 +163,20 @@ struct SweepWork {
 
 void configure_eval_kernels();
 int hub_blocks();
+
+// Grid caps of the move-evaluation bins, in blocks per SM: process-wide,
+// read at every launch. Results do not depend on them (each bin's kernel loops
+// over its units by grid stride; module statistics are exact integer sums),
+// only the time does. The hub bin is not tuned: its global table slices are
+// indexed by block.
+struct EvalTuning {
+    int mid, block, large, warp, reg;
+};
+EvalTuning eval_tuning();
+// Throws std::invalid_argument unless every value lies in [1, 64].
+void set_eval_tuning(const EvalTuning &t);
+// Changes with every set_eval_tuning (part of the sweep graph cache key).
+int eval_tuning_generation();
 int64_t warp_bin_max_degree();
 int64_t block_bin_max_degree();
 int64_t hub_slots(int64_t cap);

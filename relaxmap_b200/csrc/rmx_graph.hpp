@@ -33,9 +33,11 @@ struct SweepGraphKey {
     int nsub;
     const void *gtable;
     int64_t gcap;
+    int tuning_gen;  // eval_tuning_generation() at capture: grid sizes are part of the graph
     bool operator==(const SweepGraphKey &o) const {
         return lv == o.lv && M == o.M && I == o.I && allow_new == o.allow_new && mark == o.mark &&
-               vthresh == o.vthresh && nsub == o.nsub && gtable == o.gtable && gcap == o.gcap;
+               vthresh == o.vthresh && nsub == o.nsub && gtable == o.gtable && gcap == o.gcap &&
+               tuning_gen == o.tuning_gen;
     }
 };
 struct SweepGraph {

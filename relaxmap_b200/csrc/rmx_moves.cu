@@ -20,7 +20,10 @@
 // Module statistics are therefore always the exact fixed-point sums of the
 // current partition, and the code length is recomputed from them per sweep.
 #include <algorithm>
+#include <atomic>
 #include <climits>
+#include <mutex>
+#include <stdexcept>
 
 #include "rmx_engine.cuh"
 
@@ -201,7 +204,7 @@ constexpr int kBinReg8 = 0, kBinReg16 = 1, kBinReg32 = 2, kBinWarp = 3, kBinMid 
 // units of 129..512 links: four warps each (eight teams per SM), a 1024-slot table
 constexpr int kMidT = 128, kMidMaxDeg = 512, kMidCap = 1024;
 constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
-// resident blocks per SM of the block bin and grid multipliers of the bins
+// resident blocks per SM of the block bin; default grid caps of the block, warp and register bins
 #ifndef RMX_BLK_MINB
 #define RMX_BLK_MINB 4
 #endif
@@ -960,6 +963,33 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
 }
 
 int hub_blocks() { return num_sms(); }
+
+namespace {
+std::atomic<int> g_grid_mid{8}, g_grid_block{RMX_BLK_GRID}, g_grid_large{1}, g_grid_warp{RMX_WARP_GRID},
+    g_grid_reg{RMX_REG_GRID};
+std::atomic<int> g_tuning_gen{0};
+std::mutex g_tuning_mu;  // one setter at a time
+}  // namespace
+
+EvalTuning eval_tuning() {
+    return {g_grid_mid.load(std::memory_order_relaxed), g_grid_block.load(std::memory_order_relaxed),
+            g_grid_large.load(std::memory_order_relaxed), g_grid_warp.load(std::memory_order_relaxed),
+            g_grid_reg.load(std::memory_order_relaxed)};
+}
+
+void set_eval_tuning(const EvalTuning &t) {
+    for (int v : {t.mid, t.block, t.large, t.warp, t.reg})
+        if (v < 1 || v > 64) throw std::invalid_argument("evaluation grid caps must lie in 1..64 blocks per SM");
+    std::lock_guard<std::mutex> lk(g_tuning_mu);
+    g_grid_mid.store(t.mid);
+    g_grid_block.store(t.block);
+    g_grid_large.store(t.large);
+    g_grid_warp.store(t.warp);
+    g_grid_reg.store(t.reg);
+    g_tuning_gen.fetch_add(1);
+}
+
+int eval_tuning_generation() { return g_tuning_gen.load(); }
 int64_t block_bin_max_degree() { return kLrgMaxDeg; }
 int64_t warp_bin_max_degree() { return kWarpMaxDeg; }
 int64_t hub_slots(int64_t cap) { return cap; }
@@ -968,9 +998,7 @@ constexpr size_t kBlkSmem = (size_t)kBlkCap * (2 * sizeof(fx_t) + sizeof(int32_t
 constexpr size_t kMidSmem = (size_t)kMidCap * (2 * sizeof(fx_t) + sizeof(int32_t));
 constexpr size_t kLrgSmem = (size_t)kLrgCap * (2 * sizeof(fx_t) + sizeof(int32_t));
 
-// The bins of a sub-batch run concurrently: block, large + hub, and the warp
-// bin on three auxiliary streams forked from and joined back into s, the
-// register bins on s itself.
+// Blocks for `items` work items at per_block items a block, at most max_grid.
 static unsigned fit_grid(int64_t items, int64_t per_block, int64_t max_grid) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(max_grid, (items + per_block - 1) / per_block));
 }
@@ -988,6 +1016,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
                   n_lrg = cnt(kBinLarge, kBinLarge + 1), n_hub = a.gcap > 0 ? cnt(kBinHub, kBinHub + 1) : 0,
                   n_warp = cnt(kBinWarp, kBinWarp + 1), n_reg = cnt(kBinReg8, kBinReg32 + 1);
     const bool use[4] = {n_blk > 0, n_lrg + n_hub > 0, n_warp > 0, n_mid > 0};
+    const EvalTuning tg = eval_tuning();
     const int streams = (int)use[0] + (int)use[1] + (int)use[2] + (int)use[3] + (n_reg > 0 ? 1 : 0);
     const bool fork = streams > 1;
     auto on = [&](int k) { return fork ? W.aux[k] : s; };
@@ -998,18 +1027,18 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     }
     if (n_mid > 0) {
         a.range = bucket_off + first_bucket + kBinMid;
-        k_eval_block<kMidT, kMidCap, false><<<fit_grid(n_mid, 1, num_sms() * 8), kMidT, kMidSmem, on(3)>>>(a);
+        k_eval_block<kMidT, kMidCap, false><<<fit_grid(n_mid, 1, (int64_t)num_sms() * tg.mid), kMidT, kMidSmem, on(3)>>>(a);
         RMX_LAUNCHED();
     }
     if (n_blk > 0) {
         a.range = bucket_off + first_bucket + kBinBlock;
-        k_eval_block<kBlkT, kBlkCap, false><<<fit_grid(n_blk, 1, num_sms() * RMX_BLK_GRID), kBlkT, kBlkSmem, on(0)>>>(
+        k_eval_block<kBlkT, kBlkCap, false><<<fit_grid(n_blk, 1, (int64_t)num_sms() * tg.block), kBlkT, kBlkSmem, on(0)>>>(
             a);
         RMX_LAUNCHED();
     }
     if (n_lrg > 0) {
         a.range = bucket_off + first_bucket + kBinLarge;
-        k_eval_block<kLrgT, kLrgCap, false><<<fit_grid(n_lrg, 1, num_sms()), kLrgT, kLrgSmem, on(1)>>>(a);
+        k_eval_block<kLrgT, kLrgCap, false><<<fit_grid(n_lrg, 1, (int64_t)num_sms() * tg.large), kLrgT, kLrgSmem, on(1)>>>(a);
         RMX_LAUNCHED();
     }
     if (n_hub > 0) {  // global table slices are indexed by block: at most hub_blocks() blocks
@@ -1019,12 +1048,12 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     }
     if (n_warp > 0) {
         a.range = bucket_off + first_bucket + kBinWarp;
-        k_eval_warp<<<fit_grid(n_warp, kEvalWarps, num_sms() * RMX_WARP_GRID), kEvalWarps * 32, 0, on(2)>>>(a);
+        k_eval_warp<<<fit_grid(n_warp, kEvalWarps, (int64_t)num_sms() * tg.warp), kEvalWarps * 32, 0, on(2)>>>(a);
         RMX_LAUNCHED();
     }
     if (n_reg > 0) {
         a.range = bucket_off + first_bucket + kBinReg8;
-        k_eval_reg<<<fit_grid(n_reg, 8, num_sms() * RMX_REG_GRID), 256, 0, s>>>(a);
+        k_eval_reg<<<fit_grid(n_reg, 8, (int64_t)num_sms() * tg.reg), 256, 0, s>>>(a);
         RMX_LAUNCHED();
     }
     if (fork)
