@@ -227,7 +227,7 @@ def main():
     import numpy as np
     import torch
 
-    from relaxmap_b200 import Graph
+    from relaxmap_b200 import Graph, get_tuning
 
     torch.cuda.set_device(local)
     pg = None
@@ -332,7 +332,8 @@ def main():
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, seed 42)",
         "config": {"workload": desc, "nodes": g.n, "links": E, "solver": "seed 1..K, threshold 1e-3, vThresh 0.0, "
                    "maxIter 10, prior", "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": f"inputs larger than L2 (resident graph ~{(E * 104 + g.n * 420) / 1e9:.1f} GB)"},
+                   "l2": f"inputs larger than L2 (resident graph ~{(E * 104 + g.n * 420) / 1e9:.1f} GB)",
+                   "launch_tuning": get_tuning()},
         "quality": {"L_bits_median": statistics.median(L_bits), "n_modules": results[0]["n_modules"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(E * (8 + (8 if w is not None else 0))),
                 "d2h_bytes_per_step": int(4 * g.n + 8), "graph_build_ms": build_s * 1e3,
@@ -384,7 +385,7 @@ def bench_batched(args, world: int, rank: int, pg):
     import numpy as np
     import torch
 
-    from relaxmap_b200 import Batch, synth
+    from relaxmap_b200 import Batch, get_tuning, synth
     from relaxmap_b200.sharding import combine, lpt_assign
     G = args.graphs
     specs = synth.batched_graphs(G, seed=42)
@@ -422,7 +423,8 @@ def bench_batched(args, world: int, rank: int, pg):
                    "rank0_waves": info["waves"], "rank0_instances": info["instances"],
                    "parallelism": f"graphs sharded over {world} ranks (LPT by links)" if world > 1 else "single GPU",
                    "timing": "value: device time of the optimiser runs (graphs resident); e2e: wall time of "
-                             "rmx_batch_optimize from host arrays (packing, copies, CSR build, runs)"},
+                             "rmx_batch_optimize from host arrays (packing, copies, CSR build, runs)",
+                   "launch_tuning": get_tuning()},
         "quality": {"L_bits_mean": float(np.mean(L_bits)), "n_modules_mean": float(np.mean(n_mod))},
         "e2e": {"value": G / wall_max, "unit": "graphs/s", "h2d_bytes_per_step": int(links * 16),
                 "d2h_bytes_per_step": int(nodes * 4 + len(mine) * 16)},
