@@ -3,6 +3,7 @@
 // .clu files, so scripts can drive either binary.
 #include <sys/time.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -19,12 +20,58 @@ double now_s() {
     return t.tv_sec + 1e-6 * t.tv_usec;
 }
 
+// Applies the grid caps of a launch tuning file (the JSON that
+// relaxmap_b200.autotune writes): every "eval_*_grid": <int> found in it, the
+// others keep their values. The values change run time only, never results.
+bool apply_tuning_file(const std::string &path) {
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) {
+        printf("cannot read the tuning file %s\n", path.c_str());
+        return false;
+    }
+    std::string text;
+    char buf[4096];
+    size_t r;
+    while ((r = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, r);
+    fclose(f);
+    rmx_tuning t;
+    rmx_get_tuning(&t);
+    struct Field {
+        const char *name;
+        int32_t *v;
+    } fields[] = {{"\"eval_mid_grid\"", &t.eval_mid_grid},
+                  {"\"eval_block_grid\"", &t.eval_block_grid},
+                  {"\"eval_large_grid\"", &t.eval_large_grid},
+                  {"\"eval_warp_grid\"", &t.eval_warp_grid},
+                  {"\"eval_reg_grid\"", &t.eval_reg_grid}};
+    for (const Field &fd : fields) {
+        const size_t k = text.find(fd.name);
+        if (k == std::string::npos) continue;
+        const size_t colon = text.find(':', k);
+        if (colon == std::string::npos) continue;
+        char *end = nullptr;
+        const long v = strtol(text.c_str() + colon + 1, &end, 10);
+        if (end == text.c_str() + colon + 1) {
+            printf("tuning file %s: %s has no integer value\n", path.c_str(), fd.name);
+            return false;
+        }
+        *fd.v = (int32_t)std::max(-1L, std::min(v, 1000L));  // out-of-range values are rejected below
+    }
+    if (rmx_set_tuning(&t) != RMX_OK) {
+        printf("tuning file %s: %s\n", path.c_str(), rmx_last_error());
+        return false;
+    }
+    printf("Launch tuning from %s: grid caps (blocks per SM) mid %d, block %d, large %d, warp %d, register %d\n",
+           path.c_str(), t.eval_mid_grid, t.eval_block_grid, t.eval_large_grid, t.eval_warp_grid, t.eval_reg_grid);
+    return true;
+}
+
 }  // namespace
 
 extern "C" int rmx_cli_main(int argc, char **argv) {
     if (argc < 10) {
         printf("Call: ./ompRelaxmap <seed> <network.net> <# threads> <# attempts> <threshold> <vThresh> <maxIter> "
-               "<outDir> <prior/normal>  [selflinks]\n");
+               "<outDir> <prior/normal>  [selflinks] [--tuning=<file>]\n");
         return -1;
     }
     const std::string outDir = argv[8];
@@ -47,7 +94,19 @@ extern "C" int rmx_cli_main(int argc, char **argv) {
     o.vthresh = atof(argv[6]);
     printf("Threshold = %g, Vertex-Threshold = %g\n", o.threshold, o.vthresh);
     o.prior = std::string(argv[9]) == "prior";
-    bool selflinks = argc == 11 && std::string(argv[10]) == "selflinks";
+    // options of this build (--tuning=<file>) may follow the positional
+    // arguments; without them "selflinks" counts only as the single argument
+    // after the ninth (argc == 11, OmpRelaxmap.cpp:75-77), and so it does here
+    std::vector<std::string> extra;
+    for (int i = 10; i < argc; i++) {
+        const std::string a = argv[i];
+        if (a.rfind("--tuning=", 0) == 0) {
+            if (!apply_tuning_file(a.substr(9))) return -1;
+        } else {
+            extra.push_back(a);
+        }
+    }
+    const bool selflinks = extra.size() == 1 && extra[0] == "selflinks";
     o.verbose = 1;
 
     const double all0 = now_s();

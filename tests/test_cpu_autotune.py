@@ -104,3 +104,24 @@ def test_save_and_load_per_device(tmp_path, restore_tuning):
     p.write_text(json.dumps({"format": 7, "device": "B200|148 SMs", "tuning": tuned}))
     with pytest.raises(ValueError):
         load(p, device="B200|148 SMs")
+
+
+def test_cli_tuning_flag(tmp_path, restore_tuning):
+    """ompRelaxmap ... [selflinks] --tuning=<file> applies a tuning file before
+    the network is read (the missing network here stops the run there, so no
+    device is needed); a file with an invalid value is rejected (exit -1)
+    without changing the setting."""
+    from relaxmap_b200 import cli, get_tuning
+    from relaxmap_b200.autotune import DEFAULTS
+    good = tmp_path / "tuning.json"
+    good.write_text(json.dumps({"format": 1, "device": "any", "tuning": dict(DEFAULTS, eval_mid_grid=12,
+                                                                              eval_reg_grid=6)}))
+    args = ["ompRelaxmap", "1", str(tmp_path / "missing.txt"), "1", "1", "1e-3", "0.0", "10", str(tmp_path),
+            "prior", "selflinks"]
+    assert cli(args + [f"--tuning={good}"]) == -1  # the network file is missing
+    assert get_tuning() == dict(DEFAULTS, eval_mid_grid=12, eval_reg_grid=6)
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"tuning": {"eval_warp_grid": 0}}')
+    assert cli(args + [f"--tuning={bad}"]) == -1
+    assert get_tuning() == dict(DEFAULTS, eval_mid_grid=12, eval_reg_grid=6)
+    assert cli(args + [f"--tuning={tmp_path / 'none.json'}"]) == -1
