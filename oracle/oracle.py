@@ -161,8 +161,20 @@ def c_atol(b: bytes) -> int:
     return int(m.group(1)) if m else 0
 
 
+_HEX_RE = re.compile(rb"^[ \t\n\v\f\r]*([+-]?0[xX](?:[0-9a-fA-F]+\.?[0-9a-fA-F]*|\.[0-9a-fA-F]+)(?:[pP][+-]?[0-9]+)?)")
+
+
 def c_atof(b: bytes) -> float:
-    """C atof for decimal / inf / nan prefixes, else 0.0."""
+    """C atof (strtod) on the longest valid prefix: a hexadecimal floating
+    constant (C99, e.g. 0x1p3; the binary exponent is optional), a decimal,
+    inf / infinity or nan; else 0.0. Overflow gives +-inf as strtod does."""
+    h = _HEX_RE.match(b)
+    if h:
+        t = h.group(1).decode()
+        try:
+            return float.fromhex(t)
+        except OverflowError:
+            return float("-inf") if t.startswith("-") else float("inf")
     m = _FLT_RE.match(b)
     if not m:
         return 0.0

@@ -10,10 +10,16 @@
 // boundaries of the multi-threaded edge-list parse.
 #include "rmx_io.hpp"
 
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
-#include <climits>
 #include <cerrno>
+#include <climits>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -21,6 +27,7 @@
 #include <map>
 #include <mutex>
 #include <thread>
+#include <utility>
 
 namespace rmx {
 
@@ -64,8 +71,41 @@ long long c_atol(const Tok &t) {
     return (long long)(neg ? 0ull - v : v);  // negated unsigned: -2^63 has no signed negation
 }
 
-// C atof (strtod) on a token.
+// C atof (strtod) on a token. A token that is a plain decimal
+// [+-]digits[.digits] whose digits form an integer m < 2^53 with at most 22 of
+// them after the point takes Clinger's fast path (W. D. Clinger, "How to read
+// floating point numbers accurately", PLDI 1990): m and 10^k are then exact
+// doubles, so the one IEEE division m / 10^k is the correctly rounded value of
+// the decimal, which is what glibc's strtod returns. Any other token (an
+// exponent, inf/nan, hex, more digits, trailing characters) goes to strtod.
 double c_atof(const Tok &t) {
+    static const double kPow10[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
+                                      1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+    {
+        const char *p = t.b;
+        bool neg = false;
+        if (p < t.e && (*p == '+' || *p == '-')) neg = *p++ == '-';
+        uint64_t m = 0;
+        int digits = 0, frac = 0;
+        bool fast = true, point = false;
+        for (; p < t.e && fast; p++) {
+            const char c = *p;
+            if (c >= '0' && c <= '9') {
+                m = m * 10 + (uint64_t)(c - '0');
+                digits++;
+                if (point) frac++;
+                fast = m < (uint64_t(1) << 53) && frac <= 22;
+            } else if (c == '.' && !point) {
+                point = true;
+            } else {
+                fast = false;
+            }
+        }
+        if (fast && digits > 0) {
+            const double v = (double)m / kPow10[frac];
+            return neg ? -v : v;
+        }
+    }
     char buf[96];
     size_t n = (size_t)(t.e - t.b);
     if (n < sizeof buf) {
@@ -77,38 +117,65 @@ double c_atof(const Tok &t) {
     return strtod(s.c_str(), nullptr);
 }
 
-std::vector<char> read_all(const std::string &path) {
-    FILE *f = fopen(path.c_str(), "rb");
-    if (!f) throw IoError("cannot open " + path + ": " + strerror(errno));
-    std::vector<char> data;
-    if (fseek(f, 0, SEEK_END) == 0) {  // regular file: one read of its size
-        const long sz = ftell(f);
-        if (sz > 0) {
-            rewind(f);
-            data.resize((size_t)sz);
-            size_t got = 0, r;
-            while (got < data.size() && (r = fread(data.data() + got, 1, data.size() - got, f)) > 0) got += r;
-            data.resize(got);
-        } else {
-            rewind(f);
+// The bytes of a file: a read-only mapping of a regular file (the parser
+// threads fault its pages in themselves), else what reads from the stream
+// returned (pipes, devices).
+class FileBytes {
+  public:
+    FileBytes() = default;
+    FileBytes(const FileBytes &) = delete;
+    FileBytes &operator=(const FileBytes &) = delete;
+    FileBytes(FileBytes &&o) noexcept { *this = std::move(o); }
+    FileBytes &operator=(FileBytes &&o) noexcept {
+        if (this != &o) {
+            release();
+            map_ = o.map_;
+            n_ = o.n_;
+            buf_ = std::move(o.buf_);
+            o.map_ = nullptr;
+            o.n_ = 0;
+        }
+        return *this;
+    }
+    ~FileBytes() { release(); }
+    const char *data() const { return map_ ? static_cast<const char *>(map_) : buf_.data(); }
+    size_t size() const { return map_ ? n_ : buf_.size(); }
+    char operator[](size_t i) const { return data()[i]; }
+    void release() {
+        if (map_) munmap(map_, n_);
+        map_ = nullptr;
+        n_ = 0;
+        std::vector<char>().swap(buf_);
+    }
+    static FileBytes read(const std::string &path);
+
+  private:
+    void *map_ = nullptr;
+    size_t n_ = 0;
+    std::vector<char> buf_;
+};
+
+FileBytes FileBytes::read(const std::string &path) {
+    FileBytes out;
+    const int fd = open(path.c_str(), O_RDONLY);
+    if (fd < 0) throw IoError("cannot open " + path + ": " + strerror(errno));
+    struct stat st;
+    if (fstat(fd, &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) {
+        void *m = mmap(nullptr, (size_t)st.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+        if (m != MAP_FAILED) {
+            madvise(m, (size_t)st.st_size, MADV_SEQUENTIAL);
+            out.map_ = m;
+            out.n_ = (size_t)st.st_size;
+            close(fd);
+            return out;
         }
     }
     char chunk[1 << 16];
-    size_t r;
-    while ((r = fread(chunk, 1, sizeof chunk, f)) > 0) data.insert(data.end(), chunk, chunk + r);
-    fclose(f);
-    return data;
-}
-
-// [begin, end) of every getline() line (no trailing empty line after a final '\n').
-void split_lines(const std::vector<char> &d, size_t from, size_t to, std::vector<std::pair<size_t, size_t>> &out) {
-    size_t s = from;
-    for (size_t i = from; i < to; i++)
-        if (d[i] == '\n') {
-            out.push_back({s, i});
-            s = i + 1;
-        }
-    if (s < to) out.push_back({s, to});
+    ssize_t r;
+    while ((r = ::read(fd, chunk, sizeof chunk)) > 0) out.buf_.insert(out.buf_.end(), chunk, chunk + r);
+    close(fd);
+    if (r < 0) throw IoError("cannot read " + path + ": " + strerror(errno));
+    return out;
 }
 
 struct EdgeChunk {
@@ -119,15 +186,16 @@ struct EdgeChunk {
 }  // namespace
 
 // Lines of byte range [from, to) (from at a line start), the lines getline
-// would give, each read as load_linkList_format_network reads a line
-// (FileIO.cpp:196-222): two integers and an optional weight; `buf` is the
-// stream state entering the range.
-void parse_edge_bytes(const std::vector<char> &d, size_t from, size_t to, Tok buf, EdgeChunk &out) {
+// would give, each read as both loaders read a link line: two integers and an
+// optional weight (edge list FileIO.cpp:196-222, Pajek arcs :140-160); `buf`
+// is the stream state entering the range. Only the edge list skips '#' lines.
+void parse_edge_bytes(const FileBytes &d, size_t from, size_t to, Tok buf, bool skip_comments,
+                      EdgeChunk &out) {
     const char *base = d.data();
     size_t s = from;
     auto line = [&](size_t b0, size_t e0) {
         const char *b = base + b0, *e = base + e0;
-        if (b < e && *b == '#') return;  // FileIO.cpp:198 (line[0] of "" is '\0')
+        if (skip_comments && b < e && *b == '#') return;  // FileIO.cpp:198 (line[0] of "" is '\0')
         LineStream ss(b, e);
         ss.read(buf);
         const long long x = c_atol(buf);
@@ -151,16 +219,18 @@ void parse_edge_bytes(const std::vector<char> &d, size_t from, size_t to, Tok bu
     if (s < to) line(s, to);
 }
 
-// State of `buf` entering the line that starts at byte pos: the third token
-// (or "") of the last non-comment line before it.
-Tok state_before_pos(const std::vector<char> &d, size_t pos) {
+// State of `buf` entering the line that starts at byte pos (lo <= pos, both
+// line starts): the third token (or "") of the last line before it in
+// [lo, pos) that was read (with skip_comments, not a '#' line), else `first`,
+// the state entering lo.
+Tok state_before_pos(const FileBytes &d, size_t lo, size_t pos, bool skip_comments, Tok first) {
     const char *base = d.data();
     size_t e = pos;  // the previous line ends at e - 1 ('\n')
-    while (e > 0) {
+    while (e > lo) {
         const size_t le = e - 1;  // index of the '\n' ending the previous line
         size_t b = le;
-        while (b > 0 && base[b - 1] != '\n') b--;
-        if (!(b < le && base[b] == '#')) {
+        while (b > lo && base[b - 1] != '\n') b--;
+        if (!(skip_comments && b < le && base[b] == '#')) {
             LineStream ss(base + b, base + le);
             Tok t;
             ss.read(t);
@@ -171,62 +241,75 @@ Tok state_before_pos(const std::vector<char> &d, size_t pos) {
         }
         e = b;
     }
-    return Tok();
+    return first;
 }
 
-ParsedGraph parse_edge_list(const std::string &path, int threads) {
-    std::vector<char> d = read_all(path);
-    int T = std::max(1, std::min(threads, 64));
-    if (d.size() < (size_t(1) << 20)) T = 1;
-    // byte chunks that start at line starts
-    std::vector<size_t> cut(T + 1, d.size());
-    cut[0] = 0;
-    for (int t = 1; t < T; t++) {
-        size_t c = std::max(cut[t - 1], d.size() * t / T);
-        while (c < d.size() && c > 0 && d[c - 1] != '\n') c++;
-        cut[t] = c;
+// job(t) for t < T on T threads (inline for T == 1); the first exception a job
+// throws (or a failed thread start) is rethrown after every started thread
+// has joined.
+template <typename Job>
+void run_parallel(int T, Job &&job) {
+    if (T == 1) {
+        job(0);
+        return;
     }
-    std::vector<EdgeChunk> chunks(T);
-    std::vector<long long> lo(T, LLONG_MAX), hi(T, LLONG_MIN);
-    // job(t) on T threads; the first exception a job throws (or a failed
-    // thread start) is rethrown here after every started thread has joined
-    auto parallel = [&](auto &&job) {
-        if (T == 1) {
-            job(0);
-            return;
-        }
-        std::exception_ptr err;
-        std::mutex err_mu;
-        auto guarded = [&](int t) {
-            try {
-                job(t);
-            } catch (...) {
-                std::lock_guard<std::mutex> lk(err_mu);
-                if (!err) err = std::current_exception();
-            }
-        };
-        std::vector<std::thread> pool;
+    std::exception_ptr err;
+    std::mutex err_mu;
+    auto guarded = [&](int t) {
         try {
-            for (int t = 0; t < T; t++) pool.emplace_back(guarded, t);
+            job(t);
         } catch (...) {
             std::lock_guard<std::mutex> lk(err_mu);
             if (!err) err = std::current_exception();
         }
-        for (auto &th : pool) th.join();
-        if (err) std::rethrow_exception(err);
     };
+    std::vector<std::thread> pool;
+    try {
+        for (int t = 0; t < T; t++) pool.emplace_back(guarded, t);
+    } catch (...) {
+        std::lock_guard<std::mutex> lk(err_mu);
+        if (!err) err = std::current_exception();
+    }
+    for (auto &th : pool) th.join();
+    if (err) std::rethrow_exception(err);
+}
+
+// Threads for a byte range: one below 1 MB, else `threads` (at most 64).
+int range_threads(size_t bytes, int threads) {
+    return bytes < (size_t(1) << 20) ? 1 : std::max(1, std::min(threads, 64));
+}
+
+// [lo, hi) split into T byte ranges that start at line starts.
+std::vector<size_t> line_cuts(const FileBytes &d, size_t lo, size_t hi, int T) {
+    std::vector<size_t> cut(T + 1, hi);
+    cut[0] = lo;
+    for (int t = 1; t < T; t++) {
+        size_t c = std::max(cut[t - 1], lo + (hi - lo) * t / T);
+        while (c < hi && c > lo && d[c - 1] != '\n') c++;
+        cut[t] = c;
+    }
+    return cut;
+}
+
+ParsedGraph parse_edge_list(const std::string &path, int threads) {
+    FileBytes d = FileBytes::read(path);
+    const int T = range_threads(d.size(), threads);
+    const std::vector<size_t> cut = line_cuts(d, 0, d.size(), T);
+    std::vector<EdgeChunk> chunks(T);
+    std::vector<long long> lo(T, LLONG_MAX), hi(T, LLONG_MIN);
+    auto parallel = [&](auto &&job) { run_parallel(T, job); };
     parallel([&](int t) {
         const size_t reserve = (cut[t + 1] - cut[t]) / 16 + 16;
         chunks[t].a.reserve(reserve);
         chunks[t].b.reserve(reserve);
         chunks[t].w.reserve(reserve);
-        parse_edge_bytes(d, cut[t], cut[t + 1], state_before_pos(d, cut[t]), chunks[t]);
+        parse_edge_bytes(d, cut[t], cut[t + 1], state_before_pos(d, 0, cut[t], true, Tok()), true, chunks[t]);
         for (size_t i = 0; i < chunks[t].a.size(); i++) {
             lo[t] = std::min({lo[t], chunks[t].a[i], chunks[t].b[i]});
             hi[t] = std::max({hi[t], chunks[t].a[i], chunks[t].b[i]});
         }
     });
-    std::vector<char>().swap(d);
+    d.release();
     size_t total = 0;
     long long mn = LLONG_MAX, mx = LLONG_MIN;
     for (int t = 0; t < T; t++) {
@@ -312,32 +395,34 @@ ParsedGraph parse_edge_list(const std::string &path, int threads) {
     return g;
 }
 
-ParsedGraph parse_pajek(const std::string &path) {
-    std::vector<char> d;
+ParsedGraph parse_pajek(const std::string &path, int threads) {
+    FileBytes d;
     try {
-        d = read_all(path);
+        d = FileBytes::read(path);
     } catch (const IoError &) {
         // the reference reads from a failed stream: "not in Pajek format"
         throw FormatError("the network file is not in Pajek format...exiting");
     }
-    std::vector<std::pair<size_t, size_t>> lines;
-    split_lines(d, 0, d.size(), lines);
     const char *base = d.data();
-    size_t li = 0;
+    size_t pos = 0;  // start of the next getline line; d.size() when there is none
+    // the next line, or an empty one past the end (a failed getline reads nothing)
+    auto next_line = [&](const char *&b, const char *&e) {
+        if (pos >= d.size()) {
+            b = e = base;
+            return;
+        }
+        const char *nl = static_cast<const char *>(memchr(base + pos, '\n', d.size() - pos));
+        const size_t end = nl ? (size_t)(nl - base) : d.size();
+        b = base + pos;
+        e = base + end;
+        pos = nl ? end + 1 : d.size();
+    };
     Tok buf;
     long long n = 0;
-    auto line_at = [&](size_t i, const char *&b, const char *&e) {
-        if (i < lines.size()) {
-            b = base + lines[i].first;
-            e = base + lines[i].second;
-        } else {
-            b = e = base;
-        }
-    };
     while (n == 0) {  // FileIO.cpp:59-77
-        if (li >= lines.size()) throw FormatError("the network file is not in Pajek format...exiting");
+        if (pos >= d.size()) throw FormatError("the network file is not in Pajek format...exiting");
         const char *b, *e;
-        line_at(li++, b, e);
+        next_line(b, e);
         LineStream ss(b, e);
         ss.read(buf);
         const std::string t = buf.str();
@@ -349,14 +434,14 @@ ParsedGraph parse_pajek(const std::string &path) {
         }
     }
     if (n < 0 || n >= INT32_MAX) throw FormatError("invalid vertex count");
-    if (li + (size_t)n > lines.size()) throw FormatError("Number of nodes not matching, exiting");
     ParsedGraph g;
     g.n = (int32_t)n;
     g.names.resize((size_t)n);
     g.node_w.assign((size_t)n, 1.0);
     for (long long i = 0; i < n; i++) {  // FileIO.cpp:86-121
+        if (pos >= d.size()) throw FormatError("Number of nodes not matching, exiting");
         const char *b, *e;
-        line_at(li++, b, e);
+        next_line(b, e);
         LineStream ss(b, e);
         ss.read(buf);
         const char *q0 = nullptr, *q1 = nullptr;
@@ -384,36 +469,74 @@ ParsedGraph parse_pajek(const std::string &path) {
     }
     {  // FileIO.cpp:126-134
         const char *b, *e;
-        line_at(li++, b, e);
+        next_line(b, e);
         LineStream ss(b, e);
         ss.read(buf);
         const std::string t = buf.str();
         if (t != "*Edges" && t != "*edges" && t != "*Arcs" && t != "*arcs")
             throw FormatError("Number of nodes not matching, exiting");
     }
-    std::map<long long, double> self;
-    for (; li < lines.size(); li++) {  // FileIO.cpp:140-160
-        const char *b = base + lines[li].first, *e = base + lines[li].second;
-        LineStream ss(b, e);
-        ss.read(buf);
-        const long long x = c_atol(buf) - 1;
-        ss.read(buf);
-        const long long y = c_atol(buf) - 1;
-        buf = Tok();
-        ss.read(buf);
-        const double w = buf.empty() ? 1.0 : c_atof(buf);
-        g.n_lines++;
-        if (x == y) {  // self-links are counted then dropped (OmpRelaxmap.cpp:123-128)
-            self[x] += w;
-            continue;
+    // the link lines (FileIO.cpp:140-160) in byte ranges on all threads: the
+    // state entering the first is the header token still in buf
+    const size_t lo = pos, hi = d.size();
+    const int T = range_threads(hi - lo, threads);
+    const std::vector<size_t> cut = line_cuts(d, lo, hi, T);
+    std::vector<EdgeChunk> chunks(T);
+    const Tok header = buf;
+    run_parallel(T, [&](int t) {
+        parse_edge_bytes(d, cut[t], cut[t + 1], state_before_pos(d, lo, cut[t], false, header), false, chunks[t]);
+    });
+    // ids are 1-based; self-links are counted and dropped before the range
+    // check (OmpRelaxmap.cpp:123-128); the first link outside 1..n in file
+    // order is the error
+    auto id0 = [](long long v) { return (long long)((unsigned long long)v - 1ull); };
+    std::vector<size_t> keep(T + 1, 0);
+    std::vector<int64_t> bad(T, -1);
+    run_parallel(T, [&](int t) {
+        const EdgeChunk &c = chunks[t];
+        size_t k = 0;
+        for (size_t i = 0; i < c.a.size(); i++) {
+            const long long x = id0(c.a[i]), y = id0(c.b[i]);
+            if (x == y) continue;
+            if (x < 0 || y < 0 || x >= n || y >= n) {
+                bad[t] = (int64_t)i;
+                break;
+            }
+            k++;
         }
-        if (x < 0 || y < 0 || x >= n || y >= n)
-            throw FormatError("link " + std::to_string(x + 1) + " " + std::to_string(y + 1) + " outside 1.." +
-                              std::to_string(n));
-        g.src.push_back((int32_t)x);
-        g.dst.push_back((int32_t)y);
-        g.w.push_back(w);
+        keep[t + 1] = k;
+    });
+    for (int t = 0; t < T; t++) {
+        if (bad[t] >= 0) {
+            const size_t i = (size_t)bad[t];
+            throw FormatError("link " + std::to_string(chunks[t].a[i]) + " " + std::to_string(chunks[t].b[i]) +
+                              " outside 1.." + std::to_string(n));
+        }
+        keep[t + 1] += keep[t];
+        g.n_lines += (int64_t)chunks[t].a.size();
     }
+    g.src.resize(keep[T]);
+    g.dst.resize(keep[T]);
+    g.w.resize(keep[T]);
+    std::vector<std::vector<std::pair<long long, double>>> selfs(T);
+    run_parallel(T, [&](int t) {
+        const EdgeChunk &c = chunks[t];
+        size_t o = keep[t];
+        for (size_t i = 0; i < c.a.size(); i++) {
+            const long long x = id0(c.a[i]), y = id0(c.b[i]);
+            if (x == y) {
+                selfs[t].push_back({x, c.w[i]});
+                continue;
+            }
+            g.src[o] = (int32_t)x;
+            g.dst[o] = (int32_t)y;
+            g.w[o] = c.w[i];
+            o++;
+        }
+    });
+    std::map<long long, double> self;  // summed in file order
+    for (auto &v : selfs)
+        for (auto &kv : v) self[kv.first] += kv.second;
     for (auto &kv : self)
         if (kv.second > 0.0) g.n_self++;
     return g;
@@ -422,7 +545,7 @@ ParsedGraph parse_pajek(const std::string &path) {
 ParsedGraph parse_file(const std::string &path, int threads) {
     const size_t dot = path.find_last_of('.');
     const std::string ext = dot == std::string::npos ? std::string() : path.substr(dot);
-    if (ext == ".net") return parse_pajek(path);
+    if (ext == ".net") return parse_pajek(path, threads);
     return parse_edge_list(path, threads);
 }
 

@@ -28,7 +28,7 @@ struct ParsedGraph {
 // load_linkList_format_network (FileIO.cpp:177-265).
 ParsedGraph parse_edge_list(const std::string &path, int threads);
 // load_pajek_format_network (FileIO.cpp:32-171).
-ParsedGraph parse_pajek(const std::string &path);
+ParsedGraph parse_pajek(const std::string &path, int threads = 1);
 // Choose by extension as main does (OmpRelaxmap.cpp:60, :93-98).
 ParsedGraph parse_file(const std::string &path, int threads);
 

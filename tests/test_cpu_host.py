@@ -62,6 +62,35 @@ def test_edge_list_quirks(built_lib, oracle_mod, tmp_path):
     assert ld.names == ["-3", "0", "3", "5", "7", "9", "100"]
 
 
+def test_weights_parse_like_strtod(built_lib, oracle_mod, tmp_path):
+    """Weights read with the decimal fast path (plain decimals with a mantissa
+    below 2^53 and at most 22 fractional digits) and with strtod (all other
+    forms) equal the correctly rounded values of the oracle, weight by weight
+    (every line its own link)."""
+    rng = np.random.default_rng(8)
+    lines = []
+    for i in range(30000):
+        k = rng.integers(0, 10)
+        digits = "".join(rng.choice(list("0123456789"), size=rng.integers(1, 21)))
+        cut = int(rng.integers(0, len(digits) + 1))
+        sign = ["", "-", "+"][rng.integers(0, 3)]
+        if k < 6:    # plain decimals: both sides of the 2^53 and 22-fraction-digit limits
+            w = sign + digits[:cut] + "." + digits[cut:] if k < 4 else sign + digits
+        elif k == 6:  # long fractions, leading zeros
+            w = sign + "0." + "0" * int(rng.integers(0, 25)) + digits
+        elif k == 7:  # exponents
+            w = sign + digits[:cut] + "." + digits[cut:] + "e" + str(int(rng.integers(-30, 30)))
+        elif k == 8:  # trailing characters, bare point, infinities, hexadecimal (C99 strtod reads 0x1p3 as 8)
+            w = [sign + digits + "x", ".", sign + ".5", "inf", "-infinity", "0x1p3", sign + digits + ".e",
+                 "-0x.8p1"][rng.integers(0, 8)]
+        else:
+            w = sign + digits[:cut] + "." + digits[cut:] + "abc"
+        lines.append(f"{2 * i} {2 * i + 1} {w}")
+    p = tmp_path / "weights.txt"
+    p.write_text("\n".join(lines) + "\n")
+    _cmp_oracle(p, oracle_mod, threads=(1,))
+
+
 def test_edge_list_large_threads(built_lib, oracle_mod, tmp_path):
     rng = np.random.default_rng(2)
     lines = []
@@ -117,6 +146,44 @@ def test_pajek_quirks(built_lib, oracle_mod, tmp_path):
     ld = _cmp_oracle(p, oracle_mod)
     assert ld.names == ["a b", "c", "d", "4", "e"]
     np.testing.assert_array_equal(ld.node_w, [2.0, 1.0, 0.5, 1.0, 1.0])
+
+
+def _pajek_text(rng, n, n_arcs):
+    vert = [f"*Vertices {n}"] + [f'{i + 1} "v{i + 1}"' for i in range(n)]
+    kinds = rng.choice(6, size=n_arcs, p=[0.15, 0.05, 0.05, 0.25, 0.40, 0.10])
+    ids = rng.integers(1, n + 1, size=(n_arcs, 2))
+    wts = rng.uniform(0.0, 4.0, size=n_arcs)
+    arcs = [["", " \t ", "\r", f"{a} {b}", f"{a}\t{b}\t{x!r}", f"{a} {b} {x:.3f}\r"][k]
+            for k, (a, b), x in zip(kinds.tolist(), ids.tolist(), wts.tolist())]
+    # a blank line right after the header re-reads the header token
+    return vert + ["*Arcs", ""] + arcs
+
+
+def test_pajek_arcs_at_range_boundaries(built_lib, oracle_mod, tmp_path):
+    """The arcs section is parsed in byte ranges on all threads; each range
+    starts with the stream state of the line before it (its third token or
+    ""; the header token for the first), which blank, whitespace-only and
+    bare-CR lines re-read as a self-link."""
+    rng = np.random.default_rng(5)
+    lines = _pajek_text(rng, 3000, 150000)
+    p = tmp_path / "arcs.net"
+    p.write_text("\n".join(lines) + "\n")
+    assert len("\n".join(lines[3002:])) > (1 << 20)  # the arcs section alone takes the multi-range parse
+    _cmp_oracle(p, oracle_mod, threads=(1, 2, 7, 16, 64))
+
+
+def test_pajek_first_bad_link_in_file_order(built_lib, tmp_path):
+    from relaxmap_b200 import RmxError, parse_file
+    rng = np.random.default_rng(6)
+    lines = _pajek_text(rng, 3000, 150000)
+    lines[3002 + 60000] = "1 3001"
+    lines[3002 + 140000] = "3002 5 1.5"
+    p = tmp_path / "bad_arcs.net"
+    p.write_text("\n".join(lines) + "\n")
+    for t in (1, 8, 64):
+        with pytest.raises(RmxError) as e:
+            parse_file(p, threads=t)
+        assert e.value.status == 3 and "link 1 3001 outside 1..3000" in str(e.value)
 
 
 def test_errors_without_device(built_lib, tmp_path):
