@@ -326,18 +326,30 @@ ParsedGraph parse_edge_list(const std::string &path, int threads) {
     const unsigned long long span = (unsigned long long)mx - (unsigned long long)mn;
     const bool dense = total > 0 && span < 4ull * (2 * total) + 1024;
     if (dense) {
-        const size_t range = (size_t)span + 1;
-        std::vector<uint8_t> seen(range, 0);
+        const size_t range = (size_t)span + 1, words = (range + 63) / 64;
+        // a presence bitmap per thread (no cache line written by two threads),
+        // then OR-ed slice by slice
+        std::vector<std::vector<uint64_t>> bits(T);
         parallel([&](int t) {
-            for (size_t i = 0; i < chunks[t].a.size(); i++) {
-                __atomic_store_n(&seen[(size_t)chunks[t].a[i] - (size_t)mn], (uint8_t)1, __ATOMIC_RELAXED);
-                __atomic_store_n(&seen[(size_t)chunks[t].b[i] - (size_t)mn], (uint8_t)1, __ATOMIC_RELAXED);
+            bits[t].assign(words, 0);
+            uint64_t *b = bits[t].data();
+            const EdgeChunk &c = chunks[t];
+            for (size_t i = 0; i < c.a.size(); i++) {
+                const size_t va = (size_t)c.a[i] - (size_t)mn, vb = (size_t)c.b[i] - (size_t)mn;
+                b[va >> 6] |= uint64_t(1) << (va & 63);
+                b[vb >> 6] |= uint64_t(1) << (vb & 63);
             }
+        });
+        parallel([&](int t) {
+            const size_t w0 = words * t / T, w1 = words * (t + 1) / T;
+            for (int u = 1; u < T; u++)
+                for (size_t x = w0; x < w1; x++) bits[0][x] |= bits[u][x];
         });
         table.assign(range, -1);
         int64_t k = 0;
-        for (size_t v = 0; v < range; v++)
-            if (seen[v]) {
+        for (size_t x = 0; x < words; x++)
+            for (uint64_t m = bits[0][x]; m; m &= m - 1) {
+                const size_t v = x * 64 + (size_t)__builtin_ctzll(m);
                 table[v] = (int32_t)k++;
                 ids.push_back((long long)((unsigned long long)mn + v));
             }
@@ -355,7 +367,9 @@ ParsedGraph parse_edge_list(const std::string &path, int threads) {
     g.n = (int32_t)ids.size();
     g.n_lines = (int64_t)total;
     g.names.resize(ids.size());
-    for (size_t i = 0; i < ids.size(); i++) g.names[i] = std::to_string(ids[i]);
+    parallel([&](int t) {
+        for (size_t i = ids.size() * t / T; i < ids.size() * (t + 1) / T; i++) g.names[i] = std::to_string(ids[i]);
+    });
     auto ren = [&](long long x) -> int32_t {
         if (dense) return table[(size_t)x - (size_t)mn];
         return (int32_t)(std::lower_bound(ids.begin(), ids.end(), x) - ids.begin());

@@ -1,7 +1,12 @@
 // Host-side input parsing and output writing with the reference's rules.
 #pragma once
+#include <cstdint>
+#include <memory>
+#include <new>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 namespace rmx {
@@ -13,12 +18,37 @@ struct FormatError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
 
+// std::allocator whose default construction of trivial elements leaves them
+// uninitialised: resize() of an array that parser threads then fill touches
+// no page itself, so the pages are first touched by those threads, in
+// parallel, instead of being zeroed by one.
+template <typename T>
+struct NoInitAlloc : std::allocator<T> {
+    template <typename U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <typename U>
+    NoInitAlloc(const NoInitAlloc<U> &) noexcept {}
+    template <typename U>
+    void construct(U *p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new (static_cast<void *>(p)) U;
+    }
+    template <typename U, typename... Args>
+    void construct(U *p, Args &&...args) {
+        ::new (static_cast<void *>(p)) U(std::forward<Args>(args)...);
+    }
+};
+template <typename T>
+using HostVec = std::vector<T, NoInitAlloc<T>>;
+
 // What a reference loader leaves behind, as raw (unsummed) edges in file
 // order: the device build sums duplicates in that order.
 struct ParsedGraph {
     int32_t n = 0;
-    std::vector<int32_t> src, dst;
-    std::vector<double> w;
+    HostVec<int32_t> src, dst;
+    HostVec<double> w;
     std::vector<double> node_w;  // empty: uniform (edge-list files)
     std::vector<std::string> names;
     int64_t n_self = 0;          // self-link pairs with positive summed weight
