@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 from pathlib import Path
 
 import numpy as np
@@ -125,7 +126,10 @@ class Graph:
         return cls(h)
 
     @classmethod
-    def from_file(cls, path, threads: int = 1) -> "Graph":
+    def from_file(cls, path, threads: int | None = None) -> "Graph":
+        """Load a .net / edge-list file with the reference's rules; `threads`
+        host parsing threads (default: every core)."""
+        threads = _host_threads(threads)
         h = C.c_void_p()
         _check(lib().rmx_graph_load_file(str(path).encode(), C.c_int32(threads), C.byref(h)))
         return cls(h)
@@ -315,8 +319,14 @@ class Batch:
         self.close()
 
 
-def parse_file(path, threads: int = 1) -> dict:
-    """Host-only parse with the loader rules (no GPU needed)."""
+def _host_threads(threads: int | None) -> int:
+    return max(1, os.cpu_count() or 1) if threads is None else int(threads)
+
+
+def parse_file(path, threads: int | None = None) -> dict:
+    """Host-only parse with the loader rules (no GPU needed); `threads` host
+    threads (default: every core)."""
+    threads = _host_threads(threads)
     n, m, ns = C.c_int32(), C.c_int64(), C.c_int64()
     _check(lib().rmx_parse_file(str(path).encode(), C.c_int32(threads), C.byref(n), C.byref(m), C.byref(ns), None,
                                 None, None, None))
