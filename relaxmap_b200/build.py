@@ -2,6 +2,10 @@
 relaxmap_b200/ompRelaxmap (the drop-in command line), sm_100a only.
 
     python -m relaxmap_b200.build [--force]
+
+RMX_NVCC_EXTRA adds compiler flags, e.g. RMX_NVCC_EXTRA="-DRMX_DELTA_MINB=5" to
+build a variant of a compile-time launch bound; every object is rebuilt when
+the flags differ from the previous build's.
 """
 from __future__ import annotations
 
@@ -18,7 +22,8 @@ LIB = PKG / "librelaxmap_b200.so"
 CLI = PKG / "ompRelaxmap"
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-Wall", "-diag-suppress", "177"]
+FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3,-Wall", "-diag-suppress", "177",
+         *os.environ.get("RMX_NVCC_EXTRA", "").split()]
 CU = ["rmx_prims.cu", "rmx_flow.cu", "rmx_moves.cu", "rmx_coarsen.cu", "rmx_engine.cu", "rmx_adjoint.cu", "rmx_noalloc.cu"]
 CPP = ["rmx_io.cpp", "rmx_abi.cpp", "rmx_cli.cpp", "rmx_batch.cpp"]
 CUDA_CPP = {"rmx_abi.cpp", "rmx_batch.cpp"}
@@ -41,6 +46,10 @@ def _run(cmd):
 
 def build(force: bool = False, verbose: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
+    stamp = OBJ / "flags.txt"  # the flags the objects were built with
+    flags = " ".join([NVCC, *ARCH, *FLAGS])
+    if not stamp.exists() or stamp.read_text() != flags:
+        force = True
     hdrs = [CSRC / h for h in HEADERS] + [PKG.parent / "include" / "relaxmap_b200.h"]
     jobs = []
     objs = []
@@ -63,6 +72,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         _run([NVCC, *ARCH, *FLAGS, "-c", str(CSRC / "ompRelaxmap_main.cpp"), "-o", str(main_o)])
     if force or _stale(CLI, [main_o, LIB]):
         _run([NVCC, *ARCH, "-o", str(CLI), str(main_o), *map(str, objs), "-lpthread", "-ldl", "-lrt"])
+    stamp.write_text(flags)
     return LIB
 
 
