@@ -183,8 +183,6 @@ struct EdgeChunk {
     std::vector<double> w;
 };
 
-}  // namespace
-
 // Lines of byte range [from, to) (from at a line start), the lines getline
 // would give, each read as both loaders read a link line: two integers and an
 // optional weight (edge list FileIO.cpp:196-222, Pajek arcs :140-160); `buf`
@@ -290,6 +288,8 @@ std::vector<size_t> line_cuts(const FileBytes &d, size_t lo, size_t hi, int T) {
     }
     return cut;
 }
+
+}  // namespace
 
 ParsedGraph parse_edge_list(const std::string &path, int threads) {
     FileBytes d = FileBytes::read(path);
