@@ -247,3 +247,31 @@ def test_lpt_weights_edge_cases():
     assert [len(p) for p in parts] == [1, 0, 0, 0]
     parts = lpt_assign([1.0, 1.0, 1.0, 1.0], 2)
     assert sorted(len(p) for p in parts) == [2, 2]
+
+
+def test_header_is_c99_and_links_from_c(built_lib, tmp_path):
+    """include/relaxmap_b200.h compiles as strict C99 and a C program links
+    against the library and calls its device-free entry points (what a C
+    caller of the ABI does); skipped without gcc."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no gcc")
+    prog = tmp_path / "abi.c"
+    prog.write_text('#include <stdio.h>\n#include "relaxmap_b200.h"\n'
+                    "int main(void) {\n"
+                    "    rmx_tuning t;\n"
+                    "    rmx_opts o;\n"
+                    "    rmx_opts_default(&o);\n"
+                    "    if (rmx_get_tuning(&t) != RMX_OK) return 1;\n"
+                    "    t.eval_warp_grid = 0;\n"
+                    "    if (rmx_set_tuning(&t) != RMX_ERR_INVALID) return 2;\n"
+                    "    printf(\"%s|%d|%u\\n\", rmx_version(), t.eval_mid_grid, o.seed);\n"
+                    "    return 0;\n}\n")
+    exe = tmp_path / "abi"
+    lib_dir = built_lib.parent
+    subprocess.run([gcc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", str(ROOT / "include"), str(prog),
+                    "-L", str(lib_dir), "-lrelaxmap_b200", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
+    assert out.startswith("relaxmap_b200")
