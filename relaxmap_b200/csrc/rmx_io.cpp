@@ -563,6 +563,25 @@ ParsedGraph parse_file(const std::string &path, int threads) {
     return parse_edge_list(path, threads);
 }
 
+namespace {
+
+// Threads for formatting n output lines: one below 100K lines.
+int writer_threads(size_t n) {
+    if (n < 100000) return 1;
+    const unsigned hw = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(hw == 0 ? 1u : hw, 16u));
+}
+
+void write_all(FILE *f, const std::vector<std::string> &parts, const std::string &file) {
+    for (const std::string &s : parts)
+        if (!s.empty() && fwrite(s.data(), 1, s.size(), f) != s.size()) {
+            fclose(f);
+            throw IoError("cannot write " + file);
+        }
+}
+
+}  // namespace
+
 void write_tree(const std::string &file, double L_bits, int32_t n_modules, const std::vector<int32_t> &part,
                 const std::vector<double> &size, const std::vector<std::string> &names) {
     FILE *f = fopen(file.c_str(), "wb");
@@ -577,16 +596,31 @@ void write_tree(const std::string &file, double L_bits, int32_t n_modules, const
     std::vector<int32_t> mem(n);
     std::vector<int64_t> fill(head.begin(), head.end() - 1);
     for (size_t v = 0; v < n; v++) mem[fill[(size_t)part[v]]++] = (int32_t)v;
-    int mod = 0;
-    for (size_t m = 0; m < n; m++) {
-        if (head[m + 1] == head[m]) continue;
-        mod++;
-        for (int64_t j = head[m]; j < head[m + 1]; j++) {
-            const int32_t v = mem[j];
-            fprintf(f, "%d:%lld %g \"%s\"\n", mod, (long long)(j - head[m] + 1), size[v],
-                    v < (int32_t)names.size() ? names[v].c_str() : "");
+    std::vector<int32_t> modnum(n, 0);
+    int32_t mod = 0;
+    for (size_t m = 0; m < n; m++)
+        if (head[m + 1] > head[m]) modnum[m] = ++mod;
+    // the lines of member positions [j0, j1) formatted by each thread, written in order
+    const int T = writer_threads(n);
+    std::vector<std::string> out(T);
+    run_parallel(T, [&](int t) {
+        const int64_t j0 = (int64_t)(n * t / T), j1 = (int64_t)(n * (t + 1) / T);
+        if (j0 >= j1) return;
+        std::string &s = out[t];
+        s.reserve((size_t)(j1 - j0) * 40);
+        size_t m = (size_t)(std::upper_bound(head.begin(), head.end(), j0) - head.begin()) - 1;
+        char line[96];
+        for (int64_t j = j0; j < j1; j++) {
+            while (head[m + 1] <= j) m++;
+            const int32_t v = mem[(size_t)j];
+            const int k = snprintf(line, sizeof line, "%d:%lld %g \"", modnum[m], (long long)(j - head[m] + 1),
+                                   size[(size_t)v]);
+            s.append(line, (size_t)k);
+            if (v < (int32_t)names.size()) s.append(names[(size_t)v]);
+            s.append("\"\n");
         }
-    }
+    });
+    write_all(f, out, file);
     fclose(f);
 }
 
@@ -594,7 +628,19 @@ void write_clu(const std::string &file, const std::vector<int32_t> &part) {
     FILE *f = fopen(file.c_str(), "wb");
     if (!f) throw IoError("cannot write " + file);
     fprintf(f, "*Vertices %zu\r\n", part.size());
-    for (int32_t m : part) fprintf(f, "%d\r\n", m + 1);
+    const size_t n = part.size();
+    const int T = writer_threads(n);
+    std::vector<std::string> out(T);
+    run_parallel(T, [&](int t) {
+        std::string &s = out[t];
+        s.reserve((n / T + 1) * 8);
+        char line[24];
+        for (size_t i = n * t / T; i < n * (t + 1) / T; i++) {
+            const int k = snprintf(line, sizeof line, "%d\r\n", part[i] + 1);
+            s.append(line, (size_t)k);
+        }
+    });
+    write_all(f, out, file);
     fclose(f);
 }
 
