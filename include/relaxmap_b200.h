@@ -110,7 +110,10 @@ rmx_status rmx_graph_load_file(const char *path, int32_t threads, rmx_graph **ou
  * formed by rmx_graph_create) and self-links removed (their count in
  * *n_self). Call with NULL buffers to get *n_nodes / *n_edges, then again with
  * src/dst/w of *n_edges entries and node_w of *n_nodes entries (node_w gets
- * the Pajek node weights, 1 for edge lists). */
+ * the Pajek node weights, 1 for edge lists). The size query keeps its parse
+ * for the next call on the same thread with the same path and thread count if
+ * the file is unchanged (device, inode, size and modification time), so the
+ * pair of calls parses once; any other call drops it. */
 rmx_status rmx_parse_file(const char *path, int32_t threads, int32_t *n_nodes, int64_t *n_edges, int64_t *n_self,
                           int32_t *src, int32_t *dst, double *w, double *node_w);
 

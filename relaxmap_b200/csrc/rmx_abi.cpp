@@ -1,10 +1,13 @@
 // extern "C" boundary: every entry point converts exceptions into rmx_status
 // and records a thread-local message (no C++ exception crosses the ABI).
+#include <sys/stat.h>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
+#include <utility>
 
 #include "rmx_batch.hpp"
 #include "rmx_graph.hpp"
@@ -13,6 +16,23 @@
 namespace {
 
 thread_local std::string g_last_error;
+
+// The parse a size query of rmx_parse_file (all buffers NULL) made, kept for
+// the next call on this thread when it names the same path and thread count
+// and the file is unchanged (device, inode, size, modification time).
+struct ParseCache {
+    bool valid = false;
+    std::string path;
+    int32_t threads = 0;
+    struct stat st {};
+    rmx::ParsedGraph pg;
+};
+thread_local ParseCache g_parse_cache;
+
+bool same_file(const struct stat &a, const struct stat &b) {
+    return a.st_dev == b.st_dev && a.st_ino == b.st_ino && a.st_size == b.st_size &&
+           a.st_mtim.tv_sec == b.st_mtim.tv_sec && a.st_mtim.tv_nsec == b.st_mtim.tv_nsec;
+}
 
 rmx_status fail(rmx_status s, const std::string &msg) {
     g_last_error = msg;
@@ -109,7 +129,23 @@ rmx_status rmx_parse_file(const char *path, int32_t threads, int32_t *n_nodes, i
                           int32_t *src, int32_t *dst, double *w, double *node_w) {
     return guard([&] {
         need(path, "path");
-        rmx::ParsedGraph pg = rmx::parse_file(path, threads);
+        struct stat st {};
+        const bool have_st = stat(path, &st) == 0;
+        ParseCache &c = g_parse_cache;
+        rmx::ParsedGraph pg;
+        if (c.valid && have_st && c.path == path && c.threads == threads && same_file(c.st, st)) {
+            pg = std::move(c.pg);
+        } else {
+            c = ParseCache();
+            pg = rmx::parse_file(path, threads);
+        }
+        c = ParseCache();
+        if (!src && !dst && !w && !node_w && have_st) {  // a size query: the fill call follows
+            c.valid = true;
+            c.path = path;
+            c.threads = threads;
+            c.st = st;
+        }
         if (n_nodes) *n_nodes = pg.n;
         if (n_edges) *n_edges = (int64_t)pg.src.size();
         if (n_self) *n_self = pg.n_self;
@@ -119,6 +155,7 @@ rmx_status rmx_parse_file(const char *path, int32_t threads, int32_t *n_nodes, i
         if (w) std::memcpy(w, pg.w.data(), sizeof(double) * m);
         if (node_w)
             for (int32_t i = 0; i < pg.n; i++) node_w[i] = pg.node_w.empty() ? 1.0 : pg.node_w[i];
+        if (c.valid) c.pg = std::move(pg);
     });
 }
 

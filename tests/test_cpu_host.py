@@ -275,3 +275,34 @@ def test_header_is_c99_and_links_from_c(built_lib, tmp_path):
                     "-L", str(lib_dir), "-lrelaxmap_b200", f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout
     assert out.startswith("relaxmap_b200")
+
+
+def test_parse_size_query_then_fill(built_lib, tmp_path):
+    """rmx_parse_file's size query keeps its parse for the fill call that
+    follows (one parse for the pair); a file changed in between is parsed
+    again, so the fill returns the new contents."""
+    import ctypes as C
+    import os
+    from relaxmap_b200 import lib
+    L = lib()
+    p = tmp_path / "g.txt"
+    p.write_text("1 2 1.5\n2 3 2.5\n")
+    n, m, ns = C.c_int32(), C.c_int64(), C.c_int64()
+
+    def query():
+        assert L.rmx_parse_file(str(p).encode(), 1, C.byref(n), C.byref(m), C.byref(ns), None, None, None, None) == 0
+
+    def fill():
+        src, dst = (C.c_int32 * m.value)(), (C.c_int32 * m.value)()
+        w, nw = (C.c_double * m.value)(), (C.c_double * n.value)()
+        assert L.rmx_parse_file(str(p).encode(), 1, C.byref(n), C.byref(m), C.byref(ns), src, dst, w, nw) == 0
+        return list(src), list(dst), list(w)
+
+    query()
+    assert fill() == ([0, 1], [1, 2], [1.5, 2.5])
+    query()
+    p.write_text("1 2 7.5\n2 3 8.5\n")  # same sizes, new weights, a later modification time
+    st = os.stat(p)
+    os.utime(p, ns=(st.st_atime_ns, st.st_mtime_ns + 1_000_000_000))
+    assert fill() == ([0, 1], [1, 2], [7.5, 8.5])
+    assert fill() == ([0, 1], [1, 2], [7.5, 8.5])  # a fill without a size query parses on its own
