@@ -11,6 +11,7 @@
 #include <cstring>
 
 #include "rmx_graph.hpp"
+#include "rmx_io.hpp"
 
 using namespace rmx;
 
@@ -367,9 +368,20 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     if (n_edges >= (int64_t(1) << 31)) throw std::invalid_argument("more than 2^31-1 input edges");
     const bool repl = u && u->n_canon > 0;  // edges describe the canonical copies only
     const int32_t n_in = repl ? u->n_canon : n;
-    for (int64_t e = 0; e < n_edges; e++)
-        if ((uint32_t)src[e] >= (uint32_t)n_in || (uint32_t)dst[e] >= (uint32_t)n_in)
-            throw std::invalid_argument("edge endpoint outside 0..N-1");
+    {  // endpoints checked on host threads (one below 4M edges), before any device work
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const int T = (int)std::min<int64_t>(std::min(hw, 16u), std::max<int64_t>(1, n_edges >> 22));
+        std::vector<uint8_t> bad(std::max(T, 1), 0);
+        rmx::run_parallel(T, [&](int t) {
+            const int64_t e0 = n_edges * t / T, e1 = n_edges * (t + 1) / T;
+            bool b = false;
+            for (int64_t e = e0; e < e1; e++)
+                b |= ((uint32_t)src[e] >= (uint32_t)n_in) | ((uint32_t)dst[e] >= (uint32_t)n_in);
+            bad[t] = b;
+        });
+        for (uint8_t b : bad)
+            if (b) throw std::invalid_argument("edge endpoint outside 0..N-1");
+    }
     N = n;
     node_w.assign(n, 1.0);
     tot_w = (double)n;  // FileIO.cpp:229

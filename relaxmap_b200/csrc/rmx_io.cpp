@@ -242,36 +242,6 @@ Tok state_before_pos(const FileBytes &d, size_t lo, size_t pos, bool skip_commen
     return first;
 }
 
-// job(t) for t < T on T threads (inline for T == 1); the first exception a job
-// throws (or a failed thread start) is rethrown after every started thread
-// has joined.
-template <typename Job>
-void run_parallel(int T, Job &&job) {
-    if (T == 1) {
-        job(0);
-        return;
-    }
-    std::exception_ptr err;
-    std::mutex err_mu;
-    auto guarded = [&](int t) {
-        try {
-            job(t);
-        } catch (...) {
-            std::lock_guard<std::mutex> lk(err_mu);
-            if (!err) err = std::current_exception();
-        }
-    };
-    std::vector<std::thread> pool;
-    try {
-        for (int t = 0; t < T; t++) pool.emplace_back(guarded, t);
-    } catch (...) {
-        std::lock_guard<std::mutex> lk(err_mu);
-        if (!err) err = std::current_exception();
-    }
-    for (auto &th : pool) th.join();
-    if (err) std::rethrow_exception(err);
-}
-
 // Threads for a byte range: one below 1 MB, else `threads` (at most 64).
 int range_threads(size_t bytes, int threads) {
     return bytes < (size_t(1) << 20) ? 1 : std::max(1, std::min(threads, 64));

@@ -1,15 +1,48 @@
 // Host-side input parsing and output writing with the reference's rules.
 #pragma once
 #include <cstdint>
+#include <exception>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <utility>
 #include <vector>
 
 namespace rmx {
+
+// job(t) for t < T on T host threads (inline for T == 1); the first exception
+// a job throws (or a failed thread start) is rethrown after every started
+// thread has joined.
+template <typename Job>
+void run_parallel(int T, Job &&job) {
+    if (T <= 1) {
+        job(0);
+        return;
+    }
+    std::exception_ptr err;
+    std::mutex err_mu;
+    auto guarded = [&](int t) {
+        try {
+            job(t);
+        } catch (...) {
+            std::lock_guard<std::mutex> lk(err_mu);
+            if (!err) err = std::current_exception();
+        }
+    };
+    std::vector<std::thread> pool;
+    try {
+        for (int t = 0; t < T; t++) pool.emplace_back(guarded, t);
+    } catch (...) {
+        std::lock_guard<std::mutex> lk(err_mu);
+        if (!err) err = std::current_exception();
+    }
+    for (auto &th : pool) th.join();
+    if (err) std::rethrow_exception(err);
+}
 
 struct IoError : std::runtime_error {
     using std::runtime_error::runtime_error;

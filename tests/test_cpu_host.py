@@ -306,3 +306,21 @@ def test_parse_size_query_then_fill(built_lib, tmp_path):
     os.utime(p, ns=(st.st_atime_ns, st.st_mtime_ns + 1_000_000_000))
     assert fill() == ([0, 1], [1, 2], [7.5, 8.5])
     assert fill() == ([0, 1], [1, 2], [7.5, 8.5])  # a fill without a size query parses on its own
+
+
+@pytest.mark.parametrize("m", [10, 9_000_000])
+def test_graph_create_rejects_bad_endpoints(built_lib, m):
+    """rmx_graph_create checks every endpoint on the host (several threads for
+    large inputs) before any device work: one id outside 0..N-1, anywhere,
+    is RMX_ERR_INVALID (no device needed to see it)."""
+    from relaxmap_b200 import Graph, RmxError
+    n = 1000
+    src = (np.arange(m, dtype=np.int64) % n).astype(np.int32)
+    dst = ((np.arange(m, dtype=np.int64) + 1) % n).astype(np.int32)
+    for pos, arr, val in ((m - 1, dst, n), (m // 2, src, -1)):
+        a = arr.copy()
+        a[pos] = val
+        s, d = (a, dst) if arr is src else (src, a)
+        with pytest.raises(RmxError) as e:
+            Graph.from_edges(s, d, n=n)
+        assert e.value.status == 1 and "outside" in str(e.value)
