@@ -129,6 +129,7 @@ void Arena::destroy() {
 
 void release_device_cache() {
     std::lock_guard<std::mutex> lk(g_cache_mu);
+    if (g_cache.empty()) return;  // nothing held: no device call
     int cur = -1;
     RMX_CUDA(cudaGetDevice(&cur));
     cudaError_t first = cudaSuccess;

@@ -324,3 +324,10 @@ def test_graph_create_rejects_bad_endpoints(built_lib, m):
         with pytest.raises(RmxError) as e:
             Graph.from_edges(s, d, n=n)
         assert e.value.status == 1 and "outside" in str(e.value)
+
+
+def test_release_device_cache_without_cached_blocks(built_lib):
+    """With no cached arena blocks (as on a host without a device) the release
+    makes no device call and succeeds."""
+    from relaxmap_b200 import release_device_cache
+    release_device_cache()
