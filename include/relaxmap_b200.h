@@ -181,6 +181,14 @@ int32_t rmx_superstep_codelengths(const rmx_graph *g, double *bits, int32_t cap)
  * the partition part and code length L (nats). name keeps its leading '/'. */
 rmx_status rmx_write_outputs(rmx_graph *g, const int32_t *part, double L, const char *outdir, const char *name);
 
+/* Read a .clu file as rmx_write_outputs writes it (a "*Vertices N" line, then
+ * one label per node, module index + 1; CRLF or LF) into part_out[n_nodes]:
+ * the partition a run saved, to resume from (rmx_codelength, the adjoint,
+ * rmx_write_outputs). A vertex count other than n_nodes or a label that is
+ * not an integer in 1..n_nodes is RMX_ERR_FORMAT, an unreadable file
+ * RMX_ERR_IO. The reference writes .clu files but never reads them. */
+rmx_status rmx_read_clu(const char *path, int32_t n_nodes, int32_t *part_out);
+
 /* ---- Batched multi-graph x multi-attempt optimisation.
  * The reference optimises one network per run and its attempts one after
  * another (OmpRelaxmap.cpp:181-219); a batch optimises many graphs, each

@@ -27,7 +27,7 @@ EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_creat
            "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main",
            "rmx_steady_state_noalloc", "rmx_noalloc_last_error", "rmx_adjoint_forward", "rmx_adjoint_backward",
            "rmx_batch_create", "rmx_batch_set_wave", "rmx_batch_optimize", "rmx_batch_info", "rmx_batch_destroy",
-           "rmx_reset_flow", "rmx_release_device_cache", "rmx_get_tuning", "rmx_set_tuning"]
+           "rmx_reset_flow", "rmx_release_device_cache", "rmx_get_tuning", "rmx_set_tuning", "rmx_read_clu"]
 
 
 class RmxError(RuntimeError):
@@ -378,6 +378,13 @@ def set_tuning(**values) -> dict:
     t = Tuning(*[cur[f] for f in TUNING_FIELDS])
     _check(lib().rmx_set_tuning(C.byref(t)))
     return cur
+
+
+def read_clu(path, n: int) -> np.ndarray:
+    """The partition saved in a .clu file (rmx_read_clu): module index per node."""
+    part = np.zeros(max(int(n), 1), dtype=np.int32)
+    _check(lib().rmx_read_clu(str(path).encode(), C.c_int32(n), _p(part)))
+    return part[:n]
 
 
 def release_device_cache():

@@ -362,6 +362,16 @@ rmx_status rmx_write_outputs(rmx_graph *g, const int32_t *part, double L, const 
     });
 }
 
+rmx_status rmx_read_clu(const char *path, int32_t n_nodes, int32_t *part_out) {
+    return guard([&] {
+        need(path, "path");
+        need(part_out, "part_out");
+        if (n_nodes <= 0) throw std::invalid_argument("n_nodes must be positive");
+        const std::vector<int32_t> part = rmx::read_clu(path, n_nodes);
+        std::memcpy(part_out, part.data(), sizeof(int32_t) * part.size());
+    });
+}
+
 rmx_status rmx_set_profiling(rmx_graph *g, int32_t on) {
     return guard([&] {
         need(g, "graph");

@@ -614,4 +614,50 @@ void write_clu(const std::string &file, const std::vector<int32_t> &part) {
     fclose(f);
 }
 
+std::vector<int32_t> read_clu(const std::string &file, int32_t n) {
+    FileBytes d = FileBytes::read(file);
+    const char *p = d.data(), *end = d.data() + d.size();
+    // the next token on the current line, or an empty one at its end
+    auto token = [&](const char *&b, const char *&e) {
+        while (p < end && (*p == ' ' || *p == '\t' || *p == '\r')) p++;
+        b = p;
+        while (p < end && !is_ws(*p)) p++;
+        e = p;
+    };
+    auto next_line = [&] {
+        while (p < end && *p != '\n') p++;
+        if (p < end) p++;
+    };
+    auto integer = [&](const char *b, const char *e, long long &v) {
+        if (b == e) return false;
+        v = 0;
+        for (const char *c = b; c < e; c++) {
+            if (*c < '0' || *c > '9' || v > INT32_MAX) return false;
+            v = v * 10 + (*c - '0');
+        }
+        return true;
+    };
+    const char *b, *e;
+    token(b, e);
+    const std::string head(b, e);
+    if (head != "*Vertices" && head != "*vertices" && head != "*VERTICES")
+        throw FormatError(file + ": no *Vertices line");
+    token(b, e);
+    long long count = 0;
+    if (!integer(b, e, count) || count != n)
+        throw FormatError(file + ": " + std::string(b, e) + " vertices, the graph has " + std::to_string(n));
+    next_line();
+    std::vector<int32_t> part((size_t)n);
+    for (int32_t i = 0; i < n; i++) {
+        token(b, e);
+        long long label = 0;
+        if (!integer(b, e, label) || label < 1 || label > n)
+            throw FormatError(file + ": label of node " + std::to_string(i + 1) + " is not an integer in 1.." +
+                              std::to_string(n));
+        part[(size_t)i] = (int32_t)(label - 1);
+        next_line();
+    }
+    return part;
+}
+
 }  // namespace rmx

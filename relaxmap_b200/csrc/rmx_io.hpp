@@ -100,5 +100,10 @@ ParsedGraph parse_file(const std::string &path, int threads);
 void write_tree(const std::string &file, double L_bits, int32_t n_modules, const std::vector<int32_t> &part,
                 const std::vector<double> &size, const std::vector<std::string> &names);
 void write_clu(const std::string &file, const std::vector<int32_t> &part);
+// A .clu file as write_clu writes it ("*Vertices N", then N labels = module
+// index + 1; CRLF or LF): the module index of each of the n nodes. A vertex
+// count other than n, a label that is not an integer in 1..n, or a missing
+// label is a FormatError; an unreadable file an IoError.
+std::vector<int32_t> read_clu(const std::string &file, int32_t n);
 
 }  // namespace rmx

@@ -331,3 +331,40 @@ def test_release_device_cache_without_cached_blocks(built_lib):
     makes no device call and succeeds."""
     from relaxmap_b200 import release_device_cache
     release_device_cache()
+
+
+def test_read_clu(built_lib, tmp_path):
+    """rmx_read_clu reads what the .clu writer writes (CRLF, module index + 1
+    per node) and LF files; wrong vertex counts and labels outside 1..N are
+    RMX_ERR_FORMAT, a missing file RMX_ERR_IO."""
+    from relaxmap_b200 import RmxError, read_clu
+    part = np.array([3, 0, 0, 4, 3, 1], dtype=np.int32)
+    p = tmp_path / "a.clu"
+    p.write_bytes(b"*Vertices 6\r\n" + b"".join(b"%d\r\n" % (m + 1) for m in part))
+    np.testing.assert_array_equal(read_clu(p, 6), part)
+    p.write_bytes(b"*Vertices 6\n" + b"".join(b"%d\n" % (m + 1) for m in part))  # LF, no final newline issue
+    np.testing.assert_array_equal(read_clu(p, 6), part)
+    cases = {b"*Vertices 5\r\n1\r\n1\r\n1\r\n1\r\n1\r\n": 3,                  # 5 vertices, graph has 6
+             b"*Vertices 6\r\n1\r\n2\r\n0\r\n1\r\n1\r\n1\r\n": 3,              # label 0
+             b"*Vertices 6\r\n1\r\n2\r\n7\r\n1\r\n1\r\n1\r\n": 3,              # label above N
+             b"*Vertices 6\r\n1\r\n2\r\nx\r\n1\r\n1\r\n1\r\n": 3,              # not an integer
+             b"*Vertices 6\r\n1\r\n2\r\n3\r\n": 3,                             # labels missing
+             b"*Network 6\r\n": 3}
+    for body, status in cases.items():
+        p.write_bytes(body)
+        with pytest.raises(RmxError) as e:
+            read_clu(p, 6)
+        assert e.value.status == status, body
+    with pytest.raises(RmxError) as e:
+        read_clu(tmp_path / "none.clu", 6)
+    assert e.value.status == 2
+
+
+def test_read_clu_reference_files(built_lib):
+    """The .clu files the reference wrote read back label by label."""
+    from relaxmap_b200 import read_clu
+    files = sorted(GOLDEN.glob("*.ref.clu"))
+    assert files
+    for f in files:
+        labels = [int(x) for x in f.read_bytes().split(b"\r\n")[1:] if x]
+        np.testing.assert_array_equal(read_clu(f, len(labels)), np.array(labels) - 1)

@@ -88,3 +88,16 @@ def test_cli_normal_mode_selflinks_and_attempts(built_lib, tmp_path):
     L = float(done[-1].split("=")[1].split()[0])
     assert L <= 7.98793 * 1.005  # within the quality bar of the reference median on this graph
     assert (out / "loops.tree").exists() and (out / "loops.clu").exists()
+
+
+def test_clu_round_trip(built_lib, tmp_path):
+    """A partition written by rmx_write_outputs and read back with
+    rmx_read_clu is the same partition with the same code length (resuming
+    from a saved run)."""
+    from relaxmap_b200 import Graph, read_clu as lib_read_clu
+    with Graph.from_file(GOLDEN / "directNet_1k_sm_mu_03.txt") as G:
+        r = G.optimize(seed=2)
+        G.write_outputs(r["part"], r["L"], str(tmp_path), "/run")
+        back = lib_read_clu(tmp_path / "run.clu", G.n)
+        np.testing.assert_array_equal(back, r["part"])
+        assert abs(G.codelength(back) - r["L"]) <= 1e-10 * r["L"]
