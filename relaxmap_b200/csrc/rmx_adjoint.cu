@@ -428,6 +428,7 @@ using namespace rmx;
 // node + 8 B per link, released before returning.
 void rmx_graph::adjoint(const int32_t *part_host, double tau, double *L_out, double *p_out, double *grad_out,
                         double *dL_dtau, int *solve_iters) {
+    const NvtxRange range(grad_out || dL_dtau ? "rmx adjoint backward" : "rmx adjoint forward");
     if (!(tau > 0.0 && tau < 1.0)) throw std::invalid_argument("tau must lie in (0, 1)");
     for (int32_t v = 0; v < N; v++)
         if ((uint32_t)part_host[v] >= (uint32_t)N) throw std::invalid_argument("module id outside 0..N-1");

@@ -59,6 +59,7 @@ void rmx_batch::optimize(const rmx_opts &o, int32_t *part_out, double *L_out, in
     last_instances = 0;
     int32_t g0 = 0;
     while (g0 < G) {
+        const rmx::NvtxRange range("rmx batch wave");
         // the next wave: whole graphs (all their attempts) up to the link budget
         int32_t g1 = g0;
         int64_t links = 0, nodes = 0;

@@ -1,6 +1,7 @@
 // Shared device definitions for the B200 map-equation engine.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <cstdio>
@@ -59,6 +60,16 @@ __device__ __forceinline__ void atomic_add_fx(fx_t *a, fx_t v) {
 
 // Grid sizing: a multiple of the SM count (148 on B200).
 int num_sms();
+
+// An NVTX range over the object's lifetime: host-side phase markers (graph
+// build, flow, sweeps, coarsening, coarse-tune, adjoint, batch waves) for a
+// profiler's timeline; without a profiler attached the calls return at once.
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 struct CudaError : std::runtime_error {
     cudaError_t code;

@@ -363,6 +363,7 @@ static void replicate_csr(int32_t K, const int64_t *noff, const int64_t *cbase, 
 
 void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, int64_t n_edges, int32_t n,
                        const double *node_weights, const UnionSpec *u) {
+    const NvtxRange range("rmx graph build");
     if (n <= 0) throw std::invalid_argument("graph needs at least one node");
     if (n_edges < 0 || (n_edges > 0 && (!src || !dst))) throw std::invalid_argument("edge arrays missing");
     if (n_edges >= (int64_t(1) << 31)) throw std::invalid_argument("more than 2^31-1 input edges");
@@ -611,6 +612,7 @@ void rmx_graph::ensure_hub_table(int64_t maxdeg) {
 
 void rmx_graph::initiate() {
     if (initiated) return;
+    const NvtxRange range("rmx flow");
     timers.begin(kTimerOther, stream);
     // the CSC weights are normalised in place, once; the CSR flows are rebuilt from the raw weights
     normalise(N, out_off, out_w0, out_f, in_off, in_src, in_w, in_w, dangling, scratch, stream, !cols_normalised);
@@ -783,6 +785,7 @@ static bool any_set(const std::vector<uint8_t> &m) {
 // these rules on its own code length; an instance that stops keeps its
 // modules while the others continue.
 void rmx_graph::stage_sweeps(Level &lv, bool allow_new, std::vector<double> &L, const std::vector<uint8_t> &act) {
+    const NvtxRange range(&lv == &node_lv ? "rmx sweeps: nodes" : "rmx sweeps: super-nodes");
     const bool prior = opt.prior != 0;
     const double vthresh = prior ? -opt.vthresh : 0.0;  // OmpRelaxmap.cpp:66, Module.cpp:1490 vs :1127
     int64_t n_active = lv.n;
@@ -819,6 +822,7 @@ void rmx_graph::project_sn_to_nodes() {
 // current super-node links (a few times fewer than node links) with the same
 // result as from the node links.
 void rmx_graph::convert_to_supernodes(bool from_sn) {
+    const NvtxRange range("rmx coarsen");
     timers.begin(kTimerCoarsen, stream);
     count_units(node_lv, mods, stream);  // nodes per module
     size_t mk = scratch.mark();
@@ -862,6 +866,7 @@ void rmx_graph::convert_to_supernodes(bool from_sn) {
 // the resulting sub-modules become the super-nodes of the next superstep,
 // starting in their parent module.
 void rmx_graph::generate_sub_modules() {
+    const NvtxRange range("rmx coarse-tune");
     timers.begin(kTimerCoarsen, stream);
     count_units(node_lv, mods, stream);  // nodes per parent module
     size_t mk = scratch.mark();
