@@ -112,3 +112,22 @@ def test_batched_results_combine_over_two_ranks():
     for _ in range(world):
         rank, v = q.get(timeout=10)
         assert v == [1.5 * g for g in range(10)]  # every graph once, from whichever rank ran it
+
+
+def test_bench_edge_list_file_reads_back(tmp_path):
+    """bench.py --with-io writes the workload graph as an edge list; the
+    loader reads back the same links with the weights to 6 significant
+    digits."""
+    import numpy as np
+    import bench
+    from relaxmap_b200 import parse_file, synth
+    g = synth.config_small(seed=3)
+    g.w = np.random.default_rng(1).uniform(1, 10, g.m)
+    p = tmp_path / "g.txt"
+    size = bench.write_edge_list(p, g, chunk=1000)
+    assert size == p.stat().st_size
+    d = parse_file(p, threads=2)
+    assert d["n"] == g.n
+    np.testing.assert_array_equal(d["src"], g.src)
+    np.testing.assert_array_equal(d["dst"], g.dst)
+    np.testing.assert_allclose(d["w"], g.w, rtol=5e-6)
