@@ -20,6 +20,7 @@
 
 #include "rmx_batch.hpp"
 #include "rmx_graph.hpp"
+#include "rmx_io.hpp"
 
 void rmx_batch::create(int32_t g, const int32_t *n_nodes, const int64_t *n_edges, const int32_t *s, const int32_t *d,
                        const double *wt, const double *node_weights) {
@@ -80,27 +81,30 @@ void rmx_batch::optimize(const rmx_opts &o, int32_t *part_out, double *L_out, in
         std::vector<int32_t> us(ec), ud(ec), node_inst(nodes), canon(K);
         std::vector<double> uw(has_w ? ec : 0), unw(has_nw ? nodes : 0);
         std::vector<int64_t> inoff(K + 1, 0);
-        for (int32_t g = g0; g < g1; g++) {
-            const int32_t cb = (int32_t)(noff[g] - noff[g0]);
-            for (int64_t e = eoff[g]; e < eoff[g + 1]; e++) {
-                us[e - eoff[g0]] = src[e] + cb;
-                ud[e - eoff[g0]] = dst[e] + cb;
+        // graphs packed on host threads: graph g's canonical links fill
+        // [eoff[g], eoff[g+1]) - eoff[g0], its copy a (instance (g-g0)*A + a)
+        // the nodes from A * (noff[g] - noff[g0]) + a * n[g]
+        const int T = (int)std::min<int64_t>(16, std::max<int64_t>(1, (ec + nodes) >> 21));
+        rmx::run_parallel(T, [&](int t) {
+            for (int32_t g = g0 + t; g < g1; g += T) {
+                const int32_t cb = (int32_t)(noff[g] - noff[g0]);
+                for (int64_t e = eoff[g]; e < eoff[g + 1]; e++) {
+                    us[e - eoff[g0]] = src[e] + cb;
+                    ud[e - eoff[g0]] = dst[e] + cb;
+                }
+                if (has_w) std::copy(w.begin() + eoff[g], w.begin() + eoff[g + 1], uw.begin() + (eoff[g] - eoff[g0]));
+                const int32_t first = (g - g0) * A;
+                for (int32_t a = 0; a < A; a++) {
+                    const int32_t k = first + a;
+                    const int64_t vb = (int64_t)A * cb + (int64_t)a * n[g];
+                    canon[k] = first;
+                    inoff[k] = vb;
+                    std::fill(node_inst.begin() + vb, node_inst.begin() + vb + n[g], k);
+                    if (has_nw) std::copy(nw.begin() + noff[g], nw.begin() + noff[g + 1], unw.begin() + vb);
+                }
             }
-        }
-        if (has_w) std::copy(w.begin() + eoff[g0], w.begin() + eoff[g1], uw.begin());
-        int64_t vb = 0;
-        int32_t k = 0;
-        for (int32_t g = g0; g < g1; g++) {
-            const int32_t first = k;
-            for (int32_t a = 0; a < A; a++, k++) {
-                canon[k] = first;
-                inoff[k] = vb;
-                std::fill(node_inst.begin() + vb, node_inst.begin() + vb + n[g], k);
-                if (has_nw) std::copy(nw.begin() + noff[g], nw.begin() + noff[g + 1], unw.begin() + vb);
-                vb += n[g];
-            }
-        }
-        inoff[K] = vb;
+        });
+        inoff[K] = nodes;
         UnionSpec spec{K, node_inst.data(), inoff.data(), canon.data(), (int32_t)nc, links};
         std::unique_ptr<rmx_graph> U(new rmx_graph());
         U->create(us.data(), ud.data(), has_w ? uw.data() : nullptr, ec, (int32_t)nodes,
@@ -114,7 +118,7 @@ void rmx_batch::optimize(const rmx_opts &o, int32_t *part_out, double *L_out, in
         last_instances += K;
         // best attempt per graph, modules renumbered by first appearance
         std::vector<int32_t> label;
-        k = 0;
+        int32_t k = 0;
         for (int32_t g = g0; g < g1; g++, k += A) {
             int32_t best = 0;
             for (int32_t a = 1; a < A; a++)
