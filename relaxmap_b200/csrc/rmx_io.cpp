@@ -119,7 +119,8 @@ double c_atof(const Tok &t) {
 
 // The bytes of a file: a read-only mapping of a regular file (the parser
 // threads fault its pages in themselves), else what reads from the stream
-// returned (pipes, devices).
+// returned (pipes, devices). As with any mapped read, a file that another
+// process truncates while it is parsed raises SIGBUS.
 class FileBytes {
   public:
     FileBytes() = default;

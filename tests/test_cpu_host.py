@@ -368,3 +368,33 @@ def test_read_clu_reference_files(built_lib):
     for f in files:
         labels = [int(x) for x in f.read_bytes().split(b"\r\n")[1:] if x]
         np.testing.assert_array_equal(read_clu(f, len(labels)), np.array(labels) - 1)
+
+
+def test_degenerate_files_match_the_oracle(built_lib, oracle_mod, tmp_path):
+    """Empty and comment-only edge lists, blank lines only (the stream re-reads
+    "" and adds node 0), no final newline (one range and many), and a Pajek
+    file without links: the same nodes and links as the oracle."""
+    from relaxmap_b200 import parse_file
+    O = oracle_mod
+    cases = {"empty.txt": b"", "comments.txt": b"# a\n# b\n", "blank.txt": b"\n\n\n",
+             "nofinal.txt": b"1 2 0.5\n2 3", "crlf_nofinal.txt": b"1 2\r\n3 1 2.5\r",
+             "noarcs.net": b"*Vertices 3\n1 \"a\"\n2 \"b\"\n3 \"c\"\n*Arcs\n",
+             "noarcs_nofinal.net": b"*Vertices 2\n1\n2\n*Edges"}
+    rng = np.random.default_rng(4)
+    big = "\n".join(f"{a} {b} {x!r}" for a, b, x in zip(rng.integers(0, 900, 90000).tolist(),
+                                                       rng.integers(0, 900, 90000).tolist(),
+                                                       rng.uniform(0, 3, 90000).tolist()))
+    cases["big_nofinal.txt"] = big.encode()  # > 1 MB: the multi-range parse, last line unterminated
+    for name, body in cases.items():
+        p = tmp_path / name
+        p.write_bytes(body)
+        ld = O.parse_pajek(p) if name.endswith(".net") else O.parse_txt(p)
+        for t in (1, 7):
+            d = parse_file(p, threads=t)
+            assert d["n"] == ld.n, name
+            acc = {}
+            for a, b, x in zip(d["src"].tolist(), d["dst"].tolist(), d["w"].tolist()):
+                acc[(a, b)] = acc.get((a, b), 0.0) + x
+            ref = {(a, b): x for a, b, x in zip(ld.src.tolist(), ld.dst.tolist(), ld.w.tolist()) if a != b}
+            assert acc == ref, name
+    assert len(big) > (1 << 20)
