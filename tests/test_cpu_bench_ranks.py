@@ -131,3 +131,8 @@ def test_bench_edge_list_file_reads_back(tmp_path):
     np.testing.assert_array_equal(d["src"], g.src)
     np.testing.assert_array_equal(d["dst"], g.dst)
     np.testing.assert_allclose(d["w"], g.w, rtol=5e-6)
+    g.w = None  # unweighted: two columns, every weight read as 1
+    bench.write_edge_list(p, g, chunk=777)
+    d = parse_file(p, threads=1)
+    np.testing.assert_array_equal(d["src"], g.src)
+    np.testing.assert_array_equal(d["w"], np.ones(g.m))
