@@ -1,19 +1,25 @@
 """Benchmark: edges/s per full optimiser run on one B200 (or N replicas).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload mid|small|rmat20|rmat24]
+                    [--workload rmat24|mid|small|rmat<scale>|batched|adjoint]
+
+Default workload: R-MAT scale 24 (16,777,216 nodes, edge factor 16,
+(0.57, 0.19, 0.19, 0.05), self-loops and duplicates removed, unweighted),
+drawn on the GPU from seed 42; the largest configuration that fits one B200.
 
 One step = one full run of the map-equation optimiser (flow power iteration,
 all supersteps, final partition) on the workload graph:
-  value  graph resident in HBM (built once), device time of K runs (CUDA
-         events on the engine's stream); edges/s = input links / time per run
+  value  graph resident in HBM (CSR/CSC built once, outside the timed region),
+         device time of K runs (CUDA events on the engine's stream); each run
+         recomputes the flow; edges/s = input links / time per run
   e2e    the same through the C ABI from pinned HOST buffers every step:
          rmx_graph_create (host->device copy, device CSR/CSC build),
          rmx_optimize (partition copied back), rmx_graph_destroy
 The single-graph optimiser does not shard: with N GPUs every rank runs its own
 replica (no collective); value = all ranks' links / the slowest rank's time.
 --impl reference times the reference (compiled from its own sources, all host
-threads) on a bounded sample of the same workload family.
+threads) on a bounded sample of the same workload family (R-MAT scale 18 for
+the R-MAT workloads, 200,000 nodes for mid): not the same graph as ours.
 """
 from __future__ import annotations
 
@@ -61,17 +67,44 @@ def workload(name: str, nodes: int | None = None):
 
 
 def reference_sample(name: str):
-    """The bounded CPU sample: the same generator and distributions at 1/5 of
-    the nodes (the reference's std::map build and OpenMP sweeps on the full
-    1M-node graph take minutes per run)."""
+    """The bounded CPU sample of the workload family (the reference's
+    std::map build and OpenMP sweeps take hours on the full R-MAT scale-24
+    graph and minutes on the 1M-node mid graph): R-MAT scale 18 with the same
+    parameters, or the mid distributions at 200,000 nodes."""
     from relaxmap_b200 import synth
     if name == "mid":
         g = synth.config_mid(seed=42, n=200_000)
-        return g, "planted partition N=200,000 with the mid distributions (1/5 of the nodes), seed 1"
+        return g, "planted partition N=200,000 with the mid distributions (1/5 of the nodes)"
     if name == "small":
-        return synth.config_small(seed=42), "the full small graph, seed 1"
-    g = synth.rmat(16, 16, seed=42)
-    return g, "R-MAT scale 16 with the same parameters"
+        return synth.config_small(seed=42), "the full small graph"
+    g = synth.rmat(18, 16, seed=42)
+    return g, "R-MAT scale 18, edge factor 16, (0.57,0.19,0.19,0.05), self-loops/duplicates removed (numpy, seed 42)"
+
+
+# The reference's 8-seed final code lengths (bits) committed by
+# tests/golden/make_golden.py: the full mid graph, and the R-MAT family's CPU sample.
+QUALITY_GOLDEN = ROOT / "tests" / "golden" / "quality.ref.npz"
+
+
+def reference_quality(case: str):
+    import numpy as np
+    if not QUALITY_GOLDEN.exists():
+        return None
+    with np.load(QUALITY_GOLDEN) as z:
+        return [float(x) for x in z[case]] if case in z.files else None
+
+
+def sample_quality(G_cls, sg, case: str, seeds: int = 8) -> dict | None:
+    """Our median code length over seeds 1..8 on a graph the reference was run
+    on 8 times (its golden median), and the relative gap."""
+    ref = reference_quality(case)
+    if ref is None:
+        return None
+    with G_cls.from_edges(sg.src, sg.dst, sg.w, n=sg.n) as G:
+        ours = [G.optimize(seed=k)["L_bits"] for k in range(1, seeds + 1)]
+    rm = statistics.median(ref)
+    om = statistics.median(ours)
+    return {"ref_median_bits": rm, "gpu_median_bits": om, "gap": (om - rm) / rm, "seeds": seeds}
 
 
 def run_reference(g, threads: int, seed: int = 1) -> dict:
@@ -163,19 +196,10 @@ def peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def ncu_traffic():
-    """DRAM bytes per launch of the move-evaluation kernel from the committed
-    ncu summary (profiles/), scaled as that summary states."""
-    p = ROOT / "profiles" / "move_eval_mid400k.md"
-    if not p.exists():
-        return None
-    for line in p.read_text().splitlines():
-        if line.startswith("traffic_bytes_per_eval_link:"):
-            try:
-                return float(line.split(":", 1)[1])
-            except ValueError:
-                return None
-    return None
+# DRAM bytes per evaluated link of the move evaluation, from one ncu capture
+# on the benched R-MAT family (the command and counters are in profiles/).
+# None where no capture of that workload exists.
+EVAL_TRAFFIC_PER_LINK = {}
 
 
 def profile_run(g, desc: str):
@@ -222,7 +246,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="mid")
+    ap.add_argument("--workload", default="rmat24")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--with-io", action="store_true",
                     help="also time the drop-in path with file IO: edge-list file -> load (all host cores) -> "
@@ -318,18 +342,23 @@ def main():
         pg.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    build_s = close_s = 0.0
+    build_s = opt_s = close_s = dev_s = 0.0
     for k in range(e2e_steps):
         tb = time.perf_counter()
         Ge = Graph.from_host_ptrs(src.data_ptr(), dst.data_ptr(), w.data_ptr() if w is not None else 0, E, g.n)
-        build_s += time.perf_counter() - tb
+        to = time.perf_counter()
+        build_s += to - tb
         Ge.optimize(seed=1 + k)  # the partition is copied back to host memory inside
         tc = time.perf_counter()
+        opt_s += tc - to
+        dev_s += Ge.profile()["total_ms"] / 1e3  # device time of that run (flow + supersteps)
         Ge.close()
         close_s += time.perf_counter() - tc
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     build_s /= e2e_steps
+    opt_s /= e2e_steps
     close_s /= e2e_steps
+    dev_s /= e2e_steps
     e2e_value = job_throughput(world, E, slowest_over_ranks([e2e_s], pg, "cuda")[0])
 
     # ---- with file IO, as the reference's command line runs: file in, .tree/.clu out
@@ -351,11 +380,26 @@ def main():
                    "path": "edge-list file -> rmx_graph_load_file (all host cores) -> rmx_optimize -> "
                            "rmx_write_outputs (.tree/.clu)", "note": "weights written to 6 significant digits"}
 
+    # ---- code length against the reference's 8-seed median: the same graph
+    # (mid), or, where the reference cannot run the full graph, its CPU sample
+    quality = {"L_bits_median": statistics.median(L_bits), "n_modules": results[0]["n_modules"],
+               "seeds": len(L_bits)}
+    sg_q, rdesc = reference_sample(args.workload)
+    if args.workload == "mid" and (args.nodes or 1_000_000) == 1_000_000:
+        ref = reference_quality("planted1m_mid")
+        if ref is not None:
+            rm = statistics.median(ref)
+            quality.update(ref_median_bits=rm, gap=(quality["L_bits_median"] - rm) / rm)
+    elif args.workload.startswith("rmat") and rank == 0:
+        quality["on_reference_sample"] = sample_quality(Graph, sg_q, "rmat18")
+        quality["note"] = ("the reference cannot run the full graph within a run's time (hours on the host): its "
+                           "8-seed median is compared on the CPU sample, R-MAT scale 18")
+
     # ---- roofline of the dominant kernel class (move evaluation)
     pk = peaks()
     ev = prof["eval"]
     achieved = ev["bytes"] / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
-    per_link = ncu_traffic()
+    per_link = EVAL_TRAFFIC_PER_LINK.get(args.workload)
     traffic = None
     if per_link is not None and ev["launches"] > 0:
         traffic = per_link * prof["links_evaluated"] / ev["launches"]
@@ -369,11 +413,18 @@ def main():
         "config": {"workload": desc, "nodes": g.n, "links": E, "solver": "seed 1..K, threshold 1e-3, vThresh 0.0, "
                    "maxIter 10, prior", "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": f"inputs larger than L2 (resident graph ~{(E * 104 + g.n * 420) / 1e9:.1f} GB)",
+                   "timed_region": "value: the flow (power iteration, edge flows) and every superstep on the "
+                                   "resident graph; the device CSR/CSC build (part of the reference's w/o-IO "
+                                   "region, OmpRelaxmap.cpp:103-162) is outside it and inside e2e",
+                   "reference_arm": {"same_config": False, "sample": rdesc},
                    "launch_tuning": get_tuning()},
-        "quality": {"L_bits_median": statistics.median(L_bits), "n_modules": results[0]["n_modules"]},
+        "quality": quality,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(E * (8 + (8 if w is not None else 0))),
-                "d2h_bytes_per_step": int(4 * g.n + 8), "graph_build_ms": build_s * 1e3,
-                "graph_close_ms": close_s * 1e3},
+                "d2h_bytes_per_step": int(4 * g.n + 8),
+                "split_ms": {"graph_create": build_s * 1e3, "optimize_wall": opt_s * 1e3,
+                             "optimize_device": dev_s * 1e3, "graph_destroy": close_s * 1e3},
+                "note": "a fresh handle per step: graph_create copies the host arrays in and builds the CSR/CSC; "
+                        "optimize_wall includes the flow, the run and the partition copied back"},
         "roofline": {"kernel": "move evaluation (warp/block/hub bins)", "bound": "hbm", "achieved": achieved,
                      "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                      "peak_source": pk["source"], "traffic": traffic,
@@ -387,7 +438,7 @@ def main():
         line["with_io"] = with_io
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            sg, sdesc = reference_sample(args.workload)
+            sg, sdesc = sg_q, rdesc
             r = run_reference(sg, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": sg.m / r["seconds"], "unit": UNIT, "cores": os.cpu_count(),
                                     "kind": "reference", "sample": sdesc + f" ({sg.m} links, {r['seconds']:.2f} s, "
@@ -622,13 +673,16 @@ def bench_reference(args, world):
         return
     s = sum(secs) / len(secs)
     v = sg.m / s
-    _, desc = (None, "")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, seed 42)",
-        "config": {"workload": sdesc, "nodes": sg.n, "links": sg.m, "solver": "threshold 1e-3, vThresh 0.0, "
-                   "maxIter 10, prior", "parallelism": f"{threads} host threads"},
+        "config": {"workload": sdesc, "nodes": sg.n, "links": sg.m, "solver": "seed 1..K, threshold 1e-3, "
+                   "vThresh 0.0, maxIter 10, prior", "parallelism": f"{threads} host threads",
+                   "same_config": False,
+                   "note": f"a bounded CPU sample of the {args.workload} workload family (the full graph takes "
+                           "hours on the host); timed over the reference's w/o-IO region: edge preparation, "
+                           "initiate and every superstep"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sdesc},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))

@@ -58,7 +58,10 @@ typedef struct {
 typedef struct {
     int64_t launches;
     double ms;          /* summed event time */
-    double bytes;       /* algorithmic bytes moved (compulsory traffic model) */
+    double bytes;       /* algorithmic bytes moved (compulsory traffic model): move evaluation,
+                           per launch group, 16 B per link + 40 B per unit + 40 B per module
+                           (at most one per candidate, at most the non-empty modules); the
+                           adjoint solve, per sweep, 20 B per link + 65 B per node */
 } rmx_kernel_stat;
 
 enum {
@@ -83,6 +86,7 @@ typedef struct {
     int64_t units_evaluated; /* units evaluated since profiling was enabled */
     int64_t adjoint_iters;   /* sweeps of the transposed solve since profiling was enabled */
     double level_ms[3];      /* device time of the sweep loops on nodes, super-nodes, coarse-tune sub-problems */
+    int64_t candidates_evaluated; /* (unit, candidate module) pairs evaluated since profiling was enabled */
 } rmx_profile;
 
 const char *rmx_last_error(void);
@@ -161,9 +165,42 @@ rmx_status rmx_coarsen(rmx_graph *g, const int32_t *part, int32_t *n_sn, int64_t
  * an empty module; best_mod[u] is the module with the most negative change
  * (ties to the lowest id), -2 for a new module, -1 when none is negative;
  * best_delta[u] is that change in nats. Module statistics are formed from
- * part. No module or partition state of the handle is modified. */
+ * part. The handle's partition state is overwritten (the next rmx_optimize
+ * starts from singletons as always). */
 rmx_status rmx_evaluate_moves(rmx_graph *g, const int32_t *part, const uint8_t *allow_new, int32_t *best_mod,
                               double *best_delta);
+
+/* convertModulesToSuperNodes (Module.cpp:3008-3077) as the optimiser itself
+ * performs it (rmx_coarsen above is a separate sort-based path): module
+ * statistics from the nodes of part, super-nodes numbered by ascending module
+ * id (sn_of_mod[N], -1 for unused ids), and the super-node links aggregated by
+ * the engine's hash kernels into fixed-point flow sums. With part2 non-NULL a
+ * second conversion follows, as after a super-node stage (the super-node loop
+ * of OmpRelaxmap.cpp:379-411 calling convertModulesToSuperNodes again): every
+ * first-level module m joins module part2[m] (part2 has N entries) and the
+ * new super-nodes aggregate the first level's links; the outputs then
+ * describe that second level, sn_of_mod indexed by part2's module ids.
+ * Flows are fixed point, value * 2^62 rounded to nearest, each link sum
+ * exact: out_fx/in_fx[E] per link, sn_stat[4 * n_sn] the super-node's
+ * {flow, teleport weight, dangling flow, out-flow} (SuperNode(Module, int),
+ * Node.cpp:76-106). Rows of the CSR and CSC come in no particular order.
+ * Buffers are sized N (+1 for offsets) and E by the caller; outputs may be
+ * NULL individually. The handle's partition state is overwritten. */
+rmx_status rmx_coarsen_engine(rmx_graph *g, const int32_t *part, const int32_t *part2, int32_t *n_sn,
+                              int64_t *n_sn_links, int32_t *sn_of_mod, int64_t *out_off, int32_t *out_dst,
+                              int64_t *out_fx, int64_t *in_off, int32_t *in_src, int64_t *in_fx, int64_t *sn_stat);
+
+/* The move decision of every super-node against a fixed snapshot (the
+ * evaluation phase of Network::parallelMoveSuperNodes, Module.cpp:2198-2313,
+ * and prioritize_parallelMoveSPnodes, :2555-2670): the super-node level of
+ * part is built as rmx_coarsen_engine builds it, super-node s is placed in
+ * module sn_part[s] (n_sn entries, ids in [0,N)), module statistics are
+ * formed from the super-nodes, and every super-node is evaluated as
+ * rmx_evaluate_moves evaluates nodes (allow_new[n_sn] may be NULL). n_sn must
+ * equal the number of distinct modules of part. The handle's partition state
+ * is overwritten. */
+rmx_status rmx_evaluate_sn_moves(rmx_graph *g, const int32_t *part, int32_t n_sn, const int32_t *sn_part,
+                                 const uint8_t *allow_new, int32_t *best_mod, double *best_delta);
 
 /* The whole optimiser (OmpRelaxmap.cpp:155-233): initiate, superstep 1
  * (fine-tune), then alternating fine/coarse supersteps until a superstep gains
@@ -241,20 +278,31 @@ rmx_status rmx_adjoint_backward(rmx_graph *g, const int32_t *part, double tau, d
                                 double *L);
 
 /* Launch shape of move evaluation, process-wide: the grid cap of each degree
- * bin in blocks per SM. Results do not depend on these values (every bin's
- * kernel loops over its units by grid stride and module statistics are exact
- * integer sums), only the time does. rmx_set_tuning takes effect at the next
- * launch; sweep pipelines captured as CUDA graphs under other values are
- * captured again. Each value must lie in [1, 64] (else RMX_ERR_INVALID);
- * `reserved` is ignored. The Python module relaxmap_b200.autotune picks the
- * values by timing. No reference counterpart. */
+ * bin in blocks per SM, and the degree bounds (out + in links of a unit at
+ * its level) that assign units to the bins: up to 8, 16 and 32 links the
+ * register bins (fixed), then the warp bin up to warp_max_degree, the mid bin
+ * up to mid_max_degree, the block bin up to block_max_degree, the large bin
+ * up to large_max_degree, and the hub bin above. Results do not depend on
+ * these values (every bin's kernel loops over its units by grid stride,
+ * module statistics are exact integer sums, and every bin computes the same
+ * change per candidate), only the time does. rmx_set_tuning takes effect at
+ * the next launch; sweep pipelines captured as CUDA graphs under other values
+ * are captured again. Each grid cap must lie in [1, 64], and
+ * 32 <= warp_max <= 128, warp_max <= mid_max <= 512, mid_max <= block_max <=
+ * 1024, block_max <= large_max <= 4096 (the bins' table limits; an equal
+ * bound leaves a bin empty), else RMX_ERR_INVALID. The Python module
+ * relaxmap_b200.autotune picks the values by timing. No reference
+ * counterpart. */
 typedef struct rmx_tuning {
-    int32_t eval_mid_grid;   /* units of 129-512 links (default 8) */
-    int32_t eval_block_grid; /* 513-1024 links (default 4) */
-    int32_t eval_large_grid; /* 1025-4096 links (default 1) */
-    int32_t eval_warp_grid;  /* 33-128 links (default 3) */
-    int32_t eval_reg_grid;   /* up to 32 links (default 8) */
-    int32_t reserved[3];
+    int32_t eval_mid_grid;    /* mid bin (default 8) */
+    int32_t eval_block_grid;  /* block bin (default 4) */
+    int32_t eval_large_grid;  /* large bin (default 1) */
+    int32_t eval_warp_grid;   /* warp bin (default 3) */
+    int32_t eval_reg_grid;    /* register bins (default 8) */
+    int32_t warp_max_degree;  /* default 128 */
+    int32_t mid_max_degree;   /* default 512 */
+    int32_t block_max_degree; /* default 1024 */
+    int32_t large_max_degree; /* default 4096 */
 } rmx_tuning;
 
 rmx_status rmx_get_tuning(rmx_tuning *out);
@@ -284,11 +332,11 @@ rmx_status rmx_release_device_cache(void);
 #define RMX_NOALLOC_MAX_NODES (1 << 20)
 
 /* The stationary flow of rmx_initiate for callers that cannot allocate device
- * memory: a memory pool that owns the whole device under a fixed budget, work
- * being recorded into a CUDA graph, or a latency-bound path that must not pay
- * for an allocation's device-wide synchronisation. This entry point has no
- * counterpart in the reference (it computes calculateSteadyState only as part
- * of Network::initiate).
+ * memory: a framework whose memory pool owns the whole device under a fixed
+ * budget, or a latency-bound path that must not pay for the device-wide
+ * synchronisation an allocation implies. This entry point has no counterpart
+ * in the reference (it computes calculateSteadyState only as part of
+ * Network::initiate).
  * Every pointer is device memory owned by the caller: the in-links as CSC
  * (in_off[n_nodes+1], in_src[n_links], in_w[n_links] = row-normalised link
  * weights w_ab / sum_b w_ab), teleport[n_nodes], dangling[n_nodes] (1 for nodes
@@ -297,14 +345,20 @@ rmx_status rmx_release_device_cache(void);
  * RMX_NOALLOC_MAX_NODES (larger graphs: RMX_ERR_INVALID). The work is queued
  * on `stream` (a cudaStream_t, NULL for the legacy default stream) and the call
  * returns without waiting for it.
+ * It runs rmx_initiate's power iteration and stop rule, except that rows with
+ * very many in-links (more than 64 steps of their lanes) are summed in one
+ * pass instead of in chunks: on graphs with such in-degree hubs p agrees with
+ * rmx_initiate's to rounding (1e-12 relative L1) and the iteration count can
+ * differ by one; on other graphs both are identical.
  * Temporary storage is one array of about 8 MB inside this library, present on
  * every device that loads it until the process exits; it calls no cudaMalloc
  * or cudaFree. The first call on each device looks up that array's device
- * address (cudaGetSymbolAddress) with the device current; make that first call
- * before capturing a stream. All calls on a device share the array: calls whose
- * work overlaps on the GPU (other streams, other host threads) race and give
- * wrong results; order them on one stream or with events. Error text:
- * rmx_noalloc_last_error(). */
+ * address (cudaGetSymbolAddress) with the device current and keeps it for the
+ * life of the process: make that first call before any stream capture, and do
+ * not call again after a cudaDeviceReset of that device. All calls on a device
+ * share the array: calls whose work overlaps on the GPU (other streams, other
+ * host threads) race and give wrong results; order them on one stream or with
+ * events. Error text: rmx_noalloc_last_error(). */
 rmx_status rmx_steady_state_noalloc(int32_t n_nodes, int64_t n_links, const int64_t *in_off, const int32_t *in_src,
                                     const double *in_w, const double *teleport, const uint8_t *dangling,
                                     double *p_out, int32_t *iters_out, void *stream);

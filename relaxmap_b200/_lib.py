@@ -23,7 +23,7 @@ KERNELS = ["spmv", "eval", "commit", "coarsen", "codelen", "other", "adjoint"]
 EXPORTS = ["rmx_last_error", "rmx_version", "rmx_opts_default", "rmx_graph_create", "rmx_graph_load_file",
            "rmx_parse_file",
            "rmx_graph_destroy", "rmx_graph_info", "rmx_graph_links", "rmx_initiate", "rmx_codelength",
-           "rmx_coarsen", "rmx_evaluate_moves", "rmx_optimize", "rmx_superstep_codelengths", "rmx_write_outputs",
+           "rmx_coarsen", "rmx_evaluate_moves", "rmx_coarsen_engine", "rmx_evaluate_sn_moves", "rmx_optimize", "rmx_superstep_codelengths", "rmx_write_outputs",
            "rmx_set_profiling", "rmx_get_profile", "rmx_graph_stream", "rmx_sync", "rmx_cli_main",
            "rmx_steady_state_noalloc", "rmx_noalloc_last_error", "rmx_adjoint_forward", "rmx_adjoint_backward",
            "rmx_batch_create", "rmx_batch_set_wave", "rmx_batch_optimize", "rmx_batch_info", "rmx_batch_destroy",
@@ -50,7 +50,7 @@ class Profile(C.Structure):
     _fields_ = [("k", KernelStat * 7), ("sweeps", C.c_int64), ("supersteps", C.c_int64),
                 ("power_iters", C.c_int64), ("total_ms", C.c_double), ("kernel_launches", C.c_int64),
                 ("links_evaluated", C.c_int64), ("units_evaluated", C.c_int64), ("adjoint_iters", C.c_int64),
-                ("level_ms", C.c_double * 3)]
+                ("level_ms", C.c_double * 3), ("candidates_evaluated", C.c_int64)]
 
 
 _L = None
@@ -214,6 +214,36 @@ class Graph:
         return dict(n_sn=s, sn_of_mod=snm, out_off=oo[:s + 1], out_dst=od[:k], out_f=of[:k], in_off=io[:s + 1],
                     in_src=is_[:k], in_f=if_[:k])
 
+    def coarsen_engine(self, part, part2=None) -> dict:
+        """The optimiser's own coarsening of part (then of part2 over the
+        first level's modules): fixed-point link sums (value * 2^62), rows in
+        the engine's order."""
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        p2 = None if part2 is None else np.ascontiguousarray(part2, dtype=np.int32)
+        if p2 is not None and len(p2) != self.n:
+            raise ValueError("part2 needs one module per module id (n entries)")
+        n, m = self.n, max(self.n_links, 1)
+        nsn, nl = C.c_int32(), C.c_int64()
+        snm = np.zeros(n, dtype=np.int32)
+        oo, od, of = np.zeros(n + 1, dtype=np.int64), np.zeros(m, dtype=np.int32), np.zeros(m, dtype=np.int64)
+        io, is_, if_ = np.zeros(n + 1, dtype=np.int64), np.zeros(m, dtype=np.int32), np.zeros(m, dtype=np.int64)
+        st = np.zeros((n, 4), dtype=np.int64)
+        _check(lib().rmx_coarsen_engine(self._h, _p(part), _p(p2), C.byref(nsn), C.byref(nl), _p(snm), _p(oo),
+                                        _p(od), _p(of), _p(io), _p(is_), _p(if_), _p(st)))
+        k, s = nl.value, nsn.value
+        return dict(n_sn=s, sn_of_mod=snm, out_off=oo[:s + 1], out_dst=od[:k], out_fx=of[:k], in_off=io[:s + 1],
+                    in_src=is_[:k], in_fx=if_[:k], sn_stat=st[:s])
+
+    def evaluate_sn_moves(self, part, sn_part, allow_new=None):
+        """Move decisions of the super-nodes of part placed in modules sn_part."""
+        part = np.ascontiguousarray(part, dtype=np.int32)
+        sp = np.ascontiguousarray(sn_part, dtype=np.int32)
+        an = None if allow_new is None else np.ascontiguousarray(allow_new, dtype=np.uint8)
+        bm = np.zeros(len(sp), dtype=np.int32)
+        bd = np.zeros(len(sp))
+        _check(lib().rmx_evaluate_sn_moves(self._h, _p(part), len(sp), _p(sp), _p(an), _p(bm), _p(bd)))
+        return bm, bd
+
     def evaluate_moves(self, part, allow_new=None):
         part = np.ascontiguousarray(part, dtype=np.int32)
         an = None if allow_new is None else np.ascontiguousarray(allow_new, dtype=np.uint8)
@@ -246,7 +276,8 @@ class Graph:
                for i, name in enumerate(KERNELS)}
         out.update(sweeps=pr.sweeps, supersteps=pr.supersteps, power_iters=pr.power_iters, total_ms=pr.total_ms,
                    kernel_launches=pr.kernel_launches, links_evaluated=pr.links_evaluated,
-                   units_evaluated=pr.units_evaluated, adjoint_iters=pr.adjoint_iters,
+                   units_evaluated=pr.units_evaluated, candidates_evaluated=pr.candidates_evaluated,
+                   adjoint_iters=pr.adjoint_iters,
                    level_ms={"nodes": pr.level_ms[0], "super_nodes": pr.level_ms[1], "coarse_tune": pr.level_ms[2]})
         return out
 
@@ -352,24 +383,25 @@ def steady_state_noalloc(n_nodes: int, n_links: int, in_off_ptr: int, in_src_ptr
         raise RmxError(st, lib().rmx_noalloc_last_error().decode(errors="replace"))
 
 
-TUNING_FIELDS = ("eval_mid_grid", "eval_block_grid", "eval_large_grid", "eval_warp_grid", "eval_reg_grid")
+TUNING_FIELDS = ("eval_mid_grid", "eval_block_grid", "eval_large_grid", "eval_warp_grid", "eval_reg_grid",
+                 "warp_max_degree", "mid_max_degree", "block_max_degree", "large_max_degree")
 
 
 class Tuning(C.Structure):
-    _fields_ = [(f, C.c_int32) for f in TUNING_FIELDS] + [("reserved", C.c_int32 * 3)]
+    _fields_ = [(f, C.c_int32) for f in TUNING_FIELDS]
 
 
 def get_tuning() -> dict:
     """The process-wide launch shape of move evaluation (rmx_get_tuning): grid
-    cap of each degree bin in blocks per SM."""
+    cap of each degree bin in blocks per SM, and the degree bounds of the bins."""
     t = Tuning()
     _check(lib().rmx_get_tuning(C.byref(t)))
     return {f: getattr(t, f) for f in TUNING_FIELDS}
 
 
 def set_tuning(**values) -> dict:
-    """Change some of the grid caps (rmx_set_tuning); the others keep their
-    current values. Returns the new setting."""
+    """Change some of the grid caps or bin bounds (rmx_set_tuning); the others
+    keep their current values. Returns the new setting."""
     unknown = set(values) - set(TUNING_FIELDS)
     if unknown:
         raise ValueError(f"unknown tuning fields {sorted(unknown)}")

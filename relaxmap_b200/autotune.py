@@ -1,8 +1,10 @@
 """Autotuner for the launch shape of move evaluation (rmx_set_tuning).
 
-The grid cap of each degree bin (blocks per SM) changes the time of an
-optimiser run, never its result: every evaluation kernel loops over its bin's
-units by grid stride, and module statistics are exact integer sums. The tuner
+The grid cap of each degree bin (blocks per SM) and the degree bounds that
+assign units to the bins change the time of an optimiser run, never its
+result: every evaluation kernel loops over its bin's units by grid stride,
+module statistics are exact integer sums, and every bin computes the same
+change per candidate. The tuner
 times full runs of a representative graph under candidate caps, one knob at a
 time (coordinate descent, a few passes), keeps a candidate only when it is
 faster by more than the noise margin, and checks that every candidate
@@ -25,15 +27,22 @@ from typing import Callable
 
 from ._lib import TUNING_FIELDS, get_tuning, set_tuning
 
-# candidate grid caps (blocks per SM) of each bin; the defaults are among them
+# candidate grid caps (blocks per SM) of each bin and degree bounds of the
+# bins (links); the defaults are among them, and every combination keeps
+# warp <= mid <= block <= large
 KNOBS: dict[str, tuple[int, ...]] = {
     "eval_mid_grid": (4, 6, 8, 12, 16),
     "eval_block_grid": (2, 3, 4, 6, 8),
     "eval_large_grid": (1, 2, 3),
     "eval_warp_grid": (2, 3, 4, 6, 8),
     "eval_reg_grid": (4, 6, 8, 12, 16),
+    "warp_max_degree": (64, 96, 128),
+    "mid_max_degree": (256, 384, 512),
+    "block_max_degree": (768, 1024),
+    "large_max_degree": (2048, 3072, 4096),
 }
-DEFAULTS = {"eval_mid_grid": 8, "eval_block_grid": 4, "eval_large_grid": 1, "eval_warp_grid": 3, "eval_reg_grid": 8}
+DEFAULTS = {"eval_mid_grid": 8, "eval_block_grid": 4, "eval_large_grid": 1, "eval_warp_grid": 3, "eval_reg_grid": 8,
+            "warp_max_degree": 128, "mid_max_degree": 512, "block_max_degree": 1024, "large_max_degree": 4096}
 FORMAT = 1
 
 # measure(setting) -> (milliseconds per run, code length of the run)
@@ -81,7 +90,7 @@ def tune(measure: Measure, knobs: dict[str, tuple[int, ...]] | None = None, star
                 ms, L = run(cand)
                 if L != base_L:
                     raise TuningError(f"{k}={v} changed the code length ({L!r} against {base_L!r}): "
-                                      "grid caps must not change results")
+                                      "the launch shape must not change results")
                 if ms < best_ms * (1.0 - margin):
                     best_ms, cfg, changed = ms, cand, True
         if not changed:

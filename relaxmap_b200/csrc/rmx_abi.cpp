@@ -316,6 +316,32 @@ rmx_status rmx_evaluate_moves(rmx_graph *g, const int32_t *part, const uint8_t *
     });
 }
 
+rmx_status rmx_coarsen_engine(rmx_graph *g, const int32_t *part, const int32_t *part2, int32_t *n_sn,
+                              int64_t *n_sn_links, int32_t *sn_of_mod, int64_t *out_off, int32_t *out_dst,
+                              int64_t *out_fx, int64_t *in_off, int32_t *in_src, int64_t *in_fx, int64_t *sn_stat) {
+    return guard([&] {
+        need(g, "graph");
+        need(part, "part");
+        using fxp = rmx::fx_t *;
+        g->coarsen_engine_hook(part, part2, n_sn, n_sn_links, sn_of_mod, out_off, out_dst,
+                               reinterpret_cast<fxp>(out_fx), in_off, in_src, reinterpret_cast<fxp>(in_fx),
+                               reinterpret_cast<fxp>(sn_stat));
+    });
+}
+
+rmx_status rmx_evaluate_sn_moves(rmx_graph *g, const int32_t *part, int32_t n_sn, const int32_t *sn_part,
+                                 const uint8_t *allow_new, int32_t *best_mod, double *best_delta) {
+    return guard([&] {
+        need(g, "graph");
+        need(part, "part");
+        need(sn_part, "sn_part");
+        need(best_mod, "best_mod");
+        need(best_delta, "best_delta");
+        if (n_sn < 1) throw std::invalid_argument("n_sn must be positive");
+        g->evaluate_sn_hook(part, n_sn, sn_part, allow_new, best_mod, best_delta);
+    });
+}
+
 rmx_status rmx_optimize(rmx_graph *g, const rmx_opts *opts, int32_t *part_out, double *L_out, int32_t *n_modules) {
     return guard([&] {
         need(g, "graph");
@@ -400,13 +426,8 @@ rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out) {
         RMX_CUDA(cudaStreamSynchronize(g->stream));
         out->links_evaluated = c[0];
         out->units_evaluated = c[1];
-        // Compulsory traffic of the move evaluation, each array touched once:
-        // per link read, the neighbour id (4 B), its fixed-point flow (8 B) and
-        // the neighbour's module (4 B); per unit, its list entry (4), CSR and
-        // CSC offsets (32), attributes (32), module (4), instance (4), its own
-        // module's statistics (32), proposal and change written (12); per
-        // candidate module, its statistics record (32).
-        out->k[RMX_K_EVAL].bytes = 16.0 * (double)c[0] + 120.0 * (double)c[1] + 32.0 * (double)c[2];
+        out->candidates_evaluated = c[2];
+        out->k[RMX_K_EVAL].bytes = g->timers.eval_bytes;  // compulsory bytes per launch group (Timers)
         // The transposed solve, per sweep: link index, weight and the gathered
         // adjoint value (4 + 8 + 8 B per link); per node, the offsets, row sum,
         // right-hand side, teleport weight, dangling flag, the old value read
@@ -438,6 +459,10 @@ rmx_status rmx_get_tuning(rmx_tuning *out) {
         out->eval_large_grid = t.large;
         out->eval_warp_grid = t.warp;
         out->eval_reg_grid = t.reg;
+        out->warp_max_degree = t.warp_max;
+        out->mid_max_degree = t.mid_max;
+        out->block_max_degree = t.block_max;
+        out->large_max_degree = t.large_max;
     });
 }
 
@@ -450,6 +475,10 @@ rmx_status rmx_set_tuning(const rmx_tuning *t) {
         v.large = t->eval_large_grid;
         v.warp = t->eval_warp_grid;
         v.reg = t->eval_reg_grid;
+        v.warp_max = t->warp_max_degree;
+        v.mid_max = t->mid_max_degree;
+        v.block_max = t->block_max_degree;
+        v.large_max = t->large_max_degree;
         rmx::set_eval_tuning(v);
     });
 }

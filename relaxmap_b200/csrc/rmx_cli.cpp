@@ -20,9 +20,9 @@ double now_s() {
     return t.tv_sec + 1e-6 * t.tv_usec;
 }
 
-// Applies the grid caps of a launch tuning file (the JSON that
-// relaxmap_b200.autotune writes): every "eval_*_grid": <int> found in it, the
-// others keep their values. The values change run time only, never results.
+// Applies a launch tuning file (the JSON that relaxmap_b200.autotune writes):
+// every grid cap ("eval_*_grid") and bin bound ("*_max_degree") found in it,
+// the others keep their values. The values change run time only, never results.
 bool apply_tuning_file(const std::string &path) {
     FILE *f = fopen(path.c_str(), "rb");
     if (!f) {
@@ -43,7 +43,11 @@ bool apply_tuning_file(const std::string &path) {
                   {"\"eval_block_grid\"", &t.eval_block_grid},
                   {"\"eval_large_grid\"", &t.eval_large_grid},
                   {"\"eval_warp_grid\"", &t.eval_warp_grid},
-                  {"\"eval_reg_grid\"", &t.eval_reg_grid}};
+                  {"\"eval_reg_grid\"", &t.eval_reg_grid},
+                  {"\"warp_max_degree\"", &t.warp_max_degree},
+                  {"\"mid_max_degree\"", &t.mid_max_degree},
+                  {"\"block_max_degree\"", &t.block_max_degree},
+                  {"\"large_max_degree\"", &t.large_max_degree}};
     for (const Field &fd : fields) {
         const size_t k = text.find(fd.name);
         if (k == std::string::npos) continue;
@@ -55,14 +59,16 @@ bool apply_tuning_file(const std::string &path) {
             printf("tuning file %s: %s has no integer value\n", path.c_str(), fd.name);
             return false;
         }
-        *fd.v = (int32_t)std::max(-1L, std::min(v, 1000L));  // out-of-range values are rejected below
+        *fd.v = (int32_t)std::max(-1L, std::min(v, 100000L));  // out-of-range values are rejected below
     }
     if (rmx_set_tuning(&t) != RMX_OK) {
         printf("tuning file %s: %s\n", path.c_str(), rmx_last_error());
         return false;
     }
-    printf("Launch tuning from %s: grid caps (blocks per SM) mid %d, block %d, large %d, warp %d, register %d\n",
-           path.c_str(), t.eval_mid_grid, t.eval_block_grid, t.eval_large_grid, t.eval_warp_grid, t.eval_reg_grid);
+    printf("Launch tuning from %s: grid caps (blocks per SM) mid %d, block %d, large %d, warp %d, register %d; "
+           "bin bounds (links) warp %d, mid %d, block %d, large %d\n",
+           path.c_str(), t.eval_mid_grid, t.eval_block_grid, t.eval_large_grid, t.eval_warp_grid, t.eval_reg_grid,
+           t.warp_max_degree, t.mid_max_degree, t.block_max_degree, t.large_max_degree);
     return true;
 }
 

@@ -15,6 +15,8 @@
 //      destination gives the in-links in ascending source order.
 #include <algorithm>
 #include <climits>
+#include <mutex>
+#include <vector>
 
 #include "rmx_engine.cuh"
 
@@ -426,16 +428,25 @@ __global__ void k_agg_transpose(int32_t ng, const int64_t *g_out_off, const int3
         }
 }
 
+// The block bin's dynamic shared memory, set once per device.
+static void configure_agg_kernels() {
+    static std::mutex mu;
+    static std::vector<bool> done;
+    int dev = 0;
+    RMX_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)done.size() <= dev) done.resize(dev + 1, false);
+    if (done[dev]) return;
+    const int smem = (int)(kAggCap * (sizeof(fx_t) + sizeof(int32_t)));
+    RMX_CUDA(cudaFuncSetAttribute(k_agg_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    done[dev] = true;
+}
+
 int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *group,
                         int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx, int64_t *g_in_off,
-                        int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, fx_t *&gtab, int64_t &gtab_cap, Arena &ar,
-                        cudaStream_t s, const SweepWork *W) {
-    static bool configured = false;
-    if (!configured) {
-        const int smem = (int)(kAggCap * (sizeof(fx_t) + sizeof(int32_t)));
-        RMX_CUDA(cudaFuncSetAttribute(k_agg_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        configured = true;
-    }
+                        int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, Arena &gtab_arena, fx_t *&gtab,
+                        int64_t &gtab_cap, Arena &ar, cudaStream_t s, const SweepWork *W) {
+    configure_agg_kernels();
     int64_t E = 0;
     RMX_CUDA(cudaMemcpyAsync(&E, off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));
@@ -458,8 +469,6 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     RMX_CUDA(cudaMemsetAsync(fill, 0, sizeof(unsigned long long) * (ng + 1), s));
     k_agg_members<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, group, gmoff, fill, members);
     RMX_LAUNCHED();
-    // largest group (links) for the global tables
-    std::vector<int64_t> hl(2);
     uint8_t *fsmall = ar.alloc<uint8_t>(ng), *fmid = ar.alloc<uint8_t>(ng), *flarge = ar.alloc<uint8_t>(ng);
     RMX_CUDA(cudaMemsetAsync(tot, 0, sizeof(int64_t) * 5, s));
     k_agg_bins<<<blocks_for(ng, 256, num_sms() * 32), 256, 0, s>>>(ng, gloff, fsmall, fmid, flarge,
@@ -481,10 +490,13 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     while (need < 2 * std::min<int64_t>(maxlinks, ng)) need <<= 1;
     const int nblk = num_sms() * 2;
     if (need > kAggCap && need > gtab_cap) {
-        RMX_CUDA(cudaStreamSynchronize(s));
-        if (gtab) cudaFree(gtab);
+        RMX_CUDA(cudaStreamSynchronize(s));  // no launch still reads the old table
+        gtab_arena.destroy();
         gtab = nullptr;
-        RMX_CUDA(cudaMalloc(&gtab, (sizeof(fx_t) + sizeof(int32_t)) * need * nblk));
+        gtab_cap = 0;
+        gtab_arena.init((sizeof(fx_t) + sizeof(int32_t)) * need * nblk + 1024);
+        gtab = gtab_arena.alloc<fx_t>(need * nblk);
+        gtab_arena.alloc<int32_t>(need * nblk);  // the keys follow the values
         gtab_cap = need;
     }
     AggArgs a;
@@ -541,7 +553,6 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     RMX_CUDA(cudaMemcpyAsync(&m, tot + 2, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));
     ar.release(mk);
-    (void)hl;
     return m;
 }
 

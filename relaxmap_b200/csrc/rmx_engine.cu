@@ -163,6 +163,11 @@ __global__ void k_sn_set_out(int32_t n, const fx_t *rowsum, Stat4 *attr) {
         attr[s].OUT = rowsum[s];
 }
 
+__global__ void k_remap(int32_t n, const int32_t *map, int32_t *mod) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n; s += (int64_t)gridDim.x * blockDim.x)
+        mod[s] = map[mod[s]];
+}
+
 __global__ void k_count_nonzero(int32_t cap, const int32_t *count, unsigned long long *out) {
     unsigned long long c = 0;
     for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < cap; m += (int64_t)gridDim.x * blockDim.x)
@@ -286,6 +291,20 @@ void Timers::end(int k, cudaStream_t s) {
     if (used > 16384) resolve();
 }
 
+__global__ void k_snapshot(const int64_t *counters, int64_t *dst) {
+    if (threadIdx.x < 3) dst[threadIdx.x] = counters[kCntEdges + threadIdx.x];
+    if (threadIdx.x == 3) dst[3] = counters[kCntMods];
+}
+
+void Timers::log_eval(const int64_t *counters, cudaStream_t s) {
+    if (!on || !dlog) return;
+    if (nlog == logcap) resolve();
+    k_snapshot<<<1, 32, 0, s>>>(counters, dlog + 4 * nlog);
+    RMX_LAUNCHED();
+    log_stream = s;
+    nlog++;
+}
+
 void Timers::resolve() {
     for (auto &p : pending) {
         RMX_CUDA(cudaEventSynchronize(p.b));
@@ -295,6 +314,18 @@ void Timers::resolve() {
     }
     pending.clear();
     used = 0;
+    if (nlog > 0) {
+        std::vector<int64_t> h(4 * nlog);
+        RMX_CUDA(cudaMemcpyAsync(h.data(), dlog, sizeof(int64_t) * h.size(), cudaMemcpyDeviceToHost, log_stream));
+        RMX_CUDA(cudaStreamSynchronize(log_stream));
+        for (int64_t i = 0; i < nlog; i++) {
+            const int64_t *c = h.data() + 4 * i;
+            const double dl = (double)(c[0] - last[0]), du = (double)(c[1] - last[1]), dc = (double)(c[2] - last[2]);
+            eval_bytes += 16.0 * dl + 40.0 * du + 40.0 * std::min(dc, (double)c[3]);
+            for (int q = 0; q < 3; q++) last[q] = c[q];
+        }
+        nlog = 0;
+    }
 }
 
 void Timers::reset() {
@@ -304,6 +335,9 @@ void Timers::reset() {
         ms[k] = 0;
         launches[k] = 0;
     }
+    nlog = 0;
+    for (int64_t &v : last) v = 0;
+    eval_bytes = 0.0;
 }
 
 void Timers::destroy() {
@@ -324,9 +358,8 @@ rmx_graph::~rmx_graph() {
     if (work.fork) cudaEventDestroy(work.fork);
     for (cudaEvent_t e : work.join)
         if (e) cudaEventDestroy(e);
-    if (work.gtable) cudaFree(work.gtable);
-    if (work.gkeys) cudaFree(work.gkeys);
-    if (agg_tab) cudaFree(agg_tab);
+    hub_arena.destroy();
+    agg_arena.destroy();
     for (SweepGraph &g : sweep_graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     perm.destroy();
@@ -573,6 +606,8 @@ void rmx_graph::alloc_engine() {
     work.claim = perm.alloc<unsigned long long>(n);
     work.counters = perm.alloc<int64_t>(kCntSlots);
     work.dparams = perm.alloc<uint32_t>(64);
+    timers.logcap = 8192;
+    timers.dlog = perm.alloc<int64_t>(4 * timers.logcap);
     RMX_CUDA(cudaMemsetAsync(work.stamp, 0, sizeof(uint32_t) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.claim, 0, sizeof(unsigned long long) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.next_active, 0, n, stream));
@@ -598,15 +633,15 @@ void rmx_graph::ensure_hub_table(int64_t maxdeg) {
     int64_t cap = 64;
     while (cap < 2 * maxdeg) cap <<= 1;
     if (cap <= work.gcap) return;
-    RMX_CUDA(cudaStreamSynchronize(stream));
-    if (work.gtable) cudaFree(work.gtable);
-    if (work.gkeys) cudaFree(work.gkeys);
+    RMX_CUDA(cudaStreamSynchronize(stream));  // no launch still reads the old tables
+    hub_arena.destroy();
     work.gtable = nullptr;
     work.gkeys = nullptr;
     work.gcap = 0;
     const int64_t hb = hub_blocks(), slots = hub_slots(cap);
-    RMX_CUDA(cudaMalloc(&work.gtable, sizeof(fx_t) * 2 * slots * hb));
-    RMX_CUDA(cudaMalloc(&work.gkeys, sizeof(int32_t) * slots * hb));
+    hub_arena.init((size_t)(sizeof(fx_t) * 2 + sizeof(int32_t)) * slots * hb + 1024);
+    work.gtable = hub_arena.alloc<fx_t>(2 * slots * hb);
+    work.gkeys = hub_arena.alloc<int32_t>(slots * hb);
     work.gcap = cap;
 }
 
@@ -680,6 +715,12 @@ void rmx_graph::run_subbatches(Level &lv, int64_t n_active, ModState &M, InstSta
     // a single run on a handle is cheaper launched directly than captured: graphs
     // start with the handle's second attempt / optimiser run
     const bool graphs = !timers.on && use_graphs && runs_done > 0;
+    if (timers.on) {  // non-empty modules, for the evaluation's byte accounting
+        RMX_CUDA(cudaMemsetAsync(work.counters + kCntMods, 0, sizeof(int64_t), stream));
+        k_count_nonzero<<<blocks_for(M.cap, 256, num_sms() * 8), 256, 0, stream>>>(
+            M.cap, M.count, reinterpret_cast<unsigned long long *>(work.counters + kCntMods));
+        RMX_LAUNCHED();
+    }
     bucket_units(lv, work, n_active, seed, ns, scratch, stream, !graphs);
     for (int sb = 0; sb < ns; sb++) {
         work.hparams[2 * sb] = ++stamp;
@@ -848,11 +889,11 @@ void rmx_graph::convert_to_supernodes(bool from_sn) {
     dst.n = (int32_t)nsn;
     if (from_sn)
         dst.m = aggregate_links(src.n, src.out_off, src.out_dst, src.out_fx, group, dst.n, dst.out_off, dst.out_dst,
-                                dst.out_fx, dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_tab, agg_cap, scratch,
+                                dst.out_fx, dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_arena, agg_tab, agg_cap, scratch,
                                 stream, &work);
     else
         dst.m = aggregate_links(N, out_off, out_dst, out_fx, node_sn, dst.n, dst.out_off, dst.out_dst, dst.out_fx,
-                                dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_tab, agg_cap, scratch, stream, &work);
+                                dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_arena, agg_tab, agg_cap, scratch, stream, &work);
     scratch.release(mk);
     sn_cur = 1 - sn_cur;
     count_units(sn(), mods, stream);
@@ -954,7 +995,7 @@ void rmx_graph::generate_sub_modules() {
     {
         fx_t *rowsum = scratch.alloc<fx_t>(std::max<int64_t>(nsn, 1));
         sl.m = aggregate_links(N, out_off, out_dst, out_fx, node_sn, sl.n, sl.out_off, sl.out_dst, sl.out_fx,
-                               sl.in_off, sl.in_src, sl.in_fx, rowsum, agg_tab, agg_cap, scratch, stream, &work);
+                               sl.in_off, sl.in_src, sl.in_fx, rowsum, agg_arena, agg_tab, agg_cap, scratch, stream, &work);
         k_sn_set_out<<<blocks_for(nsn, 256, num_sms() * 32), 256, 0, stream>>>(sl.n, rowsum, sl.attr);
         RMX_LAUNCHED();
     }
@@ -1114,8 +1155,7 @@ double rmx_graph::optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modu
 
 double rmx_graph::codelength_fp64(const int32_t *part_host) {
     initiate();
-    for (int32_t v = 0; v < N; v++)
-        if ((uint32_t)part_host[v] >= (uint32_t)N) throw std::invalid_argument("module id outside 0..N-1");
+    check_partition(part_host);
     size_t mk = scratch.mark();
     int32_t *part = scratch.alloc<int32_t>(N);
     double *P = scratch.alloc<double>(N), *TW = scratch.alloc<double>(N), *D = scratch.alloc<double>(N),
@@ -1148,8 +1188,7 @@ void rmx_graph::coarsen_hook(const int32_t *part_host, int32_t *n_sn, int64_t *n
                              int64_t *o_off, int32_t *o_dst, double *o_f, int64_t *i_off, int32_t *i_src,
                              double *i_f) {
     initiate();
-    for (int32_t v = 0; v < N; v++)
-        if ((uint32_t)part_host[v] >= (uint32_t)N) throw std::invalid_argument("module id outside 0..N-1");
+    check_partition(part_host);
     size_t mk = scratch.mark();
     const int64_t Em = std::max<int64_t>(E, 1);
     int32_t *part = scratch.alloc<int32_t>(N);
@@ -1196,11 +1235,96 @@ void rmx_graph::coarsen_hook(const int32_t *part_host, int32_t *n_sn, int64_t *n
     if (n_links) *n_links = m;
 }
 
+void rmx_graph::check_partition(const int32_t *part_host) const {
+    for (int32_t v = 0; v < N; v++)
+        if ((uint32_t)part_host[v] >= (uint32_t)N) throw std::invalid_argument("module id outside 0..N-1");
+}
+
+// The first super-node level of the partition part, built as the optimiser
+// builds it after a node stage (module statistics from the nodes, then
+// convert_to_supernodes); returns the number of super-nodes.
+int32_t rmx_graph::supernodes_of(const int32_t *part_host) {
+    initiate();
+    check_partition(part_host);
+    RMX_CUDA(cudaMemcpyAsync(nmod, part_host, sizeof(int32_t) * N, cudaMemcpyHostToDevice, stream));
+    module_stats_from_units(node_lv, mods, stream);
+    convert_to_supernodes(false);
+    return sn().n;
+}
+
+void rmx_graph::coarsen_engine_hook(const int32_t *part_host, const int32_t *part2_host, int32_t *n_sn,
+                                    int64_t *n_links, int32_t *sn_of_mod, int64_t *o_off, int32_t *o_dst, fx_t *o_fx,
+                                    int64_t *i_off, int32_t *i_src, fx_t *i_fx, fx_t *sn_stat) {
+    if (part2_host) check_partition(part2_host);
+    supernodes_of(part_host);
+    if (part2_host) {
+        // the super-nodes move as whole modules: part2 relabels every first-level
+        // module, the nodes follow (project_sn_to_nodes), and the second
+        // conversion aggregates the first level's links
+        size_t mk = scratch.mark();
+        int32_t *map = scratch.alloc<int32_t>(N);
+        RMX_CUDA(cudaMemcpyAsync(map, part2_host, sizeof(int32_t) * N, cudaMemcpyHostToDevice, stream));
+        Level &l1 = sn();
+        k_remap<<<blocks_for(l1.n, 256, num_sms() * 32), 256, 0, stream>>>(l1.n, map, l1.mod);
+        RMX_LAUNCHED();
+        project_sn_to_nodes();
+        module_stats_from_units(node_lv, mods, stream);
+        RMX_CUDA(cudaStreamSynchronize(stream));
+        scratch.release(mk);
+        convert_to_supernodes(true);
+    }
+    const Level &lv = sn();
+    const int32_t ns = lv.n;
+    const int64_t m = lv.m;
+    std::vector<int32_t> smod(ns);
+    RMX_CUDA(cudaMemcpyAsync(smod.data(), lv.mod, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, stream));
+    if (o_off) RMX_CUDA(cudaMemcpyAsync(o_off, lv.out_off, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost, stream));
+    if (i_off) RMX_CUDA(cudaMemcpyAsync(i_off, lv.in_off, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost, stream));
+    if (sn_stat) RMX_CUDA(cudaMemcpyAsync(sn_stat, lv.attr, sizeof(Stat4) * ns, cudaMemcpyDeviceToHost, stream));
+    if (m > 0) {
+        if (o_dst) RMX_CUDA(cudaMemcpyAsync(o_dst, lv.out_dst, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, stream));
+        if (o_fx) RMX_CUDA(cudaMemcpyAsync(o_fx, lv.out_fx, sizeof(fx_t) * m, cudaMemcpyDeviceToHost, stream));
+        if (i_src) RMX_CUDA(cudaMemcpyAsync(i_src, lv.in_src, sizeof(int32_t) * m, cudaMemcpyDeviceToHost, stream));
+        if (i_fx) RMX_CUDA(cudaMemcpyAsync(i_fx, lv.in_fx, sizeof(fx_t) * m, cudaMemcpyDeviceToHost, stream));
+    }
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    if (sn_of_mod) {
+        for (int32_t i = 0; i < N; i++) sn_of_mod[i] = -1;
+        for (int32_t s = 0; s < ns; s++) sn_of_mod[smod[s]] = s;
+    }
+    if (n_sn) *n_sn = ns;
+    if (n_links) *n_links = m;
+}
+
+void rmx_graph::evaluate_sn_hook(const int32_t *part_host, int32_t n_sn, const int32_t *sn_part_host,
+                                 const uint8_t *allow_new_host, int32_t *best_mod, double *best_delta) {
+    for (int32_t s = 0; s < n_sn; s++)
+        if ((uint32_t)sn_part_host[s] >= (uint32_t)N) throw std::invalid_argument("module id outside 0..N-1");
+    if (supernodes_of(part_host) != n_sn)
+        throw std::invalid_argument("sn_part length differs from the number of super-nodes of part");
+    Level &lv = sn();
+    RMX_CUDA(cudaMemcpyAsync(lv.mod, sn_part_host, sizeof(int32_t) * n_sn, cudaMemcpyHostToDevice, stream));
+    size_t mk = scratch.mark();
+    uint8_t *an = nullptr;
+    if (allow_new_host) {
+        an = scratch.alloc<uint8_t>(n_sn);
+        RMX_CUDA(cudaMemcpyAsync(an, allow_new_host, n_sn, cudaMemcpyHostToDevice, stream));
+    }
+    module_stats_from_units(lv, mods, stream);
+    RMX_CUDA(cudaMemsetAsync(inst1.active, 1, (size_t)K, stream));
+    instance_codelength(mods, inst1, stream);
+    ensure_hub_table(max_degree(lv));
+    evaluate_all(lv, mods, inst1, work, an, 0.0, scratch, stream);
+    RMX_CUDA(cudaMemcpyAsync(best_mod, work.prop, sizeof(int32_t) * n_sn, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaMemcpyAsync(best_delta, work.pdelta, sizeof(double) * n_sn, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    scratch.release(mk);
+}
+
 void rmx_graph::evaluate_hook(const int32_t *part_host, const uint8_t *allow_new_host, int32_t *best_mod,
                               double *best_delta) {
     initiate();
-    for (int32_t v = 0; v < N; v++)
-        if ((uint32_t)part_host[v] >= (uint32_t)N) throw std::invalid_argument("module id outside 0..N-1");
+    check_partition(part_host);
     size_t mk = scratch.mark();
     uint8_t *an = nullptr;
     if (allow_new_host) {
@@ -1209,8 +1333,9 @@ void rmx_graph::evaluate_hook(const int32_t *part_host, const uint8_t *allow_new
     }
     RMX_CUDA(cudaMemcpyAsync(nmod, part_host, sizeof(int32_t) * N, cudaMemcpyHostToDevice, stream));
     module_stats_from_units(node_lv, mods, stream);
-    RMX_CUDA(cudaMemsetAsync(inst1.active, 1, 1, stream));
+    RMX_CUDA(cudaMemsetAsync(inst1.active, 1, (size_t)K, stream));
     instance_codelength(mods, inst1, stream);
+    ensure_hub_table(max_degree(node_lv));  // the bin bounds may have changed since initiate
     evaluate_all(node_lv, mods, inst1, work, an, 0.0, scratch, stream);
     RMX_CUDA(cudaMemcpyAsync(best_mod, work.prop, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaMemcpyAsync(best_delta, work.pdelta, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));

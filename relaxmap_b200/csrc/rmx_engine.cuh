@@ -126,15 +126,32 @@ struct Timers {
     cudaEvent_t open[kTimerCount] = {};
     double ms[kTimerCount] = {};
     int64_t launches[kTimerCount] = {};
+    // Compulsory bytes of the move evaluation, per launch group (one
+    // sub-batch's bins): 16 B per link read (neighbour id 4, fixed-point flow
+    // 8, neighbour's module 4), 40 B per unit (module id 4, statistics 32,
+    // proposal written 4), and the module statistics (40 B) once per launch,
+    // at most one per candidate: 40 * min(candidates, non-empty modules).
+    // Each launch group appends the running counters to a device log
+    // (log_eval); resolve() turns consecutive entries into per-launch counts.
+    int64_t *dlog = nullptr;  // 4 per entry: links, units, candidates (cumulative), non-empty modules
+    int64_t nlog = 0, logcap = 0;
+    cudaStream_t log_stream = nullptr;  // the stream the log entries were written on
+    int64_t last[3] = {0, 0, 0};
+    double eval_bytes = 0.0;
     void begin(int k, cudaStream_t s);
     void end(int k, cudaStream_t s);
+    void log_eval(const int64_t *counters, cudaStream_t s);
     void resolve();  // synchronises on the recorded events
     void reset();
     void destroy();
 };
 
-// Counter slots in SweepWork::counters (device int64).
-enum { kCntActive = 0, kCntFree = 1, kCntMoved = 3, kCntEdges = 4, kCntUnits = 5, kCntCands = 6, kCntSlots = 8 };
+// Counter slots in SweepWork::counters (device int64). kCntMods: non-empty
+// modules at the start of the current sweep (counted only while profiling).
+enum {
+    kCntActive = 0, kCntFree = 1, kCntMoved = 3, kCntEdges = 4, kCntUnits = 5, kCntCands = 6, kCntMods = 7,
+    kCntSlots = 8
+};
 
 // Per-level sweep workspace (sized for the largest level: N units, N modules).
 struct SweepWork {
@@ -164,20 +181,25 @@ struct SweepWork {
 void configure_eval_kernels();
 int hub_blocks();
 
-// Grid caps of the move-evaluation bins, in blocks per SM: process-wide,
-// read at every launch. Results do not depend on them (each bin's kernel loops
-// over its units by grid stride; module statistics are exact integer sums),
-// only the time does. The hub bin is not tuned: its global table slices are
-// indexed by block.
+// Launch shape of move evaluation, process-wide and read at every launch:
+// the grid cap of each bin in blocks per SM, and the degree bounds that
+// assign units to the warp, mid, block and large bins (units above large_max
+// go to the hub bin). Results do not depend on them (each bin's kernel loops
+// over its units by grid stride, every bin computes the same exact integer
+// sums and the same change per candidate), only the time does. The hub bin's
+// grid is not tuned: its global table slices are indexed by block.
 struct EvalTuning {
-    int mid, block, large, warp, reg;
+    int mid, block, large, warp, reg;              // grid caps
+    int warp_max, mid_max, block_max, large_max;   // degree bounds (at most 128, 512, 1024, 4096)
 };
 EvalTuning eval_tuning();
-// Throws std::invalid_argument unless every value lies in [1, 64].
+// Throws std::invalid_argument unless every grid cap lies in [1, 64] and
+// 32 <= warp_max <= mid_max <= block_max <= large_max, each within its bin's
+// table limit.
 void set_eval_tuning(const EvalTuning &t);
 // Changes with every set_eval_tuning (part of the sweep graph cache key).
 int eval_tuning_generation();
-int64_t warp_bin_max_degree();
+// Units above this degree need the hub bin's global tables.
 int64_t block_bin_max_degree();
 int64_t hub_slots(int64_t cap);
 void all_units(int32_t n, SweepWork &W, cudaStream_t s);
@@ -208,11 +230,12 @@ int64_t coarsen_links(int32_t n, const int64_t *out_off, const int32_t *out_dst,
 // Engine aggregation of rows (nodes or super-nodes) into groups by hashing:
 // fixed-point sums only, rows and columns in no particular order. rowsum (may
 // be NULL) receives each group's total out-flow. gtab / gtab_cap: a global
-// table grown on demand for groups too large for shared memory. W (may be
-// NULL): auxiliary streams and events on which the size bins run concurrently.
+// table in gtab_arena, grown on demand for groups too large for shared memory.
+// W (may be NULL): auxiliary streams and events on which the size bins run
+// concurrently.
 int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *group,
                         int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx, int64_t *g_in_off,
-                        int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, fx_t *&gtab, int64_t &gtab_cap, Arena &ar,
-                        cudaStream_t s, const SweepWork *W);
+                        int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, Arena &gtab_arena, fx_t *&gtab,
+                        int64_t &gtab_cap, Arena &ar, cudaStream_t s, const SweepWork *W);
 
 }  // namespace rmx

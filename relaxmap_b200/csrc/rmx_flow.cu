@@ -437,14 +437,19 @@ template <int VEC>
 static void launch_power_into(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w,
                               const double *tw, const uint8_t *dangling, double *p, double *y, double *parts,
                               int max_blocks, int *iters, cudaStream_t s) {
-    int dev = 0, per_sm = 0;
+    int dev = 0, per_sm = 0, coop = 0;
     RMX_CUDA(cudaGetDevice(&dev));
+    RMX_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    if (!coop) throw CudaError(cudaErrorNotSupported, "cooperative launch not supported on this device");
     RMX_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_power<VEC>, kPowT, 0));
     int nb = std::max(1, std::min(per_sm, RMX_POW_MINB)) * num_sms();
     nb = (int)std::min<int64_t>(nb, std::max<int64_t>(1, ((int64_t)n * VEC + kPowT - 1) / kPowT));
     nb = std::min(nb, max_blocks);
     double alpha = kAlpha;
-    PowSplit sp;  // no chunked rows: nothing beyond the caller's scratch
+    // No chunked rows: in-degree hubs are pulled in one pass by their own
+    // lanes (nothing beyond the caller's scratch), so on graphs with such
+    // hubs the sums round differently from power_iteration's.
+    PowSplit sp;
     void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w,  (void *)&tw,    (void *)&dangling, (void *)&n,
                     (void *)&p,      (void *)&y,      (void *)&parts, (void *)&iters, (void *)&alpha,    (void *)&sp};
     RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));

@@ -77,7 +77,13 @@ struct rmx_graph {
     rmx::InstState inst1, instsub;
     rmx::SweepWork work;
     rmx::Timers timers;
-    rmx::fx_t *agg_tab = nullptr;  // global hash tables of the link aggregation (grown on demand)
+    // Tables grown on demand for the largest units / groups of a level: the
+    // hub slices of move evaluation (work.gtable, work.gkeys) and the global
+    // hash tables of the link aggregation. Both are arenas, so their blocks
+    // come from and return to the process-wide block cache like the
+    // handle's other device memory (no cudaMalloc / cudaFree of their own).
+    rmx::Arena hub_arena, agg_arena;
+    rmx::fx_t *agg_tab = nullptr;
     int64_t agg_cap = 0;
 
     // ---- instances: 1 for a single graph; a batch is a disjoint union of
@@ -123,6 +129,17 @@ struct rmx_graph {
     void coarsen_hook(const int32_t *part, int32_t *n_sn, int64_t *n_links, int32_t *sn_of_mod, int64_t *o_off,
                       int32_t *o_dst, double *o_f, int64_t *i_off, int32_t *i_src, double *i_f);
     void evaluate_hook(const int32_t *part, const uint8_t *allow_new, int32_t *best_mod, double *best_delta);
+    // The optimiser's own coarsening (convert_to_supernodes, aggregate_links)
+    // on a given partition, optionally followed by a second conversion of the
+    // super-nodes (part2: module of every first-level module id); outputs the
+    // last level as the engine holds it (fixed-point flows, rows unordered).
+    void coarsen_engine_hook(const int32_t *part, const int32_t *part2, int32_t *n_sn, int64_t *n_links,
+                             int32_t *sn_of_mod, int64_t *o_off, int32_t *o_dst, rmx::fx_t *o_fx, int64_t *i_off,
+                             int32_t *i_src, rmx::fx_t *i_fx, rmx::fx_t *sn_stat);
+    // Move decisions of every super-node of the level built from part, with
+    // the super-nodes assigned to modules sn_part[n_sn].
+    void evaluate_sn_hook(const int32_t *part, int32_t n_sn, const int32_t *sn_part, const uint8_t *allow_new,
+                          int32_t *best_mod, double *best_delta);
     double optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modules);
     // Code length of a fixed partition at teleportation probability tau, and
     // optionally its gradient (rmx_adjoint.cu).
@@ -147,4 +164,6 @@ struct rmx_graph {
     int32_t count_modules();
     int sub_batches_for(int64_t n_active) const;
     int64_t max_degree(const rmx::Level &lv);
+    void check_partition(const int32_t *part_host) const;
+    int32_t supernodes_of(const int32_t *part_host);
 };

@@ -20,10 +20,10 @@
 // Module statistics are therefore always the exact fixed-point sums of the
 // current partition, and the code length is recomputed from them per sweep.
 #include <algorithm>
-#include <atomic>
 #include <climits>
 #include <mutex>
 #include <stdexcept>
+#include <vector>
 
 #include "rmx_engine.cuh"
 
@@ -965,33 +965,34 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
 int hub_blocks() { return num_sms(); }
 
 namespace {
-std::atomic<int> g_grid_mid{8}, g_grid_block{RMX_BLK_GRID}, g_grid_large{1}, g_grid_warp{RMX_WARP_GRID},
-    g_grid_reg{RMX_REG_GRID};
-std::atomic<int> g_tuning_gen{0};
-std::mutex g_tuning_mu;  // one setter at a time
+EvalTuning g_tuning{8, RMX_BLK_GRID, 1, RMX_WARP_GRID, RMX_REG_GRID, kWarpMaxDeg, kMidMaxDeg, kBlkMaxDeg, kLrgMaxDeg};
+int g_tuning_gen = 0;
+std::mutex g_tuning_mu;  // guards g_tuning and g_tuning_gen
 }  // namespace
 
 EvalTuning eval_tuning() {
-    return {g_grid_mid.load(std::memory_order_relaxed), g_grid_block.load(std::memory_order_relaxed),
-            g_grid_large.load(std::memory_order_relaxed), g_grid_warp.load(std::memory_order_relaxed),
-            g_grid_reg.load(std::memory_order_relaxed)};
+    std::lock_guard<std::mutex> lk(g_tuning_mu);
+    return g_tuning;
 }
 
 void set_eval_tuning(const EvalTuning &t) {
     for (int v : {t.mid, t.block, t.large, t.warp, t.reg})
         if (v < 1 || v > 64) throw std::invalid_argument("evaluation grid caps must lie in 1..64 blocks per SM");
+    // each bin's bound lies between the previous bin's and its own table's limit
+    if (t.warp_max < 32 || t.warp_max > kWarpMaxDeg || t.mid_max < t.warp_max || t.mid_max > kMidMaxDeg ||
+        t.block_max < t.mid_max || t.block_max > kBlkMaxDeg || t.large_max < t.block_max || t.large_max > kLrgMaxDeg)
+        throw std::invalid_argument("degree bin bounds must satisfy 32 <= warp <= 128, warp <= mid <= 512, "
+                                    "mid <= block <= 1024, block <= large <= 4096");
     std::lock_guard<std::mutex> lk(g_tuning_mu);
-    g_grid_mid.store(t.mid);
-    g_grid_block.store(t.block);
-    g_grid_large.store(t.large);
-    g_grid_warp.store(t.warp);
-    g_grid_reg.store(t.reg);
-    g_tuning_gen.fetch_add(1);
+    g_tuning = t;
+    g_tuning_gen++;
 }
 
-int eval_tuning_generation() { return g_tuning_gen.load(); }
-int64_t block_bin_max_degree() { return kLrgMaxDeg; }
-int64_t warp_bin_max_degree() { return kWarpMaxDeg; }
+int eval_tuning_generation() {
+    std::lock_guard<std::mutex> lk(g_tuning_mu);
+    return g_tuning_gen;
+}
+int64_t block_bin_max_degree() { return eval_tuning().large_max; }
 int64_t hub_slots(int64_t cap) { return cap; }
 
 constexpr size_t kBlkSmem = (size_t)kBlkCap * (2 * sizeof(fx_t) + sizeof(int32_t));
@@ -1064,9 +1065,15 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
             }
 }
 
+// Dynamic shared memory and carve-out of the evaluation bins, set once per device.
 void configure_eval_kernels() {
-    static bool done = false;
-    if (done) return;
+    static std::mutex mu;
+    static std::vector<bool> configured;
+    int dev = 0;
+    RMX_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    if ((int)configured.size() <= dev) configured.resize(dev + 1, false);
+    if (configured[dev]) return;
     RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, kBlkCap, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kBlkSmem));
     RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kLrgT, kLrgCap, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1076,7 +1083,7 @@ void configure_eval_kernels() {
     RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kLrgT, kLrgCap, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   100));
     RMX_CUDA(cudaFuncSetAttribute(k_eval_warp, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    done = true;
+    configured[dev] = true;
 }
 
 __global__ void k_iota(int32_t *list, int32_t n, int64_t *count) {
@@ -1090,8 +1097,13 @@ void all_units(int32_t n, SweepWork &W, cudaStream_t s) {
     RMX_LAUNCHED();
 }
 
+// Upper degree bounds of the warp, mid, block and large bins (run-time tuning).
+struct BinBounds {
+    int32_t warp, mid, block, large;
+};
+
 __global__ void k_bucket(const int32_t *list, const int64_t *n_active, const int64_t *out_off, const int64_t *in_off,
-                         uint32_t seed, int nsub, uint16_t *bucket) {
+                         uint32_t seed, int nsub, BinBounds bb, uint16_t *bucket) {
     const int64_t n = *n_active;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t u = list[i];
@@ -1099,11 +1111,11 @@ __global__ void k_bucket(const int32_t *list, const int64_t *n_active, const int
         const int bin = d <= 8 ? kBinReg8
                         : d <= 16 ? kBinReg16
                         : d <= 32 ? kBinReg32
-                        : d <= kWarpMaxDeg ? kBinWarp
-                        : d <= kMidMaxDeg ? kBinMid
-                        : d <= kBlkMaxDeg ? kBinBlock
-                        : d <= kLrgMaxDeg ? kBinLarge
-                                          : kBinHub;
+                        : d <= bb.warp ? kBinWarp
+                        : d <= bb.mid ? kBinMid
+                        : d <= bb.block ? kBinBlock
+                        : d <= bb.large ? kBinLarge
+                                        : kBinHub;
         const int sb = nsub > 1 ? (int)(mix32((uint32_t)u ^ seed) % (uint32_t)nsub) : 0;
         bucket[i] = (uint16_t)(sb * kBins + bin);
     }
@@ -1120,8 +1132,10 @@ __global__ void k_ranges(const int64_t *bucket_off, int nsub, int64_t *ranges) {
 void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed, int nsub, Arena &ar,
                   cudaStream_t s, bool host_counts) {
     if (nsub * kBins > 256) throw std::invalid_argument("too many sub-batches");
+    const EvalTuning t = eval_tuning();
+    const BinBounds bb{t.warp_max, t.mid_max, t.block_max, t.large_max};
     k_bucket<<<blocks_for(n_active, 256, num_sms() * 32), 256, 0, s>>>(W.list, W.counters + kCntActive, L.out_off,
-                                                                       L.in_off, seed, nsub, W.bucket);
+                                                                       L.in_off, seed, nsub, bb, W.bucket);
     RMX_LAUNCHED();
     bucket_partition(W.bucket, W.list, W.list2, n_active, nsub * kBins, W.bucket_off, ar, s);
     k_ranges<<<1, 128, 0, s>>>(W.bucket_off, nsub, W.ranges);
@@ -1161,7 +1175,10 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     ea.mark = mark_active ? 1 : 0;
     if (tm) tm->begin(kTimerEval, s);
     launch_eval(ea, W.bucket_off, sb * kBins, W, fitted, s);
-    if (tm) tm->end(kTimerEval, s);
+    if (tm) {
+        tm->end(kTimerEval, s);
+        tm->log_eval(W.counters, s);
+    }
     if (tm) tm->begin(kTimerCommit, s);
     CommitArgs ca;
     ca.list = W.list2;

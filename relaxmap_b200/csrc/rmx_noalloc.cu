@@ -2,12 +2,11 @@
 //
 // Some callers own every byte of device memory themselves or must not allocate
 // while they run: a framework that hands out memory only from its own pool
-// under a fixed budget, code that records work into a CUDA graph (cudaMalloc
-// may not be called while a stream is being captured), or a latency-bound
-// service that cannot afford the device-wide synchronisation an allocation
-// implies. rmx_steady_state_noalloc runs the same power iteration as
-// rmx_initiate on arrays such a caller already holds on the device, with its
-// temporary storage in one fixed array compiled into this library.
+// under a fixed budget, or a latency-bound service that cannot afford the
+// device-wide synchronisation an allocation implies. rmx_steady_state_noalloc
+// runs rmx_initiate's power iteration on arrays such a caller already holds on
+// the device, with its temporary storage in one fixed array compiled into this
+// library.
 #include <mutex>
 
 #include "../../include/relaxmap_b200.h"
@@ -24,7 +23,9 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 // Device address of g_noalloc_scratch per device, found once per device with
 // that device current (host code cannot take the address of a __device__
-// array directly: the name is only a host-side stand-in).
+// array directly: the name is only a host-side stand-in). Kept for the life of
+// the process, so a cudaDeviceReset after the first call leaves it stale (the
+// header says not to call again after one).
 constexpr int kMaxDevices = 64;
 void *g_addr[kMaxDevices] = {};
 std::mutex g_mu;

@@ -23,7 +23,7 @@ Writes, per fixture graph <g>:
                            (QUALITY_CASES): the reference's final code length
                            (bits, recomputed) for seeds 1..8 at 8 threads, prior
 
-    python tests/golden/make_golden.py quality   # only quality.ref.npz
+    python tests/golden/make_golden.py quality [case ...]   # only quality.ref.npz
 """
 from __future__ import annotations
 
@@ -100,12 +100,23 @@ QUALITY_CASES = {
     "rmat14": lambda: synth.rmat(14, 16, seed=42),
     "planted20k_mid": lambda: synth.config_mid(seed=42, n=20_000),
     "planted20k_adjoint": lambda: synth.config_adjoint(seed=42, n=20_000),
+    # the bench's CPU sample of the R-MAT family, and the full 1M-node mid graph
+    "rmat18": lambda: synth.rmat(18, 16, seed=42),
+    "planted1m_mid": lambda: synth.config_mid(seed=42, n=1_000_000),
 }
 
 
-def quality():
+def quality(names=None):
+    """The reference's 8-seed final code lengths of QUALITY_CASES (all, or the
+    named ones, merged into the existing file)."""
     out = {}
+    qf = HERE / "quality.ref.npz"
+    if names and qf.exists():
+        with np.load(qf) as z:
+            out = {k: z[k] for k in z.files}
     for name, make in QUALITY_CASES.items():
+        if names and name not in names:
+            continue
         g = make()
         ld = O.from_edges(g.n, g.src, g.dst, g.w)
         Lc = []
@@ -115,8 +126,8 @@ def quality():
             Lc.append(R.partition(seed=seed, threads=8, threshold=1e-3, vthresh=0.0, max_iter=10,
                                   prior=True)["L_computed_bits"])
         out[name] = np.array(Lc)
-        print(name, "N", g.n, "E", g.m, "median L bits", np.median(Lc))
-    np.savez_compressed(HERE / "quality.ref.npz", **out)
+        print(name, "N", g.n, "E", g.m, "median L bits", np.median(Lc), flush=True)
+        np.savez_compressed(qf, **out)
 
 
 def cli_outputs():
@@ -132,8 +143,8 @@ def cli_outputs():
 
 if __name__ == "__main__":
     O.build(reference=True)
-    if sys.argv[1:] == ["quality"]:
-        quality()
+    if sys.argv[1:2] == ["quality"]:
+        quality(sys.argv[2:])
         sys.exit(0)
     copy_inputs()
     for name in ("flow.net", "flow.txt", "directNet_1k_sm_mu_03.txt", "small_planted.txt"):

@@ -29,6 +29,16 @@ def test_tuning_abi_defaults_and_validation(restore_tuning):
     assert get_tuning() == dict(DEFAULTS, eval_mid_grid=12, eval_reg_grid=16)  # unchanged by a rejected call
     with pytest.raises(ValueError):
         set_tuning(eval_hub_grid=2)
+    # degree bounds: ordered, each within its bin's table limit
+    assert set_tuning(warp_max_degree=64, mid_max_degree=64)["mid_max_degree"] == 64
+    for bad in ({"warp_max_degree": 31}, {"warp_max_degree": 129}, {"mid_max_degree": 63},
+                {"mid_max_degree": 513}, {"block_max_degree": 1025}, {"large_max_degree": 1000},
+                {"large_max_degree": 4097}):
+        with pytest.raises(RmxError) as e:
+            set_tuning(**bad)
+        assert e.value.status == 1
+    assert get_tuning() == dict(DEFAULTS, eval_mid_grid=12, eval_reg_grid=16, warp_max_degree=64,
+                                mid_max_degree=64)
 
 
 def _quadratic(opt, L=1.0, calls=None):
@@ -44,7 +54,7 @@ def test_tune_finds_the_fastest_setting():
     opt = {"eval_mid_grid": 12, "eval_block_grid": 6, "eval_large_grid": 2, "eval_warp_grid": 3, "eval_reg_grid": 4}
     calls = []
     r = tune(_quadratic(opt, calls=calls))
-    assert r["tuning"] == opt
+    assert r["tuning"] == dict(DEFAULTS, **opt)  # the bin bounds do not change the modelled time
     assert r["ms"] == 100.0
     assert r["baseline_ms"] == 100.0 + 10.0 * sum((DEFAULTS[k] - opt[k]) ** 2 for k in opt)
     assert r["timed_settings"] == len(calls)
@@ -54,13 +64,13 @@ def test_tune_finds_the_fastest_setting():
 def test_tune_times_each_setting_once():
     """After a knob moves, coordinate descent meets earlier settings again
     (the old value of that knob, or a second pass): they are not re-timed."""
-    from relaxmap_b200.autotune import tune
+    from relaxmap_b200.autotune import DEFAULTS, tune
     opt = {"eval_mid_grid": 4, "eval_block_grid": 4, "eval_large_grid": 1, "eval_warp_grid": 2, "eval_reg_grid": 8}
     knobs = {"eval_mid_grid": (4, 8), "eval_warp_grid": (2, 3)}
     for passes, distinct in ((1, 3), (3, 4)):  # the second pass adds (mid 8, warp 2) only
         calls = []
         r = tune(_quadratic(opt, calls=calls), knobs=knobs, passes=passes)
-        assert r["tuning"] == opt
+        assert r["tuning"] == dict(DEFAULTS, **opt)
         keys = [tuple(sorted(c.items())) for c in calls]
         assert len(keys) == len(set(keys)) == r["timed_settings"] == distinct
 

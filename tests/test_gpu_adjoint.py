@@ -97,3 +97,52 @@ def test_adjoint_solve_cap_reports_no_convergence(built_lib):
             G.adjoint_backward(part, 1e-4)
         assert e.value.status == 6  # RMX_ERR_NO_CONVERGENCE
         _check(G, part, 0.15)
+
+
+def test_adjoint_full_size_config(built_lib):
+    """The adjoint workload at full size: N = 1,000,000, mean out-degree 20,
+    mu = 0.3, lognormal(0, 1) weights, the planted communities as the fixed
+    partition.
+
+    * Against the CPU FP64 adjoint (Neumann-series solves to 1e-16): dL/dw
+      within 1e-6 relative L1 and 1e-6 of the largest component, dL/dtau
+      within 1e-6 relative, L within 1e-12 relative.
+    * Against centred differences of rmx_adjoint_forward (h = 1e-6 of the
+      link's weight; the graph rebuilt from its own CSR with one weight
+      moved): 64 links, 32 drawn at random and the 32 of largest |dL/dw|.
+      A difference quotient carries the forward's own rounding, about
+      1e-14 |L| per evaluation (the flow solve stops at a relative L1 change
+      of 1e-15), divided by 2h: the bar is 1e-6 |g| plus that floor."""
+    from relaxmap_b200 import Graph, synth
+    g = synth.config_adjoint(seed=42, n=1_000_000)
+    part = np.ascontiguousarray(g.community, dtype=np.int32)
+    with Graph.from_edges(g.src, g.dst, g.w, n=g.n) as G:
+        off, dst, w, tw = G.links()
+        bw = G.adjoint_backward(part)
+    ref = AD.backward(off, dst, w, tw, part)
+    grad, rg = bw["dL_dw"], ref["dL_dw"]
+    assert abs(bw["L"] - ref["L"]) <= 1e-12 * abs(ref["L"])
+    assert _rel_l1(grad, rg) <= 1e-6, _rel_l1(grad, rg)
+    assert np.abs(grad - rg).max() <= 1e-6 * np.abs(rg).max()
+    assert abs(bw["dL_dtau"] - ref["dL_dt"]) <= 1e-6 * abs(ref["dL_dt"])
+    # centred differences on links of the prepared graph (CSR order = gradient order)
+    src = np.repeat(np.arange(g.n, dtype=np.int32), np.diff(off))
+    rng = np.random.default_rng(11)
+    pick = np.unique(np.concatenate([rng.choice(len(w), 32, replace=False), np.argsort(-np.abs(grad))[:32]]))
+    L0 = bw["L"]
+    worst = 0.0
+    for j in pick:
+        h = 1e-6 * w[j]
+        vals = []
+        for sgn in (1.0, -1.0):
+            wj = w.copy()
+            wj[j] += sgn * h
+            with Graph.from_edges(src, dst, wj, n=g.n) as Gp:
+                vals.append(Gp.adjoint_forward(part)["L"])
+        fd = (vals[0] - vals[1]) / (2 * h)
+        floor = 1e-14 * abs(L0) / h
+        err = abs(fd - grad[j])
+        assert err <= 1e-6 * abs(grad[j]) + floor, (j, fd, grad[j], floor)
+        worst = max(worst, err / (1e-6 * abs(grad[j]) + floor))
+    print(f"adjoint at 1M nodes: rel L1 vs CPU {_rel_l1(grad, rg):.2e}; FD worst {worst:.3f} of the bar "
+          f"on {len(pick)} links")

@@ -1,9 +1,11 @@
 """Launch tuning on the device changes time, not results: optimiser runs under
 extreme grid caps of the move-evaluation bins (one block per SM, and many)
-give the same partition and code length bit for bit as the default caps, both
-on direct launches and on sweep CUDA graphs captured after the change; the
-autotuner runs end to end, restores the setting it found, and its saved
-result applies on this device."""
+and under other degree bounds of the bins (every unit above 32 links in the
+hub bin's global tables; narrow warp and mid bins; empty bins) give the same
+partition and code length bit for bit as the defaults, both on direct
+launches and on sweep CUDA graphs captured after the change; the autotuner
+runs end to end, restores the setting it found, and its saved result applies
+on this device."""
 import numpy as np
 import pytest
 
@@ -20,14 +22,20 @@ def graph(built_lib):
     set_tuning(**before)
 
 
-def test_grid_caps_do_not_change_results(graph):
+def test_launch_shape_does_not_change_results(graph):
     from relaxmap_b200 import TUNING_FIELDS, set_tuning
     from relaxmap_b200.autotune import DEFAULTS
     G = graph
     ref = G.optimize(seed=3)
-    for cfg in ({f: 1 for f in TUNING_FIELDS},
+    caps = [f for f in TUNING_FIELDS if f.endswith("_grid")]
+    for cfg in ({f: 1 for f in caps},
                 {"eval_mid_grid": 16, "eval_block_grid": 8, "eval_large_grid": 3, "eval_warp_grid": 8,
                  "eval_reg_grid": 16},
+                DEFAULTS,
+                dict(DEFAULTS, warp_max_degree=32, mid_max_degree=32, block_max_degree=32, large_max_degree=32),
+                dict(DEFAULTS, warp_max_degree=48, mid_max_degree=200, block_max_degree=200, large_max_degree=700),
+                dict(DEFAULTS, warp_max_degree=128, mid_max_degree=128, block_max_degree=1024,
+                     large_max_degree=1024),
                 DEFAULTS):
         set_tuning(**cfg)
         for _ in range(2):  # the second run replays the sweep graphs captured by the first
