@@ -431,6 +431,11 @@ def main():
                      "algorithmic_bytes_per_launch": ev["bytes"] / max(ev["launches"], 1),
                      "launch_ms_avg": ev["ms"] / max(ev["launches"], 1)},
         "kernel_time_share": {k: round(v / tot, 4) for k, v in shares.items()},
+        "profiled_run": {"level_ms": prof["level_ms"],
+                         "eval_bin_ms": {b: round(v["ms"], 3) for b, v in prof["eval_bins"].items()},
+                         "links_evaluated": prof["links_evaluated"], "units_evaluated": prof["units_evaluated"],
+                         "candidates_evaluated": prof["candidates_evaluated"], "sweeps": prof["sweeps"],
+                         "power_iters": prof["power_iters"]},
         "gpu_launches": int(gpu_launches),
         "clocks": clk.summary(),
     }

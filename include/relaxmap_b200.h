@@ -87,6 +87,9 @@ typedef struct {
     int64_t adjoint_iters;   /* sweeps of the transposed solve since profiling was enabled */
     double level_ms[3];      /* device time of the sweep loops on nodes, super-nodes, coarse-tune sub-problems */
     int64_t candidates_evaluated; /* (unit, candidate module) pairs evaluated since profiling was enabled */
+    double eval_bin_ms[6];   /* move evaluation per degree bin (register, warp, mid, block, large, hub): summed
+                                kernel time; the bins of one sub-batch run concurrently on separate streams */
+    int64_t eval_bin_launches[6];
 } rmx_profile;
 
 const char *rmx_last_error(void);

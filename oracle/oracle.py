@@ -17,7 +17,23 @@ from pathlib import Path
 import numpy as np
 
 ORACLE_DIR = Path(__file__).resolve().parent
-REF_SRC = Path(os.environ.get("RMX_REFERENCE_DIR", "/root/reference"))
+
+
+def _ref_src() -> Path:
+    """The reference sources the oracle recipe compiles: RMX_REFERENCE_DIR if
+    set, else the recipe's own REF_DIR (oracle/Makefile)."""
+    env = os.environ.get("RMX_REFERENCE_DIR")
+    if env:
+        return Path(env)
+    try:
+        r = subprocess.run(["make", "-s", "--no-print-directory", "-C", str(ORACLE_DIR), "refdir"],
+                           capture_output=True, text=True, timeout=30)
+        return Path(r.stdout.strip()) if r.returncode == 0 and r.stdout.strip() else Path("")
+    except (OSError, subprocess.SubprocessError):
+        return Path("")
+
+
+REF_SRC = _ref_src()
 ORACLE_SO = ORACLE_DIR / "librmxoracle.so"
 REF_SO = ORACLE_DIR / "_ref" / "librmxref.so"
 REF_BIN = ORACLE_DIR / "_ref" / "ompRelaxmap"
@@ -33,7 +49,7 @@ _f64 = np.float64
 def build(reference: bool = True) -> None:
     """Compile the C restatement, and the reference harness when its sources exist."""
     targets = ["oracle"]
-    if reference and REF_SRC.is_dir():
+    if reference and (REF_SRC / "Module.cpp").is_file():
         targets.append("ref")
     subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), f"REF_DIR={REF_SRC}", *targets], check=True)
 

@@ -435,6 +435,10 @@ rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out) {
         out->k[RMX_K_ADJOINT].bytes =
             (double)g->prof.adjoint_iters * (20.0 * (double)g->E + 65.0 * (double)g->N);
         for (int k = 0; k < 3; k++) out->level_ms[k] = g->timers.ms[rmx::kTimerLvNode + k];
+        for (int k = 0; k < 6; k++) {
+            out->eval_bin_ms[k] = g->timers.ms[rmx::kTimerBinReg + k];
+            out->eval_bin_launches[k] = g->timers.launches[rmx::kTimerBinReg + k];
+        }
         out->power_iters = g->power_iters;
         out->kernel_launches = (int64_t)__atomic_load_n(&rmx::g_kernel_launches, __ATOMIC_RELAXED);
     });

@@ -259,35 +259,75 @@ struct AggArgs {
     int32_t ngroups;
 };
 
+// Members of at least a team's width of links that a block team defers to
+// its second pass, at most kAggBig per group (the rest stay with their warp).
+constexpr int kAggBig = 128;
+
+// Inserts links [e0, e1) of one member (stride `step` from the caller's
+// lane/rank) into the group's table; false once the table is full.
+template <int NT>
+__device__ __forceinline__ bool agg_links(const AggArgs &a, int32_t g, int64_t e0, int64_t e1, int step,
+                                          int32_t *keys, fx_t *vals, int mask, int *nkeys) {
+    for (int64_t e = e0; e < e1; e += step) {
+        const int32_t b = a.group[a.dst[e]];
+        if (b == g) continue;
+        bool fresh;
+        const int s = agg_insert(keys, mask, b, fresh);
+        if (s < 0) return false;  // only a table sized below the bound can fill up; nkeys > limit already
+        if (NT > 32 && fresh) atomicAdd(nkeys, 1);
+        atomicAdd(reinterpret_cast<unsigned long long *>(vals + s), (unsigned long long)a.fx[e]);
+    }
+    return true;
+}
+
 // One group by a team of NT threads (r = rank); keys/vals: a table of cap
 // slots. A table sized below twice the group's link count may hold at most
 // `limit` distinct keys: past that the group is abandoned (returns false,
-// uniformly across the team) and nothing of it is written. wsh: NT/32 + 2 ints.
+// uniformly across the team) and nothing of it is written. wsh: NT/32 + 3
+// ints; big: kAggBig ints (block teams only).
+// A warp takes one member at a time, its lanes over the member's links. In a
+// block team a member of NT links or more is deferred to a second pass in
+// which the whole team strides its links, so that one heavy member does not
+// keep one warp busy while the others wait at the next barrier.
 template <int NT>
 __device__ __forceinline__ bool agg_group(const AggArgs &a, int32_t g, int r, int32_t *keys, fx_t *vals, int64_t cap,
-                                          int limit, int *wsh) {
+                                          int limit, int *wsh, int32_t *big) {
     const int lane = r & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int mask = (int)(cap - 1);
-    int *nkeys = wsh + NT / 32 + 1;
+    int *nkeys = wsh + NT / 32 + 1, *nbig = wsh + NT / 32 + 2;
     for (int64_t s = r; s < cap; s += NT) {
         keys[s] = kNoKey;
         vals[s] = 0;
     }
-    if (NT > 32 && r == 0) *nkeys = 0;
+    if (NT > 32 && r == 0) {
+        *nkeys = 0;
+        *nbig = 0;
+    }
     if (NT == 32) __syncwarp(); else __syncthreads();
     const int64_t mb = a.gmoff[g], me = a.gmoff[g + 1];
     for (int64_t m = mb + (r >> 5); m < me; m += NT / 32) {  // a warp per member, lanes over its links
         if (NT > 32 && *(volatile int *)nkeys > limit) break;
         const int32_t u = a.members[m];
-        for (int64_t e = a.off[u] + lane; e < a.off[u + 1]; e += 32) {
-            const int32_t b = a.group[a.dst[e]];
-            if (b == g) continue;
-            bool fresh;
-            const int s = agg_insert(keys, mask, b, fresh);
-            if (s < 0) break;  // only a table sized below the bound can fill up; nkeys > limit already
-            if (NT > 32 && fresh) atomicAdd(nkeys, 1);
-            atomicAdd(reinterpret_cast<unsigned long long *>(vals + s), (unsigned long long)a.fx[e]);
+        const int64_t e0 = a.off[u], e1 = a.off[u + 1];
+        if (NT > 32 && e1 - e0 >= NT) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(nbig, 1);
+            k = __shfl_sync(kFullMask, k, 0);
+            if (k < kAggBig) {
+                if (lane == 0) big[k] = u;
+                continue;
+            }
+        }
+        agg_links<NT>(a, g, e0 + lane, e1, 32, keys, vals, mask, nkeys);
+    }
+    if (NT > 32) {
+        __syncthreads();
+        const int nb = min(*nbig, kAggBig);
+        for (int k = 0; k < nb; k++) {
+            if (*(volatile int *)nkeys > limit) break;
+            const int32_t u = big[k];
+            if (!agg_links<NT>(a, g, a.off[u] + r, a.off[u + 1], NT, keys, vals, mask, nkeys)) break;
         }
     }
     if (NT == 32) __syncwarp(); else __syncthreads();
@@ -358,21 +398,22 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_agg_warp(AggArgs a) {
         const int64_t bound = min(a.gloff[g + 1] - a.gloff[g], (int64_t)a.ngroups);
         int64_t cap = 32;
         while (cap < 2 * bound) cap <<= 1;
-        agg_group<32>(a, g, lane, skeys[w], svals[w], cap, INT_MAX, nullptr);
+        agg_group<32>(a, g, lane, skeys[w], svals[w], cap, INT_MAX, nullptr, nullptr);
     }
 }
 
 __global__ void __launch_bounds__(kAggMidT) k_agg_mid(AggArgs a) {
     __shared__ int32_t skeys[kAggMidCap];
     __shared__ fx_t svals[kAggMidCap];
-    __shared__ int wsh[kAggMidT / 32 + 2];
+    __shared__ int wsh[kAggMidT / 32 + 3];
+    __shared__ int32_t big[kAggBig];
     const int64_t n = *a.count;
     for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
         const int32_t g = a.list[i];
         const int64_t bound = min(a.gloff[g + 1] - a.gloff[g], (int64_t)a.ngroups);
         int64_t cap = 64;
         while (cap < 2 * bound) cap <<= 1;
-        agg_group<kAggMidT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh);
+        agg_group<kAggMidT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh, big);
     }
 }
 
@@ -382,7 +423,8 @@ __global__ void __launch_bounds__(kAggMidT) k_agg_mid(AggArgs a) {
 // distinct neighbours than that is redone in a global slice sized by its links.
 __global__ void __launch_bounds__(kAggT, 2) k_agg_block(AggArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
-    __shared__ int wsh[kAggT / 32 + 2];
+    __shared__ int wsh[kAggT / 32 + 3];
+    __shared__ int32_t big[kAggBig];
     fx_t *svals = reinterpret_cast<fx_t *>(dsm);
     int32_t *skeys = reinterpret_cast<int32_t *>(svals + kAggCap);
     const int64_t n = *a.count;
@@ -392,10 +434,10 @@ __global__ void __launch_bounds__(kAggT, 2) k_agg_block(AggArgs a) {
         int64_t cap = 64;
         while (cap < 2 * bound) cap <<= 1;
         if (cap <= kAggCap) {
-            agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh);
-        } else if (!agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, kAggCap, kAggCap / 4 * 3, wsh)) {
+            agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh, big);
+        } else if (!agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, kAggCap, kAggCap / 4 * 3, wsh, big)) {
             agg_group<kAggT>(a, g, threadIdx.x, a.gkeys + (int64_t)blockIdx.x * a.gcap,
-                             a.gvals + (int64_t)blockIdx.x * a.gcap, cap, INT_MAX, wsh);
+                             a.gvals + (int64_t)blockIdx.x * a.gcap, cap, INT_MAX, wsh, big);
         }
     }
 }

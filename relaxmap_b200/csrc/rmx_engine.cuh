@@ -112,7 +112,9 @@ void instance_codelength(const ModState &M, InstState &I, cudaStream_t s);
 enum {
     kTimerSpmv = 0, kTimerEval, kTimerCommit, kTimerCoarsen, kTimerCodelen, kTimerOther, kTimerAdjoint,
     // whole sweep loops by level (they contain the kernel classes above)
-    kTimerLvNode, kTimerLvSN, kTimerLvSub, kTimerCount
+    kTimerLvNode, kTimerLvSN, kTimerLvSub,
+    // each degree bin of the move evaluation (register, warp, mid, block, large, hub)
+    kTimerBinReg, kTimerBinWarp, kTimerBinMid, kTimerBinBlock, kTimerBinLarge, kTimerBinHub, kTimerCount
 };
 struct Timers {
     bool on = false;

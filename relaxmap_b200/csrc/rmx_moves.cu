@@ -27,6 +27,15 @@
 
 #include "rmx_engine.cuh"
 
+// links each thread of a shared-table bin gathers ahead of its table inserts
+#ifndef RMX_EVAL_ILP
+#define RMX_EVAL_ILP 1
+#endif
+// the total-exit term of every candidate through log1p of a per-unit log (1) or a log each (0)
+#ifndef RMX_LOG1P
+#define RMX_LOG1P 0
+#endif
+
 namespace rmx {
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -70,8 +79,25 @@ struct UnitCtx {
     double eA, nexA;        // old module exit before / after the unit leaves
     double sum_exit;
     double K;               // -plogp(se) - 2 (plogp(nexA) - plogp(eA)) + plogp(nexA + nPA) - plogp(eA + PA)
+    double S0, logS0, rS0;  // the new total exit without the target's change, its log and reciprocal
     int32_t A;
 };
+
+// plogp of the new total exit flow S0 + dm, where dm = (new - old exit of the
+// target module) is tiny next to S0 for almost every candidate: then
+// log(S0 + dm) = log(S0) + log1p(dm / S0) with log(S0) computed once per unit
+// and log1p by its Mercator series through t^6 (|t| < 2^-10: truncation below
+// 2^-70 / 7 of the value, far under FP64 rounding); otherwise the direct log.
+__device__ __forceinline__ double plogp_total(const UnitCtx &c, double dm) {
+#if RMX_LOG1P
+    const double t = dm * c.rS0;
+    if (c.rS0 > 0.0 && fabs(t) < 0x1p-10) {
+        const double l1p = t * (1.0 - t * (0.5 - t * (1.0 / 3.0 - t * (0.25 - t * (0.2 - t * (1.0 / 6.0))))));
+        return (c.S0 + dm) * (c.logS0 + l1p);
+    }
+#endif
+    return plogp(c.S0 + dm);
+}
 
 // Change of moving the unit into module with statistics st, given the unit's
 // aggregated out-/in-flow (fixed point, before the 1-tau factor) to it:
@@ -84,15 +110,14 @@ __device__ __forceinline__ double candidate_delta(const UnitCtx &c, const Stat4 
     const double om = kBeta * from_fx(ofx) + c.cu * TW;                        // Module.cpp:1058
     const double im = kBeta * from_fx(ifx) + (kAlpha * P + kBeta * D) * c.tu;  // Module.cpp:1059
     const double nexm = em + c.eu - om - im;                                   // Module.cpp:1104
-    const double nse = c.sum_exit + c.nexA + nexm - c.eA - em;                 // Module.cpp:1106
-    return plogp(nse) + c.K - 2.0 * (plogp(nexm) - t.x) + (plogp(nexm + P + c.pu) - t.y);
+    // new total exit sumAllExitPr + (nexA - eA) + (nexm - em), Module.cpp:1106
+    return plogp_total(c, nexm - em) + c.K - 2.0 * (plogp(nexm) - t.x) + (plogp(nexm + P + c.pu) - t.y);
 }
 
 // The empty-module option: exit e_u, no shared flow (Module.cpp:1072-1077).
 __device__ __forceinline__ double newmod_delta(const UnitCtx &c) {
     const double nexm = c.eu;
-    const double nse = c.sum_exit + c.nexA + nexm - c.eA;
-    return plogp(nse) + c.K - 2.0 * plogp(nexm) + plogp(nexm + c.pu);
+    return plogp_total(c, nexm) + c.K - 2.0 * plogp(nexm) + plogp(nexm + c.pu);
 }
 
 __device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, const double2 tA, double sum_exit,
@@ -110,6 +135,14 @@ __device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, co
     c.nexA = c.eA - c.eu + outA + inA;                                                          // :1084
     c.sum_exit = sum_exit;
     c.K = -plogp(sum_exit) - 2.0 * (plogp(c.nexA) - tA.x) + (plogp(c.nexA + (PA - c.pu)) - tA.y);
+    c.S0 = sum_exit + c.nexA - c.eA;
+#if RMX_LOG1P
+    const bool pos = c.S0 > 0.0;
+    c.logS0 = pos ? log(c.S0) : 0.0;
+    c.rS0 = pos ? 1.0 / c.S0 : 0.0;
+#else
+    c.logS0 = c.rS0 = 0.0;
+#endif
     c.A = A;
     return c;
 }
@@ -275,13 +308,35 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
         vi[s] = 0;
     }
     gsync<NT>();
-    for (int64_t j = r; j < d; j += NT) {
-        const bool isout = j < dout;
-        const int64_t e = isout ? ob + j : ib + (j - dout);
-        const int32_t nb = isout ? a.out_dst[e] : a.in_src[e];
-        const fx_t q = isout ? a.out_fx[e] : a.in_fx[e];
-        const int s = tab_insert(keys, mask, a.mod[nb]);
-        atomic_add_fx(isout ? vo + s : vi + s, q);
+    // Each thread takes links r, r + NT, ...; RMX_EVAL_ILP of them at a time
+    // have their neighbour ids, flows and then neighbour modules loaded before
+    // any is inserted, so that many gathers are in flight per thread.
+    for (int64_t j0 = r; j0 < d; j0 += (int64_t)RMX_EVAL_ILP * NT) {
+        int32_t key[RMX_EVAL_ILP];
+        fx_t q[RMX_EVAL_ILP];
+#pragma unroll
+        for (int k = 0; k < RMX_EVAL_ILP; k++) {
+            const int64_t j = j0 + (int64_t)k * NT;
+            key[k] = -1;
+            q[k] = 0;
+            if (j < d) {
+                const bool isout = j < dout;
+                const int64_t e = isout ? ob + j : ib + (j - dout);
+                key[k] = __ldg(isout ? a.out_dst + e : a.in_src + e);
+                q[k] = __ldg(isout ? a.out_fx + e : a.in_fx + e);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < RMX_EVAL_ILP; k++)
+            if (key[k] >= 0) key[k] = __ldg(a.mod + key[k]);
+#pragma unroll
+        for (int k = 0; k < RMX_EVAL_ILP; k++) {
+            const int64_t j = j0 + (int64_t)k * NT;
+            if (j < d) {
+                const int s = tab_insert(keys, mask, key[k]);
+                atomic_add_fx(j < dout ? vo + s : vi + s, q[k]);
+            }
+        }
     }
     gsync<NT>();
     const int32_t A = a.mod[u];
@@ -1009,7 +1064,7 @@ static unsigned fit_grid(int64_t items, int64_t per_block, int64_t max_grid) {
 // register bins on s itself. Only non-empty bins are launched (sizes from the
 // host copy of the bucket offsets); a lone bin runs on s without the fork.
 static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket, const SweepWork &W, bool fitted,
-                        cudaStream_t s) {
+                        cudaStream_t s, Timers *tm = nullptr) {
     const int64_t *h = fitted ? W.bucket_host.data() + first_bucket : nullptr;
     // without host sizes every bin counts as non-empty and takes its full grid
     auto cnt = [&](int b0, int b1) { return fitted ? h[b1] - h[b0] : (int64_t)1 << 40; };
@@ -1028,34 +1083,46 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     }
     if (n_mid > 0) {
         a.range = bucket_off + first_bucket + kBinMid;
+        if (tm) tm->begin(kTimerBinMid, on(3));
         k_eval_block<kMidT, kMidCap, false><<<fit_grid(n_mid, 1, (int64_t)num_sms() * tg.mid), kMidT, kMidSmem, on(3)>>>(a);
         RMX_LAUNCHED();
+        if (tm) tm->end(kTimerBinMid, on(3));
     }
     if (n_blk > 0) {
         a.range = bucket_off + first_bucket + kBinBlock;
+        if (tm) tm->begin(kTimerBinBlock, on(0));
         k_eval_block<kBlkT, kBlkCap, false><<<fit_grid(n_blk, 1, (int64_t)num_sms() * tg.block), kBlkT, kBlkSmem, on(0)>>>(
             a);
         RMX_LAUNCHED();
+        if (tm) tm->end(kTimerBinBlock, on(0));
     }
     if (n_lrg > 0) {
         a.range = bucket_off + first_bucket + kBinLarge;
+        if (tm) tm->begin(kTimerBinLarge, on(1));
         k_eval_block<kLrgT, kLrgCap, false><<<fit_grid(n_lrg, 1, (int64_t)num_sms() * tg.large), kLrgT, kLrgSmem, on(1)>>>(a);
         RMX_LAUNCHED();
+        if (tm) tm->end(kTimerBinLarge, on(1));
     }
     if (n_hub > 0) {  // global table slices are indexed by block: at most hub_blocks() blocks
         a.range = bucket_off + first_bucket + kBinHub;
+        if (tm) tm->begin(kTimerBinHub, on(1));
         k_eval_block<kHubT, 0, true><<<fit_grid(n_hub, 1, hub_blocks()), kHubT, 0, on(1)>>>(a);
         RMX_LAUNCHED();
+        if (tm) tm->end(kTimerBinHub, on(1));
     }
     if (n_warp > 0) {
         a.range = bucket_off + first_bucket + kBinWarp;
+        if (tm) tm->begin(kTimerBinWarp, on(2));
         k_eval_warp<<<fit_grid(n_warp, kEvalWarps, (int64_t)num_sms() * tg.warp), kEvalWarps * 32, 0, on(2)>>>(a);
         RMX_LAUNCHED();
+        if (tm) tm->end(kTimerBinWarp, on(2));
     }
     if (n_reg > 0) {
         a.range = bucket_off + first_bucket + kBinReg8;
+        if (tm) tm->begin(kTimerBinReg, s);
         k_eval_reg<<<fit_grid(n_reg, 8, (int64_t)num_sms() * tg.reg), 256, 0, s>>>(a);
         RMX_LAUNCHED();
+        if (tm) tm->end(kTimerBinReg, s);
     }
     if (fork)
         for (int k = 0; k < 4; k++)
@@ -1174,7 +1241,7 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
     EvalArgs ea = eval_args(L, M, I, W, sa.vthresh, sa.allow_new, nullptr, 1);
     ea.mark = mark_active ? 1 : 0;
     if (tm) tm->begin(kTimerEval, s);
-    launch_eval(ea, W.bucket_off, sb * kBins, W, fitted, s);
+    launch_eval(ea, W.bucket_off, sb * kBins, W, fitted, s, tm);
     if (tm) {
         tm->end(kTimerEval, s);
         tm->log_eval(W.counters, s);

@@ -1,7 +1,7 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a container where the reference sources exist (RMX_REFERENCE_DIR,
-default /root/reference); it builds oracle/_ref/ from them (oracle/Makefile).
+Run where the reference sources exist (RMX_REFERENCE_DIR, else the oracle
+recipe's REF_DIR in oracle/Makefile); it builds oracle/_ref/ from them.
 
     python tests/golden/make_golden.py
 
@@ -27,7 +27,6 @@ Writes, per fixture graph <g>:
 """
 from __future__ import annotations
 
-import os
 import shutil
 import subprocess
 import sys
@@ -44,7 +43,7 @@ sys.path.insert(0, str(ROOT))
 from oracle import oracle as O  # noqa: E402
 from relaxmap_b200 import synth  # noqa: E402
 
-REF = Path(os.environ.get("RMX_REFERENCE_DIR", "/root/reference"))
+REF = O.REF_SRC
 SEEDS = list(range(1, 9))
 
 
