@@ -253,12 +253,63 @@ __global__ void k_fp64_terms(int32_t n, const double *P, const double *TW, const
     }
 }
 
-uint32_t mix_seed(uint32_t a, uint64_t b) {
+__host__ __device__ uint32_t mix_seed(uint32_t a, uint64_t b) {
     uint64_t x = a * 0x9E3779B97F4A7C15ull ^ (b + 0x632BE59BD9B4E019ull);
     x ^= x >> 31;
     x *= 0xBF58476D1CE4E5B9ull;
     x ^= x >> 29;
     return (uint32_t)(x ^ (x >> 32));
+}
+
+// ---- a stage loop captured as one graph (while node; the body is one sweep)
+
+// Start of a sweep, as the host loop does it: the sweep number and its seed,
+// each sub-batch's stamp and hash seed (run_subbatches), the instances that
+// take part (set_active) and the code lengths before the sweep.
+__global__ void k_stage_begin(int64_t *ctl, uint32_t *seed_out, int ns, uint32_t *dparams, int32_t K,
+                              const uint8_t *sweeping, uint8_t *active, const double *L, double *oldL) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint64_t sw = (uint64_t)ctl[0] + 1;
+        const uint32_t seed = mix_seed((uint32_t)ctl[2], sw);
+        uint32_t st = (uint32_t)ctl[1];
+        for (int sb = 0; sb < ns; sb++) {
+            dparams[2 * sb] = ++st;
+            dparams[2 * sb + 1] = mix_seed(seed, (uint64_t)sb);
+        }
+        ctl[0] = (int64_t)sw;
+        ctl[1] = (int64_t)st;
+        ctl[4] = 0;
+        *seed_out = seed;
+    }
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
+        active[k] = sweeping[k];
+        oldL[k] = L[k];
+    }
+}
+
+// The stop rule of stage_sweeps per instance (OmpRelaxmap.cpp:291-339): an
+// instance stops when a sweep gained less than threshold bits and did not lose.
+__global__ void k_stage_stop(int32_t K, const double *L, const double *oldL, uint8_t *sweeping, double threshold,
+                             double ln2, unsigned long long *remaining) {
+    unsigned long long c = 0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < K; k += (int64_t)gridDim.x * blockDim.x) {
+        if (!sweeping[k]) continue;
+        const double d = oldL[k] - L[k];
+        if (d >= 0 && d / ln2 < threshold)
+            sweeping[k] = 0;
+        else
+            c++;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(kFull, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(remaining, c);
+}
+
+// Count the sweep and decide whether the while node runs its body again.
+__global__ void k_stage_cond(int64_t *ctl, int max_iter, cudaGraphConditionalHandle cond) {
+    const int64_t it = ctl[3] + 1;
+    ctl[3] = it;
+    cudaGraphSetConditional(cond, (ctl[4] > 0 && it < max_iter) ? 1u : 0u);
 }
 
 }  // namespace
@@ -361,6 +412,8 @@ rmx_graph::~rmx_graph() {
     hub_arena.destroy();
     agg_arena.destroy();
     for (SweepGraph &g : sweep_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (StageGraph &g : stage_graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     perm.destroy();
     scratch.destroy();
@@ -608,6 +661,10 @@ void rmx_graph::alloc_engine() {
     work.dparams = perm.alloc<uint32_t>(64);
     timers.logcap = 8192;
     timers.dlog = perm.alloc<int64_t>(4 * timers.logcap);
+    stage_ctl = perm.alloc<int64_t>(8);
+    stage_seed = perm.alloc<uint32_t>(8);
+    stage_sweeping = perm.alloc<uint8_t>(std::max(K, 1));
+    stage_oldL = perm.alloc<double>(std::max(K, 1));
     RMX_CUDA(cudaMemsetAsync(work.stamp, 0, sizeof(uint32_t) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.claim, 0, sizeof(unsigned long long) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.next_active, 0, n, stream));
@@ -832,6 +889,10 @@ void rmx_graph::stage_sweeps(Level &lv, bool allow_new, std::vector<double> &L, 
     int64_t n_active = lv.n;
     all_units(lv.n, work, stream);
     if (lv.n > 0) ensure_hub_table(max_degree(lv));
+    if (stage_graph_ok(lv)) {
+        stage_sweeps_graph(lv, allow_new, L, act);
+        return;
+    }
     std::vector<uint8_t> sweeping = act;
     std::vector<double> oldL;
     const int lvt = &lv == &node_lv ? kTimerLvNode : kTimerLvSN;
@@ -850,6 +911,119 @@ void rmx_graph::stage_sweeps(Level &lv, bool allow_new, std::vector<double> &L, 
             if (sweeping[k] && oldL[k] - L[k] >= 0 && (oldL[k] - L[k]) / kLn2 < opt.threshold) sweeping[k] = 0;
     }
     timers.end(lvt, stream);
+}
+
+// The stage loop runs as one captured graph once the handle has completed a
+// run (as the sweep pipelines: capture costs more than one cold run saves),
+// without profiling events and without per-sweep printing.
+bool rmx_graph::stage_graph_ok(const Level &lv) const {
+    return use_graphs && runs_done > 0 && !timers.on && opt.verbose < 2 && lv.n > 0;
+}
+
+// One sweep of stage_sweeps as the body of the while node: the host loop's
+// sweep_single with every size and seed read on the device, then its stop
+// rule. cond: the while node's condition handle.
+void rmx_graph::stage_body(Level &lv, bool allow_new, bool prior, double vthresh, int ns, unsigned long long cond) {
+    const int64_t *n_dev = stage_ctl + 5;
+    k_stage_begin<<<blocks_for(K, 256, num_sms() * 4), 256, 0, stream>>>(stage_ctl, stage_seed, ns, work.dparams, K,
+                                                                         stage_sweeping, inst1.active, inst1.L,
+                                                                         stage_oldL);
+    RMX_LAUNCHED();
+    if (!prior) all_units_dev(n_dev, N, work, stream);  // normal mode: every sweep takes all units
+    RMX_CUDA(cudaMemsetAsync(work.counters + kCntMoved, 0, sizeof(int64_t), stream));
+    if (prior) RMX_CUDA(cudaMemsetAsync(work.next_active, 0, (size_t)N, stream));
+    if (allow_new) free_modules(mods, work, scratch, stream);
+    bucket_units_dev(lv, work, N, stage_seed, ns, scratch, stream);
+    SweepArgs sa{vthresh, allow_new ? 1 : 0};
+    for (int sb = 0; sb < ns; sb++)
+        sweep_subbatch(lv, mods, inst1, work, sa, sb, work.dparams + 2 * sb, prior, false, stream, nullptr);
+    instance_codelength(mods, inst1, stream);
+    if (prior) compact_flags_dev(work.next_active, n_dev, N, work.list, work.counters + kCntActive, scratch, stream);
+    k_stage_stop<<<blocks_for(K, 256, num_sms() * 4), 256, 0, stream>>>(
+        K, inst1.L, stage_oldL, stage_sweeping, opt.threshold, kLn2,
+        reinterpret_cast<unsigned long long *>(stage_ctl + 4));
+    RMX_LAUNCHED();
+    k_stage_cond<<<1, 1, 0, stream>>>(stage_ctl, opt.max_iter, (cudaGraphConditionalHandle)cond);
+    RMX_LAUNCHED();
+}
+
+void rmx_graph::stage_sweeps_graph(Level &lv, bool allow_new, std::vector<double> &L,
+                                   const std::vector<uint8_t> &act) {
+    const bool prior = opt.prior != 0;
+    const double vthresh = prior ? -opt.vthresh : 0.0;  // OmpRelaxmap.cpp:66, Module.cpp:1490 vs :1127
+    if (!any_set(act) || opt.max_iter <= 0) return;
+    const int ns = sub_batches_for(lv.n);
+    const StageGraphKey key{&lv,      &mods,     &inst1,       allow_new ? 1 : 0, prior ? 1 : 0,
+                            opt.max_iter, ns,    vthresh,      opt.threshold,     work.gtable,
+                            work.gcap, eval_tuning_generation(), scratch.mark()};
+    StageGraph *gr = nullptr;
+    for (StageGraph &g : stage_graphs)
+        if (g.key == key) gr = &g;
+    if (!gr) {
+        bool stale = false;  // graphs captured under another launch tuning are never launched again
+        for (const StageGraph &g : stage_graphs) stale |= g.key.tuning_gen != key.tuning_gen;
+        if (stale) {
+            RMX_CUDA(cudaStreamSynchronize(stream));
+            std::vector<StageGraph> keep;
+            for (StageGraph &g : stage_graphs) {
+                if (g.key.tuning_gen == key.tuning_gen)
+                    keep.push_back(g);
+                else if (g.exec)
+                    cudaGraphExecDestroy(g.exec);
+            }
+            stage_graphs.swap(keep);
+        }
+        cudaGraph_t graph = nullptr;
+        RMX_CUDA(cudaGraphCreate(&graph, 0));
+        cudaGraphExec_t exec = nullptr;
+        unsigned long long kernels = 0;
+        try {
+            cudaGraphConditionalHandle cond;
+            RMX_CUDA(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            RMX_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            const unsigned long long c0 = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
+            RMX_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            try {
+                stage_body(lv, allow_new, prior, vthresh, ns, (unsigned long long)cond);
+            } catch (...) {
+                cudaGraph_t g2 = nullptr;
+                cudaStreamEndCapture(stream, &g2);
+                throw;
+            }
+            cudaGraph_t g2 = nullptr;
+            RMX_CUDA(cudaStreamEndCapture(stream, &g2));
+            const unsigned long long c1 = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
+            kernels = c1 - c0;
+            __atomic_fetch_sub(&g_kernel_launches, kernels, __ATOMIC_RELAXED);  // counted per sweep replayed
+            RMX_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        } catch (...) {
+            cudaGraphDestroy(graph);
+            throw;
+        }
+        cudaGraphDestroy(graph);
+        stage_graphs.push_back({key, exec, kernels});
+        gr = &stage_graphs.back();
+    }
+    // host loop state in, the loop on the device, state out (staged from
+    // pageable memory: the host arrays are free again when the calls return)
+    int64_t ctl[6] = {(int64_t)sweep_no, (int64_t)stamp, (int64_t)run_seed, 0, 0, (int64_t)lv.n};
+    RMX_CUDA(cudaMemcpyAsync(stage_ctl, ctl, sizeof ctl, cudaMemcpyHostToDevice, stream));
+    RMX_CUDA(cudaMemcpyAsync(stage_sweeping, act.data(), (size_t)K, cudaMemcpyHostToDevice, stream));
+    RMX_CUDA(cudaGraphLaunch(gr->exec, stream));
+    RMX_CUDA(cudaMemcpyAsync(L.data(), inst1.L, sizeof(double) * K, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaMemcpyAsync(ctl, stage_ctl, sizeof ctl, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+    sweep_no = (uint64_t)ctl[0];
+    stamp = (uint32_t)ctl[1];
+    prof.sweeps += ctl[3];
+    __atomic_fetch_add(&g_kernel_launches, gr->kernels * (unsigned long long)ctl[3], __ATOMIC_RELAXED);
 }
 
 void rmx_graph::project_sn_to_nodes() {

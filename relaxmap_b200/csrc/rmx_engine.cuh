@@ -208,6 +208,12 @@ void all_units(int32_t n, SweepWork &W, cudaStream_t s);
 // host_counts: also copy the bin offsets to W.bucket_host (one stream sync).
 void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed, int nsub, Arena &ar, cudaStream_t s,
                   bool host_counts = true);
+// bucket_units for a captured sweep: the active count (counters[kCntActive])
+// and the seed are read on the device; grids are sized for n_max units.
+void bucket_units_dev(const Level &L, SweepWork &W, int64_t n_max, const uint32_t *seed_dev, int nsub, Arena &ar,
+                      cudaStream_t s);
+// all_units for *n_dev units (device), grids sized for n_max.
+void all_units_dev(const int64_t *n_dev, int64_t n_max, SweepWork &W, cudaStream_t s);
 void free_modules(const ModState &M, SweepWork &W, Arena &ar, cudaStream_t s);
 // Evaluate, claim, commit and apply link deltas for sub-batch sb.
 // sp: device {stamp, hseed} of the sub-batch. stamp: unique per sub-batch over

@@ -46,6 +46,32 @@ struct SweepGraph {
     unsigned long long kernels;  // kernel nodes, counted as launches per replay
 };
 
+// A whole stage loop of sweeps (stage_sweeps) as one CUDA graph: a while
+// node whose body is one sweep plus the stop rule evaluated on the device.
+// Sizes are read on the device, so one graph serves every level held in the
+// same buffers.
+struct StageGraphKey {
+    const rmx::Level *lv;
+    const rmx::ModState *M;
+    const rmx::InstState *I;
+    int allow_new, prior, max_iter, nsub;
+    double vthresh, threshold;
+    const void *gtable;
+    int64_t gcap;
+    int tuning_gen;
+    size_t scratch_mark;  // the scratch the body's primitives use starts here
+    bool operator==(const StageGraphKey &o) const {
+        return lv == o.lv && M == o.M && I == o.I && allow_new == o.allow_new && prior == o.prior &&
+               max_iter == o.max_iter && nsub == o.nsub && vthresh == o.vthresh && threshold == o.threshold &&
+               gtable == o.gtable && gcap == o.gcap && tuning_gen == o.tuning_gen && scratch_mark == o.scratch_mark;
+    }
+};
+struct StageGraph {
+    StageGraphKey key;
+    cudaGraphExec_t exec;
+    unsigned long long kernels;  // kernel nodes of one sweep of the body
+};
+
 struct rmx_graph {
     // ---- host-side description
     int32_t N = 0;
@@ -101,6 +127,14 @@ struct rmx_graph {
     bool use_graphs = RMX_USE_GRAPHS != 0;
     int64_t runs_done = 0;  // completed optimiser runs (attempts) on this handle
     std::vector<SweepGraph> sweep_graphs;
+    std::vector<StageGraph> stage_graphs;
+    // device state of a captured stage loop: [0] sweep number, [1] sub-batch
+    // stamp, [2] attempt seed, [3] sweeps run, [4] instances still sweeping,
+    // [5] units of the level
+    int64_t *stage_ctl = nullptr;
+    uint32_t *stage_seed = nullptr;      // the current sweep's seed
+    uint8_t *stage_sweeping = nullptr;   // per instance: still sweeping
+    double *stage_oldL = nullptr;        // per instance: code length before the current sweep
 
     // ---- state
     bool initiated = false;
@@ -154,6 +188,9 @@ struct rmx_graph {
     void stage_sweeps(rmx::Level &lv, bool allow_new, std::vector<double> &L, const std::vector<uint8_t> &act);
     void sweep_single(rmx::Level &lv, bool prior, bool allow_new, double vthresh, int64_t &n_active,
                       std::vector<double> &L);
+    bool stage_graph_ok(const rmx::Level &lv) const;
+    void stage_sweeps_graph(rmx::Level &lv, bool allow_new, std::vector<double> &L, const std::vector<uint8_t> &act);
+    void stage_body(rmx::Level &lv, bool allow_new, bool prior, double vthresh, int ns, unsigned long long cond);
     void set_active(const std::vector<uint8_t> &m);
     void run_subbatches(rmx::Level &lv, int64_t n_active, rmx::ModState &M, rmx::InstState &I,
                         const rmx::SweepArgs &sa, int ns, bool mark, uint32_t seed);

@@ -329,14 +329,25 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
 #pragma unroll
         for (int k = 0; k < RMX_EVAL_ILP; k++)
             if (key[k] >= 0) key[k] = __ldg(a.mod + key[k]);
+        // first probes of all keys issued together, then each key's collisions
+        int slot[RMX_EVAL_ILP];
+        int32_t prev[RMX_EVAL_ILP];
 #pragma unroll
-        for (int k = 0; k < RMX_EVAL_ILP; k++) {
-            const int64_t j = j0 + (int64_t)k * NT;
-            if (j < d) {
-                const int s = tab_insert(keys, mask, key[k]);
-                atomic_add_fx(j < dout ? vo + s : vi + s, q[k]);
+        for (int k = 0; k < RMX_EVAL_ILP; k++)
+            if (key[k] >= 0) {
+                slot[k] = tab_slot(key[k], mask);
+                prev[k] = atomicCAS(keys + slot[k], kEmpty, key[k]);
             }
-        }
+#pragma unroll
+        for (int k = 0; k < RMX_EVAL_ILP; k++)
+            if (key[k] >= 0) {
+                // capacity >= 2 x the unit's links: a free slot exists, probing stays below mask steps
+                for (int probe = 0; prev[k] != kEmpty && prev[k] != key[k] && probe < mask; probe++) {
+                    slot[k] = (slot[k] + 1) & mask;
+                    prev[k] = atomicCAS(keys + slot[k], kEmpty, key[k]);
+                }
+                atomic_add_fx(j0 + (int64_t)k * NT < dout ? vo + slot[k] : vi + slot[k], q[k]);
+            }
     }
     gsync<NT>();
     const int32_t A = a.mod[u];
@@ -1170,8 +1181,9 @@ struct BinBounds {
 };
 
 __global__ void k_bucket(const int32_t *list, const int64_t *n_active, const int64_t *out_off, const int64_t *in_off,
-                         uint32_t seed, int nsub, BinBounds bb, uint16_t *bucket) {
+                         uint32_t seed, const uint32_t *seed_dev, int nsub, BinBounds bb, uint16_t *bucket) {
     const int64_t n = *n_active;
+    if (seed_dev) seed = *seed_dev;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int32_t u = list[i];
         const int64_t d = (out_off[u + 1] - out_off[u]) + (in_off[u + 1] - in_off[u]);
@@ -1202,7 +1214,7 @@ void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed,
     const EvalTuning t = eval_tuning();
     const BinBounds bb{t.warp_max, t.mid_max, t.block_max, t.large_max};
     k_bucket<<<blocks_for(n_active, 256, num_sms() * 32), 256, 0, s>>>(W.list, W.counters + kCntActive, L.out_off,
-                                                                       L.in_off, seed, nsub, bb, W.bucket);
+                                                                       L.in_off, seed, nullptr, nsub, bb, W.bucket);
     RMX_LAUNCHED();
     bucket_partition(W.bucket, W.list, W.list2, n_active, nsub * kBins, W.bucket_off, ar, s);
     k_ranges<<<1, 128, 0, s>>>(W.bucket_off, nsub, W.ranges);
@@ -1213,6 +1225,32 @@ void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed,
     RMX_CUDA(cudaMemcpyAsync(W.bucket_host.data(), W.bucket_off, sizeof(int64_t) * W.bucket_host.size(),
                              cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));
+}
+
+void bucket_units_dev(const Level &L, SweepWork &W, int64_t n_max, const uint32_t *seed_dev, int nsub, Arena &ar,
+                      cudaStream_t s) {
+    if (nsub * kBins > 256) throw std::invalid_argument("too many sub-batches");
+    const EvalTuning t = eval_tuning();
+    const BinBounds bb{t.warp_max, t.mid_max, t.block_max, t.large_max};
+    k_bucket<<<blocks_for(n_max, 256, num_sms() * 32), 256, 0, s>>>(W.list, W.counters + kCntActive, L.out_off,
+                                                                    L.in_off, 0u, seed_dev, nsub, bb, W.bucket);
+    RMX_LAUNCHED();
+    bucket_partition_dev(W.bucket, W.list, W.list2, W.counters + kCntActive, n_max, nsub * kBins, W.bucket_off, ar,
+                         s);
+    k_ranges<<<1, 128, 0, s>>>(W.bucket_off, nsub, W.ranges);
+    RMX_LAUNCHED();
+}
+
+__global__ void k_iota_dev(int32_t *list, const int64_t *n_dev, int64_t *count) {
+    const int64_t n = *n_dev;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        list[i] = (int32_t)i;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *count = n;
+}
+
+void all_units_dev(const int64_t *n_dev, int64_t n_max, SweepWork &W, cudaStream_t s) {
+    k_iota_dev<<<blocks_for(n_max, 256, num_sms() * 32), 256, 0, s>>>(W.list, n_dev, W.counters + kCntActive);
+    RMX_LAUNCHED();
 }
 
 __global__ void k_empty_flags(int32_t cap, const int32_t *mcount, uint8_t *flag) {

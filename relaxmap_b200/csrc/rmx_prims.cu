@@ -252,8 +252,9 @@ void scan_exclusive(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *tota
 
 // ------------------------------------------------------------- compaction
 
-__global__ void k_flag_count(const uint8_t *flags, int64_t n, long long *bsum) {
+__global__ void k_flag_count(const uint8_t *flags, int64_t n, const int64_t *n_dev, long long *bsum) {
     __shared__ long long ws[32];
+    if (n_dev) n = *n_dev;
     int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanI;
     long long c = 0;
 #pragma unroll
@@ -264,8 +265,10 @@ __global__ void k_flag_count(const uint8_t *flags, int64_t n, long long *bsum) {
     if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
 }
 
-__global__ void k_flag_scatter(const uint8_t *flags, int64_t n, const long long *boff, int32_t *out) {
+__global__ void k_flag_scatter(const uint8_t *flags, int64_t n, const int64_t *n_dev, const long long *boff,
+                               int32_t *out) {
     __shared__ long long ws[32];
+    if (n_dev) n = *n_dev;
     int64_t base = (int64_t)blockIdx.x * kScanTile + (int64_t)threadIdx.x * kScanI;
     uint8_t f[kScanI];
     long long c = 0;
@@ -281,7 +284,8 @@ __global__ void k_flag_scatter(const uint8_t *flags, int64_t n, const long long 
         if (f[i]) out[pre++] = (int32_t)(base + i);
 }
 
-void compact_flags(const uint8_t *flags, int64_t n, int32_t *out, int64_t *count, Arena &ar, cudaStream_t s) {
+static void compact_impl(const uint8_t *flags, int64_t n, const int64_t *n_dev, int32_t *out, int64_t *count,
+                         Arena &ar, cudaStream_t s) {
     if (n <= 0) {
         RMX_CUDA(cudaMemsetAsync(count, 0, sizeof(int64_t), s));
         return;
@@ -289,12 +293,21 @@ void compact_flags(const uint8_t *flags, int64_t n, int32_t *out, int64_t *count
     size_t m = ar.mark();
     int64_t nb = (n + kScanTile - 1) / kScanTile;
     long long *bsum = ar.alloc<long long>(nb);
-    k_flag_count<<<(unsigned)nb, kScanT, 0, s>>>(flags, n, bsum);
+    k_flag_count<<<(unsigned)nb, kScanT, 0, s>>>(flags, n, n_dev, bsum);
     RMX_LAUNCHED();
     scan_impl<long long>(bsum, bsum, nb, reinterpret_cast<long long *>(count), ar, s);
-    k_flag_scatter<<<(unsigned)nb, kScanT, 0, s>>>(flags, n, bsum, out);
+    k_flag_scatter<<<(unsigned)nb, kScanT, 0, s>>>(flags, n, n_dev, bsum, out);
     RMX_LAUNCHED();
     ar.release(m);
+}
+
+void compact_flags(const uint8_t *flags, int64_t n, int32_t *out, int64_t *count, Arena &ar, cudaStream_t s) {
+    compact_impl(flags, n, nullptr, out, count, ar, s);
+}
+
+void compact_flags_dev(const uint8_t *flags, const int64_t *n_dev, int64_t n_max, int32_t *out, int64_t *count,
+                       Arena &ar, cudaStream_t s) {
+    compact_impl(flags, n_max, n_dev, out, count, ar, s);
 }
 
 // ------------------------------------------------------------- radix sort
@@ -317,8 +330,10 @@ struct ArrDigit {
 };
 
 template <typename Dig>
-__global__ void __launch_bounds__(kRsT) k_rs_hist(Dig dig, int64_t n, int nb, unsigned *hist, int64_t ntiles) {
+__global__ void __launch_bounds__(kRsT) k_rs_hist(Dig dig, int64_t n, const int64_t *n_dev, int nb, unsigned *hist,
+                                                  int64_t ntiles) {
     __shared__ unsigned cnt[256];
+    if (n_dev) n = *n_dev;
     for (int i = threadIdx.x; i < nb; i += kRsT) cnt[i] = 0;
     __syncthreads();
     int64_t base = (int64_t)blockIdx.x * kRsTile;
@@ -333,8 +348,10 @@ __global__ void __launch_bounds__(kRsT) k_rs_hist(Dig dig, int64_t n, int nb, un
 
 template <typename Dig, typename K, typename V>
 __global__ void __launch_bounds__(kRsT) k_rs_scatter(Dig dig, const K *kin, K *kout, const V *vin, V *vout, int64_t n,
-                                                     int nb, const unsigned *offs, int64_t ntiles) {
+                                                     const int64_t *n_dev, int nb, const unsigned *offs,
+                                                     int64_t ntiles) {
     __shared__ unsigned run[256];
+    if (n_dev) n = *n_dev;
     __shared__ unsigned wc[kRsW][256];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < 256; i += kRsT) {
@@ -386,10 +403,10 @@ void radix_sort_pairs(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32
         int bits = std::min(8, key_bits - shift);
         int nb = 1 << bits;
         KeyDigit dig{ks, shift, (unsigned)nb - 1u};
-        k_rs_hist<<<(unsigned)ntiles, kRsT, 0, s>>>(dig, n, nb, hist, ntiles);
+        k_rs_hist<<<(unsigned)ntiles, kRsT, 0, s>>>(dig, n, nullptr, nb, hist, ntiles);
         RMX_LAUNCHED();
         scan_impl<unsigned>(hist, hist, (int64_t)nb * ntiles, nullptr, ar, s);
-        k_rs_scatter<<<(unsigned)ntiles, kRsT, 0, s>>>(dig, ks, kd, vs, vd, n, nb, hist, ntiles);
+        k_rs_scatter<<<(unsigned)ntiles, kRsT, 0, s>>>(dig, ks, kd, vs, vd, n, nullptr, nb, hist, ntiles);
         RMX_LAUNCHED();
         std::swap(ks, kd);
         std::swap(vs, vd);
@@ -401,14 +418,15 @@ void radix_sort_pairs(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32
     ar.release(m);
 }
 
-__global__ void k_bucket_bounds(const unsigned *offs, int64_t ntiles, int nb, int64_t n, int64_t *bucket_off) {
+__global__ void k_bucket_bounds(const unsigned *offs, int64_t ntiles, int nb, int64_t n, const int64_t *n_dev,
+                                int64_t *bucket_off) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < nb) bucket_off[i] = offs[(int64_t)i * ntiles];
-    if (i == nb) bucket_off[nb] = n;
+    if (i == nb) bucket_off[nb] = n_dev ? *n_dev : n;
 }
 
-void bucket_partition(const uint16_t *bucket, const int32_t *vals_in, int32_t *vals_out, int64_t n, int nb,
-                      int64_t *bucket_off, Arena &ar, cudaStream_t s) {
+static void bucket_impl(const uint16_t *bucket, const int32_t *vals_in, int32_t *vals_out, int64_t n,
+                        const int64_t *n_dev, int nb, int64_t *bucket_off, Arena &ar, cudaStream_t s) {
     if (nb < 1 || nb > 256) throw std::invalid_argument("bucket_partition: 1..256 buckets");
     if (n <= 0) {
         RMX_CUDA(cudaMemsetAsync(bucket_off, 0, sizeof(int64_t) * (nb + 1), s));
@@ -418,15 +436,25 @@ void bucket_partition(const uint16_t *bucket, const int32_t *vals_in, int32_t *v
     size_t m = ar.mark();
     unsigned *hist = ar.alloc<unsigned>((size_t)nb * ntiles);
     ArrDigit dig{bucket};
-    k_rs_hist<<<(unsigned)ntiles, kRsT, 0, s>>>(dig, n, nb, hist, ntiles);
+    k_rs_hist<<<(unsigned)ntiles, kRsT, 0, s>>>(dig, n, n_dev, nb, hist, ntiles);
     RMX_LAUNCHED();
     scan_impl<unsigned>(hist, hist, (int64_t)nb * ntiles, nullptr, ar, s);
     k_rs_scatter<ArrDigit, int32_t, int32_t>
-        <<<(unsigned)ntiles, kRsT, 0, s>>>(dig, nullptr, nullptr, vals_in, vals_out, n, nb, hist, ntiles);
+        <<<(unsigned)ntiles, kRsT, 0, s>>>(dig, nullptr, nullptr, vals_in, vals_out, n, n_dev, nb, hist, ntiles);
     RMX_LAUNCHED();
-    k_bucket_bounds<<<1, 288, 0, s>>>(hist, ntiles, nb, n, bucket_off);
+    k_bucket_bounds<<<1, 288, 0, s>>>(hist, ntiles, nb, n, n_dev, bucket_off);
     RMX_LAUNCHED();
     ar.release(m);
+}
+
+void bucket_partition(const uint16_t *bucket, const int32_t *vals_in, int32_t *vals_out, int64_t n, int nb,
+                      int64_t *bucket_off, Arena &ar, cudaStream_t s) {
+    bucket_impl(bucket, vals_in, vals_out, n, nullptr, nb, bucket_off, ar, s);
+}
+
+void bucket_partition_dev(const uint16_t *bucket, const int32_t *vals_in, int32_t *vals_out, const int64_t *n_dev,
+                          int64_t n_max, int nb, int64_t *bucket_off, Arena &ar, cudaStream_t s) {
+    bucket_impl(bucket, vals_in, vals_out, n_max, n_dev, nb, bucket_off, ar, s);
 }
 
 }  // namespace rmx

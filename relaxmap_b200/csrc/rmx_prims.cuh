@@ -40,6 +40,11 @@ void scan_exclusive(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *tota
 
 // Indices i (ascending) with flags[i] != 0 written to out; *count (device).
 void compact_flags(const uint8_t *flags, int64_t n, int32_t *out, int64_t *count, Arena &ar, cudaStream_t s);
+// The same over the first *n_dev flags (device, at most n_max): grids are
+// sized for n_max, so the launches do not depend on the count (the form a
+// captured graph replays with changing sizes).
+void compact_flags_dev(const uint8_t *flags, const int64_t *n_dev, int64_t n_max, int32_t *out, int64_t *count,
+                       Arena &ar, cudaStream_t s);
 
 // Stable sort of (key, value) pairs by key bits [0, key_bits). Sorted data ends
 // in keys/vals (the alt buffers are scratch of the same size).
@@ -51,5 +56,8 @@ void radix_sort_pairs(uint64_t *keys, uint32_t *vals, uint64_t *keys_alt, uint32
 // (device, nb+1 entries) receives the bucket boundaries.
 void bucket_partition(const uint16_t *bucket, const int32_t *vals_in, int32_t *vals_out, int64_t n, int nb,
                       int64_t *bucket_off, Arena &ar, cudaStream_t s);
+// The same for the first *n_dev items (device, at most n_max), grids sized for n_max.
+void bucket_partition_dev(const uint16_t *bucket, const int32_t *vals_in, int32_t *vals_out, const int64_t *n_dev,
+                          int64_t n_max, int nb, int64_t *bucket_off, Arena &ar, cudaStream_t s);
 
 }  // namespace rmx

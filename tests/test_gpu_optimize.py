@@ -90,3 +90,26 @@ def test_synthetic_vs_oracle_codelength(built_lib, oracle_mod):
     # the planted partition is a good solution; the optimiser must match or beat it
     L_planted = O.codelength(prep, st, sg.community)
     assert r["L"] <= L_planted * 1.005
+
+
+@pytest.mark.parametrize("prior", [1, 0])
+def test_captured_stage_loops_match_host_loops(built_lib, prior):
+    """From a handle's second run on, every stage loop of sweeps runs as one
+    CUDA graph: a while node whose body is one sweep followed by the stop rule
+    evaluated on the device. The first run, and runs with profiling on, drive
+    the loop from the host. Both give the same partition, code length,
+    per-superstep code lengths and number of sweeps."""
+    from relaxmap_b200 import Graph, synth
+    g = synth.config_mid(seed=9, n=20_000)
+    with Graph.from_edges(g.src, g.dst, g.w, n=g.n) as G:
+        G.set_profiling(True)  # host-driven loops, direct launches
+        ref = G.optimize(seed=4, prior=prior)
+        ref_sweeps = G.profile()["sweeps"]
+        G.set_profiling(False)
+        for _ in range(2):  # the first captures the stage graphs, the second replays them
+            s0 = G.profile()["sweeps"]
+            r = G.optimize(seed=4, prior=prior)
+            np.testing.assert_array_equal(r["part"], ref["part"])
+            assert r["L"] == ref["L"]
+            np.testing.assert_array_equal(r["steps_bits"], ref["steps_bits"])
+            assert G.profile()["sweeps"] - s0 == ref_sweeps
