@@ -7,6 +7,7 @@
 // one small device->host read (code length, moved nodes, next active count),
 // the only synchronisation inside the loop.
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstring>
 
@@ -953,9 +954,41 @@ void rmx_graph::stage_sweeps_graph(Level &lv, bool allow_new, std::vector<double
     const double vthresh = prior ? -opt.vthresh : 0.0;  // OmpRelaxmap.cpp:66, Module.cpp:1490 vs :1127
     if (!any_set(act) || opt.max_iter <= 0) return;
     const int ns = sub_batches_for(lv.n);
-    const StageGraphKey key{&lv,      &mods,     &inst1,       allow_new ? 1 : 0, prior ? 1 : 0,
-                            opt.max_iter, ns,    vthresh,      opt.threshold,     work.gtable,
-                            work.gcap, eval_tuning_generation(), scratch.mark()};
+    const StageGraphKey key{&lv,          &mods, &inst1,   allow_new ? 1 : 0, prior ? 1 : 0,
+                            opt.max_iter, ns,    vthresh,  opt.threshold,     work.gtable,
+                            work.gcap,    eval_tuning_generation(), scratch.mark()};
+    RMX_CUDA(cudaMemcpyAsync(stage_sweeping, act.data(), (size_t)K, cudaMemcpyHostToDevice, stream));
+    loop_graph(key, lv.n, [&](unsigned long long cond) { stage_body(lv, allow_new, prior, vthresh, ns, cond); });
+    RMX_CUDA(cudaMemcpyAsync(L.data(), inst1.L, sizeof(double) * K, cudaMemcpyDeviceToHost, stream));
+    RMX_CUDA(cudaStreamSynchronize(stream));
+}
+
+// One sweep of the coarse-tune sub-problems (generate_sub_modules) as the
+// body of the while node, and their stop rule (k_inst_stop) on the device.
+void rmx_graph::subtune_body(int ns, unsigned long long cond) {
+    k_stage_begin<<<1, 32, 0, stream>>>(stage_ctl, stage_seed, ns, work.dparams, 0, nullptr, nullptr, nullptr,
+                                        nullptr);
+    RMX_LAUNCHED();
+    all_units_dev(stage_ctl + 5, N, work, stream);
+    bucket_units_dev(sub_lv, work, N, stage_seed, ns, scratch, stream);
+    SweepArgs sa{0.0, 0};  // Network::move: best < 0, no empty module (Module.cpp:606, :667)
+    for (int sb = 0; sb < ns; sb++)
+        sweep_subbatch(sub_lv, submods, instsub, work, sa, sb, work.dparams + 2 * sb, false, false, stream, nullptr);
+    instance_codelength(submods, instsub, stream);
+    k_inst_stop<<<blocks_for(N, 256, num_sms() * 8), 256, 0, stream>>>(
+        N, instsub.L, instsub.L_prev, instsub.active, opt.threshold, kLn2,
+        reinterpret_cast<unsigned long long *>(stage_ctl + 4));
+    RMX_LAUNCHED();
+    k_stage_cond<<<1, 1, 0, stream>>>(stage_ctl, opt.max_iter, (cudaGraphConditionalHandle)cond);
+    RMX_LAUNCHED();
+}
+
+// Runs a loop of sweeps as one graph: captured once per key (a while node
+// whose body `body` enqueues, given the node's condition handle), launched
+// with the host's sweep number, stamp and attempt seed and the level's size
+// in stage_ctl, which come back with the number of sweeps run.
+void rmx_graph::loop_graph(const StageGraphKey &key, int64_t n_level,
+                           const std::function<void(unsigned long long)> &body) {
     StageGraph *gr = nullptr;
     for (StageGraph &g : stage_graphs)
         if (g.key == key) gr = &g;
@@ -987,11 +1020,11 @@ void rmx_graph::stage_sweeps_graph(Level &lv, bool allow_new, std::vector<double
             cp.conditional.size = 1;
             cudaGraphNode_t node;
             RMX_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
-            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            cudaGraph_t bg = cp.conditional.phGraph_out[0];
             const unsigned long long c0 = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
-            RMX_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+            RMX_CUDA(cudaStreamBeginCaptureToGraph(stream, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
             try {
-                stage_body(lv, allow_new, prior, vthresh, ns, (unsigned long long)cond);
+                body((unsigned long long)cond);
             } catch (...) {
                 cudaGraph_t g2 = nullptr;
                 cudaStreamEndCapture(stream, &g2);
@@ -1011,13 +1044,10 @@ void rmx_graph::stage_sweeps_graph(Level &lv, bool allow_new, std::vector<double
         stage_graphs.push_back({key, exec, kernels});
         gr = &stage_graphs.back();
     }
-    // host loop state in, the loop on the device, state out (staged from
-    // pageable memory: the host arrays are free again when the calls return)
-    int64_t ctl[6] = {(int64_t)sweep_no, (int64_t)stamp, (int64_t)run_seed, 0, 0, (int64_t)lv.n};
+    // staged from pageable memory: ctl is free again when the copies return
+    int64_t ctl[6] = {(int64_t)sweep_no, (int64_t)stamp, (int64_t)run_seed, 0, 0, n_level};
     RMX_CUDA(cudaMemcpyAsync(stage_ctl, ctl, sizeof ctl, cudaMemcpyHostToDevice, stream));
-    RMX_CUDA(cudaMemcpyAsync(stage_sweeping, act.data(), (size_t)K, cudaMemcpyHostToDevice, stream));
     RMX_CUDA(cudaGraphLaunch(gr->exec, stream));
-    RMX_CUDA(cudaMemcpyAsync(L.data(), inst1.L, sizeof(double) * K, cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaMemcpyAsync(ctl, stage_ctl, sizeof ctl, cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaStreamSynchronize(stream));
     sweep_no = (uint64_t)ctl[0];
@@ -1125,7 +1155,13 @@ void rmx_graph::generate_sub_modules() {
         Timers *tm = timers.on ? &timers : nullptr;
         SweepArgs sa{0.0, 0};  // Network::move: best < 0, no empty module (Module.cpp:606, :667)
         timers.begin(kTimerLvSub, stream);
-        for (int iter = 0; iter < opt.max_iter; iter++) {
+        const int nsg = sub_batches_for(N);
+        if (stage_graph_ok(sub_lv) && opt.max_iter > 0) {
+            const StageGraphKey key{&sub_lv, &submods, &instsub, 0, 0, opt.max_iter, nsg, 0.0, opt.threshold,
+                                    work.gtable, work.gcap, eval_tuning_generation(), scratch.mark()};
+            loop_graph(key, N, [&](unsigned long long cond) { subtune_body(nsg, cond); });
+        }
+        for (int iter = 0; iter < opt.max_iter && !stage_graph_ok(sub_lv); iter++) {
             all_units(N, work, stream);
             const uint32_t seed = mix_seed(run_seed, ++sweep_no);
             const int ns = sub_batches_for(N);

@@ -1,6 +1,7 @@
 // The opaque handle behind the C ABI: one graph resident on one device, its
 // CUDA stream, the device arenas, and the engine state of the optimiser.
 #pragma once
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -191,6 +192,8 @@ struct rmx_graph {
     bool stage_graph_ok(const rmx::Level &lv) const;
     void stage_sweeps_graph(rmx::Level &lv, bool allow_new, std::vector<double> &L, const std::vector<uint8_t> &act);
     void stage_body(rmx::Level &lv, bool allow_new, bool prior, double vthresh, int ns, unsigned long long cond);
+    void subtune_body(int ns, unsigned long long cond);
+    void loop_graph(const StageGraphKey &key, int64_t n_level, const std::function<void(unsigned long long)> &body);
     void set_active(const std::vector<uint8_t> &m);
     void run_subbatches(rmx::Level &lv, int64_t n_active, rmx::ModState &M, rmx::InstState &I,
                         const rmx::SweepArgs &sa, int ns, bool mark, uint32_t seed);
