@@ -915,10 +915,12 @@ void rmx_graph::stage_sweeps(Level &lv, bool allow_new, std::vector<double> &L, 
 }
 
 // The stage loop runs as one captured graph once the handle has completed a
-// run (as the sweep pipelines: capture costs more than one cold run saves),
-// without profiling events and without per-sweep printing.
+// run (as the sweep pipelines: capture costs more than one cold run of a
+// single graph saves), or from the first run of a union of instances (a
+// batch wave, whose many sweeps each save a host round trip); never with
+// profiling events or per-sweep printing.
 bool rmx_graph::stage_graph_ok(const Level &lv) const {
-    return use_graphs && runs_done > 0 && !timers.on && opt.verbose < 2 && lv.n > 0;
+    return use_graphs && (runs_done > 0 || K > 1) && !timers.on && opt.verbose < 2 && lv.n > 0;
 }
 
 // One sweep of stage_sweeps as the body of the while node: the host loop's

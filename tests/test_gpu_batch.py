@@ -100,3 +100,20 @@ def test_batch_rejects_bad_input(built_lib):
         Batch([(3, np.array([0, 3], np.int32), np.array([1, 2], np.int32), None)])
     with pytest.raises(RmxError):
         Batch([(0, np.zeros(0, np.int32), np.zeros(0, np.int32), None)])
+
+
+def test_batch_captured_loops_match_host_loops(built_lib, capfd):
+    """A batch wave (a union of graph-attempt instances) runs its stage loops
+    as captured while graphs from its first run; with per-sweep printing
+    (verbose 2) the same loops are driven from the host. Same partitions, code
+    lengths and best attempts."""
+    from relaxmap_b200 import Batch
+    gs = _graphs()
+    with Batch(gs) as B:
+        a = B.optimize(seed=2, attempts=3)
+        b = B.optimize(seed=2, attempts=3, verbose=2)
+    capfd.readouterr()  # the host loop's per-sweep lines
+    np.testing.assert_array_equal(a["L"], b["L"])
+    np.testing.assert_array_equal(a["best_attempt"], b["best_attempt"])
+    for pa, pb in zip(a["part"], b["part"]):
+        np.testing.assert_array_equal(pa, pb)
