@@ -157,15 +157,50 @@ CsrBuild build_csr(int32_t n, int64_t n_edges, int32_t *d_src, int32_t *d_dst, d
 
 // ------------------------------------------------------------ normalise
 
+// Per-row kernels take 32 consecutive rows per warp: a lane handles a row of
+// up to kRowSeqMax links by itself, in link order (the reference's order);
+// heavier rows (R-MAT hubs reach 10^5-10^6 links) are then taken by the whole
+// warp one at a time, lanes striding the links, so that no lane walks a hub
+// while the rest of the grid has finished.
+constexpr int64_t kRowSeqMax = 256;
+
+// Sum over the warp in a fixed butterfly order: every lane gets the same value.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// Row sums and normalised weights (Module.cpp:237-247: sum of the out-link
+// weights in link order, then each weight divided by it; a heavy row's sum is
+// formed by the warp, which rounds differently in the last bits).
 __global__ void k_normalise_rows(int32_t n, const int64_t *off, const double *w0, double *wn, double *rowsum,
                                  uint8_t *dangling) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int64_t b = off[i], e = off[i + 1];
-        double s = 0.0;
-        for (int64_t j = b; j < e; j++) s += w0[j];
-        for (int64_t j = b; j < e; j++) wn[j] = w0[j] / s;
-        rowsum[i] = s;
-        dangling[i] = (b == e) ? 1 : 0;
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = gw * 32; base < n; base += nw * 32) {
+        const int64_t i = base + lane;
+        bool heavy = false;
+        if (i < n) {
+            const int64_t b = off[i], e = off[i + 1];
+            heavy = e - b > kRowSeqMax;
+            if (!heavy) {
+                double s = 0.0;
+                for (int64_t j = b; j < e; j++) s += w0[j];
+                for (int64_t j = b; j < e; j++) wn[j] = w0[j] / s;
+                rowsum[i] = s;
+            }
+            dangling[i] = (b == e) ? 1 : 0;
+        }
+        for (unsigned hv = __ballot_sync(kFull, heavy); hv; hv &= hv - 1) {
+            const int64_t r = base + __ffs(hv) - 1;
+            const int64_t b = off[r], e = off[r + 1];
+            double s = 0.0;
+            for (int64_t j = b + lane; j < e; j += 32) s += w0[j];
+            s = warp_sum(s);
+            for (int64_t j = b + lane; j < e; j += 32) wn[j] = w0[j] / s;
+            if (lane == 0) rowsum[r] = s;
+        }
     }
 }
 
@@ -180,7 +215,7 @@ void normalise(int32_t n, const int64_t *out_off, const double *out_w0, double *
                cudaStream_t s, bool cols) {
     size_t mk = ar.mark();
     double *rowsum = ar.alloc<double>(std::max(n, 1));
-    k_normalise_rows<<<blocks_for(n, 128, num_sms() * 16), 128, 0, s>>>(n, out_off, out_w0, out_f, rowsum, dangling);
+    k_normalise_rows<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, out_off, out_w0, out_f, rowsum, dangling);
     RMX_LAUNCHED();
     int64_t m = 0;
     if (cols) {
@@ -605,30 +640,61 @@ int power_iteration(int32_t n, const int64_t *in_off, const int32_t *in_src, con
 
 // ------------------------------------------------------------ flows
 
+// Edge flows f = p_u * w~ (Module.cpp:275-286) in FP64 and fixed point, and
+// each node's unit statistics; the out-flow sum is a fixed-point (exact,
+// order-free) sum, so heavy rows done by the whole warp give the same bits.
 __global__ void k_flow_rows(int32_t n, const int64_t *off, double *f, fx_t *fx, const double *p, const double *tw,
                             const uint8_t *dangling, Stat4 *attr, fx_t *s0) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     fx_t s0l = 0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double pi = p[i];
+    for (int64_t base = gw * 32; base < n; base += nw * 32) {
+        const int64_t i = base + lane;
+        bool heavy = false;
         fx_t out = 0;
-        for (int64_t j = off[i]; j < off[i + 1]; j++) {
-            const double v = pi * f[j];  // Module.cpp:280
-            f[j] = v;
-            const fx_t q = to_fx(v);
-            fx[j] = q;
-            out += q;
+        if (i < n) {
+            const int64_t b = off[i], e = off[i + 1];
+            heavy = e - b > kRowSeqMax;
+            const double pi = p[i];
+            if (!heavy)
+                for (int64_t j = b; j < e; j++) {
+                    const double v = pi * f[j];  // Module.cpp:280
+                    f[j] = v;
+                    const fx_t q = to_fx(v);
+                    fx[j] = q;
+                    out += q;
+                }
+            s0l += to_fxl(plogp(pi));
         }
-        Stat4 a;
-        a.P = to_fx(pi);
-        a.TW = to_fx(tw[i]);
-        a.D = dangling[i] ? a.P : 0;
-        a.OUT = out;
-        attr[i] = a;
-        s0l += to_fxl(plogp(pi));
+        for (unsigned hv = __ballot_sync(kFull, heavy); hv; hv &= hv - 1) {
+            const int src = __ffs(hv) - 1;
+            const int64_t r = base + src;
+            const int64_t b = off[r], e = off[r + 1];
+            const double pr = p[r];
+            fx_t o = 0;
+            for (int64_t j = b + lane; j < e; j += 32) {
+                const double v = pr * f[j];
+                f[j] = v;
+                const fx_t q = to_fx(v);
+                fx[j] = q;
+                o += q;
+            }
+#pragma unroll
+            for (int q = 16; q > 0; q >>= 1) o += __shfl_xor_sync(kFull, o, q);
+            if (lane == src) out = o;
+        }
+        if (i < n) {
+            Stat4 a;
+            a.P = to_fx(p[i]);
+            a.TW = to_fx(tw[i]);
+            a.D = dangling[i] ? a.P : 0;
+            a.OUT = out;
+            attr[i] = a;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s0l += __shfl_xor_sync(kFull, s0l, o);
-    if ((threadIdx.x & 31) == 0 && s0l != 0) atomic_add_fx(s0, s0l);
+    if (lane == 0 && s0l != 0) atomic_add_fx(s0, s0l);
 }
 
 __global__ void k_flow_cols(int64_t m, const int32_t *in_src, const double *in_w, const double *p, fx_t *in_fx) {
@@ -640,7 +706,7 @@ void edge_flows(int32_t n, int64_t m, const int64_t *out_off, double *out_f, fx_
                 const double *in_w, fx_t *in_fx, const double *p, const double *tw, const uint8_t *dangling,
                 Stat4 *attr, fx_t *s0_acc, cudaStream_t s) {
     RMX_CUDA(cudaMemsetAsync(s0_acc, 0, sizeof(fx_t), s));
-    k_flow_rows<<<blocks_for(n, 128, num_sms() * 16), 128, 0, s>>>(n, out_off, out_f, out_fx, p, tw, dangling, attr,
+    k_flow_rows<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, out_off, out_f, out_fx, p, tw, dangling, attr,
                                                                    s0_acc);
     RMX_LAUNCHED();
     if (m > 0) {
@@ -649,19 +715,37 @@ void edge_flows(int32_t n, int64_t m, const int64_t *out_off, double *out_f, fx_
     }
 }
 
-// Singleton exit exactly as Module::Module(int, Node*) (Module.cpp:76-95).
+// Singleton exit as Module::Module(int, Node*) (Module.cpp:76-95): the
+// out-flow summed in link order, by the warp for heavy rows.
 __global__ void k_singleton_exit(int32_t n, const int64_t *off, const double *f, const double *p, const double *tw,
                                  const uint8_t *dangling, double *ex) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = gw * 32; base < n; base += nw * 32) {
+        const int64_t i = base + lane;
+        bool heavy = false;
         double s = 0.0;
-        for (int64_t j = off[i]; j < off[i + 1]; j++) s += f[j];
-        ex[i] = dangling[i] ? (1.0 - tw[i]) * p[i] : kAlpha * (1.0 - tw[i]) * p[i] + kBeta * s;
+        if (i < n) {
+            const int64_t b = off[i], e = off[i + 1];
+            heavy = e - b > kRowSeqMax;
+            if (!heavy)
+                for (int64_t j = b; j < e; j++) s += f[j];
+        }
+        for (unsigned hv = __ballot_sync(kFull, heavy); hv; hv &= hv - 1) {
+            const int src = __ffs(hv) - 1;
+            const int64_t r = base + src;
+            double t = 0.0;
+            for (int64_t j = off[r] + lane; j < off[r + 1]; j += 32) t += f[j];
+            t = warp_sum(t);
+            if (lane == src) s = t;
+        }
+        if (i < n) ex[i] = dangling[i] ? (1.0 - tw[i]) * p[i] : kAlpha * (1.0 - tw[i]) * p[i] + kBeta * s;
     }
 }
 
 void singleton_exits(int32_t n, const int64_t *out_off, const double *out_f, const double *p, const double *tw,
                      const uint8_t *dangling, double *exitpr, cudaStream_t s) {
-    k_singleton_exit<<<blocks_for(n, 128, num_sms() * 16), 128, 0, s>>>(n, out_off, out_f, p, tw, dangling, exitpr);
+    k_singleton_exit<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, out_off, out_f, p, tw, dangling, exitpr);
     RMX_LAUNCHED();
 }
 
