@@ -442,32 +442,65 @@ __global__ void __launch_bounds__(kAggT, 2) k_agg_block(AggArgs a) {
     }
 }
 
-__global__ void k_agg_pack(int32_t ng, const int64_t *gloff, const int64_t *g_out_off, const int32_t *slab_dst,
-                           const fx_t *slab_fx, int32_t *out_dst, fx_t *out_fx, unsigned long long *colcnt) {
+// Row of link e in the offsets off[0..ng]: each warp takes 32 consecutive
+// links; lane 0 finds the first link's row by binary search, and every lane
+// walks forward from there (rows in a chunk are few unless they are tiny).
+// So the work per warp is the same whatever the rows' lengths (a group of a
+// million links does not keep one warp busy).
+__device__ __forceinline__ int32_t row_of_chunk(const int64_t *off, int32_t ng, int64_t e0, int64_t e) {
+    int32_t r = 0;
+    if ((threadIdx.x & 31) == 0) {
+        int32_t lo = 0, hi = ng - 1;
+        while (lo < hi) {
+            const int32_t mid = lo + ((hi - lo + 1) >> 1);
+            if (off[mid] <= e0)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        r = lo;
+    }
+    r = __shfl_sync(kFullMask, r, 0);
+    while (off[r + 1] <= e) r++;
+    return r;
+}
+
+// Packed rows: the slab entries of row g (at gloff[g]) move to the CSR
+// position g_out_off[g]; columns are counted for the transpose.
+__global__ void k_agg_pack(int32_t ng, int64_t m, const int64_t *gloff, const int64_t *g_out_off,
+                           const int32_t *slab_dst, const fx_t *slab_fx, int32_t *out_dst, fx_t *out_fx,
+                           unsigned long long *colcnt) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t g = gw; g < ng; g += nw) {
-        const int64_t src = gloff[g], o = g_out_off[g], len = g_out_off[g + 1] - o;
-        for (int64_t j = lane; j < len; j += 32) {
-            const int32_t b = slab_dst[src + j];
-            out_dst[o + j] = b;
-            out_fx[o + j] = slab_fx[src + j];
+    for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {
+        const int64_t e = e0 + lane;
+        const int32_t g = row_of_chunk(g_out_off, ng, e0, e < m ? e : e0);
+        if (e < m) {
+            const int64_t src = gloff[g] + (e - g_out_off[g]);
+            const int32_t b = slab_dst[src];
+            out_dst[e] = b;
+            out_fx[e] = slab_fx[src];
             atomicAdd(colcnt + b, 1ull);
         }
     }
 }
 
-__global__ void k_agg_transpose(int32_t ng, const int64_t *g_out_off, const int32_t *out_dst, const fx_t *out_fx,
-                                const int64_t *g_in_off, unsigned long long *colfill, int32_t *in_src, fx_t *in_fx) {
+// In-links: every link u->b of the group CSR appended to column b.
+__global__ void k_agg_transpose(int32_t ng, int64_t m, const int64_t *g_out_off, const int32_t *out_dst,
+                                const fx_t *out_fx, const int64_t *g_in_off, unsigned long long *colfill,
+                                int32_t *in_src, fx_t *in_fx) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t g = gw; g < ng; g += nw)
-        for (int64_t e = g_out_off[g] + lane; e < g_out_off[g + 1]; e += 32) {
+    for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {
+        const int64_t e = e0 + lane;
+        const int32_t g = row_of_chunk(g_out_off, ng, e0, e < m ? e : e0);
+        if (e < m) {
             const int32_t b = out_dst[e];
             const int64_t q = g_in_off[b] + (int64_t)atomicAdd(colfill + b, 1ull);
-            in_src[q] = (int32_t)g;
+            in_src[q] = g;
             in_fx[q] = out_fx[e];
         }
+    }
 }
 
 // The block bin's dynamic shared memory, set once per device.
@@ -495,7 +528,6 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     if (rowsum) RMX_CUDA(cudaMemsetAsync(rowsum, 0, sizeof(fx_t) * std::max(ng, 1), s));
     if (ng <= 0) return 0;
     size_t mk = ar.mark();
-    const unsigned G = num_sms() * 16;
     int64_t *gmoff = ar.alloc<int64_t>(ng + 1), *gloff = ar.alloc<int64_t>(ng + 1);
     unsigned long long *fill = ar.alloc<unsigned long long>(ng + 1);
     int64_t *tot = ar.alloc<int64_t>(8);
@@ -583,16 +615,23 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
             RMX_CUDA(cudaStreamWaitEvent(s, W->join[k], 0));
         }
     scan_exclusive(rowlen, g_out_off, ng + 1, tot + 2, ar, s);
-    RMX_CUDA(cudaMemsetAsync(g_in_off, 0, sizeof(int64_t) * (ng + 1), s));
-    k_agg_pack<<<G, 256, 0, s>>>(ng, gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx,
-                                 reinterpret_cast<unsigned long long *>(g_in_off));
-    RMX_LAUNCHED();
-    scan_exclusive(g_in_off, g_in_off, ng + 1, nullptr, ar, s);
-    RMX_CUDA(cudaMemsetAsync(fill, 0, sizeof(unsigned long long) * (ng + 1), s));
-    k_agg_transpose<<<G, 256, 0, s>>>(ng, g_out_off, g_out_dst, g_out_fx, g_in_off, fill, g_in_src, g_in_fx);
-    RMX_LAUNCHED();
     int64_t m = 0;
     RMX_CUDA(cudaMemcpyAsync(&m, tot + 2, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaMemsetAsync(g_in_off, 0, sizeof(int64_t) * (ng + 1), s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    if (m > 0) {
+        const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
+        k_agg_pack<<<Gm, 256, 0, s>>>(ng, m, gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx,
+                                      reinterpret_cast<unsigned long long *>(g_in_off));
+        RMX_LAUNCHED();
+    }
+    scan_exclusive(g_in_off, g_in_off, ng + 1, nullptr, ar, s);
+    RMX_CUDA(cudaMemsetAsync(fill, 0, sizeof(unsigned long long) * (ng + 1), s));
+    if (m > 0) {
+        const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
+        k_agg_transpose<<<Gm, 256, 0, s>>>(ng, m, g_out_off, g_out_dst, g_out_fx, g_in_off, fill, g_in_src, g_in_fx);
+        RMX_LAUNCHED();
+    }
     RMX_CUDA(cudaStreamSynchronize(s));
     ar.release(mk);
     return m;
