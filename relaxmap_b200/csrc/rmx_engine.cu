@@ -696,8 +696,17 @@ void rmx_graph::ensure_hub_table(int64_t maxdeg) {
     work.gtable = nullptr;
     work.gkeys = nullptr;
     work.gcap = 0;
-    const int64_t hb = hub_blocks(), slots = hub_slots(cap);
-    hub_arena.init((size_t)(sizeof(fx_t) * 2 + sizeof(int32_t)) * slots * hb + 1024);
+    work.hub_nblk = 0;
+    const int64_t slots = hub_slots(cap);
+    const size_t per_block = (size_t)(sizeof(fx_t) * 2 + sizeof(int32_t)) * slots;
+    // as many slices as the hub bin runs blocks, fewer (one per SM) when that
+    // would take more than half of the free device memory
+    int64_t hb = hub_blocks_max();
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && per_block * hb > free_b / 2)
+        hb = std::max<int64_t>(num_sms(), 1);
+    hub_arena.init(per_block * hb + 1024);
+    work.hub_nblk = (int)hb;
     work.gtable = hub_arena.alloc<fx_t>(2 * slots * hb);
     work.gkeys = hub_arena.alloc<int32_t>(slots * hb);
     work.gcap = cap;

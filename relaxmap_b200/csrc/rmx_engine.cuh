@@ -170,9 +170,10 @@ struct SweepWork {
     int32_t *free_list = nullptr;
     unsigned long long *claim = nullptr;        // per module id
     int64_t *counters = nullptr;
-    fx_t *gtable = nullptr;                     // hub hash tables: hub_blocks() slices of
+    fx_t *gtable = nullptr;                     // hub hash tables: hub_nblk slices of
     int32_t *gkeys = nullptr;                   //   hub_slots(gcap) entries
     int64_t gcap = 0;
+    int hub_nblk = 0;                           // blocks of the hub bin (one slice each)
     std::vector<int64_t> bucket_host;  // host copy of bucket_off after bucket_units
     uint32_t *dparams = nullptr;       // device {stamp, hseed} per sub-batch of the current sweep
     uint32_t hparams[64] = {};         // host staging of dparams
@@ -181,7 +182,8 @@ struct SweepWork {
 };
 
 void configure_eval_kernels();
-int hub_blocks();
+// Blocks the hub bin runs at most (RMX_HUB_PER_SM per SM).
+int hub_blocks_max();
 
 // Launch shape of move evaluation, process-wide and read at every launch:
 // the grid cap of each bin in blocks per SM, and the degree bounds that

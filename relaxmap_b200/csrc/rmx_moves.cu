@@ -27,6 +27,10 @@
 
 #include "rmx_engine.cuh"
 
+// blocks per SM of the hub bin (each with its own global table slice)
+#ifndef RMX_HUB_PER_SM
+#define RMX_HUB_PER_SM 2
+#endif
 // links each thread of a shared-table bin gathers ahead of its table inserts
 #ifndef RMX_EVAL_ILP
 #define RMX_EVAL_ILP 1
@@ -600,7 +604,11 @@ __global__ void __launch_bounds__(kEvalWarps * 32, RMX_WARP_MINB) k_eval_warp(Ev
 }
 
 template <int NT, int CAP, bool GLOBAL>
-__global__ void __launch_bounds__(NT, NT >= 512 ? 1 : (NT == 128 ? 8 : RMX_BLK_MINB)) k_eval_block(EvalArgs a) {
+// The hub bin (GLOBAL: tables in global memory, no shared table) runs two
+// 512-thread blocks per SM (64 registers); the shared-table bins are limited by
+// their tables.
+__global__ void __launch_bounds__(NT, NT >= 512 ? (GLOBAL ? RMX_HUB_PER_SM : 1) : (NT == 128 ? 8 : RMX_BLK_MINB))
+    k_eval_block(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ GroupShared<NT> sh;
     int32_t *keys;
@@ -1028,7 +1036,7 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     return a;
 }
 
-int hub_blocks() { return num_sms(); }
+int hub_blocks_max() { return RMX_HUB_PER_SM * num_sms(); }
 
 namespace {
 EvalTuning g_tuning{8, RMX_BLK_GRID, 1, RMX_WARP_GRID, RMX_REG_GRID, kWarpMaxDeg, kMidMaxDeg, kBlkMaxDeg, kLrgMaxDeg};
@@ -1114,10 +1122,10 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
         RMX_LAUNCHED();
         if (tm) tm->end(kTimerBinLarge, on(1));
     }
-    if (n_hub > 0) {  // global table slices are indexed by block: at most hub_blocks() blocks
+    if (n_hub > 0) {  // global table slices are indexed by block: at most W.hub_nblk blocks
         a.range = bucket_off + first_bucket + kBinHub;
         if (tm) tm->begin(kTimerBinHub, on(1));
-        k_eval_block<kHubT, 0, true><<<fit_grid(n_hub, 1, hub_blocks()), kHubT, 0, on(1)>>>(a);
+        k_eval_block<kHubT, 0, true><<<fit_grid(n_hub, 1, W.hub_nblk), kHubT, 0, on(1)>>>(a);
         RMX_LAUNCHED();
         if (tm) tm->end(kTimerBinHub, on(1));
     }
