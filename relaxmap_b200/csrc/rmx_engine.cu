@@ -710,6 +710,9 @@ void rmx_graph::ensure_hub_table(int64_t maxdeg) {
     work.gtable = hub_arena.alloc<fx_t>(2 * slots * hb);
     work.gkeys = hub_arena.alloc<int32_t>(slots * hb);
     work.gcap = cap;
+    // the slices start empty; every unit the hub bin evaluates leaves its slice empty again
+    RMX_CUDA(cudaMemsetAsync(work.gtable, 0, sizeof(fx_t) * 2 * slots * hb, stream));
+    RMX_CUDA(cudaMemsetAsync(work.gkeys, 0xff, sizeof(int32_t) * slots * hb, stream));
 }
 
 void rmx_graph::initiate() {

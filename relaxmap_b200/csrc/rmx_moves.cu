@@ -306,12 +306,9 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
     int64_t cap = 32;
     while (cap < 2 * d) cap <<= 1;
     const int mask = (int)(cap - 1);
-    for (int64_t s = r; s < cap; s += NT) {
-        keys[s] = kEmpty;
-        vo[s] = 0;
-        vi[s] = 0;
-    }
-    gsync<NT>();
+    // The table is empty on entry: cleared once when the kernel starts (shared
+    // tables) or when it is allocated (global slices), and every unit leaves
+    // it empty again (below), so no clearing pass runs per unit.
     // Each thread takes links r, r + NT, ...; RMX_EVAL_ILP of them at a time
     // have their neighbour ids, flows and then neighbour modules loaded before
     // any is inserted, so that many gathers are in flight per thread.
@@ -360,7 +357,9 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
     const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
     if (NT > 32) __syncthreads();  // every lookup is done before slots are overwritten
     // Each warp compacts its own contiguous slice of the table in place (the
-    // dense position never passes the slot being read) and evaluates it.
+    // dense position never passes the slot being read) and evaluates it. A
+    // slot left beyond the dense prefix is emptied at once; the prefix is
+    // emptied as its candidates are evaluated.
     const int64_t seg = cap / (NT / 32), lo = (int64_t)(r >> 5) * seg, hi = lo + seg;
     int nc = 0;
     for (int64_t base = lo; base < hi; base += 32) {
@@ -382,13 +381,22 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
             ci[p] = i2;
         }
         nc += __popc(bal);
+        if (k != kEmpty && s >= lo + nc) {  // not overwritten by the dense prefix
+            keys[s] = kEmpty;
+            vo[s] = 0;
+            vi[s] = 0;
+        }
     }
     __syncwarp();
     double best = 0.0;
     int32_t bm = INT_MAX;
     for (int q = lane; q < nc; q += 32) {
         const int32_t m = ck[lo + q];
-        const double dl = candidate_delta(c, a.mstat[m], a.mterm[m], co[lo + q], ci[lo + q]);
+        const fx_t o = co[lo + q], i2 = ci[lo + q];
+        ck[lo + q] = kEmpty;
+        co[lo + q] = 0;
+        ci[lo + q] = 0;
+        const double dl = candidate_delta(c, a.mstat[m], a.mterm[m], o, i2);
         if (better(dl, m, best, bm)) {
             best = dl;
             bm = m;
@@ -591,6 +599,12 @@ __global__ void __launch_bounds__(kEvalWarps * 32, RMX_WARP_MINB) k_eval_warp(Ev
     const int64_t beg = a.range[0], end = a.range[1];
     const int64_t gw = (int64_t)blockIdx.x * kEvalWarps + w, nw = (int64_t)gridDim.x * kEvalWarps;
     unsigned long long seen = 0, units = 0, cands = 0;
+    for (int s = lane; s < kWarpCap; s += 32) {  // every unit leaves its table empty again
+        skey[w][s] = kEmpty;
+        sout[w][s] = 0;
+        sin_[w][s] = 0;
+    }
+    __syncwarp();
     for (int64_t i = beg + gw; i < end; i += nw) {
         const int32_t u = a.list[i];
         if (!a.inst_active[a.uinst[u]]) {
@@ -622,6 +636,12 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? (GLOBAL ? RMX_HUB_PER_SM : 1) 
         vo = reinterpret_cast<fx_t *>(dsm);
         vi = vo + CAP;
         keys = reinterpret_cast<int32_t *>(vi + CAP);
+        for (int s = threadIdx.x; s < CAP; s += NT) {  // every unit leaves its table empty again
+            keys[s] = kEmpty;
+            vo[s] = 0;
+            vi[s] = 0;
+        }
+        __syncthreads();
     }
     const int64_t beg = a.range[0], end = a.range[1];
     unsigned long long seen = 0, units = 0, cands = 0;
