@@ -33,11 +33,11 @@
 #endif
 // links each thread of a shared-table bin gathers ahead of its table inserts
 #ifndef RMX_EVAL_ILP
-#define RMX_EVAL_ILP 1
+#define RMX_EVAL_ILP 4
 #endif
 // the total-exit term of every candidate through log1p of a per-unit log (1) or a log each (0)
 #ifndef RMX_LOG1P
-#define RMX_LOG1P 0
+#define RMX_LOG1P 1
 #endif
 
 namespace rmx {
