@@ -264,7 +264,15 @@ constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
 #ifndef RMX_DELTA_MINB
 #define RMX_DELTA_MINB 6
 #endif
-constexpr int kLrgT = 512, kLrgMaxDeg = 4096, kLrgCap = 8192;
+// the large bin's shared table (slots; units of up to half as many links) and
+// its resident blocks per SM
+#ifndef RMX_LRG_CAP
+#define RMX_LRG_CAP 8192
+#endif
+#ifndef RMX_LRG_MINB
+#define RMX_LRG_MINB 1
+#endif
+constexpr int kLrgT = 512, kLrgCap = RMX_LRG_CAP, kLrgMaxDeg = kLrgCap / 2;
 constexpr int kHubT = 512;
 
 __device__ __forceinline__ int tab_find(const int32_t *keys, int mask, int32_t key) {
@@ -621,7 +629,7 @@ template <int NT, int CAP, bool GLOBAL>
 // The hub bin (GLOBAL: tables in global memory, no shared table) runs two
 // 512-thread blocks per SM (64 registers); the shared-table bins are limited by
 // their tables.
-__global__ void __launch_bounds__(NT, NT >= 512 ? (GLOBAL ? RMX_HUB_PER_SM : 1) : (NT == 128 ? 8 : RMX_BLK_MINB))
+__global__ void __launch_bounds__(NT, NT >= 512 ? (GLOBAL ? RMX_HUB_PER_SM : RMX_LRG_MINB) : (NT == 128 ? 8 : RMX_BLK_MINB))
     k_eval_block(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ GroupShared<NT> sh;
@@ -1059,7 +1067,7 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
 int hub_blocks_max() { return RMX_HUB_PER_SM * num_sms(); }
 
 namespace {
-EvalTuning g_tuning{8, RMX_BLK_GRID, 1, RMX_WARP_GRID, RMX_REG_GRID, kWarpMaxDeg, kMidMaxDeg, kBlkMaxDeg, kLrgMaxDeg};
+EvalTuning g_tuning{8, RMX_BLK_GRID, RMX_LRG_MINB, RMX_WARP_GRID, RMX_REG_GRID, kWarpMaxDeg, kMidMaxDeg, kBlkMaxDeg, kLrgMaxDeg};
 int g_tuning_gen = 0;
 std::mutex g_tuning_mu;  // guards g_tuning and g_tuning_gen
 }  // namespace
