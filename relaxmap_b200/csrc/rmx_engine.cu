@@ -471,14 +471,11 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
             if (b) throw std::invalid_argument("edge endpoint outside 0..N-1");
     }
     N = n;
-    node_w.assign(n, 1.0);
-    tot_w = (double)n;  // FileIO.cpp:229
+    tot_w = (double)n;  // FileIO.cpp:229: every node weighs 1 unless the file gives weights
     if (node_weights) {
+        node_w.assign(node_weights, node_weights + n);
         tot_w = 0.0;
-        for (int32_t i = 0; i < n; i++) {
-            node_w[i] = node_weights[i];
-            tot_w += node_weights[i];
-        }
+        for (int32_t i = 0; i < n; i++) tot_w += node_weights[i];
     }
     if (u) {  // a disjoint union of instances: node ranges, canonical copies
         if (u->K < 1 || (int64_t)u->inst_noff[u->K] != n || u->inst_noff[0] != 0)
@@ -493,7 +490,7 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     const int64_t Ein = std::max<int64_t>(n_edges, 1), Eb = std::max<int64_t>(repl ? u->full_edges : n_edges, 1);
     scratch.init((size_t)(88 * Eb + 24 * (int64_t)n + 40 * (int64_t)K) + (64u << 20));
     // long-lived arrays: node CSR/CSC, three levels, module and instance state
-    perm.init((size_t)(144 * Eb + 560 * (int64_t)n + (K > 1 ? 16 * (int64_t)n + 64 * (int64_t)K : 0)) + (64u << 20));
+    perm.init((size_t)(144 * Eb + 568 * (int64_t)n + (K > 1 ? 16 * (int64_t)n + 64 * (int64_t)K : 0)) + (64u << 20));
     out_off = perm.alloc<int64_t>(n + 1);
     in_off = perm.alloc<int64_t>(n + 1);
     int32_t *d_src = scratch.alloc<int32_t>(Ein), *d_dst = scratch.alloc<int32_t>(Ein);
@@ -564,22 +561,31 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     tw = perm.alloc<double>(n);
     p = perm.alloc<double>(n);
     dangling = perm.alloc<uint8_t>(n);
-    std::vector<double> twh(n);
-    if (K == 1) {
-        for (int32_t i = 0; i < n; i++) twh[i] = node_w[i] / tot_w;  // OmpRelaxmap.cpp:113-115
-    } else {  // teleportation normalised within every instance
-        for (int32_t k = 0; k < K; k++) {
-            double t = node_weights ? 0.0 : (double)(inst_noff[k + 1] - inst_noff[k]);
-            if (node_weights)
-                for (int64_t i = inst_noff[k]; i < inst_noff[k + 1]; i++) t += node_w[i];
-            for (int64_t i = inst_noff[k]; i < inst_noff[k + 1]; i++) twh[i] = node_w[i] / t;
+    // teleport weights w_i / sum w (OmpRelaxmap.cpp:113-115), within every instance of a union
+    if (K == 1 && !node_weights) {
+        k_fill<<<blocks_for(n, 256, 4096), 256, 0, stream>>>(tw, n, 1.0 / tot_w);
+        RMX_LAUNCHED();
+    } else {
+        std::vector<double> twh(n);
+        auto nw = [&](int64_t i) { return node_weights ? node_w[i] : 1.0; };
+        if (K == 1) {
+            for (int32_t i = 0; i < n; i++) twh[i] = nw(i) / tot_w;
+        } else {
+            for (int32_t k = 0; k < K; k++) {
+                double t = node_weights ? 0.0 : (double)(inst_noff[k + 1] - inst_noff[k]);
+                if (node_weights)
+                    for (int64_t i = inst_noff[k]; i < inst_noff[k + 1]; i++) t += node_w[i];
+                for (int64_t i = inst_noff[k]; i < inst_noff[k + 1]; i++) twh[i] = nw(i) / t;
+            }
         }
+        RMX_CUDA(cudaMemcpyAsync(tw, twh.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream));
+        RMX_CUDA(cudaStreamSynchronize(stream));  // twh is a local pageable buffer
     }
-    RMX_CUDA(cudaMemcpyAsync(tw, twh.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream));
     nattr = perm.alloc<Stat4>(n);
     nmod = perm.alloc<int32_t>(n);
     zeros = perm.alloc<int32_t>(n);
     node_sn = perm.alloc<int32_t>(n);
+    best_part = perm.alloc<int32_t>(n);
     submod = perm.alloc<int32_t>(n);
     s0 = perm.alloc<fx_t>(1);
     RMX_CUDA(cudaMemsetAsync(zeros, 0, sizeof(int32_t) * n, stream));
@@ -927,12 +933,14 @@ void rmx_graph::stage_sweeps(Level &lv, bool allow_new, std::vector<double> &L, 
 }
 
 // The stage loop runs as one captured graph once the handle has completed a
-// run (as the sweep pipelines: capture costs more than one cold run of a
-// single graph saves), or from the first run of a union of instances (a
-// batch wave, whose many sweeps each save a host round trip); never with
+// run (as the sweep pipelines: on a small graph capture costs more than one
+// cold run saves), or from the first run of a union of instances (a batch
+// wave, whose many sweeps each save a host round trip) or of a graph of at
+// least 2^22 links (a few captures are small next to its run); never with
 // profiling events or per-sweep printing.
 bool rmx_graph::stage_graph_ok(const Level &lv) const {
-    return use_graphs && (runs_done > 0 || K > 1) && !timers.on && opt.verbose < 2 && lv.n > 0;
+    return use_graphs && (runs_done > 0 || K > 1 || E >= (int64_t(1) << 22)) && !timers.on && opt.verbose < 2 &&
+           lv.n > 0;
 }
 
 // One sweep of stage_sweeps as the body of the while node: the host loop's
@@ -1341,18 +1349,23 @@ double rmx_graph::optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modu
     RMX_CUDA(cudaEventRecord(t0, stream));
     initiate();
     double best = INFINITY;
-    std::vector<int32_t> part(N);
+    int32_t best_nm = 0;
     std::vector<double> best_steps;
+    // the best attempt's partition stays on the device and is copied out once at the end
     for (int a = 0; a < opt.attempts; a++) {
         const double L = run_attempt(opt.seed + (uint32_t)a)[0];
         if (L < best) {
             best = L;
             best_steps = step_bits;
-            RMX_CUDA(cudaMemcpyAsync(part.data(), nmod, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, stream));
-            RMX_CUDA(cudaStreamSynchronize(stream));
+            best_nm = count_modules();
+            if (opt.attempts > 1)
+                RMX_CUDA(cudaMemcpyAsync(best_part, nmod, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, stream));
         }
     }
     step_bits = best_steps;
+    if (part_out)
+        RMX_CUDA(cudaMemcpyAsync(part_out, opt.attempts > 1 ? best_part : nmod, sizeof(int32_t) * N,
+                                 cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaEventRecord(t1, stream));
     RMX_CUDA(cudaEventSynchronize(t1));
     float ms = 0;
@@ -1360,17 +1373,7 @@ double rmx_graph::optimize(const rmx_opts &o, int32_t *part_out, int32_t *n_modu
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     prof.total_ms = ms;
-    if (part_out) std::memcpy(part_out, part.data(), sizeof(int32_t) * N);
-    if (n_modules) {
-        int32_t nm = 0;
-        std::vector<uint8_t> seen(N, 0);
-        for (int32_t v = 0; v < N; v++)
-            if (!seen[part[v]]) {
-                seen[part[v]] = 1;
-                nm++;
-            }
-        *n_modules = nm;
-    }
+    if (n_modules) *n_modules = best_nm;
     if (timers.on) timers.resolve();
     return best;
 }

@@ -93,6 +93,7 @@ struct rmx_graph {
     uint8_t *dangling = nullptr;
     rmx::Stat4 *nattr = nullptr;
     int32_t *nmod = nullptr, *zeros = nullptr, *node_sn = nullptr, *submod = nullptr;
+    int32_t *best_part = nullptr;  // the best attempt's partition while later attempts run
     rmx::fx_t *s0 = nullptr;
     int64_t *dtmp = nullptr;  // small device scratch (counters)
 
