@@ -692,33 +692,42 @@ int64_t rmx_graph::max_degree(const Level &lv) {
     return (int64_t)h;
 }
 
-void rmx_graph::ensure_hub_table(int64_t maxdeg) {
-    if (maxdeg <= block_bin_max_degree()) return;
-    int64_t cap = 64;
-    while (cap < 2 * maxdeg) cap <<= 1;
-    if (cap <= work.gcap) return;
-    RMX_CUDA(cudaStreamSynchronize(stream));  // no launch still reads the old tables
+// The hub pipeline's pool of tables and plan arrays, sized for every unit of
+// lv above the large bin's bound (any sub-batch of the level fits); grown, never
+// shrunk, and left empty: every slot the pipeline uses it empties again.
+void rmx_graph::ensure_hub_table(const Level &lv) {
+    if (lv.n <= 0) return;
+    int64_t need[3];
+    hub_level_needs(lv, need, dtmp + 12, stream);
+    const int64_t units = need[0], slots = need[1], items = need[2];
+    if (units == 0 || (units <= work.hub_units && slots <= work.gcap && items <= work.hub_items)) return;
+    RMX_CUDA(cudaStreamSynchronize(stream));  // no launch still reads the old pool
     hub_arena.destroy();
+    const int64_t U = std::max(units, work.hub_units) * 5 / 4 + 16, P = std::max(slots, work.gcap) * 5 / 4 + 64,
+                  I = std::max(items, work.hub_items) * 5 / 4 + 16;
     work.gtable = nullptr;
     work.gkeys = nullptr;
-    work.gcap = 0;
-    work.hub_nblk = 0;
-    const int64_t slots = hub_slots(cap);
-    const size_t per_block = (size_t)(sizeof(fx_t) * 2 + sizeof(int32_t)) * slots;
-    // as many slices as the hub bin runs blocks, fewer (one per SM) when that
-    // would take more than half of the free device memory
-    int64_t hb = hub_blocks_max();
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && per_block * hb > free_b / 2)
-        hb = std::max<int64_t>(num_sms(), 1);
-    hub_arena.init(per_block * hb + 1024);
-    work.hub_nblk = (int)hb;
-    work.gtable = hub_arena.alloc<fx_t>(2 * slots * hb);
-    work.gkeys = hub_arena.alloc<int32_t>(slots * hb);
-    work.gcap = cap;
-    // the slices start empty; every unit the hub bin evaluates leaves its slice empty again
-    RMX_CUDA(cudaMemsetAsync(work.gtable, 0, sizeof(fx_t) * 2 * slots * hb, stream));
-    RMX_CUDA(cudaMemsetAsync(work.gkeys, 0xff, sizeof(int32_t) * slots * hb, stream));
+    work.gcap = work.hub_units = work.hub_items = 0;
+    const size_t bytes = (size_t)P * (sizeof(int32_t) + 2 * sizeof(fx_t)) + (size_t)(U + 1) * 4 * sizeof(int64_t) +
+                         (size_t)U * (2 * sizeof(fx_t) + 1) + (size_t)I * (sizeof(double) + sizeof(int32_t)) +
+                         16 * 256;
+    hub_arena.init(bytes);
+    work.gkeys = hub_arena.alloc<int32_t>(P);
+    work.gtable = hub_arena.alloc<fx_t>(2 * P);
+    work.hub_cap = hub_arena.alloc<int64_t>(U + 1);
+    work.hub_toff = hub_arena.alloc<int64_t>(U + 1);
+    work.hub_coff = hub_arena.alloc<int64_t>(U + 1);
+    work.hub_eoff = hub_arena.alloc<int64_t>(U + 1);
+    work.hub_own = hub_arena.alloc<fx_t>(2 * U);
+    work.hub_act = hub_arena.alloc<uint8_t>(U);
+    work.hub_best = hub_arena.alloc<double>(I);
+    work.hub_bmod = hub_arena.alloc<int32_t>(I);
+    work.hub_tot = hub_arena.alloc<int64_t>(4);
+    RMX_CUDA(cudaMemsetAsync(work.gkeys, 0xff, sizeof(int32_t) * P, stream));
+    RMX_CUDA(cudaMemsetAsync(work.gtable, 0, sizeof(fx_t) * 2 * P, stream));
+    work.gcap = P;
+    work.hub_units = U;
+    work.hub_items = I;
 }
 
 void rmx_graph::initiate() {
@@ -750,7 +759,7 @@ void rmx_graph::initiate() {
     RMX_CUDA(cudaMemcpyAsync(L0v.data(), inst1.L, sizeof(double) * K, cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaStreamSynchronize(stream));
     L0 = L0v[0];
-    ensure_hub_table(max_degree(node_lv));
+    ensure_hub_table(node_lv);
     initiated = true;
 }
 
@@ -907,7 +916,7 @@ void rmx_graph::stage_sweeps(Level &lv, bool allow_new, std::vector<double> &L, 
     const double vthresh = prior ? -opt.vthresh : 0.0;  // OmpRelaxmap.cpp:66, Module.cpp:1490 vs :1127
     int64_t n_active = lv.n;
     all_units(lv.n, work, stream);
-    if (lv.n > 0) ensure_hub_table(max_degree(lv));
+    if (lv.n > 0) ensure_hub_table(lv);
     if (stage_graph_ok(lv)) {
         stage_sweeps_graph(lv, allow_new, L, act);
         return;
@@ -1173,7 +1182,7 @@ void rmx_graph::generate_sub_modules() {
     RMX_CUDA(cudaStreamSynchronize(stream));
     timers.end(kTimerCoarsen, stream);
     if (sub_lv.m > 0) {
-        ensure_hub_table(max_degree(sub_lv));
+        ensure_hub_table(sub_lv);
         Timers *tm = timers.on ? &timers : nullptr;
         SweepArgs sa{0.0, 0};  // Network::move: best < 0, no empty module (Module.cpp:606, :667)
         timers.begin(kTimerLvSub, stream);
@@ -1540,7 +1549,7 @@ void rmx_graph::evaluate_sn_hook(const int32_t *part_host, int32_t n_sn, const i
     module_stats_from_units(lv, mods, stream);
     RMX_CUDA(cudaMemsetAsync(inst1.active, 1, (size_t)K, stream));
     instance_codelength(mods, inst1, stream);
-    ensure_hub_table(max_degree(lv));
+    ensure_hub_table(lv);
     evaluate_all(lv, mods, inst1, work, an, 0.0, scratch, stream);
     RMX_CUDA(cudaMemcpyAsync(best_mod, work.prop, sizeof(int32_t) * n_sn, cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaMemcpyAsync(best_delta, work.pdelta, sizeof(double) * n_sn, cudaMemcpyDeviceToHost, stream));
@@ -1562,7 +1571,7 @@ void rmx_graph::evaluate_hook(const int32_t *part_host, const uint8_t *allow_new
     module_stats_from_units(node_lv, mods, stream);
     RMX_CUDA(cudaMemsetAsync(inst1.active, 1, (size_t)K, stream));
     instance_codelength(mods, inst1, stream);
-    ensure_hub_table(max_degree(node_lv));  // the bin bounds may have changed since initiate
+    ensure_hub_table(node_lv);  // the bin bounds may have changed since initiate
     evaluate_all(node_lv, mods, inst1, work, an, 0.0, scratch, stream);
     RMX_CUDA(cudaMemcpyAsync(best_mod, work.prop, sizeof(int32_t) * N, cudaMemcpyDeviceToHost, stream));
     RMX_CUDA(cudaMemcpyAsync(best_delta, work.pdelta, sizeof(double) * N, cudaMemcpyDeviceToHost, stream));

@@ -170,10 +170,19 @@ struct SweepWork {
     int32_t *free_list = nullptr;
     unsigned long long *claim = nullptr;        // per module id
     int64_t *counters = nullptr;
-    fx_t *gtable = nullptr;                     // hub hash tables: hub_nblk slices of
-    int32_t *gkeys = nullptr;                   //   hub_slots(gcap) entries
+    // hub units (above the large bin's bound), each split over many blocks:
+    // one pool of tables (gkeys, gtable = out then in values, gcap slots) and
+    // the plan arrays, sized for every hub unit of the current level
+    fx_t *gtable = nullptr;
+    int32_t *gkeys = nullptr;
     int64_t gcap = 0;
-    int hub_nblk = 0;                           // blocks of the hub bin (one slice each)
+    int64_t hub_units = 0, hub_items = 0;       // capacities: units, table slices
+    int64_t *hub_cap = nullptr, *hub_toff = nullptr, *hub_coff = nullptr, *hub_eoff = nullptr;
+    fx_t *hub_own = nullptr;
+    double *hub_best = nullptr;
+    int32_t *hub_bmod = nullptr;
+    uint8_t *hub_act = nullptr;
+    int64_t *hub_tot = nullptr;
     std::vector<int64_t> bucket_host;  // host copy of bucket_off after bucket_units
     uint32_t *dparams = nullptr;       // device {stamp, hseed} per sub-batch of the current sweep
     uint32_t hparams[64] = {};         // host staging of dparams
@@ -182,8 +191,9 @@ struct SweepWork {
 };
 
 void configure_eval_kernels();
-// Blocks the hub bin runs at most (RMX_HUB_PER_SM per SM).
-int hub_blocks_max();
+// What the hub pipeline needs for a level: hub units (above block_bin_max_degree),
+// table slots in all, table slices (out[0..2]); one device reduction, then a sync.
+void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_t s);
 
 // Launch shape of move evaluation, process-wide and read at every launch:
 // the grid cap of each bin in blocks per SM, and the degree bounds that
@@ -205,7 +215,6 @@ void set_eval_tuning(const EvalTuning &t);
 int eval_tuning_generation();
 // Units above this degree need the hub bin's global tables.
 int64_t block_bin_max_degree();
-int64_t hub_slots(int64_t cap);
 void all_units(int32_t n, SweepWork &W, cudaStream_t s);
 // host_counts: also copy the bin offsets to W.bucket_host (one stream sync).
 void bucket_units(const Level &L, SweepWork &W, int64_t n_active, uint32_t seed, int nsub, Arena &ar, cudaStream_t s,

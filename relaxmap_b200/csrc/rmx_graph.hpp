@@ -184,7 +184,7 @@ struct rmx_graph {
 
   private:
     void alloc_engine();
-    void ensure_hub_table(int64_t max_degree);
+    void ensure_hub_table(const rmx::Level &lv);
     std::vector<double> run_attempt(uint32_t seed);
     void stage(bool fine, std::vector<double> &L, const std::vector<uint8_t> &run);
     void stage_sweeps(rmx::Level &lv, bool allow_new, std::vector<double> &L, const std::vector<uint8_t> &act);

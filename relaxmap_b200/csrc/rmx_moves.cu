@@ -27,10 +27,6 @@
 
 #include "rmx_engine.cuh"
 
-// blocks per SM of the hub bin (each with its own global table slice)
-#ifndef RMX_HUB_PER_SM
-#define RMX_HUB_PER_SM 2
-#endif
 // links each thread of a shared-table bin gathers ahead of its table inserts
 #ifndef RMX_EVAL_ILP
 #define RMX_EVAL_ILP 4
@@ -174,9 +170,6 @@ struct EvalArgs {
     int allow_new;             // stage-level switch
     const uint8_t *allow_new_unit;  // optional per-unit override (parity hook)
     int swap_guard;            // singleton min-label rule
-    fx_t *gtable;              // hub tables: [block][gcap] out, in
-    int32_t *gkeys;
-    int64_t gcap;
     uint8_t *next_active;      // prioritised mode: neighbours of units that propose a move
     int mark;
 };
@@ -273,7 +266,6 @@ constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
 #define RMX_LRG_MINB 1
 #endif
 constexpr int kLrgT = 512, kLrgCap = RMX_LRG_CAP, kLrgMaxDeg = kLrgCap / 2;
-constexpr int kHubT = 512;
 
 __device__ __forceinline__ int tab_find(const int32_t *keys, int mask, int32_t key) {
     int s = tab_slot(key, mask);
@@ -301,26 +293,16 @@ struct GroupShared {  // reductions across the warps of a block group
     int ncand;
 };
 
-// One unit evaluated by a group of NT threads (a warp or a block); r = rank.
-// The candidate list overwrites the table in place (ck == keys).
+// Inserts the unit's links j = first, first + NT, ... below end (out-links
+// first, then in-links; dout of them out) into the table keys/vo/vi keyed by
+// the neighbour's module, adding each link's fixed-point flow. RMX_EVAL_ILP
+// links at a time have their neighbour ids, flows and then neighbour modules
+// loaded before any is inserted, so that many gathers are in flight per
+// thread. Capacity >= 2 x the unit's links, so probing always finds a slot.
 template <int NT>
-__device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, const int r, int32_t *keys, fx_t *vo,
-                                          fx_t *vi, int32_t *ck, fx_t *co, fx_t *ci, GroupShared<NT> *sh,
-                                          unsigned long long &seen, unsigned long long &cands) {
-    const int lane = r & 31;
-    const unsigned lt = (1u << lane) - 1u;
-    const int64_t ob = a.out_off[u], ib = a.in_off[u];
-    const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
-    int64_t cap = 32;
-    while (cap < 2 * d) cap <<= 1;
-    const int mask = (int)(cap - 1);
-    // The table is empty on entry: cleared once when the kernel starts (shared
-    // tables) or when it is allocated (global slices), and every unit leaves
-    // it empty again (below), so no clearing pass runs per unit.
-    // Each thread takes links r, r + NT, ...; RMX_EVAL_ILP of them at a time
-    // have their neighbour ids, flows and then neighbour modules loaded before
-    // any is inserted, so that many gathers are in flight per thread.
-    for (int64_t j0 = r; j0 < d; j0 += (int64_t)RMX_EVAL_ILP * NT) {
+__device__ __forceinline__ void insert_links(const EvalArgs &a, int64_t ob, int64_t ib, int64_t dout, int64_t first,
+                                             int64_t d, int32_t *keys, fx_t *vo, fx_t *vi, int mask) {
+    for (int64_t j0 = first; j0 < d; j0 += (int64_t)RMX_EVAL_ILP * NT) {
         int32_t key[RMX_EVAL_ILP];
         fx_t q[RMX_EVAL_ILP];
 #pragma unroll
@@ -358,6 +340,25 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
                 atomic_add_fx(j0 + (int64_t)k * NT < dout ? vo + slot[k] : vi + slot[k], q[k]);
             }
     }
+}
+
+// One unit evaluated by a group of NT threads (a warp or a block); r = rank.
+// The candidate list overwrites the table in place (ck == keys).
+template <int NT>
+__device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, const int r, int32_t *keys, fx_t *vo,
+                                          fx_t *vi, int32_t *ck, fx_t *co, fx_t *ci, GroupShared<NT> *sh,
+                                          unsigned long long &seen, unsigned long long &cands) {
+    const int lane = r & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t ob = a.out_off[u], ib = a.in_off[u];
+    const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
+    int64_t cap = 32;
+    while (cap < 2 * d) cap <<= 1;
+    const int mask = (int)(cap - 1);
+    // The table is empty on entry: cleared once when the kernel starts (shared
+    // tables) or when it is allocated (global slices), and every unit leaves
+    // it empty again (below), so no clearing pass runs per unit.
+    insert_links<NT>(a, ob, ib, dout, r, d, keys, vo, vi, mask);
     gsync<NT>();
     const int32_t A = a.mod[u];
     const int sA = tab_find(keys, mask, A);
@@ -625,32 +626,22 @@ __global__ void __launch_bounds__(kEvalWarps * 32, RMX_WARP_MINB) k_eval_warp(Ev
     if (lane == 0) flush_stats(a, seen, units, cands);
 }
 
-template <int NT, int CAP, bool GLOBAL>
-// The hub bin (GLOBAL: tables in global memory, no shared table) runs two
-// 512-thread blocks per SM (64 registers); the shared-table bins are limited by
-// their tables.
-__global__ void __launch_bounds__(NT, NT >= 512 ? (GLOBAL ? RMX_HUB_PER_SM : RMX_LRG_MINB) : (NT == 128 ? 8 : RMX_BLK_MINB))
+// One unit per block of NT threads, its table of CAP slots in shared memory
+// (the mid, block and large bins; the large bin's residency is RMX_LRG_MINB).
+template <int NT, int CAP>
+__global__ void __launch_bounds__(NT, NT >= 512 ? RMX_LRG_MINB : (NT == 128 ? 8 : RMX_BLK_MINB))
     k_eval_block(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ GroupShared<NT> sh;
-    int32_t *keys;
-    fx_t *vo, *vi;
-    if (GLOBAL) {
-        const int64_t slots = a.gcap;
-        keys = a.gkeys + (int64_t)blockIdx.x * slots;
-        vo = a.gtable + (int64_t)blockIdx.x * slots * 2;
-        vi = vo + slots;
-    } else {
-        vo = reinterpret_cast<fx_t *>(dsm);
-        vi = vo + CAP;
-        keys = reinterpret_cast<int32_t *>(vi + CAP);
-        for (int s = threadIdx.x; s < CAP; s += NT) {  // every unit leaves its table empty again
-            keys[s] = kEmpty;
-            vo[s] = 0;
-            vi[s] = 0;
-        }
-        __syncthreads();
+    fx_t *vo = reinterpret_cast<fx_t *>(dsm);
+    fx_t *vi = vo + CAP;
+    int32_t *keys = reinterpret_cast<int32_t *>(vi + CAP);
+    for (int s = threadIdx.x; s < CAP; s += NT) {  // every unit leaves its table empty again
+        keys[s] = kEmpty;
+        vo[s] = 0;
+        vi[s] = 0;
     }
+    __syncthreads();
     const int64_t beg = a.range[0], end = a.range[1];
     unsigned long long seen = 0, units = 0, cands = 0;
     for (int64_t i = beg + blockIdx.x; i < end; i += gridDim.x) {
@@ -664,6 +655,285 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? (GLOBAL ? RMX_HUB_PER_SM : RMX
     }
     // every warp found its own share of the candidates; thread 0 alone counted the links
     if ((threadIdx.x & 31) == 0) flush_stats_split(a, threadIdx.x == 0 ? seen : 0, threadIdx.x == 0 ? units : 0, cands);
+}
+
+// ---------------------------------------------------------------- hub units
+// Units above the large bin's bound (R-MAT hubs and the heaviest super-nodes,
+// 10^4 to 10^6 links) are each split over many blocks instead of being one
+// block's long chain of dependent gathers and atomics: every hub unit of the
+// sub-batch gets a table of its own (next_pow2(2d) slots) in one pool, and
+//   plan    one block lays out the units' tables, link chunks (kHubCh links)
+//           and table slices (kHubSi slots) by prefix sums,
+//   insert  blocks take link chunks and insert them into their unit's table,
+//   own     the flow of each unit to and from its own module is looked up,
+//   eval    blocks take table slices, evaluate the candidates in them (and
+//           empty the slots), and keep the slice's best change,
+//   finish  a warp per unit reduces its slices' bests and decides (finish_unit),
+//   mark    in prioritised sweeps, link chunks of units that found a move
+//           mark their neighbours.
+// The pool is empty between sub-batches (every evaluated slot is emptied).
+constexpr int kHubCh = 2048;  // links per insert item
+constexpr int kHubSi = 2048;  // table slots per evaluation item
+constexpr int kHubPT = 256;   // threads per block of the pipeline
+
+struct HubPlan {
+    int64_t *cap, *toff, *coff, *eoff;  // per unit (+1): table slots, table offset, first chunk, first slice
+    fx_t *own;                          // 2 per unit: out / in flow to the unit's own module
+    double *best;                       // per slice: best change found
+    int32_t *bmod;                      // per slice: its module
+    uint8_t *act;                       // per unit: found a move below the threshold
+    int64_t *tot;                       // [0] chunks, [1] slices, [2] units, [3] over capacity
+    int32_t *keys;                      // the pool: slots keys, out, in
+    fx_t *vo, *vi;
+    int64_t max_units, max_slots, max_items;  // capacities of the arrays above
+};
+
+__device__ __forceinline__ int64_t hub_cap_of(int64_t d) {
+    int64_t c = 32;
+    while (c < 2 * d) c <<= 1;
+    return c;
+}
+
+// Largest j < n with off[j] <= x (off ascending, off[0] <= x).
+__device__ __forceinline__ int32_t hub_find(const int64_t *off, int32_t n, int64_t x) {
+    int32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int32_t mid = lo + ((hi - lo + 1) >> 1);
+        if (off[mid] <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Exclusive scan over the block (blockDim.x == 1024) of one value per thread.
+__device__ __forceinline__ long long hub_block_scan(long long v, long long *ws, long long *total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(kFull, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        long long t = ws[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(kFull, t, o);
+            if (lane >= o) t += y;
+        }
+        ws[lane] = t;
+    }
+    __syncthreads();
+    const long long pre = (w > 0 ? ws[w - 1] : 0) + x - v;
+    *total = ws[31];
+    __syncthreads();
+    return pre;
+}
+
+// The capacities are sized for every hub unit of the level, so they hold any
+// sub-batch; should they not (the bin bounds changed since they were sized),
+// nothing of the sub-batch is laid out and its hub units propose no move.
+__global__ void __launch_bounds__(1024) k_hub_plan(EvalArgs a, HubPlan p) {
+    __shared__ long long ws[32];
+    const int64_t h0 = a.range[0];
+    int64_t nu = a.range[1] - h0;
+    if (nu > p.max_units) {
+        if (threadIdx.x == 0) {
+            p.tot[0] = p.tot[1] = p.tot[2] = 0;
+            p.tot[3] = 1;
+        }
+        return;
+    }
+    long long r0 = 0, r1 = 0, r2 = 0;
+    for (int64_t base = 0; base < nu; base += 1024) {
+        const int64_t j = base + threadIdx.x;
+        long long cap = 0, nch = 0, nit = 0;
+        if (j < nu) {
+            const int32_t u = a.list[h0 + j];
+            if (a.inst_active[a.uinst[u]]) {  // inactive units take no chunk and no slice
+                const int64_t d = (a.out_off[u + 1] - a.out_off[u]) + (a.in_off[u + 1] - a.in_off[u]);
+                cap = hub_cap_of(d);
+                nch = (d + kHubCh - 1) / kHubCh;
+                nit = (cap + kHubSi - 1) / kHubSi;
+            }
+        }
+        long long t0, t1, t2;
+        const long long e0 = hub_block_scan(cap, ws, &t0);
+        const long long e1 = hub_block_scan(nch, ws, &t1);
+        const long long e2 = hub_block_scan(nit, ws, &t2);
+        if (j < nu) {
+            p.cap[j] = cap;
+            p.toff[j] = r0 + e0;
+            p.coff[j] = r1 + e1;
+            p.eoff[j] = r2 + e2;
+        }
+        r0 += t0;
+        r1 += t1;
+        r2 += t2;
+    }
+    if (threadIdx.x == 0) {
+        const bool over = r0 > p.max_slots || r2 > p.max_items;
+        p.toff[nu] = r0;
+        p.coff[nu] = r1;
+        p.eoff[nu] = r2;
+        p.tot[0] = over ? 0 : r1;
+        p.tot[1] = over ? 0 : r2;
+        p.tot[2] = over ? 0 : nu;
+        p.tot[3] = over ? 1 : 0;
+    }
+}
+
+__global__ void __launch_bounds__(kHubPT) k_hub_insert(EvalArgs a, HubPlan p) {
+    const int64_t h0 = a.range[0], total = p.tot[0];
+    const int32_t nu = (int32_t)p.tot[2];
+    for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const int32_t j = hub_find(p.coff, nu, item);
+        const int32_t u = a.list[h0 + j];
+        const int64_t ob = a.out_off[u], ib = a.in_off[u];
+        const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
+        const int64_t c0 = (item - p.coff[j]) * kHubCh, c1 = min(d, c0 + kHubCh);
+        const int64_t t = p.toff[j];
+        insert_links<kHubPT>(a, ob, ib, dout, c0 + threadIdx.x, c1, p.keys + t, p.vo + t, p.vi + t,
+                             (int)(p.cap[j] - 1));
+    }
+}
+
+__global__ void k_hub_own(EvalArgs a, HubPlan p) {
+    const int64_t h0 = a.range[0], nu = p.tot[2];
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nu; j += (int64_t)gridDim.x * blockDim.x) {
+        if (p.cap[j] == 0) continue;
+        const int32_t u = a.list[h0 + j];
+        const int64_t t = p.toff[j];
+        const int s = tab_find(p.keys + t, (int)(p.cap[j] - 1), a.mod[u]);
+        p.own[2 * j] = s >= 0 ? p.vo[t + s] : 0;
+        p.own[2 * j + 1] = s >= 0 ? p.vi[t + s] : 0;
+    }
+}
+
+__global__ void __launch_bounds__(kHubPT, 4) k_hub_eval(EvalArgs a, HubPlan p) {
+    __shared__ double sb[kHubPT / 32];
+    __shared__ int32_t sm[kHubPT / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t h0 = a.range[0], total = p.tot[1];
+    const int32_t nu = (int32_t)p.tot[2];
+    unsigned long long cands = 0;
+    for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const int32_t j = hub_find(p.eoff, nu, item);
+        const int32_t u = a.list[h0 + j];
+        const int64_t t = p.toff[j], s0 = (item - p.eoff[j]) * kHubSi, s1 = min(p.cap[j], s0 + kHubSi);
+        const int32_t A = a.mod[u];
+        const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, p.own[2 * j],
+                                   p.own[2 * j + 1]);
+        double best = 0.0;
+        int32_t bm = INT_MAX;
+        for (int64_t s = s0 + threadIdx.x; s < s1; s += kHubPT) {
+            const int32_t k = p.keys[t + s];
+            if (k == kEmpty) continue;
+            const fx_t o = p.vo[t + s], i2 = p.vi[t + s];
+            p.keys[t + s] = kEmpty;  // the pool is left empty for the next sub-batch
+            p.vo[t + s] = 0;
+            p.vi[t + s] = 0;
+            if (k == A) continue;
+            cands++;
+            const double dl = candidate_delta(c, a.mstat[k], a.mterm[k], o, i2);
+            if (better(dl, k, best, bm)) {
+                best = dl;
+                bm = k;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob2 = __shfl_xor_sync(kFull, best, o);
+            const int32_t om = __shfl_xor_sync(kFull, bm, o);
+            if (better(ob2, om, best, bm)) {
+                best = ob2;
+                bm = om;
+            }
+        }
+        if (lane == 0) {
+            sb[w] = best;
+            sm[w] = bm;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int q = 1; q < kHubPT / 32; q++)
+                if (better(sb[q], sm[q], best, bm)) {
+                    best = sb[q];
+                    bm = sm[q];
+                }
+            p.best[item] = best;
+            p.bmod[item] = bm;
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cands += __shfl_xor_sync(kFull, cands, o);
+    if (lane == 0 && cands) atomicAdd(a.stats + 2, cands);
+}
+
+__global__ void k_hub_finish(EvalArgs a, HubPlan p) {
+    const int lane = threadIdx.x & 31;
+    const int64_t h0 = a.range[0], nu = p.tot[2];
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long seen = 0, units = 0;
+    if (p.tot[3]) {  // not laid out (over capacity): no proposals
+        for (int64_t i = h0 + gw * 32 + lane; i < a.range[1]; i += nw * 32) a.prop[a.list[i]] = -1;
+        return;
+    }
+    for (int64_t j = gw; j < nu; j += nw) {
+        const int32_t u = a.list[h0 + j];
+        if (p.cap[j] == 0) {  // its instance has stopped
+            if (lane == 0) {
+                a.prop[u] = -1;
+                p.act[j] = 0;
+            }
+            continue;
+        }
+        double best = 0.0;
+        int32_t bm = INT_MAX;
+        for (int64_t q = p.eoff[j] + lane; q < p.eoff[j + 1]; q += 32)
+            if (better(p.best[q], p.bmod[q], best, bm)) {
+                best = p.best[q];
+                bm = p.bmod[q];
+            }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob2 = __shfl_xor_sync(kFull, best, o);
+            const int32_t om = __shfl_xor_sync(kFull, bm, o);
+            if (better(ob2, om, best, bm)) {
+                best = ob2;
+                bm = om;
+            }
+        }
+        if (lane == 0) {
+            const int32_t A = a.mod[u];
+            const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A,
+                                       p.own[2 * j], p.own[2 * j + 1]);
+            p.act[j] = (uint8_t)finish_unit(a, u, c, best, bm);
+            seen += (a.out_off[u + 1] - a.out_off[u]) + (a.in_off[u + 1] - a.in_off[u]);
+            units++;
+        }
+    }
+    if (lane == 0) flush_stats_split(a, seen, units, 0);
+}
+
+__global__ void __launch_bounds__(kHubPT) k_hub_mark(EvalArgs a, HubPlan p) {
+    const int64_t h0 = a.range[0], total = p.tot[0];
+    const int32_t nu = (int32_t)p.tot[2];
+    for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const int32_t j = hub_find(p.coff, nu, item);
+        if (!p.act[j]) continue;
+        const int32_t u = a.list[h0 + j];
+        const int64_t ob = a.out_off[u], ib = a.in_off[u];
+        const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
+        const int64_t c0 = (item - p.coff[j]) * kHubCh, c1 = min(d, c0 + kHubCh);
+        for (int64_t l = c0 + threadIdx.x; l < c1; l += kHubPT)
+            a.next_active[l < dout ? a.out_dst[ob + l] : a.in_src[ib + (l - dout)]] = 1;
+    }
 }
 
 // ---------------------------------------------------------------- commit
@@ -1056,15 +1326,44 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     a.allow_new = allow_new;
     a.allow_new_unit = allow_unit;
     a.swap_guard = swap_guard;
-    a.gtable = W.gtable;
-    a.gkeys = W.gkeys;
-    a.gcap = W.gcap;
     a.next_active = W.next_active;
     a.mark = 0;
     return a;
 }
 
-int hub_blocks_max() { return RMX_HUB_PER_SM * num_sms(); }
+__global__ void k_hub_level(int32_t n, const int64_t *out_off, const int64_t *in_off, int64_t bound,
+                            unsigned long long *acc) {
+    unsigned long long c0 = 0, c1 = 0, c2 = 0;
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t d = (out_off[u + 1] - out_off[u]) + (in_off[u + 1] - in_off[u]);
+        if (d <= bound) continue;
+        const int64_t cap = hub_cap_of(d);
+        c0++;
+        c1 += cap;
+        c2 += (cap + kHubSi - 1) / kHubSi;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        c0 += __shfl_xor_sync(kFull, c0, o);
+        c1 += __shfl_xor_sync(kFull, c1, o);
+        c2 += __shfl_xor_sync(kFull, c2, o);
+    }
+    if ((threadIdx.x & 31) == 0 && c0) {
+        atomicAdd(acc, c0);
+        atomicAdd(acc + 1, c1);
+        atomicAdd(acc + 2, c2);
+    }
+}
+
+void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_t s) {
+    unsigned long long *acc = reinterpret_cast<unsigned long long *>(dev_tmp);
+    RMX_CUDA(cudaMemsetAsync(acc, 0, 3 * sizeof(unsigned long long), s));
+    k_hub_level<<<blocks_for(L.n, 256, num_sms() * 8), 256, 0, s>>>(L.n, L.out_off, L.in_off, block_bin_max_degree(),
+                                                                    acc);
+    RMX_LAUNCHED();
+    RMX_CUDA(cudaMemcpyAsync(out, acc, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+}
 
 namespace {
 EvalTuning g_tuning{8, RMX_BLK_GRID, RMX_LRG_MINB, RMX_WARP_GRID, RMX_REG_GRID, kWarpMaxDeg, kMidMaxDeg, kBlkMaxDeg, kLrgMaxDeg};
@@ -1095,7 +1394,6 @@ int eval_tuning_generation() {
     return g_tuning_gen;
 }
 int64_t block_bin_max_degree() { return eval_tuning().large_max; }
-int64_t hub_slots(int64_t cap) { return cap; }
 
 constexpr size_t kBlkSmem = (size_t)kBlkCap * (2 * sizeof(fx_t) + sizeof(int32_t));
 constexpr size_t kMidSmem = (size_t)kMidCap * (2 * sizeof(fx_t) + sizeof(int32_t));
@@ -1116,7 +1414,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     // without host sizes every bin counts as non-empty and takes its full grid
     auto cnt = [&](int b0, int b1) { return fitted ? h[b1] - h[b0] : (int64_t)1 << 40; };
     const int64_t n_mid = cnt(kBinMid, kBinMid + 1), n_blk = cnt(kBinBlock, kBinBlock + 1),
-                  n_lrg = cnt(kBinLarge, kBinLarge + 1), n_hub = a.gcap > 0 ? cnt(kBinHub, kBinHub + 1) : 0,
+                  n_lrg = cnt(kBinLarge, kBinLarge + 1), n_hub = W.gcap > 0 ? cnt(kBinHub, kBinHub + 1) : 0,
                   n_warp = cnt(kBinWarp, kBinWarp + 1), n_reg = cnt(kBinReg8, kBinReg32 + 1);
     const bool use[4] = {n_blk > 0, n_lrg + n_hub > 0, n_warp > 0, n_mid > 0};
     const EvalTuning tg = eval_tuning();
@@ -1131,14 +1429,14 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     if (n_mid > 0) {
         a.range = bucket_off + first_bucket + kBinMid;
         if (tm) tm->begin(kTimerBinMid, on(3));
-        k_eval_block<kMidT, kMidCap, false><<<fit_grid(n_mid, 1, (int64_t)num_sms() * tg.mid), kMidT, kMidSmem, on(3)>>>(a);
+        k_eval_block<kMidT, kMidCap><<<fit_grid(n_mid, 1, (int64_t)num_sms() * tg.mid), kMidT, kMidSmem, on(3)>>>(a);
         RMX_LAUNCHED();
         if (tm) tm->end(kTimerBinMid, on(3));
     }
     if (n_blk > 0) {
         a.range = bucket_off + first_bucket + kBinBlock;
         if (tm) tm->begin(kTimerBinBlock, on(0));
-        k_eval_block<kBlkT, kBlkCap, false><<<fit_grid(n_blk, 1, (int64_t)num_sms() * tg.block), kBlkT, kBlkSmem, on(0)>>>(
+        k_eval_block<kBlkT, kBlkCap><<<fit_grid(n_blk, 1, (int64_t)num_sms() * tg.block), kBlkT, kBlkSmem, on(0)>>>(
             a);
         RMX_LAUNCHED();
         if (tm) tm->end(kTimerBinBlock, on(0));
@@ -1146,16 +1444,46 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     if (n_lrg > 0) {
         a.range = bucket_off + first_bucket + kBinLarge;
         if (tm) tm->begin(kTimerBinLarge, on(1));
-        k_eval_block<kLrgT, kLrgCap, false><<<fit_grid(n_lrg, 1, (int64_t)num_sms() * tg.large), kLrgT, kLrgSmem, on(1)>>>(a);
+        k_eval_block<kLrgT, kLrgCap><<<fit_grid(n_lrg, 1, (int64_t)num_sms() * tg.large), kLrgT, kLrgSmem, on(1)>>>(a);
         RMX_LAUNCHED();
         if (tm) tm->end(kTimerBinLarge, on(1));
     }
-    if (n_hub > 0) {  // global table slices are indexed by block: at most W.hub_nblk blocks
+    if (n_hub > 0) {  // every hub unit split over many blocks (see k_hub_plan)
         a.range = bucket_off + first_bucket + kBinHub;
-        if (tm) tm->begin(kTimerBinHub, on(1));
-        k_eval_block<kHubT, 0, true><<<fit_grid(n_hub, 1, W.hub_nblk), kHubT, 0, on(1)>>>(a);
+        HubPlan hp;
+        hp.cap = W.hub_cap;
+        hp.toff = W.hub_toff;
+        hp.coff = W.hub_coff;
+        hp.eoff = W.hub_eoff;
+        hp.own = W.hub_own;
+        hp.best = W.hub_best;
+        hp.bmod = W.hub_bmod;
+        hp.act = W.hub_act;
+        hp.tot = W.hub_tot;
+        hp.keys = W.gkeys;
+        hp.vo = W.gtable;
+        hp.vi = W.gtable + W.gcap;
+        hp.max_units = W.hub_units;
+        hp.max_slots = W.gcap;
+        hp.max_items = W.hub_items;
+        const cudaStream_t hs = on(1);
+        const unsigned G = num_sms() * 8;
+        if (tm) tm->begin(kTimerBinHub, hs);
+        k_hub_plan<<<1, 1024, 0, hs>>>(a, hp);
         RMX_LAUNCHED();
-        if (tm) tm->end(kTimerBinHub, on(1));
+        k_hub_insert<<<G, kHubPT, 0, hs>>>(a, hp);
+        RMX_LAUNCHED();
+        k_hub_own<<<blocks_for(W.hub_units, 256, num_sms() * 8), 256, 0, hs>>>(a, hp);
+        RMX_LAUNCHED();
+        k_hub_eval<<<G, kHubPT, 0, hs>>>(a, hp);
+        RMX_LAUNCHED();
+        k_hub_finish<<<blocks_for(W.hub_units * 32, 256, num_sms() * 16), 256, 0, hs>>>(a, hp);
+        RMX_LAUNCHED();
+        if (a.mark) {
+            k_hub_mark<<<G, kHubPT, 0, hs>>>(a, hp);
+            RMX_LAUNCHED();
+        }
+        if (tm) tm->end(kTimerBinHub, hs);
     }
     if (n_warp > 0) {
         a.range = bucket_off + first_bucket + kBinWarp;
@@ -1188,13 +1516,13 @@ void configure_eval_kernels() {
     std::lock_guard<std::mutex> lk(mu);
     if ((int)configured.size() <= dev) configured.resize(dev + 1, false);
     if (configured[dev]) return;
-    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, kBlkCap, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, kBlkCap>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kBlkSmem));
-    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kLrgT, kLrgCap, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kLrgT, kLrgCap>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kLrgSmem));
-    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, kBlkCap, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kBlkT, kBlkCap>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   100));
-    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kLrgT, kLrgCap, false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kLrgT, kLrgCap>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   100));
     RMX_CUDA(cudaFuncSetAttribute(k_eval_warp, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     configured[dev] = true;
