@@ -218,6 +218,30 @@ def profile_run(g, desc: str):
                       "n_modules": r["n_modules"], "profile": p}))
 
 
+def eval_bytes(links: int, units: int, cands: int, modules: int) -> float:
+    """Compulsory bytes of one evaluation launch group: 16 per link read (id,
+    fixed-point flow, neighbour's module), 40 per unit (module id, statistics,
+    proposal), 40 per module statistics record read (at most one per candidate)."""
+    return 16.0 * links + 40.0 * units + 40.0 * min(cands, modules)
+
+
+def eval_snapshot(g, desc: str):
+    """One launch group of the evaluation kernels: every node evaluated against
+    singleton modules (rmx_evaluate_moves)."""
+    import numpy as np
+
+    from relaxmap_b200 import Graph
+    G = Graph.from_edges(g.src, g.dst, g.w, n=g.n)
+    G.initiate()
+    p0 = G.profile()
+    G.evaluate_moves(np.arange(g.n, dtype=np.int32))
+    p1 = G.profile()
+    G.close()
+    d = {k: p1[k] - p0[k] for k in ("links_evaluated", "units_evaluated", "candidates_evaluated")}
+    d["bytes"] = eval_bytes(d["links_evaluated"], d["units_evaluated"], d["candidates_evaluated"], g.n)
+    print(json.dumps({"workload": desc, "nodes": g.n, "links": g.m, "eval_group": d}))
+
+
 def slowest_over_ranks(vals, pg, device):
     """Element-wise max over ranks: the slowest rank sets the job's time.
     Every rank makes this call at the same point (one all_reduce)."""
@@ -256,6 +280,10 @@ def main():
     ap.add_argument("--profile-run", action="store_true",
                     help="build the graph, then exactly one optimiser run (seed 1); prints the engine counters "
                          "(the command profiled by ncu)")
+    ap.add_argument("--eval-snapshot", action="store_true",
+                    help="build the graph, then one move evaluation of every node against singleton modules (one "
+                         "launch group of the evaluation kernels); prints its counters and compulsory bytes (the "
+                         "command whose DRAM traffic ncu measures for the roofline)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
 
@@ -295,6 +323,9 @@ def main():
     E = g.m
     if args.profile_run:
         profile_run(g, desc)
+        return
+    if args.eval_snapshot:
+        eval_snapshot(g, desc)
         return
     # ---- resident graph
     G = Graph.from_edges(g.src, g.dst, g.w, n=g.n)

@@ -171,12 +171,12 @@ struct SweepWork {
     unsigned long long *claim = nullptr;        // per module id
     int64_t *counters = nullptr;
     // hub units (above the large bin's bound), each split over many blocks:
-    // one pool of tables (gkeys, gtable = out then in values, gcap slots) and
-    // the plan arrays, sized for every hub unit of the current level
-    fx_t *gtable = nullptr;
-    int32_t *gkeys = nullptr;
+    // one pool of tables (hub_slots, gcap 32-byte slots), the taken-slot
+    // lists and the plan arrays, sized for every hub unit of the current level
+    void *hub_slots = nullptr;
     int64_t gcap = 0;
-    int64_t hub_units = 0, hub_items = 0;       // capacities: units, table slices
+    int32_t *hub_occ = nullptr, *hub_occ_n = nullptr;
+    int64_t hub_units = 0, hub_items = 0, hub_list = 0;  // capacities: units, slices, list entries
     int64_t *hub_cap = nullptr, *hub_toff = nullptr, *hub_coff = nullptr, *hub_eoff = nullptr;
     fx_t *hub_own = nullptr;
     double *hub_best = nullptr;
@@ -192,8 +192,12 @@ struct SweepWork {
 
 void configure_eval_kernels();
 // What the hub pipeline needs for a level: hub units (above block_bin_max_degree),
-// table slots in all, table slices (out[0..2]); one device reduction, then a sync.
+// table slots in all, list slices, list entries (out[0..3]); one device
+// reduction, then a sync.
 void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_t s);
+// Empties n pool slots (at allocation); bytes of one slot.
+void hub_pool_init(void *slots, int64_t n, cudaStream_t s);
+size_t hub_slot_bytes();
 
 // Launch shape of move evaluation, process-wide and read at every launch:
 // the grid cap of each bin in blocks per SM, and the degree bounds that

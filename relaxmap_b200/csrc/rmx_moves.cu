@@ -55,17 +55,6 @@ __device__ __forceinline__ uint32_t mix32(uint32_t x) {
 
 __device__ __forceinline__ int tab_slot(int32_t key, int mask) { return (int)(mix32((uint32_t)key) & (uint32_t)mask); }
 
-// Insert key (linear probing); returns its slot. Capacity >= 2 * keys inserted.
-__device__ __forceinline__ int tab_insert(int32_t *keys, int mask, int32_t key) {
-    int s = tab_slot(key, mask);
-    for (int probe = 0; probe <= mask; probe++) {
-        int32_t prev = atomicCAS(keys + s, kEmpty, key);
-        if (prev == kEmpty || prev == key) return s;
-        s = (s + 1) & mask;
-    }
-    return -1;
-}
-
 __device__ __forceinline__ bool better(double d1, int32_t m1, double d2, int32_t m2) {
     return d1 < d2 || (d1 == d2 && m1 < m2);
 }
@@ -267,10 +256,12 @@ constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
 #endif
 constexpr int kLrgT = 512, kLrgCap = RMX_LRG_CAP, kLrgMaxDeg = kLrgCap / 2;
 
+// Slot of key, or -1 (linear probing); keys[s * KS] is slot s's key.
+template <int KS = 1>
 __device__ __forceinline__ int tab_find(const int32_t *keys, int mask, int32_t key) {
     int s = tab_slot(key, mask);
     for (int probe = 0; probe <= mask; probe++) {
-        const int32_t k = keys[s];
+        const int32_t k = keys[(int64_t)s * KS];
         if (k == key) return s;
         if (k == kEmpty) return -1;
         s = (s + 1) & mask;
@@ -295,13 +286,16 @@ struct GroupShared {  // reductions across the warps of a block group
 
 // Inserts the unit's links j = first, first + NT, ... below end (out-links
 // first, then in-links; dout of them out) into the table keys/vo/vi keyed by
-// the neighbour's module, adding each link's fixed-point flow. RMX_EVAL_ILP
-// links at a time have their neighbour ids, flows and then neighbour modules
-// loaded before any is inserted, so that many gathers are in flight per
-// thread. Capacity >= 2 x the unit's links, so probing always finds a slot.
-template <int NT>
+// the neighbour's module, adding each link's fixed-point flow; slot s's key is
+// keys[s * KS], its flows vo[s * VS], vi[s * VS]. RMX_EVAL_ILP links at a time
+// have their neighbour ids, flows and then neighbour modules loaded before any
+// is inserted, so that many gathers are in flight per thread. Capacity >= 2 x
+// the unit's links, so probing always finds a slot. With occ, every slot
+// taken by a new key is appended to the list occ (count *occ_n).
+template <int NT, int KS = 1, int VS = 1>
 __device__ __forceinline__ void insert_links(const EvalArgs &a, int64_t ob, int64_t ib, int64_t dout, int64_t first,
-                                             int64_t d, int32_t *keys, fx_t *vo, fx_t *vi, int mask) {
+                                             int64_t d, int32_t *keys, fx_t *vo, fx_t *vi, int mask,
+                                             int32_t *occ = nullptr, int32_t *occ_n = nullptr) {
     for (int64_t j0 = first; j0 < d; j0 += (int64_t)RMX_EVAL_ILP * NT) {
         int32_t key[RMX_EVAL_ILP];
         fx_t q[RMX_EVAL_ILP];
@@ -327,7 +321,7 @@ __device__ __forceinline__ void insert_links(const EvalArgs &a, int64_t ob, int6
         for (int k = 0; k < RMX_EVAL_ILP; k++)
             if (key[k] >= 0) {
                 slot[k] = tab_slot(key[k], mask);
-                prev[k] = atomicCAS(keys + slot[k], kEmpty, key[k]);
+                prev[k] = atomicCAS(keys + (int64_t)slot[k] * KS, kEmpty, key[k]);
             }
 #pragma unroll
         for (int k = 0; k < RMX_EVAL_ILP; k++)
@@ -335,9 +329,10 @@ __device__ __forceinline__ void insert_links(const EvalArgs &a, int64_t ob, int6
                 // capacity >= 2 x the unit's links: a free slot exists, probing stays below mask steps
                 for (int probe = 0; prev[k] != kEmpty && prev[k] != key[k] && probe < mask; probe++) {
                     slot[k] = (slot[k] + 1) & mask;
-                    prev[k] = atomicCAS(keys + slot[k], kEmpty, key[k]);
+                    prev[k] = atomicCAS(keys + (int64_t)slot[k] * KS, kEmpty, key[k]);
                 }
-                atomic_add_fx(j0 + (int64_t)k * NT < dout ? vo + slot[k] : vi + slot[k], q[k]);
+                if (occ && prev[k] == kEmpty) occ[atomicAdd(occ_n, 1)] = slot[k];
+                atomic_add_fx((j0 + (int64_t)k * NT < dout ? vo : vi) + (int64_t)slot[k] * VS, q[k]);
             }
     }
 }
@@ -676,16 +671,26 @@ constexpr int kHubCh = 2048;  // links per insert item
 constexpr int kHubSi = 2048;  // table slots per evaluation item
 constexpr int kHubPT = 256;   // threads per block of the pipeline
 
+// A slot of a hub unit's table: one 32-byte sector (key, out flow, in flow),
+// so that an insert or a read touches a single sector.
+struct __align__(32) HubSlot {
+    int32_t key, pad;
+    fx_t vo, vi, pad2;
+};
+constexpr int kSlotKS = (int)(sizeof(HubSlot) / sizeof(int32_t));  // key stride in int32
+constexpr int kSlotVS = (int)(sizeof(HubSlot) / sizeof(fx_t));     // flow stride in fx_t
+
 struct HubPlan {
     int64_t *cap, *toff, *coff, *eoff;  // per unit (+1): table slots, table offset, first chunk, first slice
     fx_t *own;                          // 2 per unit: out / in flow to the unit's own module
+    int32_t *occ_n;                     // per unit: slots taken (listed at occ + coff * kHubCh)
     double *best;                       // per slice: best change found
     int32_t *bmod;                      // per slice: its module
     uint8_t *act;                       // per unit: found a move below the threshold
     int64_t *tot;                       // [0] chunks, [1] slices, [2] units, [3] over capacity
-    int32_t *keys;                      // the pool: slots keys, out, in
-    fx_t *vo, *vi;
-    int64_t max_units, max_slots, max_items;  // capacities of the arrays above
+    HubSlot *slots;                     // the table pool
+    int32_t *occ;                       // the taken-slot lists (a unit's list holds at most its links)
+    int64_t max_units, max_slots, max_items, max_list;  // capacities of the arrays above
 };
 
 __device__ __forceinline__ int64_t hub_cap_of(int64_t d) {
@@ -758,7 +763,7 @@ __global__ void __launch_bounds__(1024) k_hub_plan(EvalArgs a, HubPlan p) {
                 const int64_t d = (a.out_off[u + 1] - a.out_off[u]) + (a.in_off[u + 1] - a.in_off[u]);
                 cap = hub_cap_of(d);
                 nch = (d + kHubCh - 1) / kHubCh;
-                nit = (cap + kHubSi - 1) / kHubSi;
+                nit = (d + kHubSi - 1) / kHubSi;  // slices of the taken-slot list, at most d long
             }
         }
         long long t0, t1, t2;
@@ -770,13 +775,14 @@ __global__ void __launch_bounds__(1024) k_hub_plan(EvalArgs a, HubPlan p) {
             p.toff[j] = r0 + e0;
             p.coff[j] = r1 + e1;
             p.eoff[j] = r2 + e2;
+            p.occ_n[j] = 0;
         }
         r0 += t0;
         r1 += t1;
         r2 += t2;
     }
     if (threadIdx.x == 0) {
-        const bool over = r0 > p.max_slots || r2 > p.max_items;
+        const bool over = r0 > p.max_slots || r2 > p.max_items || r1 * kHubCh > p.max_list;
         p.toff[nu] = r0;
         p.coff[nu] = r1;
         p.eoff[nu] = r2;
@@ -796,9 +802,9 @@ __global__ void __launch_bounds__(kHubPT) k_hub_insert(EvalArgs a, HubPlan p) {
         const int64_t ob = a.out_off[u], ib = a.in_off[u];
         const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
         const int64_t c0 = (item - p.coff[j]) * kHubCh, c1 = min(d, c0 + kHubCh);
-        const int64_t t = p.toff[j];
-        insert_links<kHubPT>(a, ob, ib, dout, c0 + threadIdx.x, c1, p.keys + t, p.vo + t, p.vi + t,
-                             (int)(p.cap[j] - 1));
+        HubSlot *tab = p.slots + p.toff[j];
+        insert_links<kHubPT, kSlotKS, kSlotVS>(a, ob, ib, dout, c0 + threadIdx.x, c1, &tab->key, &tab->vo, &tab->vi,
+                                               (int)(p.cap[j] - 1), p.occ + p.coff[j] * kHubCh, p.occ_n + j);
     }
 }
 
@@ -807,10 +813,10 @@ __global__ void k_hub_own(EvalArgs a, HubPlan p) {
     for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nu; j += (int64_t)gridDim.x * blockDim.x) {
         if (p.cap[j] == 0) continue;
         const int32_t u = a.list[h0 + j];
-        const int64_t t = p.toff[j];
-        const int s = tab_find(p.keys + t, (int)(p.cap[j] - 1), a.mod[u]);
-        p.own[2 * j] = s >= 0 ? p.vo[t + s] : 0;
-        p.own[2 * j + 1] = s >= 0 ? p.vi[t + s] : 0;
+        const HubSlot *tab = p.slots + p.toff[j];
+        const int s = tab_find<kSlotKS>(&tab->key, (int)(p.cap[j] - 1), a.mod[u]);
+        p.own[2 * j] = s >= 0 ? tab[s].vo : 0;
+        p.own[2 * j + 1] = s >= 0 ? tab[s].vi : 0;
     }
 }
 
@@ -824,19 +830,21 @@ __global__ void __launch_bounds__(kHubPT, 4) k_hub_eval(EvalArgs a, HubPlan p) {
     for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
         const int32_t j = hub_find(p.eoff, nu, item);
         const int32_t u = a.list[h0 + j];
-        const int64_t t = p.toff[j], s0 = (item - p.eoff[j]) * kHubSi, s1 = min(p.cap[j], s0 + kHubSi);
+        HubSlot *tab = p.slots + p.toff[j];
+        const int32_t *lst = p.occ + p.coff[j] * kHubCh;
+        const int64_t s0 = (item - p.eoff[j]) * kHubSi, s1 = min((int64_t)p.occ_n[j], s0 + kHubSi);
         const int32_t A = a.mod[u];
         const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, p.own[2 * j],
                                    p.own[2 * j + 1]);
         double best = 0.0;
         int32_t bm = INT_MAX;
-        for (int64_t s = s0 + threadIdx.x; s < s1; s += kHubPT) {
-            const int32_t k = p.keys[t + s];
-            if (k == kEmpty) continue;
-            const fx_t o = p.vo[t + s], i2 = p.vi[t + s];
-            p.keys[t + s] = kEmpty;  // the pool is left empty for the next sub-batch
-            p.vo[t + s] = 0;
-            p.vi[t + s] = 0;
+        for (int64_t q = s0 + threadIdx.x; q < s1; q += kHubPT) {
+            HubSlot *sl = tab + lst[q];
+            const int32_t k = sl->key;
+            const fx_t o = sl->vo, i2 = sl->vi;
+            sl->key = kEmpty;  // the pool is left empty for the next sub-batch
+            sl->vo = 0;
+            sl->vi = 0;
             if (k == A) continue;
             cands++;
             const double dl = candidate_delta(c, a.mstat[k], a.mterm[k], o, i2);
@@ -1333,35 +1341,54 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
 
 __global__ void k_hub_level(int32_t n, const int64_t *out_off, const int64_t *in_off, int64_t bound,
                             unsigned long long *acc) {
-    unsigned long long c0 = 0, c1 = 0, c2 = 0;
+    unsigned long long c0 = 0, c1 = 0, c2 = 0, c3 = 0;
     for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
         const int64_t d = (out_off[u + 1] - out_off[u]) + (in_off[u + 1] - in_off[u]);
         if (d <= bound) continue;
-        const int64_t cap = hub_cap_of(d);
         c0++;
-        c1 += cap;
-        c2 += (cap + kHubSi - 1) / kHubSi;
+        c1 += hub_cap_of(d);
+        c2 += (d + kHubSi - 1) / kHubSi;
+        c3 += (d + kHubCh - 1) / kHubCh * kHubCh;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         c0 += __shfl_xor_sync(kFull, c0, o);
         c1 += __shfl_xor_sync(kFull, c1, o);
         c2 += __shfl_xor_sync(kFull, c2, o);
+        c3 += __shfl_xor_sync(kFull, c3, o);
     }
     if ((threadIdx.x & 31) == 0 && c0) {
         atomicAdd(acc, c0);
         atomicAdd(acc + 1, c1);
         atomicAdd(acc + 2, c2);
+        atomicAdd(acc + 3, c3);
     }
 }
 
+__global__ void k_hub_pool_init(HubSlot *slots, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        HubSlot z;
+        z.key = kEmpty;
+        z.pad = 0;
+        z.vo = z.vi = z.pad2 = 0;
+        slots[i] = z;
+    }
+}
+
+void hub_pool_init(void *slots, int64_t n, cudaStream_t s) {
+    k_hub_pool_init<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(static_cast<HubSlot *>(slots), n);
+    RMX_LAUNCHED();
+}
+
+size_t hub_slot_bytes() { return sizeof(HubSlot); }
+
 void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_t s) {
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(dev_tmp);
-    RMX_CUDA(cudaMemsetAsync(acc, 0, 3 * sizeof(unsigned long long), s));
+    RMX_CUDA(cudaMemsetAsync(acc, 0, 4 * sizeof(unsigned long long), s));
     k_hub_level<<<blocks_for(L.n, 256, num_sms() * 8), 256, 0, s>>>(L.n, L.out_off, L.in_off, block_bin_max_degree(),
                                                                     acc);
     RMX_LAUNCHED();
-    RMX_CUDA(cudaMemcpyAsync(out, acc, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaMemcpyAsync(out, acc, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -1460,12 +1487,13 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
         hp.bmod = W.hub_bmod;
         hp.act = W.hub_act;
         hp.tot = W.hub_tot;
-        hp.keys = W.gkeys;
-        hp.vo = W.gtable;
-        hp.vi = W.gtable + W.gcap;
+        hp.occ_n = W.hub_occ_n;
+        hp.slots = static_cast<HubSlot *>(W.hub_slots);
+        hp.occ = W.hub_occ;
         hp.max_units = W.hub_units;
         hp.max_slots = W.gcap;
         hp.max_items = W.hub_items;
+        hp.max_list = W.hub_list;
         const cudaStream_t hs = on(1);
         const unsigned G = num_sms() * 8;
         if (tm) tm->begin(kTimerBinHub, hs);
