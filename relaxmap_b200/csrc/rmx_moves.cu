@@ -331,9 +331,23 @@ __device__ __forceinline__ void insert_links(const EvalArgs &a, int64_t ob, int6
                     slot[k] = (slot[k] + 1) & mask;
                     prev[k] = atomicCAS(keys + (int64_t)slot[k] * KS, kEmpty, key[k]);
                 }
-                if (occ && prev[k] == kEmpty) occ[atomicAdd(occ_n, 1)] = slot[k];
                 atomic_add_fx((j0 + (int64_t)k * NT < dout ? vo : vi) + (int64_t)slot[k] * VS, q[k]);
             }
+        if (occ) {  // list the slots this warp took: one counter update per warp, not per slot
+            const unsigned m = __activemask();
+            const int lane = threadIdx.x & 31;
+#pragma unroll
+            for (int k = 0; k < RMX_EVAL_ILP; k++) {
+                const bool fresh = key[k] >= 0 && prev[k] == kEmpty;
+                const unsigned bal = __ballot_sync(m, fresh);
+                if (!bal) continue;
+                const int leader = __ffs(bal) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(occ_n, __popc(bal));
+                base = __shfl_sync(m, base, leader);
+                if (fresh) occ[base + __popc(bal & ((1u << lane) - 1u))] = slot[k];
+            }
+        }
     }
 }
 
