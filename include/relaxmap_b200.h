@@ -285,7 +285,9 @@ rmx_status rmx_adjoint_backward(rmx_graph *g, const int32_t *part, double tau, d
  * its level) that assign units to the bins: up to 8, 16 and 32 links the
  * register bins (fixed), then the warp bin up to warp_max_degree, the mid bin
  * up to mid_max_degree, the block bin up to block_max_degree, the large bin
- * up to large_max_degree, and the hub bin above. Results do not depend on
+ * up to large_max_degree, and the hub bin above; each hub unit's links are
+ * partitioned by module into ceil(links / hub_partition_links) parts, each
+ * aggregated by one block. Results do not depend on
  * these values (every bin's kernel loops over its units by grid stride,
  * module statistics are exact integer sums, and every bin computes the same
  * change per candidate), only the time does. rmx_set_tuning takes effect at
@@ -293,7 +295,8 @@ rmx_status rmx_adjoint_backward(rmx_graph *g, const int32_t *part, double tau, d
  * are captured again. Each grid cap must lie in [1, 64], and
  * 32 <= warp_max <= 128, warp_max <= mid_max <= 512, mid_max <= block_max <=
  * 1024, block_max <= large_max <= 4096 (the bins' table limits; an equal
- * bound leaves a bin empty), else RMX_ERR_INVALID. The Python module
+ * bound leaves a bin empty), and 64 <= hub_partition_links <= 2^30, else
+ * RMX_ERR_INVALID. The Python module
  * relaxmap_b200.autotune picks the values by timing. No reference
  * counterpart. */
 typedef struct rmx_tuning {
@@ -306,6 +309,7 @@ typedef struct rmx_tuning {
     int32_t mid_max_degree;   /* default 512 */
     int32_t block_max_degree; /* default 1024 */
     int32_t large_max_degree; /* default 4096 */
+    int32_t hub_partition_links; /* default 1024 */
 } rmx_tuning;
 
 rmx_status rmx_get_tuning(rmx_tuning *out);

@@ -390,7 +390,7 @@ def steady_state_noalloc(n_nodes: int, n_links: int, in_off_ptr: int, in_src_ptr
 
 
 TUNING_FIELDS = ("eval_mid_grid", "eval_block_grid", "eval_large_grid", "eval_warp_grid", "eval_reg_grid",
-                 "warp_max_degree", "mid_max_degree", "block_max_degree", "large_max_degree")
+                 "warp_max_degree", "mid_max_degree", "block_max_degree", "large_max_degree", "hub_partition_links")
 
 
 class Tuning(C.Structure):

@@ -467,6 +467,7 @@ rmx_status rmx_get_tuning(rmx_tuning *out) {
         out->mid_max_degree = t.mid_max;
         out->block_max_degree = t.block_max;
         out->large_max_degree = t.large_max;
+        out->hub_partition_links = t.hub_part;
     });
 }
 
@@ -483,6 +484,7 @@ rmx_status rmx_set_tuning(const rmx_tuning *t) {
         v.mid_max = t->mid_max_degree;
         v.block_max = t->block_max_degree;
         v.large_max = t->large_max_degree;
+        v.hub_part = t->hub_partition_links;
         rmx::set_eval_tuning(v);
     });
 }

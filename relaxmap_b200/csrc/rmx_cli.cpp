@@ -47,7 +47,8 @@ bool apply_tuning_file(const std::string &path) {
                   {"\"warp_max_degree\"", &t.warp_max_degree},
                   {"\"mid_max_degree\"", &t.mid_max_degree},
                   {"\"block_max_degree\"", &t.block_max_degree},
-                  {"\"large_max_degree\"", &t.large_max_degree}};
+                  {"\"large_max_degree\"", &t.large_max_degree},
+                  {"\"hub_partition_links\"", &t.hub_partition_links}};
     for (const Field &fd : fields) {
         const size_t k = text.find(fd.name);
         if (k == std::string::npos) continue;
@@ -59,16 +60,16 @@ bool apply_tuning_file(const std::string &path) {
             printf("tuning file %s: %s has no integer value\n", path.c_str(), fd.name);
             return false;
         }
-        *fd.v = (int32_t)std::max(-1L, std::min(v, 100000L));  // out-of-range values are rejected below
+        *fd.v = (int32_t)std::max(-1L, std::min(v, 1L << 30));  // out-of-range values are rejected below
     }
     if (rmx_set_tuning(&t) != RMX_OK) {
         printf("tuning file %s: %s\n", path.c_str(), rmx_last_error());
         return false;
     }
     printf("Launch tuning from %s: grid caps (blocks per SM) mid %d, block %d, large %d, warp %d, register %d; "
-           "bin bounds (links) warp %d, mid %d, block %d, large %d\n",
+           "bin bounds (links) warp %d, mid %d, block %d, large %d; hub partitions of %d links\n",
            path.c_str(), t.eval_mid_grid, t.eval_block_grid, t.eval_large_grid, t.eval_warp_grid, t.eval_reg_grid,
-           t.warp_max_degree, t.mid_max_degree, t.block_max_degree, t.large_max_degree);
+           t.warp_max_degree, t.mid_max_degree, t.block_max_degree, t.large_max_degree, t.hub_partition_links);
     return true;
 }
 

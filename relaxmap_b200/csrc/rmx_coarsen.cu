@@ -475,13 +475,16 @@ __global__ void k_agg_pack(int32_t ng, int64_t m, const int64_t *gloff, const in
     for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {
         const int64_t e = e0 + lane;
         const int32_t g = row_of_chunk(g_out_off, ng, e0, e < m ? e : e0);
+        int32_t b = -1;
         if (e < m) {
             const int64_t src = gloff[g] + (e - g_out_off[g]);
-            const int32_t b = slab_dst[src];
+            b = slab_dst[src];
             out_dst[e] = b;
             out_fx[e] = slab_fx[src];
-            atomicAdd(colcnt + b, 1ull);
         }
+        // one counter update per destination and warp (hub columns take many links)
+        const unsigned peers = __match_any_sync(kFullMask, b);
+        if (b >= 0 && lane == __ffs(peers) - 1) atomicAdd(colcnt + b, (unsigned long long)__popc(peers));
     }
 }
 
@@ -494,9 +497,14 @@ __global__ void k_agg_transpose(int32_t ng, int64_t m, const int64_t *g_out_off,
     for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {
         const int64_t e = e0 + lane;
         const int32_t g = row_of_chunk(g_out_off, ng, e0, e < m ? e : e0);
-        if (e < m) {
-            const int32_t b = out_dst[e];
-            const int64_t q = g_in_off[b] + (int64_t)atomicAdd(colfill + b, 1ull);
+        const int32_t b = e < m ? out_dst[e] : -1;
+        const unsigned peers = __match_any_sync(kFullMask, b);
+        const int leader = __ffs(peers) - 1;
+        unsigned long long base = 0;
+        if (b >= 0 && lane == leader) base = atomicAdd(colfill + b, (unsigned long long)__popc(peers));
+        base = __shfl_sync(kFullMask, base, leader);
+        if (b >= 0) {
+            const int64_t q = g_in_off[b] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
             in_src[q] = g;
             in_fx[q] = out_fx[e];
         }

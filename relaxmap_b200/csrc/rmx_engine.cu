@@ -692,44 +692,42 @@ int64_t rmx_graph::max_degree(const Level &lv) {
     return (int64_t)h;
 }
 
-// The hub pipeline's pool of tables and plan arrays, sized for every unit of
-// lv above the large bin's bound (any sub-batch of the level fits); grown, never
-// shrunk, and left empty: every slot the pipeline uses it empties again.
+// The hub pipeline's plan, partition and bucket arrays, sized for every unit
+// of lv above the large bin's bound (any sub-batch of the level fits); grown,
+// never shrunk.
 void rmx_graph::ensure_hub_table(const Level &lv) {
     if (lv.n <= 0) return;
-    int64_t need[4];
+    int64_t need[3];
     hub_level_needs(lv, need, dtmp + 12, stream);
-    const int64_t units = need[0], slots = need[1], items = need[2], list = need[3];
-    if (units == 0 || (units <= work.hub_units && slots <= work.gcap && items <= work.hub_items &&
-                       list <= work.hub_list))
-        return;
-    RMX_CUDA(cudaStreamSynchronize(stream));  // no launch still reads the old pool
+    const int64_t units = need[0], parts = need[1], links = need[2];
+    if (units == 0 || (units <= work.hub_units && parts <= work.hub_parts && links <= work.hub_links)) return;
+    RMX_CUDA(cudaStreamSynchronize(stream));  // no launch still reads the old arrays
     hub_arena.destroy();
-    const int64_t U = std::max(units, work.hub_units) * 5 / 4 + 16, P = std::max(slots, work.gcap) * 5 / 4 + 64,
-                  I = std::max(items, work.hub_items) * 5 / 4 + 16, Lst = std::max(list, work.hub_list) * 5 / 4 + 64;
-    work.hub_slots = nullptr;
-    work.gcap = work.hub_units = work.hub_items = work.hub_list = 0;
-    const size_t bytes = (size_t)P * hub_slot_bytes() + (size_t)Lst * sizeof(int32_t) +
-                         (size_t)(U + 1) * 4 * sizeof(int64_t) + (size_t)U * (2 * sizeof(fx_t) + sizeof(int32_t) + 1) +
-                         (size_t)I * (sizeof(double) + sizeof(int32_t)) + 16 * 256;
+    const int64_t U = std::max(units, work.hub_units) * 5 / 4 + 16, P = std::max(parts, work.hub_parts) * 5 / 4 + 64,
+                  Lk = std::max(links, work.hub_links) * 5 / 4 + 1024;
+    work.hub_units = work.hub_parts = work.hub_links = 0;
+    work.hub_bkey = nullptr;
+    const size_t bytes = (size_t)Lk * (sizeof(int32_t) + sizeof(fx_t)) + (size_t)(U + 1) * 3 * sizeof(int64_t) +
+                         (size_t)U * (2 * sizeof(fx_t) + sizeof(int32_t) + 1) +
+                         (size_t)P * (sizeof(unsigned long long) + sizeof(double) + sizeof(int32_t)) +
+                         (size_t)(P + 1) * sizeof(int64_t) + 16 * 256;
     hub_arena.init(bytes);
-    work.hub_slots = hub_arena.alloc_bytes((size_t)P * hub_slot_bytes());
-    work.hub_occ = hub_arena.alloc<int32_t>(Lst);
-    work.hub_cap = hub_arena.alloc<int64_t>(U + 1);
-    work.hub_toff = hub_arena.alloc<int64_t>(U + 1);
+    work.hub_bfx = hub_arena.alloc<fx_t>(Lk);
+    work.hub_bkey = hub_arena.alloc<int32_t>(Lk);
     work.hub_coff = hub_arena.alloc<int64_t>(U + 1);
-    work.hub_eoff = hub_arena.alloc<int64_t>(U + 1);
+    work.hub_poff = hub_arena.alloc<int64_t>(U + 1);
+    work.hub_loff = hub_arena.alloc<int64_t>(U + 1);
     work.hub_own = hub_arena.alloc<fx_t>(2 * U);
-    work.hub_occ_n = hub_arena.alloc<int32_t>(U);
+    work.hub_nparts = hub_arena.alloc<int32_t>(U);
     work.hub_act = hub_arena.alloc<uint8_t>(U);
-    work.hub_best = hub_arena.alloc<double>(I);
-    work.hub_bmod = hub_arena.alloc<int32_t>(I);
-    work.hub_tot = hub_arena.alloc<int64_t>(4);
-    hub_pool_init(work.hub_slots, P, stream);
-    work.gcap = P;
+    work.hub_pcnt = hub_arena.alloc<unsigned long long>(P);
+    work.hub_best = hub_arena.alloc<double>(P);
+    work.hub_pstart = hub_arena.alloc<int64_t>(P + 1);
+    work.hub_bmod = hub_arena.alloc<int32_t>(P);
+    work.hub_tot = hub_arena.alloc<int64_t>(8);
     work.hub_units = U;
-    work.hub_items = I;
-    work.hub_list = Lst;
+    work.hub_parts = P;
+    work.hub_links = Lk;
 }
 
 void rmx_graph::initiate() {
@@ -821,7 +819,7 @@ void rmx_graph::run_subbatches(Level &lv, int64_t n_active, ModState &M, InstSta
             sweep_subbatch(lv, M, I, work, sa, sb, work.dparams + 2 * sb, mark, true, stream, tm);
         return;
     }
-    const SweepGraphKey key{&lv, &M, &I, sa.allow_new, mark ? 1 : 0, sa.vthresh, ns, work.hub_slots, work.gcap,
+    const SweepGraphKey key{&lv, &M, &I, sa.allow_new, mark ? 1 : 0, sa.vthresh, ns, work.hub_bkey, work.hub_links,
                             eval_tuning_generation()};
     SweepGraph *gr = nullptr;
     for (SweepGraph &g : sweep_graphs)
@@ -988,8 +986,8 @@ void rmx_graph::stage_sweeps_graph(Level &lv, bool allow_new, std::vector<double
     if (!any_set(act) || opt.max_iter <= 0) return;
     const int ns = sub_batches_for(lv.n);
     const StageGraphKey key{&lv,          &mods, &inst1,   allow_new ? 1 : 0, prior ? 1 : 0,
-                            opt.max_iter, ns,    vthresh,  opt.threshold,     work.hub_slots,
-                            work.gcap,    eval_tuning_generation(), scratch.mark()};
+                            opt.max_iter, ns,    vthresh,  opt.threshold,     work.hub_bkey,
+                            work.hub_links,    eval_tuning_generation(), scratch.mark()};
     RMX_CUDA(cudaMemcpyAsync(stage_sweeping, act.data(), (size_t)K, cudaMemcpyHostToDevice, stream));
     loop_graph(key, lv.n, [&](unsigned long long cond) { stage_body(lv, allow_new, prior, vthresh, ns, cond); });
     RMX_CUDA(cudaMemcpyAsync(L.data(), inst1.L, sizeof(double) * K, cudaMemcpyDeviceToHost, stream));
@@ -1191,7 +1189,7 @@ void rmx_graph::generate_sub_modules() {
         const int nsg = sub_batches_for(N);
         if (stage_graph_ok(sub_lv) && opt.max_iter > 0) {
             const StageGraphKey key{&sub_lv, &submods, &instsub, 0, 0, opt.max_iter, nsg, 0.0, opt.threshold,
-                                    work.hub_slots, work.gcap, eval_tuning_generation(), scratch.mark()};
+                                    work.hub_bkey, work.hub_links, eval_tuning_generation(), scratch.mark()};
             loop_graph(key, N, [&](unsigned long long cond) { subtune_body(nsg, cond); });
         }
         for (int iter = 0; iter < opt.max_iter && !stage_graph_ok(sub_lv); iter++) {

@@ -171,33 +171,32 @@ struct SweepWork {
     unsigned long long *claim = nullptr;        // per module id
     int64_t *counters = nullptr;
     // hub units (above the large bin's bound), each split over many blocks:
-    // one pool of tables (hub_slots, gcap 32-byte slots), the taken-slot
-    // lists and the plan arrays, sized for every hub unit of the current level
-    void *hub_slots = nullptr;
-    int64_t gcap = 0;
-    int32_t *hub_occ = nullptr, *hub_occ_n = nullptr;
-    int64_t hub_units = 0, hub_items = 0, hub_list = 0;  // capacities: units, slices, list entries
-    int64_t *hub_cap = nullptr, *hub_toff = nullptr, *hub_coff = nullptr, *hub_eoff = nullptr;
+    // the plan arrays (per unit), the partition arrays (per partition) and
+    // the buckets of partitioned links (hub_links entries), sized for every
+    // hub unit of the current level
+    int64_t hub_units = 0, hub_parts = 0, hub_links = 0;  // capacities
+    int64_t *hub_coff = nullptr, *hub_poff = nullptr, *hub_loff = nullptr, *hub_pstart = nullptr;
+    int32_t *hub_nparts = nullptr;
     fx_t *hub_own = nullptr;
+    uint8_t *hub_act = nullptr;
+    unsigned long long *hub_pcnt = nullptr;
     double *hub_best = nullptr;
     int32_t *hub_bmod = nullptr;
-    uint8_t *hub_act = nullptr;
+    int32_t *hub_bkey = nullptr;
+    fx_t *hub_bfx = nullptr;
     int64_t *hub_tot = nullptr;
     std::vector<int64_t> bucket_host;  // host copy of bucket_off after bucket_units
     uint32_t *dparams = nullptr;       // device {stamp, hseed} per sub-batch of the current sweep
     uint32_t hparams[64] = {};         // host staging of dparams
-    cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};  // concurrent degree bins
-    cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaStream_t aux[5] = {};  // concurrent degree bins
+    cudaEvent_t fork = nullptr, join[5] = {};
 };
 
 void configure_eval_kernels();
-// What the hub pipeline needs for a level: hub units (above block_bin_max_degree),
-// table slots in all, list slices, list entries (out[0..3]); one device
-// reduction, then a sync.
+// What the hub pipeline needs for a level: hub units (above
+// block_bin_max_degree), their partitions and their links (out[0..2]); one
+// device reduction, then a sync.
 void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_t s);
-// Empties n pool slots (at allocation); bytes of one slot.
-void hub_pool_init(void *slots, int64_t n, cudaStream_t s);
-size_t hub_slot_bytes();
 
 // Launch shape of move evaluation, process-wide and read at every launch:
 // the grid cap of each bin in blocks per SM, and the degree bounds that
@@ -209,11 +208,12 @@ size_t hub_slot_bytes();
 struct EvalTuning {
     int mid, block, large, warp, reg;              // grid caps
     int warp_max, mid_max, block_max, large_max;   // degree bounds (at most 128, 512, 1024, 4096)
+    int hub_part;                                  // mean links per partition of a hub unit
 };
 EvalTuning eval_tuning();
 // Throws std::invalid_argument unless every grid cap lies in [1, 64] and
 // 32 <= warp_max <= mid_max <= block_max <= large_max, each within its bin's
-// table limit.
+// table limit, and 64 <= hub_part <= 2^30.
 void set_eval_tuning(const EvalTuning &t);
 // Changes with every set_eval_tuning (part of the sweep graph cache key).
 int eval_tuning_generation();

@@ -32,12 +32,12 @@ struct SweepGraphKey {
     int allow_new, mark;
     double vthresh;
     int nsub;
-    const void *hub_pool;
-    int64_t gcap;
+    const void *hub_buckets;
+    int64_t hub_links;
     int tuning_gen;  // eval_tuning_generation() at capture: grid sizes are part of the graph
     bool operator==(const SweepGraphKey &o) const {
         return lv == o.lv && M == o.M && I == o.I && allow_new == o.allow_new && mark == o.mark &&
-               vthresh == o.vthresh && nsub == o.nsub && hub_pool == o.hub_pool && gcap == o.gcap &&
+               vthresh == o.vthresh && nsub == o.nsub && hub_buckets == o.hub_buckets && hub_links == o.hub_links &&
                tuning_gen == o.tuning_gen;
     }
 };
@@ -57,14 +57,14 @@ struct StageGraphKey {
     const rmx::InstState *I;
     int allow_new, prior, max_iter, nsub;
     double vthresh, threshold;
-    const void *hub_pool;
-    int64_t gcap;
+    const void *hub_buckets;
+    int64_t hub_links;
     int tuning_gen;
     size_t scratch_mark;  // the scratch the body's primitives use starts here
     bool operator==(const StageGraphKey &o) const {
         return lv == o.lv && M == o.M && I == o.I && allow_new == o.allow_new && prior == o.prior &&
                max_iter == o.max_iter && nsub == o.nsub && vthresh == o.vthresh && threshold == o.threshold &&
-               hub_pool == o.hub_pool && gcap == o.gcap && tuning_gen == o.tuning_gen && scratch_mark == o.scratch_mark;
+               hub_buckets == o.hub_buckets && hub_links == o.hub_links && tuning_gen == o.tuning_gen && scratch_mark == o.scratch_mark;
     }
 };
 struct StageGraph {
@@ -105,9 +105,9 @@ struct rmx_graph {
     rmx::InstState inst1, instsub;
     rmx::SweepWork work;
     rmx::Timers timers;
-    // Tables grown on demand for the largest units / groups of a level: the
-    // hub pipeline's pool of move evaluation (work.hub_slots and its plan
-    // arrays) and the global hash tables of the link aggregation. Both are arenas, so their blocks
+    // Arrays grown on demand for the largest units / groups of a level: the
+    // hub pipeline's buckets and plan arrays (work.hub_*) and the global hash
+    // tables of the link aggregation. Both are arenas, so their blocks
     // come from and return to the process-wide block cache like the
     // handle's other device memory (no cudaMalloc / cudaFree of their own).
     rmx::Arena hub_arena, agg_arena;

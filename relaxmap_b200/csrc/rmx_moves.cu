@@ -668,50 +668,48 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? RMX_LRG_MINB : (NT == 128 ? 8 
 
 // ---------------------------------------------------------------- hub units
 // Units above the large bin's bound (R-MAT hubs and the heaviest super-nodes,
-// 10^4 to 10^6 links) are each split over many blocks instead of being one
-// block's long chain of dependent gathers and atomics: every hub unit of the
-// sub-batch gets a table of its own (next_pow2(2d) slots) in one pool, and
-//   plan    one block lays out the units' tables, link chunks (kHubCh links)
-//           and table slices (kHubSi slots) by prefix sums,
-//   insert  blocks take link chunks and insert them into their unit's table,
-//   own     the flow of each unit to and from its own module is looked up,
-//   eval    blocks take table slices, evaluate the candidates in them (and
-//           empty the slots), and keep the slice's best change,
-//   finish  a warp per unit reduces its slices' bests and decides (finish_unit),
-//   mark    in prioritised sweeps, link chunks of units that found a move
-//           mark their neighbours.
-// The pool is empty between sub-batches (every evaluated slot is emptied).
-constexpr int kHubCh = 2048;  // links per insert item
-constexpr int kHubSi = 2048;  // table slots per evaluation item
-constexpr int kHubPT = 256;   // threads per block of the pipeline
-
-// A slot of a hub unit's table: one 32-byte sector (key, out flow, in flow),
-// so that an insert or a read touches a single sector.
-struct __align__(32) HubSlot {
-    int32_t key, pad;
-    fx_t vo, vi, pad2;
-};
-constexpr int kSlotKS = (int)(sizeof(HubSlot) / sizeof(int32_t));  // key stride in int32
-constexpr int kSlotVS = (int)(sizeof(HubSlot) / sizeof(fx_t));     // flow stride in fx_t
+// 10^4 to 10^6 links) are not left to one block's long chain of dependent
+// gathers and atomics. Every hub unit's links are radix-partitioned by a hash
+// of their neighbour's module into partitions of about part_links links, so
+// that each partition's distinct modules fit one block's shared table:
+//   plan     one block lays out, by prefix sums, every hub unit's link chunks
+//            (kHubCh links), partitions and bucket region;
+//   count    blocks take link chunks: each link's partition is counted, and the
+//            flows to the unit's own module are summed;
+//   offsets  one block turns the partition counts into bucket offsets;
+//   scatter  blocks take link chunks again and write (module, direction, flow)
+//            into their partition's bucket;
+//   evaluate a block per partition aggregates its bucket in a shared table,
+//            evaluates the candidates and keeps the partition's best change;
+//   finish   a warp per unit reduces its partitions' bests and decides;
+//   mark     in prioritised sweeps, link chunks of units that found a move
+//            mark their neighbours.
+// Counters are taken with one atomic per group of lanes that share a
+// partition (__match_any_sync), not one per link.
+constexpr int kHubCh = 2048;     // links per chunk item
+constexpr int kHubPT = 256;      // threads per block of the pipeline
+constexpr int kPartLinks = 1024; // mean links per partition (default of the run-time setting)
+constexpr int kPartCap = 4096;   // shared table slots of a partition block (at most half filled per round)
+constexpr int kMaxParts = 1 << 20;
+constexpr size_t kHubEvalSmem = (size_t)kPartCap * (2 * sizeof(fx_t) + sizeof(int32_t));
 
 struct HubPlan {
-    int64_t *cap, *toff, *coff, *eoff;  // per unit (+1): table slots, table offset, first chunk, first slice
-    fx_t *own;                          // 2 per unit: out / in flow to the unit's own module
-    int32_t *occ_n;                     // per unit: slots taken (listed at occ + coff * kHubCh)
-    double *best;                       // per slice: best change found
-    int32_t *bmod;                      // per slice: its module
-    uint8_t *act;                       // per unit: found a move below the threshold
-    int64_t *tot;                       // [0] chunks, [1] slices, [2] units, [3] over capacity
-    HubSlot *slots;                     // the table pool
-    int32_t *occ;                       // the taken-slot lists (a unit's list holds at most its links)
-    int64_t max_units, max_slots, max_items, max_list;  // capacities of the arrays above
+    int64_t *coff, *poff, *loff;   // per unit (+1): first chunk, first partition, first bucket element
+    int32_t *nparts;               // per unit: partitions
+    fx_t *own;                     // 2 per unit: out / in flow to the unit's own module
+    uint8_t *act;                  // per unit: found a move below the threshold
+    unsigned long long *pcnt;      // per partition: links (counted), then the fill position
+    int64_t *pstart;               // per partition (+1): first bucket element
+    double *best;                  // per partition: best change found
+    int32_t *bmod;                 // per partition: its module
+    int32_t *bkey;                 // bucket elements: module | direction (bit 31 set: in-link)
+    fx_t *bfx;                     //   and flow
+    int64_t *tot;                  // [0] chunks, [1] partitions, [2] units, [3] over capacity, [4] links
+    int64_t max_units, max_parts, max_links;  // capacities
+    int64_t part_links;                       // mean links per partition
 };
 
-__device__ __forceinline__ int64_t hub_cap_of(int64_t d) {
-    int64_t c = 32;
-    while (c < 2 * d) c <<= 1;
-    return c;
-}
+__device__ __forceinline__ uint32_t part_hash(int32_t key) { return mix32((uint32_t)key * 0x9E3779B1u + 0x7F4A7C15u); }
 
 // Largest j < n with off[j] <= x (off ascending, off[0] <= x).
 __device__ __forceinline__ int32_t hub_find(const int64_t *off, int32_t n, int64_t x) {
@@ -753,16 +751,19 @@ __device__ __forceinline__ long long hub_block_scan(long long v, long long *ws, 
     return pre;
 }
 
+__device__ __forceinline__ int64_t unit_links(const EvalArgs &a, int32_t u) {
+    return (a.out_off[u + 1] - a.out_off[u]) + (a.in_off[u + 1] - a.in_off[u]);
+}
+
 // The capacities are sized for every hub unit of the level, so they hold any
 // sub-batch; should they not (the bin bounds changed since they were sized),
 // nothing of the sub-batch is laid out and its hub units propose no move.
 __global__ void __launch_bounds__(1024) k_hub_plan(EvalArgs a, HubPlan p) {
     __shared__ long long ws[32];
-    const int64_t h0 = a.range[0];
-    int64_t nu = a.range[1] - h0;
+    const int64_t h0 = a.range[0], nu = a.range[1] - h0;
     if (nu > p.max_units) {
         if (threadIdx.x == 0) {
-            p.tot[0] = p.tot[1] = p.tot[2] = 0;
+            p.tot[0] = p.tot[1] = p.tot[2] = p.tot[4] = 0;
             p.tot[3] = 1;
         }
         return;
@@ -770,102 +771,228 @@ __global__ void __launch_bounds__(1024) k_hub_plan(EvalArgs a, HubPlan p) {
     long long r0 = 0, r1 = 0, r2 = 0;
     for (int64_t base = 0; base < nu; base += 1024) {
         const int64_t j = base + threadIdx.x;
-        long long cap = 0, nch = 0, nit = 0;
+        long long d = 0, nch = 0, np = 0;
         if (j < nu) {
             const int32_t u = a.list[h0 + j];
-            if (a.inst_active[a.uinst[u]]) {  // inactive units take no chunk and no slice
-                const int64_t d = (a.out_off[u + 1] - a.out_off[u]) + (a.in_off[u + 1] - a.in_off[u]);
-                cap = hub_cap_of(d);
+            if (a.inst_active[a.uinst[u]]) {  // inactive units take no chunk and no partition
+                d = unit_links(a, u);
                 nch = (d + kHubCh - 1) / kHubCh;
-                nit = (d + kHubSi - 1) / kHubSi;  // slices of the taken-slot list, at most d long
+                np = min((long long)kMaxParts, max(1ll, (d + p.part_links - 1) / p.part_links));
             }
         }
         long long t0, t1, t2;
-        const long long e0 = hub_block_scan(cap, ws, &t0);
-        const long long e1 = hub_block_scan(nch, ws, &t1);
-        const long long e2 = hub_block_scan(nit, ws, &t2);
+        const long long e0 = hub_block_scan(nch, ws, &t0);
+        const long long e1 = hub_block_scan(np, ws, &t1);
+        const long long e2 = hub_block_scan(d, ws, &t2);
         if (j < nu) {
-            p.cap[j] = cap;
-            p.toff[j] = r0 + e0;
-            p.coff[j] = r1 + e1;
-            p.eoff[j] = r2 + e2;
-            p.occ_n[j] = 0;
+            p.coff[j] = r0 + e0;
+            p.poff[j] = r1 + e1;
+            p.loff[j] = r2 + e2;
+            p.nparts[j] = (int32_t)np;
+            p.own[2 * j] = p.own[2 * j + 1] = 0;
         }
         r0 += t0;
         r1 += t1;
         r2 += t2;
     }
+    __shared__ int over;
     if (threadIdx.x == 0) {
-        const bool over = r0 > p.max_slots || r2 > p.max_items || r1 * kHubCh > p.max_list;
-        p.toff[nu] = r0;
-        p.coff[nu] = r1;
-        p.eoff[nu] = r2;
-        p.tot[0] = over ? 0 : r1;
-        p.tot[1] = over ? 0 : r2;
+        over = r1 > p.max_parts || r2 > p.max_links;
+        p.coff[nu] = r0;
+        p.poff[nu] = r1;
+        p.loff[nu] = r2;
+        p.tot[0] = over ? 0 : r0;
+        p.tot[1] = over ? 0 : r1;
         p.tot[2] = over ? 0 : nu;
-        p.tot[3] = over ? 1 : 0;
+        p.tot[3] = over;
+        p.tot[4] = over ? 0 : r2;
     }
+    __syncthreads();
+    if (!over)
+        for (int64_t q = threadIdx.x; q < r1; q += 1024) p.pcnt[q] = 0;
 }
 
-__global__ void __launch_bounds__(kHubPT) k_hub_insert(EvalArgs a, HubPlan p) {
+// Link l of unit u (out-links first): neighbour module, direction, flow.
+__device__ __forceinline__ void hub_link(const EvalArgs &a, int64_t ob, int64_t ib, int64_t dout, int64_t l,
+                                         int32_t &key, bool &in, fx_t &q) {
+    in = l >= dout;
+    const int64_t e = in ? ib + (l - dout) : ob + l;
+    key = __ldg(a.mod + __ldg(in ? a.in_src + e : a.out_dst + e));
+    q = __ldg(in ? a.in_fx + e : a.out_fx + e);
+}
+
+// Count (scatter = false) or place (scatter = true) the links of the chunks.
+// Links to the unit's own module are only summed (into own); the others are
+// combined per warp step by (module, direction) with __match_any_sync, so a
+// module that many of a hub's links reach takes one bucket element per warp
+// step instead of one per link (integer sums: exact in any order). Both
+// passes form the same groups (the same lanes read the same links), so the
+// counts hold the scatter exactly.
+template <bool SCATTER>
+__global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
+    __shared__ fx_t wq[kHubPT];
+    const int lane = threadIdx.x & 31;
     const int64_t h0 = a.range[0], total = p.tot[0];
     const int32_t nu = (int32_t)p.tot[2];
     for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
         const int32_t j = hub_find(p.coff, nu, item);
         const int32_t u = a.list[h0 + j];
+        const int32_t A = a.mod[u], np = p.nparts[j];
         const int64_t ob = a.out_off[u], ib = a.in_off[u];
         const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
         const int64_t c0 = (item - p.coff[j]) * kHubCh, c1 = min(d, c0 + kHubCh);
-        HubSlot *tab = p.slots + p.toff[j];
-        insert_links<kHubPT, kSlotKS, kSlotVS>(a, ob, ib, dout, c0 + threadIdx.x, c1, &tab->key, &tab->vo, &tab->vi,
-                                               (int)(p.cap[j] - 1), p.occ + p.coff[j] * kHubCh, p.occ_n + j);
+        fx_t oA = 0, iA = 0;
+        for (int64_t b = c0; b < c1; b += kHubPT) {  // uniform over the block: every warp runs every step
+            const int64_t l = b + threadIdx.x;
+            int32_t key = A;
+            bool in = false;
+            fx_t q = 0;
+            if (l < c1) hub_link(a, ob, ib, dout, l, key, in, q);
+            if (key == A) {  // also the lanes past the chunk (q = 0)
+                if (in)
+                    iA += q;
+                else
+                    oA += q;
+            }
+            const bool valid = key != A;
+            const uint32_t kd = in ? ((uint32_t)key | 0x80000000u) : (uint32_t)key;
+            const unsigned kpeers = __match_any_sync(kFull, valid ? (unsigned long long)kd : ~0ull);
+            const bool head = valid && lane == __ffs(kpeers) - 1;  // one lane per (module, direction)
+            const int32_t part = head ? (int32_t)(part_hash(key) % (uint32_t)np) : -1;
+            const unsigned peers = __match_any_sync(kFull, part);
+            const int leader = __ffs(peers) - 1;
+            if (!SCATTER) {
+                if (head && lane == leader) atomicAdd(p.pcnt + p.poff[j] + part, (unsigned long long)__popc(peers));
+            } else {
+                wq[threadIdx.x] = q;
+                __syncwarp();
+                fx_t sum = 0;
+                if (head)
+                    for (unsigned m = kpeers; m; m &= m - 1) sum += wq[(threadIdx.x & ~31) + __ffs(m) - 1];
+                unsigned long long base = 0;
+                const int64_t pidx = p.poff[j] + part;
+                if (head && lane == leader) base = atomicAdd(p.pcnt + pidx, (unsigned long long)__popc(peers));
+                base = __shfl_sync(kFull, base, leader);
+                if (head) {
+                    const int64_t pos = p.pstart[pidx] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
+                    p.bkey[pos] = (int32_t)kd;
+                    p.bfx[pos] = sum;
+                }
+                __syncwarp();
+            }
+        }
+        if (!SCATTER) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                oA += __shfl_xor_sync(kFull, oA, o);
+                iA += __shfl_xor_sync(kFull, iA, o);
+            }
+            if (lane == 0) {
+                if (oA) atomic_add_fx(p.own + 2 * j, oA);
+                if (iA) atomic_add_fx(p.own + 2 * j + 1, iA);
+            }
+        }
     }
 }
 
-__global__ void k_hub_own(EvalArgs a, HubPlan p) {
-    const int64_t h0 = a.range[0], nu = p.tot[2];
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nu; j += (int64_t)gridDim.x * blockDim.x) {
-        if (p.cap[j] == 0) continue;
-        const int32_t u = a.list[h0 + j];
-        const HubSlot *tab = p.slots + p.toff[j];
-        const int s = tab_find<kSlotKS>(&tab->key, (int)(p.cap[j] - 1), a.mod[u]);
-        p.own[2 * j] = s >= 0 ? tab[s].vo : 0;
-        p.own[2 * j + 1] = s >= 0 ? tab[s].vi : 0;
+// Partition counts -> bucket offsets (each unit's buckets inside its region,
+// in partition order); the counters restart at zero as fill positions.
+__global__ void __launch_bounds__(1024) k_hub_offsets(HubPlan p) {
+    __shared__ long long ws[32];
+    const int64_t np = p.tot[1];
+    long long r = 0;
+    for (int64_t base = 0; base < np; base += 1024) {
+        const int64_t q = base + threadIdx.x;
+        const long long c = q < np ? (long long)p.pcnt[q] : 0;
+        long long t;
+        const long long e = hub_block_scan(c, ws, &t);
+        if (q < np) {
+            p.pstart[q] = r + e;
+            p.pcnt[q] = 0;
+        }
+        r += t;
     }
+    if (threadIdx.x == 0) p.pstart[np] = r;
 }
 
-__global__ void __launch_bounds__(kHubPT, 4) k_hub_eval(EvalArgs a, HubPlan p) {
+// A block per partition: its bucket aggregated in a shared table, in rounds
+// (keys split by a second hash) if it holds more distinct modules than half
+// the table, which the partitioning makes vanishingly rare.
+__global__ void __launch_bounds__(kHubPT, 2) k_hub_eval(EvalArgs a, HubPlan p) {
+    extern __shared__ __align__(16) unsigned char hub_smem[];  // kHubEvalSmem bytes
+    fx_t *vo = reinterpret_cast<fx_t *>(hub_smem);
+    fx_t *vi = vo + kPartCap;
+    int32_t *keys = reinterpret_cast<int32_t *>(vi + kPartCap);
     __shared__ double sb[kHubPT / 32];
     __shared__ int32_t sm[kHubPT / 32];
+    __shared__ int nfresh;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t h0 = a.range[0], total = p.tot[1];
     const int32_t nu = (int32_t)p.tot[2];
+    const int mask = kPartCap - 1;
     unsigned long long cands = 0;
-    for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-        const int32_t j = hub_find(p.eoff, nu, item);
+    for (int s = threadIdx.x; s < kPartCap; s += kHubPT) {
+        keys[s] = kEmpty;
+        vo[s] = vi[s] = 0;
+    }
+    for (int64_t pidx = blockIdx.x; pidx < total; pidx += gridDim.x) {
+        const int32_t j = hub_find(p.poff, nu, pidx);
         const int32_t u = a.list[h0 + j];
-        HubSlot *tab = p.slots + p.toff[j];
-        const int32_t *lst = p.occ + p.coff[j] * kHubCh;
-        const int64_t s0 = (item - p.eoff[j]) * kHubSi, s1 = min((int64_t)p.occ_n[j], s0 + kHubSi);
+        const int64_t b0 = p.pstart[pidx], b1 = p.pstart[pidx + 1];
         const int32_t A = a.mod[u];
         const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, p.own[2 * j],
                                    p.own[2 * j + 1]);
         double best = 0.0;
         int32_t bm = INT_MAX;
-        for (int64_t q = s0 + threadIdx.x; q < s1; q += kHubPT) {
-            HubSlot *sl = tab + lst[q];
-            const int32_t k = sl->key;
-            const fx_t o = sl->vo, i2 = sl->vi;
-            sl->key = kEmpty;  // the pool is left empty for the next sub-batch
-            sl->vo = 0;
-            sl->vi = 0;
-            if (k == A) continue;
-            cands++;
-            const double dl = candidate_delta(c, a.mstat[k], a.mterm[k], o, i2);
-            if (better(dl, k, best, bm)) {
-                best = dl;
-                bm = k;
+        for (uint32_t R = 1;; R <<= 1) {  // R rounds; more only when a round overfills the table
+            bool overfull = false;
+            double rbest = 0.0;
+            int32_t rbm = INT_MAX;
+            unsigned long long rc = 0;
+            for (uint32_t r = 0; r < R && !overfull; r++) {
+                __syncthreads();
+                if (threadIdx.x == 0) nfresh = 0;
+                __syncthreads();
+                for (int64_t e = b0 + threadIdx.x; e < b1; e += kHubPT) {
+                    const int32_t kd = p.bkey[e];
+                    const int32_t key = kd & 0x7fffffff;
+                    if (R > 1 && (mix32((uint32_t)key) >> 20) % R != r) continue;  // bits above the slot's
+                    if (*(volatile int *)&nfresh > kPartCap / 2) break;
+                    int sl = tab_slot(key, mask);
+                    int32_t prev = atomicCAS(keys + sl, kEmpty, key);
+                    for (int probe = 0; prev != kEmpty && prev != key && probe < mask; probe++) {
+                        sl = (sl + 1) & mask;
+                        prev = atomicCAS(keys + sl, kEmpty, key);
+                    }
+                    if (prev != kEmpty && prev != key) break;  // full: nfresh is past the limit already
+                    if (prev == kEmpty) atomicAdd(&nfresh, 1);
+                    atomic_add_fx(kd < 0 ? vi + sl : vo + sl, p.bfx[e]);
+                }
+                __syncthreads();
+                overfull = nfresh > kPartCap / 2;
+                // evaluate the table's candidates (unless the round overfilled) and empty it
+                for (int s = threadIdx.x; s < kPartCap; s += kHubPT) {
+                    const int32_t k = keys[s];
+                    if (k == kEmpty) continue;
+                    if (!overfull && k != A) {
+                        rc++;
+                        const double dl = candidate_delta(c, a.mstat[k], a.mterm[k], vo[s], vi[s]);
+                        if (better(dl, k, rbest, rbm)) {
+                            rbest = dl;
+                            rbm = k;
+                        }
+                    }
+                    keys[s] = kEmpty;
+                    vo[s] = vi[s] = 0;
+                }
             }
+            __syncthreads();
+            if (!overfull) {
+                best = rbest;
+                bm = rbm;
+                cands += rc;
+                break;
+            }  // else retry with twice the rounds (the table is empty again)
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -887,10 +1014,9 @@ __global__ void __launch_bounds__(kHubPT, 4) k_hub_eval(EvalArgs a, HubPlan p) {
                     best = sb[q];
                     bm = sm[q];
                 }
-            p.best[item] = best;
-            p.bmod[item] = bm;
+            p.best[pidx] = best;
+            p.bmod[pidx] = bm;
         }
-        __syncthreads();
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cands += __shfl_xor_sync(kFull, cands, o);
@@ -908,7 +1034,7 @@ __global__ void k_hub_finish(EvalArgs a, HubPlan p) {
     }
     for (int64_t j = gw; j < nu; j += nw) {
         const int32_t u = a.list[h0 + j];
-        if (p.cap[j] == 0) {  // its instance has stopped
+        if (p.nparts[j] == 0) {  // its instance has stopped
             if (lane == 0) {
                 a.prop[u] = -1;
                 p.act[j] = 0;
@@ -917,7 +1043,7 @@ __global__ void k_hub_finish(EvalArgs a, HubPlan p) {
         }
         double best = 0.0;
         int32_t bm = INT_MAX;
-        for (int64_t q = p.eoff[j] + lane; q < p.eoff[j + 1]; q += 32)
+        for (int64_t q = p.poff[j] + lane; q < p.poff[j + 1]; q += 32)
             if (better(p.best[q], p.bmod[q], best, bm)) {
                 best = p.best[q];
                 bm = p.bmod[q];
@@ -936,7 +1062,7 @@ __global__ void k_hub_finish(EvalArgs a, HubPlan p) {
             const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A,
                                        p.own[2 * j], p.own[2 * j + 1]);
             p.act[j] = (uint8_t)finish_unit(a, u, c, best, bm);
-            seen += (a.out_off[u + 1] - a.out_off[u]) + (a.in_off[u + 1] - a.in_off[u]);
+            seen += unit_links(a, u);
             units++;
         }
     }
@@ -1353,61 +1479,43 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     return a;
 }
 
-__global__ void k_hub_level(int32_t n, const int64_t *out_off, const int64_t *in_off, int64_t bound,
+__global__ void k_hub_level(int32_t n, const int64_t *out_off, const int64_t *in_off, int64_t bound, int64_t part_links,
                             unsigned long long *acc) {
-    unsigned long long c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+    unsigned long long c0 = 0, c1 = 0, c2 = 0;
     for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
         const int64_t d = (out_off[u + 1] - out_off[u]) + (in_off[u + 1] - in_off[u]);
         if (d <= bound) continue;
         c0++;
-        c1 += hub_cap_of(d);
-        c2 += (d + kHubSi - 1) / kHubSi;
-        c3 += (d + kHubCh - 1) / kHubCh * kHubCh;
+        c1 += min((int64_t)kMaxParts, (d + part_links - 1) / part_links);
+        c2 += d;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         c0 += __shfl_xor_sync(kFull, c0, o);
         c1 += __shfl_xor_sync(kFull, c1, o);
         c2 += __shfl_xor_sync(kFull, c2, o);
-        c3 += __shfl_xor_sync(kFull, c3, o);
     }
     if ((threadIdx.x & 31) == 0 && c0) {
         atomicAdd(acc, c0);
         atomicAdd(acc + 1, c1);
         atomicAdd(acc + 2, c2);
-        atomicAdd(acc + 3, c3);
     }
 }
-
-__global__ void k_hub_pool_init(HubSlot *slots, int64_t n) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        HubSlot z;
-        z.key = kEmpty;
-        z.pad = 0;
-        z.vo = z.vi = z.pad2 = 0;
-        slots[i] = z;
-    }
-}
-
-void hub_pool_init(void *slots, int64_t n, cudaStream_t s) {
-    k_hub_pool_init<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(static_cast<HubSlot *>(slots), n);
-    RMX_LAUNCHED();
-}
-
-size_t hub_slot_bytes() { return sizeof(HubSlot); }
 
 void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_t s) {
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(dev_tmp);
-    RMX_CUDA(cudaMemsetAsync(acc, 0, 4 * sizeof(unsigned long long), s));
-    k_hub_level<<<blocks_for(L.n, 256, num_sms() * 8), 256, 0, s>>>(L.n, L.out_off, L.in_off, block_bin_max_degree(),
+    RMX_CUDA(cudaMemsetAsync(acc, 0, 3 * sizeof(unsigned long long), s));
+    const EvalTuning t = eval_tuning();
+    k_hub_level<<<blocks_for(L.n, 256, num_sms() * 8), 256, 0, s>>>(L.n, L.out_off, L.in_off, t.large_max, t.hub_part,
                                                                     acc);
     RMX_LAUNCHED();
-    RMX_CUDA(cudaMemcpyAsync(out, acc, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaMemcpyAsync(out, acc, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));
 }
 
 namespace {
-EvalTuning g_tuning{8, RMX_BLK_GRID, RMX_LRG_MINB, RMX_WARP_GRID, RMX_REG_GRID, kWarpMaxDeg, kMidMaxDeg, kBlkMaxDeg, kLrgMaxDeg};
+EvalTuning g_tuning{8,           RMX_BLK_GRID, RMX_LRG_MINB, RMX_WARP_GRID, RMX_REG_GRID,
+                    kWarpMaxDeg, kMidMaxDeg,   kBlkMaxDeg,   kLrgMaxDeg,    kPartLinks};
 int g_tuning_gen = 0;
 std::mutex g_tuning_mu;  // guards g_tuning and g_tuning_gen
 }  // namespace
@@ -1425,6 +1533,8 @@ void set_eval_tuning(const EvalTuning &t) {
         t.block_max < t.mid_max || t.block_max > kBlkMaxDeg || t.large_max < t.block_max || t.large_max > kLrgMaxDeg)
         throw std::invalid_argument("degree bin bounds must satisfy 32 <= warp <= 128, warp <= mid <= 512, "
                                     "mid <= block <= 1024, block <= large <= 4096");
+    if (t.hub_part < 64 || t.hub_part > (1 << 30))
+        throw std::invalid_argument("hub partitions must hold 64..2^30 links");
     std::lock_guard<std::mutex> lk(g_tuning_mu);
     g_tuning = t;
     g_tuning_gen++;
@@ -1455,17 +1565,60 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     // without host sizes every bin counts as non-empty and takes its full grid
     auto cnt = [&](int b0, int b1) { return fitted ? h[b1] - h[b0] : (int64_t)1 << 40; };
     const int64_t n_mid = cnt(kBinMid, kBinMid + 1), n_blk = cnt(kBinBlock, kBinBlock + 1),
-                  n_lrg = cnt(kBinLarge, kBinLarge + 1), n_hub = W.gcap > 0 ? cnt(kBinHub, kBinHub + 1) : 0,
+                  n_lrg = cnt(kBinLarge, kBinLarge + 1), n_hub = W.hub_links > 0 ? cnt(kBinHub, kBinHub + 1) : 0,
                   n_warp = cnt(kBinWarp, kBinWarp + 1), n_reg = cnt(kBinReg8, kBinReg32 + 1);
-    const bool use[4] = {n_blk > 0, n_lrg + n_hub > 0, n_warp > 0, n_mid > 0};
+    // streams: 0 block, 1 large, 2 warp, 3 mid, 4 hub, the caller's stream the register bins
+    const bool use[5] = {n_blk > 0, n_lrg > 0, n_warp > 0, n_mid > 0, n_hub > 0};
     const EvalTuning tg = eval_tuning();
-    const int streams = (int)use[0] + (int)use[1] + (int)use[2] + (int)use[3] + (n_reg > 0 ? 1 : 0);
+    int streams = n_reg > 0 ? 1 : 0;
+    for (bool b : use) streams += b ? 1 : 0;
     const bool fork = streams > 1;
     auto on = [&](int k) { return fork ? W.aux[k] : s; };
     if (fork) {
         RMX_CUDA(cudaEventRecord(W.fork, s));
-        for (int k = 0; k < 4; k++)
+        for (int k = 0; k < 5; k++)
             if (use[k]) RMX_CUDA(cudaStreamWaitEvent(W.aux[k], W.fork, 0));
+    }
+    if (n_hub > 0) {  // every hub unit split over many blocks (see k_hub_plan); first: the longest chain
+        a.range = bucket_off + first_bucket + kBinHub;
+        HubPlan hp;
+        hp.coff = W.hub_coff;
+        hp.poff = W.hub_poff;
+        hp.loff = W.hub_loff;
+        hp.nparts = W.hub_nparts;
+        hp.own = W.hub_own;
+        hp.act = W.hub_act;
+        hp.pcnt = W.hub_pcnt;
+        hp.pstart = W.hub_pstart;
+        hp.best = W.hub_best;
+        hp.bmod = W.hub_bmod;
+        hp.bkey = W.hub_bkey;
+        hp.bfx = W.hub_bfx;
+        hp.tot = W.hub_tot;
+        hp.max_units = W.hub_units;
+        hp.max_parts = W.hub_parts;
+        hp.max_links = W.hub_links;
+        hp.part_links = tg.hub_part;
+        const cudaStream_t hs = on(4);
+        const unsigned G = num_sms() * 8, GE = num_sms() * 2;
+        if (tm) tm->begin(kTimerBinHub, hs);
+        k_hub_plan<<<1, 1024, 0, hs>>>(a, hp);
+        RMX_LAUNCHED();
+        k_hub_links<false><<<G, kHubPT, 0, hs>>>(a, hp);
+        RMX_LAUNCHED();
+        k_hub_offsets<<<1, 1024, 0, hs>>>(hp);
+        RMX_LAUNCHED();
+        k_hub_links<true><<<G, kHubPT, 0, hs>>>(a, hp);
+        RMX_LAUNCHED();
+        k_hub_eval<<<GE, kHubPT, kHubEvalSmem, hs>>>(a, hp);
+        RMX_LAUNCHED();
+        k_hub_finish<<<blocks_for(W.hub_units * 32, 256, num_sms() * 16), 256, 0, hs>>>(a, hp);
+        RMX_LAUNCHED();
+        if (a.mark) {
+            k_hub_mark<<<G, kHubPT, 0, hs>>>(a, hp);
+            RMX_LAUNCHED();
+        }
+        if (tm) tm->end(kTimerBinHub, hs);
     }
     if (n_mid > 0) {
         a.range = bucket_off + first_bucket + kBinMid;
@@ -1489,44 +1642,6 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
         RMX_LAUNCHED();
         if (tm) tm->end(kTimerBinLarge, on(1));
     }
-    if (n_hub > 0) {  // every hub unit split over many blocks (see k_hub_plan)
-        a.range = bucket_off + first_bucket + kBinHub;
-        HubPlan hp;
-        hp.cap = W.hub_cap;
-        hp.toff = W.hub_toff;
-        hp.coff = W.hub_coff;
-        hp.eoff = W.hub_eoff;
-        hp.own = W.hub_own;
-        hp.best = W.hub_best;
-        hp.bmod = W.hub_bmod;
-        hp.act = W.hub_act;
-        hp.tot = W.hub_tot;
-        hp.occ_n = W.hub_occ_n;
-        hp.slots = static_cast<HubSlot *>(W.hub_slots);
-        hp.occ = W.hub_occ;
-        hp.max_units = W.hub_units;
-        hp.max_slots = W.gcap;
-        hp.max_items = W.hub_items;
-        hp.max_list = W.hub_list;
-        const cudaStream_t hs = on(1);
-        const unsigned G = num_sms() * 8;
-        if (tm) tm->begin(kTimerBinHub, hs);
-        k_hub_plan<<<1, 1024, 0, hs>>>(a, hp);
-        RMX_LAUNCHED();
-        k_hub_insert<<<G, kHubPT, 0, hs>>>(a, hp);
-        RMX_LAUNCHED();
-        k_hub_own<<<blocks_for(W.hub_units, 256, num_sms() * 8), 256, 0, hs>>>(a, hp);
-        RMX_LAUNCHED();
-        k_hub_eval<<<G, kHubPT, 0, hs>>>(a, hp);
-        RMX_LAUNCHED();
-        k_hub_finish<<<blocks_for(W.hub_units * 32, 256, num_sms() * 16), 256, 0, hs>>>(a, hp);
-        RMX_LAUNCHED();
-        if (a.mark) {
-            k_hub_mark<<<G, kHubPT, 0, hs>>>(a, hp);
-            RMX_LAUNCHED();
-        }
-        if (tm) tm->end(kTimerBinHub, hs);
-    }
     if (n_warp > 0) {
         a.range = bucket_off + first_bucket + kBinWarp;
         if (tm) tm->begin(kTimerBinWarp, on(2));
@@ -1542,7 +1657,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
         if (tm) tm->end(kTimerBinReg, s);
     }
     if (fork)
-        for (int k = 0; k < 4; k++)
+        for (int k = 0; k < 5; k++)
             if (use[k]) {
                 RMX_CUDA(cudaEventRecord(W.join[k], W.aux[k]));
                 RMX_CUDA(cudaStreamWaitEvent(s, W.join[k], 0));
@@ -1567,6 +1682,8 @@ void configure_eval_kernels() {
     RMX_CUDA(cudaFuncSetAttribute(k_eval_block<kLrgT, kLrgCap>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   100));
     RMX_CUDA(cudaFuncSetAttribute(k_eval_warp, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    RMX_CUDA(cudaFuncSetAttribute(k_hub_eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHubEvalSmem));
+    RMX_CUDA(cudaFuncSetAttribute(k_hub_eval, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
     configured[dev] = true;
 }
 

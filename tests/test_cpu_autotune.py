@@ -33,7 +33,7 @@ def test_tuning_abi_defaults_and_validation(restore_tuning):
     assert set_tuning(warp_max_degree=64, mid_max_degree=64)["mid_max_degree"] == 64
     for bad in ({"warp_max_degree": 31}, {"warp_max_degree": 129}, {"mid_max_degree": 63},
                 {"mid_max_degree": 513}, {"block_max_degree": 1025}, {"large_max_degree": 1000},
-                {"large_max_degree": 4097}):
+                {"large_max_degree": 4097}, {"hub_partition_links": 63}, {"hub_partition_links": (1 << 30) + 1}):
         with pytest.raises(RmxError) as e:
             set_tuning(**bad)
         assert e.value.status == 1

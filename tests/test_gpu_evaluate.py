@@ -115,6 +115,34 @@ def test_degree_bins_all(built_lib, oracle_mod):
         compare(O, G, prep, st, np.arange(n, dtype=np.int32), np.ones(n, dtype=np.uint8))
 
 
+@pytest.mark.parametrize("tuning", [
+    {"large_max_degree": 1024, "hub_partition_links": 64},
+    {"large_max_degree": 32, "block_max_degree": 32, "mid_max_degree": 32, "warp_max_degree": 32,
+     "hub_partition_links": 1 << 30},
+])
+def test_hub_partitions(built_lib, oracle_mod, tuning):
+    """The hub pipeline under other partition sizes: partitions of 64 links
+    (many per unit), and one partition per unit for every unit above 32 links,
+    so that units of 2500 and 5500 distinct neighbour modules overfill the
+    partition table and are aggregated in rounds."""
+    from relaxmap_b200 import Graph, get_tuning, set_tuning
+    O = oracle_mod
+    n, src, dst, w = all_bins_graph()
+    prep = O.prepare(O.from_edges(n, src, dst, w))
+    st = O.initiate(prep)
+    before = get_tuning()
+    rng = np.random.default_rng(6)
+    try:
+        set_tuning(**tuning)
+        with Graph.from_edges(src, dst, w, n=n) as G:
+            compare(O, G, prep, st, np.arange(n, dtype=np.int32))
+            for k in (400, 3):
+                part = (rng.integers(0, k, n) * (n // k)).astype(np.int32)
+                compare(O, G, prep, st, part)
+    finally:
+        set_tuning(**before)
+
+
 # ------------------------------------------------------------ super-node level
 
 def sn_units(O, G, part):
