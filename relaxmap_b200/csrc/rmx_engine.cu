@@ -728,6 +728,7 @@ void rmx_graph::ensure_hub_table(const Level &lv) {
     work.hub_units = U;
     work.hub_parts = P;
     work.hub_links = Lk;
+    work.hub_gen++;
 }
 
 void rmx_graph::initiate() {
@@ -819,7 +820,7 @@ void rmx_graph::run_subbatches(Level &lv, int64_t n_active, ModState &M, InstSta
             sweep_subbatch(lv, M, I, work, sa, sb, work.dparams + 2 * sb, mark, true, stream, tm);
         return;
     }
-    const SweepGraphKey key{&lv, &M, &I, sa.allow_new, mark ? 1 : 0, sa.vthresh, ns, work.hub_bkey, work.hub_links,
+    const SweepGraphKey key{&lv, &M, &I, sa.allow_new, mark ? 1 : 0, sa.vthresh, ns, work.hub_gen,
                             eval_tuning_generation()};
     SweepGraph *gr = nullptr;
     for (SweepGraph &g : sweep_graphs)
@@ -986,8 +987,8 @@ void rmx_graph::stage_sweeps_graph(Level &lv, bool allow_new, std::vector<double
     if (!any_set(act) || opt.max_iter <= 0) return;
     const int ns = sub_batches_for(lv.n);
     const StageGraphKey key{&lv,          &mods, &inst1,   allow_new ? 1 : 0, prior ? 1 : 0,
-                            opt.max_iter, ns,    vthresh,  opt.threshold,     work.hub_bkey,
-                            work.hub_links,    eval_tuning_generation(), scratch.mark()};
+                            opt.max_iter, ns,    vthresh,  opt.threshold,     work.hub_gen,
+                            eval_tuning_generation(), scratch.mark()};
     RMX_CUDA(cudaMemcpyAsync(stage_sweeping, act.data(), (size_t)K, cudaMemcpyHostToDevice, stream));
     loop_graph(key, lv.n, [&](unsigned long long cond) { stage_body(lv, allow_new, prior, vthresh, ns, cond); });
     RMX_CUDA(cudaMemcpyAsync(L.data(), inst1.L, sizeof(double) * K, cudaMemcpyDeviceToHost, stream));
@@ -1189,7 +1190,7 @@ void rmx_graph::generate_sub_modules() {
         const int nsg = sub_batches_for(N);
         if (stage_graph_ok(sub_lv) && opt.max_iter > 0) {
             const StageGraphKey key{&sub_lv, &submods, &instsub, 0, 0, opt.max_iter, nsg, 0.0, opt.threshold,
-                                    work.hub_bkey, work.hub_links, eval_tuning_generation(), scratch.mark()};
+                                    work.hub_gen, eval_tuning_generation(), scratch.mark()};
             loop_graph(key, N, [&](unsigned long long cond) { subtune_body(nsg, cond); });
         }
         for (int iter = 0; iter < opt.max_iter && !stage_graph_ok(sub_lv); iter++) {

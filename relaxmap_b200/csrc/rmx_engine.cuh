@@ -175,6 +175,7 @@ struct SweepWork {
     // the buckets of partitioned links (hub_links entries), sized for every
     // hub unit of the current level
     int64_t hub_units = 0, hub_parts = 0, hub_links = 0;  // capacities
+    int64_t hub_gen = 0;                                   // allocations so far
     int64_t *hub_coff = nullptr, *hub_poff = nullptr, *hub_loff = nullptr, *hub_pstart = nullptr;
     int32_t *hub_nparts = nullptr;
     fx_t *hub_own = nullptr;

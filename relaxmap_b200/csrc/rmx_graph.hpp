@@ -32,12 +32,11 @@ struct SweepGraphKey {
     int allow_new, mark;
     double vthresh;
     int nsub;
-    const void *hub_buckets;
-    int64_t hub_links;
+    int64_t hub_gen;  // the hub arrays' allocation: graphs hold their addresses
     int tuning_gen;  // eval_tuning_generation() at capture: grid sizes are part of the graph
     bool operator==(const SweepGraphKey &o) const {
         return lv == o.lv && M == o.M && I == o.I && allow_new == o.allow_new && mark == o.mark &&
-               vthresh == o.vthresh && nsub == o.nsub && hub_buckets == o.hub_buckets && hub_links == o.hub_links &&
+               vthresh == o.vthresh && nsub == o.nsub && hub_gen == o.hub_gen &&
                tuning_gen == o.tuning_gen;
     }
 };
@@ -57,14 +56,13 @@ struct StageGraphKey {
     const rmx::InstState *I;
     int allow_new, prior, max_iter, nsub;
     double vthresh, threshold;
-    const void *hub_buckets;
-    int64_t hub_links;
+    int64_t hub_gen;  // the hub arrays' allocation: graphs hold their addresses
     int tuning_gen;
     size_t scratch_mark;  // the scratch the body's primitives use starts here
     bool operator==(const StageGraphKey &o) const {
         return lv == o.lv && M == o.M && I == o.I && allow_new == o.allow_new && prior == o.prior &&
                max_iter == o.max_iter && nsub == o.nsub && vthresh == o.vthresh && threshold == o.threshold &&
-               hub_buckets == o.hub_buckets && hub_links == o.hub_links && tuning_gen == o.tuning_gen && scratch_mark == o.scratch_mark;
+               hub_gen == o.hub_gen && tuning_gen == o.tuning_gen && scratch_mark == o.scratch_mark;
     }
 };
 struct StageGraph {
