@@ -36,7 +36,7 @@ def test_launch_shape_does_not_change_results(graph):
                 dict(DEFAULTS, warp_max_degree=48, mid_max_degree=200, block_max_degree=200, large_max_degree=700),
                 dict(DEFAULTS, warp_max_degree=128, mid_max_degree=128, block_max_degree=1024,
                      large_max_degree=1024),
-                dict(DEFAULTS, large_max_degree=256, block_max_degree=256, hub_partition_links=64),
+                dict(DEFAULTS, mid_max_degree=256, block_max_degree=256, large_max_degree=256, hub_partition_links=64),
                 DEFAULTS):
         set_tuning(**cfg)
         for _ in range(2):  # the second run replays the sweep graphs captured by the first
