@@ -90,6 +90,8 @@ typedef struct {
     double eval_bin_ms[6];   /* move evaluation per degree bin (register, warp, mid, block, large, hub): summed
                                 kernel time; the bins of one sub-batch run concurrently on separate streams */
     int64_t eval_bin_launches[6];
+    int64_t eval_bin_links[6]; /* links read per degree bin since profiling was enabled */
+    double eval_bin_bytes[6];  /* compulsory bytes per degree bin (links, units, module statistics) while profiling */
 } rmx_profile;
 
 const char *rmx_last_error(void);

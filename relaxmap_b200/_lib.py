@@ -51,7 +51,8 @@ class Profile(C.Structure):
                 ("power_iters", C.c_int64), ("total_ms", C.c_double), ("kernel_launches", C.c_int64),
                 ("links_evaluated", C.c_int64), ("units_evaluated", C.c_int64), ("adjoint_iters", C.c_int64),
                 ("level_ms", C.c_double * 3), ("candidates_evaluated", C.c_int64),
-                ("eval_bin_ms", C.c_double * 6), ("eval_bin_launches", C.c_int64 * 6)]
+                ("eval_bin_ms", C.c_double * 6), ("eval_bin_launches", C.c_int64 * 6),
+                ("eval_bin_links", C.c_int64 * 6), ("eval_bin_bytes", C.c_double * 6)]
 
 
 EVAL_BINS = ["reg", "warp", "mid", "block", "large", "hub"]
@@ -283,7 +284,8 @@ class Graph:
                    units_evaluated=pr.units_evaluated, candidates_evaluated=pr.candidates_evaluated,
                    adjoint_iters=pr.adjoint_iters,
                    level_ms={"nodes": pr.level_ms[0], "super_nodes": pr.level_ms[1], "coarse_tune": pr.level_ms[2]},
-                   eval_bins={b: dict(ms=pr.eval_bin_ms[i], launches=pr.eval_bin_launches[i])
+                   eval_bins={b: dict(ms=pr.eval_bin_ms[i], launches=pr.eval_bin_launches[i],
+                                      links=pr.eval_bin_links[i], bytes=pr.eval_bin_bytes[i])
                               for i, b in enumerate(EVAL_BINS)})
         return out
 

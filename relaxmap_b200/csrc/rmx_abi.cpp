@@ -404,7 +404,8 @@ rmx_status rmx_set_profiling(rmx_graph *g, int32_t on) {
         g->timers.on = on != 0;
         g->timers.reset();
         g->prof = rmx_profile{};
-        RMX_CUDA(cudaMemsetAsync(g->work.counters + rmx::kCntEdges, 0, 3 * sizeof(int64_t), g->stream));
+        RMX_CUDA(cudaMemsetAsync(g->work.counters + rmx::kCntBins, 0, 3 * rmx::kEvalBins * sizeof(int64_t),
+                                 g->stream));
         RMX_CUDA(cudaStreamSynchronize(g->stream));
     });
 }
@@ -421,12 +422,17 @@ rmx_status rmx_get_profile(const rmx_graph *g, rmx_profile *out) {
             out->k[k].ms = g->timers.ms[k];
             out->k[k].bytes = 0.0;
         }
-        int64_t c[3];
-        RMX_CUDA(cudaMemcpyAsync(c, g->work.counters + rmx::kCntEdges, sizeof c, cudaMemcpyDeviceToHost, g->stream));
+        int64_t c[3 * rmx::kEvalBins];
+        RMX_CUDA(cudaMemcpyAsync(c, g->work.counters + rmx::kCntBins, sizeof c, cudaMemcpyDeviceToHost, g->stream));
         RMX_CUDA(cudaStreamSynchronize(g->stream));
-        out->links_evaluated = c[0];
-        out->units_evaluated = c[1];
-        out->candidates_evaluated = c[2];
+        out->links_evaluated = out->units_evaluated = out->candidates_evaluated = 0;
+        for (int b = 0; b < rmx::kEvalBins; b++) {
+            out->links_evaluated += c[3 * b];
+            out->units_evaluated += c[3 * b + 1];
+            out->candidates_evaluated += c[3 * b + 2];
+            out->eval_bin_links[b] = c[3 * b];
+            out->eval_bin_bytes[b] = g->timers.eval_bin_bytes[b];
+        }
         out->k[RMX_K_EVAL].bytes = g->timers.eval_bytes;  // compulsory bytes per launch group (Timers)
         // The transposed solve, per sweep: link index, weight and the gathered
         // adjoint value (4 + 8 + 8 B per link); per node, the offsets, row sum,

@@ -344,14 +344,14 @@ void Timers::end(int k, cudaStream_t s) {
 }
 
 __global__ void k_snapshot(const int64_t *counters, int64_t *dst) {
-    if (threadIdx.x < 3) dst[threadIdx.x] = counters[kCntEdges + threadIdx.x];
-    if (threadIdx.x == 3) dst[3] = counters[kCntMods];
+    if (threadIdx.x == 0) dst[0] = counters[kCntMods];
+    if (threadIdx.x < 3 * kEvalBins) dst[1 + threadIdx.x] = counters[kCntBins + threadIdx.x];
 }
 
 void Timers::log_eval(const int64_t *counters, cudaStream_t s) {
     if (!on || !dlog) return;
     if (nlog == logcap) resolve();
-    k_snapshot<<<1, 32, 0, s>>>(counters, dlog + 4 * nlog);
+    k_snapshot<<<1, 32, 0, s>>>(counters, dlog + kLogWords * nlog);
     RMX_LAUNCHED();
     log_stream = s;
     nlog++;
@@ -367,14 +367,23 @@ void Timers::resolve() {
     pending.clear();
     used = 0;
     if (nlog > 0) {
-        std::vector<int64_t> h(4 * nlog);
+        std::vector<int64_t> h(kLogWords * nlog);
         RMX_CUDA(cudaMemcpyAsync(h.data(), dlog, sizeof(int64_t) * h.size(), cudaMemcpyDeviceToHost, log_stream));
         RMX_CUDA(cudaStreamSynchronize(log_stream));
         for (int64_t i = 0; i < nlog; i++) {
-            const int64_t *c = h.data() + 4 * i;
-            const double dl = (double)(c[0] - last[0]), du = (double)(c[1] - last[1]), dc = (double)(c[2] - last[2]);
-            eval_bytes += 16.0 * dl + 40.0 * du + 40.0 * std::min(dc, (double)c[3]);
-            for (int q = 0; q < 3; q++) last[q] = c[q];
+            const int64_t *c = h.data() + kLogWords * i;
+            const double mods = (double)c[0];
+            double tl = 0, tu = 0, tc = 0;
+            for (int b = 0; b < kEvalBins; b++) {
+                const int64_t *cb = c + 1 + 3 * b, *lb = last + 3 * b;
+                const double dl = (double)(cb[0] - lb[0]), du = (double)(cb[1] - lb[1]), dc = (double)(cb[2] - lb[2]);
+                eval_bin_bytes[b] += 16.0 * dl + 40.0 * du + 40.0 * std::min(dc, mods);
+                tl += dl;
+                tu += du;
+                tc += dc;
+            }
+            eval_bytes += 16.0 * tl + 40.0 * tu + 40.0 * std::min(tc, mods);
+            for (int q = 0; q < 3 * kEvalBins; q++) last[q] = c[1 + q];
         }
         nlog = 0;
     }
@@ -390,6 +399,7 @@ void Timers::reset() {
     nlog = 0;
     for (int64_t &v : last) v = 0;
     eval_bytes = 0.0;
+    for (double &v : eval_bin_bytes) v = 0.0;
 }
 
 void Timers::destroy() {
@@ -667,7 +677,7 @@ void rmx_graph::alloc_engine() {
     work.counters = perm.alloc<int64_t>(kCntSlots);
     work.dparams = perm.alloc<uint32_t>(64);
     timers.logcap = 8192;
-    timers.dlog = perm.alloc<int64_t>(4 * timers.logcap);
+    timers.dlog = perm.alloc<int64_t>(Timers::kLogWords * timers.logcap);
     stage_ctl = perm.alloc<int64_t>(8);
     stage_seed = perm.alloc<uint32_t>(8);
     stage_sweeping = perm.alloc<uint8_t>(std::max(K, 1));

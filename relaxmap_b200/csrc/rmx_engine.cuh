@@ -108,6 +108,17 @@ void count_units(const Level &L, ModState &M, cudaStream_t s);
 void refresh_terms(ModState &M, cudaStream_t s);
 // Code length per instance from the module statistics.
 void instance_codelength(const ModState &M, InstState &I, cudaStream_t s);
+
+// Counter slots in SweepWork::counters (device int64). kCntMods: non-empty
+// modules at the start of the current sweep (counted only while profiling).
+// kCntBins: per degree bin of the move evaluation (register, warp, mid,
+// block, large, hub), links read, units evaluated and candidates evaluated
+// (cumulative).
+enum {
+    kCntActive = 0, kCntFree = 1, kCntMoved = 3, kCntMods = 7, kCntBins = 8, kEvalBins = 6,
+    kCntSlots = kCntBins + 3 * kEvalBins
+};
+
 // Device time per kernel class, recorded with CUDA events on the stream.
 enum {
     kTimerSpmv = 0, kTimerEval, kTimerCommit, kTimerCoarsen, kTimerCodelen, kTimerOther, kTimerAdjoint,
@@ -133,13 +144,16 @@ struct Timers {
     // 8, neighbour's module 4), 40 B per unit (module id 4, statistics 32,
     // proposal written 4), and the module statistics (40 B) once per launch,
     // at most one per candidate: 40 * min(candidates, non-empty modules).
+    // The same per degree bin (each bin's kernel reads its own statistics).
     // Each launch group appends the running counters to a device log
     // (log_eval); resolve() turns consecutive entries into per-launch counts.
-    int64_t *dlog = nullptr;  // 4 per entry: links, units, candidates (cumulative), non-empty modules
+    static constexpr int kLogWords = 1 + 3 * kEvalBins;  // non-empty modules, then the bin counters
+    int64_t *dlog = nullptr;
     int64_t nlog = 0, logcap = 0;
     cudaStream_t log_stream = nullptr;  // the stream the log entries were written on
-    int64_t last[3] = {0, 0, 0};
+    int64_t last[3 * kEvalBins] = {};
     double eval_bytes = 0.0;
+    double eval_bin_bytes[kEvalBins] = {};
     void begin(int k, cudaStream_t s);
     void end(int k, cudaStream_t s);
     void log_eval(const int64_t *counters, cudaStream_t s);
@@ -148,12 +162,6 @@ struct Timers {
     void destroy();
 };
 
-// Counter slots in SweepWork::counters (device int64). kCntMods: non-empty
-// modules at the start of the current sweep (counted only while profiling).
-enum {
-    kCntActive = 0, kCntFree = 1, kCntMoved = 3, kCntEdges = 4, kCntUnits = 5, kCntCands = 6, kCntMods = 7,
-    kCntSlots = 8
-};
 
 // Per-level sweep workspace (sized for the largest level: N units, N modules).
 struct SweepWork {

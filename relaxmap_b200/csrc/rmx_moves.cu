@@ -1469,7 +1469,7 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     a.range = nullptr;
     a.prop = W.prop;
     a.pdelta = W.pdelta;
-    a.stats = reinterpret_cast<unsigned long long *>(W.counters + kCntEdges);
+    a.stats = reinterpret_cast<unsigned long long *>(W.counters + kCntBins);  // the register bins' (the first)
     a.vthresh = vthresh;
     a.allow_new = allow_new;
     a.allow_new_unit = allow_unit;
@@ -1574,6 +1574,8 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     for (bool b : use) streams += b ? 1 : 0;
     const bool fork = streams > 1;
     auto on = [&](int k) { return fork ? W.aux[k] : s; };
+    unsigned long long *const stats0 = a.stats;  // each bin counts into its own three slots
+    auto bin_stats = [&](int timer) { return stats0 + 3 * (timer - kTimerBinReg); };
     if (fork) {
         RMX_CUDA(cudaEventRecord(W.fork, s));
         for (int k = 0; k < 5; k++)
@@ -1581,6 +1583,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     }
     if (n_hub > 0) {  // every hub unit split over many blocks (see k_hub_plan); first: the longest chain
         a.range = bucket_off + first_bucket + kBinHub;
+        a.stats = bin_stats(kTimerBinHub);
         HubPlan hp;
         hp.coff = W.hub_coff;
         hp.poff = W.hub_poff;
@@ -1622,6 +1625,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     }
     if (n_mid > 0) {
         a.range = bucket_off + first_bucket + kBinMid;
+        a.stats = bin_stats(kTimerBinMid);
         if (tm) tm->begin(kTimerBinMid, on(3));
         k_eval_block<kMidT, kMidCap><<<fit_grid(n_mid, 1, (int64_t)num_sms() * tg.mid), kMidT, kMidSmem, on(3)>>>(a);
         RMX_LAUNCHED();
@@ -1629,6 +1633,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     }
     if (n_blk > 0) {
         a.range = bucket_off + first_bucket + kBinBlock;
+        a.stats = bin_stats(kTimerBinBlock);
         if (tm) tm->begin(kTimerBinBlock, on(0));
         k_eval_block<kBlkT, kBlkCap><<<fit_grid(n_blk, 1, (int64_t)num_sms() * tg.block), kBlkT, kBlkSmem, on(0)>>>(
             a);
@@ -1637,6 +1642,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     }
     if (n_lrg > 0) {
         a.range = bucket_off + first_bucket + kBinLarge;
+        a.stats = bin_stats(kTimerBinLarge);
         if (tm) tm->begin(kTimerBinLarge, on(1));
         k_eval_block<kLrgT, kLrgCap><<<fit_grid(n_lrg, 1, (int64_t)num_sms() * tg.large), kLrgT, kLrgSmem, on(1)>>>(a);
         RMX_LAUNCHED();
@@ -1644,6 +1650,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     }
     if (n_warp > 0) {
         a.range = bucket_off + first_bucket + kBinWarp;
+        a.stats = bin_stats(kTimerBinWarp);
         if (tm) tm->begin(kTimerBinWarp, on(2));
         k_eval_warp<<<fit_grid(n_warp, kEvalWarps, (int64_t)num_sms() * tg.warp), kEvalWarps * 32, 0, on(2)>>>(a);
         RMX_LAUNCHED();
@@ -1651,6 +1658,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
     }
     if (n_reg > 0) {
         a.range = bucket_off + first_bucket + kBinReg8;
+        a.stats = bin_stats(kTimerBinReg);
         if (tm) tm->begin(kTimerBinReg, s);
         k_eval_reg<<<fit_grid(n_reg, 8, (int64_t)num_sms() * tg.reg), 256, 0, s>>>(a);
         RMX_LAUNCHED();
