@@ -830,6 +830,7 @@ __device__ __forceinline__ void hub_link(const EvalArgs &a, int64_t ob, int64_t 
 // counts hold the scatter exactly.
 template <bool SCATTER>
 __global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
+    constexpr int ILP = 4;  // links gathered per thread before any is combined
     __shared__ fx_t wq[kHubPT];
     const int lane = threadIdx.x & 31;
     const int64_t h0 = a.range[0], total = p.tot[0];
@@ -842,43 +843,56 @@ __global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
         const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
         const int64_t c0 = (item - p.coff[j]) * kHubCh, c1 = min(d, c0 + kHubCh);
         fx_t oA = 0, iA = 0;
-        for (int64_t b = c0; b < c1; b += kHubPT) {  // uniform over the block: every warp runs every step
-            const int64_t l = b + threadIdx.x;
-            int32_t key = A;
-            bool in = false;
-            fx_t q = 0;
-            if (l < c1) hub_link(a, ob, ib, dout, l, key, in, q);
-            if (key == A) {  // also the lanes past the chunk (q = 0)
-                if (in)
-                    iA += q;
-                else
-                    oA += q;
+        for (int64_t b0 = c0; b0 < c1; b0 += kHubPT * ILP) {  // uniform over the block
+            int32_t keys[ILP];
+            bool ins[ILP];
+            fx_t qs[ILP];
+#pragma unroll
+            for (int k = 0; k < ILP; k++) {
+                const int64_t l = b0 + k * kHubPT + threadIdx.x;
+                keys[k] = A;  // lanes past the chunk: flow 0 to the own module
+                ins[k] = false;
+                qs[k] = 0;
+                if (l < c1) hub_link(a, ob, ib, dout, l, keys[k], ins[k], qs[k]);
             }
-            const bool valid = key != A;
-            const uint32_t kd = in ? ((uint32_t)key | 0x80000000u) : (uint32_t)key;
-            const unsigned kpeers = __match_any_sync(kFull, valid ? (unsigned long long)kd : ~0ull);
-            const bool head = valid && lane == __ffs(kpeers) - 1;  // one lane per (module, direction)
-            const int32_t part = head ? (int32_t)(part_hash(key) % (uint32_t)np) : -1;
-            const unsigned peers = __match_any_sync(kFull, part);
-            const int leader = __ffs(peers) - 1;
-            if (!SCATTER) {
-                if (head && lane == leader) atomicAdd(p.pcnt + p.poff[j] + part, (unsigned long long)__popc(peers));
-            } else {
-                wq[threadIdx.x] = q;
-                __syncwarp();
-                fx_t sum = 0;
-                if (head)
-                    for (unsigned m = kpeers; m; m &= m - 1) sum += wq[(threadIdx.x & ~31) + __ffs(m) - 1];
-                unsigned long long base = 0;
-                const int64_t pidx = p.poff[j] + part;
-                if (head && lane == leader) base = atomicAdd(p.pcnt + pidx, (unsigned long long)__popc(peers));
-                base = __shfl_sync(kFull, base, leader);
-                if (head) {
-                    const int64_t pos = p.pstart[pidx] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
-                    p.bkey[pos] = (int32_t)kd;
-                    p.bfx[pos] = sum;
+#pragma unroll
+            for (int k = 0; k < ILP; k++) {
+                const int32_t key = keys[k];
+                const bool in = ins[k];
+                const fx_t q = qs[k];
+                if (key == A) {
+                    if (in)
+                        iA += q;
+                    else
+                        oA += q;
                 }
-                __syncwarp();
+                const bool valid = key != A;
+                const uint32_t kd = in ? ((uint32_t)key | 0x80000000u) : (uint32_t)key;
+                const unsigned kpeers = __match_any_sync(kFull, valid ? (unsigned long long)kd : ~0ull);
+                const bool head = valid && lane == __ffs(kpeers) - 1;  // one lane per (module, direction)
+                const int32_t part = head ? (int32_t)(part_hash(key) % (uint32_t)np) : -1;
+                const unsigned peers = __match_any_sync(kFull, part);
+                const int leader = __ffs(peers) - 1;
+                if (!SCATTER) {
+                    if (head && lane == leader)
+                        atomicAdd(p.pcnt + p.poff[j] + part, (unsigned long long)__popc(peers));
+                } else {
+                    wq[threadIdx.x] = q;
+                    __syncwarp();
+                    fx_t sum = 0;
+                    if (head)
+                        for (unsigned m = kpeers; m; m &= m - 1) sum += wq[(threadIdx.x & ~31) + __ffs(m) - 1];
+                    unsigned long long base = 0;
+                    const int64_t pidx = p.poff[j] + part;
+                    if (head && lane == leader) base = atomicAdd(p.pcnt + pidx, (unsigned long long)__popc(peers));
+                    base = __shfl_sync(kFull, base, leader);
+                    if (head) {
+                        const int64_t pos = p.pstart[pidx] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
+                        p.bkey[pos] = (int32_t)kd;
+                        p.bfx[pos] = sum;
+                    }
+                    __syncwarp();
+                }
             }
         }
         if (!SCATTER) {
@@ -925,6 +939,7 @@ __global__ void __launch_bounds__(kHubPT, 2) k_hub_eval(EvalArgs a, HubPlan p) {
     int32_t *keys = reinterpret_cast<int32_t *>(vi + kPartCap);
     __shared__ double sb[kHubPT / 32];
     __shared__ int32_t sm[kHubPT / 32];
+    __shared__ int16_t taken[kPartCap / 2 + kHubPT];  // slots taken in this round, in the order taken
     __shared__ int nfresh;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t h0 = a.range[0], total = p.tot[1];
@@ -964,16 +979,19 @@ __global__ void __launch_bounds__(kHubPT, 2) k_hub_eval(EvalArgs a, HubPlan p) {
                         sl = (sl + 1) & mask;
                         prev = atomicCAS(keys + sl, kEmpty, key);
                     }
-                    if (prev != kEmpty && prev != key) break;  // full: nfresh is past the limit already
-                    if (prev == kEmpty) atomicAdd(&nfresh, 1);
+                    if (prev != kEmpty && prev != key) continue;  // unreachable: the table is never full
+                    if (prev == kEmpty) taken[atomicAdd(&nfresh, 1)] = (int16_t)sl;
                     atomic_add_fx(kd < 0 ? vi + sl : vo + sl, p.bfx[e]);
                 }
                 __syncthreads();
-                overfull = nfresh > kPartCap / 2;
-                // evaluate the table's candidates (unless the round overfilled) and empty it
-                for (int s = threadIdx.x; s < kPartCap; s += kHubPT) {
+                // at most kPartCap / 2 + kHubPT slots were taken (every thread checks the
+                // count before it inserts), so the table never fills and the list holds them all
+                const int nt = nfresh;
+                overfull = nt > kPartCap / 2;
+                // evaluate the taken slots' candidates (unless the round overfilled) and empty them
+                for (int i = threadIdx.x; i < nt; i += kHubPT) {
+                    const int s = taken[i];
                     const int32_t k = keys[s];
-                    if (k == kEmpty) continue;
                     if (!overfull && k != A) {
                         rc++;
                         const double dl = candidate_delta(c, a.mstat[k], a.mterm[k], vo[s], vi[s]);
