@@ -196,10 +196,15 @@ def peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-# DRAM bytes per evaluated link of the move evaluation, from one ncu capture
-# on the benched R-MAT family (the command and counters are in profiles/).
-# None where no capture of that workload exists.
+# DRAM bytes (read + write) per link evaluated by the dominant evaluation
+# kernel, keyed by (workload, degree bin): from one ncu capture of that kernel
+# on the benched graph (the command and the counters are in profiles/).
 EVAL_TRAFFIC_PER_LINK = {}
+
+# The kernel (or kernel chain) each degree bin of the evaluation launches.
+EVAL_BIN_KERNELS = {"reg": "k_eval_reg", "warp": "k_eval_warp", "mid": "k_eval_block<128, 1024>",
+                    "block": "k_eval_block<256, 2048>", "large": "k_eval_block<512, 8192>",
+                    "hub": "k_hub_plan/links/offsets/eval/finish/mark"}
 
 
 def profile_run(g, desc: str):
@@ -239,6 +244,7 @@ def eval_snapshot(g, desc: str):
     G.close()
     d = {k: p1[k] - p0[k] for k in ("links_evaluated", "units_evaluated", "candidates_evaluated")}
     d["bytes"] = eval_bytes(d["links_evaluated"], d["units_evaluated"], d["candidates_evaluated"], g.n)
+    d["bin_links"] = {b: p1["eval_bins"][b]["links"] - p0["eval_bins"][b]["links"] for b in p1["eval_bins"]}
     print(json.dumps({"workload": desc, "nodes": g.n, "links": g.m, "eval_group": d}))
 
 
@@ -426,14 +432,20 @@ def main():
         quality["note"] = ("the reference cannot run the full graph within a run's time (hours on the host): its "
                            "8-seed median is compared on the CPU sample, R-MAT scale 18")
 
-    # ---- roofline of the dominant kernel class (move evaluation)
+    # ---- roofline of the dominant kernel: the evaluation bin with the most
+    # device time (each bin's kernel timed on its own stream, its compulsory
+    # bytes counted from its own links, units and candidates)
     pk = peaks()
     ev = prof["eval"]
-    achieved = ev["bytes"] / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
-    per_link = EVAL_TRAFFIC_PER_LINK.get(args.workload)
+    bins = prof["eval_bins"]
+    dom = max(bins, key=lambda b: bins[b]["ms"])
+    db = bins[dom]
+    achieved = db["bytes"] / (db["ms"] / 1e3) / 1e9 if db["ms"] > 0 else 0.0
+    per_link = EVAL_TRAFFIC_PER_LINK.get((args.workload, dom))
     traffic = None
-    if per_link is not None and ev["launches"] > 0:
-        traffic = per_link * prof["links_evaluated"] / ev["launches"]
+    if per_link is not None and db["launches"] > 0:
+        traffic = per_link * db["links"] / db["launches"]
+    group_gbs = ev["bytes"] / (ev["ms"] / 1e3) / 1e9 if ev["ms"] > 0 else 0.0
     shares = {k: prof[k]["ms"] for k in ("spmv", "eval", "commit", "coarsen", "codelen", "other")}
     tot = sum(shares.values()) or 1.0
 
@@ -456,11 +468,18 @@ def main():
                              "optimize_device": dev_s * 1e3, "graph_destroy": close_s * 1e3},
                 "note": "a fresh handle per step: graph_create copies the host arrays in and builds the CSR/CSC; "
                         "optimize_wall includes the flow, the run and the partition copied back"},
-        "roofline": {"kernel": "move evaluation (warp/block/hub bins)", "bound": "hbm", "achieved": achieved,
-                     "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
+        "roofline": {"kernel": f"move evaluation, {dom} bin ({EVAL_BIN_KERNELS[dom]})", "bound": "hbm",
+                     "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                      "peak_source": pk["source"], "traffic": traffic,
-                     "algorithmic_bytes_per_launch": ev["bytes"] / max(ev["launches"], 1),
-                     "launch_ms_avg": ev["ms"] / max(ev["launches"], 1)},
+                     "algorithmic_bytes_per_launch": db["bytes"] / max(db["launches"], 1),
+                     "launch_ms_avg": db["ms"] / max(db["launches"], 1),
+                     "bins": {b: {"ms": round(v["ms"], 3), "launches": v["launches"], "links": v["links"],
+                                  "GB/s": round(v["bytes"] / v["ms"] / 1e6, 1) if v["ms"] > 0 else None}
+                              for b, v in bins.items()},
+                     "launch_group": {"GB/s": group_gbs, "frac": group_gbs / pk["hbm_gbs"],
+                                      "bytes_per_launch": ev["bytes"] / max(ev["launches"], 1),
+                                      "ms_avg": ev["ms"] / max(ev["launches"], 1),
+                                      "note": "one sub-batch: every bin, concurrently on six streams"}},
         "kernel_time_share": {k: round(v / tot, 4) for k, v in shares.items()},
         "profiled_run": {"level_ms": prof["level_ms"],
                          "eval_bin_ms": {b: round(v["ms"], 3) for b, v in prof["eval_bins"].items()},

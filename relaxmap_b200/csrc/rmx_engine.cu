@@ -686,7 +686,13 @@ void rmx_graph::alloc_engine() {
     RMX_CUDA(cudaMemsetAsync(work.claim, 0, sizeof(unsigned long long) * n, stream));
     RMX_CUDA(cudaMemsetAsync(work.next_active, 0, n, stream));
     RMX_CUDA(cudaMemsetAsync(work.counters, 0, sizeof(int64_t) * kCntSlots, stream));
-    for (cudaStream_t &a : work.aux) RMX_CUDA(cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking));
+    // the hub pipeline's stream (aux[4]) at the highest priority: its chain of
+    // dependent kernels is the longest of a sub-batch, so its blocks go first
+    // whenever the other bins' blocks leave an SM
+    int prio_low = 0, prio_high = 0;
+    RMX_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    for (int k = 0; k < 5; k++)
+        RMX_CUDA(cudaStreamCreateWithPriority(&work.aux[k], cudaStreamNonBlocking, k == 4 ? prio_high : prio_low));
     RMX_CUDA(cudaEventCreateWithFlags(&work.fork, cudaEventDisableTiming));
     for (cudaEvent_t &e : work.join) RMX_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 }
@@ -707,20 +713,23 @@ int64_t rmx_graph::max_degree(const Level &lv) {
 // never shrunk.
 void rmx_graph::ensure_hub_table(const Level &lv) {
     if (lv.n <= 0) return;
-    int64_t need[3];
+    int64_t need[4];
     hub_level_needs(lv, need, dtmp + 12, stream);
-    const int64_t units = need[0], parts = need[1], links = need[2];
-    if (units == 0 || (units <= work.hub_units && parts <= work.hub_parts && links <= work.hub_links)) return;
+    const int64_t units = need[0], parts = need[1], links = need[2], chunks = need[3];
+    if (units == 0 || (units <= work.hub_units && parts <= work.hub_parts && links <= work.hub_links &&
+                       chunks <= work.hub_chunks))
+        return;
     RMX_CUDA(cudaStreamSynchronize(stream));  // no launch still reads the old arrays
     hub_arena.destroy();
     const int64_t U = std::max(units, work.hub_units) * 5 / 4 + 16, P = std::max(parts, work.hub_parts) * 5 / 4 + 64,
-                  Lk = std::max(links, work.hub_links) * 5 / 4 + 1024;
-    work.hub_units = work.hub_parts = work.hub_links = 0;
+                  Lk = std::max(links, work.hub_links) * 5 / 4 + 1024,
+                  C = std::max(chunks, work.hub_chunks) * 5 / 4 + 64;
+    work.hub_units = work.hub_parts = work.hub_links = work.hub_chunks = 0;
     work.hub_bkey = nullptr;
     const size_t bytes = (size_t)Lk * (sizeof(int32_t) + sizeof(fx_t)) + (size_t)(U + 1) * 3 * sizeof(int64_t) +
                          (size_t)U * (2 * sizeof(fx_t) + sizeof(int32_t) + 1) +
                          (size_t)P * (sizeof(unsigned long long) + sizeof(double) + sizeof(int32_t)) +
-                         (size_t)(P + 1) * sizeof(int64_t) + 16 * 256;
+                         (size_t)(P + 1) * sizeof(int64_t) + (size_t)(C + P) * sizeof(int32_t) + 16 * 256;
     hub_arena.init(bytes);
     work.hub_bfx = hub_arena.alloc<fx_t>(Lk);
     work.hub_bkey = hub_arena.alloc<int32_t>(Lk);
@@ -735,9 +744,12 @@ void rmx_graph::ensure_hub_table(const Level &lv) {
     work.hub_pstart = hub_arena.alloc<int64_t>(P + 1);
     work.hub_bmod = hub_arena.alloc<int32_t>(P);
     work.hub_tot = hub_arena.alloc<int64_t>(8);
+    work.hub_cunit = hub_arena.alloc<int32_t>(C);
+    work.hub_punit = hub_arena.alloc<int32_t>(P);
     work.hub_units = U;
     work.hub_parts = P;
     work.hub_links = Lk;
+    work.hub_chunks = C;
     work.hub_gen++;
 }
 

@@ -182,10 +182,10 @@ struct SweepWork {
     // the plan arrays (per unit), the partition arrays (per partition) and
     // the buckets of partitioned links (hub_links entries), sized for every
     // hub unit of the current level
-    int64_t hub_units = 0, hub_parts = 0, hub_links = 0;  // capacities
+    int64_t hub_units = 0, hub_parts = 0, hub_links = 0, hub_chunks = 0;  // capacities
     int64_t hub_gen = 0;                                   // allocations so far
     int64_t *hub_coff = nullptr, *hub_poff = nullptr, *hub_loff = nullptr, *hub_pstart = nullptr;
-    int32_t *hub_nparts = nullptr;
+    int32_t *hub_nparts = nullptr, *hub_cunit = nullptr, *hub_punit = nullptr;
     fx_t *hub_own = nullptr;
     uint8_t *hub_act = nullptr;
     unsigned long long *hub_pcnt = nullptr;
@@ -203,8 +203,8 @@ struct SweepWork {
 
 void configure_eval_kernels();
 // What the hub pipeline needs for a level: hub units (above
-// block_bin_max_degree), their partitions and their links (out[0..2]); one
-// device reduction, then a sync.
+// block_bin_max_degree), their partitions, their links and their link chunks
+// (out[0..3]); one device reduction, then a sync.
 void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_t s);
 
 // Launch shape of move evaluation, process-wide and read at every launch:

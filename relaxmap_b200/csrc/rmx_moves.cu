@@ -704,8 +704,9 @@ struct HubPlan {
     int32_t *bmod;                 // per partition: its module
     int32_t *bkey;                 // bucket elements: module | direction (bit 31 set: in-link)
     fx_t *bfx;                     //   and flow
+    int32_t *cunit, *punit;        // unit (index in the sub-batch) of every chunk item and partition
     int64_t *tot;                  // [0] chunks, [1] partitions, [2] units, [3] over capacity, [4] links
-    int64_t max_units, max_parts, max_links;  // capacities
+    int64_t max_units, max_parts, max_links, max_chunks;  // capacities
     int64_t part_links;                       // mean links per partition
 };
 
@@ -797,7 +798,7 @@ __global__ void __launch_bounds__(1024) k_hub_plan(EvalArgs a, HubPlan p) {
     }
     __shared__ int over;
     if (threadIdx.x == 0) {
-        over = r1 > p.max_parts || r2 > p.max_links;
+        over = r1 > p.max_parts || r2 > p.max_links || r0 > p.max_chunks;
         p.coff[nu] = r0;
         p.poff[nu] = r1;
         p.loff[nu] = r2;
@@ -836,12 +837,19 @@ __global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
     const int64_t h0 = a.range[0], total = p.tot[0];
     const int32_t nu = (int32_t)p.tot[2];
     for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-        const int32_t j = hub_find(p.coff, nu, item);
+        // the count pass finds each chunk's unit and lists it (and the unit's
+        // partitions, from its first chunk) for the later kernels
+        const int32_t j = SCATTER ? p.cunit[item] : hub_find(p.coff, nu, item);
         const int32_t u = a.list[h0 + j];
         const int32_t A = a.mod[u], np = p.nparts[j];
         const int64_t ob = a.out_off[u], ib = a.in_off[u];
         const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
         const int64_t c0 = (item - p.coff[j]) * kHubCh, c1 = min(d, c0 + kHubCh);
+        if (!SCATTER) {
+            if (threadIdx.x == 0) p.cunit[item] = j;
+            if (c0 == 0)
+                for (int q = threadIdx.x; q < np; q += kHubPT) p.punit[p.poff[j] + q] = j;
+        }
         fx_t oA = 0, iA = 0;
         for (int64_t b0 = c0; b0 < c1; b0 += kHubPT * ILP) {  // uniform over the block
             int32_t keys[ILP];
@@ -951,7 +959,7 @@ __global__ void __launch_bounds__(kHubPT, 2) k_hub_eval(EvalArgs a, HubPlan p) {
         vo[s] = vi[s] = 0;
     }
     for (int64_t pidx = blockIdx.x; pidx < total; pidx += gridDim.x) {
-        const int32_t j = hub_find(p.poff, nu, pidx);
+        const int32_t j = p.punit[pidx];
         const int32_t u = a.list[h0 + j];
         const int64_t b0 = p.pstart[pidx], b1 = p.pstart[pidx + 1];
         const int32_t A = a.mod[u];
@@ -1091,7 +1099,7 @@ __global__ void __launch_bounds__(kHubPT) k_hub_mark(EvalArgs a, HubPlan p) {
     const int64_t h0 = a.range[0], total = p.tot[0];
     const int32_t nu = (int32_t)p.tot[2];
     for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-        const int32_t j = hub_find(p.coff, nu, item);
+        const int32_t j = p.cunit[item];
         if (!p.act[j]) continue;
         const int32_t u = a.list[h0 + j];
         const int64_t ob = a.out_off[u], ib = a.in_off[u];
@@ -1499,35 +1507,38 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
 
 __global__ void k_hub_level(int32_t n, const int64_t *out_off, const int64_t *in_off, int64_t bound, int64_t part_links,
                             unsigned long long *acc) {
-    unsigned long long c0 = 0, c1 = 0, c2 = 0;
+    unsigned long long c0 = 0, c1 = 0, c2 = 0, c3 = 0;
     for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
         const int64_t d = (out_off[u + 1] - out_off[u]) + (in_off[u + 1] - in_off[u]);
         if (d <= bound) continue;
         c0++;
         c1 += min((int64_t)kMaxParts, (d + part_links - 1) / part_links);
         c2 += d;
+        c3 += (d + kHubCh - 1) / kHubCh;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         c0 += __shfl_xor_sync(kFull, c0, o);
         c1 += __shfl_xor_sync(kFull, c1, o);
         c2 += __shfl_xor_sync(kFull, c2, o);
+        c3 += __shfl_xor_sync(kFull, c3, o);
     }
     if ((threadIdx.x & 31) == 0 && c0) {
         atomicAdd(acc, c0);
         atomicAdd(acc + 1, c1);
         atomicAdd(acc + 2, c2);
+        atomicAdd(acc + 3, c3);
     }
 }
 
 void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_t s) {
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(dev_tmp);
-    RMX_CUDA(cudaMemsetAsync(acc, 0, 3 * sizeof(unsigned long long), s));
+    RMX_CUDA(cudaMemsetAsync(acc, 0, 4 * sizeof(unsigned long long), s));
     const EvalTuning t = eval_tuning();
     k_hub_level<<<blocks_for(L.n, 256, num_sms() * 8), 256, 0, s>>>(L.n, L.out_off, L.in_off, t.large_max, t.hub_part,
                                                                     acc);
     RMX_LAUNCHED();
-    RMX_CUDA(cudaMemcpyAsync(out, acc, 3 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaMemcpyAsync(out, acc, 4 * sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -1619,6 +1630,9 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
         hp.max_units = W.hub_units;
         hp.max_parts = W.hub_parts;
         hp.max_links = W.hub_links;
+        hp.max_chunks = W.hub_chunks;
+        hp.cunit = W.hub_cunit;
+        hp.punit = W.hub_punit;
         hp.part_links = tg.hub_part;
         const cudaStream_t hs = on(4);
         const unsigned G = num_sms() * 8, GE = num_sms() * 2;
