@@ -289,7 +289,8 @@ rmx_status rmx_adjoint_backward(rmx_graph *g, const int32_t *part, double tau, d
  * up to mid_max_degree, the block bin up to block_max_degree, the large bin
  * up to large_max_degree, and the hub bin above; each hub unit's links are
  * partitioned by module into ceil(links / hub_partition_links) parts, each
- * aggregated by one block. Results do not depend on
+ * aggregated by one block (so are the links of a super-node of more than
+ * 16384 member links when the coarsening sums them). Results do not depend on
  * these values (every bin's kernel loops over its units by grid stride,
  * module statistics are exact integer sums, and every bin computes the same
  * change per candidate), only the time does. rmx_set_tuning takes effect at

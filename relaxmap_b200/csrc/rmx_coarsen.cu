@@ -183,6 +183,9 @@ constexpr int32_t kNoKey = -1;
 constexpr int kAggWarpLinks = 128, kAggWarpCap = 256, kAggWarps = 8;
 constexpr int kAggMidT = 128, kAggMidLinks = 1024, kAggMidCap = 2048;
 constexpr int kAggT = 512, kAggCap = 8192;
+// groups of more member links than this are split over many blocks (k_hg_*)
+constexpr int64_t kAggSplit = 16384;
+constexpr int kHgCh = 2048;  // links per chunk item (the mean links per partition is the hub_part tuning)
 
 __device__ __forceinline__ uint32_t agg_hash(uint32_t x) {
     x ^= x >> 16;
@@ -225,19 +228,42 @@ __global__ void k_agg_members(int32_t n, const int32_t *group, const int64_t *gm
 }
 
 // Groups by the bound on their distinct neighbours, min(links, groups): a
-// warp (<= 128), a 128-thread block (<= 1024) or a 512-thread block.
-__global__ void k_agg_bins(int32_t ng, const int64_t *gloff, uint8_t *small, uint8_t *mid, uint8_t *large,
-                           unsigned long long *maxlinks) {
-    unsigned long long mx = 0;
+// warp (<= 128), a 128-thread block (<= 1024) or a 512-thread block; groups
+// of more than kAggSplit links go to the split pipeline instead. maxlinks:
+// the most links of a group outside it; htot: the split pipeline's links,
+// chunks and partitions.
+__global__ void k_agg_bins(int32_t ng, const int64_t *gloff, int64_t part_links, uint8_t *small, uint8_t *mid,
+                           uint8_t *large, uint8_t *huge, unsigned long long *maxlinks, unsigned long long *htot) {
+    unsigned long long mx = 0, hl = 0, hc = 0, hp = 0;
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x) {
         const int64_t l = gloff[g + 1] - gloff[g], b = min(l, (int64_t)ng);
-        small[g] = b <= kAggWarpLinks ? 1 : 0;
-        mid[g] = b > kAggWarpLinks && b <= kAggMidLinks ? 1 : 0;
-        large[g] = b > kAggMidLinks ? 1 : 0;
-        mx = max(mx, (unsigned long long)l);
+        const bool hg = l > kAggSplit;
+        small[g] = !hg && b <= kAggWarpLinks ? 1 : 0;
+        mid[g] = !hg && b > kAggWarpLinks && b <= kAggMidLinks ? 1 : 0;
+        large[g] = !hg && b > kAggMidLinks ? 1 : 0;
+        huge[g] = hg ? 1 : 0;
+        if (hg) {
+            hl += l;
+            hc += (l + kHgCh - 1) / kHgCh;
+            hp += (l + part_links - 1) / part_links;
+        } else {
+            mx = max(mx, (unsigned long long)l);
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFullMask, mx, o));
-    if ((threadIdx.x & 31) == 0 && mx) atomicMax(maxlinks, mx);
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = max(mx, __shfl_xor_sync(kFullMask, mx, o));
+        hl += __shfl_xor_sync(kFullMask, hl, o);
+        hc += __shfl_xor_sync(kFullMask, hc, o);
+        hp += __shfl_xor_sync(kFullMask, hp, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (mx) atomicMax(maxlinks, mx);
+        if (hl) {
+            atomicAdd(htot, hl);
+            atomicAdd(htot + 1, hc);
+            atomicAdd(htot + 2, hp);
+        }
+    }
 }
 
 struct AggArgs {
@@ -442,6 +468,350 @@ __global__ void __launch_bounds__(kAggT, 2) k_agg_block(AggArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Huge groups (more than kAggSplit member links: the modules around R-MAT
+// hubs, up to millions of links) are not left to one block. Their links are
+// laid out in one virtual order (nonzero-degree members in member order, each
+// member's links in CSR order), cut into chunks of kHgCh links and
+// radix-partitioned by a hash of the destination group into partitions of
+// about part_links links, so that each partition's distinct destinations
+// fit one block's shared table:
+//   index    hidx (group -> huge index), the nonzero-degree members (hml),
+//            their virtual positions (hmo), each group's first member (hmb)
+//   plan     one block: chunk and partition offsets per huge group
+//   starts   every member lists the chunks that start inside it (cmem, cgrp)
+//   count    blocks take chunks and count each partition's elements
+//   offsets  one block turns the counts into bucket offsets
+//   scatter  blocks take chunks again and write (destination, flow)
+//   reduce   a block per partition sums its bucket in a shared table and
+//            appends the distinct destinations to the group's row
+// Lanes of a warp that reach the same destination are combined with
+// __match_any_sync before any counter update or bucket write (a hub's links
+// concentrate on a few large groups); both link passes form the same groups.
+constexpr int kHgT = 256, kHgCap = 4096;
+constexpr size_t kHgSmem = (size_t)kHgCap * (sizeof(fx_t) + sizeof(int32_t));
+
+struct HugeArgs {
+    const int64_t *off;
+    const int32_t *dst;
+    const fx_t *fx;
+    const int32_t *group;
+    const int32_t *members;
+    const int64_t *gloff;
+    const int32_t *hlist;   // huge groups, ascending
+    const int64_t *nh;      // their count (device)
+    int32_t *hidx;          // per group: index in hlist, or -1
+    const int32_t *hml;     // nonzero-degree members of huge groups (indices into members), ascending
+    const int64_t *nhm;     // their count (device)
+    int64_t *hmo;           // virtual position of each hml entry (nhm + 1)
+    int32_t *hgj;           // huge group of each hml entry
+    int64_t *hmb;           // per huge group (+1): first hml index
+    int64_t *coff, *poff;   // per huge group (+1): first chunk, first partition
+    int32_t *cmem, *cgrp;   // per chunk: hml index holding its first link, huge group
+    int32_t *pgrp;          // per partition: huge group
+    unsigned long long *pcnt;  // per partition: elements (counted), then the fill position
+    int64_t *pstart;        // per partition (+1): first bucket element
+    int32_t *bkey;          // bucket elements: destination group
+    fx_t *bfx;              //   and flow
+    int64_t *tot;           // [0] chunks [1] partitions [2] over capacity
+    int64_t max_chunks, max_parts, max_links;
+    int64_t part_links;     // mean links per partition
+    int32_t *slab_dst;
+    fx_t *slab_fx;
+    int64_t *rowlen;
+    fx_t *rowsum;
+};
+
+__device__ __forceinline__ uint32_t hg_part_hash(int32_t key) {
+    return agg_hash((uint32_t)key * 0x9E3779B1u + 0x7F4A7C15u);
+}
+
+__global__ void k_hg_index(HugeArgs a) {
+    const int64_t nh = *a.nh;
+    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nh; h += (int64_t)gridDim.x * blockDim.x)
+        a.hidx[a.hlist[h]] = (int32_t)h;
+}
+
+// flag[i]: member i belongs to a huge group and has links.
+__global__ void k_hg_member_flags(int32_t n, HugeArgs a, uint8_t *flag) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t u = a.members[i];
+        flag[i] = a.hidx[a.group[u]] >= 0 && a.off[u + 1] > a.off[u] ? 1 : 0;
+    }
+}
+
+// Degree of every hml entry (0 past the count, for the scan), its huge group,
+// and the first entry of every huge group.
+__global__ void k_hg_members(int32_t n, HugeArgs a, int64_t *deg) {
+    const int64_t nhm = *a.nhm;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
+        if (j >= nhm) {
+            deg[j] = 0;
+            continue;
+        }
+        const int32_t u = a.members[a.hml[j]];
+        deg[j] = a.off[u + 1] - a.off[u];
+        const int32_t h = a.hidx[a.group[u]];
+        a.hgj[j] = h;
+        if (j == 0 || a.hidx[a.group[a.members[a.hml[j - 1]]]] != h) a.hmb[h] = j;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.hmb[*a.nh] = nhm;
+}
+
+// Exclusive scan over the block (blockDim.x == 1024) of one value per thread.
+__device__ __forceinline__ long long hg_block_scan(long long v, long long *ws, long long *total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    long long x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(kFullMask, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) ws[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        long long t = ws[lane];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long long y = __shfl_up_sync(kFullMask, t, o);
+            if (lane >= o) t += y;
+        }
+        ws[lane] = t;
+    }
+    __syncthreads();
+    const long long pre = (w > 0 ? ws[w - 1] : 0) + x - v;
+    *total = ws[31];
+    __syncthreads();
+    return pre;
+}
+
+// Largest j < n with off[j] <= x (off ascending, off[0] <= x).
+template <typename T>
+__device__ __forceinline__ int32_t hg_find(const T *off, int32_t n, int64_t x) {
+    int32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int32_t mid = lo + ((hi - lo + 1) >> 1);
+        if ((int64_t)off[mid] <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(1024) k_hg_plan(HugeArgs a) {
+    __shared__ long long ws[32];
+    __shared__ int over;
+    const int64_t nh = *a.nh;
+    long long r0 = 0, r1 = 0;
+    for (int64_t base = 0; base < nh; base += 1024) {
+        const int64_t h = base + threadIdx.x;
+        long long nch = 0, np = 0;
+        if (h < nh) {
+            const int64_t l = a.hmo[a.hmb[h + 1]] - a.hmo[a.hmb[h]];
+            nch = (l + kHgCh - 1) / kHgCh;
+            np = max(1ll, (long long)((l + a.part_links - 1) / a.part_links));
+        }
+        long long t0, t1;
+        const long long e0 = hg_block_scan(nch, ws, &t0);
+        const long long e1 = hg_block_scan(np, ws, &t1);
+        if (h < nh) {
+            a.coff[h] = r0 + e0;
+            a.poff[h] = r1 + e1;
+        }
+        r0 += t0;
+        r1 += t1;
+    }
+    if (threadIdx.x == 0) {
+        over = r0 > a.max_chunks || r1 > a.max_parts || a.hmo[*a.nhm] > a.max_links;
+        a.coff[nh] = r0;
+        a.poff[nh] = r1;
+        a.tot[0] = over ? 0 : r0;
+        a.tot[1] = over ? 0 : r1;
+        a.tot[2] = over;
+    }
+    __syncthreads();
+    if (!over)
+        for (int64_t q = threadIdx.x; q < r1; q += 1024) a.pcnt[q] = 0;
+}
+
+// Every member lists the chunks of its group that start inside its links.
+__global__ void k_hg_starts(HugeArgs a) {
+    if (a.tot[2]) return;
+    const int64_t nhm = *a.nhm;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nhm; j += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t h = a.hgj[j];
+        const int64_t base = a.hmo[a.hmb[h]], v0 = a.hmo[j], v1 = a.hmo[j + 1];
+        for (int64_t k = (v0 - base + kHgCh - 1) / kHgCh; base + k * kHgCh < v1; k++) {
+            a.cmem[a.coff[h] + k] = (int32_t)j;
+            a.cgrp[a.coff[h] + k] = h;
+        }
+    }
+}
+
+// Count (SCATTER false) or place (SCATTER true) the crossing links of the chunks.
+template <bool SCATTER>
+__global__ void __launch_bounds__(kHgT) k_hg_links(HugeArgs a) {
+    __shared__ int64_t smo[kHgCh + 2];   // virtual positions of the chunk's members (+ the next)
+    __shared__ int64_t sest[kHgCh + 1];  // CSR position minus virtual position, per member
+    __shared__ fx_t wq[kHgT];
+    const int lane = threadIdx.x & 31;
+    const int64_t total = a.tot[0];
+    for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const int32_t h = a.cgrp[item], g = a.hlist[h];
+        const int64_t np = a.poff[h + 1] - a.poff[h];
+        const int64_t vend = a.hmo[a.hmb[h + 1]];
+        const int64_t P0 = a.hmo[a.hmb[h]] + (item - a.coff[h]) * kHgCh, P1 = min(vend, P0 + kHgCh);
+        const int32_t j0 = a.cmem[item];
+        const int32_t j1 = item + 1 < a.coff[h + 1] ? a.cmem[item + 1] : (int32_t)(a.hmb[h + 1] - 1);
+        const int K = j1 - j0 + 1;  // members overlapping the chunk: at most kHgCh + 1 (each has a link)
+        if (!SCATTER && item == a.coff[h])
+            for (int64_t q = threadIdx.x; q < np; q += kHgT) a.pgrp[a.poff[h] + q] = h;
+        __syncthreads();  // the previous item's readers are done with the staging arrays
+        for (int k = threadIdx.x; k <= K; k += kHgT) {
+            const int64_t v = a.hmo[j0 + k];  // j0 + K <= nhm: hmo holds nhm + 1 entries
+            smo[k] = v;
+            if (k < K) sest[k] = a.off[a.members[a.hml[j0 + k]]] - v;
+        }
+        __syncthreads();
+        for (int64_t b0 = P0; b0 < P1; b0 += kHgT) {  // uniform over the block
+            const int64_t V = b0 + threadIdx.x;
+            int32_t key = g;  // lanes past the chunk: internal (skipped)
+            fx_t q = 0;
+            if (V < P1) {
+                const int k = hg_find(smo, K, V);
+                const int64_t e = sest[k] + V;
+                key = __ldg(a.group + __ldg(a.dst + e));
+                q = __ldg(a.fx + e);
+            }
+            const bool valid = key != g;  // links inside the group are not kept
+            const unsigned kpeers = __match_any_sync(kFullMask, valid ? key : -1);
+            const bool head = valid && lane == __ffs(kpeers) - 1;
+            const int32_t part = head ? (int32_t)(hg_part_hash(key) % (uint32_t)np) : -1;
+            const unsigned peers = __match_any_sync(kFullMask, part);
+            const int leader = __ffs(peers) - 1;
+            if (!SCATTER) {
+                if (head && lane == leader)
+                    atomicAdd(a.pcnt + a.poff[h] + part, (unsigned long long)__popc(peers));
+            } else {
+                wq[threadIdx.x] = q;
+                __syncwarp();
+                fx_t sum = 0;
+                if (head)
+                    for (unsigned m = kpeers; m; m &= m - 1) sum += wq[(threadIdx.x & ~31) + __ffs(m) - 1];
+                unsigned long long base = 0;
+                const int64_t pidx = a.poff[h] + part;
+                if (head && lane == leader) base = atomicAdd(a.pcnt + pidx, (unsigned long long)__popc(peers));
+                base = __shfl_sync(kFullMask, base, leader);
+                if (head) {
+                    const int64_t pos = a.pstart[pidx] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
+                    a.bkey[pos] = key;
+                    a.bfx[pos] = sum;
+                }
+                __syncwarp();
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_hg_offsets(HugeArgs a) {
+    __shared__ long long ws[32];
+    const int64_t np = a.tot[1];
+    long long r = 0;
+    for (int64_t base = 0; base < np; base += 1024) {
+        const int64_t q = base + threadIdx.x;
+        const long long c = q < np ? (long long)a.pcnt[q] : 0;
+        long long t;
+        const long long e = hg_block_scan(c, ws, &t);
+        if (q < np) {
+            a.pstart[q] = r + e;
+            a.pcnt[q] = 0;
+        }
+        r += t;
+    }
+    if (threadIdx.x == 0) a.pstart[np] = r;
+}
+
+// A block per partition: its bucket summed in a shared table and the distinct
+// destinations appended to the group's row. A bucket with more distinct
+// destinations than half the table is taken in subsets: subset (R, r) holds
+// the keys whose second hash h2 (a bijection of the key) has h2 mod R == r;
+// a subset that overfills the table is emptied unwritten and replaced by its
+// two halves (2R, r) and (2R, r + R). Every key lands in exactly one written
+// subset, and a subset of R = 2^31 holds at most two keys, so this ends.
+__device__ __forceinline__ uint32_t hg_split_hash(int32_t key) { return agg_hash((uint32_t)key ^ 0x5bd1e995u); }
+
+__global__ void __launch_bounds__(kHgT, 2) k_hg_reduce(HugeArgs a) {
+    extern __shared__ __align__(16) unsigned char hg_smem[];  // kHgSmem bytes
+    fx_t *vals = reinterpret_cast<fx_t *>(hg_smem);
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + kHgCap);
+    __shared__ int16_t taken[kHgCap / 2 + kHgT];
+    __shared__ int nfresh;
+    __shared__ unsigned long long obase;
+    const int mask = kHgCap - 1;
+    const int64_t total = a.tot[1];
+    for (int s = threadIdx.x; s < kHgCap; s += kHgT) {
+        keys[s] = kNoKey;
+        vals[s] = 0;
+    }
+    fx_t rsum = 0;
+    for (int64_t pidx = blockIdx.x; pidx < total; pidx += gridDim.x) {
+        const int32_t h = a.pgrp[pidx], g = a.hlist[h];
+        const int64_t b0 = a.pstart[pidx], b1 = a.pstart[pidx + 1];
+        uint32_t stR[33], str[33];  // subsets still to take (uniform across the block)
+        int sp = 0;
+        stR[sp] = 1;
+        str[sp++] = 0;
+        while (sp > 0) {
+            sp--;
+            const uint32_t R = stR[sp], r = str[sp];
+            __syncthreads();
+            if (threadIdx.x == 0) nfresh = 0;
+            __syncthreads();
+            for (int64_t e = b0 + threadIdx.x; e < b1; e += kHgT) {
+                const int32_t key = a.bkey[e];
+                if (R > 1 && (hg_split_hash(key) & (R - 1)) != r) continue;
+                if (*(volatile int *)&nfresh > kHgCap / 2) break;
+                bool fresh;
+                const int sl = agg_insert(keys, mask, key, fresh);
+                if (sl < 0) continue;  // unreachable: at most kHgCap / 2 + kHgT keys are inserted
+                if (fresh) taken[atomicAdd(&nfresh, 1)] = (int16_t)sl;
+                atomicAdd(reinterpret_cast<unsigned long long *>(vals + sl), (unsigned long long)a.bfx[e]);
+            }
+            __syncthreads();
+            const int nt = nfresh;
+            const bool overfull = nt > kHgCap / 2;
+            if (!overfull && threadIdx.x == 0)
+                obase = atomicAdd(reinterpret_cast<unsigned long long *>(a.rowlen + g), (unsigned long long)nt);
+            __syncthreads();
+            for (int i = threadIdx.x; i < nt; i += kHgT) {
+                const int sl = taken[i];
+                if (!overfull) {
+                    const int64_t pos = a.gloff[g] + (int64_t)obase + i;
+                    a.slab_dst[pos] = keys[sl];
+                    a.slab_fx[pos] = vals[sl];
+                    rsum += vals[sl];
+                }
+                keys[sl] = kNoKey;
+                vals[sl] = 0;
+            }
+            if (overfull) {  // its two halves, the lower one taken first
+                stR[sp] = 2 * R;
+                str[sp++] = r + R;
+                stR[sp] = 2 * R;
+                str[sp++] = r;
+            }
+        }
+        if (a.rowsum) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) rsum += __shfl_xor_sync(kFullMask, rsum, o);
+            if ((threadIdx.x & 31) == 0 && rsum)
+                atomicAdd(reinterpret_cast<unsigned long long *>(a.rowsum + g), (unsigned long long)rsum);
+        }
+        rsum = 0;
+    }
+}
+
 // Row of link e in the offsets off[0..ng]: each warp takes 32 consecutive
 // links; lane 0 finds the first link's row by binary search, and every lane
 // walks forward from there (rows in a chunk are few unless they are tiny).
@@ -511,7 +881,7 @@ __global__ void k_agg_transpose(int32_t ng, int64_t m, const int64_t *g_out_off,
     }
 }
 
-// The block bin's dynamic shared memory, set once per device.
+// The block bin's and the split pipeline's dynamic shared memory, set once per device.
 static void configure_agg_kernels() {
     static std::mutex mu;
     static std::vector<bool> done;
@@ -522,6 +892,7 @@ static void configure_agg_kernels() {
     if (done[dev]) return;
     const int smem = (int)(kAggCap * (sizeof(fx_t) + sizeof(int32_t)));
     RMX_CUDA(cudaFuncSetAttribute(k_agg_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    RMX_CUDA(cudaFuncSetAttribute(k_hg_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHgSmem));
     done[dev] = true;
 }
 
@@ -538,7 +909,9 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     size_t mk = ar.mark();
     int64_t *gmoff = ar.alloc<int64_t>(ng + 1), *gloff = ar.alloc<int64_t>(ng + 1);
     unsigned long long *fill = ar.alloc<unsigned long long>(ng + 1);
-    int64_t *tot = ar.alloc<int64_t>(8);
+    // tot: [0] small [1] large [2] links out [3] max links [4] mid [5] huge groups, [6..8] their links,
+    // chunks and partitions [9] split pipeline over capacity
+    int64_t *tot = ar.alloc<int64_t>(16);
     RMX_CUDA(cudaMemsetAsync(gmoff, 0, sizeof(int64_t) * (ng + 1), s));
     RMX_CUDA(cudaMemsetAsync(gloff, 0, sizeof(int64_t) * (ng + 1), s));
     k_agg_count<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, off, group,
@@ -551,23 +924,29 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     RMX_CUDA(cudaMemsetAsync(fill, 0, sizeof(unsigned long long) * (ng + 1), s));
     k_agg_members<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, group, gmoff, fill, members);
     RMX_LAUNCHED();
-    uint8_t *fsmall = ar.alloc<uint8_t>(ng), *fmid = ar.alloc<uint8_t>(ng), *flarge = ar.alloc<uint8_t>(ng);
-    RMX_CUDA(cudaMemsetAsync(tot, 0, sizeof(int64_t) * 5, s));
-    k_agg_bins<<<blocks_for(ng, 256, num_sms() * 32), 256, 0, s>>>(ng, gloff, fsmall, fmid, flarge,
-                                                                   reinterpret_cast<unsigned long long *>(tot + 3));
+    uint8_t *fsmall = ar.alloc<uint8_t>(ng), *fmid = ar.alloc<uint8_t>(ng), *flarge = ar.alloc<uint8_t>(ng),
+            *fhuge = ar.alloc<uint8_t>(ng);
+    RMX_CUDA(cudaMemsetAsync(tot, 0, sizeof(int64_t) * 16, s));
+    const int64_t part_links = eval_tuning().hub_part;
+    k_agg_bins<<<blocks_for(ng, 256, num_sms() * 32), 256, 0, s>>>(
+        ng, gloff, part_links, fsmall, fmid, flarge, fhuge, reinterpret_cast<unsigned long long *>(tot + 3),
+        reinterpret_cast<unsigned long long *>(tot + 6));
     RMX_LAUNCHED();
-    int32_t *lsmall = ar.alloc<int32_t>(ng), *lmid = ar.alloc<int32_t>(ng), *llarge = ar.alloc<int32_t>(ng);
+    int32_t *lsmall = ar.alloc<int32_t>(ng), *lmid = ar.alloc<int32_t>(ng), *llarge = ar.alloc<int32_t>(ng),
+            *lhuge = ar.alloc<int32_t>(ng);
     compact_flags(fsmall, ng, lsmall, tot + 0, ar, s);
     compact_flags(fmid, ng, lmid, tot + 4, ar, s);
     compact_flags(flarge, ng, llarge, tot + 1, ar, s);
+    compact_flags(fhuge, ng, lhuge, tot + 5, ar, s);
     int32_t *slab_dst = ar.alloc<int32_t>(std::max<int64_t>(E, 1));
     fx_t *slab_fx = ar.alloc<fx_t>(std::max<int64_t>(E, 1));
     int64_t *rowlen = g_out_off;  // row lengths, scanned in place into offsets below
     RMX_CUDA(cudaMemsetAsync(rowlen, 0, sizeof(int64_t) * (ng + 1), s));
     // a group of L links needs a table of next_pow2(2L) slots; beyond shared memory, a global slice per block
-    int64_t maxlinks = 0;
-    RMX_CUDA(cudaMemcpyAsync(&maxlinks, tot + 3, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    int64_t th[6];  // max links outside the split pipeline; huge groups, their links, chunks, partitions
+    RMX_CUDA(cudaMemcpyAsync(th, tot + 3, sizeof th, cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));
+    const int64_t maxlinks = th[0], n_huge = th[2], huge_links = th[3], huge_chunks = th[4], huge_parts = th[5];
     int64_t need = 64;
     while (need < 2 * std::min<int64_t>(maxlinks, ng)) need <<= 1;
     const int nblk = num_sms() * 2;
@@ -597,13 +976,76 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     a.gkeys = gtab ? reinterpret_cast<int32_t *>(gtab + gtab_cap * nblk) : nullptr;
     a.gcap = gtab_cap;
     a.ngroups = ng;
-    // the three bins run concurrently: warp and mid bins on the two auxiliary streams
-    cudaStream_t s_small = s, s_mid = s;
+    // the bins run concurrently: the split pipeline (the longest chain, first),
+    // warp and mid bins on three auxiliary streams
+    cudaStream_t s_small = s, s_mid = s, s_huge = s;
     if (W) {
         RMX_CUDA(cudaEventRecord(W->fork, s));
-        for (int k = 0; k < 2; k++) RMX_CUDA(cudaStreamWaitEvent(W->aux[k], W->fork, 0));
+        for (int k = 0; k < 3; k++) RMX_CUDA(cudaStreamWaitEvent(W->aux[k], W->fork, 0));
         s_small = W->aux[0];
         s_mid = W->aux[1];
+        s_huge = W->aux[2];
+    }
+    if (n_huge > 0) {
+        HugeArgs h;
+        h.off = off;
+        h.dst = dst;
+        h.fx = fx;
+        h.group = group;
+        h.members = members;
+        h.gloff = gloff;
+        h.hlist = lhuge;
+        h.nh = tot + 5;
+        const int64_t cap_m = std::max<int64_t>(1, std::min<int64_t>(n, huge_links));  // nonzero-degree members
+        h.hidx = ar.alloc<int32_t>(ng);
+        uint8_t *mflag = ar.alloc<uint8_t>(std::max(n, 1));
+        int32_t *hml = ar.alloc<int32_t>(cap_m);
+        h.hml = hml;
+        h.nhm = tot + 10;
+        h.hmo = ar.alloc<int64_t>(cap_m + 1);
+        h.hgj = ar.alloc<int32_t>(cap_m);
+        h.hmb = ar.alloc<int64_t>(n_huge + 1);
+        h.coff = ar.alloc<int64_t>(n_huge + 1);
+        h.poff = ar.alloc<int64_t>(n_huge + 1);
+        h.cmem = ar.alloc<int32_t>(huge_chunks);
+        h.cgrp = ar.alloc<int32_t>(huge_chunks);
+        h.pgrp = ar.alloc<int32_t>(huge_parts);
+        h.pcnt = ar.alloc<unsigned long long>(huge_parts);
+        h.pstart = ar.alloc<int64_t>(huge_parts + 1);
+        h.bkey = ar.alloc<int32_t>(huge_links);
+        h.bfx = ar.alloc<fx_t>(huge_links);
+        h.tot = tot + 12;
+        h.max_chunks = huge_chunks;
+        h.max_parts = huge_parts;
+        h.max_links = huge_links;
+        h.part_links = part_links;
+        h.slab_dst = slab_dst;
+        h.slab_fx = slab_fx;
+        h.rowlen = rowlen;
+        h.rowsum = rowsum;
+        const cudaStream_t hs = s_huge;
+        RMX_CUDA(cudaMemsetAsync(h.hidx, 0xff, sizeof(int32_t) * ng, hs));
+        k_hg_index<<<blocks_for(n_huge, 256, num_sms() * 4), 256, 0, hs>>>(h);
+        RMX_LAUNCHED();
+        k_hg_member_flags<<<blocks_for(n, 256, num_sms() * 32), 256, 0, hs>>>(n, h, mflag);
+        RMX_LAUNCHED();
+        compact_flags(mflag, n, hml, tot + 10, ar, hs);
+        k_hg_members<<<blocks_for(cap_m, 256, num_sms() * 32), 256, 0, hs>>>((int32_t)cap_m, h, h.hmo);
+        RMX_LAUNCHED();
+        scan_exclusive(h.hmo, h.hmo, cap_m, h.hmo + cap_m, ar, hs);
+        k_hg_plan<<<1, 1024, 0, hs>>>(h);
+        RMX_LAUNCHED();
+        k_hg_starts<<<blocks_for(cap_m, 256, num_sms() * 32), 256, 0, hs>>>(h);
+        RMX_LAUNCHED();
+        const unsigned G = num_sms() * 6;
+        k_hg_links<false><<<G, kHgT, 0, hs>>>(h);
+        RMX_LAUNCHED();
+        k_hg_offsets<<<1, 1024, 0, hs>>>(h);
+        RMX_LAUNCHED();
+        k_hg_links<true><<<G, kHgT, 0, hs>>>(h);
+        RMX_LAUNCHED();
+        k_hg_reduce<<<num_sms() * 2, kHgT, kHgSmem, hs>>>(h);
+        RMX_LAUNCHED();
     }
     a.list = lsmall;
     a.count = tot + 0;
@@ -618,15 +1060,18 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     k_agg_block<<<nblk, kAggT, kAggCap * (sizeof(fx_t) + sizeof(int32_t)), s>>>(a);
     RMX_LAUNCHED();
     if (W)
-        for (int k = 0; k < 2; k++) {
+        for (int k = 0; k < 3; k++) {
             RMX_CUDA(cudaEventRecord(W->join[k], W->aux[k]));
             RMX_CUDA(cudaStreamWaitEvent(s, W->join[k], 0));
         }
     scan_exclusive(rowlen, g_out_off, ng + 1, tot + 2, ar, s);
-    int64_t m = 0;
+    int64_t m = 0, over = 0;
     RMX_CUDA(cudaMemcpyAsync(&m, tot + 2, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    if (n_huge > 0) RMX_CUDA(cudaMemcpyAsync(&over, tot + 14, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaMemsetAsync(g_in_off, 0, sizeof(int64_t) * (ng + 1), s));
     RMX_CUDA(cudaStreamSynchronize(s));
+    if (over)  // the sizes come from the same counts the plan sums, so this does not happen
+        throw std::runtime_error("aggregate_links: split pipeline over its capacity");
     if (m > 0) {
         const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
         k_agg_pack<<<Gm, 256, 0, s>>>(ng, m, gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx,

@@ -217,7 +217,7 @@ void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_
 struct EvalTuning {
     int mid, block, large, warp, reg;              // grid caps
     int warp_max, mid_max, block_max, large_max;   // degree bounds (at most 128, 512, 1024, 4096)
-    int hub_part;                                  // mean links per partition of a hub unit
+    int hub_part;                                  // mean links per partition of a hub unit / huge group
 };
 EvalTuning eval_tuning();
 // Throws std::invalid_argument unless every grid cap lies in [1, 64] and

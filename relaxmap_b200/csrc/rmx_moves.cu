@@ -937,9 +937,11 @@ __global__ void __launch_bounds__(1024) k_hub_offsets(HubPlan p) {
     if (threadIdx.x == 0) p.pstart[np] = r;
 }
 
-// A block per partition: its bucket aggregated in a shared table, in rounds
-// (keys split by a second hash) if it holds more distinct modules than half
-// the table, which the partitioning makes vanishingly rare.
+// A block per partition: its bucket aggregated in a shared table, in R rounds
+// if it holds more distinct modules than half the table (which the
+// partitioning makes rare): round r takes the keys whose second hash h2 (a
+// bijection of the key) has h2 mod R == r, and R doubles until no round
+// overfills (at R = 2^31 a round holds at most two keys).
 __global__ void __launch_bounds__(kHubPT, 2) k_hub_eval(EvalArgs a, HubPlan p) {
     extern __shared__ __align__(16) unsigned char hub_smem[];  // kHubEvalSmem bytes
     fx_t *vo = reinterpret_cast<fx_t *>(hub_smem);
@@ -979,7 +981,7 @@ __global__ void __launch_bounds__(kHubPT, 2) k_hub_eval(EvalArgs a, HubPlan p) {
                 for (int64_t e = b0 + threadIdx.x; e < b1; e += kHubPT) {
                     const int32_t kd = p.bkey[e];
                     const int32_t key = kd & 0x7fffffff;
-                    if (R > 1 && (mix32((uint32_t)key) >> 20) % R != r) continue;  // bits above the slot's
+                    if (R > 1 && (mix32((uint32_t)key ^ 0x5bd1e995u) & (R - 1)) != r) continue;
                     if (*(volatile int *)&nfresh > kPartCap / 2) break;
                     int sl = tab_slot(key, mask);
                     int32_t prev = atomicCAS(keys + sl, kEmpty, key);

@@ -15,7 +15,9 @@ Bars:
 * converted to FP64, a link sum of k member links lies within
   k * 2^-62 + (k + 1) * 2^-52 * |ref| of the reference's FP64 sum (the
   fixed-point rounding of each term plus the reference's own FP64 rounding).
-The second-level case converts the super-nodes again (the super-node stage's
+Groups of more than 16384 member links take the split pipeline (links
+partitioned by destination over many blocks); the two-group, second-level
+(300, 2) and huge-group cases cover it. The second-level case converts the super-nodes again (the super-node stage's
 repeated conversion, OmpRelaxmap.cpp:379-411): the engine aggregates the first
 level's links, the reference converts the composite node partition."""
 import numpy as np
@@ -155,6 +157,30 @@ def test_random_partitions(built_lib, oracle_mod, planted, k):
     with Graph.from_edges(sg.src, sg.dst, sg.w, n=sg.n) as G:
         ref, off, dst, f, p, tw, dg, grp = reference_level(oracle_mod, G, part, graph=sg)
         cv = G.coarsen_engine(part)
+    check_against(cv, ref, off, dst, f, p, tw, dg, grp)
+
+
+@pytest.mark.parametrize("part_links", [64, 1024, 1 << 30])
+def test_huge_groups(built_lib, oracle_mod, planted, part_links):
+    """A group of half the nodes (about 49,000 member links, above the bound
+    past which a group's links are summed by the split pipeline) next to
+    singletons, under three partition sizes of that pipeline: many small
+    partitions; the default; and one partition holding all of the group's
+    3000 distinct destinations, more than half its table, so that it is
+    summed in subsets."""
+    from relaxmap_b200 import Graph, get_tuning, set_tuning
+    sg = planted
+    part = np.arange(sg.n, dtype=np.int32)
+    part[: sg.n // 2] = 0
+    before = get_tuning()
+    try:
+        set_tuning(hub_partition_links=part_links)
+        with Graph.from_edges(sg.src, sg.dst, sg.w, n=sg.n) as G:
+            ref, off, dst, f, p, tw, dg, grp = reference_level(oracle_mod, G, part, graph=sg)
+            cv = G.coarsen_engine(part)
+    finally:
+        set_tuning(**before)
+    assert np.diff(cv["out_off"])[0] > 2048  # the group's row: distinct destinations
     check_against(cv, ref, off, dst, f, p, tw, dg, grp)
 
 
