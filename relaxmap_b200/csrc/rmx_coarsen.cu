@@ -170,12 +170,19 @@ int64_t coarsen_links(int32_t n, const int64_t *out_off, const int32_t *out_dst,
 //
 // The move engine needs the group links' fixed-point sums, which are exact in
 // any order, and it never depends on the order of links inside a row. So
-// instead of sorting every crossing link, the members of each group are
-// listed (counting sort by group), and one warp (small groups) or one block
-// (large groups) per group sums its members' links into a hash table keyed
-// by the destination group, in shared memory or, for the largest groups, in a
-// per-block slice of a global table. The rows are then packed and transposed
-// with a counting sort by destination.
+// instead of sorting every crossing link:
+//   1. each group's capacity (its members' links) is counted and scanned;
+//   2. one pass over the links in CSR order (every link's row is known)
+//      gathers each crossing link's (destination group, flow) into its
+//      source group's range, in no particular order;
+//   3. one warp (small groups), one block (large groups) or the split
+//      pipeline (huge groups) per group sums the range in a hash table keyed
+//      by the destination group and writes the distinct destinations back
+//      to the start of the range;
+//   4. the rows are packed (teams of 8 lanes per row, a block per long row),
+//      every packed link's row written beside it, and transposed by a
+//      counting sort on the destination.
+// No pass searches for the row of a link or walks a group's members.
 namespace rmx {
 
 constexpr unsigned kFullMask = 0xffffffffu;
@@ -210,35 +217,71 @@ __device__ __forceinline__ int agg_insert(int32_t *keys, int mask, int32_t key, 
     return -1;
 }
 
-__global__ void k_agg_count(int32_t n, const int64_t *off, const int32_t *group, unsigned long long *gcnt,
-                            unsigned long long *glinks) {
+__global__ void k_rows_of_links(int32_t n, const int64_t *off, int32_t *src) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t r = gw; r < n; r += nw)
+        for (int64_t e = off[r] + lane; e < off[r + 1]; e += 32) src[e] = (int32_t)r;
+}
+
+void rows_of_links(int32_t n, const int64_t *off, int32_t *src, cudaStream_t s) {
+    k_rows_of_links<<<blocks_for((int64_t)n * 32, 256, num_sms() * 32), 256, 0, s>>>(n, off, src);
+    RMX_LAUNCHED();
+}
+
+// glinks[g]: links of g's members (the capacity of g's range).
+__global__ void k_agg_count(int32_t n, const int64_t *off, const int32_t *group, unsigned long long *glinks) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t g = group[r];
-        atomicAdd(gcnt + g, 1ull);
-        atomicAdd(glinks + g, (unsigned long long)(off[r + 1] - off[r]));
+        const int64_t d = off[r + 1] - off[r];
+        if (d) atomicAdd(glinks + group[r], (unsigned long long)d);
     }
 }
 
-__global__ void k_agg_members(int32_t n, const int32_t *group, const int64_t *gmoff, unsigned long long *gfill,
-                              int32_t *members) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t g = group[r];
-        members[gmoff[g] + (int64_t)atomicAdd(gfill + g, 1ull)] = (int32_t)r;
+// Every crossing link u->w (group(u) != group(w)) appended to group(u)'s
+// range: gk = group(w), gq = its flow; gcross[g] counts them. Lanes of a warp
+// with the same source group (consecutive links of one row, mostly) take
+// their positions with one counter update.
+__global__ void k_agg_gather(int64_t m, const int32_t *src, const int32_t *dst, const fx_t *fx, const int32_t *group,
+                             const int64_t *gloff, unsigned long long *gcross, int32_t *gk, fx_t *gq) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {  // warp-uniform
+        const int64_t e = e0 + lane;
+        int32_t g = -1, b = -1;
+        fx_t q = 0;
+        if (e < m) {
+            g = __ldg(group + __ldg(src + e));
+            b = __ldg(group + __ldg(dst + e));
+            q = __ldg(fx + e);
+            if (b == g) g = -1;  // links inside a group are not kept
+        }
+        const unsigned peers = __match_any_sync(kFullMask, g);
+        const int leader = __ffs(peers) - 1;
+        unsigned long long base = 0;
+        if (g >= 0 && lane == leader) base = atomicAdd(gcross + g, (unsigned long long)__popc(peers));
+        base = __shfl_sync(kFullMask, base, leader);
+        if (g >= 0) {
+            const int64_t p = gloff[g] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
+            gk[p] = b;
+            gq[p] = q;
+        }
     }
 }
 
-// Groups by the bound on their distinct neighbours, min(links, groups): a
-// warp (<= 128), a 128-thread block (<= 1024) or a 512-thread block; groups
-// of more than kAggSplit links go to the split pipeline instead. maxlinks:
-// the most links of a group outside it; htot: the split pipeline's links,
-// chunks and partitions.
-__global__ void k_agg_bins(int32_t ng, const int64_t *gloff, int64_t part_links, uint8_t *small, uint8_t *mid,
-                           uint8_t *large, uint8_t *huge, unsigned long long *maxlinks, unsigned long long *htot) {
+// Groups by the bound on their distinct neighbours, min(crossing links,
+// groups): a warp (<= 128), a 128-thread block (<= 1024) or a 512-thread
+// block; groups of more than kAggSplit crossing links go to the split
+// pipeline instead (groups without one go nowhere). maxlinks: the most links
+// of a group outside it; htot: the split pipeline's links, chunks and
+// partitions.
+__global__ void k_agg_bins(int32_t ng, const unsigned long long *gcross, int64_t part_links, uint8_t *small,
+                           uint8_t *mid, uint8_t *large, uint8_t *huge, unsigned long long *maxlinks,
+                           unsigned long long *htot) {
     unsigned long long mx = 0, hl = 0, hc = 0, hp = 0;
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < ng; g += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t l = gloff[g + 1] - gloff[g], b = min(l, (int64_t)ng);
+        const int64_t l = (int64_t)gcross[g], b = min(l, (int64_t)ng);
         const bool hg = l > kAggSplit;
-        small[g] = !hg && b <= kAggWarpLinks ? 1 : 0;
+        small[g] = !hg && b > 0 && b <= kAggWarpLinks ? 1 : 0;
         mid[g] = !hg && b > kAggWarpLinks && b <= kAggMidLinks ? 1 : 0;
         large[g] = !hg && b > kAggMidLinks ? 1 : 0;
         huge[g] = hg ? 1 : 0;
@@ -267,13 +310,9 @@ __global__ void k_agg_bins(int32_t ng, const int64_t *gloff, int64_t part_links,
 }
 
 struct AggArgs {
-    const int64_t *off;
-    const int32_t *dst;
-    const fx_t *fx;
-    const int32_t *group;
-    const int64_t *gmoff, *gloff;
-    const int32_t *members;
-    int32_t *slab_dst;  // packed rows at gloff[g] (capacity = member links)
+    const int64_t *gloff;                 // start of each group's range
+    const unsigned long long *gcross;     // crossing links gathered into it
+    int32_t *slab_dst;  // the ranges: gathered links in, distinct destinations out (at the same start)
     fx_t *slab_fx;
     int64_t *rowlen;
     fx_t *rowsum;        // optional: sum of the row's flows (out-flow of the group)
@@ -285,76 +324,51 @@ struct AggArgs {
     int32_t ngroups;
 };
 
-// Members of at least a team's width of links that a block team defers to
-// its second pass, at most kAggBig per group (the rest stay with their warp).
-constexpr int kAggBig = 128;
-
-// Inserts links [e0, e1) of one member (stride `step` from the caller's
-// lane/rank) into the group's table; false once the table is full.
-template <int NT>
-__device__ __forceinline__ bool agg_links(const AggArgs &a, int32_t g, int64_t e0, int64_t e1, int step,
-                                          int32_t *keys, fx_t *vals, int mask, int *nkeys) {
-    for (int64_t e = e0; e < e1; e += step) {
-        const int32_t b = a.group[a.dst[e]];
-        if (b == g) continue;
-        bool fresh;
-        const int s = agg_insert(keys, mask, b, fresh);
-        if (s < 0) return false;  // only a table sized below the bound can fill up; nkeys > limit already
-        if (NT > 32 && fresh) atomicAdd(nkeys, 1);
-        atomicAdd(reinterpret_cast<unsigned long long *>(vals + s), (unsigned long long)a.fx[e]);
-    }
-    return true;
-}
-
 // One group by a team of NT threads (r = rank); keys/vals: a table of cap
 // slots. A table sized below twice the group's link count may hold at most
 // `limit` distinct keys: past that the group is abandoned (returns false,
 // uniformly across the team) and nothing of it is written. wsh: NT/32 + 3
-// ints; big: kAggBig ints (block teams only).
-// A warp takes one member at a time, its lanes over the member's links. In a
-// block team a member of NT links or more is deferred to a second pass in
-// which the whole team strides its links, so that one heavy member does not
-// keep one warp busy while the others wait at the next barrier.
+// ints (block teams only). The team strides the group's gathered range, four
+// links per thread loaded before any is inserted.
 template <int NT>
 __device__ __forceinline__ bool agg_group(const AggArgs &a, int32_t g, int r, int32_t *keys, fx_t *vals, int64_t cap,
-                                          int limit, int *wsh, int32_t *big) {
+                                          int limit, int *wsh) {
+    constexpr int ILP = 4;
     const int lane = r & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int mask = (int)(cap - 1);
-    int *nkeys = wsh + NT / 32 + 1, *nbig = wsh + NT / 32 + 2;
+    int *nkeys = wsh ? wsh + NT / 32 + 1 : nullptr;
     for (int64_t s = r; s < cap; s += NT) {
         keys[s] = kNoKey;
         vals[s] = 0;
     }
-    if (NT > 32 && r == 0) {
-        *nkeys = 0;
-        *nbig = 0;
-    }
+    if (NT > 32 && r == 0) *nkeys = 0;
     if (NT == 32) __syncwarp(); else __syncthreads();
-    const int64_t mb = a.gmoff[g], me = a.gmoff[g + 1];
-    for (int64_t m = mb + (r >> 5); m < me; m += NT / 32) {  // a warp per member, lanes over its links
+    const int64_t b0 = a.gloff[g], b1 = b0 + (int64_t)a.gcross[g];
+    for (int64_t j0 = b0 + r; j0 < b1; j0 += (int64_t)NT * ILP) {
         if (NT > 32 && *(volatile int *)nkeys > limit) break;
-        const int32_t u = a.members[m];
-        const int64_t e0 = a.off[u], e1 = a.off[u + 1];
-        if (NT > 32 && e1 - e0 >= NT) {
-            int k = 0;
-            if (lane == 0) k = atomicAdd(nbig, 1);
-            k = __shfl_sync(kFullMask, k, 0);
-            if (k < kAggBig) {
-                if (lane == 0) big[k] = u;
+        int32_t key[ILP];
+        fx_t q[ILP];
+#pragma unroll
+        for (int k = 0; k < ILP; k++) {
+            const int64_t j = j0 + (int64_t)k * NT;
+            key[k] = j < b1 ? a.slab_dst[j] : kNoKey;
+            q[k] = j < b1 ? a.slab_fx[j] : 0;
+        }
+        bool full = false;
+#pragma unroll
+        for (int k = 0; k < ILP; k++) {
+            if (key[k] == kNoKey || full) continue;
+            bool fresh;
+            const int s = agg_insert(keys, mask, key[k], fresh);
+            if (s < 0) {  // only a table sized below the bound can fill up; nkeys > limit already
+                full = true;
                 continue;
             }
+            if (NT > 32 && fresh) atomicAdd(nkeys, 1);
+            atomicAdd(reinterpret_cast<unsigned long long *>(vals + s), (unsigned long long)q[k]);
         }
-        agg_links<NT>(a, g, e0 + lane, e1, 32, keys, vals, mask, nkeys);
-    }
-    if (NT > 32) {
-        __syncthreads();
-        const int nb = min(*nbig, kAggBig);
-        for (int k = 0; k < nb; k++) {
-            if (*(volatile int *)nkeys > limit) break;
-            const int32_t u = big[k];
-            if (!agg_links<NT>(a, g, a.off[u] + r, a.off[u + 1], NT, keys, vals, mask, nkeys)) break;
-        }
+        if (full) break;
     }
     if (NT == 32) __syncwarp(); else __syncthreads();
     if (NT > 32 && *nkeys > limit) {
@@ -421,10 +435,10 @@ __global__ void __launch_bounds__(kAggWarps * 32) k_agg_warp(AggArgs a) {
     const int64_t n = *a.count;
     for (int64_t i = (int64_t)blockIdx.x * kAggWarps + w; i < n; i += (int64_t)gridDim.x * kAggWarps) {
         const int32_t g = a.list[i];
-        const int64_t bound = min(a.gloff[g + 1] - a.gloff[g], (int64_t)a.ngroups);
+        const int64_t bound = min((int64_t)a.gcross[g], (int64_t)a.ngroups);
         int64_t cap = 32;
         while (cap < 2 * bound) cap <<= 1;
-        agg_group<32>(a, g, lane, skeys[w], svals[w], cap, INT_MAX, nullptr, nullptr);
+        agg_group<32>(a, g, lane, skeys[w], svals[w], cap, INT_MAX, nullptr);
     }
 }
 
@@ -432,14 +446,13 @@ __global__ void __launch_bounds__(kAggMidT) k_agg_mid(AggArgs a) {
     __shared__ int32_t skeys[kAggMidCap];
     __shared__ fx_t svals[kAggMidCap];
     __shared__ int wsh[kAggMidT / 32 + 3];
-    __shared__ int32_t big[kAggBig];
     const int64_t n = *a.count;
     for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
         const int32_t g = a.list[i];
-        const int64_t bound = min(a.gloff[g + 1] - a.gloff[g], (int64_t)a.ngroups);
+        const int64_t bound = min((int64_t)a.gcross[g], (int64_t)a.ngroups);
         int64_t cap = 64;
         while (cap < 2 * bound) cap <<= 1;
-        agg_group<kAggMidT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh, big);
+        agg_group<kAggMidT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh);
     }
 }
 
@@ -450,37 +463,33 @@ __global__ void __launch_bounds__(kAggMidT) k_agg_mid(AggArgs a) {
 __global__ void __launch_bounds__(kAggT, 2) k_agg_block(AggArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ int wsh[kAggT / 32 + 3];
-    __shared__ int32_t big[kAggBig];
     fx_t *svals = reinterpret_cast<fx_t *>(dsm);
     int32_t *skeys = reinterpret_cast<int32_t *>(svals + kAggCap);
     const int64_t n = *a.count;
     for (int64_t i = blockIdx.x; i < n; i += gridDim.x) {
         const int32_t g = a.list[i];
-        const int64_t bound = min(a.gloff[g + 1] - a.gloff[g], (int64_t)a.ngroups);
+        const int64_t bound = min((int64_t)a.gcross[g], (int64_t)a.ngroups);
         int64_t cap = 64;
         while (cap < 2 * bound) cap <<= 1;
         if (cap <= kAggCap) {
-            agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh, big);
-        } else if (!agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, kAggCap, kAggCap / 4 * 3, wsh, big)) {
+            agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, cap, INT_MAX, wsh);
+        } else if (!agg_group<kAggT>(a, g, threadIdx.x, skeys, svals, kAggCap, kAggCap / 4 * 3, wsh)) {
             agg_group<kAggT>(a, g, threadIdx.x, a.gkeys + (int64_t)blockIdx.x * a.gcap,
-                             a.gvals + (int64_t)blockIdx.x * a.gcap, cap, INT_MAX, wsh, big);
+                             a.gvals + (int64_t)blockIdx.x * a.gcap, cap, INT_MAX, wsh);
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// Huge groups (more than kAggSplit member links: the modules around R-MAT
-// hubs, up to millions of links) are not left to one block. Their links are
-// laid out in one virtual order (nonzero-degree members in member order, each
-// member's links in CSR order), cut into chunks of kHgCh links and
-// radix-partitioned by a hash of the destination group into partitions of
-// about part_links links, so that each partition's distinct destinations
-// fit one block's shared table:
-//   index    hidx (group -> huge index), the nonzero-degree members (hml),
-//            their virtual positions (hmo), each group's first member (hmb)
+// Huge groups (more than kAggSplit crossing links: the modules around R-MAT
+// hubs, up to millions of links) are not left to one block. Their gathered
+// ranges are cut into chunks of kHgCh links and radix-partitioned by a hash
+// of the destination group into partitions of about part_links links, so that
+// each partition's distinct destinations fit one block's shared table:
 //   plan     one block: chunk and partition offsets per huge group
-//   starts   every member lists the chunks that start inside it (cmem, cgrp)
-//   count    blocks take chunks and count each partition's elements
+//   count    blocks take chunks (finding each chunk's group once and listing
+//            it, and every partition's group) and count each partition's
+//            elements
 //   offsets  one block turns the counts into bucket offsets
 //   scatter  blocks take chunks again and write (destination, flow)
 //   reduce   a block per partition sums its bucket in a shared table and
@@ -492,22 +501,12 @@ constexpr int kHgT = 256, kHgCap = 4096;
 constexpr size_t kHgSmem = (size_t)kHgCap * (sizeof(fx_t) + sizeof(int32_t));
 
 struct HugeArgs {
-    const int64_t *off;
-    const int32_t *dst;
-    const fx_t *fx;
-    const int32_t *group;
-    const int32_t *members;
-    const int64_t *gloff;
+    const int64_t *gloff;                // start of each group's gathered range
+    const unsigned long long *gcross;    // its crossing links
     const int32_t *hlist;   // huge groups, ascending
     const int64_t *nh;      // their count (device)
-    int32_t *hidx;          // per group: index in hlist, or -1
-    const int32_t *hml;     // nonzero-degree members of huge groups (indices into members), ascending
-    const int64_t *nhm;     // their count (device)
-    int64_t *hmo;           // virtual position of each hml entry (nhm + 1)
-    int32_t *hgj;           // huge group of each hml entry
-    int64_t *hmb;           // per huge group (+1): first hml index
     int64_t *coff, *poff;   // per huge group (+1): first chunk, first partition
-    int32_t *cmem, *cgrp;   // per chunk: hml index holding its first link, huge group
+    int32_t *cgrp;          // per chunk: huge group
     int32_t *pgrp;          // per partition: huge group
     unsigned long long *pcnt;  // per partition: elements (counted), then the fill position
     int64_t *pstart;        // per partition (+1): first bucket element
@@ -516,7 +515,7 @@ struct HugeArgs {
     int64_t *tot;           // [0] chunks [1] partitions [2] over capacity
     int64_t max_chunks, max_parts, max_links;
     int64_t part_links;     // mean links per partition
-    int32_t *slab_dst;
+    int32_t *slab_dst;      // the gathered ranges (read by the link passes, written by the reduction)
     fx_t *slab_fx;
     int64_t *rowlen;
     fx_t *rowsum;
@@ -524,38 +523,6 @@ struct HugeArgs {
 
 __device__ __forceinline__ uint32_t hg_part_hash(int32_t key) {
     return agg_hash((uint32_t)key * 0x9E3779B1u + 0x7F4A7C15u);
-}
-
-__global__ void k_hg_index(HugeArgs a) {
-    const int64_t nh = *a.nh;
-    for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < nh; h += (int64_t)gridDim.x * blockDim.x)
-        a.hidx[a.hlist[h]] = (int32_t)h;
-}
-
-// flag[i]: member i belongs to a huge group and has links.
-__global__ void k_hg_member_flags(int32_t n, HugeArgs a, uint8_t *flag) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t u = a.members[i];
-        flag[i] = a.hidx[a.group[u]] >= 0 && a.off[u + 1] > a.off[u] ? 1 : 0;
-    }
-}
-
-// Degree of every hml entry (0 past the count, for the scan), its huge group,
-// and the first entry of every huge group.
-__global__ void k_hg_members(int32_t n, HugeArgs a, int64_t *deg) {
-    const int64_t nhm = *a.nhm;
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
-        if (j >= nhm) {
-            deg[j] = 0;
-            continue;
-        }
-        const int32_t u = a.members[a.hml[j]];
-        deg[j] = a.off[u + 1] - a.off[u];
-        const int32_t h = a.hidx[a.group[u]];
-        a.hgj[j] = h;
-        if (j == 0 || a.hidx[a.group[a.members[a.hml[j - 1]]]] != h) a.hmb[h] = j;
-    }
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.hmb[*a.nh] = nhm;
 }
 
 // Exclusive scan over the block (blockDim.x == 1024) of one value per thread.
@@ -608,7 +575,7 @@ __global__ void __launch_bounds__(1024) k_hg_plan(HugeArgs a) {
         const int64_t h = base + threadIdx.x;
         long long nch = 0, np = 0;
         if (h < nh) {
-            const int64_t l = a.hmo[a.hmb[h + 1]] - a.hmo[a.hmb[h]];
+            const int64_t l = (int64_t)a.gcross[a.hlist[h]];
             nch = (l + kHgCh - 1) / kHgCh;
             np = max(1ll, (long long)((l + a.part_links - 1) / a.part_links));
         }
@@ -623,7 +590,7 @@ __global__ void __launch_bounds__(1024) k_hg_plan(HugeArgs a) {
         r1 += t1;
     }
     if (threadIdx.x == 0) {
-        over = r0 > a.max_chunks || r1 > a.max_parts || a.hmo[*a.nhm] > a.max_links;
+        over = r0 > a.max_chunks || r1 > a.max_parts;
         a.coff[nh] = r0;
         a.poff[nh] = r1;
         a.tot[0] = over ? 0 : r0;
@@ -635,56 +602,33 @@ __global__ void __launch_bounds__(1024) k_hg_plan(HugeArgs a) {
         for (int64_t q = threadIdx.x; q < r1; q += 1024) a.pcnt[q] = 0;
 }
 
-// Every member lists the chunks of its group that start inside its links.
-__global__ void k_hg_starts(HugeArgs a) {
-    if (a.tot[2]) return;
-    const int64_t nhm = *a.nhm;
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < nhm; j += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t h = a.hgj[j];
-        const int64_t base = a.hmo[a.hmb[h]], v0 = a.hmo[j], v1 = a.hmo[j + 1];
-        for (int64_t k = (v0 - base + kHgCh - 1) / kHgCh; base + k * kHgCh < v1; k++) {
-            a.cmem[a.coff[h] + k] = (int32_t)j;
-            a.cgrp[a.coff[h] + k] = h;
-        }
-    }
-}
-
-// Count (SCATTER false) or place (SCATTER true) the crossing links of the chunks.
+// Count (SCATTER false) or place (SCATTER true) the links of the chunks.
 template <bool SCATTER>
 __global__ void __launch_bounds__(kHgT) k_hg_links(HugeArgs a) {
-    __shared__ int64_t smo[kHgCh + 2];   // virtual positions of the chunk's members (+ the next)
-    __shared__ int64_t sest[kHgCh + 1];  // CSR position minus virtual position, per member
     __shared__ fx_t wq[kHgT];
     const int lane = threadIdx.x & 31;
     const int64_t total = a.tot[0];
+    const int32_t nh = (int32_t)*a.nh;
     for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
-        const int32_t h = a.cgrp[item], g = a.hlist[h];
+        const int32_t h = SCATTER ? a.cgrp[item] : hg_find(a.coff, nh, item);
+        const int32_t g = a.hlist[h];
         const int64_t np = a.poff[h + 1] - a.poff[h];
-        const int64_t vend = a.hmo[a.hmb[h + 1]];
-        const int64_t P0 = a.hmo[a.hmb[h]] + (item - a.coff[h]) * kHgCh, P1 = min(vend, P0 + kHgCh);
-        const int32_t j0 = a.cmem[item];
-        const int32_t j1 = item + 1 < a.coff[h + 1] ? a.cmem[item + 1] : (int32_t)(a.hmb[h + 1] - 1);
-        const int K = j1 - j0 + 1;  // members overlapping the chunk: at most kHgCh + 1 (each has a link)
-        if (!SCATTER && item == a.coff[h])
-            for (int64_t q = threadIdx.x; q < np; q += kHgT) a.pgrp[a.poff[h] + q] = h;
-        __syncthreads();  // the previous item's readers are done with the staging arrays
-        for (int k = threadIdx.x; k <= K; k += kHgT) {
-            const int64_t v = a.hmo[j0 + k];  // j0 + K <= nhm: hmo holds nhm + 1 entries
-            smo[k] = v;
-            if (k < K) sest[k] = a.off[a.members[a.hml[j0 + k]]] - v;
+        const int64_t c0 = (item - a.coff[h]) * kHgCh;
+        const int64_t P0 = a.gloff[g] + c0, P1 = a.gloff[g] + min((int64_t)a.gcross[g], c0 + kHgCh);
+        if (!SCATTER) {
+            if (threadIdx.x == 0) a.cgrp[item] = h;
+            if (c0 == 0)
+                for (int64_t q = threadIdx.x; q < np; q += kHgT) a.pgrp[a.poff[h] + q] = h;
         }
-        __syncthreads();
         for (int64_t b0 = P0; b0 < P1; b0 += kHgT) {  // uniform over the block
             const int64_t V = b0 + threadIdx.x;
-            int32_t key = g;  // lanes past the chunk: internal (skipped)
+            int32_t key = -1;  // lanes past the chunk
             fx_t q = 0;
             if (V < P1) {
-                const int k = hg_find(smo, K, V);
-                const int64_t e = sest[k] + V;
-                key = __ldg(a.group + __ldg(a.dst + e));
-                q = __ldg(a.fx + e);
+                key = a.slab_dst[V];
+                q = a.slab_fx[V];
             }
-            const bool valid = key != g;  // links inside the group are not kept
+            const bool valid = key >= 0;
             const unsigned kpeers = __match_any_sync(kFullMask, valid ? key : -1);
             const bool head = valid && lane == __ffs(kpeers) - 1;
             const int32_t part = head ? (int32_t)(hg_part_hash(key) % (uint32_t)np) : -1;
@@ -812,61 +756,74 @@ __global__ void __launch_bounds__(kHgT, 2) k_hg_reduce(HugeArgs a) {
     }
 }
 
-// Row of link e in the offsets off[0..ng]: each warp takes 32 consecutive
-// links; lane 0 finds the first link's row by binary search, and every lane
-// walks forward from there (rows in a chunk are few unless they are tiny).
-// So the work per warp is the same whatever the rows' lengths (a group of a
-// million links does not keep one warp busy).
-__device__ __forceinline__ int32_t row_of_chunk(const int64_t *off, int32_t ng, int64_t e0, int64_t e) {
-    int32_t r = 0;
-    if ((threadIdx.x & 31) == 0) {
-        int32_t lo = 0, hi = ng - 1;
-        while (lo < hi) {
-            const int32_t mid = lo + ((hi - lo + 1) >> 1);
-            if (off[mid] <= e0)
-                lo = mid;
-            else
-                hi = mid - 1;
-        }
-        r = lo;
+// Packed rows: the distinct destinations of row g (at gloff[g]) move to the
+// CSR position g_out_off[g], each with its row beside it; columns are counted
+// for the transpose (one counter update per destination and warp: hub
+// columns take many links). Teams of kPackTeam lanes take a row each; rows
+// longer than kPackLong are listed for k_agg_pack_long.
+constexpr int kPackTeam = 8, kPackLong = 512;
+
+__device__ __forceinline__ void pack_link(int64_t i, int64_t len, int64_t from, int64_t to, int32_t g,
+                                          const int32_t *slab_dst, const fx_t *slab_fx, int32_t *out_dst,
+                                          fx_t *out_fx, int32_t *out_src, unsigned long long *colcnt) {
+    int32_t b = -1;
+    if (i < len) {
+        b = slab_dst[from + i];
+        out_dst[to + i] = b;
+        out_fx[to + i] = slab_fx[from + i];
+        out_src[to + i] = g;
     }
-    r = __shfl_sync(kFullMask, r, 0);
-    while (off[r + 1] <= e) r++;
-    return r;
+    const unsigned peers = __match_any_sync(kFullMask, b);  // every lane of the warp calls it
+    if (b >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(colcnt + b, (unsigned long long)__popc(peers));
 }
 
-// Packed rows: the slab entries of row g (at gloff[g]) move to the CSR
-// position g_out_off[g]; columns are counted for the transpose.
-__global__ void k_agg_pack(int32_t ng, int64_t m, const int64_t *gloff, const int64_t *g_out_off,
-                           const int32_t *slab_dst, const fx_t *slab_fx, int32_t *out_dst, fx_t *out_fx,
-                           unsigned long long *colcnt) {
-    const int lane = threadIdx.x & 31;
+__global__ void k_agg_pack(int32_t ng, const int64_t *gloff, const int64_t *g_out_off, const int32_t *slab_dst,
+                           const fx_t *slab_fx, int32_t *out_dst, fx_t *out_fx, int32_t *out_src,
+                           unsigned long long *colcnt, int32_t *longrows, unsigned long long *nlong) {
+    constexpr int kTeams = 32 / kPackTeam;
+    const int lane = threadIdx.x & 31, r = lane % kPackTeam;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {
-        const int64_t e = e0 + lane;
-        const int32_t g = row_of_chunk(g_out_off, ng, e0, e < m ? e : e0);
-        int32_t b = -1;
-        if (e < m) {
-            const int64_t src = gloff[g] + (e - g_out_off[g]);
-            b = slab_dst[src];
-            out_dst[e] = b;
-            out_fx[e] = slab_fx[src];
+    for (int64_t g0 = gw * kTeams; g0 < ng; g0 += nw * kTeams) {  // warp-uniform
+        const int64_t g = g0 + lane / kPackTeam;
+        int64_t len = 0, from = 0, to = 0;
+        if (g < ng) {
+            to = g_out_off[g];
+            len = g_out_off[g + 1] - to;
+            from = gloff[g];
         }
-        // one counter update per destination and warp (hub columns take many links)
-        const unsigned peers = __match_any_sync(kFullMask, b);
-        if (b >= 0 && lane == __ffs(peers) - 1) atomicAdd(colcnt + b, (unsigned long long)__popc(peers));
+        if (len > kPackLong) {
+            if (r == 0) longrows[atomicAdd(nlong, 1ull)] = (int32_t)g;
+            len = 0;
+        }
+        int64_t mx = len;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFullMask, mx, o));
+        for (int64_t i0 = 0; i0 < mx; i0 += kPackTeam)
+            pack_link(i0 + r, len, from, to, (int32_t)g, slab_dst, slab_fx, out_dst, out_fx, out_src, colcnt);
     }
 }
 
-// In-links: every link u->b of the group CSR appended to column b.
-__global__ void k_agg_transpose(int32_t ng, int64_t m, const int64_t *g_out_off, const int32_t *out_dst,
-                                const fx_t *out_fx, const int64_t *g_in_off, unsigned long long *colfill,
-                                int32_t *in_src, fx_t *in_fx) {
+// The listed long rows, a block each.
+__global__ void k_agg_pack_long(const int64_t *gloff, const int64_t *g_out_off, const int32_t *slab_dst,
+                                const fx_t *slab_fx, int32_t *out_dst, fx_t *out_fx, int32_t *out_src,
+                                unsigned long long *colcnt, const int32_t *longrows, const unsigned long long *nlong) {
+    const int64_t nl = (int64_t)*nlong;
+    for (int64_t k = blockIdx.x; k < nl; k += gridDim.x) {
+        const int32_t g = longrows[k];
+        const int64_t to = g_out_off[g], len = g_out_off[g + 1] - to, from = gloff[g];
+        for (int64_t i0 = 0; i0 < len; i0 += blockDim.x)  // uniform over the block
+            pack_link(i0 + threadIdx.x, len, from, to, g, slab_dst, slab_fx, out_dst, out_fx, out_src, colcnt);
+    }
+}
+
+// In-links: every link g->b of the group CSR appended to column b.
+__global__ void k_agg_transpose(int64_t m, const int32_t *out_src, const int32_t *out_dst, const fx_t *out_fx,
+                                const int64_t *g_in_off, unsigned long long *colfill, int32_t *in_src, fx_t *in_fx) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {
+    for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {  // warp-uniform
         const int64_t e = e0 + lane;
-        const int32_t g = row_of_chunk(g_out_off, ng, e0, e < m ? e : e0);
+        const int32_t g = e < m ? out_src[e] : -1;
         const int32_t b = e < m ? out_dst[e] : -1;
         const unsigned peers = __match_any_sync(kFullMask, b);
         const int leader = __ffs(peers) - 1;
@@ -896,10 +853,11 @@ static void configure_agg_kernels() {
     done[dev] = true;
 }
 
-int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *group,
-                        int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx, int64_t *g_in_off,
-                        int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, Arena &gtab_arena, fx_t *&gtab,
-                        int64_t &gtab_cap, Arena &ar, cudaStream_t s, const SweepWork *W) {
+int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *src,
+                        const int32_t *group, int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx,
+                        int32_t *g_out_src, int64_t *g_in_off, int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum,
+                        Arena &gtab_arena, fx_t *&gtab, int64_t &gtab_cap, Arena &ar, cudaStream_t s,
+                        const SweepWork *W) {
     configure_agg_kernels();
     int64_t E = 0;
     RMX_CUDA(cudaMemcpyAsync(&E, off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -907,29 +865,31 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     if (rowsum) RMX_CUDA(cudaMemsetAsync(rowsum, 0, sizeof(fx_t) * std::max(ng, 1), s));
     if (ng <= 0) return 0;
     size_t mk = ar.mark();
-    int64_t *gmoff = ar.alloc<int64_t>(ng + 1), *gloff = ar.alloc<int64_t>(ng + 1);
-    unsigned long long *fill = ar.alloc<unsigned long long>(ng + 1);
+    int64_t *gloff = ar.alloc<int64_t>(ng + 1);
+    unsigned long long *gcross = ar.alloc<unsigned long long>(ng + 1);
     // tot: [0] small [1] large [2] links out [3] max links [4] mid [5] huge groups, [6..8] their links,
-    // chunks and partitions [9] split pipeline over capacity
+    // chunks and partitions [10] long rows [12..14] split pipeline: chunks, partitions, over capacity
     int64_t *tot = ar.alloc<int64_t>(16);
-    RMX_CUDA(cudaMemsetAsync(gmoff, 0, sizeof(int64_t) * (ng + 1), s));
     RMX_CUDA(cudaMemsetAsync(gloff, 0, sizeof(int64_t) * (ng + 1), s));
+    RMX_CUDA(cudaMemsetAsync(gcross, 0, sizeof(unsigned long long) * (ng + 1), s));
+    RMX_CUDA(cudaMemsetAsync(tot, 0, sizeof(int64_t) * 16, s));
     k_agg_count<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, off, group,
-                                                                    reinterpret_cast<unsigned long long *>(gmoff),
                                                                     reinterpret_cast<unsigned long long *>(gloff));
     RMX_LAUNCHED();
-    scan_exclusive(gmoff, gmoff, ng + 1, nullptr, ar, s);
     scan_exclusive(gloff, gloff, ng + 1, nullptr, ar, s);
-    int32_t *members = ar.alloc<int32_t>(std::max(n, 1));
-    RMX_CUDA(cudaMemsetAsync(fill, 0, sizeof(unsigned long long) * (ng + 1), s));
-    k_agg_members<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, group, gmoff, fill, members);
-    RMX_LAUNCHED();
+    // the gathered ranges; each group's distinct destinations are written back to the start of its range
+    int32_t *slab_dst = ar.alloc<int32_t>(std::max<int64_t>(E, 1));
+    fx_t *slab_fx = ar.alloc<fx_t>(std::max<int64_t>(E, 1));
+    if (E > 0) {
+        k_agg_gather<<<blocks_for((E + 31) / 32 * 32, 256, num_sms() * 16), 256, 0, s>>>(E, src, dst, fx, group, gloff,
+                                                                                        gcross, slab_dst, slab_fx);
+        RMX_LAUNCHED();
+    }
     uint8_t *fsmall = ar.alloc<uint8_t>(ng), *fmid = ar.alloc<uint8_t>(ng), *flarge = ar.alloc<uint8_t>(ng),
             *fhuge = ar.alloc<uint8_t>(ng);
-    RMX_CUDA(cudaMemsetAsync(tot, 0, sizeof(int64_t) * 16, s));
     const int64_t part_links = eval_tuning().hub_part;
     k_agg_bins<<<blocks_for(ng, 256, num_sms() * 32), 256, 0, s>>>(
-        ng, gloff, part_links, fsmall, fmid, flarge, fhuge, reinterpret_cast<unsigned long long *>(tot + 3),
+        ng, gcross, part_links, fsmall, fmid, flarge, fhuge, reinterpret_cast<unsigned long long *>(tot + 3),
         reinterpret_cast<unsigned long long *>(tot + 6));
     RMX_LAUNCHED();
     int32_t *lsmall = ar.alloc<int32_t>(ng), *lmid = ar.alloc<int32_t>(ng), *llarge = ar.alloc<int32_t>(ng),
@@ -938,8 +898,6 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     compact_flags(fmid, ng, lmid, tot + 4, ar, s);
     compact_flags(flarge, ng, llarge, tot + 1, ar, s);
     compact_flags(fhuge, ng, lhuge, tot + 5, ar, s);
-    int32_t *slab_dst = ar.alloc<int32_t>(std::max<int64_t>(E, 1));
-    fx_t *slab_fx = ar.alloc<fx_t>(std::max<int64_t>(E, 1));
     int64_t *rowlen = g_out_off;  // row lengths, scanned in place into offsets below
     RMX_CUDA(cudaMemsetAsync(rowlen, 0, sizeof(int64_t) * (ng + 1), s));
     // a group of L links needs a table of next_pow2(2L) slots; beyond shared memory, a global slice per block
@@ -961,13 +919,8 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
         gtab_cap = need;
     }
     AggArgs a;
-    a.off = off;
-    a.dst = dst;
-    a.fx = fx;
-    a.group = group;
-    a.gmoff = gmoff;
     a.gloff = gloff;
-    a.members = members;
+    a.gcross = gcross;
     a.slab_dst = slab_dst;
     a.slab_fx = slab_fx;
     a.rowlen = rowlen;
@@ -988,26 +941,12 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     }
     if (n_huge > 0) {
         HugeArgs h;
-        h.off = off;
-        h.dst = dst;
-        h.fx = fx;
-        h.group = group;
-        h.members = members;
         h.gloff = gloff;
+        h.gcross = gcross;
         h.hlist = lhuge;
         h.nh = tot + 5;
-        const int64_t cap_m = std::max<int64_t>(1, std::min<int64_t>(n, huge_links));  // nonzero-degree members
-        h.hidx = ar.alloc<int32_t>(ng);
-        uint8_t *mflag = ar.alloc<uint8_t>(std::max(n, 1));
-        int32_t *hml = ar.alloc<int32_t>(cap_m);
-        h.hml = hml;
-        h.nhm = tot + 10;
-        h.hmo = ar.alloc<int64_t>(cap_m + 1);
-        h.hgj = ar.alloc<int32_t>(cap_m);
-        h.hmb = ar.alloc<int64_t>(n_huge + 1);
         h.coff = ar.alloc<int64_t>(n_huge + 1);
         h.poff = ar.alloc<int64_t>(n_huge + 1);
-        h.cmem = ar.alloc<int32_t>(huge_chunks);
         h.cgrp = ar.alloc<int32_t>(huge_chunks);
         h.pgrp = ar.alloc<int32_t>(huge_parts);
         h.pcnt = ar.alloc<unsigned long long>(huge_parts);
@@ -1024,20 +963,9 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
         h.rowlen = rowlen;
         h.rowsum = rowsum;
         const cudaStream_t hs = s_huge;
-        RMX_CUDA(cudaMemsetAsync(h.hidx, 0xff, sizeof(int32_t) * ng, hs));
-        k_hg_index<<<blocks_for(n_huge, 256, num_sms() * 4), 256, 0, hs>>>(h);
-        RMX_LAUNCHED();
-        k_hg_member_flags<<<blocks_for(n, 256, num_sms() * 32), 256, 0, hs>>>(n, h, mflag);
-        RMX_LAUNCHED();
-        compact_flags(mflag, n, hml, tot + 10, ar, hs);
-        k_hg_members<<<blocks_for(cap_m, 256, num_sms() * 32), 256, 0, hs>>>((int32_t)cap_m, h, h.hmo);
-        RMX_LAUNCHED();
-        scan_exclusive(h.hmo, h.hmo, cap_m, h.hmo + cap_m, ar, hs);
         k_hg_plan<<<1, 1024, 0, hs>>>(h);
         RMX_LAUNCHED();
-        k_hg_starts<<<blocks_for(cap_m, 256, num_sms() * 32), 256, 0, hs>>>(h);
-        RMX_LAUNCHED();
-        const unsigned G = num_sms() * 6;
+        const unsigned G = num_sms() * 8;
         k_hg_links<false><<<G, kHgT, 0, hs>>>(h);
         RMX_LAUNCHED();
         k_hg_offsets<<<1, 1024, 0, hs>>>(h);
@@ -1073,16 +1001,22 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     if (over)  // the sizes come from the same counts the plan sums, so this does not happen
         throw std::runtime_error("aggregate_links: split pipeline over its capacity");
     if (m > 0) {
-        const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
-        k_agg_pack<<<Gm, 256, 0, s>>>(ng, m, gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx,
-                                      reinterpret_cast<unsigned long long *>(g_in_off));
+        int32_t *longrows = lsmall;  // the bin lists are done with
+        unsigned long long *nlong = reinterpret_cast<unsigned long long *>(tot + 10);
+        k_agg_pack<<<blocks_for((int64_t)ng * kPackTeam, 256, num_sms() * 16), 256, 0, s>>>(
+            ng, gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx, g_out_src,
+            reinterpret_cast<unsigned long long *>(g_in_off), longrows, nlong);
+        RMX_LAUNCHED();
+        k_agg_pack_long<<<num_sms() * 4, 256, 0, s>>>(gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx,
+                                                     g_out_src, reinterpret_cast<unsigned long long *>(g_in_off),
+                                                     longrows, nlong);
         RMX_LAUNCHED();
     }
     scan_exclusive(g_in_off, g_in_off, ng + 1, nullptr, ar, s);
-    RMX_CUDA(cudaMemsetAsync(fill, 0, sizeof(unsigned long long) * (ng + 1), s));
+    RMX_CUDA(cudaMemsetAsync(gcross, 0, sizeof(unsigned long long) * (ng + 1), s));  // the column fill counters
     if (m > 0) {
         const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
-        k_agg_transpose<<<Gm, 256, 0, s>>>(ng, m, g_out_off, g_out_dst, g_out_fx, g_in_off, fill, g_in_src, g_in_fx);
+        k_agg_transpose<<<Gm, 256, 0, s>>>(m, g_out_src, g_out_dst, g_out_fx, g_in_off, gcross, g_in_src, g_in_fx);
         RMX_LAUNCHED();
     }
     RMX_CUDA(cudaStreamSynchronize(s));

@@ -500,7 +500,7 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     const int64_t Ein = std::max<int64_t>(n_edges, 1), Eb = std::max<int64_t>(repl ? u->full_edges : n_edges, 1);
     scratch.init((size_t)(88 * Eb + 24 * (int64_t)n + 40 * (int64_t)K) + (64u << 20));
     // long-lived arrays: node CSR/CSC, three levels, module and instance state
-    perm.init((size_t)(144 * Eb + 568 * (int64_t)n + (K > 1 ? 16 * (int64_t)n + 64 * (int64_t)K : 0)) + (64u << 20));
+    perm.init((size_t)(156 * Eb + 568 * (int64_t)n + (K > 1 ? 16 * (int64_t)n + 64 * (int64_t)K : 0)) + (64u << 20));
     out_off = perm.alloc<int64_t>(n + 1);
     in_off = perm.alloc<int64_t>(n + 1);
     int32_t *d_src = scratch.alloc<int32_t>(Ein), *d_dst = scratch.alloc<int32_t>(Ein);
@@ -625,6 +625,9 @@ void rmx_graph::alloc_engine() {
     node_lv.mod = nmod;
     node_lv.inst = K > 1 ? node_inst : zeros;
     node_lv.nnodes = nullptr;
+    node_lv.out_src = perm.alloc<int32_t>(Em);  // the coarsening reads every link's row
+    if (E > 0) rows_of_links(n, out_off, node_lv.out_src, stream);
+    for (Level &lv : sn_buf) lv.out_src = perm.alloc<int32_t>(Em);
     for (Level *lv : {&sn_buf[0], &sn_buf[1], &sub_lv}) {
         lv->out_off = perm.alloc<int64_t>(n + 1);
         lv->in_off = perm.alloc<int64_t>(n + 1);
@@ -1146,12 +1149,13 @@ void rmx_graph::convert_to_supernodes(bool from_sn) {
     RMX_CUDA(cudaStreamSynchronize(stream));
     dst.n = (int32_t)nsn;
     if (from_sn)
-        dst.m = aggregate_links(src.n, src.out_off, src.out_dst, src.out_fx, group, dst.n, dst.out_off, dst.out_dst,
-                                dst.out_fx, dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_arena, agg_tab, agg_cap, scratch,
-                                stream, &work);
+        dst.m = aggregate_links(src.n, src.out_off, src.out_dst, src.out_fx, src.out_src, group, dst.n, dst.out_off,
+                                dst.out_dst, dst.out_fx, dst.out_src, dst.in_off, dst.in_src, dst.in_fx, nullptr,
+                                agg_arena, agg_tab, agg_cap, scratch, stream, &work);
     else
-        dst.m = aggregate_links(N, out_off, out_dst, out_fx, node_sn, dst.n, dst.out_off, dst.out_dst, dst.out_fx,
-                                dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_arena, agg_tab, agg_cap, scratch, stream, &work);
+        dst.m = aggregate_links(N, out_off, out_dst, out_fx, node_lv.out_src, node_sn, dst.n, dst.out_off, dst.out_dst,
+                                dst.out_fx, dst.out_src, dst.in_off, dst.in_src, dst.in_fx, nullptr, agg_arena, agg_tab,
+                                agg_cap, scratch, stream, &work);
     scratch.release(mk);
     sn_cur = 1 - sn_cur;
     count_units(sn(), mods, stream);
@@ -1258,8 +1262,9 @@ void rmx_graph::generate_sub_modules() {
     RMX_LAUNCHED();
     {
         fx_t *rowsum = scratch.alloc<fx_t>(std::max<int64_t>(nsn, 1));
-        sl.m = aggregate_links(N, out_off, out_dst, out_fx, node_sn, sl.n, sl.out_off, sl.out_dst, sl.out_fx,
-                               sl.in_off, sl.in_src, sl.in_fx, rowsum, agg_arena, agg_tab, agg_cap, scratch, stream, &work);
+        sl.m = aggregate_links(N, out_off, out_dst, out_fx, node_lv.out_src, node_sn, sl.n, sl.out_off, sl.out_dst,
+                               sl.out_fx, sl.out_src, sl.in_off, sl.in_src, sl.in_fx, rowsum, agg_arena, agg_tab, agg_cap,
+                               scratch, stream, &work);
         k_sn_set_out<<<blocks_for(nsn, 256, num_sms() * 32), 256, 0, stream>>>(sl.n, rowsum, sl.attr);
         RMX_LAUNCHED();
     }

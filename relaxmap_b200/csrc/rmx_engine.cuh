@@ -24,6 +24,7 @@ struct Level {
     int64_t m = 0;      // links
     int64_t *out_off = nullptr, *in_off = nullptr;
     int32_t *out_dst = nullptr, *in_src = nullptr;
+    int32_t *out_src = nullptr;  // row of every out-link (levels that are coarsened again)
     fx_t *out_fx = nullptr, *in_fx = nullptr;
     Stat4 *attr = nullptr;
     int32_t *mod = nullptr;     // module id of each unit
@@ -260,14 +261,18 @@ int64_t coarsen_links(int32_t n, const int64_t *out_off, const int32_t *out_dst,
                       fx_t *g_in_fx, Arena &ar, cudaStream_t s);
 
 // Engine aggregation of rows (nodes or super-nodes) into groups by hashing:
-// fixed-point sums only, rows and columns in no particular order. rowsum (may
-// be NULL) receives each group's total out-flow. gtab / gtab_cap: a global
-// table in gtab_arena, grown on demand for groups too large for shared memory.
-// W (may be NULL): auxiliary streams and events on which the size bins run
-// concurrently.
-int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *group,
-                        int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx, int64_t *g_in_off,
-                        int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum, Arena &gtab_arena, fx_t *&gtab,
-                        int64_t &gtab_cap, Arena &ar, cudaStream_t s, const SweepWork *W);
+// fixed-point sums only, rows and columns in no particular order. src: the
+// row of every input link (CSR order); g_out_src receives the row (group) of
+// every output link. rowsum (may be NULL) receives each group's total
+// out-flow. gtab / gtab_cap: a global table in gtab_arena, grown on demand for
+// groups too large for shared memory. W (may be NULL): auxiliary streams and
+// events on which the size bins run concurrently.
+int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const fx_t *fx, const int32_t *src,
+                        const int32_t *group, int32_t ng, int64_t *g_out_off, int32_t *g_out_dst, fx_t *g_out_fx,
+                        int32_t *g_out_src, int64_t *g_in_off, int32_t *g_in_src, fx_t *g_in_fx, fx_t *rowsum,
+                        Arena &gtab_arena, fx_t *&gtab, int64_t &gtab_cap, Arena &ar, cudaStream_t s,
+                        const SweepWork *W);
+// src[e] = the row of link e for the CSR offsets off[0..n] (a warp per row).
+void rows_of_links(int32_t n, const int64_t *off, int32_t *src, cudaStream_t s);
 
 }  // namespace rmx
