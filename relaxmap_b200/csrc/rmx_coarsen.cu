@@ -760,8 +760,9 @@ __global__ void __launch_bounds__(kHgT, 2) k_hg_reduce(HugeArgs a) {
 // CSR position g_out_off[g], each with its row beside it; columns are counted
 // for the transpose (one counter update per destination and warp: hub
 // columns take many links). Teams of kPackTeam lanes take a row each; rows
-// longer than kPackLong are listed for k_agg_pack_long.
-constexpr int kPackTeam = 8, kPackLong = 512;
+// longer than kPackLong are listed, in chunks of kPackChunk entries, for
+// k_agg_pack_long.
+constexpr int kPackTeam = 8, kPackLong = 512, kPackChunk = 8192;
 
 __device__ __forceinline__ void pack_link(int64_t i, int64_t len, int64_t from, int64_t to, int32_t g,
                                           const int32_t *slab_dst, const fx_t *slab_fx, int32_t *out_dst,
@@ -779,7 +780,7 @@ __device__ __forceinline__ void pack_link(int64_t i, int64_t len, int64_t from, 
 
 __global__ void k_agg_pack(int32_t ng, const int64_t *gloff, const int64_t *g_out_off, const int32_t *slab_dst,
                            const fx_t *slab_fx, int32_t *out_dst, fx_t *out_fx, int32_t *out_src,
-                           unsigned long long *colcnt, int32_t *longrows, unsigned long long *nlong) {
+                           unsigned long long *colcnt, int64_t *longrows, unsigned long long *nlong) {
     constexpr int kTeams = 32 / kPackTeam;
     const int lane = threadIdx.x & 31, r = lane % kPackTeam;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -791,8 +792,12 @@ __global__ void k_agg_pack(int32_t ng, const int64_t *gloff, const int64_t *g_ou
             len = g_out_off[g + 1] - to;
             from = gloff[g];
         }
-        if (len > kPackLong) {
-            if (r == 0) longrows[atomicAdd(nlong, 1ull)] = (int32_t)g;
+        if (len > kPackLong) {  // listed as chunks of kPackChunk entries
+            const int64_t nc = (len + kPackChunk - 1) / kPackChunk;
+            if (r == 0) {
+                const unsigned long long k0 = atomicAdd(nlong, (unsigned long long)nc);
+                for (int64_t c = 0; c < nc; c++) longrows[k0 + c] = ((int64_t)g << 32) | c;
+            }
             len = 0;
         }
         int64_t mx = len;
@@ -803,16 +808,83 @@ __global__ void k_agg_pack(int32_t ng, const int64_t *gloff, const int64_t *g_ou
     }
 }
 
-// The listed long rows, a block each.
+// The listed chunks of long rows (row << 32 | chunk), a block each.
 __global__ void k_agg_pack_long(const int64_t *gloff, const int64_t *g_out_off, const int32_t *slab_dst,
                                 const fx_t *slab_fx, int32_t *out_dst, fx_t *out_fx, int32_t *out_src,
-                                unsigned long long *colcnt, const int32_t *longrows, const unsigned long long *nlong) {
+                                unsigned long long *colcnt, const int64_t *longrows, const unsigned long long *nlong) {
     const int64_t nl = (int64_t)*nlong;
     for (int64_t k = blockIdx.x; k < nl; k += gridDim.x) {
-        const int32_t g = longrows[k];
-        const int64_t to = g_out_off[g], len = g_out_off[g + 1] - to, from = gloff[g];
+        const int32_t g = (int32_t)(longrows[k] >> 32);
+        const int64_t c0 = (longrows[k] & 0xffffffffll) * kPackChunk;
+        const int64_t row = g_out_off[g + 1] - g_out_off[g];
+        const int64_t to = g_out_off[g] + c0, len = min((int64_t)kPackChunk, row - c0), from = gloff[g] + c0;
         for (int64_t i0 = 0; i0 < len; i0 += blockDim.x)  // uniform over the block
             pack_link(i0 + threadIdx.x, len, from, to, g, slab_dst, slab_fx, out_dst, out_fx, out_src, colcnt);
+    }
+}
+
+// The transpose of a large level in two passes, so that the scattered writes
+// of the second land in a window of the CSC small enough for L2 to merge:
+//   partition  blocks take tiles of kTrTile links, count them per column
+//              bucket (kTrBuckets buckets of W consecutive columns) in shared
+//              memory, reserve each bucket's share with one atomic per
+//              bucket and block, and write (row, column, flow) there: the
+//              staging array ends up ordered by column bucket, each bucket at
+//              its columns' own CSC offset;
+//   place      threads take staged links in order and put each one in its
+//              column (k_agg_transpose's step), the blocks in flight all
+//              working inside one or two buckets' stretch of the CSC.
+constexpr int kTrTile = 32768, kTrBuckets = 2048;
+
+__global__ void __launch_bounds__(256) k_tr_partition(int64_t m, int32_t ng, int32_t W, const int32_t *out_src,
+                                                      const int32_t *out_dst, const fx_t *out_fx,
+                                                      const int64_t *g_in_off, unsigned long long *bfill,
+                                                      int2 *st_gb, fx_t *st_fx) {
+    __shared__ unsigned int hist[kTrBuckets];
+    __shared__ unsigned long long base[kTrBuckets];
+    const int nb = (ng + W - 1) / W;
+    for (int64_t t0 = (int64_t)blockIdx.x * kTrTile; t0 < m; t0 += (int64_t)gridDim.x * kTrTile) {
+        const int64_t t1 = min(m, t0 + kTrTile);
+        __syncthreads();  // the previous tile's readers of base are done
+        for (int k = threadIdx.x; k < nb; k += blockDim.x) hist[k] = 0;
+        __syncthreads();
+        for (int64_t e = t0 + threadIdx.x; e < t1; e += blockDim.x) atomicAdd(hist + out_dst[e] / W, 1u);
+        __syncthreads();
+        for (int k = threadIdx.x; k < nb; k += blockDim.x) {
+            const unsigned int c = hist[k];
+            if (c) base[k] = (unsigned long long)g_in_off[(int64_t)k * W] + atomicAdd(bfill + k, (unsigned long long)c);
+            hist[k] = 0;  // now the block's cursor per bucket
+        }
+        __syncthreads();
+        for (int64_t e = t0 + threadIdx.x; e < t1; e += blockDim.x) {
+            const int32_t b = out_dst[e];
+            const int k = b / W;
+            const int64_t p = (int64_t)base[k] + atomicAdd(hist + k, 1u);
+            st_gb[p] = make_int2(out_src[e], b);
+            st_fx[p] = out_fx[e];
+        }
+    }
+}
+
+__global__ void k_tr_place(int64_t m, const int2 *st_gb, const fx_t *st_fx, const int64_t *g_in_off,
+                           unsigned long long *colfill, int32_t *in_src, fx_t *in_fx) {
+    const int lane = threadIdx.x & 31;
+    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {  // warp-uniform
+        const int64_t e = e0 + lane;
+        int2 gb = make_int2(-1, -1);
+        if (e < m) gb = st_gb[e];
+        const int32_t b = gb.y;
+        const unsigned peers = __match_any_sync(kFullMask, b);
+        const int leader = __ffs(peers) - 1;
+        unsigned long long base = 0;
+        if (b >= 0 && lane == leader) base = atomicAdd(colfill + b, (unsigned long long)__popc(peers));
+        base = __shfl_sync(kFullMask, base, leader);
+        if (b >= 0) {
+            const int64_t q = g_in_off[b] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
+            in_src[q] = gb.x;
+            in_fx[q] = st_fx[e];
+        }
     }
 }
 
@@ -1001,21 +1073,33 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     if (over)  // the sizes come from the same counts the plan sums, so this does not happen
         throw std::runtime_error("aggregate_links: split pipeline over its capacity");
     if (m > 0) {
-        int32_t *longrows = lsmall;  // the bin lists are done with
+        // chunks of long rows: fewer than ng + m / kPackChunk + 1
+        int64_t *longrows = ar.alloc<int64_t>(ng + m / kPackChunk + 1);
         unsigned long long *nlong = reinterpret_cast<unsigned long long *>(tot + 10);
         k_agg_pack<<<blocks_for((int64_t)ng * kPackTeam, 256, num_sms() * 16), 256, 0, s>>>(
             ng, gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx, g_out_src,
             reinterpret_cast<unsigned long long *>(g_in_off), longrows, nlong);
         RMX_LAUNCHED();
-        k_agg_pack_long<<<num_sms() * 4, 256, 0, s>>>(gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx,
+        k_agg_pack_long<<<num_sms() * 8, 256, 0, s>>>(gloff, g_out_off, slab_dst, slab_fx, g_out_dst, g_out_fx,
                                                      g_out_src, reinterpret_cast<unsigned long long *>(g_in_off),
                                                      longrows, nlong);
         RMX_LAUNCHED();
     }
     scan_exclusive(g_in_off, g_in_off, ng + 1, nullptr, ar, s);
     RMX_CUDA(cudaMemsetAsync(gcross, 0, sizeof(unsigned long long) * (ng + 1), s));  // the column fill counters
-    if (m > 0) {
-        const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
+    const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
+    if (m >= ((int64_t)1 << 22) && ng > kTrBuckets) {  // two passes (k_tr_partition)
+        const int32_t W = (ng + kTrBuckets - 1) / kTrBuckets;
+        unsigned long long *bfill = ar.alloc<unsigned long long>(kTrBuckets);
+        int2 *st_gb = ar.alloc<int2>(m);
+        fx_t *st_fx = ar.alloc<fx_t>(m);
+        RMX_CUDA(cudaMemsetAsync(bfill, 0, sizeof(unsigned long long) * kTrBuckets, s));
+        k_tr_partition<<<(unsigned)std::min<int64_t>((m + kTrTile - 1) / kTrTile, num_sms() * 8), 256, 0, s>>>(
+            m, ng, W, g_out_src, g_out_dst, g_out_fx, g_in_off, bfill, st_gb, st_fx);
+        RMX_LAUNCHED();
+        k_tr_place<<<Gm, 256, 0, s>>>(m, st_gb, st_fx, g_in_off, gcross, g_in_src, g_in_fx);
+        RMX_LAUNCHED();
+    } else if (m > 0) {
         k_agg_transpose<<<Gm, 256, 0, s>>>(m, g_out_src, g_out_dst, g_out_fx, g_in_off, gcross, g_in_src, g_in_fx);
         RMX_LAUNCHED();
     }

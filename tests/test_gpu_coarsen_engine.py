@@ -184,6 +184,35 @@ def test_huge_groups(built_lib, oracle_mod, planted, part_links):
     check_against(cv, ref, off, dst, f, p, tw, dg, grp)
 
 
+def test_large_level():
+    """A level of more than 2^22 links over more than 2048 groups, so that the
+    in-links are placed by the two-pass transpose (column buckets first): the
+    CSR sums equal the exact integer sums of the member links, and the CSC is
+    exactly the transpose of the CSR."""
+    from relaxmap_b200 import Graph, synth
+    sg = synth.planted_partition(400_000, 14, 400, 10, 300, 0.5, seed=5)
+    rng = np.random.default_rng(8)
+    part = (rng.integers(0, 5000, sg.n) * 7).astype(np.int32)
+    with Graph.from_edges(sg.src, sg.dst, sg.w, n=sg.n) as G:
+        st = G.initiate()
+        off, dst, _, _ = G.links()
+        cv = G.coarsen_engine(part)
+    nsn = cv["n_sn"]
+    grp = np.searchsorted(np.unique(part), part).astype(np.int64)
+    exp = expected_links(off, dst, st["f"], grp, nsn)
+    assert len(exp["csr"][0]) > (1 << 22) and nsn > 2048
+    od, ofx = rows_sorted(cv["out_off"], cv["out_dst"], cv["out_fx"])
+    np.testing.assert_array_equal(ofx, exp["csr"][0])
+    # the CSC as (column, row, flow) triples equals the CSR's, ordered the same way
+    orow = np.repeat(np.arange(nsn), np.diff(cv["out_off"]))
+    icol = np.repeat(np.arange(nsn), np.diff(cv["in_off"]))
+    a = np.lexsort((orow, cv["out_dst"]))
+    b = np.lexsort((cv["in_src"], icol))
+    np.testing.assert_array_equal(cv["out_dst"][a], icol[b])
+    np.testing.assert_array_equal(orow[a], cv["in_src"][b])
+    np.testing.assert_array_equal(cv["out_fx"][a], cv["in_fx"][b])
+
+
 @pytest.mark.parametrize("k1,k2", [(400, 17), (1500, 300), (300, 2)])
 def test_second_level(built_lib, oracle_mod, planted, k1, k2):
     """Super-nodes converted again: level 2 aggregated from level 1's links
