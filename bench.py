@@ -197,9 +197,12 @@ def peaks() -> dict:
 
 
 # DRAM bytes (read + write) per link evaluated by the dominant evaluation
-# kernel, keyed by (workload, degree bin): from one ncu capture of that kernel
-# on the benched graph (the command and the counters are in profiles/).
-EVAL_TRAFFIC_PER_LINK = {}
+# kernel, keyed by (workload, degree bin): one ncu capture of that kernel (one
+# launch, dram__bytes_read.sum + dram__bytes_write.sum, a single pass) in the
+# evaluation snapshot of the benched graph (--eval-snapshot: every node against
+# singleton modules), divided by the links that launch read; the command and
+# the counters are in profiles/eval_large_rmat24.md.
+EVAL_TRAFFIC_PER_LINK = {("rmat24", "large"): (17.10e9 + 6.19e6) / 97_860_671}
 
 DOMINANT_BIN = "large"
 
@@ -476,6 +479,11 @@ def main():
         "roofline": {"kernel": f"move evaluation, {dom} bin ({EVAL_BIN_KERNELS[dom]})", "bound": "hbm",
                      "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": achieved / pk["hbm_gbs"],
                      "peak_source": pk["source"], "traffic": traffic,
+                     "traffic_note": "per launch: DRAM bytes per link from one ncu capture of this kernel on this "
+                                     "graph x the links per launch here; the random gathers (the neighbour's module, "
+                                     "the candidate's statistics and terms) each move a 32-byte sector",
+                     "traffic_frac": (traffic / (db["ms"] / max(db["launches"], 1) / 1e3) / 1e9 / pk["hbm_gbs"]
+                                      if traffic is not None and db["ms"] > 0 else None),
                      "algorithmic_bytes_per_launch": db["bytes"] / max(db["launches"], 1),
                      "launch_ms_avg": db["ms"] / max(db["launches"], 1),
                      "bins": {b: {"ms": round(v["ms"], 3), "launches": v["launches"], "links": v["links"],

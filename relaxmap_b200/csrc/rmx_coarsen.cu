@@ -823,71 +823,6 @@ __global__ void k_agg_pack_long(const int64_t *gloff, const int64_t *g_out_off, 
     }
 }
 
-// The transpose of a large level in two passes, so that the scattered writes
-// of the second land in a window of the CSC small enough for L2 to merge:
-//   partition  blocks take tiles of kTrTile links, count them per column
-//              bucket (kTrBuckets buckets of W consecutive columns) in shared
-//              memory, reserve each bucket's share with one atomic per
-//              bucket and block, and write (row, column, flow) there: the
-//              staging array ends up ordered by column bucket, each bucket at
-//              its columns' own CSC offset;
-//   place      threads take staged links in order and put each one in its
-//              column (k_agg_transpose's step), the blocks in flight all
-//              working inside one or two buckets' stretch of the CSC.
-constexpr int kTrTile = 32768, kTrBuckets = 2048;
-
-__global__ void __launch_bounds__(256) k_tr_partition(int64_t m, int32_t ng, int32_t W, const int32_t *out_src,
-                                                      const int32_t *out_dst, const fx_t *out_fx,
-                                                      const int64_t *g_in_off, unsigned long long *bfill,
-                                                      int2 *st_gb, fx_t *st_fx) {
-    __shared__ unsigned int hist[kTrBuckets];
-    __shared__ unsigned long long base[kTrBuckets];
-    const int nb = (ng + W - 1) / W;
-    for (int64_t t0 = (int64_t)blockIdx.x * kTrTile; t0 < m; t0 += (int64_t)gridDim.x * kTrTile) {
-        const int64_t t1 = min(m, t0 + kTrTile);
-        __syncthreads();  // the previous tile's readers of base are done
-        for (int k = threadIdx.x; k < nb; k += blockDim.x) hist[k] = 0;
-        __syncthreads();
-        for (int64_t e = t0 + threadIdx.x; e < t1; e += blockDim.x) atomicAdd(hist + out_dst[e] / W, 1u);
-        __syncthreads();
-        for (int k = threadIdx.x; k < nb; k += blockDim.x) {
-            const unsigned int c = hist[k];
-            if (c) base[k] = (unsigned long long)g_in_off[(int64_t)k * W] + atomicAdd(bfill + k, (unsigned long long)c);
-            hist[k] = 0;  // now the block's cursor per bucket
-        }
-        __syncthreads();
-        for (int64_t e = t0 + threadIdx.x; e < t1; e += blockDim.x) {
-            const int32_t b = out_dst[e];
-            const int k = b / W;
-            const int64_t p = (int64_t)base[k] + atomicAdd(hist + k, 1u);
-            st_gb[p] = make_int2(out_src[e], b);
-            st_fx[p] = out_fx[e];
-        }
-    }
-}
-
-__global__ void k_tr_place(int64_t m, const int2 *st_gb, const fx_t *st_fx, const int64_t *g_in_off,
-                           unsigned long long *colfill, int32_t *in_src, fx_t *in_fx) {
-    const int lane = threadIdx.x & 31;
-    const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {  // warp-uniform
-        const int64_t e = e0 + lane;
-        int2 gb = make_int2(-1, -1);
-        if (e < m) gb = st_gb[e];
-        const int32_t b = gb.y;
-        const unsigned peers = __match_any_sync(kFullMask, b);
-        const int leader = __ffs(peers) - 1;
-        unsigned long long base = 0;
-        if (b >= 0 && lane == leader) base = atomicAdd(colfill + b, (unsigned long long)__popc(peers));
-        base = __shfl_sync(kFullMask, base, leader);
-        if (b >= 0) {
-            const int64_t q = g_in_off[b] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
-            in_src[q] = gb.x;
-            in_fx[q] = st_fx[e];
-        }
-    }
-}
-
 // In-links: every link g->b of the group CSR appended to column b.
 __global__ void k_agg_transpose(int64_t m, const int32_t *out_src, const int32_t *out_dst, const fx_t *out_fx,
                                 const int64_t *g_in_off, unsigned long long *colfill, int32_t *in_src, fx_t *in_fx) {
@@ -1087,19 +1022,8 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     }
     scan_exclusive(g_in_off, g_in_off, ng + 1, nullptr, ar, s);
     RMX_CUDA(cudaMemsetAsync(gcross, 0, sizeof(unsigned long long) * (ng + 1), s));  // the column fill counters
-    const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
-    if (m >= ((int64_t)1 << 22) && ng > kTrBuckets) {  // two passes (k_tr_partition)
-        const int32_t W = (ng + kTrBuckets - 1) / kTrBuckets;
-        unsigned long long *bfill = ar.alloc<unsigned long long>(kTrBuckets);
-        int2 *st_gb = ar.alloc<int2>(m);
-        fx_t *st_fx = ar.alloc<fx_t>(m);
-        RMX_CUDA(cudaMemsetAsync(bfill, 0, sizeof(unsigned long long) * kTrBuckets, s));
-        k_tr_partition<<<(unsigned)std::min<int64_t>((m + kTrTile - 1) / kTrTile, num_sms() * 8), 256, 0, s>>>(
-            m, ng, W, g_out_src, g_out_dst, g_out_fx, g_in_off, bfill, st_gb, st_fx);
-        RMX_LAUNCHED();
-        k_tr_place<<<Gm, 256, 0, s>>>(m, st_gb, st_fx, g_in_off, gcross, g_in_src, g_in_fx);
-        RMX_LAUNCHED();
-    } else if (m > 0) {
+    if (m > 0) {
+        const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
         k_agg_transpose<<<Gm, 256, 0, s>>>(m, g_out_src, g_out_dst, g_out_fx, g_in_off, gcross, g_in_src, g_in_fx);
         RMX_LAUNCHED();
     }

@@ -185,10 +185,9 @@ def test_huge_groups(built_lib, oracle_mod, planted, part_links):
 
 
 def test_large_level():
-    """A level of more than 2^22 links over more than 2048 groups, so that the
-    in-links are placed by the two-pass transpose (column buckets first): the
-    CSR sums equal the exact integer sums of the member links, and the CSC is
-    exactly the transpose of the CSR."""
+    """A level of more than 2^22 links over 5000 groups (long rows packed in
+    chunks by many blocks): the CSR sums equal the exact integer sums of the
+    member links, and the CSC is exactly the transpose of the CSR."""
     from relaxmap_b200 import Graph, synth
     sg = synth.planted_partition(400_000, 14, 400, 10, 300, 0.5, seed=5)
     rng = np.random.default_rng(8)
