@@ -689,7 +689,15 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? RMX_LRG_MINB : (NT == 128 ? 8 
 constexpr int kHubCh = 2048;     // links per chunk item
 constexpr int kHubPT = 256;      // threads per block of the pipeline
 constexpr int kPartLinks = 1024; // mean links per partition (default of the run-time setting)
-constexpr int kPartCap = 4096;   // shared table slots of a partition block (at most half filled per round)
+// shared table slots of a partition block (at most half filled per round) and
+// its resident blocks per SM
+#ifndef RMX_HUB_CAP
+#define RMX_HUB_CAP 2048
+#endif
+#ifndef RMX_HUB_MINB
+#define RMX_HUB_MINB 4
+#endif
+constexpr int kPartCap = RMX_HUB_CAP;
 constexpr int kMaxParts = 1 << 20;
 constexpr size_t kHubEvalSmem = (size_t)kPartCap * (2 * sizeof(fx_t) + sizeof(int32_t));
 
@@ -942,7 +950,7 @@ __global__ void __launch_bounds__(1024) k_hub_offsets(HubPlan p) {
 // partitioning makes rare): round r takes the keys whose second hash h2 (a
 // bijection of the key) has h2 mod R == r, and R doubles until no round
 // overfills (at R = 2^31 a round holds at most two keys).
-__global__ void __launch_bounds__(kHubPT, 2) k_hub_eval(EvalArgs a, HubPlan p) {
+__global__ void __launch_bounds__(kHubPT, RMX_HUB_MINB) k_hub_eval(EvalArgs a, HubPlan p) {
     extern __shared__ __align__(16) unsigned char hub_smem[];  // kHubEvalSmem bytes
     fx_t *vo = reinterpret_cast<fx_t *>(hub_smem);
     fx_t *vi = vo + kPartCap;
@@ -1637,7 +1645,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
         hp.punit = W.hub_punit;
         hp.part_links = tg.hub_part;
         const cudaStream_t hs = on(4);
-        const unsigned G = num_sms() * 8, GE = num_sms() * 2;
+        const unsigned G = num_sms() * 8, GE = num_sms() * RMX_HUB_MINB;
         if (tm) tm->begin(kTimerBinHub, hs);
         k_hub_plan<<<1, 1024, 0, hs>>>(a, hp);
         RMX_LAUNCHED();
