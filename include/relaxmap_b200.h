@@ -305,7 +305,7 @@ rmx_status rmx_adjoint_backward(rmx_graph *g, const int32_t *part, double tau, d
 typedef struct rmx_tuning {
     int32_t eval_mid_grid;    /* mid bin (default 8) */
     int32_t eval_block_grid;  /* block bin (default 4) */
-    int32_t eval_large_grid;  /* large bin (default 1) */
+    int32_t eval_large_grid;  /* large bin (default 2) */
     int32_t eval_warp_grid;   /* warp bin (default 3) */
     int32_t eval_reg_grid;    /* register bins (default 8) */
     int32_t warp_max_degree;  /* default 128 */

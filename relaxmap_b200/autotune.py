@@ -42,7 +42,7 @@ KNOBS: dict[str, tuple[int, ...]] = {
     "large_max_degree": (2048, 3072, 4096),
     "hub_partition_links": (512, 1024, 2048),
 }
-DEFAULTS = {"eval_mid_grid": 8, "eval_block_grid": 4, "eval_large_grid": 1, "eval_warp_grid": 3, "eval_reg_grid": 8,
+DEFAULTS = {"eval_mid_grid": 8, "eval_block_grid": 4, "eval_large_grid": 2, "eval_warp_grid": 3, "eval_reg_grid": 8,
             "warp_max_degree": 128, "mid_max_degree": 512, "block_max_degree": 1024, "large_max_degree": 4096,
             "hub_partition_links": 1024}
 FORMAT = 1

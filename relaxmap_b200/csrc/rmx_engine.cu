@@ -739,7 +739,7 @@ void rmx_graph::ensure_hub_table(const Level &lv) {
     work.hub_coff = hub_arena.alloc<int64_t>(U + 1);
     work.hub_poff = hub_arena.alloc<int64_t>(U + 1);
     work.hub_loff = hub_arena.alloc<int64_t>(U + 1);
-    work.hub_own = hub_arena.alloc<fx_t>(2 * U);
+    work.hub_own = hub_arena.alloc<fx_t>(U);
     work.hub_nparts = hub_arena.alloc<int32_t>(U);
     work.hub_act = hub_arena.alloc<uint8_t>(U);
     work.hub_pcnt = hub_arena.alloc<unsigned long long>(P);

@@ -89,16 +89,16 @@ __device__ __forceinline__ double plogp_total(const UnitCtx &c, double dm) {
 }
 
 // Change of moving the unit into module with statistics st, given the unit's
-// aggregated out-/in-flow (fixed point, before the 1-tau factor) to it:
-// d_all - 2 d_exit + d_stay of Module.cpp:1109-1115 with the unit terms in K.
-// t = the module's cached {plogp(exit), plogp(exit + P)}.
-__device__ __forceinline__ double candidate_delta(const UnitCtx &c, const Stat4 &st, const double2 t, fx_t ofx,
-                                                  fx_t ifx) {
+// link flow to and from it (fixed point, out-links plus in-links, before the
+// 1-tau factor): d_all - 2 d_exit + d_stay of Module.cpp:1109-1115 with the
+// unit terms in K. The out- and in-flows (Module.cpp:1058, :1059) enter the
+// change only through their sum (the new exit, :1104), so the tables keep one
+// sum per module. t = the module's cached {plogp(exit), plogp(exit + P)}.
+__device__ __forceinline__ double candidate_delta(const UnitCtx &c, const Stat4 &st, const double2 t, fx_t sfx) {
     const double P = from_fx(st.P), TW = from_fx(st.TW), D = from_fx(st.D), OUT = from_fx(st.OUT);
     const double em = exit_flow(P, TW, D, OUT);
-    const double om = kBeta * from_fx(ofx) + c.cu * TW;                        // Module.cpp:1058
-    const double im = kBeta * from_fx(ifx) + (kAlpha * P + kBeta * D) * c.tu;  // Module.cpp:1059
-    const double nexm = em + c.eu - om - im;                                   // Module.cpp:1104
+    const double om_im = kBeta * from_fx(sfx) + c.cu * TW + (kAlpha * P + kBeta * D) * c.tu;  // :1058 + :1059
+    const double nexm = em + c.eu - om_im;                                                    // Module.cpp:1104
     // new total exit sumAllExitPr + (nexA - eA) + (nexm - em), Module.cpp:1106
     return plogp_total(c, nexm - em) + c.K - 2.0 * (plogp(nexm) - t.x) + (plogp(nexm + P + c.pu) - t.y);
 }
@@ -110,7 +110,7 @@ __device__ __forceinline__ double newmod_delta(const UnitCtx &c) {
 }
 
 __device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, const double2 tA, double sum_exit,
-                                            int32_t A, fx_t oA, fx_t iA) {
+                                            int32_t A, fx_t sA) {
     UnitCtx c;
     c.pu = from_fx(ua.P);
     c.tu = from_fx(ua.TW);
@@ -119,9 +119,10 @@ __device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, co
     c.cu = kAlpha * c.pu + kBeta * du;
     const double PA = from_fx(ma.P), TWA = from_fx(ma.TW), DA = from_fx(ma.D);
     c.eA = exit_flow(PA, TWA, DA, from_fx(ma.OUT));
-    const double outA = kBeta * from_fx(oA) + c.cu * (TWA - c.tu);                             // :1047
-    const double inA = kBeta * from_fx(iA) + (kAlpha * (PA - c.pu) + kBeta * (DA - du)) * c.tu;  // :1048
-    c.nexA = c.eA - c.eu + outA + inA;                                                          // :1084
+    // outFlow + inFlow to the old module (Module.cpp:1047, :1048), sA = their link flows' sum
+    const double outA_inA = kBeta * from_fx(sA) + c.cu * (TWA - c.tu) +
+                            (kAlpha * (PA - c.pu) + kBeta * (DA - du)) * c.tu;
+    c.nexA = c.eA - c.eu + outA_inA;  // :1084
     c.sum_exit = sum_exit;
     c.K = -plogp(sum_exit) - 2.0 * (plogp(c.nexA) - tA.x) + (plogp(c.nexA + (PA - c.pu)) - tA.y);
     c.S0 = sum_exit + c.nexA - c.eA;
@@ -252,7 +253,7 @@ constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
 #define RMX_LRG_CAP 8192
 #endif
 #ifndef RMX_LRG_MINB
-#define RMX_LRG_MINB 1
+#define RMX_LRG_MINB 2
 #endif
 constexpr int kLrgT = 512, kLrgCap = RMX_LRG_CAP, kLrgMaxDeg = kLrgCap / 2;
 
@@ -285,17 +286,15 @@ struct GroupShared {  // reductions across the warps of a block group
 };
 
 // Inserts the unit's links j = first, first + NT, ... below end (out-links
-// first, then in-links; dout of them out) into the table keys/vo/vi keyed by
-// the neighbour's module, adding each link's fixed-point flow; slot s's key is
-// keys[s * KS], its flows vo[s * VS], vi[s * VS]. RMX_EVAL_ILP links at a time
-// have their neighbour ids, flows and then neighbour modules loaded before any
-// is inserted, so that many gathers are in flight per thread. Capacity >= 2 x
-// the unit's links, so probing always finds a slot. With occ, every slot
-// taken by a new key is appended to the list occ (count *occ_n).
-template <int NT, int KS = 1, int VS = 1>
+// first, then in-links; dout of them out) into the table keys/vals keyed by
+// the neighbour's module, adding each link's fixed-point flow to the slot's
+// sum. RMX_EVAL_ILP links at a time have their neighbour ids, flows and then
+// neighbour modules loaded before any is inserted, so that many gathers are in
+// flight per thread. Capacity >= 2 x the unit's links, so probing always
+// finds a slot.
+template <int NT>
 __device__ __forceinline__ void insert_links(const EvalArgs &a, int64_t ob, int64_t ib, int64_t dout, int64_t first,
-                                             int64_t d, int32_t *keys, fx_t *vo, fx_t *vi, int mask,
-                                             int32_t *occ = nullptr, int32_t *occ_n = nullptr) {
+                                             int64_t d, int32_t *keys, fx_t *vals, int mask) {
     for (int64_t j0 = first; j0 < d; j0 += (int64_t)RMX_EVAL_ILP * NT) {
         int32_t key[RMX_EVAL_ILP];
         fx_t q[RMX_EVAL_ILP];
@@ -321,7 +320,7 @@ __device__ __forceinline__ void insert_links(const EvalArgs &a, int64_t ob, int6
         for (int k = 0; k < RMX_EVAL_ILP; k++)
             if (key[k] >= 0) {
                 slot[k] = tab_slot(key[k], mask);
-                prev[k] = atomicCAS(keys + (int64_t)slot[k] * KS, kEmpty, key[k]);
+                prev[k] = atomicCAS(keys + slot[k], kEmpty, key[k]);
             }
 #pragma unroll
         for (int k = 0; k < RMX_EVAL_ILP; k++)
@@ -329,34 +328,18 @@ __device__ __forceinline__ void insert_links(const EvalArgs &a, int64_t ob, int6
                 // capacity >= 2 x the unit's links: a free slot exists, probing stays below mask steps
                 for (int probe = 0; prev[k] != kEmpty && prev[k] != key[k] && probe < mask; probe++) {
                     slot[k] = (slot[k] + 1) & mask;
-                    prev[k] = atomicCAS(keys + (int64_t)slot[k] * KS, kEmpty, key[k]);
+                    prev[k] = atomicCAS(keys + slot[k], kEmpty, key[k]);
                 }
-                atomic_add_fx((j0 + (int64_t)k * NT < dout ? vo : vi) + (int64_t)slot[k] * VS, q[k]);
+                atomic_add_fx(vals + slot[k], q[k]);
             }
-        if (occ) {  // list the slots this warp took: one counter update per warp, not per slot
-            const unsigned m = __activemask();
-            const int lane = threadIdx.x & 31;
-#pragma unroll
-            for (int k = 0; k < RMX_EVAL_ILP; k++) {
-                const bool fresh = key[k] >= 0 && prev[k] == kEmpty;
-                const unsigned bal = __ballot_sync(m, fresh);
-                if (!bal) continue;
-                const int leader = __ffs(bal) - 1;
-                int base = 0;
-                if (lane == leader) base = atomicAdd(occ_n, __popc(bal));
-                base = __shfl_sync(m, base, leader);
-                if (fresh) occ[base + __popc(bal & ((1u << lane) - 1u))] = slot[k];
-            }
-        }
     }
 }
 
 // One unit evaluated by a group of NT threads (a warp or a block); r = rank.
-// The candidate list overwrites the table in place (ck == keys).
+// The candidate list overwrites the table in place.
 template <int NT>
-__device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, const int r, int32_t *keys, fx_t *vo,
-                                          fx_t *vi, int32_t *ck, fx_t *co, fx_t *ci, GroupShared<NT> *sh,
-                                          unsigned long long &seen, unsigned long long &cands) {
+__device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, const int r, int32_t *keys, fx_t *vals,
+                                          GroupShared<NT> *sh, unsigned long long &seen, unsigned long long &cands) {
     const int lane = r & 31;
     const unsigned lt = (1u << lane) - 1u;
     const int64_t ob = a.out_off[u], ib = a.in_off[u];
@@ -367,12 +350,12 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
     // The table is empty on entry: cleared once when the kernel starts (shared
     // tables) or when it is allocated (global slices), and every unit leaves
     // it empty again (below), so no clearing pass runs per unit.
-    insert_links<NT>(a, ob, ib, dout, r, d, keys, vo, vi, mask);
+    insert_links<NT>(a, ob, ib, dout, r, d, keys, vals, mask);
     gsync<NT>();
     const int32_t A = a.mod[u];
     const int sA = tab_find(keys, mask, A);
-    const fx_t oA = sA >= 0 ? vo[sA] : 0, iA = sA >= 0 ? vi[sA] : 0;
-    const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
+    const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A,
+                               sA >= 0 ? vals[sA] : 0);
     if (NT > 32) __syncthreads();  // every lookup is done before slots are overwritten
     // Each warp compacts its own contiguous slice of the table in place (the
     // dense position never passes the slot being read) and evaluates it. A
@@ -383,38 +366,34 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
     for (int64_t base = lo; base < hi; base += 32) {
         const int64_t s = base + lane;
         int32_t k = kEmpty;
-        fx_t o = 0, i2 = 0;
+        fx_t v = 0;
         if (s < hi) {
             k = keys[s];
-            o = vo[s];
-            i2 = vi[s];
+            v = vals[s];
         }
         const bool occ = k != kEmpty && k != A;
         const unsigned bal = __ballot_sync(kFull, occ);
         __syncwarp();
         if (occ) {
             const int64_t p = lo + nc + __popc(bal & lt);
-            ck[p] = k;
-            co[p] = o;
-            ci[p] = i2;
+            keys[p] = k;
+            vals[p] = v;
         }
         nc += __popc(bal);
         if (k != kEmpty && s >= lo + nc) {  // not overwritten by the dense prefix
             keys[s] = kEmpty;
-            vo[s] = 0;
-            vi[s] = 0;
+            vals[s] = 0;
         }
     }
     __syncwarp();
     double best = 0.0;
     int32_t bm = INT_MAX;
     for (int q = lane; q < nc; q += 32) {
-        const int32_t m = ck[lo + q];
-        const fx_t o = co[lo + q], i2 = ci[lo + q];
-        ck[lo + q] = kEmpty;
-        co[lo + q] = 0;
-        ci[lo + q] = 0;
-        const double dl = candidate_delta(c, a.mstat[m], a.mterm[m], o, i2);
+        const int32_t m = keys[lo + q];
+        const fx_t v = vals[lo + q];
+        keys[lo + q] = kEmpty;
+        vals[lo + q] = 0;
+        const double dl = candidate_delta(c, a.mstat[m], a.mterm[m], v);
         if (better(dl, m, best, bm)) {
             best = dl;
             bm = m;
@@ -468,7 +447,7 @@ __device__ __forceinline__ void eval_unit_reg(const EvalArgs &a, const int32_t u
                                               const unsigned gmask, unsigned long long &seen,
                                               unsigned long long &cands) {
     int32_t key = INT_MAX, nbr = -1;
-    fx_t vo = 0, vi = 0;
+    fx_t v = 0;
     int64_t d = 0;
     int32_t A = -1;
     if (valid) {
@@ -481,26 +460,21 @@ __device__ __forceinline__ void eval_unit_reg(const EvalArgs &a, const int32_t u
             const int64_t e = isout ? ob + gl : ib + (gl - dout);
             nbr = isout ? a.out_dst[e] : a.in_src[e];
             key = a.mod[nbr];
-            if (isout)
-                vo = a.out_fx[e];
-            else
-                vi = a.in_fx[e];
+            v = isout ? a.out_fx[e] : a.in_fx[e];
         }
     }
-    // bitonic sort of (key, vo, vi) by key within the group
+    // bitonic sort of (key, flow) by key within the group
 #pragma unroll
     for (int k = 2; k <= W; k <<= 1) {
 #pragma unroll
         for (int j = k >> 1; j > 0; j >>= 1) {
             const int32_t pk = __shfl_xor_sync(kFull, key, j, W);
-            const fx_t po = __shfl_xor_sync(kFull, vo, j, W);
-            const fx_t pi = __shfl_xor_sync(kFull, vi, j, W);
+            const fx_t pv = __shfl_xor_sync(kFull, v, j, W);
             const bool up = (gl & k) == 0, lower = (gl & j) == 0;
             const bool take = lower == up ? pk < key : pk > key;
             if (take) {
                 key = pk;
-                vo = po;
-                vi = pi;
+                v = pv;
             }
         }
     }
@@ -508,27 +482,23 @@ __device__ __forceinline__ void eval_unit_reg(const EvalArgs &a, const int32_t u
 #pragma unroll
     for (int off = 1; off < W; off <<= 1) {
         const int32_t k2 = __shfl_up_sync(kFull, key, off, W);
-        const fx_t o2 = __shfl_up_sync(kFull, vo, off, W);
-        const fx_t i2 = __shfl_up_sync(kFull, vi, off, W);
-        if (gl >= off && k2 == key) {
-            vo += o2;
-            vi += i2;
-        }
+        const fx_t v2 = __shfl_up_sync(kFull, v, off, W);
+        if (gl >= off && k2 == key) v += v2;
     }
     const int32_t nk = __shfl_down_sync(kFull, key, 1, W);
     const bool tail = key != INT_MAX && (gl == W - 1 || nk != key);
-    // flows to the unit's own module from the lane ending A's run
+    // the flow to and from the unit's own module from the lane ending A's run
     const unsigned own = __ballot_sync(kFull, tail && key == A) & gmask;
     const int src = own ? __ffs(own) - 1 : (threadIdx.x & 31);
-    fx_t oA = __shfl_sync(kFull, vo, src), iA = __shfl_sync(kFull, vi, src);
-    if (!own) oA = iA = 0;
+    fx_t sA = __shfl_sync(kFull, v, src);
+    if (!own) sA = 0;
     double best = 0.0;
     int32_t bm = INT_MAX;
     UnitCtx c;
     if (valid) {
-        c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, oA, iA);
+        c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, sA);
         if (tail && key != A) {
-            best = candidate_delta(c, a.mstat[key], a.mterm[key], vo, vi);
+            best = candidate_delta(c, a.mstat[key], a.mterm[key], v);
             bm = key;
         }
     }
@@ -611,16 +581,14 @@ __device__ __forceinline__ void flush_stats_split(const EvalArgs &a, unsigned lo
 
 __global__ void __launch_bounds__(kEvalWarps * 32, RMX_WARP_MINB) k_eval_warp(EvalArgs a) {
     __shared__ int32_t skey[kEvalWarps][kWarpCap];
-    __shared__ fx_t sout[kEvalWarps][kWarpCap];
-    __shared__ fx_t sin_[kEvalWarps][kWarpCap];
+    __shared__ fx_t sval[kEvalWarps][kWarpCap];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t beg = a.range[0], end = a.range[1];
     const int64_t gw = (int64_t)blockIdx.x * kEvalWarps + w, nw = (int64_t)gridDim.x * kEvalWarps;
     unsigned long long seen = 0, units = 0, cands = 0;
     for (int s = lane; s < kWarpCap; s += 32) {  // every unit leaves its table empty again
         skey[w][s] = kEmpty;
-        sout[w][s] = 0;
-        sin_[w][s] = 0;
+        sval[w][s] = 0;
     }
     __syncwarp();
     for (int64_t i = beg + gw; i < end; i += nw) {
@@ -629,7 +597,7 @@ __global__ void __launch_bounds__(kEvalWarps * 32, RMX_WARP_MINB) k_eval_warp(Ev
             if (lane == 0) a.prop[u] = -1;
             continue;
         }
-        eval_unit<32>(a, u, lane, skey[w], sout[w], sin_[w], skey[w], sout[w], sin_[w], nullptr, seen, cands);
+        eval_unit<32>(a, u, lane, skey[w], sval[w], nullptr, seen, cands);
         units++;
     }
     if (lane == 0) flush_stats(a, seen, units, cands);
@@ -642,13 +610,11 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? RMX_LRG_MINB : (NT == 128 ? 8 
     k_eval_block(EvalArgs a) {
     extern __shared__ __align__(16) unsigned char dsm[];
     __shared__ GroupShared<NT> sh;
-    fx_t *vo = reinterpret_cast<fx_t *>(dsm);
-    fx_t *vi = vo + CAP;
-    int32_t *keys = reinterpret_cast<int32_t *>(vi + CAP);
+    fx_t *vals = reinterpret_cast<fx_t *>(dsm);
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + CAP);
     for (int s = threadIdx.x; s < CAP; s += NT) {  // every unit leaves its table empty again
         keys[s] = kEmpty;
-        vo[s] = 0;
-        vi[s] = 0;
+        vals[s] = 0;
     }
     __syncthreads();
     const int64_t beg = a.range[0], end = a.range[1];
@@ -659,7 +625,7 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? RMX_LRG_MINB : (NT == 128 ? 8 
             if (threadIdx.x == 0) a.prop[u] = -1;
             continue;
         }
-        eval_unit<NT>(a, u, threadIdx.x, keys, vo, vi, keys, vo, vi, &sh, seen, cands);
+        eval_unit<NT>(a, u, threadIdx.x, keys, vals, &sh, seen, cands);
         units++;
     }
     // every warp found its own share of the candidates; thread 0 alone counted the links
@@ -675,10 +641,10 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? RMX_LRG_MINB : (NT == 128 ? 8 
 //   plan     one block lays out, by prefix sums, every hub unit's link chunks
 //            (kHubCh links), partitions and bucket region;
 //   count    blocks take link chunks: each link's partition is counted, and the
-//            flows to the unit's own module are summed;
+//            flow to and from the unit's own module is summed;
 //   offsets  one block turns the partition counts into bucket offsets;
-//   scatter  blocks take link chunks again and write (module, direction, flow)
-//            into their partition's bucket;
+//   scatter  blocks take link chunks again and write (module, flow) into
+//            their partition's bucket;
 //   evaluate a block per partition aggregates its bucket in a shared table,
 //            evaluates the candidates and keeps the partition's best change;
 //   finish   a warp per unit reduces its partitions' bests and decides;
@@ -699,18 +665,18 @@ constexpr int kPartLinks = 1024; // mean links per partition (default of the run
 #endif
 constexpr int kPartCap = RMX_HUB_CAP;
 constexpr int kMaxParts = 1 << 20;
-constexpr size_t kHubEvalSmem = (size_t)kPartCap * (2 * sizeof(fx_t) + sizeof(int32_t));
+constexpr size_t kHubEvalSmem = (size_t)kPartCap * (sizeof(fx_t) + sizeof(int32_t));
 
 struct HubPlan {
     int64_t *coff, *poff, *loff;   // per unit (+1): first chunk, first partition, first bucket element
     int32_t *nparts;               // per unit: partitions
-    fx_t *own;                     // 2 per unit: out / in flow to the unit's own module
+    fx_t *own;                     // per unit: the link flow to and from the unit's own module
     uint8_t *act;                  // per unit: found a move below the threshold
     unsigned long long *pcnt;      // per partition: links (counted), then the fill position
     int64_t *pstart;               // per partition (+1): first bucket element
     double *best;                  // per partition: best change found
     int32_t *bmod;                 // per partition: its module
-    int32_t *bkey;                 // bucket elements: module | direction (bit 31 set: in-link)
+    int32_t *bkey;                 // bucket elements: module
     fx_t *bfx;                     //   and flow
     int32_t *cunit, *punit;        // unit (index in the sub-batch) of every chunk item and partition
     int64_t *tot;                  // [0] chunks, [1] partitions, [2] units, [3] over capacity, [4] links
@@ -798,7 +764,7 @@ __global__ void __launch_bounds__(1024) k_hub_plan(EvalArgs a, HubPlan p) {
             p.poff[j] = r1 + e1;
             p.loff[j] = r2 + e2;
             p.nparts[j] = (int32_t)np;
-            p.own[2 * j] = p.own[2 * j + 1] = 0;
+            p.own[j] = 0;
         }
         r0 += t0;
         r1 += t1;
@@ -821,10 +787,10 @@ __global__ void __launch_bounds__(1024) k_hub_plan(EvalArgs a, HubPlan p) {
         for (int64_t q = threadIdx.x; q < r1; q += 1024) p.pcnt[q] = 0;
 }
 
-// Link l of unit u (out-links first): neighbour module, direction, flow.
+// Link l of unit u (out-links first): neighbour module and flow.
 __device__ __forceinline__ void hub_link(const EvalArgs &a, int64_t ob, int64_t ib, int64_t dout, int64_t l,
-                                         int32_t &key, bool &in, fx_t &q) {
-    in = l >= dout;
+                                         int32_t &key, fx_t &q) {
+    const bool in = l >= dout;
     const int64_t e = in ? ib + (l - dout) : ob + l;
     key = __ldg(a.mod + __ldg(in ? a.in_src + e : a.out_dst + e));
     q = __ldg(in ? a.in_fx + e : a.out_fx + e);
@@ -832,7 +798,7 @@ __device__ __forceinline__ void hub_link(const EvalArgs &a, int64_t ob, int64_t 
 
 // Count (scatter = false) or place (scatter = true) the links of the chunks.
 // Links to the unit's own module are only summed (into own); the others are
-// combined per warp step by (module, direction) with __match_any_sync, so a
+// combined per warp step by module with __match_any_sync, so a
 // module that many of a hub's links reach takes one bucket element per warp
 // step instead of one per link (integer sums: exact in any order). Both
 // passes form the same groups (the same lanes read the same links), so the
@@ -858,34 +824,25 @@ __global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
             if (c0 == 0)
                 for (int q = threadIdx.x; q < np; q += kHubPT) p.punit[p.poff[j] + q] = j;
         }
-        fx_t oA = 0, iA = 0;
+        fx_t sA = 0;
         for (int64_t b0 = c0; b0 < c1; b0 += kHubPT * ILP) {  // uniform over the block
             int32_t keys[ILP];
-            bool ins[ILP];
             fx_t qs[ILP];
 #pragma unroll
             for (int k = 0; k < ILP; k++) {
                 const int64_t l = b0 + k * kHubPT + threadIdx.x;
                 keys[k] = A;  // lanes past the chunk: flow 0 to the own module
-                ins[k] = false;
                 qs[k] = 0;
-                if (l < c1) hub_link(a, ob, ib, dout, l, keys[k], ins[k], qs[k]);
+                if (l < c1) hub_link(a, ob, ib, dout, l, keys[k], qs[k]);
             }
 #pragma unroll
             for (int k = 0; k < ILP; k++) {
                 const int32_t key = keys[k];
-                const bool in = ins[k];
                 const fx_t q = qs[k];
-                if (key == A) {
-                    if (in)
-                        iA += q;
-                    else
-                        oA += q;
-                }
+                if (key == A) sA += q;
                 const bool valid = key != A;
-                const uint32_t kd = in ? ((uint32_t)key | 0x80000000u) : (uint32_t)key;
-                const unsigned kpeers = __match_any_sync(kFull, valid ? (unsigned long long)kd : ~0ull);
-                const bool head = valid && lane == __ffs(kpeers) - 1;  // one lane per (module, direction)
+                const unsigned kpeers = __match_any_sync(kFull, valid ? key : -1);
+                const bool head = valid && lane == __ffs(kpeers) - 1;  // one lane per module
                 const int32_t part = head ? (int32_t)(part_hash(key) % (uint32_t)np) : -1;
                 const unsigned peers = __match_any_sync(kFull, part);
                 const int leader = __ffs(peers) - 1;
@@ -904,7 +861,7 @@ __global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
                     base = __shfl_sync(kFull, base, leader);
                     if (head) {
                         const int64_t pos = p.pstart[pidx] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
-                        p.bkey[pos] = (int32_t)kd;
+                        p.bkey[pos] = key;
                         p.bfx[pos] = sum;
                     }
                     __syncwarp();
@@ -913,14 +870,8 @@ __global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
         }
         if (!SCATTER) {
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                oA += __shfl_xor_sync(kFull, oA, o);
-                iA += __shfl_xor_sync(kFull, iA, o);
-            }
-            if (lane == 0) {
-                if (oA) atomic_add_fx(p.own + 2 * j, oA);
-                if (iA) atomic_add_fx(p.own + 2 * j + 1, iA);
-            }
+            for (int o = 16; o > 0; o >>= 1) sA += __shfl_xor_sync(kFull, sA, o);
+            if (lane == 0 && sA) atomic_add_fx(p.own + j, sA);
         }
     }
 }
@@ -952,9 +903,8 @@ __global__ void __launch_bounds__(1024) k_hub_offsets(HubPlan p) {
 // overfills (at R = 2^31 a round holds at most two keys).
 __global__ void __launch_bounds__(kHubPT, RMX_HUB_MINB) k_hub_eval(EvalArgs a, HubPlan p) {
     extern __shared__ __align__(16) unsigned char hub_smem[];  // kHubEvalSmem bytes
-    fx_t *vo = reinterpret_cast<fx_t *>(hub_smem);
-    fx_t *vi = vo + kPartCap;
-    int32_t *keys = reinterpret_cast<int32_t *>(vi + kPartCap);
+    fx_t *vals = reinterpret_cast<fx_t *>(hub_smem);
+    int32_t *keys = reinterpret_cast<int32_t *>(vals + kPartCap);
     __shared__ double sb[kHubPT / 32];
     __shared__ int32_t sm[kHubPT / 32];
     __shared__ int16_t taken[kPartCap / 2 + kHubPT];  // slots taken in this round, in the order taken
@@ -966,15 +916,14 @@ __global__ void __launch_bounds__(kHubPT, RMX_HUB_MINB) k_hub_eval(EvalArgs a, H
     unsigned long long cands = 0;
     for (int s = threadIdx.x; s < kPartCap; s += kHubPT) {
         keys[s] = kEmpty;
-        vo[s] = vi[s] = 0;
+        vals[s] = 0;
     }
     for (int64_t pidx = blockIdx.x; pidx < total; pidx += gridDim.x) {
         const int32_t j = p.punit[pidx];
         const int32_t u = a.list[h0 + j];
         const int64_t b0 = p.pstart[pidx], b1 = p.pstart[pidx + 1];
         const int32_t A = a.mod[u];
-        const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, p.own[2 * j],
-                                   p.own[2 * j + 1]);
+        const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, p.own[j]);
         double best = 0.0;
         int32_t bm = INT_MAX;
         for (uint32_t R = 1;; R <<= 1) {  // R rounds; more only when a round overfills the table
@@ -987,8 +936,7 @@ __global__ void __launch_bounds__(kHubPT, RMX_HUB_MINB) k_hub_eval(EvalArgs a, H
                 if (threadIdx.x == 0) nfresh = 0;
                 __syncthreads();
                 for (int64_t e = b0 + threadIdx.x; e < b1; e += kHubPT) {
-                    const int32_t kd = p.bkey[e];
-                    const int32_t key = kd & 0x7fffffff;
+                    const int32_t key = p.bkey[e];
                     if (R > 1 && (mix32((uint32_t)key ^ 0x5bd1e995u) & (R - 1)) != r) continue;
                     if (*(volatile int *)&nfresh > kPartCap / 2) break;
                     int sl = tab_slot(key, mask);
@@ -999,7 +947,7 @@ __global__ void __launch_bounds__(kHubPT, RMX_HUB_MINB) k_hub_eval(EvalArgs a, H
                     }
                     if (prev != kEmpty && prev != key) continue;  // unreachable: the table is never full
                     if (prev == kEmpty) taken[atomicAdd(&nfresh, 1)] = (int16_t)sl;
-                    atomic_add_fx(kd < 0 ? vi + sl : vo + sl, p.bfx[e]);
+                    atomic_add_fx(vals + sl, p.bfx[e]);
                 }
                 __syncthreads();
                 // at most kPartCap / 2 + kHubPT slots were taken (every thread checks the
@@ -1012,14 +960,14 @@ __global__ void __launch_bounds__(kHubPT, RMX_HUB_MINB) k_hub_eval(EvalArgs a, H
                     const int32_t k = keys[s];
                     if (!overfull && k != A) {
                         rc++;
-                        const double dl = candidate_delta(c, a.mstat[k], a.mterm[k], vo[s], vi[s]);
+                        const double dl = candidate_delta(c, a.mstat[k], a.mterm[k], vals[s]);
                         if (better(dl, k, rbest, rbm)) {
                             rbest = dl;
                             rbm = k;
                         }
                     }
                     keys[s] = kEmpty;
-                    vo[s] = vi[s] = 0;
+                    vals[s] = 0;
                 }
             }
             __syncthreads();
@@ -1096,7 +1044,7 @@ __global__ void k_hub_finish(EvalArgs a, HubPlan p) {
         if (lane == 0) {
             const int32_t A = a.mod[u];
             const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A,
-                                       p.own[2 * j], p.own[2 * j + 1]);
+                                       p.own[j]);
             p.act[j] = (uint8_t)finish_unit(a, u, c, best, bm);
             seen += unit_links(a, u);
             units++;
@@ -1585,9 +1533,9 @@ int eval_tuning_generation() {
 }
 int64_t block_bin_max_degree() { return eval_tuning().large_max; }
 
-constexpr size_t kBlkSmem = (size_t)kBlkCap * (2 * sizeof(fx_t) + sizeof(int32_t));
-constexpr size_t kMidSmem = (size_t)kMidCap * (2 * sizeof(fx_t) + sizeof(int32_t));
-constexpr size_t kLrgSmem = (size_t)kLrgCap * (2 * sizeof(fx_t) + sizeof(int32_t));
+constexpr size_t kBlkSmem = (size_t)kBlkCap * (sizeof(fx_t) + sizeof(int32_t));
+constexpr size_t kMidSmem = (size_t)kMidCap * (sizeof(fx_t) + sizeof(int32_t));
+constexpr size_t kLrgSmem = (size_t)kLrgCap * (sizeof(fx_t) + sizeof(int32_t));
 
 // Blocks for `items` work items at per_block items a block, at most max_grid.
 static unsigned fit_grid(int64_t items, int64_t per_block, int64_t max_grid) {
