@@ -65,7 +65,7 @@ def test_tune_times_each_setting_once():
     """After a knob moves, coordinate descent meets earlier settings again
     (the old value of that knob, or a second pass): they are not re-timed."""
     from relaxmap_b200.autotune import DEFAULTS, tune
-    opt = {"eval_mid_grid": 4, "eval_block_grid": 4, "eval_large_grid": 1, "eval_warp_grid": 2, "eval_reg_grid": 8}
+    opt = {"eval_mid_grid": 4, "eval_warp_grid": 2}  # the other knobs keep their defaults
     knobs = {"eval_mid_grid": (4, 8), "eval_warp_grid": (2, 3)}
     for passes, distinct in ((1, 3), (3, 4)):  # the second pass adds (mid 8, warp 2) only
         calls = []
