@@ -173,11 +173,16 @@ def main(argv=None) -> int:
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--passes", type=int, default=2)
+    ap.add_argument("--rmat", type=int, default=None,
+                    help="tune on a synthetic R-MAT graph of this scale (edge factor 16, seed 42) instead")
     ap.add_argument("--out", required=True)
     a = ap.parse_args(argv)
     from . import Graph, synth
     if a.graph:
         G = Graph.from_file(a.graph)
+    elif a.rmat is not None:
+        g = synth.rmat_device(a.rmat, 16, seed=42) if a.rmat >= 22 else synth.rmat(a.rmat, 16, seed=42)
+        G = Graph.from_edges(g.src, g.dst, g.w, n=g.n)
     else:
         g = synth.config_mid(seed=42, n=a.nodes)
         G = Graph.from_edges(g.src, g.dst, g.w, n=g.n)
