@@ -284,21 +284,36 @@ struct PowSplit {
     int64_t heavy_deg = INT64_MAX;
 };
 
+// The flow vector's gathered copy: on graphs whose flow vector is larger
+// than L2 the pull gathers from a copy holding only the nodes that have
+// out-links (rank[i] >= 0: node i's place in it; gsrc: in_src renumbered to
+// those places), small enough to stay in L2. Values are the same doubles,
+// so the sums are unchanged.
+struct PowGather {
+    const int32_t *gsrc = nullptr;  // nullptr: gather from x itself
+    const int32_t *rank = nullptr;
+    double *xc = nullptr;
+};
+
 template <int VEC>
 __global__ void __launch_bounds__(kPowT, RMX_POW_MINB) k_power(const int64_t *__restrict__ in_off, const int32_t *__restrict__ in_src,
                                                  const double *__restrict__ in_w, const double *__restrict__ tw,
                                                  const uint8_t *__restrict__ dang, int32_t n, double *x, double *y,
-                                                 double *parts, int *iters_out, double alpha, PowSplit sp) {
+                                                 double *parts, int *iters_out, double alpha, PowSplit sp,
+                                                 PowGather pg) {
     cg::grid_group grid = cg::this_grid();
     __shared__ double sh[32];
     const int nb = gridDim.x;
     double *Sp = parts, *Dp = parts + nb, *Ep = parts + 2 * nb;
     const int64_t gtid = (int64_t)blockIdx.x * kPowT + threadIdx.x, gthreads = (int64_t)nb * kPowT;
 
+    const double *xg = pg.gsrc ? pg.xc : x;        // the vector the pull gathers from
+    const int32_t *gs = pg.gsrc ? pg.gsrc : in_src;  // and the links' places in it
     double dl = 0.0;
     const double x0 = 1.0 / n;
     for (int64_t i = gtid; i < n; i += gthreads) {
         x[i] = x0;
+        if (pg.gsrc && pg.rank[i] >= 0) pg.xc[pg.rank[i]] = x0;
         if (dang[i]) dl += x0;
     }
     dl = block_sum<kPowT>(dl, sh);
@@ -322,7 +337,7 @@ __global__ void __launch_bounds__(kPowT, RMX_POW_MINB) k_power(const int64_t *__
                 const int64_t b = in_off[r], e = in_off[r + 1];
                 mine = e - b <= sp.heavy_deg;
                 if (mine)
-                    for (int64_t k = b + lv; k < e; k += VEC) acc += beta * in_w[k] * __ldcg(x + in_src[k]);
+                    for (int64_t k = b + lv; k < e; k += VEC) acc += beta * in_w[k] * __ldcg(xg + gs[k]);
             }
 #pragma unroll
             for (int o = VEC / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
@@ -336,7 +351,7 @@ __global__ void __launch_bounds__(kPowT, RMX_POW_MINB) k_power(const int64_t *__
             for (int64_t c = gwarp; c < sp.n_chunks; c += nwarps) {
                 double acc = 0.0;
                 for (int64_t k = sp.chunk_beg[c] + lane; k < sp.chunk_end[c]; k += 32)
-                    acc += beta * in_w[k] * __ldcg(x + in_src[k]);
+                    acc += beta * in_w[k] * __ldcg(xg + gs[k]);
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
                 if (lane == 0) sp.cpart[c] = acc;
@@ -365,6 +380,7 @@ __global__ void __launch_bounds__(kPowT, RMX_POW_MINB) k_power(const int64_t *__
             const double xn = __ldcg(y + i) / S;
             el += fabs(xn - x[i]);
             x[i] = xn;
+            if (pg.gsrc && pg.rank[i] >= 0) pg.xc[pg.rank[i]] = xn;
             if (dang[i]) dl += xn;
         }
         el = block_sum<kPowT>(el, sh);
@@ -440,6 +456,57 @@ static PowSplit heavy_split(int32_t n, const int64_t *in_off, int64_t heavy_deg,
     return sp;
 }
 
+__global__ void k_src_flags(int64_t m, const int32_t *in_src, uint32_t *flag) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+        flag[in_src[k]] = 1u;  // every writer stores the same value
+}
+
+__global__ void k_src_rank(int32_t n, const uint32_t *flag, const uint32_t *pos, int32_t *rank) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        rank[i] = flag[i] ? (int32_t)pos[i] : -1;
+}
+
+__global__ void k_src_remap(int64_t m, const int32_t *in_src, const int32_t *rank, int32_t *gsrc) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x)
+        gsrc[k] = rank[in_src[k]];
+}
+
+// The gathered copy (PowGather) where the flow vector is larger than a
+// quarter of L2 and at most three quarters of the nodes have out-links;
+// otherwise none. In arena memory (released with the caller's mark).
+static PowGather gather_copy(int32_t n, const int64_t *in_off, const int32_t *in_src, Arena &ar, cudaStream_t s) {
+    PowGather pg;
+    constexpr int64_t kMinNodes = (int64_t)32 << 20 >> 3;  // 32 MB of doubles
+    if ((int64_t)n < kMinNodes) return pg;
+    int64_t m = 0;
+    RMX_CUDA(cudaMemcpyAsync(&m, in_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    if (m <= 0) return pg;
+    const size_t mk = ar.mark();
+    uint32_t *flag = ar.alloc<uint32_t>(n), *pos = ar.alloc<uint32_t>(n + 1);
+    RMX_CUDA(cudaMemsetAsync(flag, 0, sizeof(uint32_t) * n, s));
+    k_src_flags<<<blocks_for(m, 256, num_sms() * 32), 256, 0, s>>>(m, in_src, flag);
+    RMX_LAUNCHED();
+    scan_exclusive(flag, pos, n, pos + n, ar, s);
+    uint32_t cnt = 0;
+    RMX_CUDA(cudaMemcpyAsync(&cnt, pos + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    RMX_CUDA(cudaStreamSynchronize(s));
+    if ((int64_t)cnt * 4 > (int64_t)n * 3) {
+        ar.release(mk);
+        return pg;
+    }
+    int32_t *rank = ar.alloc<int32_t>(n), *gsrc = ar.alloc<int32_t>(m);
+    double *xc = ar.alloc<double>(std::max<uint32_t>(cnt, 1));
+    k_src_rank<<<blocks_for(n, 256, num_sms() * 32), 256, 0, s>>>(n, flag, pos, rank);
+    RMX_LAUNCHED();
+    k_src_remap<<<blocks_for(m, 256, num_sms() * 32), 256, 0, s>>>(m, in_src, rank, gsrc);
+    RMX_LAUNCHED();
+    pg.gsrc = gsrc;
+    pg.rank = rank;
+    pg.xc = xc;
+    return pg;
+}
+
 template <int VEC>
 static int launch_power(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
                         const uint8_t *dangling, double *p, Arena &ar, cudaStream_t s, double alpha) {
@@ -455,8 +522,10 @@ static int launch_power(int32_t n, const int64_t *in_off, const int32_t *in_src,
     double *parts = ar.alloc<double>(3 * nb);
     int *iters = ar.alloc<int>(1);
     PowSplit sp = heavy_split(n, in_off, 64 * VEC, ar, s);
+    PowGather pg = gather_copy(n, in_off, in_src, ar, s);
     void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w,  (void *)&tw,    (void *)&dangling, (void *)&n,
-                    (void *)&p,      (void *)&y,      (void *)&parts, (void *)&iters, (void *)&alpha,    (void *)&sp};
+                    (void *)&p,      (void *)&y,      (void *)&parts, (void *)&iters, (void *)&alpha,    (void *)&sp,
+                    (void *)&pg};
     RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));
     RMX_LAUNCHED();
     int h = 0;
@@ -483,10 +552,12 @@ static void launch_power_into(int32_t n, const int64_t *in_off, const int32_t *i
     double alpha = kAlpha;
     // No chunked rows: in-degree hubs are pulled in one pass by their own
     // lanes (nothing beyond the caller's scratch), so on graphs with such
-    // hubs the sums round differently from power_iteration's.
+    // hubs the sums round differently from power_iteration's. No gathered copy.
     PowSplit sp;
+    PowGather pg;
     void *args[] = {(void *)&in_off, (void *)&in_src, (void *)&in_w,  (void *)&tw,    (void *)&dangling, (void *)&n,
-                    (void *)&p,      (void *)&y,      (void *)&parts, (void *)&iters, (void *)&alpha,    (void *)&sp};
+                    (void *)&p,      (void *)&y,      (void *)&parts, (void *)&iters, (void *)&alpha,    (void *)&sp,
+                    (void *)&pg};
     RMX_CUDA(cudaLaunchCooperativeKernel((void *)k_power<VEC>, dim3(nb), dim3(kPowT), args, 0, s));
     RMX_LAUNCHED();
 }

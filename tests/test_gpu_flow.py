@@ -115,6 +115,27 @@ def test_flow_with_in_degree_hubs(built_lib, oracle_mod):
     assert np.abs(got["p"] - st["p"]).sum() / np.abs(st["p"]).sum() <= 1e-12
 
 
+def test_flow_gathered_copy(built_lib, oracle_mod):
+    """A flow vector above 32 MB (2^22 nodes) of which half the nodes have no
+    out-link: the pull gathers from the compact copy of the out-linked nodes'
+    flows. The flow, the iteration count and the initial code length match the
+    oracle's one-thread steady state on the library's own prepared links."""
+    from relaxmap_b200 import Graph
+    O = oracle_mod
+    n, m = 1 << 22, 8_000_000
+    rng = np.random.default_rng(21)
+    src = rng.integers(0, n // 2, m)
+    dst = rng.integers(0, n, m)
+    with Graph.from_edges(src, dst, None, n=n) as G:
+        off, dst_k, w, tw = G.links()
+        got = G.initiate()
+    st = O.initiate(O.Prepared(n, off, dst_k, w, tw))
+    assert got["iters"] == st["iters"]
+    assert rel_l1(got["p"], st["p"]) <= 1e-12
+    assert rel_l1(got["f"], st["f"]) <= 1e-12
+    assert abs(got["L0"] - st["L0"]) <= 1e-10
+
+
 def test_flow_with_weighted_out_degree_hubs(built_lib, oracle_mod):
     """Rows of more than 256 out-links are normalised, turned into edge flows
     and summed into singleton exits by a whole warp (the reference sums them
