@@ -471,12 +471,14 @@ __global__ void k_src_remap(int64_t m, const int32_t *in_src, const int32_t *ran
         gsrc[k] = rank[in_src[k]];
 }
 
-// The gathered copy (PowGather) where the flow vector is larger than a
-// quarter of L2 and at most three quarters of the nodes have out-links;
-// otherwise none. In arena memory (released with the caller's mark).
+// The gathered copy (PowGather) where the flow vector is larger than three
+// quarters of L2 (smaller ones mostly stay there anyway: measured slower at
+// 2^22 nodes, the copy's set-up costing more than it saved) and at most three
+// quarters of the nodes have out-links; otherwise none. In arena memory
+// (released with the caller's mark).
 static PowGather gather_copy(int32_t n, const int64_t *in_off, const int32_t *in_src, Arena &ar, cudaStream_t s) {
     PowGather pg;
-    constexpr int64_t kMinNodes = (int64_t)32 << 20 >> 3;  // 32 MB of doubles
+    constexpr int64_t kMinNodes = (int64_t)96 << 20 >> 3;  // 96 MB of doubles
     if ((int64_t)n < kMinNodes) return pg;
     int64_t m = 0;
     RMX_CUDA(cudaMemcpyAsync(&m, in_off + n, sizeof(int64_t), cudaMemcpyDeviceToHost, s));

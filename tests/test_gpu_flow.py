@@ -116,19 +116,20 @@ def test_flow_with_in_degree_hubs(built_lib, oracle_mod):
 
 
 def test_flow_gathered_copy(built_lib, oracle_mod):
-    """A flow vector above 32 MB (2^22 nodes) of which half the nodes have no
+    """A flow vector above 96 MB (2^24 nodes) of which half the nodes have no
     out-link: the pull gathers from the compact copy of the out-linked nodes'
     flows. The iteration count matches the oracle's one-thread steady state on
     the library's own prepared links, and the flow matches a restatement of
     the same iteration with scipy's sparse product and numpy's pairwise sums
-    to 1e-12 relative L1. At this size the oracle's serial FP64 sums of 4M
-    terms (the reference's loop) are themselves off: its flow differs from the
-    same iteration with exactly rounded sums by 8.6e-12 (the pairwise one by
-    2e-17), so against the oracle the bar is 1e-10."""
+    to 1e-12 relative L1. At this size the oracle's serial FP64 sums of
+    millions of terms (the reference's loop) are themselves off (at 2^22 nodes
+    its flow differs from the same iteration with exactly rounded sums by
+    8.6e-12, the pairwise one by 2e-17), so against the oracle the bar is
+    1e-10."""
     import scipy.sparse as sparse
     from relaxmap_b200 import Graph
     O = oracle_mod
-    n, m = 1 << 22, 8_000_000
+    n, m = 1 << 24, 12_000_000
     rng = np.random.default_rng(21)
     src = rng.integers(0, n // 2, m)
     dst = rng.integers(0, n, m)
