@@ -118,14 +118,15 @@ def test_flow_with_in_degree_hubs(built_lib, oracle_mod):
 def test_flow_gathered_copy(built_lib, oracle_mod):
     """A flow vector above 96 MB (2^24 nodes) of which half the nodes have no
     out-link: the pull gathers from the compact copy of the out-linked nodes'
-    flows. The iteration count matches the oracle's one-thread steady state on
-    the library's own prepared links, and the flow matches a restatement of
-    the same iteration with scipy's sparse product and numpy's pairwise sums
-    to 1e-12 relative L1. At this size the oracle's serial FP64 sums of
+    flows. The flow matches a restatement of the same iteration (as many
+    sweeps) with scipy's sparse product and numpy's pairwise sums to 1e-12
+    relative L1, and the oracle's one-thread steady state on the library's own
+    prepared links to 1e-10. At this size the oracle's serial FP64 sums of
     millions of terms (the reference's loop) are themselves off (at 2^22 nodes
     its flow differs from the same iteration with exactly rounded sums by
-    8.6e-12, the pairwise one by 2e-17), so against the oracle the bar is
-    1e-10."""
+    8.6e-12, the pairwise one by 2e-17), and its L1 change never falls to the
+    1e-15 stop threshold, so it runs the 200-sweep cap where the GPU stops
+    at the rule's 50."""
     import scipy.sparse as sparse
     from relaxmap_b200 import Graph
     O = oracle_mod
@@ -137,7 +138,7 @@ def test_flow_gathered_copy(built_lib, oracle_mod):
         off, dst_k, w, tw = G.links()
         got = G.initiate()
     st = O.initiate(O.Prepared(n, off, dst_k, w, tw))
-    assert got["iters"] == st["iters"]
+    assert 50 <= got["iters"] <= st["iters"]
     # the reference's iteration (Module.cpp:340-469) with scipy's product
     s = np.repeat(np.arange(n), np.diff(off))
     outw = np.bincount(s, weights=w, minlength=n)
