@@ -222,7 +222,10 @@ constexpr int kBins = 8;
 constexpr int kBinReg8 = 0, kBinReg16 = 1, kBinReg32 = 2, kBinWarp = 3, kBinMid = 4, kBinBlock = 5, kBinLarge = 6,
               kBinHub = 7;
 // units of 129..512 links: four warps each (eight teams per SM), a 1024-slot table
-constexpr int kMidT = 128, kMidMaxDeg = 512, kMidCap = 1024;
+#ifndef RMX_MID_CAP
+#define RMX_MID_CAP 1024
+#endif
+constexpr int kMidT = 128, kMidCap = RMX_MID_CAP, kMidMaxDeg = kMidCap / 2, kMidDefault = 512;
 constexpr int kBlkT = 256, kBlkMaxDeg = 1024, kBlkCap = 2048;
 // resident blocks per SM of the block bin; default grid caps of the block, warp and register bins
 #ifndef RMX_BLK_MINB
@@ -1502,7 +1505,7 @@ void hub_level_needs(const Level &L, int64_t *out, int64_t *dev_tmp, cudaStream_
 
 namespace {
 EvalTuning g_tuning{8,           RMX_BLK_GRID, RMX_LRG_MINB, RMX_WARP_GRID, RMX_REG_GRID,
-                    kWarpMaxDeg, kMidMaxDeg,   kBlkMaxDeg,   kLrgMaxDeg,    kPartLinks};
+                    kWarpMaxDeg, kMidDefault,  kBlkMaxDeg,   kLrgMaxDeg,    kPartLinks};
 int g_tuning_gen = 0;
 std::mutex g_tuning_mu;  // guards g_tuning and g_tuning_gen
 }  // namespace
