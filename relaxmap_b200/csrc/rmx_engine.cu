@@ -500,7 +500,7 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     const int64_t Ein = std::max<int64_t>(n_edges, 1), Eb = std::max<int64_t>(repl ? u->full_edges : n_edges, 1);
     scratch.init((size_t)(88 * Eb + 24 * (int64_t)n + 40 * (int64_t)K) + (64u << 20));
     // long-lived arrays: node CSR/CSC, three levels, module and instance state
-    perm.init((size_t)(156 * Eb + 568 * (int64_t)n + (K > 1 ? 16 * (int64_t)n + 64 * (int64_t)K : 0)) + (64u << 20));
+    perm.init((size_t)(156 * Eb + 696 * (int64_t)n + (K > 1 ? 16 * (int64_t)n + 64 * (int64_t)K : 0)) + (64u << 20));
     out_off = perm.alloc<int64_t>(n + 1);
     in_off = perm.alloc<int64_t>(n + 1);
     int32_t *d_src = scratch.alloc<int32_t>(Ein), *d_dst = scratch.alloc<int32_t>(Ein);
@@ -649,6 +649,7 @@ void rmx_graph::alloc_engine() {
         M->cap = n;
         M->stat = perm.alloc<Stat4>(n);
         M->term = perm.alloc<double2>(n);
+        M->rec = perm.alloc<ModRec>(n);
         M->count = perm.alloc<int32_t>(n);
         M->inst = perm.alloc<int32_t>(n);
     }

@@ -32,10 +32,20 @@ struct Level {
     int32_t *nnodes = nullptr;  // original nodes inside each unit
 };
 
+// A module's statistics and cached terms in one 64-byte record (two sectors
+// of one 128-byte line): what the move evaluation reads per candidate, so a
+// candidate costs one random line instead of one in each of two arrays.
+struct __align__(64) ModRec {
+    Stat4 s;
+    double2 t;
+    double2 pad;
+};
+
 struct ModState {
     int32_t cap = 0;
     Stat4 *stat = nullptr;
     double2 *term = nullptr;    // cached {plogp(exit), plogp(exit + P)} of each module
+    ModRec *rec = nullptr;      // stat and term together, written with term (read by the evaluation)
     int32_t *count = nullptr;   // units of the current level in the module
     int32_t *inst = nullptr;
 };

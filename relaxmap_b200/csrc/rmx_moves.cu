@@ -94,7 +94,9 @@ __device__ __forceinline__ double plogp_total(const UnitCtx &c, double dm) {
 // unit terms in K. The out- and in-flows (Module.cpp:1058, :1059) enter the
 // change only through their sum (the new exit, :1104), so the tables keep one
 // sum per module. t = the module's cached {plogp(exit), plogp(exit + P)}.
-__device__ __forceinline__ double candidate_delta(const UnitCtx &c, const Stat4 &st, const double2 t, fx_t sfx) {
+__device__ __forceinline__ double candidate_delta(const UnitCtx &c, const ModRec &r, fx_t sfx) {
+    const Stat4 &st = r.s;
+    const double2 t = r.t;
     const double P = from_fx(st.P), TW = from_fx(st.TW), D = from_fx(st.D), OUT = from_fx(st.OUT);
     const double em = exit_flow(P, TW, D, OUT);
     const double om_im = kBeta * from_fx(sfx) + c.cu * TW + (kAlpha * P + kBeta * D) * c.tu;  // :1058 + :1059
@@ -109,8 +111,10 @@ __device__ __forceinline__ double newmod_delta(const UnitCtx &c) {
     return plogp_total(c, nexm) + c.K - 2.0 * plogp(nexm) + plogp(nexm + c.pu);
 }
 
-__device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const Stat4 &ma, const double2 tA, double sum_exit,
-                                            int32_t A, fx_t sA) {
+__device__ __forceinline__ UnitCtx make_ctx(const Stat4 &ua, const ModRec &mA, double sum_exit, int32_t A,
+                                            fx_t sA) {
+    const Stat4 &ma = mA.s;
+    const double2 tA = mA.t;
     UnitCtx c;
     c.pu = from_fx(ua.P);
     c.tu = from_fx(ua.TW);
@@ -145,8 +149,7 @@ struct EvalArgs {
     const Stat4 *attr;
     const int32_t *mod, *uinst;
     // modules / instances
-    const Stat4 *mstat;
-    const double2 *mterm;
+    const ModRec *mrec;     // per module: statistics and cached terms
     const int32_t *mcount;
     const double *inst_sum_exit;
     const uint8_t *inst_active;
@@ -357,7 +360,7 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
     gsync<NT>();
     const int32_t A = a.mod[u];
     const int sA = tab_find(keys, mask, A);
-    const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A,
+    const UnitCtx c = make_ctx(a.attr[u], a.mrec[A], a.inst_sum_exit[a.uinst[u]], A,
                                sA >= 0 ? vals[sA] : 0);
     if (NT > 32) __syncthreads();  // every lookup is done before slots are overwritten
     // Each warp compacts its own contiguous slice of the table in place (the
@@ -396,7 +399,7 @@ __device__ __forceinline__ void eval_unit(const EvalArgs &a, const int32_t u, co
         const fx_t v = vals[lo + q];
         keys[lo + q] = kEmpty;
         vals[lo + q] = 0;
-        const double dl = candidate_delta(c, a.mstat[m], a.mterm[m], v);
+        const double dl = candidate_delta(c, a.mrec[m], v);
         if (better(dl, m, best, bm)) {
             best = dl;
             bm = m;
@@ -499,9 +502,9 @@ __device__ __forceinline__ void eval_unit_reg(const EvalArgs &a, const int32_t u
     int32_t bm = INT_MAX;
     UnitCtx c;
     if (valid) {
-        c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, sA);
+        c = make_ctx(a.attr[u], a.mrec[A], a.inst_sum_exit[a.uinst[u]], A, sA);
         if (tail && key != A) {
-            best = candidate_delta(c, a.mstat[key], a.mterm[key], v);
+            best = candidate_delta(c, a.mrec[key], v);
             bm = key;
         }
     }
@@ -926,7 +929,7 @@ __global__ void __launch_bounds__(kHubPT, RMX_HUB_MINB) k_hub_eval(EvalArgs a, H
         const int32_t u = a.list[h0 + j];
         const int64_t b0 = p.pstart[pidx], b1 = p.pstart[pidx + 1];
         const int32_t A = a.mod[u];
-        const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A, p.own[j]);
+        const UnitCtx c = make_ctx(a.attr[u], a.mrec[A], a.inst_sum_exit[a.uinst[u]], A, p.own[j]);
         double best = 0.0;
         int32_t bm = INT_MAX;
         for (uint32_t R = 1;; R <<= 1) {  // R rounds; more only when a round overfills the table
@@ -963,7 +966,7 @@ __global__ void __launch_bounds__(kHubPT, RMX_HUB_MINB) k_hub_eval(EvalArgs a, H
                     const int32_t k = keys[s];
                     if (!overfull && k != A) {
                         rc++;
-                        const double dl = candidate_delta(c, a.mstat[k], a.mterm[k], vals[s]);
+                        const double dl = candidate_delta(c, a.mrec[k], vals[s]);
                         if (better(dl, k, rbest, rbm)) {
                             rbest = dl;
                             rbm = k;
@@ -1046,7 +1049,7 @@ __global__ void k_hub_finish(EvalArgs a, HubPlan p) {
         }
         if (lane == 0) {
             const int32_t A = a.mod[u];
-            const UnitCtx c = make_ctx(a.attr[u], a.mstat[A], a.mterm[A], a.inst_sum_exit[a.uinst[u]], A,
+            const UnitCtx c = make_ctx(a.attr[u], a.mrec[A], a.inst_sum_exit[a.uinst[u]], A,
                                        p.own[j]);
             p.act[j] = (uint8_t)finish_unit(a, u, c, best, bm);
             seen += unit_links(a, u);
@@ -1267,20 +1270,30 @@ __device__ __forceinline__ double2 module_terms(const Stat4 &st) {
     return make_double2(plogp(e), plogp(e + P));
 }
 
-__global__ void k_terms_all(int32_t cap, const Stat4 *mstat, double2 *term) {
+// A module's cached terms and its evaluation record.
+__device__ __forceinline__ void write_terms(const Stat4 *mstat, double2 *term, ModRec *rec, int32_t m) {
+    const Stat4 st = mstat[m];
+    const double2 t = module_terms(st);
+    term[m] = t;
+    rec[m].s = st;
+    rec[m].t = t;
+}
+
+__global__ void k_terms_all(int32_t cap, const Stat4 *mstat, double2 *term, ModRec *rec) {
     for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < cap; m += (int64_t)gridDim.x * blockDim.x)
-        term[m] = module_terms(mstat[m]);
+        write_terms(mstat, term, rec, (int32_t)m);
 }
 
 void refresh_terms(ModState &M, cudaStream_t s) {
-    k_terms_all<<<blocks_for(M.cap, 256, num_sms() * 32), 256, 0, s>>>(M.cap, M.stat, M.term);
+    k_terms_all<<<blocks_for(M.cap, 256, num_sms() * 32), 256, 0, s>>>(M.cap, M.stat, M.term, M.rec);
     RMX_LAUNCHED();
 }
 
 // After a sub-batch: the two modules of every mover get fresh cached terms
 // (a module touched by several movers is written with the same value).
 __global__ void k_terms_movers(const int32_t *list, const int64_t *range, const uint32_t *stamp_of, const uint32_t *sp,
-                               const int32_t *mod, const int32_t *prevmod, const Stat4 *mstat, double2 *term) {
+                               const int32_t *mod, const int32_t *prevmod, const Stat4 *mstat, double2 *term,
+                               ModRec *rec) {
     const uint32_t stamp = sp[0];
     const int64_t beg = range[0], end = range[1];
     for (int64_t i = beg + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < end;
@@ -1288,8 +1301,8 @@ __global__ void k_terms_movers(const int32_t *list, const int64_t *range, const 
         const int32_t u = list[i];
         if (stamp_of[u] != stamp) continue;
         const int32_t A = prevmod[u], T = mod[u];
-        term[A] = module_terms(mstat[A]);
-        term[T] = module_terms(mstat[T]);
+        write_terms(mstat, term, rec, A);
+        write_terms(mstat, term, rec, T);
     }
 }
 
@@ -1447,8 +1460,7 @@ static EvalArgs eval_args(const Level &L, const ModState &M, const InstState &I,
     a.attr = L.attr;
     a.mod = L.mod;
     a.uinst = L.inst;
-    a.mstat = M.stat;
-    a.mterm = M.term;
+    a.mrec = M.rec;
     a.mcount = M.count;
     a.inst_sum_exit = I.sum_exit;
     a.inst_active = I.active;
@@ -1862,7 +1874,8 @@ void sweep_subbatch(const Level &L, ModState &M, const InstState &I, SweepWork &
         k_delta_block<<<fitted ? fit_grid(n_heavy, 1, num_sms() * 4) : num_sms() * 4, 256, 0, s>>>(da);
         RMX_LAUNCHED();
     }
-    k_terms_movers<<<G, 256, 0, s>>>(W.list2, W.ranges + 2 * sb, W.stamp, sp, L.mod, W.prevmod, M.stat, M.term);
+    k_terms_movers<<<G, 256, 0, s>>>(W.list2, W.ranges + 2 * sb, W.stamp, sp, L.mod, W.prevmod, M.stat, M.term,
+                                     M.rec);
     RMX_LAUNCHED();
     if (tm) tm->end(kTimerCommit, s);
 }
