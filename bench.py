@@ -202,7 +202,7 @@ def peaks() -> dict:
 # evaluation snapshot of the benched graph (--eval-snapshot: every node against
 # singleton modules), divided by the links that launch read; the command and
 # the counters are in profiles/eval_large_rmat24.md.
-EVAL_TRAFFIC_PER_LINK = {("rmat24", "large"): (17.10e9 + 6.19e6) / 97_860_671}
+EVAL_TRAFFIC_PER_LINK = {("rmat24", "large"): (9.31e9 + 6.87e6) / 97_860_671}
 
 DOMINANT_BIN = "large"
 
