@@ -607,7 +607,11 @@ void rmx_graph::create(const int32_t *src, const int32_t *dst, const double *w, 
     RMX_CUDA(cudaStreamSynchronize(stream));
     // SpMV sub-warp width from the mean in-degree
     const double avg = (double)E / n;
+#ifdef RMX_SPMV_VEC
+    spmv_vec = RMX_SPMV_VEC;  // a build option for timing other widths
+#else
     spmv_vec = spmv_width(avg);
+#endif
 }
 
 void rmx_graph::alloc_engine() {

@@ -695,9 +695,10 @@ int power_iteration_components(int32_t n, int32_t n_comp, const int64_t *comp, c
 
 // About 2.5 links per lane: more rows in flight per warp hide the gather
 // latency better than idle lanes do (mean in-degree 20: 8 lanes, 6.7 ms
-// against 9.2 ms with 16 lanes for 50 iterations on 19.5M links).
+// against 9.2 ms with 16 lanes for 50 iterations on 19.5M links; R-MAT scale
+// 24, mean 15.7: 4 lanes 7% faster than 8, 16 lanes 10% slower).
 int spmv_width(double mean_in_degree) {
-    return mean_in_degree <= 12 ? 4 : (mean_in_degree <= 24 ? 8 : (mean_in_degree <= 48 ? 16 : 32));
+    return mean_in_degree <= 16 ? 4 : (mean_in_degree <= 24 ? 8 : (mean_in_degree <= 48 ? 16 : 32));
 }
 
 int power_iteration(int32_t n, const int64_t *in_off, const int32_t *in_src, const double *in_w, const double *tw,
