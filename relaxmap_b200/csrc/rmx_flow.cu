@@ -307,6 +307,8 @@ __global__ void __launch_bounds__(kPowT, RMX_POW_MINB) k_power(const int64_t *__
     double *Sp = parts, *Dp = parts + nb, *Ep = parts + 2 * nb;
     const int64_t gtid = (int64_t)blockIdx.x * kPowT + threadIdx.x, gthreads = (int64_t)nb * kPowT;
 
+    // the link arrays are streamed with the evict-first hint so that the
+    // gathered vector stays in L2 between iterations
     const double *xg = pg.gsrc ? pg.xc : x;        // the vector the pull gathers from
     const int32_t *gs = pg.gsrc ? pg.gsrc : in_src;  // and the links' places in it
     double dl = 0.0;
@@ -337,7 +339,7 @@ __global__ void __launch_bounds__(kPowT, RMX_POW_MINB) k_power(const int64_t *__
                 const int64_t b = in_off[r], e = in_off[r + 1];
                 mine = e - b <= sp.heavy_deg;
                 if (mine)
-                    for (int64_t k = b + lv; k < e; k += VEC) acc += beta * in_w[k] * __ldcg(xg + gs[k]);
+                    for (int64_t k = b + lv; k < e; k += VEC) acc += beta * __ldcs(in_w + k) * __ldcg(xg + __ldcs(gs + k));
             }
 #pragma unroll
             for (int o = VEC / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
@@ -351,7 +353,7 @@ __global__ void __launch_bounds__(kPowT, RMX_POW_MINB) k_power(const int64_t *__
             for (int64_t c = gwarp; c < sp.n_chunks; c += nwarps) {
                 double acc = 0.0;
                 for (int64_t k = sp.chunk_beg[c] + lane; k < sp.chunk_end[c]; k += 32)
-                    acc += beta * in_w[k] * __ldcg(xg + gs[k]);
+                    acc += beta * __ldcs(in_w + k) * __ldcg(xg + __ldcs(gs + k));
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
                 if (lane == 0) sp.cpart[c] = acc;
