@@ -312,8 +312,9 @@ __device__ __forceinline__ void insert_links(const EvalArgs &a, int64_t ob, int6
             if (j < d) {
                 const bool isout = j < dout;
                 const int64_t e = isout ? ob + j : ib + (j - dout);
-                key[k] = __ldg(isout ? a.out_dst + e : a.in_src + e);
-                q[k] = __ldg(isout ? a.out_fx + e : a.in_fx + e);
+                // links are streamed (evict-first) so that the module ids they point to stay in L2
+                key[k] = __ldcs(isout ? a.out_dst + e : a.in_src + e);
+                q[k] = __ldcs(isout ? a.out_fx + e : a.in_fx + e);
             }
         }
 #pragma unroll
@@ -798,8 +799,8 @@ __device__ __forceinline__ void hub_link(const EvalArgs &a, int64_t ob, int64_t 
                                          int32_t &key, fx_t &q) {
     const bool in = l >= dout;
     const int64_t e = in ? ib + (l - dout) : ob + l;
-    key = __ldg(a.mod + __ldg(in ? a.in_src + e : a.out_dst + e));
-    q = __ldg(in ? a.in_fx + e : a.out_fx + e);
+    key = __ldg(a.mod + __ldcs(in ? a.in_src + e : a.out_dst + e));  // links streamed, module ids kept
+    q = __ldcs(in ? a.in_fx + e : a.out_fx + e);
 }
 
 // Count (scatter = false) or place (scatter = true) the links of the chunks.
