@@ -250,9 +250,9 @@ __global__ void k_agg_gather(int64_t m, const int32_t *src, const int32_t *dst, 
         int32_t g = -1, b = -1;
         fx_t q = 0;
         if (e < m) {
-            g = __ldg(group + __ldg(src + e));
-            b = __ldg(group + __ldg(dst + e));
-            q = __ldg(fx + e);
+            g = __ldg(group + __ldcs(src + e));  // links streamed, group ids kept in L2
+            b = __ldg(group + __ldcs(dst + e));
+            q = __ldcs(fx + e);
             if (b == g) g = -1;  // links inside a group are not kept
         }
         const unsigned peers = __match_any_sync(kFullMask, g);

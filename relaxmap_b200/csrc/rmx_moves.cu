@@ -465,9 +465,9 @@ __device__ __forceinline__ void eval_unit_reg(const EvalArgs &a, const int32_t u
         if (gl < d) {
             const bool isout = gl < dout;
             const int64_t e = isout ? ob + gl : ib + (gl - dout);
-            nbr = isout ? a.out_dst[e] : a.in_src[e];
-            key = a.mod[nbr];
-            v = isout ? a.out_fx[e] : a.in_fx[e];
+            nbr = __ldcs(isout ? a.out_dst + e : a.in_src + e);  // links streamed, module ids kept
+            key = __ldg(a.mod + nbr);
+            v = __ldcs(isout ? a.out_fx + e : a.in_fx + e);
         }
     }
     // bitonic sort of (key, flow) by key within the group
