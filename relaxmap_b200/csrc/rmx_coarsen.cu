@@ -845,94 +845,6 @@ __global__ void k_agg_transpose(int64_t m, const int32_t *out_src, const int32_t
     }
 }
 
-// Columns of many in-links (hub super-nodes) are not placed by one atomic
-// per link: a row lists distinct destinations, so the lanes of a warp rarely
-// share a column, and every in-link of a hub column would queue on the same
-// counter and wait for its return. Instead (k_agg_transpose_hot) a block
-// takes a tile of kTrTile links, ranks the links of each hot column inside
-// the tile with shared-memory counters, reserves the tile's share of every
-// hot column it touched with one atomic, and places them; other columns as
-// in k_agg_transpose. At most kHotMax hot columns: those of at least 2^t
-// in-links, t the smallest from kHotMinLog2 up that leaves no more.
-constexpr int kTrTile = 4096, kHotMax = 4096, kHotMinLog2 = 10;
-constexpr size_t kTrSmem = (size_t)kHotMax * (sizeof(unsigned int) + sizeof(unsigned long long)) +
-                           (size_t)kTrTile * sizeof(int32_t);
-
-// hist[k]: columns of 2^k .. 2^(k+1)-1 in-links (k < 48).
-__global__ void k_col_hist(int32_t ng, const int64_t *g_in_off, unsigned long long *hist) {
-    __shared__ unsigned int h[48];
-    for (int k = threadIdx.x; k < 48; k += blockDim.x) h[k] = 0;
-    __syncthreads();
-    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < ng; b += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t c = g_in_off[b + 1] - g_in_off[b];
-        if (c > 0) atomicAdd(h + (63 - __clzll(c)), 1u);
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < 48; k += blockDim.x)
-        if (h[k]) atomicAdd(hist + k, (unsigned long long)h[k]);
-}
-
-// hidx[b]: the hot index of column b (at least T in-links), else -1; hot[h] = b.
-__global__ void k_col_hot(int32_t ng, const int64_t *g_in_off, int64_t T, int32_t *hidx, int32_t *hot,
-                          unsigned long long *nhot) {
-    for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < ng; b += (int64_t)gridDim.x * blockDim.x) {
-        int32_t h = -1;
-        if (g_in_off[b + 1] - g_in_off[b] >= T) {
-            h = (int32_t)atomicAdd(nhot, 1ull);
-            hot[h] = (int32_t)b;
-        }
-        hidx[b] = h;
-    }
-}
-
-__global__ void __launch_bounds__(256) k_agg_transpose_hot(int64_t m, const int32_t *out_src, const int32_t *out_dst,
-                                                           const fx_t *out_fx, const int64_t *g_in_off,
-                                                           unsigned long long *colfill, const int32_t *hidx,
-                                                           const int32_t *hot, int nh, int32_t *in_src, fx_t *in_fx) {
-    extern __shared__ __align__(16) unsigned char tr_smem[];  // kTrSmem bytes
-    unsigned long long *sbase = reinterpret_cast<unsigned long long *>(tr_smem);
-    unsigned int *scnt = reinterpret_cast<unsigned int *>(sbase + kHotMax);
-    int32_t *rk = reinterpret_cast<int32_t *>(scnt + kHotMax);
-    const int lane = threadIdx.x & 31;
-    for (int64_t t0 = (int64_t)blockIdx.x * kTrTile; t0 < m; t0 += (int64_t)gridDim.x * kTrTile) {
-        __syncthreads();  // the previous tile's readers of sbase are done
-        for (int h = threadIdx.x; h < nh; h += blockDim.x) scnt[h] = 0;
-        __syncthreads();
-        for (int i0 = 0; i0 < kTrTile; i0 += blockDim.x) {  // uniform over the block
-            const int i = i0 + threadIdx.x;
-            const int64_t e = t0 + i;
-            int32_t b = e < m ? out_dst[e] : -1;
-            const int32_t h = b >= 0 ? hidx[b] : -1;
-            rk[i] = h >= 0 ? (int32_t)atomicAdd(scnt + h, 1u) : -1;
-            if (h >= 0) b = -1;  // placed below
-            const unsigned peers = __match_any_sync(kFullMask, b);
-            const int leader = __ffs(peers) - 1;
-            unsigned long long base = 0;
-            if (b >= 0 && lane == leader) base = atomicAdd(colfill + b, (unsigned long long)__popc(peers));
-            base = __shfl_sync(kFullMask, base, leader);
-            if (b >= 0) {
-                const int64_t q = g_in_off[b] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
-                in_src[q] = out_src[e];
-                in_fx[q] = out_fx[e];
-            }
-        }
-        __syncthreads();
-        for (int h = threadIdx.x; h < nh; h += blockDim.x) {
-            const unsigned int c = scnt[h];
-            if (c) sbase[h] = atomicAdd(colfill + hot[h], (unsigned long long)c);
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < kTrTile; i += blockDim.x) {
-            if (rk[i] < 0) continue;
-            const int64_t e = t0 + i;
-            const int32_t b = out_dst[e];
-            const int64_t q = g_in_off[b] + (int64_t)sbase[hidx[b]] + rk[i];
-            in_src[q] = out_src[e];
-            in_fx[q] = out_fx[e];
-        }
-    }
-}
-
 // The block bin's and the split pipeline's dynamic shared memory, set once per device.
 static void configure_agg_kernels() {
     static std::mutex mu;
@@ -945,7 +857,6 @@ static void configure_agg_kernels() {
     const int smem = (int)(kAggCap * (sizeof(fx_t) + sizeof(int32_t)));
     RMX_CUDA(cudaFuncSetAttribute(k_agg_block, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     RMX_CUDA(cudaFuncSetAttribute(k_hg_reduce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kHgSmem));
-    RMX_CUDA(cudaFuncSetAttribute(k_agg_transpose_hot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrSmem));
     done[dev] = true;
 }
 
@@ -1112,31 +1023,9 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     scan_exclusive(g_in_off, g_in_off, ng + 1, nullptr, ar, s);
     RMX_CUDA(cudaMemsetAsync(gcross, 0, sizeof(unsigned long long) * (ng + 1), s));  // the column fill counters
     if (m > 0) {
-        // hot columns: the fewest in-links 2^t (t >= kHotMinLog2) that leave at most kHotMax of them
-        unsigned long long *hist = reinterpret_cast<unsigned long long *>(ar.alloc<int64_t>(49));
-        RMX_CUDA(cudaMemsetAsync(hist, 0, sizeof(unsigned long long) * 49, s));
-        k_col_hist<<<blocks_for(ng, 256, num_sms() * 8), 256, 0, s>>>(ng, g_in_off, hist);
+        const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
+        k_agg_transpose<<<Gm, 256, 0, s>>>(m, g_out_src, g_out_dst, g_out_fx, g_in_off, gcross, g_in_src, g_in_fx);
         RMX_LAUNCHED();
-        unsigned long long hh[48];
-        RMX_CUDA(cudaMemcpyAsync(hh, hist, sizeof hh, cudaMemcpyDeviceToHost, s));
-        RMX_CUDA(cudaStreamSynchronize(s));
-        int t = 47;
-        unsigned long long above = 0;  // columns of at least 2^t in-links
-        while (t > kHotMinLog2 && above + hh[t - 1] <= (unsigned long long)kHotMax) above += hh[--t];
-        if (t == 47 || above == 0) {
-            const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
-            k_agg_transpose<<<Gm, 256, 0, s>>>(m, g_out_src, g_out_dst, g_out_fx, g_in_off, gcross, g_in_src, g_in_fx);
-            RMX_LAUNCHED();
-        } else {
-            int32_t *hidx = ar.alloc<int32_t>(ng), *hot = ar.alloc<int32_t>(kHotMax);
-            k_col_hot<<<blocks_for(ng, 256, num_sms() * 16), 256, 0, s>>>(ng, g_in_off, (int64_t)1 << t, hidx, hot,
-                                                                            hist + 48);
-            RMX_LAUNCHED();
-            const unsigned Gt = (unsigned)std::min<int64_t>((m + kTrTile - 1) / kTrTile, num_sms() * 3);
-            k_agg_transpose_hot<<<Gt, 256, kTrSmem, s>>>(m, g_out_src, g_out_dst, g_out_fx, g_in_off, gcross, hidx, hot,
-                                                         (int)above, g_in_src, g_in_fx);
-            RMX_LAUNCHED();
-        }
     }
     RMX_CUDA(cudaStreamSynchronize(s));
     ar.release(mk);
