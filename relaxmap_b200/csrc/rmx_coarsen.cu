@@ -823,15 +823,17 @@ __global__ void k_agg_pack_long(const int64_t *gloff, const int64_t *g_out_off, 
     }
 }
 
-// In-links: every link g->b of the group CSR appended to column b.
+// In-links: every link g->b of the group CSR appended to column b, as one
+// 16-byte (row, flow) record in a staging array: one scattered store per
+// link instead of two partial-sector ones (k_agg_split then writes the CSC
+// arrays in order).
 __global__ void k_agg_transpose(int64_t m, const int32_t *out_src, const int32_t *out_dst, const fx_t *out_fx,
-                                const int64_t *g_in_off, unsigned long long *colfill, int32_t *in_src, fx_t *in_fx) {
+                                const int64_t *g_in_off, unsigned long long *colfill, longlong2 *staged) {
     const int lane = threadIdx.x & 31;
     const int64_t gw = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t e0 = gw * 32; e0 < m; e0 += nw * 32) {  // warp-uniform
         const int64_t e = e0 + lane;
-        const int32_t g = e < m ? out_src[e] : -1;
-        const int32_t b = e < m ? out_dst[e] : -1;
+        const int32_t b = e < m ? __ldcs(out_dst + e) : -1;
         const unsigned peers = __match_any_sync(kFullMask, b);
         const int leader = __ffs(peers) - 1;
         unsigned long long base = 0;
@@ -839,9 +841,16 @@ __global__ void k_agg_transpose(int64_t m, const int32_t *out_src, const int32_t
         base = __shfl_sync(kFullMask, base, leader);
         if (b >= 0) {
             const int64_t q = g_in_off[b] + (int64_t)base + __popc(peers & ((1u << lane) - 1u));
-            in_src[q] = g;
-            in_fx[q] = out_fx[e];
+            staged[q] = make_longlong2((long long)__ldcs(out_src + e), (long long)__ldcs(out_fx + e));
         }
+    }
+}
+
+__global__ void k_agg_split(int64_t m, const longlong2 *staged, int32_t *in_src, fx_t *in_fx) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < m; q += (int64_t)gridDim.x * blockDim.x) {
+        const longlong2 r = __ldcs(staged + q);
+        in_src[q] = (int32_t)r.x;
+        in_fx[q] = (fx_t)r.y;
     }
 }
 
@@ -1024,7 +1033,10 @@ int64_t aggregate_links(int32_t n, const int64_t *off, const int32_t *dst, const
     RMX_CUDA(cudaMemsetAsync(gcross, 0, sizeof(unsigned long long) * (ng + 1), s));  // the column fill counters
     if (m > 0) {
         const unsigned Gm = blocks_for((m + 31) / 32 * 32, 256, num_sms() * 16);
-        k_agg_transpose<<<Gm, 256, 0, s>>>(m, g_out_src, g_out_dst, g_out_fx, g_in_off, gcross, g_in_src, g_in_fx);
+        longlong2 *staged = ar.alloc<longlong2>(m);
+        k_agg_transpose<<<Gm, 256, 0, s>>>(m, g_out_src, g_out_dst, g_out_fx, g_in_off, gcross, staged);
+        RMX_LAUNCHED();
+        k_agg_split<<<blocks_for(m, 256, num_sms() * 16), 256, 0, s>>>(m, staged, g_in_src, g_in_fx);
         RMX_LAUNCHED();
     }
     RMX_CUDA(cudaStreamSynchronize(s));
