@@ -329,8 +329,8 @@ void *rmx_graph_stream(const rmx_graph *g);
 rmx_status rmx_sync(rmx_graph *g);
 
 /* The device memory of a graph handle (and the scratch of an adjoint call)
- * is kept in a process-wide cache when the handle closes, up to a quarter of
- * each device's memory: the next handle or call of similar size (a cached
+ * is kept in a process-wide cache when the handle closes, up to half of each
+ * device's memory: the next handle or call of similar size (a cached
  * block is reused for requests of at least half its size) takes it without a
  * cudaMalloc / cudaFree pair, and an allocation that fails empties the cache
  * and retries. This frees every cached block (all devices); handles still open

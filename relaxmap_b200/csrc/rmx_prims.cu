@@ -40,7 +40,7 @@ size_t cache_budget() {
         (void)cudaGetLastError();
         return 0;
     }
-    return total_b / 4;
+    return total_b / 2;
 }
 
 // cudaFree the cached blocks of device dev (current), oldest first, until at
