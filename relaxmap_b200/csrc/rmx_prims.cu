@@ -346,45 +346,107 @@ __global__ void __launch_bounds__(kRsT) k_rs_hist(Dig dig, int64_t n, const int6
     for (int i = threadIdx.x; i < nb; i += kRsT) hist[(int64_t)i * ntiles + blockIdx.x] = cnt[i];
 }
 
+// The scatter stages half a tile (kRsHalf elements) in shared memory in
+// output order before writing it, so that each digit's run of the half leaves
+// as consecutive stores instead of one scattered store per element. Output
+// positions are those of the plain per-element scatter: input order within a
+// digit (rows, then warps, then lanes).
+constexpr int kRsRows = kRsI / 2, kRsHalf = kRsT * kRsRows;
+
 template <typename Dig, typename K, typename V>
 __global__ void __launch_bounds__(kRsT) k_rs_scatter(Dig dig, const K *kin, K *kout, const V *vin, V *vout, int64_t n,
                                                      const int64_t *n_dev, int nb, const unsigned *offs,
                                                      int64_t ntiles) {
-    __shared__ unsigned run[256];
+    __shared__ unsigned run[256];            // global output position of each digit's next element
+    __shared__ unsigned hc[256], hs[256];    // the half's count and start of each digit
+    __shared__ unsigned wc[kRsW][256];       // one row's count per warp and digit
+    __shared__ K skey[kRsHalf];
+    __shared__ V sval[kRsHalf];
+    __shared__ uint16_t sdig[kRsHalf];
     if (n_dev) n = *n_dev;
-    __shared__ unsigned wc[kRsW][256];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < 256; i += kRsT) {
         run[i] = i < nb ? offs[(int64_t)i * ntiles + blockIdx.x] : 0u;
+        hc[i] = 0;
 #pragma unroll
         for (int q = 0; q < kRsW; q++) wc[q][i] = 0;
     }
     __syncthreads();
     const unsigned lt = (1u << lane) - 1u;
-    int64_t base = (int64_t)blockIdx.x * kRsTile;
-    for (int r = 0; r < kRsI; r++) {
-        int64_t e = base + (int64_t)r * kRsT + threadIdx.x;
-        bool valid = e < n;
-        unsigned d = valid ? dig(e) : 0x10000u;
-        unsigned peers = __match_any_sync(kFull, d);
-        unsigned rank = __popc(peers & lt);
-        if (valid && rank == 0) wc[w][d] = __popc(peers);
+    const int64_t base = (int64_t)blockIdx.x * kRsTile;
+    for (int half = 0; half < 2; half++) {
+        unsigned dg[kRsRows], lr[kRsRows];
+        for (int r = 0; r < kRsRows; r++) {
+            const int64_t e = base + (int64_t)(half * kRsRows + r) * kRsT + threadIdx.x;
+            const bool valid = e < n;
+            const unsigned d = valid ? dig(e) : 0x10000u;
+            const unsigned peers = __match_any_sync(kFull, d);
+            const unsigned rank = __popc(peers & lt);
+            if (valid && rank == 0) wc[w][d] = __popc(peers);
+            __syncthreads();
+            dg[r] = d;
+            if (valid) {
+                unsigned pos = hc[d] + rank;
+                for (int q = 0; q < w; q++) pos += wc[q][d];
+                lr[r] = pos;
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < nb; i += kRsT) {
+                unsigned t = 0;
+#pragma unroll
+                for (int q = 0; q < kRsW; q++) {
+                    t += wc[q][i];
+                    wc[q][i] = 0;
+                }
+                hc[i] += t;
+            }
+            __syncthreads();
+        }
+        // digit starts within the half (nb <= 256: one warp scans 8 per lane)
+        if (w == 0) {
+            unsigned v[8], t = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int i = lane * 8 + k;
+                v[k] = i < nb ? hc[i] : 0u;
+                t += v[k];
+            }
+            unsigned x = t;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(kFull, x, o);
+                if (lane >= o) x += y;
+            }
+            unsigned acc = x - t;
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                hs[lane * 8 + k] = acc;
+                acc += v[k];
+            }
+        }
         __syncthreads();
-        if (valid) {
-            unsigned pos = run[d] + rank;
-            for (int q = 0; q < w; q++) pos += wc[q][d];
-            if (kout) kout[pos] = kin[e];
-            vout[pos] = vin[e];
+        for (int r = 0; r < kRsRows; r++) {
+            const int64_t e = base + (int64_t)(half * kRsRows + r) * kRsT + threadIdx.x;
+            if (e < n) {
+                const unsigned q = hs[dg[r]] + lr[r];
+                if (kout) skey[q] = kin[e];
+                sval[q] = vin[e];
+                sdig[q] = (uint16_t)dg[r];
+            }
+        }
+        __syncthreads();
+        const int64_t rem = n - (base + (int64_t)half * kRsHalf);
+        const int cnt = rem <= 0 ? 0 : (rem < kRsHalf ? (int)rem : kRsHalf);
+        for (int q = threadIdx.x; q < cnt; q += kRsT) {
+            const unsigned d = sdig[q];
+            const unsigned g = run[d] + (unsigned)q - hs[d];
+            if (kout) kout[g] = skey[q];
+            vout[g] = sval[q];
         }
         __syncthreads();
         for (int i = threadIdx.x; i < nb; i += kRsT) {
-            unsigned t = 0;
-#pragma unroll
-            for (int q = 0; q < kRsW; q++) {
-                t += wc[q][i];
-                wc[q][i] = 0;
-            }
-            run[i] += t;
+            run[i] += hc[i];
+            hc[i] = 0;
         }
         __syncthreads();
     }
