@@ -733,14 +733,15 @@ void rmx_graph::ensure_hub_table(const Level &lv) {
                   Lk = std::max(links, work.hub_links) * 5 / 4 + 1024,
                   C = std::max(chunks, work.hub_chunks) * 5 / 4 + 64;
     work.hub_units = work.hub_parts = work.hub_links = work.hub_chunks = 0;
-    work.hub_bkey = nullptr;
-    const size_t bytes = (size_t)Lk * (sizeof(int32_t) + sizeof(fx_t)) + (size_t)(U + 1) * 3 * sizeof(int64_t) +
+    work.hub_bkey = work.hub_lkey = nullptr;
+    const size_t bytes = (size_t)Lk * (2 * sizeof(int32_t) + sizeof(fx_t)) + (size_t)(U + 1) * 3 * sizeof(int64_t) +
                          (size_t)U * (2 * sizeof(fx_t) + sizeof(int32_t) + 1) +
                          (size_t)P * (sizeof(unsigned long long) + sizeof(double) + sizeof(int32_t)) +
                          (size_t)(P + 1) * sizeof(int64_t) + (size_t)(C + P) * sizeof(int32_t) + 16 * 256;
     hub_arena.init(bytes);
     work.hub_bfx = hub_arena.alloc<fx_t>(Lk);
     work.hub_bkey = hub_arena.alloc<int32_t>(Lk);
+    work.hub_lkey = hub_arena.alloc<int32_t>(Lk);
     work.hub_coff = hub_arena.alloc<int64_t>(U + 1);
     work.hub_poff = hub_arena.alloc<int64_t>(U + 1);
     work.hub_loff = hub_arena.alloc<int64_t>(U + 1);

@@ -203,6 +203,7 @@ struct SweepWork {
     double *hub_best = nullptr;
     int32_t *hub_bmod = nullptr;
     int32_t *hub_bkey = nullptr;
+    int32_t *hub_lkey = nullptr;   // per hub link: its neighbour's module (count pass -> scatter pass)
     fx_t *hub_bfx = nullptr;
     int64_t *hub_tot = nullptr;
     std::vector<int64_t> bucket_host;  // host copy of bucket_off after bucket_units

@@ -684,6 +684,7 @@ struct HubPlan {
     double *best;                  // per partition: best change found
     int32_t *bmod;                 // per partition: its module
     int32_t *bkey;                 // bucket elements: module
+    int32_t *lkey;                 // per link (at loff + link): the neighbour's module, from the count pass
     fx_t *bfx;                     //   and flow
     int32_t *cunit, *punit;        // unit (index in the sub-batch) of every chunk item and partition
     int64_t *tot;                  // [0] chunks, [1] partitions, [2] units, [3] over capacity, [4] links
@@ -809,7 +810,8 @@ __device__ __forceinline__ void hub_link(const EvalArgs &a, int64_t ob, int64_t 
 // module that many of a hub's links reach takes one bucket element per warp
 // step instead of one per link (integer sums: exact in any order). Both
 // passes form the same groups (the same lanes read the same links), so the
-// counts hold the scatter exactly.
+// counts hold the scatter exactly. The count pass stores each link's module,
+// which the scatter pass reads back in order instead of gathering it again.
 template <bool SCATTER>
 __global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
     constexpr int ILP = 4;  // links gathered per thread before any is combined
@@ -826,6 +828,7 @@ __global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
         const int64_t ob = a.out_off[u], ib = a.in_off[u];
         const int64_t dout = a.out_off[u + 1] - ob, d = dout + (a.in_off[u + 1] - ib);
         const int64_t c0 = (item - p.coff[j]) * kHubCh, c1 = min(d, c0 + kHubCh);
+        int32_t *const lk = p.lkey + p.loff[j];  // the unit's links' modules
         if (!SCATTER) {
             if (threadIdx.x == 0) p.cunit[item] = j;
             if (c0 == 0)
@@ -840,7 +843,16 @@ __global__ void __launch_bounds__(kHubPT) k_hub_links(EvalArgs a, HubPlan p) {
                 const int64_t l = b0 + k * kHubPT + threadIdx.x;
                 keys[k] = A;  // lanes past the chunk: flow 0 to the own module
                 qs[k] = 0;
-                if (l < c1) hub_link(a, ob, ib, dout, l, keys[k], qs[k]);
+                if (l < c1) {
+                    if (!SCATTER) {
+                        hub_link(a, ob, ib, dout, l, keys[k], qs[k]);
+                        lk[l] = keys[k];
+                    } else {  // the module the count pass found: no second gather
+                        const bool in = l >= dout;
+                        keys[k] = __ldcs(lk + l);
+                        qs[k] = __ldcs(in ? a.in_fx + ib + (l - dout) : a.out_fx + ob + l);
+                    }
+                }
             }
 #pragma unroll
             for (int k = 0; k < ILP; k++) {
@@ -1599,6 +1611,7 @@ static void launch_eval(EvalArgs a, const int64_t *bucket_off, int first_bucket,
         hp.best = W.hub_best;
         hp.bmod = W.hub_bmod;
         hp.bkey = W.hub_bkey;
+        hp.lkey = W.hub_lkey;
         hp.bfx = W.hub_bfx;
         hp.tot = W.hub_tot;
         hp.max_units = W.hub_units;
