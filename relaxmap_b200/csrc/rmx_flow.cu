@@ -129,8 +129,7 @@ CsrBuild build_csr(int32_t n, int64_t n_edges, int32_t *d_src, int32_t *d_dst, d
     int64_t U = 0;
     RMX_CUDA(cudaMemcpyAsync(&U, cnt + 0, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
     RMX_CUDA(cudaStreamSynchronize(s));
-    int32_t *kept = head;  // heads no longer needed after k_sum_dups... (it is: read above, stream-ordered)
-    kept = ar.alloc<int32_t>(std::max<int64_t>(U, 1));
+    int32_t *kept = ar.alloc<int32_t>(std::max<int64_t>(U, 1));
     compact_flags(keep, U, kept, cnt + 1, ar, s);
     int32_t *lsrc = ar.alloc<int32_t>(std::max<int64_t>(U, 1));
     k_gather_kept<<<G, T, 0, s>>>(kept, cnt + 1, usrc, udst, uw, lsrc, out_dst, out_w0,
