@@ -181,7 +181,8 @@ int64_t coarsen_links(int32_t n, const int64_t *out_off, const int32_t *out_dst,
 //      to the start of the range;
 //   4. the rows are packed (teams of 8 lanes per row, a block per long row),
 //      every packed link's row written beside it, and transposed by a
-//      counting sort on the destination.
+//      counting sort on the destination (each link placed as one 16-byte
+//      (row, flow) record, then split into the CSC arrays in order).
 // No pass searches for the row of a link or walks a group's members.
 namespace rmx {
 
